@@ -1,0 +1,901 @@
+"""CPU restatement (numpy, float64 / float32) of loadpath's voxel SIMP inner loop.
+
+TEST INFRASTRUCTURE ONLY. This module is the oracle the CUDA path is checked
+against: only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+may import it, and only as the checker. The product package (loadpath_b200)
+never imports it and has no CPU fallback.
+
+Pinning: every function below is checked against golden vectors produced by
+the reference implementation itself (tests/golden/make_golden.py imports
+loadpath read-only and writes tests/golden/*.npz; tests/test_oracle_golden.py
+compares). Each function names the reference file:line whose algorithm it
+restates (paths are relative to the loadpath project root).
+
+Layouts follow the reference:
+- corner k of a cell sits at (k & 1, k >> 1 & 1, k >> 2 & 1)   (loadpath/fem.py:30)
+- node fields are (3, nx+1, ny+1, nz+1), component-major, C order (loadpath/mg.py:495-511)
+- cell fields are (nx, ny, nz)
+- a cell's 24 dofs are ordered 3 * corner + component          (loadpath/fem.py:127-145)
+"""
+from __future__ import annotations
+
+import numpy as np
+
+CORNERS = np.array([[(k >> 0) & 1, (k >> 1) & 1, (k >> 2) & 1] for k in range(8)])
+OFFS = [tuple(int(v) for v in c) for c in CORNERS]
+LMAX_SAFETY = 1.3          # loadpath/mg.py:81
+STALL = 100                # loadpath/mg.py:930
+
+
+# --------------------------------------------------------------------------
+# element (loadpath/fem.py:113-224)
+# --------------------------------------------------------------------------
+
+def elastic_c(nu: float) -> np.ndarray:
+    """Isotropic 6x6 elasticity at E = 1, engineering shear (loadpath/fem.py:113-124)."""
+    lam = nu / ((1 + nu) * (1 - 2 * nu))
+    mu = 1.0 / (2 * (1 + nu))
+    c = np.zeros((6, 6))
+    c[:3, :3] = lam
+    for i in range(3):
+        c[i, i] = lam + 2 * mu
+        c[3 + i, 3 + i] = mu
+    return c
+
+
+def _strain_rows(b, col, g):
+    """Fill the six strain rows for one displacement basis function whose
+    gradient is g = (gx, gy, gz); shear order xy, yz, zx (loadpath/fem.py:40)."""
+    gx, gy, gz = g
+    b[0, col] = gx
+    b[1, col + 1] = gy
+    b[2, col + 2] = gz
+    b[3, col] = gy
+    b[3, col + 1] = gx
+    b[4, col + 1] = gz
+    b[4, col + 2] = gy
+    b[5, col] = gz
+    b[5, col + 2] = gx
+
+
+def b_matrix(xi, eta, zeta) -> np.ndarray:
+    """6x24 strain-displacement of the unit cube at a natural point (loadpath/fem.py:127-145)."""
+    s = 2.0 * CORNERS - 1.0
+    b = np.zeros((6, 24))
+    for k in range(8):
+        gx = 0.25 * s[k, 0] * (1 + eta * s[k, 1]) * (1 + zeta * s[k, 2])
+        gy = 0.25 * s[k, 1] * (1 + xi * s[k, 0]) * (1 + zeta * s[k, 2])
+        gz = 0.25 * s[k, 2] * (1 + xi * s[k, 0]) * (1 + eta * s[k, 1])
+        _strain_rows(b, 3 * k, (gx, gy, gz))
+    return b
+
+
+def b_bubble(xi, eta, zeta) -> np.ndarray:
+    """6x9 strain of Wilson's incompatible modes (1 - x_m^2) (loadpath/fem.py:172-188)."""
+    x = (xi, eta, zeta)
+    b = np.zeros((6, 9))
+    for m in range(3):
+        g = [0.0, 0.0, 0.0]
+        g[m] = -4.0 * x[m]
+        _strain_rows(b, 3 * m, g)
+    return b
+
+
+def hex8_ke(nu: float, element: str = "im") -> np.ndarray:
+    """Unit-cube stiffness at E = 1 with 2x2x2 Gauss; "im" condenses the nine
+    bubble modes, "plain" is the trilinear brick; symmetrised
+    (loadpath/fem.py:191-224)."""
+    c = elastic_c(nu)
+    g = 1.0 / np.sqrt(3.0)
+    kuu = np.zeros((24, 24))
+    kua = np.zeros((24, 9))
+    kaa = np.zeros((9, 9))
+    for xi in (-g, g):
+        for eta in (-g, g):
+            for zeta in (-g, g):
+                b = b_matrix(xi, eta, zeta)
+                ba = b_bubble(xi, eta, zeta)
+                kuu += b.T @ c @ b * 0.125
+                kua += b.T @ c @ ba * 0.125
+                kaa += ba.T @ c @ ba * 0.125
+    if element == "plain":
+        k = kuu
+    elif element == "im":
+        k = kuu - kua @ np.linalg.solve(kaa, kua.T)
+    else:
+        raise ValueError(element)
+    return 0.5 * (k + k.T)
+
+
+# --------------------------------------------------------------------------
+# grid transfers (loadpath/mg.py:57-132)
+# --------------------------------------------------------------------------
+
+def child_prolongations() -> np.ndarray:
+    """P_k (8, 24, 24): coarse-cell dofs -> dofs of the child at CORNERS[k]
+    (loadpath/mg.py:57-75)."""
+    out = np.zeros((8, 24, 24))
+    for k in range(8):
+        for q in range(8):
+            pos = (CORNERS[k] + CORNERS[q]) / 2.0
+            for r in range(8):
+                w = np.prod(np.where(CORNERS[r] == 1, pos, 1.0 - pos))
+                if w:
+                    for i in range(3):
+                        out[k, 3 * q + i, 3 * r + i] = w
+    return out
+
+
+PK = child_prolongations()
+
+
+def prolong(c: np.ndarray) -> np.ndarray:
+    """Trilinear (..., n0, n1, n2) -> (..., 2n0-1, 2n1-1, 2n2-1) (loadpath/mg.py:84-108)."""
+    out = c
+    for ax in (-3, -2, -1):
+        out = np.moveaxis(out, ax, 0)
+        n = out.shape[0]
+        f = np.empty((2 * n - 1,) + out.shape[1:], out.dtype)
+        f[0::2] = out
+        f[1::2] = (out[:-1] + out[1:]) * out.dtype.type(0.5)
+        out = np.moveaxis(f, 0, ax)
+    return np.ascontiguousarray(out)
+
+
+def restrict(f: np.ndarray) -> np.ndarray:
+    """Transpose of prolong (loadpath/mg.py:111-132)."""
+    out = f
+    for ax in (-3, -2, -1):
+        out = np.moveaxis(out, ax, 0)
+        n = (out.shape[0] + 1) // 2
+        c = out[0::2].copy()
+        half = out[1::2] * out.dtype.type(0.5)
+        c[:n - 1] += half
+        c[1:n] += half
+        out = np.moveaxis(c, 0, ax)
+    return np.ascontiguousarray(out)
+
+
+def restrict_masked_residual(b, ax, m, cm, coarse_shape):
+    """restrict(((b - ax) * m) zero-padded to twice the coarse cells) * cm
+    (loadpath/mgops.py:753-763, with :666-711)."""
+    rf = np.zeros((3,) + tuple(2 * n - 1 for n in coarse_shape[1:]), b.dtype)
+    sx, sy, sz = b.shape[1:]
+    rf[:, :sx, :sy, :sz] = (b - ax) * m
+    return restrict(rf) * cm
+
+
+def prolong_add(xc, cm, m, x):
+    """x += prolong(xc * cm)[:, :x's nodes] * m (loadpath/mgops.py:766-773)."""
+    sx, sy, sz = x.shape[1:]
+    x += prolong(xc * cm)[:, :sx, :sy, :sz] * m
+    return x
+
+
+# --------------------------------------------------------------------------
+# levels and operators (loadpath/mg.py:174-387)
+# --------------------------------------------------------------------------
+
+def gather_cells(u, dims):
+    """(24, nx, ny, nz): the 24 corner dofs of every cell of a node field."""
+    nx, ny, nz = dims
+    out = np.empty((24, nx, ny, nz), u.dtype)
+    for k, (dx, dy, dz) in enumerate(OFFS):
+        out[3 * k:3 * k + 3] = u[:, dx:dx + nx, dy:dy + ny, dz:dz + nz]
+    return out
+
+
+def scatter_cells(f, out):
+    """out += f (24, cells) at every cell's corners."""
+    nx, ny, nz = f.shape[1:]
+    for k, (dx, dy, dz) in enumerate(OFFS):
+        out[:, dx:dx + nx, dy:dy + ny, dz:dz + nz] += f[3 * k:3 * k + 3]
+    return out
+
+
+class Level:
+    """One grid level (loadpath/mg.py:174-199).
+
+    kind "scaled": cell matrix e[c] * ke.  kind "weights": sum_k w[k, c] M_k
+    plus an explicit patch (patch_ijk, patch_k).  kind "explicit": k (24, 24,
+    cells).  The operator is mask * K * mask + (1 - mask)."""
+
+    def __init__(self, kind, dims, dtype):
+        self.kind = kind
+        self.dims = tuple(int(d) for d in dims)
+        self.dtype = np.dtype(dtype)
+        self.ke = self.e = self.mcat = self.w = None
+        self.patch_ijk = self.patch_k = self.k = None
+        self.mask = self.dinv = self.lmax = None
+
+    @property
+    def node_shape(self):
+        return (3,) + tuple(d + 1 for d in self.dims)
+
+    def cell_products(self, cells24):
+        """(24, cells) products of every cell's matrix with its gathered dofs
+        (loadpath/mg.py:213-230)."""
+        flat = cells24.reshape(24, -1)
+        if self.kind == "scaled":
+            f = (self.ke.astype(flat.dtype) @ flat) * self.e.reshape(1, -1).astype(flat.dtype)
+        elif self.kind == "weights":
+            g = (self.mcat.astype(flat.dtype) @ flat).reshape(8, 24, -1)
+            w = self.w.reshape(8, 1, -1).astype(flat.dtype)
+            f = (g * w).sum(axis=0)
+        else:
+            kk = self.k.reshape(24, 24, -1).astype(flat.dtype)
+            f = np.einsum("ijn,jn->in", kk, flat)
+        return f.reshape(cells24.shape)
+
+    def patch_index(self):
+        """(npatch, 24) flat (3, nodes) indices of patch cells' dofs (loadpath/mg.py:299-309)."""
+        nshape = self.node_shape[1:]
+        nn = int(np.prod(nshape))
+        idx = np.empty((len(self.patch_ijk), 24), np.int64)
+        for k, off in enumerate(OFFS):
+            node = np.ravel_multi_index(tuple((self.patch_ijk + np.array(off)).T), nshape)
+            for i in range(3):
+                idx[:, 3 * k + i] = i * nn + node
+        return idx
+
+    def apply_k(self, u):
+        """Unmasked K u (loadpath/mg.py:251-276)."""
+        out = np.zeros(self.node_shape, u.dtype)
+        scatter_cells(self.cell_products(gather_cells(u, self.dims)), out)
+        if self.patch_ijk is not None and len(self.patch_ijk):
+            idx = self.patch_index()
+            fe = np.einsum("nij,nj->ni", self.patch_k.astype(u.dtype), u.reshape(-1)[idx])
+            np.add.at(out.reshape(-1), idx.ravel(), fe.ravel())
+        return out
+
+    def apply(self, u):
+        """mask * K (mask * u) + (1 - mask) * u (loadpath/mg.py:317-346)."""
+        m = self.mask.astype(u.dtype)
+        out = self.apply_k(u * m)
+        return out * m + (1 - m) * u
+
+    def cell_matrices(self):
+        """float64 (24, 24, nx, ny, nz) matrices of every cell (loadpath/mg.py:373-387)."""
+        if self.kind == "explicit":
+            return self.k.astype(np.float64)
+        if self.kind == "scaled":
+            return self.ke.astype(np.float64)[:, :, None, None, None] * self.e[None, None].astype(np.float64)
+        mk = self.mcat.reshape(8, 576).astype(np.float64)
+        out = (mk.T @ self.w.reshape(8, -1).astype(np.float64)).reshape((24, 24) + self.dims)
+        if self.patch_ijk is not None and len(self.patch_ijk):
+            p = self.patch_ijk
+            out[:, :, p[:, 0], p[:, 1], p[:, 2]] += np.moveaxis(self.patch_k.astype(np.float64), 0, -1)
+        return out
+
+    def diagonal(self):
+        """float64 diagonal of the unmasked K (loadpath/mg.py:348-371)."""
+        km = self.cell_matrices()
+        dc = np.einsum("iixyz->ixyz", km)
+        d = np.zeros(self.node_shape)
+        return scatter_cells(dc, d)
+
+    def active(self):
+        """Cells with a nonzero matrix outside the patch (loadpath/mg.py:205-211)."""
+        if self.kind == "scaled":
+            return self.e != 0
+        if self.kind == "weights":
+            return self.w.any(axis=0)
+        return np.einsum("iixyz->xyz", self.k) > 0
+
+
+# --------------------------------------------------------------------------
+# hierarchy (loadpath/mg.py:515-754)
+# --------------------------------------------------------------------------
+
+class Hierarchy:
+    """GridElasticity's level hierarchy and PCG on a full rectangular grid.
+
+    ke: (24, 24) unit-cube stiffness already multiplied by the pitch
+    (loadpath/mg.py:446). fixed_grid: bool (3, nodes). Cells are padded to
+    even counts by the caller (loadpath/mg.py:438-442)."""
+
+    def __init__(self, ke, cells, fixed_grid, rtol=1e-6, maxiter=500, coarse_cells=2000, degree=2,
+                 dtype=np.float32, lu_max_dofs=60_000):
+        self.ke = np.asarray(ke, np.float64)
+        self.cells = tuple(int(c) for c in cells)
+        self.fixed_grid = np.asarray(fixed_grid, bool)
+        self.rtol, self.maxiter = rtol, maxiter
+        self.coarse_cells, self.degree = int(coarse_cells), int(degree)
+        self.dtype = np.dtype(dtype)
+        self.lu_max_dofs = lu_max_dofs
+        self.strict = False
+        self.levels = []
+        self.coarse = None
+        self.lmax_vec = {}
+        self.last_iters = 0
+
+    def op(self, i):
+        return self.l0s if i == 0 else self.levels[i]
+
+    def set_moduli(self, e_grid):
+        """Rebuild every level for cell moduli (loadpath/mg.py:515-591)."""
+        e_grid = np.asarray(e_grid, np.float64)
+        self.e_grid = e_grid
+        dt = self.dtype
+        l0 = Level("scaled", self.cells, np.float64)
+        l0.ke = self.ke
+        l0.e = e_grid
+        d0 = l0.diagonal()
+        alive = d0 > 1e-300
+        l0.mask = (alive & ~self.fixed_grid).astype(np.float64)
+        l0.dinv = np.where(l0.mask > 0, 1.0 / np.where(alive, d0, 1.0), 1.0)
+        self.alive = alive
+        self.levels = [l0]
+        s = Level("scaled", self.cells, dt)
+        s.ke = self.ke.astype(dt)
+        s.e = e_grid.astype(dt)
+        s.mask = l0.mask.astype(dt)
+        s.dinv = l0.dinv.astype(dt)
+        self.l0s = s
+        fine = l0
+        n_active = int((e_grid > 0).sum())
+        depth = 0
+        held = alive & self.fixed_grid
+        while n_active > self.coarse_cells and min(fine.dims) >= 2:
+            coarse = self.coarsen(fine, first=(depth == 0))
+            depth += 1
+            d = coarse.diagonal()
+            dmax = float(d.max()) if d.size else 0.0
+            live = d > 1e-12 * max(dmax, 1e-300)
+            if self.strict:
+                hc = np.zeros((3,) + coarse.node_shape[1:], bool)
+                inj = held[:, ::2, ::2, ::2]
+                hc[:, :inj.shape[1], :inj.shape[2], :inj.shape[3]] = inj[:, :hc.shape[1], :hc.shape[2], :hc.shape[3]]
+                held = hc
+                kept = np.zeros((3,) + coarse.node_shape[1:])
+                r = restrict(np.asarray(fine.mask, np.float64))
+                kept[:, :r.shape[1], :r.shape[2], :r.shape[3]] = r[:, :kept.shape[1], :kept.shape[2], :kept.shape[3]]
+                live &= ~held & (kept >= 1.0)
+            coarse.mask = live.astype(dt)
+            coarse.dinv = np.where(live, 1.0 / np.where(live, d, 1.0), 1.0).astype(dt)
+            n_active = self.active_cells(coarse)
+            self.levels.append(coarse)
+            fine = coarse
+        try:
+            self.build_coarse(self.levels[-1])
+        except np.linalg.LinAlgError:
+            if self.strict:
+                raise
+            self.strict = True
+            return self.set_moduli(e_grid)
+        for i in range(len(self.levels)):
+            self.op(i).lmax = self.estimate_lmax(i)
+
+    @staticmethod
+    def active_cells(lv):
+        """(loadpath/mg.py:593-599)"""
+        if lv.kind == "weights":
+            act = lv.w.any(axis=0)
+            if lv.patch_ijk is not None and len(lv.patch_ijk):
+                act[tuple(lv.patch_ijk.T)] = True
+            return int(act.sum())
+        return int(np.abs(lv.k).max(axis=(0, 1)).astype(bool).sum())
+
+    def coarsen(self, fine, first):
+        """Galerkin coarse level (loadpath/mg.py:601-677)."""
+        dt = self.dtype
+        nx, ny, nz = fine.dims
+        half = (nx // 2, ny // 2, nz // 2)
+        cdims = tuple(h + h % 2 if h > 1 else h for h in half)
+        hx, hy, hz = half
+        if first:
+            held = (1 - fine.mask) * self.alive
+            held_node = held.any(axis=0)
+            touch = np.zeros(fine.dims, bool)
+            for (dx, dy, dz) in OFFS:
+                touch |= held_node[dx:dx + nx, dy:dy + ny, dz:dz + nz]
+            touch &= fine.e > 0
+            w = np.zeros((8,) + cdims)
+            ptouch = np.zeros(cdims, bool)
+            for k, (a, b, c) in enumerate(OFFS):
+                w[k, :hx, :hy, :hz] = fine.e[a::2, b::2, c::2]
+                ptouch[:hx, :hy, :hz] |= touch[a::2, b::2, c::2]
+            lv = Level("weights", cdims, dt)
+            mk = np.einsum("kai,ab,kbj->kij", PK, fine.ke, PK)
+            lv.mcat = mk.reshape(8 * 24, 24).astype(dt)
+            pij = np.argwhere(ptouch)
+            pk = np.zeros((len(pij), 24, 24))
+            fm = fine.mask
+            for k, (a, b, c) in enumerate(OFFS):
+                fi = 2 * pij + np.array([a, b, c])
+                ec = fine.e[tuple(fi.T)]
+                dm = np.empty((len(pij), 24))
+                for q, (qx, qy, qz) in enumerate(OFFS):
+                    dm[:, 3 * q:3 * q + 3] = fm[:, fi[:, 0] + qx, fi[:, 1] + qy, fi[:, 2] + qz].T
+                kc = ec[:, None, None] * fine.ke[None] * dm[:, :, None] * dm[:, None, :]
+                pk += PK[k].T[None] @ kc @ PK[k][None]
+            w[:, ptouch] = 0.0
+            lv.w = w.astype(dt)
+            lv.patch_ijk = pij
+            lv.patch_k = pk.astype(dt)
+            return lv
+        lv = Level("explicit", cdims, dt)
+        k = np.zeros((24, 24) + cdims, dt)
+        kf = fine.cell_matrices()
+        if self.strict:
+            fm = fine.mask
+            dm = np.empty((24,) + kf.shape[2:])
+            for q, (qx, qy, qz) in enumerate(OFFS):
+                dm[3 * q:3 * q + 3] = fm[:, qx:qx + nx, qy:qy + ny, qz:qz + nz]
+            kf = kf * dm[:, None] * dm[None, :]
+        for ch, (ox, oy, oz) in enumerate(OFFS):
+            sub = kf[:, :, ox::2, oy::2, oz::2]
+            shp = sub.shape[2:]
+            t = np.einsum("ai,abn,bj->ijn", PK[ch], sub.reshape(24, 24, -1), PK[ch])
+            k[:, :, :shp[0], :shp[1], :shp[2]] += t.reshape((24, 24) + shp).astype(dt)
+        lv.k = k
+        return lv
+
+    def build_coarse(self, lv):
+        """Assemble the coarsest level over the dofs of its active cells, as
+        D K D + (I - D), symmetrised, and factor it (loadpath/mg.py:708-754).
+        The reference factors with SuperLU in SPD mode; the same operator is
+        factored here by a dense Cholesky (an exact solve of the same system)."""
+        if lv is self.levels[0]:
+            self.coarse = None
+            return
+        kall = lv.cell_matrices()
+        act = np.abs(kall).max(axis=(0, 1)) > 0
+        ijk = np.argwhere(act)
+        if len(ijk) == 0:
+            self.coarse = None
+            return
+        nshape = lv.node_shape[1:]
+        nn = int(np.prod(nshape))
+        used = np.zeros(nn, bool)
+        for off in OFFS:
+            used[np.ravel_multi_index(tuple((ijk + np.array(off)).T), nshape)] = True
+        gnode = np.flatnonzero(used)
+        gdof = np.concatenate([[i * nn + gnode[j] for i in range(3)] for j in range(len(gnode))]).astype(np.int64)
+        loc = np.full(3 * nn, -1, np.int64)
+        loc[gdof] = np.arange(len(gdof))
+        n = len(gdof)
+        kd = np.zeros((n, n))
+        for c, (i, j, l) in enumerate(ijk):
+            dofs = np.empty(24, np.int64)
+            for q, off in enumerate(OFFS):
+                node = np.ravel_multi_index((i + off[0], j + off[1], l + off[2]), nshape)
+                for comp in range(3):
+                    dofs[3 * q + comp] = loc[comp * nn + node]
+            kd[np.ix_(dofs, dofs)] += kall[:, :, i, j, l]
+        m = lv.mask.reshape(-1)[gdof].astype(np.float64)
+        kd = m[:, None] * kd * m[None, :] + np.diag(1.0 - m)
+        kd = 0.5 * (kd + kd.T)
+        chol = np.linalg.cholesky(kd)
+        self.coarse = {"gdof": gdof, "chol": chol, "n": n}
+
+    def coarse_solve(self, b):
+        """(loadpath/mg.py:756-766)"""
+        c = self.coarse
+        flat = b.reshape(-1)
+        rhs = flat[c["gdof"]].astype(np.float64)
+        y = np.linalg.solve(c["chol"], rhs)
+        x = np.linalg.solve(c["chol"].T, y)
+        out = np.zeros_like(flat)
+        out[c["gdof"]] = x
+        return out.reshape(b.shape)
+
+    def initial_vector(self, i):
+        """The power iteration's start on level i (loadpath/mg.py:779-786)."""
+        lv = self.op(i)
+        prev = self.lmax_vec.get(i)
+        if prev is not None and prev.shape == lv.node_shape:
+            return prev.astype(lv.dinv.dtype) * lv.mask
+        rng = np.random.default_rng(i)
+        return (rng.random(lv.node_shape) - 0.5).astype(lv.dinv.dtype) * lv.mask
+
+    def estimate_lmax(self, i, its=12):
+        """12 power iterations of D^-1 A, times 1.3 (loadpath/mg.py:771-794)."""
+        lv = self.op(i)
+        v = self.initial_vector(i)
+        lam = 1.0
+        for _ in range(its):
+            nv = float(np.dot(v.reshape(-1).astype(np.float64), v.reshape(-1).astype(np.float64))) ** 0.5
+            if nv == 0:
+                return 2.0
+            v = v / v.dtype.type(nv)
+            av = lv.dinv * lv.apply(v) * lv.mask
+            lam = float(np.dot(v.reshape(-1).astype(np.float64), av.reshape(-1).astype(np.float64)))
+            v = av
+        self.lmax_vec[i] = v
+        return LMAX_SAFETY * max(lam, 1e-12)
+
+    def smooth(self, lv, b, x):
+        """Chebyshev on D^-1 A over [lmax/30, lmax], degree self.degree
+        (loadpath/mg.py:796-835, fused-kernel arithmetic of loadpath/mgops.py:312-343)."""
+        t = b.dtype.type
+        hi = lv.lmax
+        lo = hi / 30.0
+        theta = 0.5 * (hi + lo)
+        delta = 0.5 * (hi - lo)
+        sigma = theta / delta
+        rho = 1.0 / sigma
+        if x is None:
+            x = np.zeros_like(b)
+            r = b.copy()
+            d = (lv.dinv * b) * t(1.0 / theta)
+        else:
+            r = b - lv.apply(x)
+            d = t(1.0 / theta) * lv.dinv * r
+        for it in range(self.degree):
+            x = x + d
+            if it + 1 == self.degree:
+                break
+            r = r - lv.apply(d)
+            rho_new = 1.0 / (2.0 * sigma - rho)
+            d = t(rho_new * rho) * d + t(2.0 * rho_new / delta) * lv.dinv * r
+            rho = rho_new
+        return x
+
+    def vcycle(self, i, b):
+        """(loadpath/mg.py:837-860)"""
+        lv = self.op(i)
+        if i == len(self.levels) - 1:
+            if self.coarse is not None:
+                return self.coarse_solve(b)
+            x = self.smooth(lv, b, None)
+            return self.smooth(lv, b, x)
+        x = self.smooth(lv, b, None)
+        ax = lv.apply(x)
+        nxt = self.op(i + 1)
+        rc = restrict_masked_residual(b, ax, lv.mask, nxt.mask, nxt.node_shape)
+        xc = self.vcycle(i + 1, rc.astype(self.dtype))
+        prolong_add(xc, nxt.mask, lv.mask, x)
+        return self.smooth(lv, b, x)
+
+    def precondition(self, r):
+        return self.vcycle(0, r.astype(self.dtype)).astype(np.float64)
+
+    def pcg(self, b, x0):
+        """float64 PCG with the energy-optimal warm start (loadpath/mg.py:872-926)."""
+        a = self.levels[0]
+        dot = lambda p, q: float(np.dot(p.reshape(-1), q.reshape(-1)))
+        bnorm = dot(b, b) ** 0.5
+        if bnorm == 0:
+            return np.zeros_like(b), 0, True
+        x = np.zeros(a.node_shape) if x0 is None else x0.copy()
+        r = b.copy()
+        if x0 is not None:
+            ax = a.apply(x)
+            xax = dot(x, ax)
+            s = dot(b, x) / xax if xax > 0 else 0.0
+            if s > 0:
+                rs = b - s * ax
+                if dot(rs, rs) ** 0.5 < bnorm:
+                    x *= s
+                    r = rs
+                else:
+                    x[:] = 0
+            else:
+                x[:] = 0
+        z = self.precondition(r)
+        p = z.copy()
+        rz = dot(r, z)
+        tol = self.rtol * bnorm
+        for it in range(1, self.maxiter + 1):
+            ap = a.apply(p)
+            pap = dot(p, ap)
+            if pap <= 0:
+                return x, it, False
+            alpha = rz / pap
+            x += alpha * p
+            r -= alpha * ap
+            if dot(r, r) ** 0.5 <= tol:
+                return x, it, True
+            z = self.precondition(r)
+            rz_new = dot(r, z)
+            p = z + (rz_new / rz) * p
+            rz = rz_new
+        return x, self.maxiter, False
+
+    def solve(self, b, x0=None):
+        """One right-hand side on the grid (masked), with the strict fallback
+        after STALL iterations (loadpath/mg.py:932-965)."""
+        m = self.levels[0].mask
+        b = b * m
+        g0 = x0 * m if x0 is not None else None
+        if self.strict or len(self.levels) < 2:
+            x, it, ok = self.pcg(b, g0)
+        else:
+            full = self.maxiter
+            self.maxiter = min(full, STALL)
+            try:
+                x, it, ok = self.pcg(b, g0)
+            finally:
+                self.maxiter = full
+            if not ok:
+                self.strict = True
+                self.set_moduli(self.e_grid)
+                x, it2, ok = self.pcg(b, g0)
+                it += it2
+        if not ok:
+            raise RuntimeError(f"linear solve did not converge ({it} iterations); "
+                               "the structure may be a mechanism (check supports)")
+        self.last_iters = it
+        return x * m
+
+    def strain_energy(self, u_grid):
+        """Per-cell u_e^T Ke u_e at unit modulus (loadpath/mg.py:975-988)."""
+        g = gather_cells(u_grid, self.cells).reshape(24, -1)
+        return np.einsum("in,in->n", g, self.ke @ g).reshape(self.cells)
+
+
+# --------------------------------------------------------------------------
+# SIMP pieces (loadpath/simp.py, loadpath/benchmarks/reference.py)
+# --------------------------------------------------------------------------
+
+def filter_taps(radius: float, pitch: float = 1.0):
+    """Cone taps w = r - |d| pitch > 0 within floor(r / pitch) cells
+    (loadpath/simp.py:1148-1161)."""
+    reach = int(np.floor(radius / pitch))
+    taps = []
+    for dx in range(-reach, reach + 1):
+        for dy in range(-reach, reach + 1):
+            for dz in range(-reach, reach + 1):
+                w = radius - np.sqrt(dx * dx + dy * dy + dz * dz) * pitch
+                if w > 0:
+                    taps.append(((dx, dy, dz), float(w)))
+    return taps
+
+
+def grid_filter(v: np.ndarray, taps) -> np.ndarray:
+    """H v on the cell grid with zeros outside it (loadpath/simp.py:1164-1172).
+    H is symmetric, so this is also H^T v."""
+    reach = max(max(abs(c) for c in d) for d, _ in taps)
+    nx, ny, nz = v.shape
+    g = np.zeros((nx + 2 * reach, ny + 2 * reach, nz + 2 * reach))
+    g[reach:reach + nx, reach:reach + ny, reach:reach + nz] = v
+    out = np.zeros(v.shape)
+    for (dx, dy, dz), w in taps:
+        out += w * g[reach + dx:reach + dx + nx, reach + dy:reach + dy + ny, reach + dz:reach + dz + nz]
+    return out
+
+
+def filter_row_sums(dims, taps):
+    """Row sums of the truncated stencil (top3d's Hs; loadpath/benchmarks/reference.py:48-71)."""
+    return grid_filter(np.ones(dims), taps)
+
+
+def simp_moduli(xphys, penal=3.0, emin=1e-9):
+    """E = Emin + x^p (1 - Emin) (loadpath/benchmarks/reference.py:89; loadpath/simp.py:1861)."""
+    return emin + xphys ** penal * (1 - emin)
+
+
+def oc_top3d(x, dc, dv, volfrac, h_apply, hs, move=0.2):
+    """top3d's OC bisection on the volume multiplier; volume measured on the
+    filtered physical densities (loadpath/benchmarks/reference.py:100-110).
+    Returns (xnew, xphys)."""
+    n = x.size
+    l1, l2 = 0.0, 1e9
+    while (l2 - l1) / (l1 + l2) > 1e-3:
+        lmid = 0.5 * (l2 + l1)
+        xnew = np.maximum(0, np.maximum(x - move, np.minimum(1, np.minimum(x + move, x * np.sqrt(-dc / dv / lmid)))))
+        xphys = h_apply(xnew) / hs
+        if xphys.sum() > volfrac * n:
+            l1 = lmid
+        else:
+            l2 = lmid
+    return xnew, xphys
+
+
+# --------------------------------------------------------------------------
+# assembled direct solve for tiny grids (loadpath/benchmarks/evaluate.py:111-117)
+# --------------------------------------------------------------------------
+
+def assembled_solve(ke, e_grid, fixed_grid, f_grid):
+    """Direct sparse solve of K(e) u = f on the full node grid, fixed dofs
+    removed (the evaluator's scheme). Returns the node-grid displacement."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    dims = e_grid.shape
+    nshape = tuple(d + 1 for d in dims)
+    nn = int(np.prod(nshape))
+    ijk = np.argwhere(np.ones(dims, bool))
+    dofs = np.empty((len(ijk), 24), np.int64)
+    for q, off in enumerate(OFFS):
+        node = np.ravel_multi_index(tuple((ijk + np.array(off)).T), nshape)
+        for c in range(3):
+            dofs[:, 3 * q + c] = c * nn + node
+    rows = np.repeat(dofs, 24, axis=1).ravel()
+    cols = np.tile(dofs, (1, 24)).ravel()
+    data = (e_grid[tuple(ijk.T)][:, None, None] * ke[None]).ravel()
+    k = sp.csr_matrix((data, (rows, cols)), shape=(3 * nn, 3 * nn))
+    free = np.flatnonzero(~fixed_grid.reshape(-1))
+    u = np.zeros(3 * nn)
+    u[free] = spla.spsolve(k[free][:, free].tocsc(), f_grid.reshape(-1)[free])
+    return u.reshape((3,) + nshape)
+
+
+def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, emin=1e-9, move=0.2,
+               solve=None):
+    """top3d's loop with the density filter (loadpath/benchmarks/reference.py:74-117).
+    Returns (x, xphys, compliance history, change history)."""
+    solve = solve or (lambda e: assembled_solve(ke, e, fixed_grid, f_grid))
+    taps = filter_taps(rmin)
+    hs = filter_row_sums(dims, taps)
+    hap = lambda v: grid_filter(v, taps)
+    x = np.full(dims, volfrac)
+    xphys = x.copy()
+    hist_c, hist_ch = [], []
+    for _ in range(iters):
+        e = simp_moduli(xphys, penal, emin)
+        u = solve(e)
+        g = gather_cells(u, dims).reshape(24, -1)
+        ce = np.einsum("in,in->n", g, ke @ g).reshape(dims)
+        c = float(np.sum(e * ce))
+        dc = -penal * (1 - emin) * xphys ** (penal - 1) * ce
+        dc = hap(dc / hs)
+        dv = hap(np.ones(dims) / hs)
+        xnew, xphys = oc_top3d(x, dc, dv, volfrac, hap, hs, move)
+        hist_c.append(c)
+        hist_ch.append(float(np.abs(xnew - x).max()))
+        x = xnew
+    return x, xphys, hist_c, hist_ch
+
+
+# --------------------------------------------------------------------------
+# MMA (loadpath/mma.py:31-214), restated from Svanberg's published method
+# --------------------------------------------------------------------------
+
+class MMA:
+    """Svanberg's MMA with a primal-dual interior-point subproblem solver, in
+    the reference's parameterisation (loadpath/mma.py:31-55)."""
+
+    def __init__(self, n, m, xmin=0.0, xmax=1.0, move=0.2, c=1000.0, asyinit=0.5, asyincr=1.2, asydecr=0.7):
+        self.n, self.m = n, m
+        self.xmin = np.broadcast_to(np.asarray(xmin, float), (n,)).copy()
+        self.xmax = np.broadcast_to(np.asarray(xmax, float), (n,)).copy()
+        self.move = move
+        self.a0, self.a, self.c, self.d = 1.0, np.zeros(m), np.full(m, float(c)), np.ones(m)
+        self.asyinit, self.asyincr, self.asydecr = asyinit, asyincr, asydecr
+        self.xold1 = self.xold2 = self.low = self.upp = None
+        self.iter = 0
+
+    def update(self, x, f0, df0, f, df):
+        """One MMA step (loadpath/mma.py:57-112)."""
+        xmin, xmax = self.xmin, self.xmax
+        x = np.clip(np.nan_to_num(np.asarray(x, float), nan=0.5), xmin, xmax)
+        f = np.nan_to_num(np.asarray(f, float).reshape(self.m), nan=1e6, posinf=1e6, neginf=-1e6)
+        df = np.nan_to_num(np.asarray(df, float).reshape(self.m, self.n), nan=0.0, posinf=1e6, neginf=-1e6)
+        df0 = np.nan_to_num(np.asarray(df0, float), nan=0.0, posinf=1e6, neginf=-1e6)
+        self.iter += 1
+        span = xmax - xmin
+        if self.iter <= 2 or self.low is None:
+            self.low = x - self.asyinit * span
+            self.upp = x + self.asyinit * span
+        else:
+            sgn = (x - self.xold1) * (self.xold1 - self.xold2)
+            fac = np.where(sgn > 0, self.asyincr, np.where(sgn < 0, self.asydecr, 1.0))
+            self.low = np.clip(x - fac * (self.xold1 - self.low), x - 10 * span, x - 0.01 * span)
+            self.upp = np.clip(x + fac * (self.upp - self.xold1), x + 0.01 * span, x + 10 * span)
+        low, upp = self.low, self.upp
+        alfa = np.maximum(np.maximum(low + 0.1 * (x - low), x - self.move * span), xmin)
+        beta = np.minimum(np.minimum(upp - 0.1 * (upp - x), x + self.move * span), xmax)
+        xmami = np.maximum(span, 1e-5)
+        ux1, xl1 = upp - x, x - low
+        ux2, xl2 = ux1 * ux1, xl1 * xl1
+        p0, q0 = np.maximum(df0, 0.0), np.maximum(-df0, 0.0)
+        pq0 = 0.001 * (p0 + q0) + 1e-5 / xmami
+        p0, q0 = (p0 + pq0) * ux2, (q0 + pq0) * xl2
+        P, Q = np.maximum(df, 0.0), np.maximum(-df, 0.0)
+        PQ = 0.001 * (P + Q) + 1e-5 / xmami
+        P, Q = (P + PQ) * ux2, (Q + PQ) * xl2
+        b = P @ (1.0 / ux1) + Q @ (1.0 / xl1) - f
+        with np.errstate(divide="ignore", invalid="ignore"):
+            xnew = self.subsolv(low, upp, alfa, beta, p0, q0, P, Q, b)
+        if not np.all(np.isfinite(xnew)):
+            xnew = np.where(np.isfinite(xnew), xnew, x)
+        xnew = np.clip(xnew, alfa, beta)
+        self.xold2 = self.xold1 if self.xold1 is not None else x.copy()
+        self.xold1 = x.copy()
+        return xnew
+
+    def subsolv(self, low, upp, alfa, beta, p0, q0, P, Q, b, epsimin=1e-7):
+        """Primal-dual Newton on the separable subproblem (loadpath/mma.py:114-214)."""
+        m = self.m
+        a0, a, c, d = self.a0, self.a, self.c, self.d
+        x = 0.5 * (alfa + beta)
+        y, z, lam = np.ones(m), 1.0, np.ones(m)
+        xsi = np.maximum(1.0 / (x - alfa), 1.0)
+        eta = np.maximum(1.0 / (beta - x), 1.0)
+        mu, zet, s = np.maximum(1.0, 0.5 * c), 1.0, np.ones(m)
+        epsi = 1.0
+
+        def resid(x, y, z, lam, xsi, eta, mu, zet, s, epsi):
+            ux1, xl1 = upp - x, x - low
+            plam, qlam = p0 + P.T @ lam, q0 + Q.T @ lam
+            gvec = P @ (1.0 / ux1) + Q @ (1.0 / xl1)
+            dpsidx = plam / (ux1 * ux1) - qlam / (xl1 * xl1)
+            return np.concatenate([dpsidx - xsi + eta, c + d * y - mu - lam, [a0 - zet - a @ lam],
+                                   gvec - a * z - y + s - b, xsi * (x - alfa) - epsi, eta * (beta - x) - epsi,
+                                   mu * y - epsi, [zet * z - epsi], lam * s - epsi])
+
+        while epsi > epsimin:
+            r = resid(x, y, z, lam, xsi, eta, mu, zet, s, epsi)
+            norm = np.linalg.norm(r)
+            rmax = np.abs(r).max()
+            it = 0
+            while rmax > 0.9 * epsi and it < 200:
+                it += 1
+                ux1, xl1 = upp - x, x - low
+                ux2, xl2 = ux1 * ux1, xl1 * xl1
+                ux3, xl3 = ux1 * ux2, xl1 * xl2
+                plam, qlam = p0 + P.T @ lam, q0 + Q.T @ lam
+                gvec = P @ (1.0 / ux1) + Q @ (1.0 / xl1)
+                GG = P / ux2 - Q / xl2
+                dpsidx = plam / ux2 - qlam / xl2
+                delx = dpsidx - epsi / (x - alfa) + epsi / (beta - x)
+                dely = c + d * y - lam - epsi / y
+                delz = a0 - a @ lam - epsi / z
+                dellam = gvec - a * z - y - b + epsi / lam
+                diagx = 2.0 * (plam / ux3 + qlam / xl3) + xsi / (x - alfa) + eta / (beta - x)
+                diagy = d + mu / y
+                diaglamyi = s / lam + 1.0 / diagy
+                blam = dellam + dely / diagy - GG @ (delx / diagx)
+                aa = np.zeros((m + 1, m + 1))
+                aa[:m, :m] = np.diag(diaglamyi) + (GG / diagx) @ GG.T
+                aa[:m, m] = a
+                aa[m, :m] = a
+                aa[m, m] = -zet / z
+                sol = np.linalg.solve(aa, np.concatenate([blam, [delz]]))
+                dlam, dz = sol[:m], sol[m]
+                dx = -delx / diagx - (GG.T @ dlam) / diagx
+                dy = -dely / diagy + dlam / diagy
+                dxsi = -xsi + epsi / (x - alfa) - xsi * dx / (x - alfa)
+                deta = -eta + epsi / (beta - x) + eta * dx / (beta - x)
+                dmu = -mu + epsi / y - mu * dy / y
+                dzet = -zet + epsi / z - zet * dz / z
+                ds = -s + epsi / lam - s * dlam / lam
+                xx = np.concatenate([y, [z], lam, xsi, eta, mu, [zet], s])
+                dxx = np.concatenate([dy, [dz], dlam, dxsi, deta, dmu, [dzet], ds])
+                stmxx = np.max(-1.01 * dxx / xx)
+                stmalfa = np.max(-1.01 * dx / (x - alfa))
+                stmbeta = np.max(1.01 * dx / (beta - x))
+                steg = 1.0 / max(stmalfa, stmbeta, stmxx, 1.0)
+                old = (x, y, z, lam, xsi, eta, mu, zet, s)
+                for _ in range(50):
+                    x, y, z, lam, xsi, eta, mu, zet, s = (o + steg * dd for o, dd in zip(
+                        old, (dx, dy, dz, dlam, dxsi, deta, dmu, dzet, ds)))
+                    r = resid(x, y, z, lam, xsi, eta, mu, zet, s, epsi)
+                    newnorm = np.linalg.norm(r)
+                    if newnorm < 2.0 * norm:
+                        break
+                    steg /= 2.0
+                norm = newnorm
+                rmax = np.abs(r).max()
+            epsi *= 0.1
+        self.lam = lam
+        return x
+
+
+# --------------------------------------------------------------------------
+# problem builders shared by the tests and the CPU baseline
+# --------------------------------------------------------------------------
+
+def cantilever_bc(dims, total=-1.0):
+    """All dofs of the x = 0 face held; a -z force of `total` spread evenly
+    over the nodes of the bottom edge at x = nx (z = 0), as the benchmark
+    configs describe (the top3d cantilever, loadpath/benchmarks/problems.py:109-119,
+    with the load rescaled to a unit total)."""
+    nx, ny, nz = dims
+    nshape = (nx + 1, ny + 1, nz + 1)
+    fixed = np.zeros((3,) + nshape, bool)
+    fixed[:, 0] = True
+    f = np.zeros((3,) + nshape)
+    f[2, nx, :, 0] = total / (ny + 1)
+    return fixed, f
+
+
+def log_uniform_density(dims, seed, lo=1e-3, radius=2.0):
+    """Seeded log-uniform densities in [lo, 1], smoothed by the row-normalised
+    cone filter of `radius` (the benchmark configs' synthetic density)."""
+    rng = np.random.default_rng(seed)
+    x = np.exp(rng.uniform(np.log(lo), 0.0, size=dims))
+    taps = filter_taps(radius)
+    return grid_filter(x, taps) / filter_row_sums(dims, taps)

@@ -1,0 +1,263 @@
+"""Generate the golden fixtures in this folder from the reference implementation.
+
+Run in a container that has the loadpath source tree (read-only is fine):
+
+    LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py
+
+It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
+benchmarks.*), runs them on small seeded inputs and stores inputs and outputs
+as .npz files here. The tests in tests/test_oracle_golden.py pin the oracle
+against these files; the GPU tests then pin the CUDA path against the oracle.
+Nothing at test time reads the loadpath tree.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.environ.get("LOADPATH_SRC", "/root/reference")
+os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "lp_numba_cache"))
+os.environ["LOADPATH_DEVICE"] = "cpu"
+sys.path.insert(0, SRC)
+
+
+def _full_mesh(dims, pitch=1.0):
+    from loadpath.fem import HexMesh
+
+    ijk = np.argwhere(np.ones(dims, bool))
+    return HexMesh(ijk, pitch, np.zeros(3))
+
+
+def _cantilever(mesh, dims):
+    nx = dims[0]
+    fixed = np.zeros(mesh.n_dof, bool)
+    root = np.flatnonzero(mesh.node_ijk[:, 0] == 0)
+    for i in range(3):
+        fixed[3 * root + i] = True
+    f = np.zeros(mesh.n_dof)
+    tip = np.flatnonzero((mesh.node_ijk[:, 0] == nx) & (mesh.node_ijk[:, 2] == 0))
+    f[3 * tip + 2] = -1.0 / len(tip)
+    return fixed, f
+
+
+def make_element():
+    from loadpath.fem import hex8_ke
+
+    out = {}
+    for el in ("plain", "im"):
+        for nu in (0.3, 0.35):
+            out[f"ke_{el}_{nu}"] = hex8_ke(nu, el)
+    np.savez_compressed(os.path.join(HERE, "element.npz"), **out)
+
+
+def make_transfers():
+    from loadpath.mg import _PK, prolong, restrict
+
+    rng = np.random.default_rng(11)
+    c = rng.standard_normal((3, 5, 4, 6))
+    f = rng.standard_normal((3, 9, 7, 11))
+    c32 = c.astype(np.float32)
+    np.savez_compressed(os.path.join(HERE, "transfers.npz"), pk=_PK, c=c, f=f, prolong_c=prolong(c),
+                        restrict_f=restrict(f), c32=c32, prolong_c32=prolong(c32))
+
+
+def make_hierarchy(name, dims, element, seed, coarse_cells, void_frac, pitch=1.0, smooth=True):
+    """A GridElasticity hierarchy on a full grid with some removed cells; the
+    densities are seeded log-uniform, smoothed by the r = 2 cone filter (as
+    the benchmark configs describe) unless `smooth` is False."""
+    os.environ["LOADPATH_HEX8"] = element
+    from loadpath.mg import GridElasticity
+    from loadpath import mgops
+
+    mesh = _full_mesh(dims, pitch)
+    fixed, f = _cantilever(mesh, dims)
+    rng = np.random.default_rng(seed)
+    x = np.exp(rng.uniform(np.log(1e-3), 0.0, mesh.n_elem))
+    if smooth:
+        x = _smoothed(x.reshape(dims), 2.0).reshape(-1)
+    e = 1e-9 + x ** 3 * (1 - 1e-9)
+    e[rng.random(mesh.n_elem) < void_frac] = 0.0
+    g = GridElasticity(mesh, 0.3, fixed, rtol=1e-10, maxiter=3000, coarse_cells=coarse_cells, device="cpu")
+    g.set_moduli(e)
+    out = dict(dims=np.array(dims), cells=np.array(g.cells), pitch=pitch, e_mesh=e, f_mesh=f, fixed_mesh=fixed,
+               e_grid=g.cell_grid(e), f_grid=g.to_grid(f), fixed_grid=g.fixed_grid, ke=g.ke, strict=g.strict,
+               nlevels=len(g.levels), alive=g.alive)
+    for i in range(len(g.levels)):
+        lv = g._op(i)
+        out[f"L{i}_kind"] = lv.kind
+        out[f"L{i}_mask"] = lv.mask
+        out[f"L{i}_dinv"] = lv.dinv
+        out[f"L{i}_lmax"] = lv.lmax
+        if lv.kind == "weights":
+            out[f"L{i}_w"] = lv.w
+            out[f"L{i}_patch_ijk"] = lv.patch_ijk
+            out[f"L{i}_patch_k"] = lv.patch_k
+            out[f"L{i}_mcat"] = lv.mcat
+        elif lv.kind == "explicit":
+            out[f"L{i}_k"] = lv.k
+        # the operator on seeded inputs, both precisions on the fine level
+        u = rng.standard_normal(lv.node_shape).astype(lv.mask.dtype)
+        out[f"L{i}_u"] = u
+        out[f"L{i}_apply"] = lv.apply(u)
+        out[f"L{i}_diag"] = lv.diagonal()
+    l0 = g.levels[0]
+    u64 = rng.standard_normal(l0.node_shape)
+    out["L0_u64"] = u64
+    out["L0_apply64"] = l0.apply(u64)
+    # transfers between level 0 and 1 in the V-cycle precision
+    if len(g.levels) > 1:
+        lv, nxt = g._op(0), g._op(1)
+        b = rng.standard_normal(lv.node_shape).astype(np.float32)
+        ax = rng.standard_normal(lv.node_shape).astype(np.float32)
+        xc = rng.standard_normal(nxt.node_shape).astype(np.float32)
+        x = rng.standard_normal(lv.node_shape).astype(np.float32)
+        out.update(t_b=b, t_ax=ax, t_xc=xc, t_x=x,
+                   t_coarse_residual=mgops.coarse_residual(b, ax, lv.mask, nxt.mask, nxt.node_shape))
+        x2 = x.copy()
+        mgops.add_correction(xc, nxt.mask, lv.mask, x2)
+        out["t_add_correction"] = x2
+    # one V-cycle on a seeded residual, then the full solve and its energies
+    r = (rng.standard_normal(l0.node_shape) * l0.mask)
+    out["vc_r"] = r
+    out["vc_z"] = g.precondition(r)
+    u = g.solve_many([f])[0]
+    out["u_mesh"] = u
+    out["u_grid"] = g.to_grid(u)
+    out["iters"] = g.last_iters
+    out["compliance"] = float(f @ u)
+    out["strain_energy"] = g.strain_energy(u)
+    # warm start from a scaled copy
+    g.set_moduli(e * 1.1)
+    w = g.solve_many([f], [u])[0]
+    out["u_warm_grid"] = g.to_grid(w)
+    out["iters_warm"] = g.last_iters
+    np.savez_compressed(os.path.join(HERE, f"hier_{name}.npz"), **out)
+    print(name, "levels", len(g.levels), "iters", out["iters"], "warm", out["iters_warm"], "strict", g.strict)
+
+
+def _smoothed(x, radius):
+    """Row-normalised cone filter of the reference's top3d port on a full grid."""
+    from loadpath.benchmarks.evaluate import Evaluator
+    from loadpath.benchmarks.problems import Problem
+    from loadpath.benchmarks.reference import _filter
+
+    p = Problem(name="s", title="", source="", dims=x.shape, volfrac=0.3, rmin=radius, fixed=[], loads=[],
+                references=[])
+    ev = Evaluator(p)
+    h, hs = _filter(ev, radius)
+    out = np.zeros(x.shape)
+    out[ev.cell] = (h @ ev.cells(x)) / hs
+    return out
+
+
+def make_femops():
+    os.environ["LOADPATH_HEX8"] = "im"
+    from loadpath import femops
+    from loadpath.fem import HexMesh, hex8_ke
+
+    rng = np.random.default_rng(5)
+    dims = (7, 5, 4)
+    mesh = _full_mesh(dims)
+    u = rng.standard_normal(mesh.n_dof)
+    v = rng.standard_normal(mesh.n_dof)
+    ke = hex8_ke(0.3, "im")
+    out = femops.element_energy(u, v, mesh.edof, ke)
+    uu = femops.element_energy(u, None, mesh.edof, ke)
+    assert isinstance(mesh, HexMesh)
+    np.savez_compressed(os.path.join(HERE, "femops.npz"), dims=np.array(dims), u=u, v=v, ke=ke, uv=out, uu=uu,
+                        edof=mesh.edof)
+
+
+def make_filter():
+    from loadpath.benchmarks.evaluate import Evaluator
+    from loadpath.benchmarks.problems import Problem
+    from loadpath.benchmarks.reference import _filter
+    from loadpath.simp import GridFilter, _dproject, _project
+
+    class _Dom:
+        pass
+
+    dims = (9, 7, 5)
+    out = {"dims": np.array(dims)}
+    rng = np.random.default_rng(7)
+    v = rng.random(dims)
+    out["v"] = v
+    for r in (1.5, 2.0, 3.0):
+        d = _Dom()
+        d.mesh = _full_mesh(dims)
+        d.dims = dims
+        d.pitch = 1.0
+        h = GridFilter(d, r)
+        out[f"grid_{r}"] = h @ v[tuple(d.mesh.elem_ijk.T)]
+        out[f"ntaps_{r}"] = len(h.taps)
+        p = Problem(name="f", title="", source="", dims=dims, volfrac=0.3, rmin=r, fixed=[], loads=[], references=[])
+        ev = Evaluator(p)
+        hh, hs = _filter(ev, r)
+        out[f"top3d_{r}"] = hh @ ev.cells(v)
+        out[f"top3d_hs_{r}"] = hs
+        out[f"top3d_cellorder_{r}"] = np.stack(ev.cell, axis=1)
+    xt = rng.random(50)
+    out["proj_x"] = xt
+    for beta in (1.0, 8.0):
+        out[f"proj_{beta}"] = _project(xt, beta, 0.5)
+        out[f"dproj_{beta}"] = _dproject(xt, beta, 0.5)
+    np.savez_compressed(os.path.join(HERE, "filter.npz"), **out)
+
+
+def make_top3d():
+    import loadpath.benchmarks.reference as ref
+    from loadpath.benchmarks.problems import cantilever_3d, get
+
+    os.environ["LOADPATH_HEX8"] = "plain"
+    p = cantilever_3d(12, 4, 6, 0.3, 1.5)
+    hist = []
+    ref.TOP3D_MAXIT = 8
+    rec = ref.optimize_reference(p, "top3d", on_iter=lambda loop, c, ch: hist.append((c, ch)))
+    ref.TOP3D_MAXIT = 200
+    stored = ref.load_reference(get("cantilever-3d"), "top3d")
+    np.savez_compressed(os.path.join(HERE, "top3d.npz"), dims=np.array(p.dims), volfrac=p.volfrac, rmin=p.rmin,
+                        xphys=rec["x"], hist=np.array(hist), stored_x=stored["x"].astype(np.float32),
+                        stored_iters=stored["iterations"], stored_c=stored["compliance_reported"],
+                        stored_dims=np.array(get("cantilever-3d").dims))
+
+
+def make_mma():
+    from loadpath.mma import MMA
+
+    rng = np.random.default_rng(9)
+    n, m = 40, 2
+    mma = MMA(n, m, move=0.2)
+    x = rng.random(n) * 0.8 + 0.1
+    steps = []
+    for it in range(4):
+        df0 = rng.standard_normal(n)
+        f = rng.standard_normal(m) * 0.1
+        df = rng.standard_normal((m, n))
+        xn = mma.update(x, 1.0, df0, f, df)
+        steps.append((x.copy(), df0, f, df, xn))
+        x = xn
+    out = {}
+    for i, (a, b, c, d, e) in enumerate(steps):
+        out.update({f"x{i}": a, f"df0{i}": b, f"f{i}": c, f"df{i}": d, f"xn{i}": e})
+    np.savez_compressed(os.path.join(HERE, "mma.npz"), n=n, m=m, steps=len(steps), **out)
+
+
+def main():
+    make_element()
+    make_transfers()
+    make_femops()
+    make_filter()
+    make_mma()
+    make_hierarchy("even_im", (12, 6, 6), "im", 1, 50, 0.02)
+    make_hierarchy("odd_plain", (11, 5, 7), "plain", 2, 30, 0.0)
+    make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0)
+    make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)
+    make_top3d()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+"""The oracle (oracle/ref_numpy.py) against golden vectors made by the
+reference implementation itself (tests/golden/make_golden.py). CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ref_numpy as R
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+COARSE_CELLS = {"even_im": 50, "odd_plain": 30, "deep_im": 20, "rough_strict": 20}
+
+
+def _load(name):
+    return np.load(os.path.join(GOLD, name), allow_pickle=False)
+
+
+def test_element_matrices():
+    g = _load("element.npz")
+    for el in ("plain", "im"):
+        for nu in (0.3, 0.35):
+            np.testing.assert_allclose(R.hex8_ke(nu, el), g[f"ke_{el}_{nu}"], rtol=0, atol=1e-14)
+
+
+def test_transfers():
+    g = _load("transfers.npz")
+    np.testing.assert_array_equal(R.PK, g["pk"])
+    np.testing.assert_allclose(R.prolong(g["c"]), g["prolong_c"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(R.restrict(g["f"]), g["restrict_f"], rtol=0, atol=1e-14)
+    # float32: the reference's compiled path sums the corners before scaling, the
+    # numpy path axis by axis; the two agree to rounding
+    np.testing.assert_allclose(R.prolong(g["c32"]), g["prolong_c32"], rtol=1e-6, atol=1e-6)
+    # adjoint pair, as the reference's own test pins (tests/test_mg.py:56-63)
+    c, f = g["c"], g["f"]
+    assert abs(np.vdot(R.prolong(c), f) - np.vdot(c, R.restrict(f))) < 1e-10
+
+
+def _hierarchy(name):
+    g = _load(f"hier_{name}.npz")
+    h = R.Hierarchy(g["ke"], tuple(g["cells"]), g["fixed_grid"], rtol=1e-10, maxiter=3000,
+                    coarse_cells=COARSE_CELLS[name])
+    h.set_moduli(g["e_grid"])
+    return g, h
+
+
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_hierarchy_levels(name):
+    g, h = _hierarchy(name)
+    assert len(h.levels) == int(g["nlevels"])
+    assert h.strict == bool(g["strict"])
+    np.testing.assert_array_equal(h.alive, g["alive"])
+    for i in range(len(h.levels)):
+        lv = h.op(i)
+        assert lv.kind == str(g[f"L{i}_kind"])
+        np.testing.assert_array_equal(lv.mask, g[f"L{i}_mask"])
+        np.testing.assert_allclose(lv.dinv, g[f"L{i}_dinv"], rtol=2e-6)
+        np.testing.assert_allclose(lv.lmax, float(g[f"L{i}_lmax"]), rtol=1e-4)
+        if lv.kind == "weights":
+            np.testing.assert_array_equal(lv.w, g[f"L{i}_w"])
+            np.testing.assert_array_equal(lv.patch_ijk, g[f"L{i}_patch_ijk"])
+            np.testing.assert_allclose(lv.patch_k, g[f"L{i}_patch_k"], rtol=1e-6, atol=1e-7)
+            np.testing.assert_allclose(lv.mcat, g[f"L{i}_mcat"], rtol=1e-6, atol=1e-7)
+        elif lv.kind == "explicit":
+            ref = g[f"L{i}_k"]
+            np.testing.assert_allclose(lv.k, ref, rtol=1e-5, atol=1e-6 * np.abs(ref).max())
+        np.testing.assert_allclose(lv.diagonal(), g[f"L{i}_diag"], rtol=1e-6, atol=1e-12)
+        u = g[f"L{i}_u"]
+        want = g[f"L{i}_apply"]
+        tol = 1e-5 if u.dtype == np.float32 else 1e-12
+        np.testing.assert_allclose(lv.apply(u), want, rtol=tol, atol=tol * np.abs(want).max())
+    want = g["L0_apply64"]
+    np.testing.assert_allclose(h.levels[0].apply(g["L0_u64"]), want, rtol=1e-12, atol=1e-13 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_transfers_and_vcycle(name):
+    g, h = _hierarchy(name)
+    if "t_b" in g:
+        lv, nxt = h.op(0), h.op(1)
+        rc = R.restrict_masked_residual(g["t_b"], g["t_ax"], lv.mask, nxt.mask, nxt.node_shape)
+        np.testing.assert_allclose(rc, g["t_coarse_residual"], rtol=1e-6, atol=1e-6)
+        x = g["t_x"].copy()
+        R.prolong_add(g["t_xc"], nxt.mask, lv.mask, x)
+        np.testing.assert_allclose(x, g["t_add_correction"], rtol=1e-6, atol=1e-6)
+    z = h.precondition(g["vc_r"])
+    want = g["vc_z"]
+    np.testing.assert_allclose(z, want, rtol=1e-4, atol=1e-4 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_solve_matches_reference(name):
+    g, h = _hierarchy(name)
+    u = h.solve(g["f_grid"])
+    ref = g["u_grid"]
+    assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref)
+    assert abs(h.last_iters - int(g["iters"])) <= max(2, int(0.05 * int(g["iters"])))
+    c = float(np.vdot(g["f_grid"], u))
+    assert abs(c - float(g["compliance"])) <= 1e-9 * abs(float(g["compliance"]))
+    se = h.strain_energy(ref)
+    nx, ny, nz = g["dims"]
+    np.testing.assert_allclose(se[:nx, :ny, :nz].reshape(-1), g["strain_energy"], rtol=1e-10,
+                               atol=1e-12 * np.abs(g["strain_energy"]).max())
+    h.set_moduli(g["e_grid"] * 1.1)
+    w = h.solve(g["f_grid"], u)
+    assert np.linalg.norm(w - g["u_warm_grid"]) <= 1e-8 * np.linalg.norm(g["u_warm_grid"])
+
+
+def test_element_energy():
+    g = _load("femops.npz")
+    dims = tuple(g["dims"])
+    u, v, edof, ke = g["u"], g["v"], g["edof"], g["ke"]
+    ue, ve = u[edof], v[edof]
+    np.testing.assert_allclose(np.einsum("ij,jk,ik->i", ue, ke, ve), g["uv"], rtol=1e-13)
+    # the grid form used by the CUDA path: node-grid field, cells in C order
+    nshape = tuple(d + 1 for d in dims)
+    ug = u.reshape(-1, 3).T.reshape((3,) + nshape)
+    cells = R.gather_cells(ug, dims).reshape(24, -1)
+    np.testing.assert_allclose(np.einsum("in,in->n", cells, ke @ cells), g["uu"], rtol=1e-12)
+
+
+def test_filters():
+    g = _load("filter.npz")
+    dims = tuple(g["dims"])
+    v = g["v"]
+    for r in (1.5, 2.0, 3.0):
+        taps = R.filter_taps(r)
+        assert len(taps) == int(g[f"ntaps_{r}"])
+        np.testing.assert_allclose(R.grid_filter(v, taps).reshape(-1), g[f"grid_{r}"], rtol=1e-13)
+        order = tuple(g[f"top3d_cellorder_{r}"].T)
+        np.testing.assert_allclose(R.grid_filter(v, taps)[order], g[f"top3d_{r}"], rtol=1e-13)
+        np.testing.assert_allclose(R.filter_row_sums(dims, taps)[order], g[f"top3d_hs_{r}"], rtol=1e-13)
+
+
+def test_top3d_history():
+    g = _load("top3d.npz")
+    dims = tuple(int(d) for d in g["dims"])
+    ke = R.hex8_ke(0.3, "plain")
+    nx, ny, nz = dims
+    fixed = np.zeros((3, nx + 1, ny + 1, nz + 1), bool)
+    fixed[:, 0] = True
+    f = np.zeros(fixed.shape)
+    f[2, nx, :, 0] = -1.0           # the stock problem: -1 on each bottom-edge node
+    hist = g["hist"]
+    x, xphys, hc, hch = R.top3d_loop(dims, float(g["volfrac"]), float(g["rmin"]), ke, fixed, f, len(hist))
+    np.testing.assert_allclose(hc, hist[:, 0], rtol=1e-9)
+    np.testing.assert_allclose(hch, hist[:, 1], rtol=1e-7, atol=1e-12)
+    np.testing.assert_allclose(xphys, g["xphys"], rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.slow
+def test_top3d_stored_cantilever_compliance():
+    """The stored top3d design of the 60x4x20 cantilever (the reference's own
+    golden file): its penalised compliance, evaluated by the oracle's direct
+    solve, is the compliance top3d reported on its last iteration up to the
+    float32 storage of the design."""
+    g = _load("top3d.npz")
+    dims = tuple(int(d) for d in g["stored_dims"])
+    nx, ny, nz = dims
+    ke = R.hex8_ke(0.3, "plain")
+    fixed = np.zeros((3, nx + 1, ny + 1, nz + 1), bool)
+    fixed[:, 0] = True
+    f = np.zeros(fixed.shape)
+    f[2, nx, :, 0] = -1.0
+    x = g["stored_x"].astype(np.float64)
+    u = R.assembled_solve(ke, R.simp_moduli(x), fixed, f)
+    c = float(np.vdot(f, u))
+    assert abs(c - float(g["stored_c"])) < 2e-4 * float(g["stored_c"]), (c, float(g["stored_c"]))
+    assert int(g["stored_iters"]) == 133
+
+
+def test_mma_steps():
+    g = _load("mma.npz")
+    n, m = int(g["n"]), int(g["m"])
+    mma = R.MMA(n, m, move=0.2)
+    for i in range(int(g["steps"])):
+        xn = mma.update(g[f"x{i}"], 1.0, g[f"df0{i}"], g[f"f{i}"], g[f"df{i}"])
+        np.testing.assert_allclose(xn, g[f"xn{i}"], rtol=1e-10, atol=1e-12)
