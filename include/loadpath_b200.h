@@ -1,0 +1,133 @@
+/* loadpath_b200 — C ABI of the B200 (sm_100a) voxel SIMP inner loop.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream (void *, NULL = the
+ * legacy default stream) and returns an int status: 0 ok, -1 bad arguments, -2 launch error,
+ * -3 size beyond a kernel's limit. Nothing allocates: callers own every buffer.
+ *
+ * Layouts (C order):
+ *   node field  (3, nx+1, ny+1, pz)  pz >= nz+1 is the z pitch in elements
+ *   cell field  (nx, ny, cpz)        cpz >= nz
+ *   node mask   (nx+1, ny+1, pz) uint8: bits 0..2 solved dof per component (alive and not
+ *               held), bits 3..5 alive (carries stiffness) per component
+ *   cell matrices (cells, 24, 24), rows/cols ordered 3*corner + component, corner k at
+ *               (k & 1, k >> 1 & 1, k >> 2 & 1)
+ * `LP_GRID` below stands for the five ints  nx, ny, nz, pz, cpz  of one level;
+ * `LP_FC` for the ten ints of a fine level then its coarse level.
+ *
+ * The reference interfaces cited are loadpath's (paths relative to its project root).
+ */
+#ifndef LOADPATH_B200_H
+#define LOADPATH_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- level operators: out = m * K (m * u) + (1 - m) * u  (finish=1), or K (m * u) (finish=0).
+ * mask_in=0 skips the input mask (callers whose u is zero on masked dofs).
+ * Replaces mg._Level.apply / apply_k (loadpath/mg.py:251-346) and
+ * mgops.apply_masked / apply_scaled / apply_weights / apply_explicit (loadpath/mgops.py:247-299). */
+int lpb_apply_scaled_f32(float* out, const float* u, const float* e, const uint8_t* mask, const float* ke, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+int lpb_apply_scaled_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* ke, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+int lpb_apply_weights_f32(float* out, const float* u, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+int lpb_apply_weights_f64(double* out, const double* u, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+int lpb_apply_explicit_f32(float* out, const float* u, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+int lpb_apply_explicit_f64(double* out, const double* u, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
+
+/* ---- fine-level apply, tiled (the solver's hot path): same result as lpb_apply_scaled_* with
+ * mask_in = 0 and finish = 1 on inputs that are zero on masked dofs; kmodal is a HOST pointer to
+ * the 45 corner-parity coefficients from lpb_modal_ke (they are passed as kernel parameters).
+ * Needs pz % 4 == 0 and cpz == pz. Replaces mgops._product_scaled + _scatter_into with finish
+ * (loadpath/mgops.py:86-103, :181-217). */
+int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const float* kmodal, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* the element matrix (24 x 24, float64, host pointer) in the corner-parity basis that
+ * lpb_apply_fine_* reads (45 coefficients, host pointer out); returns the count or < 0 */
+int lpb_modal_ke(const double* ke, double* kmodal_out);
+
+/* ---- diagonal of K in float64 (loadpath/mg.py:348-371) */
+int lpb_diag_scaled_f64(double* d, const double* e, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_diag_weights_f32(double* d, const float* w, const float* mcat, const int* patch_id, const float* patch_k, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_diag_weights_f64(double* d, const double* w, const double* mcat, const int* patch_id, const double* patch_k, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_diag_explicit_f32(double* d, const float* k, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_diag_explicit_f64(double* d, const double* k, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+/* ---- masks and inverse diagonal (loadpath/mg.py:537-550, :575-576): alive = d > alive_thr,
+ * solved = d > live_thr and not held (held_bits may be NULL) and, when kept != NULL, kept >= 1;
+ * dinv = solved ? 1/d : 1 (either dinv pointer may be NULL). */
+int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, const uint8_t* held_bits, const float* kept, int nx, int ny, int nz, int pz, int cpz, double alive_thr, double live_thr, void* stream);
+/* *out = max(a[0:n]); part: >= 1024 doubles of scratch (loadpath/mg.py:560) */
+int lpb_max_f64(const double* a, long long n, double* part, double* out, void* stream);
+
+/* ---- Galerkin coarsening (loadpath/mg.py:601-677) */
+int lpb_weights_from_e_f64_f32(float* w, const double* e, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_weights_from_e_f64_f64(double* w, const double* e, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_patch_flags(uint8_t* flag, const double* e, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_patch_matrices_f32(float* pk, float* w, int* patch_id, const long long* pcells, int npatch, const double* e, const double* ke, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_patch_matrices_f64(double* pk, double* w, int* patch_id, const long long* pcells, int npatch, const double* e, const double* ke, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_galerkin_explicit_f32(float* kout, int fine_kind, const float* fw, const float* mcat, const int* patch_id, const float* patch_k, const float* fk, const uint8_t* mf, int strict, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_galerkin_explicit_f64(double* kout, int fine_kind, const double* fw, const double* mcat, const int* patch_id, const double* patch_k, const double* fk, const uint8_t* mf, int strict, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+/* strict hierarchy: held dofs injected down a level and restrict(fine mask) (loadpath/mg.py:562-574) */
+int lpb_strict_held_kept(uint8_t* held_c, float* kept, const uint8_t* held_f, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_held0(uint8_t* held, const uint8_t* mask0, const uint8_t* fixed_bits, long long n, void* stream);
+
+/* ---- coarsest level (loadpath/mg.py:708-766): dense D K D + (I - D), symmetrised, over all
+ * nodes of the level (n = 3 * nodes <= 40000); solve by a dense inverse the caller forms */
+int lpb_coarse_dense_f32(double* a, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_coarse_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_coarse_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+/* ---- V-cycle vector passes (loadpath/mgops.py:312-343) and damped Jacobi */
+int lpb_cheb_start_f32(const float* b, const float* dinv, float s, float* x, float* r, float* d, long long n, void* stream);
+int lpb_cheb_start_f64(const double* b, const double* dinv, double s, double* x, double* r, double* d, long long n, void* stream);
+int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, float s, float* r, float* d, long long n, void* stream);
+int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, double s, double* r, double* d, long long n, void* stream);
+int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, float c1, float c2, int last, long long n, void* stream);
+int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, double c1, double c2, int last, long long n, void* stream);
+int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero, long long n, void* stream);
+int lpb_jacobi_f64(double* x, const double* b, const double* ax, const double* dinv, double omega, int from_zero, long long n, void* stream);
+
+/* ---- grid transfers (loadpath/mgops.py:666-773: coarse_residual, add_correction) */
+int lpb_restrict_residual_f32(float* rc, const float* b, const float* ax, const uint8_t* m, const uint8_t* cm, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, const uint8_t* m, const uint8_t* cm, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint8_t* m, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const uint8_t* m, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+
+/* ---- PCG and power-iteration vector passes (loadpath/mgops.py:346-360, :557-585; mg.py:771-794,
+ * :872-926). Reductions are deterministic: part needs lpb_reduce_blocks() doubles; results land
+ * in device memory. alpha / beta are read as *num / *den on the device. */
+int lpb_reduce_blocks(void);
+int lpb_dot_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream);
+int lpb_dot_f32(const float* a, const float* b, long long n, double* part, double* out, void* stream);
+int lpb_dot_f64_f32(const double* a, const float* b, long long n, double* part, double* out, void* stream);
+int lpb_cg_step(double* x, double* r, const double* p, const double* ap, float* r32, long long n, const double* num, const double* den, double* part, double* rr, void* stream);
+int lpb_xpby_f32(double* p, const float* z, long long n, const double* num, const double* den, void* stream);
+int lpb_xpby_f64(double* p, const double* z, long long n, const double* num, const double* den, void* stream);
+int lpb_axpby_f64(double* out, double a, const double* x, double b, const double* y, long long n, void* stream);
+int lpb_axpby_f32(float* out, float a, const float* x, float b, const float* y, long long n, void* stream);
+int lpb_cast_f64_f32(float* out, const double* a, long long n, void* stream);
+int lpb_cast_f32_f64(double* out, const float* a, long long n, void* stream);
+int lpb_mask_field_f32(float* out, const float* u, const uint8_t* m, int nx, int ny, int nz, int pz, int cpz, int bitshift, void* stream);
+int lpb_mask_field_f64(double* out, const double* u, const uint8_t* m, int nx, int ny, int nz, int pz, int cpz, int bitshift, void* stream);
+int lpb_scale_rsqrt_f32(float* v, long long n, const double* nrm2, void* stream);
+int lpb_scale_rsqrt_f64(double* v, long long n, const double* nrm2, void* stream);
+int lpb_dinv_mask_f32(float* av, const float* dinv, const uint8_t* m, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_dinv_mask_f64(double* av, const double* dinv, const uint8_t* m, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+/* ---- SIMP loop (loadpath/simp.py:1143-1228, :1861, :1901-1904, :2001;
+ * loadpath/benchmarks/reference.py:48-110; loadpath/femops.py:51-78, loadpath/mg.py:975-988) */
+int lpb_filter(double* out, const double* v, const int* toff, const double* tw, int ntaps, const double* hs_in, const double* hs_out, double* e_out, double penal, double emin, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_simp_law(double* e, const double* x, double penal, double emin, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_element_energy_f64(double* ce, const double* u, const double* v, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_element_energy_f32(double* ce, const float* u, const float* v, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const double* e, double penal, double emin, double scale, int accumulate, double* part, double* comp, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* volumes[j] of the clipped OC step at nl = 31 multipliers lam[j] (device), weights gv = H (1 / hs) */
+int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv, const double* lam, int nl, double move, double* part, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* dv, double lam, double move, double* part, double* change, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LOADPATH_B200_H */

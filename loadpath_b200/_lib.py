@@ -1,0 +1,94 @@
+"""ctypes binding of liblpb200.so, typed from include/loadpath_b200.h.
+
+Every function the header declares is bound with its argument types; a declared symbol
+missing from the library is an import error, and a nonzero status from any call raises
+LpError. There is no fallback: without the built library (python -m loadpath_b200.build)
+nothing in this package computes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblpb200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "loadpath_b200.h")
+
+_CTYPES = {
+    "int": ctypes.c_int,
+    "long long": ctypes.c_longlong,
+    "float": ctypes.c_float,
+    "double": ctypes.c_double,
+    "void": None,
+}
+_STATUS = {-1: "bad arguments", -2: "kernel launch failed", -3: "size beyond the kernel's limit"}
+
+
+class LpError(RuntimeError):
+    pass
+
+
+def parse_header(path: str = HEADER):
+    """[(name, restype, [argtype, ...])] of every `lpb_*` declaration in the header."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = []
+    for m in re.finditer(r"\b(int|void)\s+(lpb_\w+)\s*\(([^)]*)\)\s*;", text):
+        ret, name, args = m.group(1), m.group(2), m.group(3).strip()
+        types = []
+        if args and args != "void":
+            for a in args.split(","):
+                a = a.strip()
+                if "*" in a:
+                    types.append(ctypes.c_void_p)
+                    continue
+                a = re.sub(r"\bconst\b", "", a).strip()
+                base = " ".join(a.split()[:-1])
+                if base not in _CTYPES:
+                    raise LpError(f"{name}: unsupported argument type {a!r}")
+                types.append(_CTYPES[base])
+        out.append((name, _CTYPES[ret], types))
+    return out
+
+
+class _Lib:
+    def __init__(self):
+        if not os.path.exists(LIB_PATH):
+            raise LpError(f"{LIB_PATH} is not built: run `python -m loadpath_b200.build` "
+                          "(loadpath_b200 has no CPU fallback)")
+        self.dll = ctypes.CDLL(LIB_PATH)
+        self.decls = parse_header()
+        self.fns = {}
+        for name, ret, types in self.decls:
+            try:
+                fn = getattr(self.dll, name)
+            except AttributeError as e:
+                raise LpError(f"{LIB_PATH} does not export {name} declared in {HEADER}") from e
+            fn.restype = ret
+            fn.argtypes = types
+            self.fns[name] = fn
+
+    def __getattr__(self, name):
+        fn = self.fns.get(name)
+        if fn is None:
+            raise AttributeError(name)
+
+        def call(*args):
+            st = fn(*args)
+            if st is not None and st < 0:
+                raise LpError(f"{name}: {_STATUS.get(st, 'error')} (status {st})")
+            return st
+
+        call.__name__ = name
+        return call
+
+
+_LIB = None
+
+
+def lib() -> _Lib:
+    global _LIB
+    if _LIB is None:
+        _LIB = _Lib()
+    return _LIB

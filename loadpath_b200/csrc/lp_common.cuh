@@ -1,0 +1,83 @@
+// Shared definitions for the loadpath_b200 CUDA kernels (sm_100a).
+//
+// Layouts (all C order):
+//   node field  (3, NX, NY, PZ)   NX = nx + 1, NY = ny + 1, PZ >= nz + 1 (z pitch, elements)
+//   cell field  (nx, ny, CPZ)     CPZ >= nz
+//   node mask   (NX, NY, PZ) uint8: bits 0..2 = dof is solved for (alive and not held) per
+//               component; bits 3..5 = dof carries stiffness (alive) per component.
+// Corner k of a cell sits at (k & 1, k >> 1 & 1, k >> 2 & 1); a cell's 24 dofs are ordered
+// 3 * corner + component (loadpath/fem.py:30, loadpath/fem.py:127-145).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define LP_OK 0
+#define LP_ERR_ARG -1
+#define LP_ERR_LAUNCH -2
+#define LP_ERR_SIZE -3
+
+struct LpGrid {
+  int nx, ny, nz;   // cells
+  int pz;           // node z pitch
+  int cpz;          // cell z pitch
+  __host__ __device__ int NX() const { return nx + 1; }
+  __host__ __device__ int NY() const { return ny + 1; }
+  __host__ __device__ int NZ() const { return nz + 1; }
+  __host__ __device__ long long comp_stride() const { return (long long)(nx + 1) * (ny + 1) * pz; }
+  __host__ __device__ long long node(int x, int y, int z) const {
+    return ((long long)x * (ny + 1) + y) * pz + z;
+  }
+  __host__ __device__ long long cell(int x, int y, int z) const {
+    return ((long long)x * ny + y) * cpz + z;
+  }
+  __host__ __device__ long long nodes_padded() const { return (long long)(nx + 1) * (ny + 1) * pz; }
+  __host__ __device__ long long cells_padded() const { return (long long)nx * ny * cpz; }
+};
+
+static inline LpGrid lp_grid(int nx, int ny, int nz, int pz, int cpz) {
+  LpGrid g;
+  g.nx = nx; g.ny = ny; g.nz = nz; g.pz = pz; g.cpz = cpz;
+  return g;
+}
+
+static inline bool lp_grid_ok(const LpGrid& g) {
+  return g.nx >= 1 && g.ny >= 1 && g.nz >= 1 && g.pz >= g.nz + 1 && g.cpz >= g.nz;
+}
+
+static inline int lp_blocks(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 2147483647LL) b = 2147483647LL;
+  return (int)b;
+}
+
+#define LP_LAUNCH_CHECK()                                   \
+  do {                                                      \
+    cudaError_t _e = cudaGetLastError();                    \
+    if (_e != cudaSuccess) return LP_ERR_LAUNCH;            \
+  } while (0)
+
+// corner offsets
+__host__ __device__ __forceinline__ int cx_(int k) { return k & 1; }
+__host__ __device__ __forceinline__ int cy_(int k) { return (k >> 1) & 1; }
+__host__ __device__ __forceinline__ int cz_(int k) { return (k >> 2) & 1; }
+
+template <typename T>
+__device__ __forceinline__ T lp_ldg(const T* p) { return __ldg(p); }
+
+// Block-wide sum of a double; every thread gets the result. blockDim.x <= 1024.
+__device__ __forceinline__ double lp_block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) sh[0] = v;
+  __syncthreads();
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}

@@ -1,0 +1,314 @@
+// SIMP-loop kernels: the cone density filter and its transpose (loadpath/simp.py:1143-1228,
+// loadpath/benchmarks/reference.py:48-71), the SIMP law (loadpath/simp.py:1861), element
+// strain energy u_e^T Ke v_e (loadpath/femops.py:51-78, loadpath/mg.py:975-988), sensitivities
+// (loadpath/benchmarks/reference.py:89-99) and the OC volume pass (reference.py:100-110).
+// All in float64.
+#include "lp_common.cuh"
+
+#define LP_MAX_TAPS 1024
+#define LP_MAX_LAMBDA 64
+
+namespace {
+
+// out[c] = sum_t w_t v[c + d_t] (zeros outside the grid); optional pre-division of v by hs
+// and post-division of out by hs2; optional SIMP law on the result.
+//   mode 0: out = H v
+//   mode 1: out = H (v / hs_in)
+//   mode 2: out = (H v) / hs_out ; e_out = emin + out^p (1 - emin) if e_out != null
+__global__ void k_filter(double* __restrict__ out, const double* __restrict__ v, const int* __restrict__ toff,
+                         const double* __restrict__ tw, int ntaps, const double* __restrict__ hs_in,
+                         const double* __restrict__ hs_out, double* __restrict__ e_out, double penal, double emin,
+                         LpGrid g) {
+  extern __shared__ unsigned char smem_raw[];
+  int* so = reinterpret_cast<int*>(smem_raw);
+  double* sw = reinterpret_cast<double*>(smem_raw + ((3 * ntaps * sizeof(int) + 15) & ~15));
+  for (int i = threadIdx.x; i < ntaps; i += blockDim.x) {
+    so[3 * i] = toff[3 * i];
+    so[3 * i + 1] = toff[3 * i + 1];
+    so[3 * i + 2] = toff[3 * i + 2];
+    sw[i] = tw[i];
+  }
+  __syncthreads();
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    int y = (int)(q % g.ny);
+    int x = (int)(q / g.ny);
+    double s = 0.0;
+    for (int i = 0; i < ntaps; ++i) {
+      int xx = x + so[3 * i], yy = y + so[3 * i + 1], zz = z + so[3 * i + 2];
+      if (xx < 0 || yy < 0 || zz < 0 || xx >= g.nx || yy >= g.ny || zz >= g.nz) continue;
+      long long c = g.cell(xx, yy, zz);
+      double vi = v[c];
+      if (hs_in) vi = vi / hs_in[c];
+      s += sw[i] * vi;
+    }
+    long long c = g.cell(x, y, z);
+    if (hs_out) s = s / hs_out[c];
+    out[c] = s;
+    if (e_out) e_out[c] = emin + pow(s, penal) * (1.0 - emin);
+  }
+}
+
+// e = emin + x^p (1 - emin) on the grid's cells (padding untouched)
+__global__ void k_simp_law(double* __restrict__ e, const double* __restrict__ x, double penal, double emin, LpGrid g) {
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    long long c = g.cell((int)(q / g.ny), (int)(q % g.ny), z);
+    e[c] = emin + pow(x[c], penal) * (1.0 - emin);
+  }
+}
+
+// per-cell u_e^T ke v_e on the node grid (v = u when v is null), float64; also optional
+// compliance partial sum_c e_c * ce_c
+template <typename T>
+__global__ void k_element_energy(double* __restrict__ ce, const T* __restrict__ u, const T* __restrict__ v,
+                                 const double* __restrict__ ke, LpGrid g) {
+  __shared__ double sk[576];
+  for (int i = threadIdx.x; i < 576; i += blockDim.x) sk[i] = ke[i];
+  __syncthreads();
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long cs = g.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    int y = (int)(q % g.ny);
+    int x = (int)(q / g.ny);
+    double ue[24], ve[24];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      long long n = g.node(x + cx_(k), y + cy_(k), z + cz_(k));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ue[3 * k + c] = (double)u[c * cs + n];
+        ve[3 * k + c] = v ? (double)v[c * cs + n] : ue[3 * k + c];
+      }
+    }
+    // j outer, k inner, (u_j ke_jk) v_k: the reference's summation order
+    double s = 0.0;
+    for (int j = 0; j < 24; ++j) {
+      double uj = ue[j];
+#pragma unroll
+      for (int k = 0; k < 24; ++k) s += uj * sk[j * 24 + k] * ve[k];
+    }
+    ce[g.cell(x, y, z)] = s;
+  }
+}
+
+// dc = -p (1 - emin) x^(p-1) ce * scale (accumulated into dc when accumulate != 0);
+// partial compliance sum_c e_c ce_c into part[block]
+__global__ void k_sensitivity(double* __restrict__ dc, const double* __restrict__ xphys, const double* __restrict__ ce,
+                              const double* __restrict__ e, double penal, double emin, double scale, int accumulate,
+                              LpGrid g, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  double acc = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    int y = (int)(q % g.ny);
+    int x = (int)(q / g.ny);
+    long long c = g.cell(x, y, z);
+    double xv = xphys[c];
+    double d = -penal * (1.0 - emin) * pow(xv, penal - 1.0) * ce[c] * scale;
+    dc[c] = accumulate ? dc[c] + d : d;
+    if (e) acc += e[c] * ce[c] * scale;
+  }
+  acc = lp_block_sum(acc, sh);
+  if (part && threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// OC trial step for NL multipliers at once (the next levels of the bisection tree): for each
+// lambda_j the step x sqrt(-dc / dv / lambda_j) clipped to [max(0, x - move), min(1, x + move)]
+// (loadpath/benchmarks/reference.py:103), and partial sums of xnew * gv where gv = H (1 / hs)
+// weighs a cell's share of the filtered volume. The step is formed as
+// (x sqrt(-dc / dv)) / sqrt(lambda_j): one square root per cell; only the volume comparisons use
+// it, the accepted step is recomputed with the reference's expression by k_oc_apply.
+template <int NL>
+__global__ void __launch_bounds__(256) k_oc_volumes(const double* __restrict__ x, const double* __restrict__ dc,
+                                                    const double* __restrict__ dv, const double* __restrict__ gv,
+                                                    const double* __restrict__ lam, double move, LpGrid g,
+                                                    double* __restrict__ part) {
+  __shared__ double s_isl[NL];
+  __shared__ double sacc[NL][8];
+  if (threadIdx.x < NL) s_isl[threadIdx.x] = 1.0 / sqrt(lam[threadIdx.x]);
+  __syncthreads();
+  double acc[NL];
+#pragma unroll
+  for (int j = 0; j < NL; ++j) acc[j] = 0.0;
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    int y = (int)(q % g.ny);
+    int xx = (int)(q / g.ny);
+    long long c = g.cell(xx, y, z);
+    double xv = x[c], gw = gv[c];
+    double ts = xv * sqrt(-dc[c] / dv[c]);
+    double lo = fmax(0.0, xv - move), hi = fmin(1.0, xv + move);
+#pragma unroll
+    for (int j = 0; j < NL; ++j) acc[j] += fmax(lo, fmin(hi, ts * s_isl[j])) * gw;
+  }
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NL; ++j) {
+    double s = acc[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) sacc[j][wid] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NL) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += sacc[threadIdx.x][w];
+    part[(long long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void k_oc_final(const double* __restrict__ part, int nblocks, int nl, double* __restrict__ out) {
+  __shared__ double sh[32];
+  for (int j = 0; j < nl; ++j) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) s += part[(long long)j * nblocks + i];
+    s = lp_block_sum(s, sh);
+    if (threadIdx.x == 0) out[j] = s;
+  }
+}
+
+// the OC step at one multiplier: xnew and the change max|xnew - x| partials
+__global__ void k_oc_apply(double* __restrict__ xnew, const double* __restrict__ x, const double* __restrict__ dc,
+                           const double* __restrict__ dv, double lam, double move, LpGrid g,
+                           double* __restrict__ part) {
+  __shared__ double sh[32];
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  double mx = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % g.nz);
+    long long q = t / g.nz;
+    int y = (int)(q % g.ny);
+    int xx = (int)(q / g.ny);
+    long long c = g.cell(xx, y, z);
+    double xv = x[c];
+    double xn = xv * sqrt(-dc[c] / dv[c] / lam);
+    xn = fmax(0.0, fmax(xv - move, fmin(1.0, fmin(xv + move, xn))));
+    xnew[c] = xn;
+    mx = fmax(mx, fabs(xn - xv));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+    part[blockIdx.x] = m;
+  }
+}
+
+__global__ void k_max_final2(const double* __restrict__ part, int n, double* __restrict__ out) {
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, part[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  __shared__ double sh[32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sh[w]);
+    *out = r;
+  }
+}
+
+__global__ void k_sum_final_s(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
+}
+
+}  // namespace
+
+#define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
+#define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
+#define LP_ST ((cudaStream_t)stream)
+#define LP_SIMP_BLOCKS 592
+
+extern "C" {
+
+int lpb_filter(double* out, const double* v, const int* toff, const double* tw, int ntaps, const double* hs_in,
+               const double* hs_out, double* e_out, double penal, double emin, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !out || !v || !toff || !tw || ntaps < 1 || ntaps > LP_MAX_TAPS) return LP_ERR_ARG;
+  if (out == v) return LP_ERR_ARG;
+  size_t smem = ((3 * ntaps * sizeof(int) + 15) & ~(size_t)15) + ntaps * sizeof(double);
+  long long total = (long long)g.nx * g.ny * g.nz;
+  k_filter<<<lp_blocks(total, 256), 256, smem, LP_ST>>>(out, v, toff, tw, ntaps, hs_in, hs_out, e_out, penal, emin, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_simp_law(double* e, const double* x, double penal, double emin, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !e || !x) return LP_ERR_ARG;
+  long long total = (long long)g.nx * g.ny * g.nz;
+  k_simp_law<<<lp_blocks(total, 256), 256, 0, LP_ST>>>(e, x, penal, emin, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_element_energy_f64(double* ce, const double* u, const double* v, const double* ke, LP_GRID_ARGS,
+                           void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
+  long long total = (long long)g.nx * g.ny * g.nz;
+  k_element_energy<double><<<lp_blocks(total, 128), 128, 0, LP_ST>>>(ce, u, v, ke, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_element_energy_f32(double* ce, const float* u, const float* v, const double* ke, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
+  long long total = (long long)g.nx * g.ny * g.nz;
+  k_element_energy<float><<<lp_blocks(total, 128), 128, 0, LP_ST>>>(ce, u, v, ke, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// dc (+)= -p (1 - emin) x^(p-1) ce * scale; *comp = sum e * ce * scale (if e and comp given)
+int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const double* e, double penal, double emin,
+                    double scale, int accumulate, double* part, double* comp, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !dc || !xphys || !ce || !part) return LP_ERR_ARG;
+  k_sensitivity<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(dc, xphys, ce, e, penal, emin, scale, accumulate, g, part);
+  if (comp) k_sum_final_s<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, comp);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// volumes[j] = sum_c xnew(lam[j])_c gv_c for nl = 31 multipliers; part: nl * 592 doubles
+int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv,
+                   const double* lam, int nl, double move, double* part, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || nl < 1 || nl > LP_MAX_LAMBDA || !volumes || !x || !dc || !dv || !gv || !lam || !part)
+    return LP_ERR_ARG;
+  if (nl != 31) return LP_ERR_ARG;
+  k_oc_volumes<31><<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(x, dc, dv, gv, lam, move, g, part);
+  k_oc_final<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, nl, volumes);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* dv, double lam, double move,
+                 double* part, double* change, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !xnew || !x || !dc || !dv || !part || !change) return LP_ERR_ARG;
+  k_oc_apply<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xnew, x, dc, dv, lam, move, g, part);
+  k_max_final2<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, change);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,472 @@
+// Vector passes of the V-cycle and the PCG (loadpath/mgops.py:302-360, :557-585, :593-773):
+// Chebyshev updates, fused CG step with |r|^2, p = z + beta p, dots, casts, and the grid
+// transfers (residual -> pad -> full-weighting restriction -> coarse mask; prolongation ->
+// fine mask -> add).
+//
+// Reductions are deterministic: a fixed number of blocks (LP_RED_BLOCKS) each write a
+// partial sum and one block adds the partials in order, so a given input always gives the
+// same bits. Scalars the solver needs between kernels (rz, pap, |r|^2, alpha, beta) live in
+// device memory so an iteration never waits on the host.
+#include "lp_common.cuh"
+
+#define LP_RED_BLOCKS 592   // 4 per SM on 148 SMs
+#define LP_RED_THREADS 512
+
+namespace {
+
+template <typename Ta, typename Tb>
+__global__ void k_dot_partial(const Ta* __restrict__ a, const Tb* __restrict__ b, long long n,
+                              double* __restrict__ part) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// out[0] = sum(part); optional: out_sqrt = sqrt(sum)
+__global__ void k_sum_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
+}
+
+// x += alpha p ; r -= alpha ap ; r32 = (float) r ; partial |r|^2. alpha = num / den.
+__global__ void k_cg_step(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                          const double* __restrict__ ap, float* __restrict__ r32, long long n,
+                          const double* __restrict__ num, const double* __restrict__ den, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const double alpha = (*num) / (*den);
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * ap[i];
+    r[i] = ri;
+    if (r32) r32[i] = (float)ri;
+    s += ri * ri;
+  }
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// p = z + (num / den) p, z in float32 or float64
+template <typename Tz>
+__global__ void k_xpby(double* __restrict__ p, const Tz* __restrict__ z, long long n, const double* __restrict__ num,
+                       const double* __restrict__ den) {
+  const double beta = (*num) / (*den);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = (double)z[i] + beta * p[i];
+}
+
+template <typename Ta, typename Tb>
+__global__ void k_cast(Tb* __restrict__ out, const Ta* __restrict__ a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (Tb)a[i];
+}
+
+// out = a x + b y
+template <typename T>
+__global__ void k_axpby(T* __restrict__ out, T a, const T* __restrict__ x, T b, const T* __restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = a * x[i] + (y ? b * y[i] : T(0));
+}
+
+// Chebyshev start from zero: x = 0; r = b; d = (dinv b) s        (loadpath/mgops.py:321-328)
+template <typename T>
+__global__ void k_cheb_start(const T* __restrict__ b, const T* __restrict__ dinv, T s, T* __restrict__ x,
+                             T* __restrict__ r, T* __restrict__ d, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T bi = b[i];
+    x[i] = T(0);
+    r[i] = bi;
+    d[i] = (dinv[i] * bi) * s;
+  }
+}
+
+// r = b - ax; d = s dinv r                                        (loadpath/mgops.py:314-319)
+template <typename T>
+__global__ void k_residual_scaled(const T* __restrict__ b, const T* __restrict__ ax, const T* __restrict__ dinv, T s,
+                                  T* __restrict__ r, T* __restrict__ d, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T ri = b[i] - ax[i];
+    r[i] = ri;
+    d[i] = s * dinv[i] * ri;
+  }
+}
+
+// x += d; unless last: r -= ad; d = c1 d + c2 dinv r             (loadpath/mgops.py:334-343)
+template <typename T>
+__global__ void k_cheb(T* __restrict__ x, T* __restrict__ d, T* __restrict__ r, const T* __restrict__ ad,
+                       const T* __restrict__ dinv, T c1, T c2, int last, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T di = d[i];
+    x[i] += di;
+    if (!last) {
+      T ri = r[i] - ad[i];
+      r[i] = ri;
+      d[i] = c1 * di + c2 * dinv[i] * ri;
+    }
+  }
+}
+
+// damped Jacobi: x += omega dinv (b - ax), x = 0 start handled by the caller
+template <typename T>
+__global__ void k_jacobi(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ax,
+                         const T* __restrict__ dinv, T omega, int from_zero, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (from_zero)
+      x[i] = omega * dinv[i] * b[i];
+    else
+      x[i] += omega * dinv[i] * (b[i] - ax[i]);
+  }
+}
+
+// rc = restrict(((b - ax) * m) zero-padded) * cm, one coarse node per thread
+// (loadpath/mgops.py:666-711)
+template <typename T>
+__global__ void k_restrict_residual(T* __restrict__ rc, const T* __restrict__ b, const T* __restrict__ ax,
+                                    const uint8_t* __restrict__ m, const uint8_t* __restrict__ cm, LpGrid gf,
+                                    LpGrid gc) {
+  const int CX = gc.NX(), CY = gc.NY(), CZ = gc.NZ();
+  const int FX = gf.NX(), FY = gf.NY(), FZ = gf.NZ();
+  const long long total = (long long)CX * CY * CZ;
+  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int Z = (int)(t % CZ);
+    long long q = t / CZ;
+    int Y = (int)(q % CY);
+    int X = (int)(q / CY);
+    long long cn = gc.node(X, Y, Z);
+    uint8_t cmb = cm[cn];
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int a = -1; a <= 1; ++a) {
+      int x = 2 * X + a;
+      if (x < 0 || x >= FX) continue;
+      T wa = a ? T(0.5) : T(1);
+      for (int bb = -1; bb <= 1; ++bb) {
+        int y = 2 * Y + bb;
+        if (y < 0 || y >= FY) continue;
+        T wb = wa * (bb ? T(0.5) : T(1));
+        for (int e = -1; e <= 1; ++e) {
+          int z = 2 * Z + e;
+          if (z < 0 || z >= FZ) continue;
+          T we = wb * (e ? T(0.5) : T(1));
+          long long fn = gf.node(x, y, z);
+          uint8_t mb = m[fn];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            if ((mb >> i) & 1) acc[i] += (b[i * fcs + fn] - ax[i * fcs + fn]) * we;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) rc[i * ccs + cn] = ((cmb >> i) & 1) ? acc[i] : T(0);
+  }
+}
+
+// x += prolong(xc * cm)[fine nodes] * m, one fine node per thread (loadpath/mgops.py:714-750)
+template <typename T>
+__global__ void k_prolong_add(T* __restrict__ x, const T* __restrict__ xc, const uint8_t* __restrict__ cm,
+                              const uint8_t* __restrict__ m, LpGrid gf, LpGrid gc) {
+  const int FX = gf.NX(), FY = gf.NY(), FZ = gf.NZ();
+  const long long total = (long long)FX * FY * FZ;
+  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int z = (int)(t % FZ);
+    long long q = t / FZ;
+    int y = (int)(q % FY);
+    int xx = (int)(q / FY);
+    long long fn = gf.node(xx, y, z);
+    uint8_t mb = m[fn];
+    if ((mb & 7) == 0) continue;
+    int x0 = xx >> 1, y0 = y >> 1, z0 = z >> 1;
+    int nxo = (xx & 1) + 1, nyo = (y & 1) + 1, nzo = (z & 1) + 1;
+    T w = T(1);
+    if (xx & 1) w *= T(0.5);
+    if (y & 1) w *= T(0.5);
+    if (z & 1) w *= T(0.5);
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int a = 0; a < nxo; ++a)
+      for (int bb = 0; bb < nyo; ++bb)
+        for (int e = 0; e < nzo; ++e) {
+          long long cn = gc.node(x0 + a, y0 + bb, z0 + e);
+          uint8_t cmb = cm[cn];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+            if ((cmb >> i) & 1) acc[i] += xc[i * ccs + cn];
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      if ((mb >> i) & 1) x[i * fcs + fn] += acc[i] * w;
+  }
+}
+
+// out = u * mask (per component bit)
+template <typename T>
+__global__ void k_mask_field(T* __restrict__ out, const T* __restrict__ u, const uint8_t* __restrict__ m, LpGrid g,
+                             int bitshift) {
+  const long long nn = g.nodes_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
+    int c = (int)(t / nn);
+    long long n = t - c * nn;
+    out[t] = ((m[n] >> (c + bitshift)) & 1) ? u[t] : T(0);
+  }
+}
+
+// v *= 1 / sqrt(*nrm2) (power iteration normalisation); leaves v alone when the norm is 0
+template <typename T>
+__global__ void k_scale_rsqrt(T* __restrict__ v, long long n, const double* __restrict__ nrm2) {
+  double s = *nrm2;
+  if (s <= 0.0) return;
+  T f = (T)(1.0 / sqrt(s));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = v[i] / (T)sqrt(s);
+  (void)f;
+}
+
+// av = dinv * av * mask
+template <typename T>
+__global__ void k_dinv_mask(T* __restrict__ av, const T* __restrict__ dinv, const uint8_t* __restrict__ m, LpGrid g) {
+  const long long nn = g.nodes_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
+    int c = (int)(t / nn);
+    long long n = t - c * nn;
+    av[t] = ((m[n] >> c) & 1) ? dinv[t] * av[t] : T(0);
+  }
+}
+
+}  // namespace
+
+#define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
+#define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
+#define LP_ST ((cudaStream_t)stream)
+#define LP_VEC_GRID(n) lp_blocks((n), 256) > 148 * 32 ? 148 * 32 : lp_blocks((n), 256), 256, 0, LP_ST
+
+extern "C" {
+
+int lpb_reduce_blocks(void) { return LP_RED_BLOCKS; }
+
+int lpb_dot_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream) {
+  if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;
+  k_dot_partial<double, double><<<LP_RED_BLOCKS, LP_RED_THREADS, 0, LP_ST>>>(a, b, n, part);
+  k_sum_final<<<1, 1024, 0, LP_ST>>>(part, LP_RED_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_dot_f32(const float* a, const float* b, long long n, double* part, double* out, void* stream) {
+  if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;
+  k_dot_partial<float, float><<<LP_RED_BLOCKS, LP_RED_THREADS, 0, LP_ST>>>(a, b, n, part);
+  k_sum_final<<<1, 1024, 0, LP_ST>>>(part, LP_RED_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_dot_f64_f32(const double* a, const float* b, long long n, double* part, double* out, void* stream) {
+  if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;
+  k_dot_partial<double, float><<<LP_RED_BLOCKS, LP_RED_THREADS, 0, LP_ST>>>(a, b, n, part);
+  k_sum_final<<<1, 1024, 0, LP_ST>>>(part, LP_RED_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cg_step(double* x, double* r, const double* p, const double* ap, float* r32, long long n, const double* num,
+                const double* den, double* part, double* rr, void* stream) {
+  if (!x || !r || !p || !ap || !num || !den || !part || !rr) return LP_ERR_ARG;
+  k_cg_step<<<LP_RED_BLOCKS, LP_RED_THREADS, 0, LP_ST>>>(x, r, p, ap, r32, n, num, den, part);
+  k_sum_final<<<1, 1024, 0, LP_ST>>>(part, LP_RED_BLOCKS, rr);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_xpby_f32(double* p, const float* z, long long n, const double* num, const double* den, void* stream) {
+  if (!p || !z || !num || !den) return LP_ERR_ARG;
+  k_xpby<float><<<LP_VEC_GRID(n)>>>(p, z, n, num, den);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_xpby_f64(double* p, const double* z, long long n, const double* num, const double* den, void* stream) {
+  if (!p || !z || !num || !den) return LP_ERR_ARG;
+  k_xpby<double><<<LP_VEC_GRID(n)>>>(p, z, n, num, den);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_axpby_f64(double* out, double a, const double* x, double b, const double* y, long long n, void* stream) {
+  if (!out || !x) return LP_ERR_ARG;
+  k_axpby<double><<<LP_VEC_GRID(n)>>>(out, a, x, b, y, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_axpby_f32(float* out, float a, const float* x, float b, const float* y, long long n, void* stream) {
+  if (!out || !x) return LP_ERR_ARG;
+  k_axpby<float><<<LP_VEC_GRID(n)>>>(out, a, x, b, y, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cast_f64_f32(float* out, const double* a, long long n, void* stream) {
+  if (!out || !a) return LP_ERR_ARG;
+  k_cast<double, float><<<LP_VEC_GRID(n)>>>(out, a, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cast_f32_f64(double* out, const float* a, long long n, void* stream) {
+  if (!out || !a) return LP_ERR_ARG;
+  k_cast<float, double><<<LP_VEC_GRID(n)>>>(out, a, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cheb_start_f32(const float* b, const float* dinv, float s, float* x, float* r, float* d, long long n,
+                       void* stream) {
+  k_cheb_start<float><<<LP_VEC_GRID(n)>>>(b, dinv, s, x, r, d, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cheb_start_f64(const double* b, const double* dinv, double s, double* x, double* r, double* d, long long n,
+                       void* stream) {
+  k_cheb_start<double><<<LP_VEC_GRID(n)>>>(b, dinv, s, x, r, d, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, float s, float* r, float* d,
+                            long long n, void* stream) {
+  k_residual_scaled<float><<<LP_VEC_GRID(n)>>>(b, ax, dinv, s, r, d, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, double s, double* r, double* d,
+                            long long n, void* stream) {
+  k_residual_scaled<double><<<LP_VEC_GRID(n)>>>(b, ax, dinv, s, r, d, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, float c1, float c2, int last,
+                 long long n, void* stream) {
+  k_cheb<float><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, c1, c2, last, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, double c1, double c2, int last,
+                 long long n, void* stream) {
+  k_cheb<double><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, c1, c2, last, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero,
+                   long long n, void* stream) {
+  k_jacobi<float><<<LP_VEC_GRID(n)>>>(x, b, ax, dinv, omega, from_zero, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_jacobi_f64(double* x, const double* b, const double* ax, const double* dinv, double omega, int from_zero,
+                   long long n, void* stream) {
+  k_jacobi<double><<<LP_VEC_GRID(n)>>>(x, b, ax, dinv, omega, from_zero, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+#define LP_FC_ARGS int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz
+#define LP_GF lp_grid(fnx, fny, fnz, fpz, fcpz)
+#define LP_GC lp_grid(cnx, cny, cnz, cpz_, ccpz)
+
+int lpb_restrict_residual_f32(float* rc, const float* b, const float* ax, const uint8_t* m, const uint8_t* cm,
+                              LP_FC_ARGS, void* stream) {
+  LpGrid gf = LP_GF, gc = LP_GC;
+  if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
+  k_restrict_residual<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, const uint8_t* m, const uint8_t* cm,
+                              LP_FC_ARGS, void* stream) {
+  LpGrid gf = LP_GF, gc = LP_GC;
+  if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
+  k_restrict_residual<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
+  LpGrid gf = LP_GF, gc = LP_GC;
+  if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
+  k_prolong_add<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
+  LpGrid gf = LP_GF, gc = LP_GC;
+  if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
+  k_prolong_add<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_mask_field_f32(float* out, const float* u, const uint8_t* m, LP_GRID_ARGS, int bitshift, void* stream) {
+  LpGrid g = LP_GRID;
+  long long n = 3 * g.nodes_padded();
+  k_mask_field<float><<<LP_VEC_GRID(n)>>>(out, u, m, g, bitshift);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_mask_field_f64(double* out, const double* u, const uint8_t* m, LP_GRID_ARGS, int bitshift, void* stream) {
+  LpGrid g = LP_GRID;
+  long long n = 3 * g.nodes_padded();
+  k_mask_field<double><<<LP_VEC_GRID(n)>>>(out, u, m, g, bitshift);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_scale_rsqrt_f32(float* v, long long n, const double* nrm2, void* stream) {
+  k_scale_rsqrt<float><<<LP_VEC_GRID(n)>>>(v, n, nrm2);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_scale_rsqrt_f64(double* v, long long n, const double* nrm2, void* stream) {
+  k_scale_rsqrt<double><<<LP_VEC_GRID(n)>>>(v, n, nrm2);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_dinv_mask_f32(float* av, const float* dinv, const uint8_t* m, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  long long n = 3 * g.nodes_padded();
+  k_dinv_mask<float><<<LP_VEC_GRID(n)>>>(av, dinv, m, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_dinv_mask_f64(double* av, const double* dinv, const uint8_t* m, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  long long n = 3 * g.nodes_padded();
+  k_dinv_mask<double><<<LP_VEC_GRID(n)>>>(av, dinv, m, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+}  // extern "C"

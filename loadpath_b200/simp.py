@@ -1,0 +1,238 @@
+"""The SIMP loop on the device: density filter, SIMP law, solve, sensitivities, OC update.
+
+Mirrors the reference pieces that sit on the hot path:
+  - `density_filter(dims, radius, pad)` -> (H, hs) with H supporting `@` and `.T`
+    (loadpath/simp.py:1143-1228: the cone stencil w = r - |d| pitch > 0 within floor(r / pitch)
+    cells; H is symmetric; hs = full-kernel sum if padded, else row sums)
+  - `_project` / `_dproject` (loadpath/simp.py:1443-1450)
+  - `Top3dLoop`: the plain SIMP loop of the reference's top3d port
+    (loadpath/benchmarks/reference.py:74-117): E = Emin + x^p (1 - Emin), compliance and
+    sensitivities, density-filter chain rule, OC bisection on the multiplier with the volume
+    measured on the filtered densities, stop on change <= 0.01 or the iteration cap.
+Everything per iteration runs in this package's kernels on device-resident fields; the host
+walks the bisection tree (a few doubles per pass) and reads the compliance and change.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from ._lib import lib
+from .grid import DevGrid, ptr, stream_handle
+from .mg import BoxMesh, GridElasticity
+
+__all__ = ["filter_taps", "DeviceFilter", "density_filter", "Top3dLoop", "_project", "_dproject"]
+
+
+def filter_taps(radius: float, pitch: float = 1.0):
+    """[(dx, dy, dz), w] of the cone filter (loadpath/simp.py:1148-1161)."""
+    reach = int(np.floor(radius / pitch))
+    out = []
+    for dx in range(-reach, reach + 1):
+        for dy in range(-reach, reach + 1):
+            for dz in range(-reach, reach + 1):
+                w = radius - math.sqrt(dx * dx + dy * dy + dz * dz) * pitch
+                if w > 0:
+                    out.append(((dx, dy, dz), float(w)))
+    return out
+
+
+class DeviceFilter:
+    """H on a device cell grid (zeros outside the grid)."""
+
+    def __init__(self, grid: DevGrid, radius: float, pitch: float = 1.0, pad: bool = False):
+        self.grid = grid
+        taps = filter_taps(radius, pitch)
+        self.ntaps = len(taps)
+        self.toff = torch.tensor([list(d) for d, _ in taps], dtype=torch.int32, device=grid.device).reshape(-1)
+        self.tw = torch.tensor([w for _, w in taps], dtype=torch.float64, device=grid.device)
+        self.full = float(sum(w for _, w in taps))
+        ones = grid.cell_field(torch.float64)
+        ones[:, :, :grid.nz] = 1.0
+        self.rowsum = self.apply(grid.cell_field(torch.float64), ones)
+        if pad:
+            self.hs = grid.cell_field(torch.float64)
+            self.hs[:, :, :grid.nz] = self.full
+        else:
+            self.hs = self.rowsum
+        # H (1 / hs): the filtered volume's weights, and top3d's dv = H (1 / hs)
+        self.gv = self.apply(grid.cell_field(torch.float64), ones, hs_in=self.hs)
+
+    def apply(self, out, v, hs_in=None, hs_out=None, e_out=None, penal=3.0, emin=1e-9):
+        """out = H (v / hs_in) / hs_out; with e_out also e_out = emin + out^p (1 - emin)."""
+        lib().lpb_filter(out.data_ptr(), v.data_ptr(), self.toff.data_ptr(), self.tw.data_ptr(), self.ntaps,
+                         ptr(hs_in), ptr(hs_out), ptr(e_out), float(penal), float(emin), *self.grid.args,
+                         stream_handle())
+        return out
+
+
+class _HostFilter:
+    """`H @ v` / `H.T @ v` on host vectors in the grid's C order, computed on the device."""
+
+    def __init__(self, dev: DeviceFilter):
+        self.dev = dev
+        self.T = self
+        n = dev.grid.nx * dev.grid.ny * dev.grid.nz
+        self.shape = (n, n)
+
+    def __matmul__(self, v):
+        g = self.dev.grid
+        vd = g.cells_to_dev(np.asarray(v, np.float64).reshape(g.cells), torch.float64)
+        out = self.dev.apply(g.cell_field(torch.float64), vd)
+        return g.cells_to_host(out).reshape(-1)
+
+    def sum(self, axis=1):
+        return self.dev.grid.cells_to_host(self.dev.rowsum).reshape(-1)
+
+
+def density_filter(dims, radius, pad=True, pitch=1.0, device="cuda"):
+    """(H, hs) of the cone filter on a full box of cells in C order (loadpath/simp.py:1181-1228)."""
+    g = DevGrid(dims, device)
+    f = DeviceFilter(g, radius, pitch, pad)
+    return _HostFilter(f), g.cells_to_host(f.hs).reshape(-1)
+
+
+def _project(xt, beta, eta):
+    """tanh Heaviside projection (loadpath/simp.py:1443-1446)."""
+    den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+    return (np.tanh(beta * eta) + np.tanh(beta * (xt - eta))) / den
+
+
+def _dproject(xt, beta, eta):
+    """its derivative (loadpath/simp.py:1448-1450)."""
+    den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+    return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+class Top3dLoop:
+    """top3d's SIMP loop with the density filter, on the device
+    (loadpath/benchmarks/reference.py:74-117), solved by the device MG-PCG.
+
+    dims: cells (even counts); fixed_grid: bool (3, nx+1, ny+1, nz+1); f_grid: float64 loads on
+    the same grid; x0: optional initial density (cells), default volfrac everywhere."""
+
+    def __init__(self, dims, volfrac, rmin, fixed_grid, f_grid, nu=0.3, element=None, penal=3.0, emin=1e-9,
+                 move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=500,
+                 smoother="chebyshev", warm_start=True, device="cuda"):
+        dims = tuple(int(d) for d in dims)
+        if any(d % 2 for d in dims):
+            raise ValueError("the device SIMP loop takes even cell counts (the multigrid pads odd ones)")
+        self.dims = dims
+        self.volfrac, self.penal, self.emin, self.move = float(volfrac), float(penal), float(emin), float(move)
+        self.mesh = BoxMesh(dims)
+        flat = np.asarray(fixed_grid, bool).reshape(3, -1)
+        fixed = np.empty(self.mesh.n_dof, bool)
+        for i in range(3):
+            fixed[i::3] = flat[i]
+        self.ge = GridElasticity(self.mesh, nu, fixed, rtol=rtol, maxiter=maxiter, coarse_cells=coarse_cells,
+                                 dtype=dtype, element=element, smoother=smoother, device=device)
+        g = self.ge.g0
+        self.grid = g
+        self.filter = DeviceFilter(g, rmin, pad=False)
+        self.f = g.nodes_to_dev(np.asarray(f_grid, np.float64), torch.float64)
+        self.x = g.cell_field(torch.float64)
+        if x0 is None:
+            self.x[:, :, :g.nz] = self.volfrac
+        else:
+            g.cells_to_dev(np.asarray(x0, np.float64), torch.float64, out=self.x)
+        self.xphys = self.x.clone()
+        self.xnew = g.cell_field(torch.float64)
+        self.e = g.cell_field(torch.float64)
+        self.ce = g.cell_field(torch.float64)
+        self.dc = g.cell_field(torch.float64)
+        self.dcf = g.cell_field(torch.float64)
+        self.u = None
+        self.warm_start = warm_start
+        self.ncell = dims[0] * dims[1] * dims[2]
+        self._scal = torch.zeros(64, dtype=torch.float64, device=g.device)
+        self._part = torch.zeros(31 * 592 + 1024, dtype=torch.float64, device=g.device)
+        self._lam = torch.zeros(31, dtype=torch.float64, device=g.device)
+        self._vols = torch.zeros(31, dtype=torch.float64, device=g.device)
+        self.loop = 0
+        self.history = []
+        lib().lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, stream_handle())
+
+    # ---- one iteration -------------------------------------------------------------------
+    def solve(self):
+        self.ge.set_moduli_device(self.e)
+        x0 = self.u if (self.warm_start and self.u is not None) else None
+        self.u = self.ge.solve_device(self.f, x0)
+        return self.u
+
+    def sensitivities(self):
+        """ce, compliance (device scalar), dc = H (dc_raw / hs) (loadpath/benchmarks/reference.py:91-99)."""
+        L = lib()
+        st = stream_handle()
+        g = self.grid
+        self.ge.strain_energy_device(self.u, out=self.ce)
+        L.lpb_sensitivity(self.dc.data_ptr(), self.xphys.data_ptr(), self.ce.data_ptr(), self.e.data_ptr(),
+                          self.penal, self.emin, 1.0, 0, self._part.data_ptr(), self._scal[0:].data_ptr(), *g.args, st)
+        self.filter.apply(self.dcf, self.dc, hs_in=self.filter.hs)
+
+    def oc(self):
+        """top3d's bisection on the volume multiplier (loadpath/benchmarks/reference.py:100-110),
+        five levels of the bisection tree per pass over the cells."""
+        L = lib()
+        st = stream_handle()
+        g = self.grid
+        target = self.volfrac * self.ncell
+        l1, l2 = 0.0, 1e9
+        lmid = None
+        while (l2 - l1) / (l1 + l2) > 1e-3:
+            # the 31 midpoints the next five bisection levels can reach, breadth first
+            nodes = [(l1, l2)]
+            cands = []
+            for depth in range(5):
+                nxt = []
+                for a, b in nodes:
+                    m = 0.5 * (b + a)
+                    cands.append(m)
+                    nxt += [(a, m), (m, b)]
+                nodes = nxt
+            self._lam.copy_(torch.tensor(cands, dtype=torch.float64))
+            L.lpb_oc_volumes(self._vols.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(),
+                             self.filter.gv.data_ptr(), self._lam.data_ptr(), 31, self.move, self._part.data_ptr(),
+                             *g.args, st)
+            vols = self._vols.cpu().numpy()
+            idx = 0
+            for depth in range(5):
+                if not (l2 - l1) / (l1 + l2) > 1e-3:
+                    break
+                lmid = 0.5 * (l2 + l1)
+                if vols[idx] > target:
+                    l1 = lmid
+                    idx = 2 * idx + 2
+                else:
+                    l2 = lmid
+                    idx = 2 * idx + 1
+        L.lpb_oc_apply(self.xnew.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(), lmid,
+                       self.move, self._part.data_ptr(), self._scal[1:].data_ptr(), *g.args, st)
+        self.lmid = lmid
+
+    def step(self):
+        """One iteration; returns (compliance, change) as top3d reports them."""
+        g = self.grid
+        self.loop += 1
+        self.solve()
+        self.sensitivities()
+        self.oc()
+        # xphys = H xnew / hs, and the next iteration's moduli
+        self.filter.apply(self.xphys, self.xnew, hs_out=self.filter.hs, e_out=self.e, penal=self.penal,
+                          emin=self.emin)
+        self.x, self.xnew = self.xnew, self.x
+        c, change = (float(v) for v in self._scal[:2].cpu().numpy())
+        self.history.append((c, change, self.ge.last_iters))
+        return c, change
+
+    def run(self, maxit=200, on_iter=None):
+        change = 1.0
+        while change > 0.01 and self.loop < maxit:
+            c, change = self.step()
+            if on_iter is not None:
+                on_iter(self.loop, c, change)
+        return self
+
+    def xphys_host(self):
+        return self.grid.cells_to_host(self.xphys)

@@ -1,0 +1,61 @@
+"""The C ABI library: builds for sm_100a, loads without a GPU, and exports exactly what
+include/loadpath_b200.h declares. CPU only (no kernel is called)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+
+from loadpath_b200 import build
+from loadpath_b200._lib import HEADER, LIB_PATH, lib, parse_header
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    build.build()
+    assert os.path.exists(LIB_PATH)
+    decls = parse_header()
+    names = [d[0] for d in decls]
+    assert len(names) == len(set(names))
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (lpb_\w+)", out))
+    assert set(names) <= exported, sorted(set(names) - exported)
+    # nothing exported that the header does not declare
+    assert exported <= set(names), sorted(exported - set(names))
+    L = lib()
+    assert set(L.fns) == set(names)
+
+
+def test_header_is_plain_c():
+    text = open(HEADER).read()
+    assert "torch" not in text and "at::" not in text and "std::" not in text
+    for name, ret, types in parse_header():
+        assert ret is ctypes.c_int, name
+
+
+def test_modal_ke_pattern_host_only():
+    # lpb_modal_ke is host code: the 45 corner-parity coefficients reproduce Ke exactly
+    from loadpath_b200.fem import CORNERS, hex8_ke
+
+    s = 2 * CORNERS - 1
+    h = np.array([[np.prod([s[k, a] for a in range(3) if (m >> a) & 1]) for k in range(8)] for m in range(8)])
+    t = np.kron(h, np.eye(3))
+    rows = [3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12, 13, 13, 14, 14, 14, 15, 15,
+            16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21, 22, 23]
+    cols = [3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12, 8, 13, 3, 7, 14, 15, 19,
+            11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22, 23]
+    for el in ("im", "plain"):
+        for nu in (0.2, 0.3, 0.45):
+            ke = np.ascontiguousarray(hex8_ke(nu, el))
+            km = np.zeros(45)
+            assert lib().lpb_modal_ke(ke.ctypes.data, km.ctypes.data) == 45
+            khat = np.zeros((24, 24))
+            khat[rows, cols] = km
+            np.testing.assert_allclose(t.T @ khat @ t, ke, rtol=0, atol=1e-14)
+    bad = np.random.default_rng(0).standard_normal((24, 24))
+    km = np.zeros(45)
+    try:
+        lib().lpb_modal_ke(np.ascontiguousarray(bad + bad.T).ctypes.data, km.ctypes.data)
+        raise AssertionError("a matrix outside the pattern must be rejected")
+    except RuntimeError:
+        pass

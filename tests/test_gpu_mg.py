@@ -1,0 +1,164 @@
+"""CUDA path against the reference's golden vectors and the oracle (GPU).
+
+Tolerances: float64 operator results to 1e-12 relative (different summation order only);
+float32 V-cycle quantities to 1e-5; solutions of the float64 PCG to 1e-8 relative at
+rtol 1e-10 (both sides converge to the same float64 answer)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+CASES = {"even_im": ("im", 50), "odd_plain": ("plain", 30), "deep_im": ("im", 20), "rough_strict": ("im", 20)}
+
+
+def _load(name):
+    return np.load(os.path.join(GOLD, f"hier_{name}.npz"), allow_pickle=False)
+
+
+def _ge(name, rtol=1e-10, dtype=np.float32, **kw):
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+
+    g = _load(name)
+    element, cc = CASES[name]
+    mesh = BoxMesh(tuple(int(d) for d in g["dims"]), float(g["pitch"]))
+    ge = GridElasticity(mesh, 0.3, g["fixed_mesh"], rtol=rtol, maxiter=3000, coarse_cells=cc, dtype=dtype,
+                        element=element, **kw)
+    ge.set_moduli(g["e_mesh"])
+    return g, ge
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_hierarchy_matches_reference(name):
+    g, ge = _ge(name)
+    assert len(ge.levels) == int(g["nlevels"])
+    assert ge.strict == bool(g["strict"])
+    for i in range(len(ge.levels)):
+        np.testing.assert_array_equal(ge.level_mask(i), g[f"L{i}_mask"], err_msg=f"mask L{i}")
+        np.testing.assert_allclose(ge.level_dinv(i), g[f"L{i}_dinv"], rtol=2e-6, err_msg=f"dinv L{i}")
+        np.testing.assert_allclose(ge._op(i).lmax, float(g[f"L{i}_lmax"]), rtol=1e-4, err_msg=f"lmax L{i}")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_level_operators_match_reference(name):
+    from loadpath_b200.grid import stream_handle  # noqa: F401
+
+    g, ge = _ge(name)
+    for i in range(len(ge.levels)):
+        lv = ge._op(i)
+        gr = lv.grid
+        u = g[f"L{i}_u"]
+        want = g[f"L{i}_apply"]
+        dt = torch.float32 if u.dtype == np.float32 else torch.float64
+        ud = gr.nodes_to_dev(u, dt)
+        out = gr.node_field(dt)
+        lv.apply(out, ud, mask_in=True)          # general kernel: arbitrary u
+        got = gr.nodes_to_host(out)
+        tol = 2e-5 if dt == torch.float32 else 1e-12
+        np.testing.assert_allclose(got, want, rtol=tol, atol=tol * np.abs(want).max(), err_msg=f"L{i}")
+        # the tiled / zero-on-masked path: same numbers on a masked input
+        m = ge.level_mask(i).astype(u.dtype)
+        um = gr.nodes_to_dev(u * m, dt)
+        lv.apply(out, um, mask_in=False)
+        ref2 = gr.nodes_to_host(out)
+        lv.apply(out, um, mask_in=True, fine_kernel=False)
+        np.testing.assert_allclose(ref2, gr.nodes_to_host(out), rtol=tol, atol=tol * np.abs(ref2).max())
+    # float64 fine operator
+    l0 = ge.levels[0]
+    u64 = g["L0_u64"]
+    out = l0.grid.node_field(torch.float64)
+    l0.apply(out, l0.grid.nodes_to_dev(u64, torch.float64), mask_in=True)
+    want = g["L0_apply64"]
+    np.testing.assert_allclose(l0.grid.nodes_to_host(out), want, rtol=1e-12, atol=1e-13 * np.abs(want).max())
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_vcycle_and_solve_match_reference(name):
+    g, ge = _ge(name)
+    gr = ge.g0
+    r = gr.nodes_to_dev(g["vc_r"], torch.float64)
+    z = gr.node_field(torch.float64)
+    ge.precondition_device(r, z)
+    want = g["vc_z"]
+    np.testing.assert_allclose(gr.nodes_to_host(z), want, rtol=1e-4, atol=1e-4 * np.abs(want).max())
+    u = ge.solve_many([g["f_mesh"]])[0]
+    ref = g["u_mesh"]
+    assert np.linalg.norm(u - ref) <= 1e-8 * np.linalg.norm(ref)
+    assert abs(ge.last_iters - int(g["iters"])) <= max(2, int(0.05 * int(g["iters"])))
+    c = float(g["f_mesh"] @ u)
+    assert abs(c - float(g["compliance"])) <= 1e-9 * abs(float(g["compliance"]))
+    se = ge.strain_energy(ref)
+    np.testing.assert_allclose(se, g["strain_energy"], rtol=1e-10, atol=1e-12 * np.abs(g["strain_energy"]).max())
+    ge.set_moduli(g["e_mesh"] * 1.1)
+    w = ge.solve_many([g["f_mesh"]], [u])[0]
+    w_ref = ge.from_grid(g["u_warm_grid"])
+    assert np.linalg.norm(w - w_ref) <= 1e-8 * np.linalg.norm(w_ref)
+
+
+def test_fine_kernel_matches_general_kernel_medium():
+    """The tiled fine-level kernel against the general node-centric kernel on a grid that
+    spans several blocks in x and y and odd z padding, float32 and float64."""
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+
+    dims = (40, 34, 21)
+    mesh = BoxMesh(dims)
+    rng = np.random.default_rng(3)
+    fixed = np.zeros(mesh.n_dof, bool)
+    fixed[3 * np.flatnonzero(mesh.node_ijk[:, 0] == 0)[:, None] + np.arange(3)] = True
+    e = 1e-9 + rng.random(mesh.n_elem) ** 3
+    e[rng.random(mesh.n_elem) < 0.05] = 0.0
+    ge = GridElasticity(mesh, 0.3, fixed, coarse_cells=10 ** 9)
+    ge.set_moduli(e)
+    for lv in (ge.levels[0], ge._l0s):
+        gr = lv.grid
+        m = ge.level_mask(0)
+        u = (rng.standard_normal(gr.node_shape) * m).astype(np.float64 if lv.dtype == torch.float64 else np.float32)
+        ud = gr.nodes_to_dev(u, lv.dtype)
+        a = gr.node_field(lv.dtype)
+        b = gr.node_field(lv.dtype)
+        lv.apply(a, ud, mask_in=False, fine_kernel=True)
+        lv.apply(b, ud, mask_in=False, fine_kernel=False)
+        tol = 1e-12 if lv.dtype == torch.float64 else 2e-5
+        ga, gb = gr.nodes_to_host(a), gr.nodes_to_host(b)
+        np.testing.assert_allclose(ga, gb, rtol=tol, atol=tol * np.abs(gb).max())
+        # padding stays zero
+        assert float(a[:, :, :, gr.NZ:].abs().max()) == 0.0 if gr.pz > gr.NZ else True
+
+
+def test_solve_matches_oracle_mixed_and_fp64():
+    """A 24x12x12 cantilever with smoothed log-uniform density (the benchmark's synthetic
+    field): the device solve in both precisions against the oracle's float64 solve."""
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from oracle import ref_numpy as R
+
+    dims = (24, 12, 12)
+    x = R.log_uniform_density(dims, 7)
+    e = R.simp_moduli(x)
+    fixed, f = R.cantilever_bc(dims)
+    ke = R.hex8_ke(0.3, "im")
+    h = R.Hierarchy(ke, dims, fixed, rtol=1e-10, maxiter=2000, coarse_cells=100)
+    h.set_moduli(e)
+    u_ref = h.solve(f)
+    c_ref = float(np.vdot(f, u_ref))
+    mesh = BoxMesh(dims)
+    for dt in (np.float32, np.float64):
+        ge = GridElasticity(mesh, 0.3, ge_fixed(mesh, fixed), rtol=1e-10, maxiter=2000, coarse_cells=100, dtype=dt,
+                            element="im")
+        ge.set_moduli(e.reshape(-1))
+        u = ge.solve_many([ge.from_grid(f)])[0]
+        ug = ge.to_grid(u)
+        assert np.linalg.norm(ug - u_ref) <= 1e-8 * np.linalg.norm(u_ref)
+        assert abs(float(np.vdot(f, ug)) - c_ref) <= 1e-9 * c_ref
+        assert abs(ge.last_iters - h.last_iters) <= 2
+
+
+def ge_fixed(mesh, fixed_grid):
+    """bool per mesh dof from a (3, nodes...) grid."""
+    flat = fixed_grid.reshape(3, -1)
+    out = np.empty(mesh.n_dof, bool)
+    for i in range(3):
+        out[i::3] = flat[i]
+    return out
