@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""SIMP iterations per second at 256x128x128 hex8 (12.8M DOF) on B200, mixed precision,
+with the plain FP64 GPU path and the K*u apply's HBM roofline beside it.
+
+One step = one SIMP iteration of the plain top3d loop on the device: SIMP law, Galerkin
+multigrid hierarchy build, MG-PCG solve to rtol 1e-6 (warm-started), element energies,
+compliance and sensitivities, density-filter chain rule, OC bisection, filtered densities.
+Workload (synthetic, seeded): cantilever with the x = 0 face held and a unit -z load spread over
+the bottom edge at x = nx; initial density log-uniform in [1e-3, 1] (seed 1) smoothed by the
+r = 2 cone filter; E0 = 1, Emin = 1e-9, nu = 0.3, p = 3, volume fraction 0.3, filter r = 2,
+move 0.2, incompatible-mode hex8, 5-level hierarchy (coarse_cells 2000).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of the workload
+(the loop does not shard: replicas only), the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+DIMS = (256, 128, 128)
+VOLFRAC, RMIN, RTOL, PENAL, EMIN, MOVE = 0.3, 2.0, 1e-6, 3.0, 1e-9, 0.2
+METRIC = "SIMP iter/s & K*u GB/s at 12.7M DOF: mixed-prec vs FP64 GPU, <=1e-6 rel err"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--dims", default=",".join(str(d) for d in DIMS))
+    p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-e2e", action="store_true")
+    a = p.parse_args()
+    a.warmup = max(a.warmup, 3)
+    a.dims = tuple(int(v) for v in a.dims.split(","))
+    return a
+
+
+def cantilever(dims):
+    nx, ny, nz = dims
+    fixed = np.zeros((3, nx + 1, ny + 1, nz + 1), bool)
+    fixed[:, 0] = True
+    f = np.zeros((3, nx + 1, ny + 1, nz + 1))
+    f[2, nx, :, 0] = -1.0 / (ny + 1)
+    return fixed, f
+
+
+def apply_bytes(dims, itemsize):
+    """Algorithmic bytes of one fine K*u apply: read u, write K u (3 N values each), read E."""
+    nx, ny, nz = dims
+    n = (nx + 1) * (ny + 1) * (nz + 1)
+    return 2 * 3 * n * itemsize + nx * ny * nz * itemsize
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- clocks during the timed region ----------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [v.strip() for v in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- CPU baseline: the oracle's C port of the reference's two-pass CPU operator ---------------
+def cpu_apply_times(dims, reps64=3, reps32=3):
+    """Seconds per fine-level apply (float64, float32) of the C port on all host cores."""
+    from oracle import cport
+    from oracle import ref_numpy as R
+
+    nx, ny, nz = dims
+    rng = np.random.default_rng(101)
+    e = R.simp_moduli(np.exp(rng.uniform(np.log(1e-3), 0.0, dims)))
+    m = np.ones((3, nx + 1, ny + 1, nz + 1))
+    m[:, 0] = 0.0
+    ke = R.hex8_ke(0.3, "im")
+    u = rng.standard_normal(m.shape) * m
+    out = {}
+    for dt, reps in ((np.float64, reps64), (np.float32, reps32)):
+        op = cport.MaskedApply(ke, e, m, dt)
+        uu = u.astype(dt)
+        o = np.empty_like(uu)
+        op(uu, o)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            op(uu, o)
+        out[np.dtype(dt).name] = (time.perf_counter() - t0) / reps
+    return out, cport.threads()
+
+
+def cpu_iteration_estimate(dims, n64, n32):
+    t, cores = cpu_apply_times(dims)
+    sec = n64 * t["float64"] + n32 * t["float32"]
+    return {"value": 1.0 / sec, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
+            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) on {cores} threads: "
+                       f"{t['float64'] * 1e3:.1f} ms per float64 and {t['float32'] * 1e3:.1f} ms per float32 "
+                       f"fine-level apply at {dims[0]}x{dims[1]}x{dims[2]}, times the {n64} float64 + {n32} float32 "
+                       "fine applies one SIMP iteration makes; coarse levels, setup, filter and OC not counted "
+                       "(a lower bound on the CPU iteration time)")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    # fine applies per SIMP iteration of the mixed path at this size: 17 CG iterations (the
+    # reference's count at this workload) + the warm-start apply in float64; four per V-cycle
+    # (18 V-cycles) plus 12 power iterations in float32
+    n64, n32 = 18, 4 * 18 + 12
+    cb = cpu_iteration_estimate(args.dims, n64, n32)
+    vals = []
+    for _ in range(args.warmup + args.steps):
+        t, _ = cpu_apply_times(args.dims, 1, 1)
+        vals.append(1.0 / (n64 * t["float64"] + n32 * t["float32"]))
+    v = statistics.median(vals[args.warmup:])
+    line = {"metric": METRIC, "value": v, "unit": "SIMP iter/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "config": {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, args.dims))} hex8"},
+            "impl": "reference", "cpu_baseline": dict(cb, value=v),
+            "e2e": {"value": v, "unit": "SIMP iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---- the B200 arm ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from loadpath_b200 import _lib, mg
+    from loadpath_b200.grid import DevGrid
+    from loadpath_b200.simp import DeviceFilter, Top3dLoop
+
+    dims = args.dims
+    fixed, f = cantilever(dims)
+    # synthetic density: seeded log-uniform in [1e-3, 1], smoothed by the r = 2 cone filter
+    g = DevGrid(dims)
+    rng = np.random.default_rng(1)
+    xr = g.cells_to_dev(np.exp(rng.uniform(np.log(1e-3), 0.0, dims)), torch.float64)
+    flt = DeviceFilter(g, 2.0)
+    x0 = flt.apply(g.cell_field(torch.float64), xr, hs_out=flt.hs)
+    x0_host = g.cells_to_host(x0)
+    del flt, xr
+
+    def new_loop(dtype):
+        return Top3dLoop(dims, VOLFRAC, RMIN, fixed, f, rtol=RTOL, dtype=dtype, x0=x0_host, penal=PENAL, emin=EMIN,
+                         move=MOVE, element="im")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident timing -----------------------------------------------------------
+    loop = new_loop(np.float32)
+    for _ in range(args.warmup):
+        loop.step()
+    probe = mg.FineApplyProbe()
+    barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    calls0 = _lib.launches()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    mg.set_probe(probe)
+    t0.record()
+    iters = []
+    for _ in range(args.steps):
+        loop.step()
+        iters.append(loop.ge.last_iters)
+    t1.record()
+    torch.cuda.synchronize()
+    mg.set_probe(None)
+    barrier()
+    clocks = clk.stop()
+    launches = _lib.launches() - calls0
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.steps / (ms / 1e3)
+    fine = probe.summary()
+    peak, peak_kind = peaks()
+    b32 = apply_bytes(dims, 4)
+    roofline = None
+    if fine["f32_count"]:
+        avg = fine["f32_ms"] / fine["f32_count"] / 1e3
+        achieved = b32 / avg / 1e9
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "fine_apply_f32_traffic.json")
+        if os.path.exists(prof):
+            with open(prof) as fh:
+                pd = json.load(fh)
+            if tuple(pd.get("dims", ())) == tuple(dims):
+                traffic = pd.get("dram_bytes_per_launch")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "kernel": "k_apply_fine<float>",
+                    "algorithmic_bytes": b32, "avg_launch_us": avg * 1e6, "launches_timed": fine["f32_count"],
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
+    extra = {"cg_iterations": iters, "compliance": loop.history[-1][0],
+             "fine_apply_f64_us": (fine["f64_ms"] / fine["f64_count"] * 1e3) if fine["f64_count"] else None,
+             "fine_applies_per_step": {"f64": fine["f64_count"] / args.steps, "f32": fine["f32_count"] / args.steps}}
+    del loop
+    torch.cuda.empty_cache()
+
+    # ---- accuracy and the plain FP64 GPU path ---------------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        ref = new_loop(np.float64)
+        mix = new_loop(np.float32)
+        # the first design, solved three ways: mixed and plain FP64 at rtol 1e-6, and a tight
+        # FP64 solve (rtol 1e-10) as the GPU oracle
+        def first(lp, rtol):
+            lp.ge.rtol = rtol
+            lp.u = None
+            lp.solve()
+            lp.sensitivities()
+            return float(lp._scal[0].item()), lp.u.clone(), lp.dcf.clone()
+
+        c32, u32, dc32 = first(mix, RTOL)
+        c64, _, _ = first(ref, RTOL)
+        c_or, u_or, dc_or = first(ref, 1e-10)
+        du = float((u32 - u_or).norm() / u_or.norm())
+        dsens = float((dc32 - dc_or).norm() / dc_or.norm())
+        del u32, dc32, u_or, dc_or
+        ref.ge.rtol = RTOL
+        for _ in range(args.warmup - 1):
+            ref.step()
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(args.steps):
+            ref.step()
+        a1.record()
+        torch.cuda.synchronize()
+        v64 = args.steps / (a0.elapsed_time(a1) / 1e3)
+        fp64 = {"value": v64, "unit": "SIMP iter/s", "mixed_over_fp64": value / world / v64,
+                "rel_err_vs_fp64_oracle": {"compliance": abs(c32 - c_or) / abs(c_or),
+                                           "compliance_fp64_path": abs(c64 - c_or) / abs(c_or),
+                                           "displacement": du, "sensitivity": dsens}}
+        del ref, mix
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the host-facing step ----------------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        loop = new_loop(np.float32)
+        x_host = torch.from_numpy(np.ascontiguousarray(x0_host)).pin_memory()
+        out_host = torch.empty_like(x_host).pin_memory()
+        for _ in range(1):
+            loop.step_host(x_host, out_host)
+        barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            c, _ = loop.step_host(x_host, out_host)
+            x_host.copy_(out_host)
+        torch.cuda.synchronize()
+        w = time.perf_counter() - w0
+        if world > 1:
+            tt = torch.tensor([w], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            w = float(tt.item())
+        nb = int(np.prod(dims)) * 8
+        e2e = {"value": world * args.steps / w, "unit": "SIMP iter/s", "h2d_bytes_per_step": nb,
+               "d2h_bytes_per_step": nb + 16,
+               "api": "Top3dLoop.step_host: design in from pinned host memory, filtered design and compliance out"}
+        del loop
+
+    # ---- CPU baseline (rank 0, N = 1 only) -----------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        n64 = int(round(extra["fine_applies_per_step"]["f64"]))
+        n32 = int(round(extra["fine_applies_per_step"]["f32"]))
+        cpu = cpu_iteration_estimate(dims, n64, n32)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "SIMP iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded log-uniform density smoothed by the r=2 filter; cantilever loads)",
+            "config": {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, dims))} hex8 "
+                                   f"({3 * math.prod(d + 1 for d in dims)} DOF), MG-PCG rtol {RTOL}, "
+                                   "V-cycle float32, CG float64",
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (fields of 51-103 MB)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "fp64_gpu_path": fp64, "detail": extra}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    sys.path.insert(0, ROOT)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -23,6 +23,17 @@ _CTYPES = {
     "void": None,
 }
 _STATUS = {-1: "bad arguments", -2: "kernel launch failed", -3: "size beyond the kernel's limit"}
+# kernels each entry point launches (1 when not listed; 0 for host-only entries)
+_KERNELS = {"lpb_modal_ke": 0, "lpb_reduce_blocks": 0, "lpb_max_f64": 2, "lpb_dot_f64": 2, "lpb_dot_f32": 2,
+            "lpb_dot_f64_f32": 2, "lpb_cg_step": 2, "lpb_coarse_solve_f32": 2, "lpb_coarse_solve_f64": 2,
+            "lpb_oc_volumes": 2, "lpb_oc_apply": 2}
+_COUNT = [0]
+
+
+def launches() -> int:
+    """Kernels launched through this binding so far (sensitivity with a compliance output counts
+    as 2)."""
+    return _COUNT[0]
 
 
 class LpError(RuntimeError):
@@ -74,7 +85,10 @@ class _Lib:
         if fn is None:
             raise AttributeError(name)
 
+        nk = _KERNELS.get(name, 1)
+
         def call(*args):
+            _COUNT[0] += nk + (1 if name == "lpb_sensitivity" and args[9] is not None else 0)
             st = fn(*args)
             if st is not None and st < 0:
                 raise LpError(f"{name}: {_STATUS.get(st, 'error')} (status {st})")

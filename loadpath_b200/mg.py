@@ -58,6 +58,29 @@ class BoxMesh:
         return len(self.elem_ijk)
 
 
+class FineApplyProbe:
+    """CUDA events around every fine-level tiled apply while set (bench.py's roofline)."""
+
+    def __init__(self):
+        self.events = []
+
+    def summary(self):
+        torch.cuda.synchronize()
+        out = {"f32_ms": 0.0, "f32_count": 0, "f64_ms": 0.0, "f64_count": 0}
+        for dt, a, b in self.events:
+            k = "f32" if dt == torch.float32 else "f64"
+            out[k + "_ms"] += a.elapsed_time(b)
+            out[k + "_count"] += 1
+        return out
+
+
+_PROBE = [None]
+
+
+def set_probe(p):
+    _PROBE[0] = p
+
+
 class DevLevel:
     """One level on the device (loadpath/mg.py:174-199)."""
 
@@ -94,8 +117,15 @@ class DevLevel:
         sfx = self._sfx()
         if self.kind == "scaled":
             if fine_kernel and not mask_in:
+                probe = _PROBE[0]
+                if probe is not None:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record()
                 getattr(L, f"lpb_apply_fine_{sfx}")(out.data_ptr(), u.data_ptr(), self.e.data_ptr(),
                                                      self.mask.data_ptr(), self.kmodal.ctypes.data, *g.args, st)
+                if probe is not None:
+                    b.record()
+                    probe.events.append((self.dtype, a, b))
             else:
                 getattr(L, f"lpb_apply_scaled_{sfx}")(out.data_ptr(), u.data_ptr(), self.e.data_ptr(),
                                                        self.mask.data_ptr(), self.ke.data_ptr(), *g.args,

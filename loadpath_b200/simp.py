@@ -226,6 +226,19 @@ class Top3dLoop:
         self.history.append((c, change, self.ge.last_iters))
         return c, change
 
+    def step_host(self, x_host, out_host):
+        """One iteration on a design held in host memory (pinned, so the copies are async):
+        the design x (cells, float64) goes in, its physical densities H x / hs and moduli are
+        formed on the device, and the updated design comes back in out_host. Returns
+        (compliance, change)."""
+        g = self.grid
+        self.x[:, :, :g.nz].copy_(x_host, non_blocking=True)
+        self.filter.apply(self.xphys, self.x, hs_out=self.filter.hs, e_out=self.e, penal=self.penal, emin=self.emin)
+        c, change = self.step()
+        out_host.copy_(self.x[:, :, :g.nz], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return c, change
+
     def run(self, maxit=200, on_iter=None):
         change = 1.0
         while change > 0.01 and self.loop < maxit:

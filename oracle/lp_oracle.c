@@ -1,0 +1,93 @@
+/* TEST INFRASTRUCTURE ONLY: C restatement of the reference's compiled CPU operator, used as
+ * the CPU baseline (bench.py --impl reference, and bench.py's cpu_baseline) and as a checker.
+ * Never linked into or called by the product (loadpath_b200).
+ *
+ * lpo_apply_masked_{f64,f32}: out = m * K (m * u) + (1 - m) * u on the node grid
+ * (3, nx+1, ny+1, nz+1), K = sum over cells of e[c] * ke, in the reference's two passes
+ * (loadpath/mgops.py:247-261): a product pass over blocks of cells gathering their 24 corner
+ * values (mask read in the gather) and multiplying by ke (loadpath/mgops.py:66-103), then a
+ * node pass summing each node's up-to-8 cells' rows and finishing with the mask
+ * (loadpath/mgops.py:181-217). OpenMP threads over blocks / (x, y) node columns.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define BLOCK 256
+
+#define DEFINE_APPLY(T, SFX)                                                                        \
+  int lpo_apply_masked_##SFX(T* out, const T* u, const T* e, const T* m, const double* ke64,       \
+                             int nx, int ny, int nz, T* ft) {                                        \
+    const long long NX = nx + 1, NY = ny + 1, NZ = nz + 1;                                           \
+    const long long nn = NX * NY * NZ, ncell = (long long)nx * ny * nz;                              \
+    T ke[576];                                                                                       \
+    for (int i = 0; i < 576; ++i) ke[i] = (T)ke64[i];                                                \
+    long long off[24];                                                                               \
+    for (int k = 0; k < 8; ++k)                                                                      \
+      for (int d = 0; d < 3; ++d)                                                                    \
+        off[3 * k + d] = d * nn + (k & 1) * NY * NZ + ((k >> 1) & 1) * NZ + ((k >> 2) & 1);          \
+    const long long nblk = (ncell + BLOCK - 1) / BLOCK;                                              \
+    _Pragma("omp parallel for schedule(static)")                                                     \
+    for (long long b = 0; b < nblk; ++b) {                                                          \
+      T ubt[24][BLOCK];                                                                              \
+      long long c0 = b * BLOCK;                                                                      \
+      int cnt = (int)((ncell - c0) < BLOCK ? (ncell - c0) : BLOCK);                                  \
+      long long base[BLOCK];                                                                         \
+      for (int c = 0; c < cnt; ++c) {                                                                \
+        long long cell = c0 + c;                                                                     \
+        long long z = cell % nz, y = (cell / nz) % ny, x = cell / ((long long)nz * ny);              \
+        base[c] = (x * NY + y) * NZ + z;                                                             \
+      }                                                                                              \
+      for (int i = 0; i < 24; ++i)                                                                   \
+        for (int c = 0; c < cnt; ++c) {                                                              \
+          long long k = base[c] + off[i];                                                            \
+          ubt[i][c] = u[k] * m[k];                                                                   \
+        }                                                                                            \
+      for (int i = 0; i < 24; ++i) {                                                                 \
+        T* fr = ft + (long long)i * ncell + c0;                                                      \
+        for (int c = 0; c < cnt; ++c) fr[c] = 0;                                                     \
+        for (int j = 0; j < 24; ++j) {                                                               \
+          T kij = ke[i * 24 + j];                                                                    \
+          for (int c = 0; c < cnt; ++c) fr[c] += kij * ubt[j][c];                                    \
+        }                                                                                            \
+        for (int c = 0; c < cnt; ++c) fr[c] *= e[c0 + c];                                            \
+      }                                                                                              \
+    }                                                                                                \
+    _Pragma("omp parallel for schedule(static)")                                                     \
+    for (long long xy = 0; xy < NX * NY; ++xy) {                                                     \
+      long long x = xy / NY, y = xy % NY;                                                            \
+      for (long long z = 0; z < NZ; ++z) {                                                           \
+        T a[3] = {0, 0, 0};                                                                          \
+        for (int k = 0; k < 8; ++k) {                                                                \
+          long long cx = x - (k & 1), cy = y - ((k >> 1) & 1), cz = z - ((k >> 2) & 1);              \
+          if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) continue;              \
+          long long r = (cx * ny + cy) * nz + cz;                                                    \
+          for (int d = 0; d < 3; ++d) a[d] += ft[(long long)(3 * k + d) * ncell + r];                \
+        }                                                                                            \
+        long long n = (x * NY + y) * NZ + z;                                                         \
+        for (int d = 0; d < 3; ++d) {                                                                \
+          T md = m[d * nn + n];                                                                      \
+          out[d * nn + n] = a[d] * md + (1 - md) * u[d * nn + n];                                    \
+        }                                                                                            \
+      }                                                                                              \
+    }                                                                                                \
+    return 0;                                                                                        \
+  }
+
+DEFINE_APPLY(double, f64)
+DEFINE_APPLY(float, f32)
+
+int lpo_threads(void) {
+  int n = 1;
+#ifdef _OPENMP
+#pragma omp parallel
+  {
+#pragma omp single
+    n = omp_get_num_threads();
+  }
+#endif
+  return n;
+}

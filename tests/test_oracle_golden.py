@@ -175,3 +175,19 @@ def test_mma_steps():
     for i in range(int(g["steps"])):
         xn = mma.update(g[f"x{i}"], 1.0, g[f"df0{i}"], g[f"f{i}"], g[f"df{i}"])
         np.testing.assert_allclose(xn, g[f"xn{i}"], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_c_port_apply_matches_golden(name):
+    """The oracle's C port of the reference's two-pass CPU apply (the CPU baseline) gives the
+    reference's level-0 operator."""
+    from oracle import cport
+
+    g, h = _hierarchy(name)
+    l0 = h.levels[0]
+    op = cport.MaskedApply(l0.ke, l0.e, l0.mask, np.float64)
+    want = g["L0_apply64"]
+    np.testing.assert_allclose(op(g["L0_u64"]), want, rtol=1e-12, atol=1e-13 * np.abs(want).max())
+    op32 = cport.MaskedApply(l0.ke, l0.e, l0.mask, np.float32)
+    want = g["L0_apply"]
+    np.testing.assert_allclose(op32(g["L0_u"]), want, rtol=2e-5, atol=2e-5 * np.abs(want).max())
