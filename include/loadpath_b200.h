@@ -35,13 +35,14 @@ int lpb_apply_weights_f64(double* out, const double* u, const double* w, const d
 int lpb_apply_explicit_f32(float* out, const float* u, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
 int lpb_apply_explicit_f64(double* out, const double* u, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, int mask_in, int finish, void* stream);
 
-/* ---- fine-level apply, tiled (the solver's hot path): same result as lpb_apply_scaled_* with
+/* ---- fine-level apply, TMA-tiled (the solver's hot path): same result as lpb_apply_scaled_* with
  * mask_in = 0 and finish = 1 on inputs that are zero on masked dofs; kmodal is a HOST pointer to
- * the 45 corner-parity coefficients from lpb_modal_ke (they are passed as kernel parameters).
- * Needs pz % 4 == 0 and cpz == pz. Replaces mgops._product_scaled + _scatter_into with finish
- * (loadpath/mgops.py:86-103, :181-217). */
-int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const float* kmodal, int nx, int ny, int nz, int pz, int cpz, void* stream);
-int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int nx, int ny, int nz, int pz, int cpz, void* stream);
+ * the 45 corner-parity coefficients (float64) from lpb_modal_ke (passed as kernel parameters);
+ * err: device int the kernel sets to 1 if a shared-memory load wait gives up (never expected).
+ * Needs pz % 4 == 0, cpz == pz and 16-byte aligned fields. Replaces mgops._product_scaled +
+ * _scatter_into with finish (loadpath/mgops.py:86-103, :181-217). */
+int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* the element matrix (24 x 24, float64, host pointer) in the corner-parity basis that
  * lpb_apply_fine_* reads (45 coefficients, host pointer out); returns the count or < 0 */
 int lpb_modal_ke(const double* ke, double* kmodal_out);

@@ -24,6 +24,7 @@
 // hold zeros in the z padding; u is zero on dofs whose mask bit is 0, so the identity rows
 // (1 - m) u of the masked operator vanish and the kernel writes m * K u.
 #include "lp_common.cuh"
+#include "lp_tma.cuh"
 
 namespace {
 
@@ -46,6 +47,13 @@ struct Vec4<float> {
   static __device__ __forceinline__ void store(float* p, const float (&v)[4]) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
   }
+  static __device__ __forceinline__ void lds(const float* p, float (&v)[4]) {
+    float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+  static __device__ __forceinline__ void sts(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
 };
 template <>
 struct Vec4<double> {
@@ -55,6 +63,15 @@ struct Vec4<double> {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
   }
   static __device__ __forceinline__ void store(double* p, const double (&v)[4]) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+  }
+  static __device__ __forceinline__ void lds(const double* p, double (&v)[4]) {
+    double2 a = *reinterpret_cast<const double2*>(p);
+    double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  static __device__ __forceinline__ void sts(double* p, const double (&v)[4]) {
     *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
     *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
   }
@@ -88,140 +105,283 @@ __device__ __forceinline__ void modal_product(const KModal<T>& km, const T (&v)[
   f[23] = km.c[44] * v[23];
 }
 
+constexpr int NSTAGE = 3;           // TMA ring depth (chunks of four z-planes)
+constexpr int BOX = TXC + 1;         // 17 node columns per side in a loaded box
+
+// every TMA destination / source starts on a 128-byte boundary
+template <typename T, int N>
+struct alignas(128) Slot {
+  T v[(N * sizeof(T) + 127) / 128 * 128 / sizeof(T)];
+};
+
 template <typename T>
-__global__ void __launch_bounds__(TXC * TYC, 1)
-k_apply_fine(T* __restrict__ out, const T* __restrict__ u, const T* __restrict__ e,
-             const uint8_t* __restrict__ mask, const KModal<T> km, LpGrid g) {
-  // corner forces for the neighbours: [corner 10/01/11][component][plane][thread]
+struct FineSmem {
+  Slot<T, 3 * BOX * BOX * 4> u[NSTAGE];              // node values: [comp][x][y][z]
+  Slot<T, BOX * BOX * 4> e[NSTAGE];                  // cell moduli: [x][y][z] (16 used per side)
+  Slot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store
+  T red[3][4][TXC * TYC];                            // y-neighbour exchange
+  alignas(8) uint64_t full[NSTAGE];
+};
+
+template <typename T>
+__device__ __forceinline__ T* u_at(FineSmem<T>& sm, int s, int c, int x, int y) {
+  return &sm.u[s].v[((c * BOX + x) * BOX + y) * 4];
+}
+
+template <typename T>
+struct TileMaps {
+  CUtensorMap u;    // (pz, NY, NX, 3), box (4, 17, 17, 3)
+  CUtensorMap e;    // (cpz, ny, nx),    box (4, 17, 17)
+  CUtensorMap out;  // (pz, NY, NX, 3), box (4, 15, 15, 3)
+};
+
+template <typename T>
+__device__ __forceinline__ void xy_modes(const T (&v)[4], T (&a)[4]) {
+  // v: node columns 00, 10, 01, 11 -> modes 1, sx, sy, sxsy
+  T sx0 = v[0] + v[1], dx0 = v[1] - v[0], sx1 = v[2] + v[3], dx1 = v[3] - v[2];
+  a[0] = sx0 + sx1;
+  a[1] = dx0 + dx1;
+  a[2] = sx1 - sx0;
+  a[3] = dx1 - dx0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TXC * TYC, (sizeof(T) == 4 ? 2 : 1))
+k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict__ mask, const KModal<T> km,
+             LpGrid g, int zch, int nchunks, int* __restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
-  T(*red)[3][4][TXC * TYC] = reinterpret_cast<T(*)[3][4][TXC * TYC]>(smem_raw);
+  // 128-byte alignment in the shared window (what TMA addresses), not in the generic space
+  const uint32_t raw_off = lp_smem_addr(smem_raw);
+  FineSmem<T>& sm = *reinterpret_cast<FineSmem<T>*>(smem_raw + ((128u - (raw_off & 127u)) & 127u));
   const int tid = threadIdx.x;
   const int i = tid % TXC, j = tid / TXC;
   const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
-  const int cx = x0 - 1 + i, cy = y0 - 1 + j;  // this thread's cell column = its owned node column
-  const int NX = g.NX(), NY = g.NY();
-  const long long cs = g.comp_stride();
-  const bool cell_ok = cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny;
-  const bool own = i >= 1 && j >= 1 && cx < NX && cy < NY;
-  bool col_ok[4];
-  long long col_base[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    int nx_ = cx + (q & 1), ny_ = cy + (q >> 1);
-    col_ok[q] = nx_ >= 0 && nx_ < NX && ny_ >= 0 && ny_ < NY;
-    col_base[q] = col_ok[q] ? g.node(nx_, ny_, 0) : 0;
-  }
-  const long long ebase = cell_ok ? g.cell(cx, cy, 0) : 0;
-  const long long obase = own ? g.node(cx, cy, 0) : 0;
+  const int c_begin = blockIdx.z * zch;
+  const int c_end = min(c_begin + zch, nchunks);
+  if (c_begin >= c_end) return;
+  const int cstart = c_begin > 0 ? c_begin - 1 : 0;     // one halo chunk below the segment
+  const int nload = min(c_end + 1, nchunks) - cstart;   // + the plane above the last chunk
+  const int nproc = c_end - cstart;
+  const bool own = i >= 1 && j >= 1;
+  constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(T);
+  constexpr uint32_t EBYTES = BOX * BOX * 4 * sizeof(T);
 
-  T up_carry[4][3];    // upper-face modal force of the cell below this chunk
+  // alignment contract of every TMA operand and vector access, checked once per block: a
+  // violation is recorded in *err (codes 10..16) and the block returns without touching memory
+  __shared__ int bad;
+  if (tid == 0) {
+    int code = 0;
+    uint32_t so = 0;
+    for (int s = 0; s < NSTAGE; ++s) so |= lp_smem_addr(sm.u[s].v) | lp_smem_addr(sm.e[s].v);
+    so |= lp_smem_addr(sm.o[0].v) | lp_smem_addr(sm.o[1].v);
+    if (so & 127) code = 10;
+    else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 11;
+    else if (reinterpret_cast<uintptr_t>(&maps.e) & 63) code = 12;
+    else if (reinterpret_cast<uintptr_t>(&maps.out) & 63) code = 13;
+    else if (lp_smem_addr(&sm.full[0]) & 7) code = 15;
+    else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 16;
+    bad = code;
+    if (code) atomicExch(err, code);
+  }
+  __syncthreads();
+  if (bad) return;
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; ++s) lp_mbar_init(&sm.full[s], 1);
+    lp_fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    const int s = k % NSTAGE;
+    const int z = 4 * (cstart + k);
+    lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, z, y0 - 1, x0 - 1, 0, &sm.full[s]);
+    lp_tma_load_3d(sm.e[s].v, &maps.e, z, y0 - 1, x0 - 1, &sm.full[s]);
+  };
+  if (tid == 0) {
+    issue(0);
+    if (nload > 1) issue(1);
+  }
+
+  T up_carry[4][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
     for (int c = 0; c < 3; ++c) up_carry[q][c] = T(0);
 
-  for (int z = 0; z < g.pz; z += 4) {
-    // ---- planes z..z+3 of the four node columns (16-byte loads) and plane z+4 (scalar)
+  for (int k = 0; k < nproc; ++k) {
+    const int c = cstart + k;
+    const bool halo = c < c_begin;
+    const int s = k % NSTAGE;
+    if (tid == 0) {
+      if (k + 2 < nload) issue(k + 2);
+      lp_bulk_wait_read<1>();   // the store from two chunks ago has read its staging buffer
+    }
+    bool ok = lp_mbar_wait(&sm.full[s], (k / NSTAGE) & 1);
+    const bool has_next = k + 1 < nload;
+    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NSTAGE], ((k + 1) / NSTAGE) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        // let the loads already issued land before the block exits (bounded as well)
+        for (int kk = k; kk < min(k + 3, nload); ++kk) lp_mbar_wait(&sm.full[kk % NSTAGE], (kk / NSTAGE) & 1);
+      }
+      break;
+    }
+    // ---- this thread's four node columns: planes z..z+3 and plane z+4
     T un[4][3][5];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
+      for (int cc = 0; cc < 3; ++cc) {
+        const T* col = u_at(sm, s, cc, i + (q & 1), j + (q >> 1));
         T v4[4];
-        if (col_ok[q]) {
-          Vec4<T>::load(u + c * cs + col_base[q] + z, v4);
-        } else {
-          v4[0] = v4[1] = v4[2] = v4[3] = T(0);
-        }
-        un[q][c][0] = v4[0]; un[q][c][1] = v4[1]; un[q][c][2] = v4[2]; un[q][c][3] = v4[3];
-        un[q][c][4] = (col_ok[q] && z + 4 < g.pz) ? __ldg(u + c * cs + col_base[q] + z + 4) : T(0);
+        Vec4<T>::lds(col, v4);
+        un[q][cc][0] = v4[0]; un[q][cc][1] = v4[1]; un[q][cc][2] = v4[2]; un[q][cc][3] = v4[3];
+        un[q][cc][4] = has_next ? *u_at(sm, (k + 1) % NSTAGE, cc, i + (q & 1), j + (q >> 1)) : T(0);
       }
     T ev[4];
-    if (cell_ok) {
-      Vec4<T>::load(e + ebase + z, ev);
-    } else {
-      ev[0] = ev[1] = ev[2] = ev[3] = T(0);
-    }
-    // x-y modes of plane z
+    Vec4<T>::lds(&sm.e[s].v[(i * BOX + j) * 4], ev);
+
     T a_lo[4][3];
+    {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      T u00 = un[0][c][0], u10 = un[1][c][0], u01 = un[2][c][0], u11 = un[3][c][0];
-      T sx0 = u00 + u10, dx0 = u10 - u00, sx1 = u01 + u11, dx1 = u11 - u01;
-      a_lo[0][c] = sx0 + sx1;
-      a_lo[1][c] = dx0 + dx1;
-      a_lo[2][c] = sx1 - sx0;
-      a_lo[3][c] = dx1 - dx0;
+      for (int cc = 0; cc < 3; ++cc) {
+        T v[4], a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = halo ? un[q][cc][3] : un[q][cc][0];
+        xy_modes(v, a);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a_lo[q][cc] = a[q];
+      }
     }
-    // ---- cells z .. z+3: lower plane z+t, upper plane z+t+1
-    T own_f[4][3];  // corner-00 force of this thread's cell column on node planes z..z+3
+    T s0v[4][3];   // this node column's force from its own and its -x neighbour's cells
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
+      if (halo && t < 3) continue;
       T a_hi[4][3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        T u00 = un[0][c][t + 1], u10 = un[1][c][t + 1], u01 = un[2][c][t + 1], u11 = un[3][c][t + 1];
-        T sx0 = u00 + u10, dx0 = u10 - u00, sx1 = u01 + u11, dx1 = u11 - u01;
-        a_hi[0][c] = sx0 + sx1;
-        a_hi[1][c] = dx0 + dx1;
-        a_hi[2][c] = sx1 - sx0;
-        a_hi[3][c] = dx1 - dx0;
+      for (int cc = 0; cc < 3; ++cc) {
+        T v[4] = {un[0][cc][t + 1], un[1][cc][t + 1], un[2][cc][t + 1], un[3][cc][t + 1]}, a[4];
+        xy_modes(v, a);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a_hi[q][cc] = a[q];
       }
       const T ec = ev[t];
       T v[24], f[24];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          T lo = a_lo[q][c], hi = a_hi[q][c];
-          v[3 * q + c] = (lo + hi) * ec;
-          v[3 * (q + 4) + c] = (hi - lo) * ec;
+        for (int cc = 0; cc < 3; ++cc) {
+          T lo = a_lo[q][cc], hi = a_hi[q][cc];
+          v[3 * q + cc] = (lo + hi) * ec;
+          v[3 * (q + 4) + cc] = (hi - lo) * ec;
         }
       modal_product<T>(km, v, f);
-      // node plane z+t: upper face of the cell below + lower face of this cell
       T fp[4][3];
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          T f0 = f[3 * q + c], f1 = f[3 * (q + 4) + c];
-          fp[q][c] = up_carry[q][c] + (f0 - f1);
-          up_carry[q][c] = f0 + f1;
-          a_lo[q][c] = a_hi[q][c];
+        for (int cc = 0; cc < 3; ++cc) {
+          T f0 = f[3 * q + cc], f1 = f[3 * (q + 4) + cc];
+          fp[q][cc] = up_carry[q][cc] + (f0 - f1);
+          up_carry[q][cc] = f0 + f1;
+          a_lo[q][cc] = a_hi[q][cc];
         }
-      // back to the four corner columns
+      if (!halo) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        T t0 = fp[0][c] - fp[2][c], t1 = fp[1][c] - fp[3][c];
-        T t2 = fp[0][c] + fp[2][c], t3 = fp[1][c] + fp[3][c];
-        own_f[t][c] = t0 - t1;                 // corner 00
-        red[0][c][t][tid] = t0 + t1;           // corner 10 -> node (cx + 1, cy)
-        red[1][c][t][tid] = t2 - t3;           // corner 01 -> node (cx, cy + 1)
-        red[2][c][t][tid] = t2 + t3;           // corner 11 -> node (cx + 1, cy + 1)
+        for (int cc = 0; cc < 3; ++cc) {
+          T t0 = fp[0][cc] - fp[2][cc], t1 = fp[1][cc] - fp[3][cc];
+          T t2 = fp[0][cc] + fp[2][cc], t3 = fp[1][cc] + fp[3][cc];
+          // corners 00, 10 (-> x+1), 01 (-> y+1), 11 (-> x+1, y+1); x through shuffles
+          T c10 = __shfl_up_sync(0xffffffffu, t0 + t1, 1, TXC);
+          T c11 = __shfl_up_sync(0xffffffffu, t2 + t3, 1, TXC);
+          s0v[t][cc] = (t0 - t1) + c10;
+          sm.red[cc][t][tid] = (t2 - t3) + c11;
+        }
       }
     }
+    if (halo) {           // uniform across the block: the halo chunk only sets up_carry
+      __syncthreads();    // its stage is refilled next iteration: every thread is done reading
+      continue;
+    }
     __syncthreads();
-    // ---- own node columns: add the three neighbours' corner forces, store planes z..z+3
     if (own) {
-      const int t10 = tid - 1, t01 = tid - TXC, t11 = tid - TXC - 1;
-      const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + obase + z);
-      const uint8_t mbs[4] = {mb.x, mb.y, mb.z, mb.w};
+      const long long obase = g.node(x0 - 1 + i, y0 - 1 + j, 0);
+      const bool inside = x0 - 1 + i < g.NX() && y0 - 1 + j < g.NY();
+      uint8_t mbs[4] = {0, 0, 0, 0};
+      if (inside) {
+        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + obase + 4 * c);
+        mbs[0] = mb.x; mbs[1] = mb.y; mbs[2] = mb.z; mbs[3] = mb.w;
+      }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
+      for (int cc = 0; cc < 3; ++cc) {
         T o[4];
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-          T s = own_f[t][c] + red[0][c][t][t10] + red[1][c][t][t01] + red[2][c][t][t11];
-          o[t] = ((mbs[t] >> c) & 1) ? s : T(0);
+          T v = s0v[t][cc] + sm.red[cc][t][tid - TXC];
+          o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
         }
-        Vec4<T>::store(out + c * cs + obase + z, o);
+        Vec4<T>::sts(&sm.o[k & 1].v[((cc * (TXC - 1) + (i - 1)) * (TYC - 1) + (j - 1)) * 4], o);
       }
     }
+    lp_fence_proxy_async();
     __syncthreads();
+    if (tid == 0) {
+      lp_tma_store_4d(&maps.out, 4 * c, y0, x0, 0, sm.o[k & 1].v);
+      lp_bulk_commit();
+    }
   }
+  if (tid == 0) lp_bulk_wait_all();
 }
 
 }  // namespace
+
+static bool fine_args_ok(const LpGrid& g) { return lp_grid_ok(g) && g.pz % 4 == 0 && g.cpz == g.pz; }
+
+template <typename T>
+static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, const double* kmodal_host, int* err,
+                       LpGrid g, cudaStream_t st) {
+  if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal_host || !err || out == u) return LP_ERR_ARG;
+  KModal<T> km;
+  for (int i = 0; i < 45; ++i) km.c[i] = (T)kmodal_host[i];
+  TileMaps<T> maps;
+  const uint64_t nd[4] = {(uint64_t)g.pz, (uint64_t)g.NY(), (uint64_t)g.NX(), 3};
+  const uint64_t cd[3] = {(uint64_t)g.cpz, (uint64_t)g.ny, (uint64_t)g.nx};
+  const uint32_t bin[4] = {4, BOX, BOX, 3};
+  const uint32_t be[3] = {4, BOX, BOX};
+  const uint32_t bout[4] = {4, TXC - 1, TYC - 1, 3};
+  if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.e, e, 3, cd, be, sizeof(T)) ||
+      !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
+    return LP_ERR_ARG;
+  const int smem = (int)sizeof(FineSmem<T>) + 128;
+  static long long slots = 0;   // resident blocks on the device (queried once per process)
+  if (!slots) {
+    if (cudaFuncSetAttribute(k_apply_fine<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return LP_ERR_LAUNCH;
+    int per_sm = 1, dev = 0, nsm = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_fine<T>, TXC * TYC, smem);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    slots = (long long)(per_sm > 0 ? per_sm : 1) * nsm;
+  }
+  const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
+  const int nchunks = g.pz / 4;
+  // z segments: balance the grid over the resident blocks; a segment recomputes one halo cell
+  int best_zch = nchunks;
+  double best = 1e30;
+  for (int zch = 2; zch <= nchunks; ++zch) {
+    const long long nseg = (nchunks + zch - 1) / zch;
+    const long long units = (long long)gx * gy * nseg;
+    const long long waves = (units + slots - 1) / slots;
+    const double cost = (double)waves * (zch + (nseg > 1 ? 0.3 : 0.0));
+    if (cost < best - 1e-9) { best = cost; best_zch = zch; }
+  }
+  const int nseg = (nchunks + best_zch - 1) / best_zch;
+  dim3 grid(gx, gy, nseg);
+  k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
 
 extern "C" {
 
@@ -263,39 +423,15 @@ int lpb_modal_ke(const double* ke, double* kmodal_out) {
   return 45;
 }
 
-static bool fine_args_ok(const LpGrid& g) { return lp_grid_ok(g) && g.pz % 4 == 0 && g.cpz == g.pz; }
 
-// kmodal: host memory (copied into the launch parameters)
-
-int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const float* kmodal, int nx,
-                       int ny, int nz, int pz, int cpz, void* stream) {
-  LpGrid g = lp_grid(nx, ny, nz, pz, cpz);
-  if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal || out == u) return LP_ERR_ARG;
-  KModal<float> km;
-  for (int i = 0; i < 45; ++i) km.c[i] = kmodal[i];
-  dim3 grid((g.NX() + TXC - 2) / (TXC - 1), (g.NY() + TYC - 2) / (TYC - 1));
-  const int smem = 3 * 3 * 4 * TXC * TYC * sizeof(float);
-  k_apply_fine<float><<<grid, TXC * TYC, smem, (cudaStream_t)stream>>>(out, u, e, mask, km, g);
-  LP_LAUNCH_CHECK();
-  return LP_OK;
+int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const double* kmodal,
+                       int* err, int nx, int ny, int nz, int pz, int cpz, void* stream) {
+  return launch_fine<float>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream);
 }
 
 int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal,
-                       int nx, int ny, int nz, int pz, int cpz, void* stream) {
-  LpGrid g = lp_grid(nx, ny, nz, pz, cpz);
-  if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal || out == u) return LP_ERR_ARG;
-  KModal<double> km;
-  for (int i = 0; i < 45; ++i) km.c[i] = kmodal[i];
-  dim3 grid((g.NX() + TXC - 2) / (TXC - 1), (g.NY() + TYC - 2) / (TYC - 1));
-  const int smem = 3 * 3 * 4 * TXC * TYC * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_apply_fine<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
-  k_apply_fine<double><<<grid, TXC * TYC, smem, (cudaStream_t)stream>>>(out, u, e, mask, km, g);
-  LP_LAUNCH_CHECK();
-  return LP_OK;
+                       int* err, int nx, int ny, int nz, int pz, int cpz, void* stream) {
+  return launch_fine<double>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream);
 }
 
 }  // extern "C"

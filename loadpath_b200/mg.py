@@ -89,6 +89,7 @@ class DevLevel:
         self.grid = grid
         self.dtype = dtype
         self.e = self.ke = self.kmodal = None
+        self.err = None          # device int the tiled fine kernel flags a given-up wait in
         self.w = self.mcat = self.patch_id = self.patch_k = None
         self.npatch = 0
         self.k = None
@@ -122,7 +123,8 @@ class DevLevel:
                     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                     a.record()
                 getattr(L, f"lpb_apply_fine_{sfx}")(out.data_ptr(), u.data_ptr(), self.e.data_ptr(),
-                                                     self.mask.data_ptr(), self.kmodal.ctypes.data, *g.args, st)
+                                                     self.mask.data_ptr(), self.kmodal.ctypes.data,
+                                                     self.err.data_ptr(), *g.args, st)
                 if probe is not None:
                     b.record()
                     probe.events.append((self.dtype, a, b))
@@ -201,9 +203,9 @@ class GridElasticity:
         n = lib().lpb_modal_ke(self.ke.ctypes.data, km.ctypes.data)
         if n != 45:
             raise LpError("the element matrix is not in the corner-parity pattern the fine kernel uses")
-        # host arrays: the fine kernel takes the coefficients as launch parameters
-        self.kmodal64 = np.ascontiguousarray(km, np.float64)
-        self.kmodal32 = np.ascontiguousarray(km, np.float32)
+        # host array: the fine kernel takes the coefficients as launch parameters
+        self.kmodal = np.ascontiguousarray(km, np.float64)
+        self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.ke64 = torch.tensor(self.ke.reshape(-1), dtype=torch.float64, device=self.device)
         self.ke32 = self.ke64.float()
         pk = fem.child_prolongations()
@@ -264,7 +266,8 @@ class GridElasticity:
         l0 = DevLevel("scaled", g0, torch.float64)
         l0.e = e_dev
         l0.ke = self.ke64
-        l0.kmodal = self.kmodal64
+        l0.kmodal = self.kmodal
+        l0.err = self._err
         d0 = self._buf("diag0", g0, torch.float64)
         L.lpb_diag_scaled_f64(d0.data_ptr(), e_dev.data_ptr(), self.ke64.data_ptr(), *g0.args, st)
         l0.mask = g0.mask_field()
@@ -278,7 +281,8 @@ class GridElasticity:
             s.e = g0.cell_field(torch.float32)
             L.lpb_cast_f64_f32(s.e.data_ptr(), e_dev.data_ptr(), g0.n_cell_field, st)
             s.ke = self.ke32
-            s.kmodal = self.kmodal32
+            s.kmodal = self.kmodal
+            s.err = self._err
             s.mask = l0.mask
             s.dinv = dinv32
             self._l0s = s
@@ -654,6 +658,7 @@ class GridElasticity:
             L.lpb_mask_field_f64(x0m.data_ptr(), x0.data_ptr(), m.data_ptr(), *g.args, 0, st)
         x, it, ok = self._solve_device(bm, x0m)
         self.last_iters = it
+        self.check_device()
         if not ok:
             raise RuntimeError(f"linear solve did not converge ({it} iterations); "
                                "the structure may be a mechanism (check supports)")
@@ -708,6 +713,11 @@ class GridElasticity:
         ud = g.nodes_to_dev(self.to_grid(u), torch.float64)
         se = g.cells_to_host(self.strain_energy_device(ud))
         return se[tuple(self.elem_ijk.T)]
+
+    def check_device(self):
+        """Raise if a tiled fine-apply launch flagged a shared-memory wait that gave up."""
+        if int(self._err.item()) != 0:
+            raise RuntimeError("fine-level apply: a TMA load wait gave up (device error flag set)")
 
     # diagnostics used by the parity tests
     def level_mask(self, i):
