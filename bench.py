@@ -318,8 +318,10 @@ def run_b200(args):
         loop = new_loop(np.float32)
         x_host = torch.from_numpy(np.ascontiguousarray(x0_host)).pin_memory()
         out_host = torch.empty_like(x_host).pin_memory()
-        for _ in range(1):
+        # the same warm-up as the device-timed loop, so both time the same SIMP iterations
+        for _ in range(args.warmup):
             loop.step_host(x_host, out_host)
+            x_host.copy_(out_host)
         barrier()
         torch.cuda.synchronize()
         w0 = time.perf_counter()

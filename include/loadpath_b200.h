@@ -47,6 +47,23 @@ int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint
  * lpb_apply_fine_* reads (45 coefficients, host pointer out); returns the count or < 0 */
 int lpb_modal_ke(const double* ke, double* kmodal_out);
 
+/* ---- coarse levels on the hot path (u zero on masked dofs; out = m K u):
+ * level 1: z-marching kernel in the corner-parity basis; g1 is a HOST pointer to the 279
+ * coefficients from lpb_modal_g1; pbox (HOST, 6 ints: x0, y0, z0, nx, ny, nz) bounds the nodes
+ * touched by patch cells (patch_id/patch_k may be NULL when there are none). Needs pz % 4 == 0,
+ * cpz == pz. Replaces mgops._product_weights + _scatter_into (loadpath/mgops.py:106-128, 181-217).
+ * explicit levels: kp holds the 300 upper-triangle entries of each cell's symmetric matrix,
+ * entry-major ((300, cells)); ft is caller scratch of 24 * cells values. Replaces
+ * mgops._product_explicit + _scatter_into (loadpath/mgops.py:131-146, 181-217). */
+int lpb_modal_g1(const double* ke, double* g1_out);
+int lpb_apply_weights_march_f32(float* out, const float* u, const float* w, const int* patch_id, const float* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, const int* patch_id, const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* (cells, 24, 24) matrices -> packed symmetric entry-major (the mean of K and K^T) */
+int lpb_pack_sym_f32(float* kp, const float* k, long long ncells, void* stream);
+int lpb_pack_sym_f64(double* kp, const double* k, long long ncells, void* stream);
+
 /* ---- diagonal of K in float64 (loadpath/mg.py:348-371) */
 int lpb_diag_scaled_f64(double* d, const double* e, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_diag_weights_f32(double* d, const float* w, const float* mcat, const int* patch_id, const float* patch_k, int nx, int ny, int nz, int pz, int cpz, void* stream);

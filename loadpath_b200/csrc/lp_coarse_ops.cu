@@ -1,0 +1,639 @@
+// Coarse-level operators on the solver's hot path (loadpath/mg.py:174-346 for the level kinds,
+// loadpath/mgops.py:106-146 for the products they replace).
+//
+// Level 1 ("weights"): K_c = sum_k w[k, c] M_k with M_k = P_k^T Ke P_k, the reference's first
+// Galerkin level. With the child moduli's Walsh transform c = H w, sum_k w_k M_k =
+// sum_t c_t G_t, G_t = sum_k H[t, k] M_k / 8, and in the corner-parity basis of the coarse cell
+// the eight G_t together have 279 non-zeros, each (row, col) entry belonging to exactly one t.
+// The kernel marches z like the fine kernel (four cells per step, x neighbours by shuffles, y
+// neighbours through shared memory) and forms each cell's product in that basis: ~450 flops
+// against the 4608 of the dense sum. Cells touching held dofs ("patch" cells: weights zero,
+// an explicit masked matrix instead) are added by a second, node-centric pass over the box of
+// nodes they touch.
+//
+// Levels >= 2 ("explicit"): K_c stored per cell, symmetric, as the 300 upper-triangle entries
+// in entry-major order (entry p of consecutive cells contiguous, so a warp's loads coalesce).
+// Two passes: a cell pass forms the 24 corner forces f_c = K_c u_c into a caller-provided
+// (24, cells) buffer, a node pass sums each node's eight cells' rows and applies the mask.
+#include "lp_common.cuh"
+
+namespace {
+
+constexpr int TXC = 16, TYC = 16;
+
+template <typename T>
+struct G1 {
+  T c[279];
+};
+
+template <typename T>
+struct V4;
+template <>
+struct V4<float> {
+  static __device__ __forceinline__ void ld(const float* p, float (&v)[4]) {
+    float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+  static __device__ __forceinline__ void st(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct V4<double> {
+  static __device__ __forceinline__ void ld(const double* p, double (&v)[4]) {
+    double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  static __device__ __forceinline__ void st(double* p, const double (&v)[4]) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+  }
+};
+
+// f = sum_t c_t G^_t v on the corner-parity modes (index 3 * mode + component)
+template <typename T>
+__device__ __forceinline__ void g1_product(const G1<T>& g, const T (&c)[8], const T (&v)[24], T (&f)[24]) {
+  f[0] = f[1] = f[2] = T(0);
+  f[3] = c[0] * (g.c[0] * v[3] + g.c[1] * v[7] + g.c[2] * v[14])
+         + c[1] * (g.c[3] * v[10] + g.c[4] * v[17])
+         + c[2] * (g.c[5] * v[9] + g.c[6] * v[20])
+         + c[3] * (g.c[7] * v[23])
+         + c[4] * (g.c[8] * v[15] + g.c[9] * v[19])
+         + c[5] * (g.c[10] * v[22])
+         + c[6] * (g.c[11] * v[21]);
+  f[4] = c[0] * (g.c[12] * v[4] + g.c[13] * v[6])
+         + c[1] * (g.c[14] * v[9])
+         + c[2] * (g.c[15] * v[10])
+         + c[4] * (g.c[16] * v[16] + g.c[17] * v[18])
+         + c[5] * (g.c[18] * v[21])
+         + c[6] * (g.c[19] * v[22]);
+  f[5] = c[0] * (g.c[20] * v[5] + g.c[21] * v[12])
+         + c[1] * (g.c[22] * v[15])
+         + c[2] * (g.c[23] * v[11] + g.c[24] * v[18])
+         + c[3] * (g.c[25] * v[21])
+         + c[4] * (g.c[26] * v[17])
+         + c[6] * (g.c[27] * v[23]);
+  f[6] = c[0] * (g.c[28] * v[4] + g.c[29] * v[6])
+         + c[1] * (g.c[30] * v[9])
+         + c[2] * (g.c[31] * v[10])
+         + c[4] * (g.c[32] * v[16] + g.c[33] * v[18])
+         + c[5] * (g.c[34] * v[21])
+         + c[6] * (g.c[35] * v[22]);
+  f[7] = c[0] * (g.c[36] * v[3] + g.c[37] * v[7] + g.c[38] * v[14])
+         + c[1] * (g.c[39] * v[10] + g.c[40] * v[17])
+         + c[2] * (g.c[41] * v[9] + g.c[42] * v[20])
+         + c[3] * (g.c[43] * v[23])
+         + c[4] * (g.c[44] * v[15] + g.c[45] * v[19])
+         + c[5] * (g.c[46] * v[22])
+         + c[6] * (g.c[47] * v[21]);
+  f[8] = c[0] * (g.c[48] * v[8] + g.c[49] * v[13])
+         + c[1] * (g.c[50] * v[11] + g.c[51] * v[16])
+         + c[2] * (g.c[52] * v[19])
+         + c[3] * (g.c[53] * v[22])
+         + c[4] * (g.c[54] * v[20])
+         + c[5] * (g.c[55] * v[23]);
+  f[9] = c[0] * (g.c[56] * v[9] + g.c[57] * v[20])
+         + c[1] * (g.c[58] * v[4] + g.c[59] * v[6] + g.c[60] * v[23])
+         + c[2] * (g.c[61] * v[3] + g.c[62] * v[7] + g.c[63] * v[14])
+         + c[3] * (g.c[64] * v[10] + g.c[65] * v[17])
+         + c[4] * (g.c[66] * v[21])
+         + c[5] * (g.c[67] * v[16] + g.c[68] * v[18])
+         + c[6] * (g.c[69] * v[15] + g.c[70] * v[19])
+         + c[7] * (g.c[71] * v[22]);
+  f[10] = c[0] * (g.c[72] * v[10] + g.c[73] * v[17])
+         + c[1] * (g.c[74] * v[3] + g.c[75] * v[7] + g.c[76] * v[14])
+         + c[2] * (g.c[77] * v[4] + g.c[78] * v[6] + g.c[79] * v[23])
+         + c[3] * (g.c[80] * v[9] + g.c[81] * v[20])
+         + c[4] * (g.c[82] * v[22])
+         + c[5] * (g.c[83] * v[15] + g.c[84] * v[19])
+         + c[6] * (g.c[85] * v[16] + g.c[86] * v[18])
+         + c[7] * (g.c[87] * v[21]);
+  f[11] = c[0] * (g.c[88] * v[11] + g.c[89] * v[16] + g.c[90] * v[18])
+         + c[1] * (g.c[91] * v[8] + g.c[92] * v[13] + g.c[93] * v[21])
+         + c[2] * (g.c[94] * v[5] + g.c[95] * v[12] + g.c[96] * v[22])
+         + c[3] * (g.c[97] * v[15] + g.c[98] * v[19])
+         + c[4] * (g.c[99] * v[23])
+         + c[5] * (g.c[100] * v[20])
+         + c[6] * (g.c[101] * v[17]);
+  f[12] = c[0] * (g.c[102] * v[5] + g.c[103] * v[12])
+         + c[1] * (g.c[104] * v[15])
+         + c[2] * (g.c[105] * v[11] + g.c[106] * v[18])
+         + c[3] * (g.c[107] * v[21])
+         + c[4] * (g.c[108] * v[17])
+         + c[6] * (g.c[109] * v[23]);
+  f[13] = c[0] * (g.c[110] * v[8] + g.c[111] * v[13])
+         + c[1] * (g.c[112] * v[11] + g.c[113] * v[16])
+         + c[2] * (g.c[114] * v[19])
+         + c[3] * (g.c[115] * v[22])
+         + c[4] * (g.c[116] * v[20])
+         + c[5] * (g.c[117] * v[23]);
+  f[14] = c[0] * (g.c[118] * v[3] + g.c[119] * v[7] + g.c[120] * v[14])
+         + c[1] * (g.c[121] * v[10] + g.c[122] * v[17])
+         + c[2] * (g.c[123] * v[9] + g.c[124] * v[20])
+         + c[3] * (g.c[125] * v[23])
+         + c[4] * (g.c[126] * v[15] + g.c[127] * v[19])
+         + c[5] * (g.c[128] * v[22])
+         + c[6] * (g.c[129] * v[21]);
+  f[15] = c[0] * (g.c[130] * v[15] + g.c[131] * v[19])
+         + c[1] * (g.c[132] * v[5] + g.c[133] * v[12] + g.c[134] * v[22])
+         + c[2] * (g.c[135] * v[21])
+         + c[3] * (g.c[136] * v[11] + g.c[137] * v[18])
+         + c[4] * (g.c[138] * v[3] + g.c[139] * v[7] + g.c[140] * v[14])
+         + c[5] * (g.c[141] * v[10] + g.c[142] * v[17])
+         + c[6] * (g.c[143] * v[9] + g.c[144] * v[20])
+         + c[7] * (g.c[145] * v[23]);
+  f[16] = c[0] * (g.c[146] * v[11] + g.c[147] * v[16] + g.c[148] * v[18])
+         + c[1] * (g.c[149] * v[8] + g.c[150] * v[13] + g.c[151] * v[21])
+         + c[2] * (g.c[152] * v[22])
+         + c[3] * (g.c[153] * v[19])
+         + c[4] * (g.c[154] * v[4] + g.c[155] * v[6] + g.c[156] * v[23])
+         + c[5] * (g.c[157] * v[9] + g.c[158] * v[20])
+         + c[6] * (g.c[159] * v[10]);
+  f[17] = c[0] * (g.c[160] * v[10] + g.c[161] * v[17])
+         + c[1] * (g.c[162] * v[3] + g.c[163] * v[7] + g.c[164] * v[14])
+         + c[2] * (g.c[165] * v[23])
+         + c[3] * (g.c[166] * v[9] + g.c[167] * v[20])
+         + c[4] * (g.c[168] * v[5] + g.c[169] * v[12] + g.c[170] * v[22])
+         + c[5] * (g.c[171] * v[15] + g.c[172] * v[19])
+         + c[6] * (g.c[173] * v[11] + g.c[174] * v[18])
+         + c[7] * (g.c[175] * v[21]);
+  f[18] = c[0] * (g.c[176] * v[11] + g.c[177] * v[16] + g.c[178] * v[18])
+         + c[1] * (g.c[179] * v[21])
+         + c[2] * (g.c[180] * v[5] + g.c[181] * v[12] + g.c[182] * v[22])
+         + c[3] * (g.c[183] * v[15])
+         + c[4] * (g.c[184] * v[4] + g.c[185] * v[6] + g.c[186] * v[23])
+         + c[5] * (g.c[187] * v[9])
+         + c[6] * (g.c[188] * v[10] + g.c[189] * v[17]);
+  f[19] = c[0] * (g.c[190] * v[15] + g.c[191] * v[19])
+         + c[1] * (g.c[192] * v[22])
+         + c[2] * (g.c[193] * v[8] + g.c[194] * v[13] + g.c[195] * v[21])
+         + c[3] * (g.c[196] * v[11] + g.c[197] * v[16])
+         + c[4] * (g.c[198] * v[3] + g.c[199] * v[7] + g.c[200] * v[14])
+         + c[5] * (g.c[201] * v[10] + g.c[202] * v[17])
+         + c[6] * (g.c[203] * v[9] + g.c[204] * v[20])
+         + c[7] * (g.c[205] * v[23]);
+  f[20] = c[0] * (g.c[206] * v[9] + g.c[207] * v[20])
+         + c[1] * (g.c[208] * v[23])
+         + c[2] * (g.c[209] * v[3] + g.c[210] * v[7] + g.c[211] * v[14])
+         + c[3] * (g.c[212] * v[10] + g.c[213] * v[17])
+         + c[4] * (g.c[214] * v[8] + g.c[215] * v[13] + g.c[216] * v[21])
+         + c[5] * (g.c[217] * v[11] + g.c[218] * v[16])
+         + c[6] * (g.c[219] * v[15] + g.c[220] * v[19])
+         + c[7] * (g.c[221] * v[22]);
+  f[21] = c[0] * (g.c[222] * v[21])
+         + c[1] * (g.c[223] * v[11] + g.c[224] * v[16] + g.c[225] * v[18])
+         + c[2] * (g.c[226] * v[15] + g.c[227] * v[19])
+         + c[3] * (g.c[228] * v[5] + g.c[229] * v[12] + g.c[230] * v[22])
+         + c[4] * (g.c[231] * v[9] + g.c[232] * v[20])
+         + c[5] * (g.c[233] * v[4] + g.c[234] * v[6] + g.c[235] * v[23])
+         + c[6] * (g.c[236] * v[3] + g.c[237] * v[7] + g.c[238] * v[14])
+         + c[7] * (g.c[239] * v[10] + g.c[240] * v[17]);
+  f[22] = c[0] * (g.c[241] * v[22])
+         + c[1] * (g.c[242] * v[15] + g.c[243] * v[19])
+         + c[2] * (g.c[244] * v[11] + g.c[245] * v[16] + g.c[246] * v[18])
+         + c[3] * (g.c[247] * v[8] + g.c[248] * v[13] + g.c[249] * v[21])
+         + c[4] * (g.c[250] * v[10] + g.c[251] * v[17])
+         + c[5] * (g.c[252] * v[3] + g.c[253] * v[7] + g.c[254] * v[14])
+         + c[6] * (g.c[255] * v[4] + g.c[256] * v[6] + g.c[257] * v[23])
+         + c[7] * (g.c[258] * v[9] + g.c[259] * v[20]);
+  f[23] = c[0] * (g.c[260] * v[23])
+         + c[1] * (g.c[261] * v[9] + g.c[262] * v[20])
+         + c[2] * (g.c[263] * v[10] + g.c[264] * v[17])
+         + c[3] * (g.c[265] * v[3] + g.c[266] * v[7] + g.c[267] * v[14])
+         + c[4] * (g.c[268] * v[11] + g.c[269] * v[16] + g.c[270] * v[18])
+         + c[5] * (g.c[271] * v[8] + g.c[272] * v[13] + g.c[273] * v[21])
+         + c[6] * (g.c[274] * v[5] + g.c[275] * v[12] + g.c[276] * v[22])
+         + c[7] * (g.c[277] * v[15] + g.c[278] * v[19]);
+}
+
+// modes 1, s (per axis) of a pair: (a, b) -> (a + b, b - a)
+template <typename T>
+__device__ __forceinline__ void fwht8(const T (&w)[8], T (&c)[8]) {
+  T a[8], b[8];
+#pragma unroll
+  for (int k = 0; k < 8; k += 2) { a[k] = w[k] + w[k + 1]; a[k + 1] = w[k + 1] - w[k]; }
+#pragma unroll
+  for (int k = 0; k < 8; k += 4) {
+    b[k] = a[k] + a[k + 2]; b[k + 2] = a[k + 2] - a[k];
+    b[k + 1] = a[k + 1] + a[k + 3]; b[k + 3] = a[k + 3] - a[k + 1];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { c[k] = b[k] + b[k + 4]; c[k + 4] = b[k + 4] - b[k]; }
+}
+
+template <typename T>
+__device__ __forceinline__ void xy4(T u00, T u10, T u01, T u11, T (&a)[4]) {
+  T sx0 = u00 + u10, dx0 = u10 - u00, sx1 = u01 + u11, dx1 = u11 - u01;
+  a[0] = sx0 + sx1;
+  a[1] = dx0 + dx1;
+  a[2] = sx1 - sx0;
+  a[3] = dx1 - dx0;
+}
+
+// x-y modes of node plane z of the four columns around cell column (cx, cy), one component
+template <typename T>
+__device__ __forceinline__ void plane_modes(const T* __restrict__ u, const long long (&col)[4], const bool (&ok)[4],
+                                            long long cs, int z, int pz, T (&a)[4][3]) {
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    T v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = (ok[q] && z < pz) ? __ldg(u + cc * cs + col[q] + z) : T(0);
+    T m[4];
+    xy4(v[0], v[1], v[2], v[3], m);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q][cc] = m[q];
+  }
+}
+
+// one cell's modal forces from the x-y modes of its lower and upper node planes
+template <typename T>
+__device__ __forceinline__ void weights_cell(const G1<T>& gc, const T (&a_lo)[4][3], const T (&a_hi)[4][3],
+                                             const T (&wk)[8], T (&f)[24]) {
+  T v[24], cw[8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const T lo = a_lo[q][cc], hi = a_hi[q][cc];
+      v[3 * q + cc] = lo + hi;
+      v[3 * (q + 4) + cc] = hi - lo;
+    }
+  fwht8(wk, cw);
+  g1_product<T>(gc, cw, v, f);
+}
+
+// level-1 operator, u zero on masked dofs: out = m K u
+template <typename T>
+__global__ void __launch_bounds__(TXC * TYC, 1)
+k_weights_march(T* __restrict__ out, const T* __restrict__ u, const T* __restrict__ w,
+                const uint8_t* __restrict__ mask, const G1<T> gc, LpGrid g, int zch, int nchunks) {
+  __shared__ T red[3][4][TXC * TYC];     // corner 01 + 11 (-> y + 1)
+  __shared__ T own_s[3][4][TXC * TYC];   // corner 00 + 10 of the -x neighbour
+  const int tid = threadIdx.x;
+  const int i = tid % TXC, j = tid / TXC;
+  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
+  const int c_begin = blockIdx.z * zch;
+  const int c_end = min(c_begin + zch, nchunks);
+  if (c_begin >= c_end) return;
+  const int cx = x0 - 1 + i, cy = y0 - 1 + j;
+  const int NX = g.NX(), NY = g.NY();
+  const long long cs = g.comp_stride(), ncp = g.cells_padded();
+  const bool cell_ok = cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny;
+  const bool own = i >= 1 && j >= 1 && cx < NX && cy < NY;
+  bool col_ok[4];
+  long long col_base[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int nx_ = cx + (q & 1), ny_ = cy + (q >> 1);
+    col_ok[q] = nx_ >= 0 && nx_ < NX && ny_ >= 0 && ny_ < NY;
+    col_base[q] = col_ok[q] ? g.node(nx_, ny_, 0) : 0;
+  }
+  const long long ebase = cell_ok ? g.cell(cx, cy, 0) : 0;
+  const long long obase = own ? g.node(cx, cy, 0) : 0;
+  T up_carry[4][3], a_lo[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) up_carry[q][c] = T(0);
+  const int z0 = 4 * c_begin;
+  if (c_begin > 0) {
+    // the cell below the segment: its upper face starts the carry
+    T a_hi[4][3], wk[8], f[24];
+    plane_modes(u, col_base, col_ok, cs, z0 - 1, g.pz, a_lo);
+    plane_modes(u, col_base, col_ok, cs, z0, g.pz, a_hi);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) wk[k] = cell_ok ? __ldg(w + k * ncp + ebase + z0 - 1) : T(0);
+    weights_cell(gc, a_lo, a_hi, wk, f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        up_carry[q][cc] = f[3 * q + cc] + f[3 * (q + 4) + cc];
+        a_lo[q][cc] = a_hi[q][cc];
+      }
+  } else {
+    plane_modes(u, col_base, col_ok, cs, 0, g.pz, a_lo);
+  }
+
+  for (int ch = c_begin; ch < c_end; ++ch) {
+    const int z = 4 * ch;
+#pragma unroll 1
+    for (int t = 0; t < 4; ++t) {
+      T a_hi[4][3], wk[8], f[24];
+      plane_modes(u, col_base, col_ok, cs, z + t + 1, g.pz, a_hi);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) wk[k] = cell_ok ? __ldg(w + k * ncp + ebase + z + t) : T(0);
+      weights_cell(gc, a_lo, a_hi, wk, f);
+      T fp[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const T f0 = f[3 * q + cc], f1 = f[3 * (q + 4) + cc];
+          fp[q][cc] = up_carry[q][cc] + (f0 - f1);
+          up_carry[q][cc] = f0 + f1;
+          a_lo[q][cc] = a_hi[q][cc];
+        }
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const T t0 = fp[0][cc] - fp[2][cc], t1 = fp[1][cc] - fp[3][cc];
+        const T t2 = fp[0][cc] + fp[2][cc], t3 = fp[1][cc] + fp[3][cc];
+        const T c10 = __shfl_up_sync(0xffffffffu, t0 + t1, 1, TXC);
+        const T c11 = __shfl_up_sync(0xffffffffu, t2 + t3, 1, TXC);
+        own_s[cc][t][tid] = (t0 - t1) + c10;
+        red[cc][t][tid] = (t2 - t3) + c11;
+      }
+    }
+    __syncthreads();
+    if (own) {
+      const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + obase + z);
+      const uint8_t mbs[4] = {mb.x, mb.y, mb.z, mb.w};
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        T o[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const T sv = own_s[cc][t][tid] + red[cc][t][tid - TXC];
+          o[t] = ((mbs[t] >> cc) & 1) ? sv : T(0);
+        }
+        V4<T>::st(out + cc * cs + obase + z, o);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// patch cells (weights zero, an explicit masked matrix): out += m * sum of their rows times
+// u, node by node over the box of nodes they touch; runs after k_weights_march
+template <typename T>
+__global__ void k_patch_add(T* __restrict__ out, const T* __restrict__ u, const int* __restrict__ pid,
+                            const T* __restrict__ pk, const uint8_t* __restrict__ mask, LpGrid g, int bx0, int by0,
+                            int bz0, int bnx, int bny, int bnz) {
+  const long long total = (long long)bnx * bny * bnz;
+  const long long cs = g.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int z = bz0 + (int)(t % bnz);
+    const long long q = t / bnz;
+    const int y = by0 + (int)(q % bny), x = bx0 + (int)(q / bny);
+    T a[3] = {T(0), T(0), T(0)};
+    bool any = false;
+    for (int kk = 0; kk < 8; ++kk) {
+      const int cx = x - cx_(kk), cy = y - cy_(kk), cz = z - cz_(kk);
+      if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
+      const int p = pid[g.cell(cx, cy, cz)];
+      if (p < 0) continue;
+      any = true;
+      const T* kp = pk + (long long)p * 576;
+      for (int q2 = 0; q2 < 8; ++q2) {
+        const long long n2 = g.node(cx + cx_(q2), cy + cy_(q2), cz + cz_(q2));
+        for (int c2 = 0; c2 < 3; ++c2) {
+          const T uv = u[c2 * cs + n2];
+          for (int cc = 0; cc < 3; ++cc) a[cc] += kp[(3 * kk + cc) * 24 + 3 * q2 + c2] * uv;
+        }
+      }
+    }
+    if (!any) continue;
+    const long long n = g.node(x, y, z);
+    const uint8_t mb = mask[n];
+    for (int cc = 0; cc < 3; ++cc)
+      if ((mb >> cc) & 1) out[cc * cs + n] += a[cc];
+  }
+}
+
+// ---- explicit levels: packed symmetric matrices, entry-major ---------------------------------
+__host__ __device__ __forceinline__ int sym_index(int i, int j) {  // i <= j
+  return i * 24 - (i * (i - 1)) / 2 + (j - i);
+}
+
+template <typename T>
+__global__ void k_explicit_cells(T* __restrict__ ft, const T* __restrict__ u, const T* __restrict__ kp, LpGrid g) {
+  const long long ncell = (long long)g.nx * g.ny * g.nz;
+  const long long ncp = g.cells_padded();
+  const long long cs = g.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell; t += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(t % g.nz);
+    const long long q = t / g.nz;
+    const int y = (int)(q % g.ny), x = (int)(q / g.ny);
+    const long long c = g.cell(x, y, z);
+    T uc[24], f[24];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const long long n = g.node(x + cx_(k), y + cy_(k), z + cz_(k));
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) uc[3 * k + cc] = u[cc * cs + n];
+    }
+#pragma unroll
+    for (int r = 0; r < 24; ++r) f[r] = T(0);
+#pragma unroll
+    for (int a = 0; a < 24; ++a) {
+#pragma unroll
+      for (int b = a; b < 24; ++b) {
+        const T kab = __ldg(kp + (long long)sym_index(a, b) * ncp + c);
+        f[a] += kab * uc[b];
+        if (b != a) f[b] += kab * uc[a];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 24; ++r) ft[(long long)r * ncp + c] = f[r];
+  }
+}
+
+template <typename T>
+__global__ void k_explicit_gather(T* __restrict__ out, const T* __restrict__ ft, const uint8_t* __restrict__ mask,
+                                  LpGrid g) {
+  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
+  const long long total = (long long)NX * NY * NZ;
+  const long long ncp = g.cells_padded(), cs = g.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(t % NZ);
+    const long long q = t / NZ;
+    const int y = (int)(q % NY), x = (int)(q / NY);
+    T a[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int cx = x - cx_(k), cy = y - cy_(k), cz = z - cz_(k);
+      if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
+      const long long c = g.cell(cx, cy, cz);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) a[cc] += ft[(long long)(3 * k + cc) * ncp + c];
+    }
+    const long long n = g.node(x, y, z);
+    const uint8_t mb = mask[n];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) out[cc * cs + n] = ((mb >> cc) & 1) ? a[cc] : T(0);
+  }
+}
+
+// full (cells, 576) matrices -> packed symmetric entry-major (the average of K and K^T)
+template <typename Ti, typename To>
+__global__ void k_pack_sym(To* __restrict__ kp, const Ti* __restrict__ k, long long ncp) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 300 * ncp; t += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(t / ncp);
+    const long long c = t % ncp;
+    int a = 0, rem = p;
+    while (rem >= 24 - a) { rem -= 24 - a; ++a; }
+    const int b = a + rem;
+    kp[t] = (To)(0.5 * ((double)k[c * 576 + a * 24 + b] + (double)k[c * 576 + b * 24 + a]));
+  }
+}
+
+}  // namespace
+
+#define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
+#define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
+#define LP_ST ((cudaStream_t)stream)
+
+static double pw_host(int k, int q, int r) {
+  double w = 1.0;
+  for (int a = 0; a < 3; ++a) {
+    const int p = ((k >> a) & 1) + ((q >> a) & 1);
+    const double t = 0.5 * p;
+    w *= ((r >> a) & 1) ? t : 1.0 - t;
+  }
+  return w;
+}
+
+static const int G1_ROWS[279] = {3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 4, 4, 4, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 5, 5, 5, 6, 6, 6, 6, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 8, 8, 8, 8, 8, 8, 8, 8, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 12, 12, 12, 12, 12, 12, 12, 12, 13, 13, 13, 13, 13, 13, 13, 13, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 20, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 21, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 22, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23, 23};
+static const int G1_TS[279] = {0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6, 0, 0, 1, 2, 4, 4, 5, 6, 0, 0, 1, 2, 2, 3, 4, 6, 0, 0, 1, 2, 4, 4, 5, 6, 0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6, 0, 0, 1, 1, 2, 3, 4, 5, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5, 5, 6, 6, 7, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5, 5, 6, 6, 7, 0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5, 6, 0, 0, 1, 2, 2, 3, 4, 6, 0, 0, 1, 1, 2, 3, 4, 5, 0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6, 0, 0, 1, 1, 1, 2, 3, 3, 4, 4, 4, 5, 5, 6, 6, 7, 0, 0, 0, 1, 1, 1, 2, 3, 4, 4, 4, 5, 5, 6, 0, 0, 1, 1, 1, 2, 3, 3, 4, 4, 4, 5, 5, 6, 6, 7, 0, 0, 0, 1, 2, 2, 2, 3, 4, 4, 4, 5, 6, 6, 0, 0, 1, 2, 2, 2, 3, 3, 4, 4, 4, 5, 5, 6, 6, 7, 0, 0, 1, 2, 2, 2, 3, 3, 4, 4, 4, 5, 5, 6, 6, 7, 0, 1, 1, 1, 2, 2, 3, 3, 3, 4, 4, 5, 5, 5, 6, 6, 6, 7, 7, 0, 1, 1, 2, 2, 2, 3, 3, 3, 4, 4, 5, 5, 5, 6, 6, 6, 7, 7, 0, 1, 1, 2, 2, 3, 3, 3, 4, 4, 4, 5, 5, 5, 6, 6, 6, 7, 7};
+static const int G1_COLS[279] = {3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 4, 6, 9, 10, 16, 18, 21, 22, 5, 12, 15, 11, 18, 21, 17, 23, 4, 6, 9, 10, 16, 18, 21, 22, 3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 8, 13, 11, 16, 19, 22, 20, 23, 9, 20, 4, 6, 23, 3, 7, 14, 10, 17, 21, 16, 18, 15, 19, 22, 10, 17, 3, 7, 14, 4, 6, 23, 9, 20, 22, 15, 19, 16, 18, 21, 11, 16, 18, 8, 13, 21, 5, 12, 22, 15, 19, 23, 20, 17, 5, 12, 15, 11, 18, 21, 17, 23, 8, 13, 11, 16, 19, 22, 20, 23, 3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 15, 19, 5, 12, 22, 21, 11, 18, 3, 7, 14, 10, 17, 9, 20, 23, 11, 16, 18, 8, 13, 21, 22, 19, 4, 6, 23, 9, 20, 10, 10, 17, 3, 7, 14, 23, 9, 20, 5, 12, 22, 15, 19, 11, 18, 21, 11, 16, 18, 21, 5, 12, 22, 15, 4, 6, 23, 9, 10, 17, 15, 19, 22, 8, 13, 21, 11, 16, 3, 7, 14, 10, 17, 9, 20, 23, 9, 20, 23, 3, 7, 14, 10, 17, 8, 13, 21, 11, 16, 15, 19, 22, 21, 11, 16, 18, 15, 19, 5, 12, 22, 9, 20, 4, 6, 23, 3, 7, 14, 10, 17, 22, 15, 19, 11, 16, 18, 8, 13, 21, 10, 17, 3, 7, 14, 4, 6, 23, 9, 20, 23, 9, 20, 10, 17, 3, 7, 14, 11, 16, 18, 8, 13, 21, 5, 12, 22, 15, 19};
+
+template <typename T>
+static int launch_weights(T* out, const T* u, const T* w, const int* pid, const T* pk, const uint8_t* mask,
+                          const double* g1_host, const int* pbox, LpGrid g, cudaStream_t st) {
+  if (!lp_grid_ok(g) || g.pz % 4 || g.cpz != g.pz || !out || !u || !w || !mask || !g1_host || out == u)
+    return LP_ERR_ARG;
+  G1<T> gc;
+  for (int i = 0; i < 279; ++i) gc.c[i] = (T)g1_host[i];
+  const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
+  const int nchunks = g.pz / 4;
+  int dev = 0, nsm = 148;  // one resident block per SM
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int best = nchunks;
+  double bc = 1e30;
+  for (int zch = 2; zch <= nchunks; ++zch) {
+    const long long nseg = (nchunks + zch - 1) / zch, units = (long long)gx * gy * nseg;
+    const double cost = (double)((units + nsm - 1) / nsm) * (zch + (nseg > 1 ? 0.3 : 0.0));
+    if (cost < bc - 1e-9) { bc = cost; best = zch; }
+  }
+  dim3 grid(gx, gy, (nchunks + best - 1) / best);
+  k_weights_march<T><<<grid, TXC * TYC, 0, st>>>(out, u, w, mask, gc, g, best, nchunks);
+  if (pid && pk && pbox && pbox[3] > 0 && pbox[4] > 0 && pbox[5] > 0) {
+    const long long nb = (long long)pbox[3] * pbox[4] * pbox[5];
+    k_patch_add<T><<<lp_blocks(nb, 128), 128, 0, st>>>(out, u, pid, pk, mask, g, pbox[0], pbox[1], pbox[2], pbox[3],
+                                                       pbox[4], pbox[5]);
+  }
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+template <typename T>
+static int launch_explicit(T* out, const T* u, const T* kp, T* ft, const uint8_t* mask, LpGrid g, cudaStream_t st) {
+  if (!lp_grid_ok(g) || !out || !u || !kp || !ft || !mask || out == u) return LP_ERR_ARG;
+  const long long ncell = (long long)g.nx * g.ny * g.nz;
+  const long long nn = (long long)g.NX() * g.NY() * g.NZ();
+  k_explicit_cells<T><<<lp_blocks(ncell, 128), 128, 0, st>>>(ft, u, kp, g);
+  k_explicit_gather<T><<<lp_blocks(nn, 256), 256, 0, st>>>(out, ft, mask, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+extern "C" {
+
+// the 279 corner-parity coefficients of the eight G_t = sum_k H[t, k] P_k^T Ke P_k / 8 (host)
+int lpb_modal_g1(const double* ke, double* g1_out) {
+  if (!ke || !g1_out) return LP_ERR_ARG;
+  double h[8][8];
+  for (int m = 0; m < 8; ++m)
+    for (int k = 0; k < 8; ++k) {
+      double v = 1.0;
+      for (int a = 0; a < 3; ++a)
+        if ((m >> a) & 1) v *= ((k >> a) & 1) ? 1.0 : -1.0;
+      h[m][k] = v;
+    }
+  // M_k = P_k^T Ke P_k
+  static double mk[8][24][24];
+  for (int k = 0; k < 8; ++k)
+    for (int i = 0; i < 24; ++i)
+      for (int jj = 0; jj < 24; ++jj) {
+        const int ri = i / 3, ci = i % 3, rj = jj / 3, cj = jj % 3;
+        double s = 0.0;
+        for (int q1 = 0; q1 < 8; ++q1) {
+          const double p1 = pw_host(k, q1, ri);
+          if (p1 == 0.0) continue;
+          for (int q2 = 0; q2 < 8; ++q2) {
+            const double p2 = pw_host(k, q2, rj);
+            if (p2 == 0.0) continue;
+            s += p1 * ke[(3 * q1 + ci) * 24 + 3 * q2 + cj] * p2;
+          }
+        }
+        mk[k][i][jj] = s;
+      }
+  double amax = 0.0;
+  static double gh[8][24][24];
+  for (int t = 0; t < 8; ++t)
+    for (int r = 0; r < 24; ++r)
+      for (int c = 0; c < 24; ++c) {
+        const int mr = r / 3, cr = r % 3, mc = c / 3, cc = c % 3;
+        double s = 0.0;
+        for (int k1 = 0; k1 < 8; ++k1)
+          for (int k2 = 0; k2 < 8; ++k2) {
+            double gsum = 0.0;
+            for (int k = 0; k < 8; ++k) gsum += h[t][k] * mk[k][3 * k1 + cr][3 * k2 + cc];
+            s += h[mr][k1] * gsum * h[mc][k2];
+          }
+        gh[t][r][c] = s / (8.0 * 64.0);
+        if (fabs(gh[t][r][c]) > amax) amax = fabs(gh[t][r][c]);
+      }
+  static bool used[8][24][24];
+  for (int t = 0; t < 8; ++t)
+    for (int r = 0; r < 24; ++r)
+      for (int c = 0; c < 24; ++c) used[t][r][c] = false;
+  for (int i = 0; i < 279; ++i) used[G1_TS[i]][G1_ROWS[i]][G1_COLS[i]] = true;
+  for (int t = 0; t < 8; ++t)
+    for (int r = 0; r < 24; ++r)
+      for (int c = 0; c < 24; ++c)
+        if (!used[t][r][c] && fabs(gh[t][r][c]) > 1e-12 * amax) return -1;
+  for (int i = 0; i < 279; ++i) g1_out[i] = gh[G1_TS[i]][G1_ROWS[i]][G1_COLS[i]];
+  return 279;
+}
+
+// pbox (host, 6 ints): node box x0, y0, z0, nx, ny, nz holding every node a patch cell touches
+int lpb_apply_weights_march_f32(float* out, const float* u, const float* w, const int* patch_id, const float* patch_k,
+                                const uint8_t* mask, const double* g1, const int* pbox, LP_GRID_ARGS, void* stream) {
+  return launch_weights<float>(out, u, w, patch_id, patch_k, mask, g1, pbox, LP_GRID, LP_ST);
+}
+
+int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, const int* patch_id,
+                                const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox,
+                                LP_GRID_ARGS, void* stream) {
+  return launch_weights<double>(out, u, w, patch_id, patch_k, mask, g1, pbox, LP_GRID, LP_ST);
+}
+
+int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask,
+                               LP_GRID_ARGS, void* stream) {
+  return launch_explicit<float>(out, u, kp, ft, mask, LP_GRID, LP_ST);
+}
+
+int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask,
+                               LP_GRID_ARGS, void* stream) {
+  return launch_explicit<double>(out, u, kp, ft, mask, LP_GRID, LP_ST);
+}
+
+int lpb_pack_sym_f32(float* kp, const float* k, long long ncells, void* stream) {
+  if (!kp || !k || ncells < 0) return LP_ERR_ARG;
+  k_pack_sym<float, float><<<lp_blocks(300 * ncells, 256), 256, 0, LP_ST>>>(kp, k, ncells);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_pack_sym_f64(double* kp, const double* k, long long ncells, void* stream) {
+  if (!kp || !k || ncells < 0) return LP_ERR_ARG;
+  k_pack_sym<double, double><<<lp_blocks(300 * ncells, 256), 256, 0, LP_ST>>>(kp, k, ncells);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+}  // extern "C"

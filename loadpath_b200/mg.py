@@ -93,6 +93,10 @@ class DevLevel:
         self.w = self.mcat = self.patch_id = self.patch_k = None
         self.npatch = 0
         self.k = None
+        self.kp = None           # explicit: packed symmetric (300, cells)
+        self.ft = None           # explicit: (24, cells) scratch of the cell pass
+        self.g1 = None           # weights: 279 corner-parity coefficients (host)
+        self.pbox = None         # weights: node box of the patch cells (host, 6 ints)
         self.mask = None
         self.dinv = None
         self.lmax = None
@@ -133,12 +137,24 @@ class DevLevel:
                                                        self.mask.data_ptr(), self.ke.data_ptr(), *g.args,
                                                        int(mask_in), 1, st)
         elif self.kind == "weights":
-            getattr(L, f"lpb_apply_weights_{sfx}")(out.data_ptr(), u.data_ptr(), self.w.data_ptr(),
-                                                    self.mcat.data_ptr(), ptr(self.patch_id), ptr(self.patch_k),
-                                                    self.mask.data_ptr(), *g.args, int(mask_in), 1, st)
+            if fine_kernel and not mask_in:
+                getattr(L, f"lpb_apply_weights_march_{sfx}")(out.data_ptr(), u.data_ptr(), self.w.data_ptr(),
+                                                              ptr(self.patch_id) if self.npatch else None,
+                                                              ptr(self.patch_k) if self.npatch else None,
+                                                              self.mask.data_ptr(), self.g1.ctypes.data,
+                                                              self.pbox.ctypes.data, *g.args, st)
+            else:
+                getattr(L, f"lpb_apply_weights_{sfx}")(out.data_ptr(), u.data_ptr(), self.w.data_ptr(),
+                                                        self.mcat.data_ptr(), ptr(self.patch_id),
+                                                        ptr(self.patch_k), self.mask.data_ptr(), *g.args,
+                                                        int(mask_in), 1, st)
         else:
-            getattr(L, f"lpb_apply_explicit_{sfx}")(out.data_ptr(), u.data_ptr(), self.k.data_ptr(),
-                                                     self.mask.data_ptr(), *g.args, int(mask_in), 1, st)
+            if fine_kernel and not mask_in:
+                getattr(L, f"lpb_apply_explicit_sym_{sfx}")(out.data_ptr(), u.data_ptr(), self.kp.data_ptr(),
+                                                             self.ft.data_ptr(), self.mask.data_ptr(), *g.args, st)
+            else:
+                getattr(L, f"lpb_apply_explicit_{sfx}")(out.data_ptr(), u.data_ptr(), self.k.data_ptr(),
+                                                         self.mask.data_ptr(), *g.args, int(mask_in), 1, st)
         return out
 
     def diagonal(self, d):
@@ -210,6 +226,10 @@ class GridElasticity:
         self.ke32 = self.ke64.float()
         pk = fem.child_prolongations()
         self._mcat = np.einsum("kai,ab,kbj->kij", pk, self.ke, pk).reshape(8, 576)
+        g1 = np.zeros(279)
+        if lib().lpb_modal_g1(np.ascontiguousarray(self.ke).ctypes.data, g1.ctypes.data) != 279:
+            raise LpError("the level-1 Galerkin matrices are not in the corner-parity pattern of the kernel")
+        self.g1 = g1
         self.levels = []
         self.strict = False
         self.last_iters = 0
@@ -372,6 +392,17 @@ class GridElasticity:
             else:
                 lv.patch_k = None
             lv.patch_cells = pcells
+            lv.g1 = self.g1
+            lv.pbox = np.zeros(6, np.int32)
+            if lv.npatch:
+                z = pcells % gc.cpz
+                yx = pcells // gc.cpz
+                y = yx % gc.ny
+                x = yx // gc.ny
+                lo = torch.stack([x.min(), y.min(), z.min()]).cpu().numpy()
+                hi = torch.stack([x.max(), y.max(), z.max()]).cpu().numpy() + 2   # nodes of the last cell
+                lv.pbox[:3] = lo
+                lv.pbox[3:] = hi - lo
             return lv
         lv = DevLevel("explicit", gc, dt)
         lv.k = torch.zeros((gc.nx * gc.ny * gc.cpz, 576), dtype=dt, device=self.device)
@@ -382,6 +413,10 @@ class GridElasticity:
         else:
             getattr(L, f"lpb_galerkin_explicit_{sfx}")(lv.k.data_ptr(), 2, None, None, None, None, fine.k.data_ptr(),
                                                        fine.mask.data_ptr(), int(self.strict), *gf.args, *gc.args, st)
+        ncp = gc.nx * gc.ny * gc.cpz
+        lv.kp = torch.empty((300, ncp), dtype=dt, device=self.device)
+        getattr(L, f"lpb_pack_sym_{sfx}")(lv.kp.data_ptr(), lv.k.data_ptr(), ncp, st)
+        lv.ft = torch.empty((24, ncp), dtype=dt, device=self.device)
         return lv
 
     def _build_coarse(self, lv: DevLevel) -> bool:
