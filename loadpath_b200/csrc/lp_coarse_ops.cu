@@ -17,6 +17,8 @@
 // (24, cells) buffer, a node pass sums each node's eight cells' rows and applies the mask.
 #include "lp_common.cuh"
 
+#include <mutex>
+
 namespace {
 
 constexpr int TXC = 16, TYC = 16;
@@ -540,6 +542,31 @@ static int launch_explicit(T* out, const T* u, const T* kp, T* ft, const uint8_t
   return LP_OK;
 }
 
+// ---- the explicit-level apply without caller scratch -----------------------------------------
+// For callers that cannot allocate device memory: a host application or language binding that
+// owns every device allocation and hands this library only the pointers it needs, or a loop
+// that must never call cudaMalloc / cudaFree (they synchronize the device). The cell pass's
+// (24, cells) intermediate lives in this file-scope array instead of a caller buffer. Every GPU
+// that loads the library holds it (6 MB) until the process exits.
+#define LP_NOALLOC_MAX_CELLS (1 << 16)   // padded cells (nx * ny * cpz) one call may cover
+#define LP_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) float g_explicit_scratch[24 * LP_NOALLOC_MAX_CELLS];
+
+// the array's device address on the current device, looked up once per device
+static float* explicit_scratch_address() {
+  static std::mutex mu;
+  static float* addr[LP_NOALLOC_MAX_DEVICES] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= LP_NOALLOC_MAX_DEVICES) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_explicit_scratch) != cudaSuccess || !p) return nullptr;
+    addr[dev] = static_cast<float*>(p);
+  }
+  return addr[dev];
+}
+
 extern "C" {
 
 // the 279 corner-parity coefficients of the eight G_t = sum_k H[t, k] P_k^T Ke P_k / 8 (host)
@@ -620,6 +647,22 @@ int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, floa
 int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask,
                                LP_GRID_ARGS, void* stream) {
   return launch_explicit<double>(out, u, kp, ft, mask, LP_GRID, LP_ST);
+}
+
+// lpb_apply_explicit_sym_f32 with its (24, cells) scratch in the library's static array: no
+// allocation by the caller or the library. Grids with more than LP_NOALLOC_MAX_CELLS padded
+// cells return LP_ERR_SIZE. The first call on a device looks the array's address up (it should
+// come before any stream capture); calls that overlap on the GPU share the array and race. The
+// cell pass writes every entry the node pass reads, so stale contents from an earlier call are
+// never used and nothing needs clearing.
+int lpb_apply_explicit_sym_noalloc_f32(float* out, const float* u, const float* kp, const uint8_t* mask, LP_GRID_ARGS,
+                                       void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g)) return LP_ERR_ARG;
+  if (g.cells_padded() > LP_NOALLOC_MAX_CELLS) return LP_ERR_SIZE;
+  float* ft = explicit_scratch_address();
+  if (!ft) return LP_ERR_LAUNCH;
+  return launch_explicit<float>(out, u, kp, ft, mask, g, LP_ST);
 }
 
 int lpb_pack_sym_f32(float* kp, const float* k, long long ncells, void* stream) {
