@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--micro", choices=["apply"], default=None,
+                   help="only the fine-level K*u microbenchmark (config 1: applies on seeded N(0,1) vectors)")
+    p.add_argument("--reps", type=int, default=100)
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     a.dims = tuple(int(v) for v in a.dims.split(","))
@@ -232,6 +235,7 @@ def run_b200(args):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     mg.set_probe(probe)
+    loop.timing = []
     t0.record()
     iters = []
     for _ in range(args.steps):
@@ -267,7 +271,11 @@ def run_b200(args):
                     "traffic": traffic, "kernel": "k_apply_fine<float>",
                     "algorithmic_bytes": b32, "avg_launch_us": avg * 1e6, "launches_timed": fine["f32_count"],
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
+    phases = np.array([[a.elapsed_time(b) for a, b in zip(ev[:-1], ev[1:])] for ev in loop.timing])
+    loop.timing = None
     extra = {"cg_iterations": iters, "compliance": loop.history[-1][0],
+             "phase_ms_per_step": dict(zip(("hierarchy", "solve", "sensitivities", "oc"),
+                                           np.round(phases.mean(axis=0), 3).tolist())),
              "fine_apply_f64_us": (fine["f64_ms"] / fine["f64_count"] * 1e3) if fine["f64_count"] else None,
              "fine_applies_per_step": {"f64": fine["f64_count"] / args.steps, "f32": fine["f32_count"] / args.steps}}
     del loop
@@ -366,9 +374,64 @@ def run_b200(args):
     return 0
 
 
+def run_micro_apply(args):
+    """args.reps fine-level applies (float32 and float64) on seeded N(0,1) vectors at the bench's
+    density, timed with CUDA events; one JSON line."""
+    import torch
+
+    from loadpath_b200.grid import DevGrid
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from loadpath_b200.simp import DeviceFilter
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    g = DevGrid(dims)
+    rng = np.random.default_rng(1)
+    flt = DeviceFilter(g, 2.0)
+    xr = g.cells_to_dev(np.exp(rng.uniform(np.log(1e-3), 0.0, dims)), torch.float64)
+    x = flt.apply(g.cell_field(torch.float64), xr, hs_out=flt.hs)
+    e = g.cell_field(torch.float64)
+    from loadpath_b200._lib import lib
+    from loadpath_b200.grid import stream_handle
+
+    lib().lpb_simp_law(e.data_ptr(), x.data_ptr(), PENAL, EMIN, *g.args, stream_handle())
+    fixed, _ = cantilever(dims)
+    mesh = BoxMesh(dims)
+    fx = np.empty(mesh.n_dof, bool)
+    for i in range(3):
+        fx[i::3] = fixed[i].reshape(-1)
+    ge = GridElasticity(mesh, 0.3, fx, coarse_cells=10 ** 12, element="im")
+    ge.set_moduli_device(e)
+    out = {}
+    for lv in (ge._l0s, ge.levels[0]):
+        gr = lv.grid
+        m = torch.stack([((lv.mask >> c) & 1) for c in range(3)]).to(lv.dtype)
+        u = torch.randn((3, gr.NX, gr.NY, gr.pz), generator=torch.Generator(device="cuda").manual_seed(101),
+                        device="cuda", dtype=torch.float64).to(lv.dtype) * m
+        o = gr.node_field(lv.dtype)
+        for _ in range(3):
+            lv.apply(o, u)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.reps):
+            lv.apply(o, u)
+        b.record()
+        torch.cuda.synchronize()
+        us = a.elapsed_time(b) / args.reps * 1e3
+        isz = 4 if lv.dtype == torch.float32 else 8
+        gbs = apply_bytes(dims, isz) / (us * 1e-6) / 1e9
+        out["f32" if isz == 4 else "f64"] = {"us_per_apply": us, "GBps": gbs, "frac_of_peak": gbs / peaks()[0]}
+    ge.check_device()
+    print(json.dumps({"micro": "fine K*u apply", "dims": list(dims), "reps": args.reps, **out}))
+    return 0
+
+
 def main():
     args = parse()
     sys.path.insert(0, ROOT)
+    if args.micro == "apply":
+        return run_micro_apply(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

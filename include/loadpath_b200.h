@@ -103,7 +103,6 @@ int lpb_coarse_dense_f32(double* a, int kind, const float* w, const float* mcat,
 int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_coarse_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_coarse_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
-
 /* ---- V-cycle vector passes (loadpath/mgops.py:312-343) and damped Jacobi */
 int lpb_cheb_start_f32(const float* b, const float* dinv, float s, float* x, float* r, float* d, long long n, void* stream);
 int lpb_cheb_start_f64(const double* b, const double* dinv, double s, double* x, double* r, double* d, long long n, void* stream);
@@ -124,6 +123,10 @@ int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const ui
  * :872-926). Reductions are deterministic: part needs lpb_reduce_blocks() doubles; results land
  * in device memory. alpha / beta are read as *num / *den on the device. */
 int lpb_reduce_blocks(void);
+/* record a CUDA event on a stream; inside a stream capture it is recorded with
+ * cudaEventRecordExternal, so it becomes a graph node that every replay repeats (kernel timing
+ * inside CUDA graphs) */
+int lpb_event_record(void* event, void* stream);
 int lpb_dot_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream);
 int lpb_dot_f32(const float* a, const float* b, long long n, double* part, double* out, void* stream);
 int lpb_dot_f64_f32(const double* a, const float* b, long long n, double* part, double* out, void* stream);
@@ -151,6 +154,20 @@ int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const dou
 /* volumes[j] of the clipped OC step at nl = 31 multipliers lam[j] (device), weights gv = H (1 / hs) */
 int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv, const double* lam, int nl, double move, double* part, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* dv, double lam, double move, double* part, double* change, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+/* ---- CUDA graphs of a stream's work (the solver records one CG iteration per solve) */
+int lpb_capture_begin(void* stream);
+int lpb_capture_end(void* stream, void** exec);
+int lpb_graph_launch(void* exec, void* stream);
+int lpb_graph_free(void* exec);
+int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
+
+/* ---- coarsest level: inverse of the dense SPD operator in place (cuSOLVER potrf + potri, then
+ * the triangle mirrored); info: two device ints (factorization, inversion), nonzero when the
+ * matrix is not positive definite (the reference then rebuilds the hierarchy strict,
+ * loadpath/mg.py:580-586) */
+long long lpb_coarse_inverse_work(int n);
+int lpb_coarse_inverse(double* a, int n, double* work, long long lwork, int* info, void* stream);
 
 #ifdef __cplusplus
 }

@@ -45,7 +45,7 @@ def parse_header(path: str = HEADER):
     text = open(path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     out = []
-    for m in re.finditer(r"\b(int|void)\s+(lpb_\w+)\s*\(([^)]*)\)\s*;", text):
+    for m in re.finditer(r"\b(int|void|long long)\s+(lpb_\w+)\s*\(([^)]*)\)\s*;", text):
         ret, name, args = m.group(1), m.group(2), m.group(3).strip()
         types = []
         if args and args != "void":

@@ -368,37 +368,45 @@ k_weights_march(T* __restrict__ out, const T* __restrict__ u, const T* __restric
 }
 
 // patch cells (weights zero, an explicit masked matrix): out += m * sum of their rows times
-// u, node by node over the box of nodes they touch; runs after k_weights_march
+// u, node by node over the box of nodes they touch (one warp per node: the lanes split the
+// 8 cells x 24 columns); runs after k_weights_march
 template <typename T>
 __global__ void k_patch_add(T* __restrict__ out, const T* __restrict__ u, const int* __restrict__ pid,
                             const T* __restrict__ pk, const uint8_t* __restrict__ mask, LpGrid g, int bx0, int by0,
                             int bz0, int bnx, int bny, int bnz) {
   const long long total = (long long)bnx * bny * bnz;
   const long long cs = g.comp_stride();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int z = bz0 + (int)(t % bnz);
-    const long long q = t / bnz;
-    const int y = by0 + (int)(q % bny), x = bx0 + (int)(q / bny);
-    T a[3] = {T(0), T(0), T(0)};
-    bool any = false;
-    for (int kk = 0; kk < 8; ++kk) {
-      const int cx = x - cx_(kk), cy = y - cy_(kk), cz = z - cz_(kk);
-      if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
-      const int p = pid[g.cell(cx, cy, cz)];
-      if (p < 0) continue;
-      any = true;
-      const T* kp = pk + (long long)p * 576;
-      for (int q2 = 0; q2 < 8; ++q2) {
-        const long long n2 = g.node(cx + cx_(q2), cy + cy_(q2), cz + cz_(q2));
-        for (int c2 = 0; c2 < 3; ++c2) {
-          const T uv = u[c2 * cs + n2];
-          for (int cc = 0; cc < 3; ++cc) a[cc] += kp[(3 * kk + cc) * 24 + 3 * q2 + c2] * uv;
-        }
-      }
+  const int lane = threadIdx.x & 31;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (warp >= total) return;
+  const int z = bz0 + (int)(warp % bnz);
+  const long long q = warp / bnz;
+  const int y = by0 + (int)(q % bny), x = bx0 + (int)(q / bny);
+  // lane -> (cell corner kk = lane / 4, column block of 6 = lane % 4)
+  const int kk = lane >> 2, cb = lane & 3;
+  T a[3] = {T(0), T(0), T(0)};
+  const int cx = x - cx_(kk), cy = y - cy_(kk), cz = z - cz_(kk);
+  int p = -1;
+  if (cx >= 0 && cy >= 0 && cz >= 0 && cx < g.nx && cy < g.ny && cz < g.nz) p = pid[g.cell(cx, cy, cz)];
+  if (p >= 0) {
+    const T* kp = pk + (long long)p * 576;
+#pragma unroll
+    for (int c6 = 0; c6 < 6; ++c6) {
+      const int col = 6 * cb + c6, q2 = col / 3, c2 = col % 3;
+      const T uv = u[c2 * cs + g.node(cx + cx_(q2), cy + cy_(q2), cz + cz_(q2))];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) a[cc] += kp[(3 * kk + cc) * 24 + col] * uv;
     }
-    if (!any) continue;
+  }
+  const unsigned any = __ballot_sync(0xffffffffu, p >= 0);
+  if (!any) return;
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+    for (int o = 16; o > 0; o >>= 1) a[cc] += __shfl_down_sync(0xffffffffu, a[cc], o);
+  if (lane == 0) {
     const long long n = g.node(x, y, z);
     const uint8_t mb = mask[n];
+#pragma unroll
     for (int cc = 0; cc < 3; ++cc)
       if ((mb >> cc) & 1) out[cc * cs + n] += a[cc];
   }
@@ -524,8 +532,8 @@ static int launch_weights(T* out, const T* u, const T* w, const int* pid, const 
   k_weights_march<T><<<grid, TXC * TYC, 0, st>>>(out, u, w, mask, gc, g, best, nchunks);
   if (pid && pk && pbox && pbox[3] > 0 && pbox[4] > 0 && pbox[5] > 0) {
     const long long nb = (long long)pbox[3] * pbox[4] * pbox[5];
-    k_patch_add<T><<<lp_blocks(nb, 128), 128, 0, st>>>(out, u, pid, pk, mask, g, pbox[0], pbox[1], pbox[2], pbox[3],
-                                                       pbox[4], pbox[5]);
+    k_patch_add<T><<<lp_blocks(nb * 32, 256), 256, 0, st>>>(out, u, pid, pk, mask, g, pbox[0], pbox[1], pbox[2],
+                                                            pbox[3], pbox[4], pbox[5]);
   }
   LP_LAUNCH_CHECK();
   return LP_OK;

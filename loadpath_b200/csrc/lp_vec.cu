@@ -169,7 +169,9 @@ __global__ void k_restrict_residual(T* __restrict__ rc, const T* __restrict__ b,
   }
 }
 
-// x += prolong(xc * cm)[fine nodes] * m, one fine node per thread (loadpath/mgops.py:714-750)
+// x += prolong(xc * cm)[fine nodes] * m, one fine node per thread (loadpath/mgops.py:714-750).
+// Every node reads the 2 x 2 x 2 coarse corners around it; on an even coordinate the two
+// taps of that axis coincide and the second gets weight zero, so the loop has no branches.
 template <typename T>
 __global__ void k_prolong_add(T* __restrict__ x, const T* __restrict__ xc, const uint8_t* __restrict__ cm,
                               const uint8_t* __restrict__ m, LpGrid gf, LpGrid gc) {
@@ -178,32 +180,37 @@ __global__ void k_prolong_add(T* __restrict__ x, const T* __restrict__ xc, const
   const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % FZ);
-    long long q = t / FZ;
-    int y = (int)(q % FY);
-    int xx = (int)(q / FY);
-    long long fn = gf.node(xx, y, z);
-    uint8_t mb = m[fn];
+    const int z = (int)(t % FZ);
+    const long long q = t / FZ;
+    const int y = (int)(q % FY);
+    const int xx = (int)(q / FY);
+    const long long fn = gf.node(xx, y, z);
+    const uint8_t mb = m[fn];
     if ((mb & 7) == 0) continue;
-    int x0 = xx >> 1, y0 = y >> 1, z0 = z >> 1;
-    int nxo = (xx & 1) + 1, nyo = (y & 1) + 1, nzo = (z & 1) + 1;
-    T w = T(1);
-    if (xx & 1) w *= T(0.5);
-    if (y & 1) w *= T(0.5);
-    if (z & 1) w *= T(0.5);
+    const int x0 = xx >> 1, y0 = y >> 1, z0 = z >> 1;
+    const int ox = xx & 1, oy = y & 1, oz = z & 1;
+    const T wx[2] = {ox ? T(0.5) : T(1), ox ? T(0.5) : T(0)};
+    const T wy[2] = {oy ? T(0.5) : T(1), oy ? T(0.5) : T(0)};
+    const T wz[2] = {oz ? T(0.5) : T(1), oz ? T(0.5) : T(0)};
     T acc[3] = {T(0), T(0), T(0)};
-    for (int a = 0; a < nxo; ++a)
-      for (int bb = 0; bb < nyo; ++bb)
-        for (int e = 0; e < nzo; ++e) {
-          long long cn = gc.node(x0 + a, y0 + bb, z0 + e);
-          uint8_t cmb = cm[cn];
 #pragma unroll
-          for (int i = 0; i < 3; ++i)
-            if ((cmb >> i) & 1) acc[i] += xc[i * ccs + cn];
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const long long cn = gc.node(x0 + a * ox, y0 + bb * oy, z0 + e * oz);
+          const uint8_t cmb = cm[cn];
+          const T w = wx[a] * wy[bb] * wz[e];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            const T v = ((cmb >> i) & 1) ? xc[i * ccs + cn] : T(0);
+            acc[i] += w * v;
+          }
         }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-      if ((mb >> i) & 1) x[i * fcs + fn] += acc[i] * w;
+      if ((mb >> i) & 1) x[i * fcs + fn] += acc[i];
   }
 }
 
@@ -251,6 +258,18 @@ __global__ void k_dinv_mask(T* __restrict__ av, const T* __restrict__ dinv, cons
 extern "C" {
 
 int lpb_reduce_blocks(void) { return LP_RED_BLOCKS; }
+
+// record a CUDA event on a stream; inside a stream capture it becomes an event-record node, so
+// every replay of the graph records it again (for timing kernels inside graphs)
+int lpb_event_record(void* event, void* stream) {
+  if (!event) return LP_ERR_ARG;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(LP_ST, &cs) != cudaSuccess) return LP_ERR_LAUNCH;
+  const cudaError_t e = cs == cudaStreamCaptureStatusActive
+                            ? cudaEventRecordWithFlags((cudaEvent_t)event, LP_ST, cudaEventRecordExternal)
+                            : cudaEventRecord((cudaEvent_t)event, LP_ST);
+  return e == cudaSuccess ? LP_OK : LP_ERR_LAUNCH;
+}
 
 int lpb_dot_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream) {
   if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;

@@ -22,6 +22,7 @@ outer CG, its operator, residual and inner products always in float64.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -59,19 +60,48 @@ class BoxMesh:
 
 
 class FineApplyProbe:
-    """CUDA events around every fine-level tiled apply while set (bench.py's roofline)."""
+    """CUDA events around every fine-level tiled apply while set (bench.py's roofline).
 
-    def __init__(self):
-        self.events = []
+    The events are recorded as external event nodes, so inside a CUDA graph every replay
+    records them again; the solver hands the pairs of a replay back (harvest) once that replay
+    is known to be complete."""
+
+    def __init__(self, n=512):
+        self.pending = []        # eager launches, read at summary()
+        self.capture = None      # pairs recorded while a graph is being captured
+        self.totals = {"f32_ms": 0.0, "f32_count": 0, "f64_ms": 0.0, "f64_count": 0}
+        self.pool = []
+        self._grow(n)
+
+    def _grow(self, n):
+        # torch creates a CUDA event at its first record: record each once here, outside any
+        # capture, so the raw handles exist
+        for _ in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            b.record()
+            self.pool.append((a, b))
+
+    def take(self):
+        if not self.pool:
+            if torch.cuda.is_current_stream_capturing():
+                raise RuntimeError("fine-apply probe: event pool exhausted during a graph capture")
+            self._grow(256)
+        return self.pool.pop()
+
+    def harvest(self, pairs, recycle=False):
+        for dt, a, b in pairs:
+            k = "f32" if dt == torch.float32 else "f64"
+            self.totals[k + "_ms"] += a.elapsed_time(b)
+            self.totals[k + "_count"] += 1
+            if recycle:
+                self.pool.append((a, b))
 
     def summary(self):
         torch.cuda.synchronize()
-        out = {"f32_ms": 0.0, "f32_count": 0, "f64_ms": 0.0, "f64_count": 0}
-        for dt, a, b in self.events:
-            k = "f32" if dt == torch.float32 else "f64"
-            out[k + "_ms"] += a.elapsed_time(b)
-            out[k + "_count"] += 1
-        return out
+        self.harvest(self.pending, recycle=True)
+        self.pending = []
+        return dict(self.totals)
 
 
 _PROBE = [None]
@@ -124,14 +154,17 @@ class DevLevel:
             if fine_kernel and not mask_in:
                 probe = _PROBE[0]
                 if probe is not None:
-                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    a.record()
+                    a, b = probe.take()
+                    L.lpb_event_record(a.cuda_event, st)
                 getattr(L, f"lpb_apply_fine_{sfx}")(out.data_ptr(), u.data_ptr(), self.e.data_ptr(),
                                                      self.mask.data_ptr(), self.kmodal.ctypes.data,
                                                      self.err.data_ptr(), *g.args, st)
                 if probe is not None:
-                    b.record()
-                    probe.events.append((self.dtype, a, b))
+                    L.lpb_event_record(b.cuda_event, st)
+                    if probe.capture is not None:
+                        probe.capture.append((self.dtype, a, b))
+                    else:
+                        probe.pending.append((self.dtype, a, b))
             else:
                 getattr(L, f"lpb_apply_scaled_{sfx}")(out.data_ptr(), u.data_ptr(), self.e.data_ptr(),
                                                        self.mask.data_ptr(), self.ke.data_ptr(), *g.args,
@@ -240,6 +273,10 @@ class GridElasticity:
         self._host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
         self._work = {}
         self._e_dev = None
+        # CUDA graphs for the CG iteration (captured once per solve)
+        self.use_graphs = True
+        self._graphs = None
+        self._cap_stream = torch.cuda.Stream(device=self.device)
 
     # --- layout conversion (loadpath/mg.py:495-511) -----------------------------------
     def to_grid(self, v, dtype=np.float64):
@@ -261,6 +298,13 @@ class GridElasticity:
         return g
 
     # --- device work buffers -----------------------------------------------------------
+    def _flat_buf(self, key, n, dtype):
+        t = self._work.get(key)
+        if t is None or t.dtype != dtype or t.numel() < n:
+            t = torch.zeros(max(n, 1), dtype=dtype, device=self.device)
+            self._work[key] = t
+        return t
+
     def _buf(self, key, grid: DevGrid, dtype):
         t = self._work.get(key)
         if t is None or t.dtype != dtype or tuple(t.shape) != (3, grid.NX, grid.NY, grid.pz):
@@ -441,15 +485,15 @@ class GridElasticity:
         else:
             getattr(L, f"lpb_coarse_dense_{sfx}")(a.data_ptr(), 2, None, None, None, None, lv.k.data_ptr(),
                                                   lv.mask.data_ptr(), *g.args, st)
-        # SPD factor on the device (cuSOLVER through torch, once per hierarchy); the V-cycle
-        # then applies the inverse with this package's dense kernel
-        chol, info = torch.linalg.cholesky_ex(a)
-        if int(info.item()) != 0:
+        # the dense inverse on the device, once per hierarchy (cuSOLVER potrf + potri); the
+        # V-cycle applies it with this package's GEMV kernel
+        lw = int(L.lpb_coarse_inverse_work(n))
+        work = self._flat_buf("coarse_work", lw, torch.float64)
+        info = self._flat_buf("coarse_info", 2, torch.int32)
+        L.lpb_coarse_inverse(a.data_ptr(), n, work.data_ptr(), lw, info.data_ptr(), st)
+        if bool((info[:2] != 0).any().item()):
             return False
-        ainv = torch.cholesky_inverse(chol)
-        self._coarse = {"ainv": ainv.contiguous(), "v": torch.zeros(n, dtype=torch.float64, device=self.device),
-                        "n": n}
-        del a, chol
+        self._coarse = {"ainv": a, "v": torch.zeros(n, dtype=torch.float64, device=self.device), "n": n}
         return True
 
     def _op(self, i):
@@ -629,37 +673,88 @@ class GridElasticity:
             x.zero_()
         self.precondition_device(r, z)
         p.copy_(z)
-        rz_slot, rzn_slot = 1, 2
-        self._dot64(r, z, rz_slot)
+        self._dot64(r, z, 1)
         tol = self.rtol * bnorm
         r32 = self._buf("cg_r32", g, torch.float32) if self.tdtype == torch.float32 else None
         host = self._host
-        ev = torch.cuda.Event()
-        for it in range(1, self.maxiter + 1):
+
+        def head():
+            # ap = A p; pap; x += alpha p; r -= alpha ap (and its float32 copy); |r|^2; scalars out
             a.apply(ap, p)
             self._dot64(p, ap, 3)
             L.lpb_cg_step(x.data_ptr(), r.data_ptr(), p.data_ptr(), ap.data_ptr(), ptr(r32), n,
-                          sc[rz_slot].data_ptr(), sc[3].data_ptr(), self._part.data_ptr(), sc[4].data_ptr(), st)
-            host[:2].copy_(sc[3:5], non_blocking=True)
+                          sc[1].data_ptr(), sc[3].data_ptr(), self._part.data_ptr(), sc[4].data_ptr(),
+                          stream_handle())
+            L.lpb_memcpy_async(host.data_ptr(), sc[3:5].data_ptr(), 16, stream_handle())
+
+        def tail():
+            # z = V(r); rz_new; p = z + (rz_new / rz) p; rz = rz_new
+            if r32 is not None:
+                xv = self._vcycle(0, r32)
+                L.lpb_dot_f64_f32(r.data_ptr(), xv.data_ptr(), n, self._part.data_ptr(), sc[2].data_ptr(),
+                                  stream_handle())
+                L.lpb_xpby_f32(p.data_ptr(), xv.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), stream_handle())
+            else:
+                self.precondition_device(r, z)
+                self._dot64(r, z, 2)
+                L.lpb_xpby_f64(p.data_ptr(), z.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), stream_handle())
+            L.lpb_memcpy_async(sc[1:2].data_ptr(), sc[2:3].data_ptr(), 8, stream_handle())
+
+        graphs = None
+        probe = _PROBE[0]
+        gpairs = [[], []]
+        if self.use_graphs and self.maxiter > 1:
+            # one capture per solve: buffers and smoother coefficients are fixed within it
+            self._free_graphs()
+            graphs = []
+            # captured on a side stream (the legacy default stream cannot be captured), launched
+            # on the working stream
+            for gi, fn in enumerate((head, tail)):
+                if probe is not None:
+                    probe.capture = gpairs[gi]
+                with torch.cuda.stream(self._cap_stream):
+                    st0 = stream_handle()
+                    L.lpb_capture_begin(st0)
+                    try:
+                        fn()
+                    finally:
+                        exec_ = ctypes.c_void_p()
+                        L.lpb_capture_end(st0, ctypes.byref(exec_))
+                        if probe is not None:
+                            probe.capture = None
+                graphs.append(exec_)
+            self._graphs = graphs      # freed at the next capture
+        ev = torch.cuda.Event()
+
+        def finish(result):
+            if graphs is not None and probe is not None:
+                torch.cuda.current_stream().synchronize()
+                probe.harvest(gpairs[1])          # the last (speculative) tail replay
+            return result
+
+        for it in range(1, self.maxiter + 1):
+            if graphs is not None:
+                L.lpb_graph_launch(graphs[0], stream_handle())
+            else:
+                head()
             ev.record()
             # the next preconditioner step is queued before the host looks at |r|: the
             # device never waits on the convergence test (a converged solve discards it)
-            if r32 is not None:
-                xv = self._vcycle(0, r32)
-                L.lpb_dot_f64_f32(r.data_ptr(), xv.data_ptr(), n, self._part.data_ptr(), sc[rzn_slot].data_ptr(), st)
-                L.lpb_xpby_f32(p.data_ptr(), xv.data_ptr(), n, sc[rzn_slot].data_ptr(), sc[rz_slot].data_ptr(), st)
+            if graphs is not None:
+                L.lpb_graph_launch(graphs[1], stream_handle())
             else:
-                self.precondition_device(r, z)
-                self._dot64(r, z, rzn_slot)
-                L.lpb_xpby_f64(p.data_ptr(), z.data_ptr(), n, sc[rzn_slot].data_ptr(), sc[rz_slot].data_ptr(), st)
+                tail()
             ev.synchronize()
+            if graphs is not None and probe is not None:
+                # this head replay is complete and the next is not launched yet; a tail replay
+                # may be re-recording its events now, so tails are read once, at the end
+                probe.harvest(gpairs[0])
             pap, rr = float(host[0]), float(host[1])
             if not pap > 0:
-                return x, it, False
+                return finish((x, it, False))
             if math.sqrt(rr) <= tol:
-                return x, it, True
-            rz_slot, rzn_slot = rzn_slot, rz_slot
-        return x, self.maxiter, False
+                return finish((x, it, True))
+        return finish((x, self.maxiter, False))
 
     def _solve_device(self, b, x0):
         """One right-hand side with the strict fallback (loadpath/mg.py:951-965)."""
@@ -748,6 +843,19 @@ class GridElasticity:
         ud = g.nodes_to_dev(self.to_grid(u), torch.float64)
         se = g.cells_to_host(self.strain_energy_device(ud))
         return se[tuple(self.elem_ijk.T)]
+
+    def _free_graphs(self):
+        if self._graphs:
+            torch.cuda.current_stream().synchronize()
+            for gexec in self._graphs:
+                lib().lpb_graph_free(gexec)
+        self._graphs = None
+
+    def __del__(self):
+        try:
+            self._free_graphs()
+        except Exception:
+            pass
 
     def check_device(self):
         """Raise if a tiled fine-apply launch flagged a shared-memory wait that gave up."""

@@ -152,6 +152,7 @@ class Top3dLoop:
         self._vols = torch.zeros(31, dtype=torch.float64, device=g.device)
         self.loop = 0
         self.history = []
+        self.timing = None       # a list to collect per-phase CUDA events into, or None
         lib().lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, stream_handle())
 
     # ---- one iteration -------------------------------------------------------------------
@@ -215,9 +216,24 @@ class Top3dLoop:
         """One iteration; returns (compliance, change) as top3d reports them."""
         g = self.grid
         self.loop += 1
-        self.solve()
-        self.sensitivities()
-        self.oc()
+        t = self.timing
+        if t is not None:
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            ev[0].record()
+            self.ge.set_moduli_device(self.e)
+            ev[1].record()
+            x0 = self.u if (self.warm_start and self.u is not None) else None
+            self.u = self.ge.solve_device(self.f, x0)
+            ev[2].record()
+            self.sensitivities()
+            ev[3].record()
+            self.oc()
+            ev[4].record()
+            t.append(ev)
+        else:
+            self.solve()
+            self.sensitivities()
+            self.oc()
         # xphys = H xnew / hs, and the next iteration's moduli
         self.filter.apply(self.xphys, self.xnew, hs_out=self.filter.hs, e_out=self.e, penal=self.penal,
                           emin=self.emin)
