@@ -78,12 +78,24 @@ int lpb_diag_weights_f64(double* d, const double* w, const double* mcat, const i
 int lpb_diag_explicit_f32(double* d, const float* k, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_diag_explicit_f64(double* d, const double* k, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
-/* ---- masks and inverse diagonal (loadpath/mg.py:537-550, :575-576): alive = d > alive_thr,
+/* ---- masks and inverse diagonal (loadpath/mg.py:537-550, :560-576): alive = d > alive_thr,
  * solved = d > live_thr and not held (held_bits may be NULL) and, when kept != NULL, kept >= 1;
- * dinv = solved ? 1/d : 1 (either dinv pointer may be NULL). */
-int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, const uint8_t* held_bits, const float* kept, int nx, int ny, int nz, int pz, int cpz, double alive_thr, double live_thr, void* stream);
+ * dinv = solved ? 1/d : 1 (either dinv pointer may be NULL). With thr_scale != NULL (a device
+ * scalar, e.g. the level's largest diagonal from lpb_max_f64) both thresholds are multiplied by
+ * max(*thr_scale, 1e-300) on the device. */
+int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, const uint8_t* held_bits, const float* kept, int nx, int ny, int nz, int pz, int cpz, double alive_thr, double live_thr, const double* thr_scale, void* stream);
 /* *out = max(a[0:n]); part: >= 1024 doubles of scratch (loadpath/mg.py:560) */
 int lpb_max_f64(const double* a, long long n, double* part, double* out, void* stream);
+/* counts into a device float64 scalar (exact), part: >= 592 doubles of scratch. Cells with
+ * modulus > 0 (loadpath/mg.py:559), active cells of a level-1 (weights) or explicit level
+ * (loadpath/mg.py:593-599: _active_cells), and positions where two byte arrays differ (the
+ * hierarchy's reuse check: patch flags of a rebuild against the last build's). */
+int lpb_count_positive_f64(const double* e, long long n, double* part, double* out, void* stream);
+int lpb_count_active_weights_f32(const float* w, const int* patch_id, int nx, int ny, int nz, int pz, int cpz, double* part, double* out, void* stream);
+int lpb_count_active_weights_f64(const double* w, const int* patch_id, int nx, int ny, int nz, int pz, int cpz, double* part, double* out, void* stream);
+int lpb_count_active_explicit_f32(const float* k, int nx, int ny, int nz, int pz, int cpz, double* part, double* out, void* stream);
+int lpb_count_active_explicit_f64(const double* k, int nx, int ny, int nz, int pz, int cpz, double* part, double* out, void* stream);
+int lpb_count_ne_u8(const uint8_t* a, const uint8_t* b, long long n, double* part, double* out, void* stream);
 
 /* ---- Galerkin coarsening (loadpath/mg.py:601-677) */
 int lpb_weights_from_e_f64_f32(float* w, const double* e, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
@@ -98,18 +110,41 @@ int lpb_strict_held_kept(uint8_t* held_c, float* kept, const uint8_t* held_f, co
 int lpb_held0(uint8_t* held, const uint8_t* mask0, const uint8_t* fixed_bits, long long n, void* stream);
 
 /* ---- coarsest level (loadpath/mg.py:708-766): dense D K D + (I - D), symmetrised, over all
- * nodes of the level (n = 3 * nodes <= 40000); solve by a dense inverse the caller forms */
+ * nodes of the level, dof (c, node) -> c * nodes + node (a check of the band path below) */
 int lpb_coarse_dense_f32(double* a, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
-int lpb_coarse_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
-int lpb_coarse_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
-/* ---- V-cycle vector passes (loadpath/mgops.py:312-343) and damped Jacobi */
-int lpb_cheb_start_f32(const float* b, const float* dinv, float s, float* x, float* r, float* d, long long n, void* stream);
-int lpb_cheb_start_f64(const double* b, const double* dinv, double s, double* x, double* r, double* d, long long n, void* stream);
-int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, float s, float* r, float* d, long long n, void* stream);
-int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, double s, double* r, double* d, long long n, void* stream);
-int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, float c1, float c2, int last, long long n, void* stream);
-int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, double c1, double c2, int last, long long n, void* stream);
+/* ---- coarsest level as a band (loadpath/mg.py:708-766; the reference factors the same
+ * operator with SuperLU on the host). Dofs numbered 3 * node + component with the longest
+ * axis slowest, half-bandwidth bw = 3 (N1 N2 + N2 + 1) + 2 (N1 >= N2 the shorter node extents);
+ * the lower band is stored as 32 x 32 tiles, tile (R, d) = rows 32R.., columns 32(R-d)..,
+ * row-major at t + (R (D + 1) + d) * 1024, padding dofs past n as identity rows.
+ * lpb_band_dims: out = {n, nt, D, bw}, returns the tile count nt (D + 1).
+ * lpb_band_factor: in-place tiled Cholesky (one cooperative launch; bounded grid barrier);
+ *   linv: nt * 1024 doubles; info: 0 or the 1-based band dof of the first non-positive pivot;
+ *   bar: 64 device words of scratch; err: set when a barrier wait gave up.
+ * lpb_band_inverse: ainv (32 nt x 32 nt, row-major, band numbering) = A^-1 from the factor.
+ * lpb_band_solve_*: f_out = A^-1 f_in through the band numbering; v: 32 nt doubles scratch. */
+int lpb_coarse_band_f32(double* t, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_coarse_band_f64(double* t, int kind, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+long long lpb_band_dims(int nx, int ny, int nz, long long* out);
+int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_inverse(double* ainv, const double* t, const double* linv, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
+/* ---- Chebyshev smoother (loadpath/mg.py:771-821, loadpath/mgops.py:312-343) with its
+ * coefficients in device memory: lpb_cheb_coef turns the power iteration's dots (vv[k] = |v|^2
+ * before step k, vav[k] = v.D^-1 A v after it) into coef[0] = lmax (safety * max(vav[its-1],
+ * 1e-12), or 2 when some vv[k] == 0), coef[1] = 1/theta, coef[2+2k], coef[3+2k] = the two
+ * update coefficients of step k; degree <= 7 (16 doubles). The passes read coef on the device,
+ * so no smoother step needs lmax on the host. */
+int lpb_cheb_coef(double* coef, const double* vv, const double* vav, int its, int degree, double safety, void* stream);
+int lpb_cheb_start_f32(const float* b, const float* dinv, const double* coef, float* x, float* r, float* d, long long n, void* stream);
+int lpb_cheb_start_f64(const double* b, const double* dinv, const double* coef, double* x, double* r, double* d, long long n, void* stream);
+int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, const double* coef, float* r, float* d, long long n, void* stream);
+int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, const double* coef, double* r, double* d, long long n, void* stream);
+int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, const double* coef, int step, int last, long long n, void* stream);
+int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, const double* coef, int step, int last, long long n, void* stream);
 int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero, long long n, void* stream);
 int lpb_jacobi_f64(double* x, const double* b, const double* ax, const double* dinv, double omega, int from_zero, long long n, void* stream);
 
@@ -133,6 +168,11 @@ int lpb_dot_f64_f32(const double* a, const float* b, long long n, double* part, 
 int lpb_cg_step(double* x, double* r, const double* p, const double* ap, float* r32, long long n, const double* num, const double* den, double* part, double* rr, void* stream);
 int lpb_xpby_f32(double* p, const float* z, long long n, const double* num, const double* den, void* stream);
 int lpb_xpby_f64(double* p, const double* z, long long n, const double* num, const double* den, void* stream);
+/* warm start of the PCG on the device (loadpath/mg.py:878-895); sc holds [0] b.b, [5] x.Ax,
+ * [6] b.x, [7] |rs|^2 and s = b.x / x.Ax (0 unless x.Ax > 0). lpb_warm_residual: rs = b - s Ax;
+ * lpb_warm_select: x = s x, r = rs when s > 0 and |rs| < |b|, else x = 0, r = b. */
+int lpb_warm_residual(double* rs, const double* b, const double* ax, const double* sc, long long n, void* stream);
+int lpb_warm_select(double* x, double* r, const double* b, const double* rs, const double* sc, long long n, void* stream);
 int lpb_axpby_f64(double* out, double a, const double* x, double b, const double* y, long long n, void* stream);
 int lpb_axpby_f32(float* out, float a, const float* x, float b, const float* y, long long n, void* stream);
 int lpb_cast_f64_f32(float* out, const double* a, long long n, void* stream);
@@ -161,13 +201,12 @@ int lpb_capture_end(void* stream, void** exec);
 int lpb_graph_launch(void* exec, void* stream);
 int lpb_graph_free(void* exec);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
+int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 
 /* ---- coarsest level: inverse of the dense SPD operator in place (cuSOLVER potrf + potri, then
  * the triangle mirrored); info: two device ints (factorization, inversion), nonzero when the
  * matrix is not positive definite (the reference then rebuilds the hierarchy strict,
  * loadpath/mg.py:580-586) */
-long long lpb_coarse_inverse_work(int n);
-int lpb_coarse_inverse(double* a, int n, double* work, long long lwork, int* info, void* stream);
 
 #ifdef __cplusplus
 }

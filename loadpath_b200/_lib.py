@@ -24,16 +24,26 @@ _CTYPES = {
 }
 _STATUS = {-1: "bad arguments", -2: "kernel launch failed", -3: "size beyond the kernel's limit"}
 # kernels each entry point launches (1 when not listed; 0 for host-only entries)
-_KERNELS = {"lpb_modal_ke": 0, "lpb_reduce_blocks": 0, "lpb_max_f64": 2, "lpb_dot_f64": 2, "lpb_dot_f32": 2,
-            "lpb_dot_f64_f32": 2, "lpb_cg_step": 2, "lpb_coarse_solve_f32": 2, "lpb_coarse_solve_f64": 2,
-            "lpb_oc_volumes": 2, "lpb_oc_apply": 2}
+_KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_max_f64": 2, "lpb_dot_f64": 2,
+            "lpb_dot_f32": 2, "lpb_dot_f64_f32": 2, "lpb_cg_step": 2, "lpb_oc_volumes": 2, "lpb_oc_apply": 2,
+            "lpb_band_dims": 0, "lpb_band_inverse": 2, "lpb_band_solve_f32": 2, "lpb_band_solve_f64": 2,
+            "lpb_count_positive_f64": 2, "lpb_count_active_weights_f32": 2, "lpb_count_active_weights_f64": 2,
+            "lpb_count_active_explicit_f32": 2, "lpb_count_active_explicit_f64": 2, "lpb_count_ne_u8": 2,
+            "lpb_memcpy_async": 0, "lpb_memset_async": 0, "lpb_event_record": 0, "lpb_capture_begin": 0,
+            "lpb_capture_end": 0, "lpb_graph_launch": 0, "lpb_graph_free": 0}
 _COUNT = [0]
 
 
 def launches() -> int:
     """Kernels launched through this binding so far (sensitivity with a compliance output counts
-    as 2)."""
+    as 2; a CUDA graph replay counts the kernels it holds, see add_launches)."""
     return _COUNT[0]
+
+
+def add_launches(n: int) -> None:
+    """Adjust the count: a graph capture subtracts the launches it recorded (they did not run)
+    and each replay of the graph adds them back."""
+    _COUNT[0] += n
 
 
 class LpError(RuntimeError):

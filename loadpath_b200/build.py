@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = LIB + ".tmp"
-    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcusolver"]
+    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -1,0 +1,440 @@
+// The coarsest level's direct solve (loadpath/mg.py:708-766: the reference factors D K D + (I - D)
+// with SuperLU on the host). Here the operator is a band (a 27-point block stencil whose nodes
+// are numbered longest axis slowest, half-bandwidth 3 (N1 N2 + N2 + 1) + 2 dofs), so:
+//   1. k_band_factor: Cholesky of the band stored as 32 x 32 tiles (tile (R, d) = rows 32R..,
+//      columns 32(R - d)..), right-looking by tile columns; one cooperative launch whose blocks
+//      meet at a bounded grid barrier twice per tile column. A tile column's diagonal block is
+//      factored (and its lower-triangular inverse formed) by one warp in registers.
+//   2. k_band_inverse: A^-1 = L^-T L^-1 applied to the identity, eight columns per block: a
+//      forward then a backward block substitution over the band tiles. Only the lower triangle
+//      is needed (rows >= the block's first column); k_sym_lower copies it across.
+//   3. per V-cycle: gather the level's field into the band numbering, one GEMV with the dense
+//      inverse, scatter back (the inverse stays resident; a GEMV has no sequential chain).
+// The factorisation costs O(n bw^2) instead of the dense O(n^3): at the 17 x 9 x 9-node coarsest
+// level of a 256 x 128 x 128 grid, n = 4131 and bw = 275.
+#include "lp_common.cuh"
+
+#define LP_BAR_LIMIT (1u << 22)   // polls before a grid-barrier wait gives up and flags an error
+
+namespace {
+
+__device__ __forceinline__ double* tile_at(double* t, const LpBand& bd, int R, int d) {
+  return t + ((long long)R * (bd.D + 1) + d) * 1024;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// bounded sense-counting barrier over all blocks of a cooperative launch; false when a wait
+// gave up (the caller stops and the error flag is set)
+__device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int* err) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned g = gen;
+    if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicExch(&bar[32], g + 1u);
+    } else {
+      unsigned it = 0;
+      while (ld_acquire(&bar[32]) == g) {
+        if (++it > LP_BAR_LIMIT) {
+          ok = 0;
+          atomicExch(err, 1);
+          break;
+        }
+        if (it > 64) __nanosleep(32);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  gen += 1u;
+  return ok_s != 0;
+}
+
+// Tiles another block wrote are read with ld.global.cg (L2, not a possibly stale L1 line).
+
+// Cholesky of one 32 x 32 diagonal tile (lower part read) by warp 0: lane i holds row i in
+// registers. Writes L (upper part zero) over the tile and L^-1 (row-major) to linv. A pivot
+// that is not positive records its dof (1-based) in *info; the arithmetic continues.
+__device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv, long long row0, int* info,
+                            double (*sm)[33]) {
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    double a[32];
+    int bad = 0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) a[m] = m <= i ? __ldcg(tile + i * 32 + m) : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const double p = __shfl_sync(0xffffffffu, a[j], j);
+      if (!(p > 0.0) && bad == 0) bad = (int)(row0 + j + 1);
+      const double d = sqrt(p), rd = 1.0 / d;
+      const double l = i > j ? a[j] * rd : (i == j ? d : 0.0);
+      a[j] = l;
+#pragma unroll
+      for (int t = j + 1; t < 32; ++t) {   // entries above the diagonal of row i take garbage
+        const double lt = __shfl_sync(0xffffffffu, l, t);   // here; a[t] is zeroed before use
+        a[t] -= l * lt;                                      // (l = 0 at pivot t > i)
+      }
+    }
+    if (i == 0 && bad) atomicCAS(info, 0, bad);
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      const double v = m <= i ? a[m] : 0.0;
+      tile[i * 32 + m] = v;
+      sm[i][m] = v;
+    }
+    __syncwarp();
+    // lane c: column c of L^-1, right-looking (the 32 row updates of a step are independent)
+    const int c = i;
+    const double rd = 1.0 / sm[c][c];
+    double x[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) x[r] = r == c ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      const double xm = x[m] * __shfl_sync(0xffffffffu, rd, m);
+      x[m] = m >= c ? xm : 0.0;
+#pragma unroll
+      for (int r = m + 1; r < 32; ++r) x[r] -= sm[r][m] * x[m];
+    }
+#pragma unroll
+    for (int r = 0; r < 32; ++r) linv[r * 32 + c] = x[r];
+  }
+}
+
+// a (32 x 32 tile, global, in place) = a * li^T with li lower triangular (the panel solve
+// L_a = A_a L_kk^-T)
+__device__ void panel_tile(double* __restrict__ a, const double* __restrict__ li, double (*sa)[33],
+                           double (*sl)[33]) {
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    sa[e >> 5][e & 31] = __ldcg(a + e);
+    sl[e >> 5][e & 31] = __ldcg(li + e);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int r = e >> 5, c = e & 31;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; m += 4) {   // sl[c][m] = 0 for m > c (lower triangular)
+      s0 += sa[r][m] * sl[c][m];
+      s1 += sa[r][m + 1] * sl[c][m + 1];
+      s2 += sa[r][m + 2] * sl[c][m + 2];
+      s3 += sa[r][m + 3] * sl[c][m + 3];
+    }
+    a[e] = (s0 + s1) + (s2 + s3);
+  }
+  __syncthreads();
+}
+
+// x (32 x 32 tile, global, in place) -= la * lc^T
+__device__ void update_tile(double* __restrict__ x, const double* __restrict__ la, const double* __restrict__ lc,
+                            double (*sa)[33], double (*sl)[33]) {
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    sa[e >> 5][e & 31] = __ldcg(la + e);
+    sl[e >> 5][e & 31] = __ldcg(lc + e);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+    const int r = e >> 5, c = e & 31;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; m += 4) {
+      s0 += sa[r][m] * sl[c][m];
+      s1 += sa[r][m + 1] * sl[c][m + 1];
+      s2 += sa[r][m + 2] * sl[c][m + 2];
+      s3 += sa[r][m + 3] * sl[c][m + 3];
+    }
+    x[e] = __ldcg(x + e) - ((s0 + s1) + (s2 + s3));
+  }
+  __syncthreads();
+}
+
+// Right-looking tiled band Cholesky over tile columns k. Panel phase: tile (k + a, k),
+// a = 1..D, goes to block (a - 1) mod gridDim. Update phase: the D (D + 1) / 2 trailing tiles
+// (k + a, k + c), 1 <= c <= a <= D, numbered u = a (a - 1) / 2 + c - 1, go to block u mod gridDim;
+// block 0 (which owns u = 0, tile (k + 1, k + 1)) then factors that tile. bar: two zeroed words;
+// err: set when a barrier wait gave up.
+__global__ void __launch_bounds__(256, 1) k_band_factor(double* __restrict__ t, double* __restrict__ linv, LpBand bd,
+                                                        int* __restrict__ info, unsigned* __restrict__ bar,
+                                                        int* __restrict__ err) {
+  __shared__ double sa[32][33];
+  __shared__ double sl[32][33];
+  unsigned gen = 0;
+  const unsigned nb = gridDim.x;
+  const int b = blockIdx.x;
+  const int nu = bd.D * (bd.D + 1) / 2;
+  if (b == 0) factor_diag(tile_at(t, bd, 0, 0), linv, 0, info, sa);
+  if (!grid_barrier(bar, nb, gen, err)) return;
+  for (int k = 0; k + 1 < bd.nt; ++k) {
+    for (int a = 1 + b; a <= bd.D && k + a < bd.nt; a += nb)
+      panel_tile(tile_at(t, bd, k + a, a), linv + (long long)k * 1024, sa, sl);
+    if (!grid_barrier(bar, nb, gen, err)) return;
+    for (int u = b; u < nu; u += nb) {
+      int a = 1;
+      while ((a + 1) * a / 2 <= u) ++a;         // u in [a (a - 1) / 2, a (a + 1) / 2)
+      const int c = u - a * (a - 1) / 2 + 1;
+      if (k + a < bd.nt) update_tile(tile_at(t, bd, k + a, a - c), tile_at(t, bd, k + a, a), tile_at(t, bd, k + c, c), sa, sl);
+    }
+    if (b == 0) factor_diag(tile_at(t, bd, k + 1, 0), linv + (long long)(k + 1) * 1024, 32LL * (k + 1), info, sa);
+    if (!grid_barrier(bar, nb, gen, err)) return;
+  }
+}
+
+// FP64 tensor-core MMA, m8n8k4 (row-major A 8 x 4, column-major B 4 x 8, C/D 8 x 8). Lane l holds
+// A[l >> 2][l & 3], B[l & 3][l >> 2] and D[l >> 2][2 (l & 3) + i], i = 0, 1.
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Columns j0..j0+31 of A^-1 (rows >= the first column's tile row) into ainv (n_pad x n_pad,
+// row-major): Y = L^-1 E by forward substitution, then X = L^-T Y backwards, one tile row per
+// step. A step stages, in chunks of at most `chunk` pairs, its band tiles (8 KB each) with the
+// matching earlier result blocks (read back from ainv through L2) in shared memory; each of 16
+// warps forms one 8 x 8 block of the 32 x 32 result with FP64 MMAs:
+//   forward  S = E - sum_d T_(k,d) Y_(k-d),      Y_k = L_kk^-1 S
+//   backward S = Y_k - sum_d T_(k+d,d)^T X_(k+d), X_k = L_kk^-T S
+// Shared row strides of 36 doubles spread each MMA operand load over all banks.
+constexpr int INV_COLS = 32;
+constexpr int INV_LD = 36;
+constexpr int INV_TILE = 32 * INV_LD;   // doubles per staged 32 x 32 block
+
+__global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ainv, const double* __restrict__ t,
+                                                         const double* __restrict__ linv, LpBand bd, int chunk) {
+  extern __shared__ double sm_inv[];
+  double* tiles = sm_inv;                           // chunk band tiles
+  double* blks = sm_inv + (long long)chunk * INV_TILE;  // chunk result blocks
+  double* diag = blks + (long long)chunk * INV_TILE;    // L_kk^-1
+  double* tmp = diag + INV_TILE;                         // S
+  const int R1 = bd.D + 1;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int row0 = 8 * (w >> 2), col0 = 8 * (w & 3);
+  const int orow = row0 + g, ocol = col0 + 2 * q;   // this lane's two outputs: (orow, ocol + i)
+  const long long np = 32LL * bd.nt;
+  const int j0 = INV_COLS * blockIdx.x;
+  const int kb = j0 >> 5;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool fwd = pass == 0;
+    for (int step = 0; step < bd.nt - kb; ++step) {
+      const int k = fwd ? kb + step : bd.nt - 1 - step;
+      const int dm = fwd ? min(bd.D, k - kb) : min(bd.D, bd.nt - 1 - k);
+      double p0 = 0.0, p1 = 0.0, r0 = 0.0, r1 = 0.0;
+      for (int d0 = 1; d0 <= dm; d0 += chunk) {
+        const int nc = min(chunk, dm - d0 + 1);
+        for (int e = threadIdx.x; e < nc * 1024; e += blockDim.x) {
+          const int d = d0 + (e >> 10), rr = (e >> 5) & 31, cc = e & 31;
+          const long long tk = fwd ? k : k + d;   // band tile (tk, d)
+          const long long bk = fwd ? k - d : k + d;   // earlier result block
+          tiles[(e >> 10) * INV_TILE + rr * INV_LD + cc] = __ldg(t + (tk * R1 + d) * 1024 + rr * 32 + cc);
+          blks[(e >> 10) * INV_TILE + rr * INV_LD + cc] = __ldcg(ainv + (32 * bk + rr) * np + j0 + cc);
+        }
+        if (d0 == 1)
+          for (int e = threadIdx.x; e < 1024; e += blockDim.x)
+            diag[(e >> 5) * INV_LD + (e & 31)] = __ldg(linv + (long long)k * 1024 + e);
+        __syncthreads();
+        for (int c = 0; c < nc; ++c) {
+          const double* tc = tiles + c * INV_TILE;
+          const double* yb = blks + c * INV_TILE + q * INV_LD + col0 + g;
+          if (fwd) {
+            const double* ta = tc + (row0 + g) * INV_LD + q;
+#pragma unroll
+            for (int m = 0; m < 32; m += 8) {
+              dmma(p0, p1, ta[m], yb[m * INV_LD]);
+              dmma(r0, r1, ta[m + 4], yb[(m + 4) * INV_LD]);
+            }
+          } else {
+            const double* ta = tc + q * INV_LD + row0 + g;   // A[row][m] = T[m][row]
+#pragma unroll
+            for (int m = 0; m < 32; m += 8) {
+              dmma(p0, p1, ta[m * INV_LD], yb[m * INV_LD]);
+              dmma(r0, r1, ta[(m + 4) * INV_LD], yb[(m + 4) * INV_LD]);
+            }
+          }
+        }
+        __syncthreads();
+      }
+      if (dm == 0) {
+        for (int e = threadIdx.x; e < 1024; e += blockDim.x)
+          diag[(e >> 5) * INV_LD + (e & 31)] = __ldg(linv + (long long)k * 1024 + e);
+      }
+      double* out = ainv + (32LL * k + orow) * np + j0 + ocol;
+      if (fwd) {
+        const long long gr = 32LL * k + orow;
+        tmp[orow * INV_LD + ocol] = (gr == j0 + ocol ? 1.0 : 0.0) - (p0 + r0);
+        tmp[orow * INV_LD + ocol + 1] = (gr == j0 + ocol + 1 ? 1.0 : 0.0) - (p1 + r1);
+      } else {
+        const double2 yk = __ldcg(reinterpret_cast<const double2*>(out));
+        tmp[orow * INV_LD + ocol] = yk.x - (p0 + r0);
+        tmp[orow * INV_LD + ocol + 1] = yk.y - (p1 + r1);
+      }
+      __syncthreads();
+      double y0 = 0.0, y1 = 0.0;
+      if (fwd) {
+#pragma unroll
+        for (int m = 0; m < 32; m += 4)
+          dmma(y0, y1, diag[(row0 + g) * INV_LD + m + q], tmp[(m + q) * INV_LD + col0 + g]);
+      } else {
+#pragma unroll
+        for (int m = 0; m < 32; m += 4)   // A = L_kk^-T
+          dmma(y0, y1, diag[(m + q) * INV_LD + row0 + g], tmp[(m + q) * INV_LD + col0 + g]);
+      }
+      *reinterpret_cast<double2*>(out) = make_double2(y0, y1);
+      __syncthreads();
+    }
+  }
+}
+
+// a[i][j] = a[j][i] for i < j (copy the lower triangle onto the upper), 32 x 32 tiles via
+// shared memory; block (bi, bj) with bi <= bj writes tile (bi, bj)
+__global__ void k_sym_lower(double* __restrict__ a, long long np) {
+  __shared__ double s[32][33];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bi > bj) return;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+  for (int r = ty; r < 32; r += 8) s[r][tx] = a[(32LL * bj + r) * np + 32LL * bi + tx];   // tile (bj, bi)
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const long long i = 32LL * bi + r, j = 32LL * bj + tx;
+    if (i < j) a[i * np + j] = s[tx][r];
+  }
+}
+
+// v[i] = field at band dof i (0 past n)
+template <typename T>
+__global__ void k_field_to_band(double* __restrict__ v, const T* __restrict__ f, LpGrid g, LpBand bd) {
+  const long long np = 32LL * bd.nt;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < np; i += (long long)gridDim.x * blockDim.x) {
+    double x = 0.0;
+    if (i < bd.n) {
+      int nx_, ny_, nz_;
+      bd.coords(i / 3, nx_, ny_, nz_);
+      x = (double)f[(i % 3) * g.comp_stride() + g.node(nx_, ny_, nz_)];
+    }
+    v[i] = x;
+  }
+}
+
+// field at band dof i = row i of ainv . v, one warp per row
+template <typename T>
+__global__ void k_band_gemv_to_field(T* __restrict__ f, const double* __restrict__ a, const double* __restrict__ v,
+                                     LpGrid g, LpBand bd) {
+  const long long np = 32LL * bd.nt;
+  const int lane = threadIdx.x & 31;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (row >= bd.n) return;
+  const double* ar = a + row * np;
+  double s = 0.0;
+  for (long long j = lane; j < np; j += 32) s += ar[j] * v[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    int nx_, ny_, nz_;
+    bd.coords(row / 3, nx_, ny_, nz_);
+    f[(row % 3) * g.comp_stride() + g.node(nx_, ny_, nz_)] = (T)s;
+  }
+}
+
+template <typename T>
+int band_solve(T* f_out, const T* f_in, const double* ainv, double* v, LpGrid g, cudaStream_t st) {
+  if (!lp_grid_ok(g) || !f_out || !f_in || !ainv || !v) return LP_ERR_ARG;
+  const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  const long long np = 32LL * bd.nt;
+  k_field_to_band<T><<<lp_blocks(np, 256), 256, 0, st>>>(v, f_in, g, bd);
+  k_band_gemv_to_field<T><<<lp_blocks(bd.n * 32, 256), 256, 0, st>>>(f_out, ainv, v, g, bd);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+}  // namespace
+
+#define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
+#define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
+#define LP_ST ((cudaStream_t)stream)
+
+extern "C" {
+
+// the band layout of a level: out[0] = n (dofs), out[1] = nt (32-row tiles), out[2] = D
+// (off-diagonal tiles per tile row), out[3] = half-bandwidth; returns the tile count nt (D + 1)
+long long lpb_band_dims(int nx, int ny, int nz, long long* out) {
+  if (nx < 1 || ny < 1 || nz < 1) return LP_ERR_ARG;
+  const LpBand bd = lp_band(nx + 1, ny + 1, nz + 1);
+  if (out) {
+    out[0] = bd.n;
+    out[1] = bd.nt;
+    out[2] = bd.D;
+    out[3] = 3LL * ((long long)bd.N1 * bd.N2 + bd.N2 + 1) + 2;
+  }
+  return (long long)bd.nt * (bd.D + 1);
+}
+
+// Cholesky of the band in t (from lpb_coarse_band_*), in place; linv: nt x 1024 doubles (the
+// inverses of the diagonal factor tiles); info: one device int, 0 or the first dof (1-based)
+// whose pivot was not positive; bar: 64 device words of scratch; err: one device int, set when
+// a barrier wait gave up. One cooperative launch of max(D, D (D + 1) / 2) blocks.
+int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !t || !linv || !info || !bar || !err) return LP_ERR_ARG;
+  LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  int dev = 0, nsm = 0, per_sm = 0, coop = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band_factor, 256, 0);
+  // one block per trailing tile while they all fit at once (a cooperative launch needs every
+  // block resident), fewer blocks with several tiles each beyond that
+  long long nblocks = (long long)bd.D * (bd.D + 1) / 2;
+  const long long cap = (long long)per_sm * nsm;
+  if (nblocks > cap) nblocks = cap;
+  if (!coop || nblocks < 1) return LP_ERR_SIZE;
+  if (cudaMemsetAsync(bar, 0, 64 * sizeof(unsigned), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
+  if (cudaMemsetAsync(info, 0, sizeof(int), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
+  void* args[] = {&t, &linv, &bd, &info, &bar, &err};
+  if (cudaLaunchCooperativeKernel((const void*)k_band_factor, dim3((unsigned)nblocks), dim3(256), args, 0, LP_ST) !=
+      cudaSuccess)
+    return LP_ERR_LAUNCH;
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// ainv (32 nt x 32 nt doubles, row-major, band numbering) = A^-1 from the factor
+int lpb_band_inverse(double* ainv, const double* t, const double* linv, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !ainv || !t || !linv) return LP_ERR_ARG;
+  const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  const long long np = 32LL * bd.nt;
+  // as many (tile, block) pairs per chunk as fit in 227 KB next to the diagonal inverse and S
+  int chunk = (int)((227 * 1024 / (INV_TILE * (long long)sizeof(double)) - 2) / 2);
+  if (chunk > bd.D) chunk = bd.D;
+  if (chunk < 1) return LP_ERR_SIZE;
+  const long long smem = (2LL * chunk + 2) * INV_TILE * sizeof(double);
+  if (cudaFuncSetAttribute(k_band_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return LP_ERR_SIZE;
+  k_band_inverse<<<(unsigned)(np / INV_COLS), 512, (size_t)smem, LP_ST>>>(ainv, t, linv, bd, chunk);
+  k_sym_lower<<<dim3(bd.nt, bd.nt), 256, 0, LP_ST>>>(ainv, np);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// f_out = A^-1 f_in on the coarsest level (fields of the level, any component masks already in
+// the operator); v: 32 nt doubles of scratch
+int lpb_band_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, LP_GRID_ARGS, void* stream) {
+  return band_solve<float>(f_out, f_in, ainv, v, LP_GRID, LP_ST);
+}
+
+int lpb_band_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, LP_GRID_ARGS,
+                       void* stream) {
+  return band_solve<double>(f_out, f_in, ainv, v, LP_GRID, LP_ST);
+}
+
+}  // extern "C"

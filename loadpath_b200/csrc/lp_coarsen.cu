@@ -245,8 +245,54 @@ __global__ void k_held0(uint8_t* __restrict__ held, const uint8_t* __restrict__ 
     held[i] = (uint8_t)(((mask0[i] >> 3) & fixed_bits[i]) & 7);
 }
 
+// one entry of the coarsest operator D K D + (I - D), symmetrised (loadpath/mg.py:735-740):
+// row dof (ci at node ix, iy, iz), column dof (cj at node jx, jy, jz)
+template <typename Tw>
+__device__ __forceinline__ double coarse_entry(int kind, const Tw* __restrict__ w, const Tw* __restrict__ mcat,
+                                               const int* __restrict__ patch_id, const Tw* __restrict__ patch_k,
+                                               const Tw* __restrict__ k, const uint8_t* __restrict__ mask,
+                                               const LpGrid& g, int ci, int ix, int iy, int iz, int cj, int jx,
+                                               int jy, int jz) {
+  double s = 0.0;
+  if (abs(ix - jx) <= 1 && abs(iy - jy) <= 1 && abs(iz - jz) <= 1) {
+    for (int kk = 0; kk < 8; ++kk) {
+      int cx = ix - cx_(kk), cy = iy - cy_(kk), cz = iz - cz_(kk);
+      if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
+      int ox = jx - cx, oy = jy - cy, oz = jz - cz;
+      if (ox < 0 || ox > 1 || oy < 0 || oy > 1 || oz < 0 || oz > 1) continue;
+      int kj = ox | (oy << 1) | (oz << 2);
+      long long c = g.cell(cx, cy, cz);
+      int r1 = 3 * kk + ci, c1 = 3 * kj + cj;
+      int e1 = r1 * 24 + c1, e2 = c1 * 24 + r1;
+      double v1, v2;
+      if (kind == 1) {
+        v1 = v2 = 0.0;
+        for (int q = 0; q < 8; ++q) {
+          double wq = (double)w[q * g.cells_padded() + c];
+          v1 += (double)mcat[q * 576 + e1] * wq;
+          v2 += (double)mcat[q * 576 + e2] * wq;
+        }
+        int p = patch_id ? patch_id[c] : -1;
+        if (p >= 0) {
+          v1 += (double)patch_k[(long long)p * 576 + e1];
+          v2 += (double)patch_k[(long long)p * 576 + e2];
+        }
+      } else {
+        v1 = (double)k[c * 576 + e1];
+        v2 = (double)k[c * 576 + e2];
+      }
+      s += 0.5 * (v1 + v2);
+    }
+  }
+  double mi = ((mask[g.node(ix, iy, iz)] >> ci) & 1) ? 1.0 : 0.0;
+  double mj = ((mask[g.node(jx, jy, jz)] >> cj) & 1) ? 1.0 : 0.0;
+  double v = mi * s * mj;
+  if (ci == cj && ix == jx && iy == jy && iz == jz) v += 1.0 - mi;
+  return v;
+}
+
 // dense coarsest operator over every node of the level, dof (c, node) -> c * NN + node with
-// node = (x * NY + y) * NZ + z: a = D K D + (I - D), symmetrised (loadpath/mg.py:735-740)
+// node = (x * NY + y) * NZ + z
 template <typename Tw>
 __global__ void k_coarse_dense(double* __restrict__ a, int kind, const Tw* __restrict__ w,
                                const Tw* __restrict__ mcat, const int* __restrict__ patch_id,
@@ -255,83 +301,48 @@ __global__ void k_coarse_dense(double* __restrict__ a, int kind, const Tw* __res
   const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
   const long long NN = (long long)NX * NY * NZ;
   const long long n = 3 * NN;
+  (void)NX;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n; t += (long long)gridDim.x * blockDim.x) {
     long long I = t / n, J = t % n;
     int ci = (int)(I / NN), cj = (int)(J / NN);
     long long ni = I % NN, nj = J % NN;
     int iz = (int)(ni % NZ), iy = (int)((ni / NZ) % NY), ix = (int)(ni / ((long long)NZ * NY));
     int jz = (int)(nj % NZ), jy = (int)((nj / NZ) % NY), jx = (int)(nj / ((long long)NZ * NY));
-    double s = 0.0;
-    if (abs(ix - jx) <= 1 && abs(iy - jy) <= 1 && abs(iz - jz) <= 1) {
-      for (int kk = 0; kk < 8; ++kk) {
-        int cx = ix - cx_(kk), cy = iy - cy_(kk), cz = iz - cz_(kk);
-        if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
-        int ox = jx - cx, oy = jy - cy, oz = jz - cz;
-        if (ox < 0 || ox > 1 || oy < 0 || oy > 1 || oz < 0 || oz > 1) continue;
-        int kj = ox | (oy << 1) | (oz << 2);
-        long long c = g.cell(cx, cy, cz);
-        int r1 = 3 * kk + ci, c1 = 3 * kj + cj;
-        int e1 = r1 * 24 + c1, e2 = c1 * 24 + r1;
-        double v1, v2;
-        if (kind == 1) {
-          v1 = v2 = 0.0;
-          for (int q = 0; q < 8; ++q) {
-            double wq = (double)w[q * g.cells_padded() + c];
-            v1 += (double)mcat[q * 576 + e1] * wq;
-            v2 += (double)mcat[q * 576 + e2] * wq;
-          }
-          int p = patch_id ? patch_id[c] : -1;
-          if (p >= 0) {
-            v1 += (double)patch_k[(long long)p * 576 + e1];
-            v2 += (double)patch_k[(long long)p * 576 + e2];
-          }
-        } else {
-          v1 = (double)k[c * 576 + e1];
-          v2 = (double)k[c * 576 + e2];
-        }
-        s += 0.5 * (v1 + v2);
+    a[t] = coarse_entry(kind, w, mcat, patch_id, patch_k, k, mask, g, ci, ix, iy, iz, cj, jx, jy, jz);
+  }
+}
+
+// ---- the coarsest operator as a band (for lp_band.cu's Cholesky) ---------------------------
+// Dofs are numbered 3 * node + component with the node's coordinates ordered so the longest
+// axis varies slowest: the half-bandwidth is then 3 (N1 N2 + N2 + 1) + 2 for the two shorter
+// extents N1 >= N2. The lower band is stored as 32 x 32 tiles: tile (R, d) holds rows
+// 32R..32R+31, columns 32(R-d)..32(R-d)+31, row-major, at t + (R (D + 1) + d) 1024; dofs past n
+// (padding to a multiple of 32) are identity rows.
+template <typename Tw>
+__global__ void k_coarse_band(double* __restrict__ t, int kind, const Tw* __restrict__ w, const Tw* __restrict__ mcat,
+                              const int* __restrict__ patch_id, const Tw* __restrict__ patch_k,
+                              const Tw* __restrict__ k, const uint8_t* __restrict__ mask, LpGrid g, LpBand bd) {
+  const long long total = (long long)bd.nt * (bd.D + 1) * 1024;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int rc = (int)(e & 1023);
+    const long long td = e >> 10;
+    const int d = (int)(td % (bd.D + 1));
+    const int R = (int)(td / (bd.D + 1));
+    const long long i = 32LL * R + (rc >> 5), j = 32LL * (R - d) + (rc & 31);
+    double v = 0.0;
+    if (j >= 0 && j <= i) {
+      if (i >= bd.n || j >= bd.n) {
+        v = i == j ? 1.0 : 0.0;
+      } else {
+        int ix, iy, iz, jx, jy, jz;
+        bd.coords(i / 3, ix, iy, iz);
+        bd.coords(j / 3, jx, jy, jz);
+        v = coarse_entry(kind, w, mcat, patch_id, patch_k, k, mask, g, (int)(i % 3), ix, iy, iz, (int)(j % 3), jx, jy,
+                         jz);
       }
     }
-    double mi = ((mask[g.node(ix, iy, iz)] >> ci) & 1) ? 1.0 : 0.0;
-    double mj = ((mask[g.node(jx, jy, jz)] >> cj) & 1) ? 1.0 : 0.0;
-    double v = mi * s * mj;
-    if (I == J) v += 1.0 - mi;
-    a[t] = v;
-  }
-}
-
-// x = ainv b on the coarsest level: gather b (float field) into a dense float64 vector,
-// one warp per row of ainv, scatter back. (The dense inverse is formed once per hierarchy.)
-template <typename T>
-__global__ void k_field_to_dense(double* __restrict__ v, const T* __restrict__ f, LpGrid g) {
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long NN = (long long)NX * NY * NZ;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * NN; t += (long long)gridDim.x * blockDim.x) {
-    int c = (int)(t / NN);
-    long long nd = t % NN;
-    int z = (int)(nd % NZ), y = (int)((nd / NZ) % NY), x = (int)(nd / ((long long)NZ * NY));
-    v[t] = (double)f[c * g.comp_stride() + g.node(x, y, z)];
-  }
-}
-
-template <typename T>
-__global__ void k_dense_gemv_to_field(T* __restrict__ f, const double* __restrict__ a, const double* __restrict__ v,
-                                      LpGrid g) {
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long NN = (long long)NX * NY * NZ;
-  const long long n = 3 * NN;
-  int lane = threadIdx.x & 31;
-  long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  if (row >= n) return;
-  const double* ar = a + row * n;
-  double s = 0.0;
-  for (long long j = lane; j < n; j += 32) s += ar[j] * v[j];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (lane == 0) {
-    int c = (int)(row / NN);
-    long long nd = row % NN;
-    int z = (int)(nd % NZ), y = (int)((nd / NZ) % NY), x = (int)(nd / ((long long)NZ * NY));
-    f[c * g.comp_stride() + g.node(x, y, z)] = (T)s;
+    t[e] = v;
   }
 }
 
@@ -461,23 +472,26 @@ int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mca
 }
 
 // f = ainv * f on the coarsest level; v: scratch of 3 * nodes doubles
-int lpb_coarse_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, LP_GRID_ARGS, void* stream) {
+// the coarsest operator as band tiles (layout: lpb_band_dims); t: nt (D + 1) x 1024 doubles
+int lpb_coarse_band_f32(double* t, int kind, const float* w, const float* mcat, const int* patch_id,
+                        const float* patch_k, const float* k, const uint8_t* mask, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
-  if (!lp_grid_ok(g) || !f_out || !f_in || !ainv || !v) return LP_ERR_ARG;
-  long long n = 3LL * g.NX() * g.NY() * g.NZ();
-  k_field_to_dense<float><<<lp_blocks(n, 256), 256, 0, LP_ST>>>(v, f_in, g);
-  k_dense_gemv_to_field<float><<<lp_blocks(n * 32, 256), 256, 0, LP_ST>>>(f_out, ainv, v, g);
+  if (!lp_grid_ok(g) || !t || !mask || (kind == 1 && (!w || !mcat)) || (kind == 2 && !k)) return LP_ERR_ARG;
+  const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  const long long total = (long long)bd.nt * (bd.D + 1) * 1024;
+  k_coarse_band<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(t, kind, w, mcat, patch_id, patch_k, k, mask, g, bd);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_coarse_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, LP_GRID_ARGS,
-                         void* stream) {
+int lpb_coarse_band_f64(double* t, int kind, const double* w, const double* mcat, const int* patch_id,
+                        const double* patch_k, const double* k, const uint8_t* mask, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
-  if (!lp_grid_ok(g) || !f_out || !f_in || !ainv || !v) return LP_ERR_ARG;
-  long long n = 3LL * g.NX() * g.NY() * g.NZ();
-  k_field_to_dense<double><<<lp_blocks(n, 256), 256, 0, LP_ST>>>(v, f_in, g);
-  k_dense_gemv_to_field<double><<<lp_blocks(n * 32, 256), 256, 0, LP_ST>>>(f_out, ainv, v, g);
+  if (!lp_grid_ok(g) || !t || !mask || (kind == 1 && (!w || !mcat)) || (kind == 2 && !k)) return LP_ERR_ARG;
+  const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  const long long total = (long long)bd.nt * (bd.D + 1) * 1024;
+  k_coarse_band<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(t, kind, w, mcat, patch_id, patch_k, k, mask, g,
+                                                                  bd);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

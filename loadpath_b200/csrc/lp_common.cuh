@@ -51,6 +51,44 @@ static inline int lp_blocks(long long n, int threads) {
   return (int)b;
 }
 
+// The coarsest level as a band: dofs numbered 3 * node + component, nodes ordered with the
+// longest axis slowest (perm[0]) and the shortest fastest (perm[2]); half-bandwidth
+// bw = 3 (N1 N2 + N2 + 1) + 2; 32-row tiles, D off-diagonal tiles per tile row.
+struct LpBand {
+  int perm[3];
+  int N1, N2;      // extents of axes perm[1], perm[2]
+  long long n;     // 3 * nodes
+  int nt, D;       // n padded to 32 * nt
+  __host__ __device__ void coords(long long node, int& x, int& y, int& z) const {
+    const int p2 = (int)(node % N2);
+    const long long q = node / N2;
+    const int p1 = (int)(q % N1), p0 = (int)(q / N1);
+    int c[3];
+    c[perm[0]] = p0;
+    c[perm[1]] = p1;
+    c[perm[2]] = p2;
+    x = c[0];
+    y = c[1];
+    z = c[2];
+  }
+};
+
+static inline LpBand lp_band(int NX, int NY, int NZ) {
+  const int ext[3] = {NX, NY, NZ};
+  LpBand b;
+  b.perm[0] = 0; b.perm[1] = 1; b.perm[2] = 2;
+  for (int i = 0; i < 3; ++i)          // stable sort of the axes by extent, longest first
+    for (int j = 0; j + 1 < 3 - i; ++j)
+      if (ext[b.perm[j]] < ext[b.perm[j + 1]]) { int t = b.perm[j]; b.perm[j] = b.perm[j + 1]; b.perm[j + 1] = t; }
+  b.N1 = ext[b.perm[1]];
+  b.N2 = ext[b.perm[2]];
+  b.n = 3LL * NX * NY * NZ;
+  b.nt = (int)((b.n + 31) / 32);
+  const long long bw = 3LL * ((long long)b.N1 * b.N2 + b.N2 + 1) + 2;
+  b.D = (int)((bw + 31) / 32);
+  return b;
+}
+
 #define LP_LAUNCH_CHECK()                                   \
   do {                                                      \
     cudaError_t _e = cudaGetLastError();                    \

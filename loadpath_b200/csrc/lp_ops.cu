@@ -208,9 +208,17 @@ int launch_diag(double* d, LpGrid g, LevelArgs<T> a, cudaStream_t st) {
 //   alive = d > alive_thr;  live = d > live_thr
 //   solved = live & ~held (held from held_bits) ; strict: also & kept >= 1
 //   dinv = solved ? 1 / d : 1
+// With thr_scale given (a device scalar, the level's largest diagonal), both thresholds are
+// relative: thr * max(*thr_scale, 1e-300) (loadpath/mg.py:565-567), so no host read is needed.
 __global__ void k_masks(uint8_t* __restrict__ mask, double* __restrict__ dinv64, float* __restrict__ dinv32,
                         const double* __restrict__ d, const uint8_t* __restrict__ held_bits,
-                        const float* __restrict__ kept, LpGrid g, double alive_thr, double live_thr) {
+                        const float* __restrict__ kept, LpGrid g, double alive_thr, double live_thr,
+                        const double* __restrict__ thr_scale) {
+  if (thr_scale) {
+    const double sc = fmax(*thr_scale, 1e-300);
+    alive_thr *= sc;
+    live_thr *= sc;
+  }
   const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
   const long long total = (long long)NX * NY * NZ;
   const long long cs = g.comp_stride();
@@ -268,6 +276,79 @@ __global__ void k_max_final(const double* __restrict__ part, int n, double* __re
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
     if (threadIdx.x == 0) *out = m;
   }
+}
+
+
+// ---- active-cell and mismatch counts (loadpath/mg.py:559, :593-599), into device scalars --
+// Each block writes a partial count, one block adds them in order: exact integer sums in
+// float64, the same bits every run, and no host read between the kernels that need them.
+#define LP_COUNT_BLOCKS 592
+
+__device__ __forceinline__ void lp_count_store(double c, double* part) {
+  __shared__ double sh[32];
+  c = lp_block_sum(c, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = c;
+}
+
+// cells with modulus > 0 (all padded cells; the padding holds zeros)
+__global__ void k_count_pos(const double* __restrict__ e, long long n, double* __restrict__ part) {
+  double c = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    c += e[i] > 0.0 ? 1.0 : 0.0;
+  lp_count_store(c, part);
+}
+
+// level-1 cells with a non-zero child weight or a patch matrix
+template <typename T>
+__global__ void k_count_weights(const T* __restrict__ w, const int* __restrict__ patch_id, LpGrid g,
+                                double* __restrict__ part) {
+  const long long total = (long long)g.nx * g.ny * g.nz, ncp = g.cells_padded();
+  double c = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(t % g.nz);
+    const long long q = t / g.nz;
+    const long long cell = g.cell((int)(q / g.ny), (int)(q % g.ny), z);
+    bool act = patch_id && patch_id[cell] >= 0;
+    for (int k = 0; k < 8 && !act; ++k) act = w[k * ncp + cell] != T(0);
+    c += act ? 1.0 : 0.0;
+  }
+  lp_count_store(c, part);
+}
+
+// explicit-level cells whose 24 x 24 matrix has a non-zero entry; one warp per cell
+template <typename T>
+__global__ void k_count_explicit(const T* __restrict__ k, LpGrid g, double* __restrict__ part) {
+  const long long total = (long long)g.nx * g.ny * g.nz;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  double c = 0.0;
+  for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < total; t += warps) {
+    const int z = (int)(t % g.nz);
+    const long long q = t / g.nz;
+    const T* kc = k + g.cell((int)(q / g.ny), (int)(q % g.ny), z) * 576;
+    bool nz = false;
+    for (int i = lane; i < 576; i += 32) nz = nz || kc[i] != T(0);
+    if (__any_sync(0xffffffffu, nz) && lane == 0) c += 1.0;
+  }
+  lp_count_store(c, part);
+}
+
+// positions where two byte arrays differ
+__global__ void k_count_ne_u8(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, long long n,
+                              double* __restrict__ part) {
+  double c = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    c += a[i] != b[i] ? 1.0 : 0.0;
+  lp_count_store(c, part);
+}
+
+__global__ void k_count_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace
@@ -363,12 +444,13 @@ int lpb_diag_explicit_f32(double* d, const float* k, LP_GRID_ARGS, void* stream)
 }
 
 int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, const uint8_t* held_bits,
-              const float* kept, LP_GRID_ARGS, double alive_thr, double live_thr, void* stream) {
+              const float* kept, LP_GRID_ARGS, double alive_thr, double live_thr, const double* thr_scale,
+              void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !mask || !d) return LP_ERR_ARG;
   long long total = (long long)g.NX() * g.NY() * g.NZ();
   k_masks<<<lp_blocks(total, 256), 256, 0, (cudaStream_t)stream>>>(mask, dinv64, dinv32, d, held_bits, kept, g,
-                                                                   alive_thr, live_thr);
+                                                                   alive_thr, live_thr, thr_scale);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -380,6 +462,61 @@ int lpb_max_f64(const double* a, long long n, double* part, double* out, void* s
   if (blocks > 1024) blocks = 1024;
   k_max_partial<<<blocks, 256, 0, (cudaStream_t)stream>>>(a, n, part);
   k_max_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, blocks, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// ---- counts into a device scalar; part: scratch of at least 592 doubles ----------------
+int lpb_count_positive_f64(const double* e, long long n, double* part, double* out, void* stream) {
+  if (!e || !part || !out || n < 0) return LP_ERR_ARG;
+  k_count_pos<<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(e, n, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_count_active_weights_f32(const float* w, const int* patch_id, LP_GRID_ARGS, double* part, double* out,
+                                 void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !w || !part || !out) return LP_ERR_ARG;
+  k_count_weights<float><<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(w, patch_id, g, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_count_active_weights_f64(const double* w, const int* patch_id, LP_GRID_ARGS, double* part, double* out,
+                                 void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !w || !part || !out) return LP_ERR_ARG;
+  k_count_weights<double><<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(w, patch_id, g, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_count_active_explicit_f32(const float* k, LP_GRID_ARGS, double* part, double* out, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !k || !part || !out) return LP_ERR_ARG;
+  k_count_explicit<float><<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(k, g, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_count_active_explicit_f64(const double* k, LP_GRID_ARGS, double* part, double* out, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !k || !part || !out) return LP_ERR_ARG;
+  k_count_explicit<double><<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(k, g, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_count_ne_u8(const uint8_t* a, const uint8_t* b, long long n, double* part, double* out, void* stream) {
+  if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;
+  k_count_ne_u8<<<LP_COUNT_BLOCKS, 256, 0, (cudaStream_t)stream>>>(a, b, n, part);
+  k_count_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, LP_COUNT_BLOCKS, out);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -11,6 +11,7 @@
 
 #define LP_RED_BLOCKS 592   // 4 per SM on 148 SMs
 #define LP_RED_THREADS 512
+#define LP_CHEB_MAX_DEGREE 7   // coefficient block of 16 doubles per level
 
 namespace {
 
@@ -74,10 +75,15 @@ __global__ void k_axpby(T* __restrict__ out, T a, const T* __restrict__ x, T b, 
     out[i] = a * x[i] + (y ? b * y[i] : T(0));
 }
 
+// Smoother coefficients live in device memory (written by k_cheb_coef after the power
+// iteration), so a V-cycle never needs lmax on the host and a captured V-cycle stays valid when
+// the hierarchy is rebuilt: coef[1] = 1 / theta, coef[2 + 2k], coef[3 + 2k] = c1, c2 of step k.
+
 // Chebyshev start from zero: x = 0; r = b; d = (dinv b) s        (loadpath/mgops.py:321-328)
 template <typename T>
-__global__ void k_cheb_start(const T* __restrict__ b, const T* __restrict__ dinv, T s, T* __restrict__ x,
-                             T* __restrict__ r, T* __restrict__ d, long long n) {
+__global__ void k_cheb_start(const T* __restrict__ b, const T* __restrict__ dinv, const double* __restrict__ coef,
+                             T* __restrict__ x, T* __restrict__ r, T* __restrict__ d, long long n) {
+  const T s = (T)coef[1];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     T bi = b[i];
     x[i] = T(0);
@@ -88,8 +94,9 @@ __global__ void k_cheb_start(const T* __restrict__ b, const T* __restrict__ dinv
 
 // r = b - ax; d = s dinv r                                        (loadpath/mgops.py:314-319)
 template <typename T>
-__global__ void k_residual_scaled(const T* __restrict__ b, const T* __restrict__ ax, const T* __restrict__ dinv, T s,
-                                  T* __restrict__ r, T* __restrict__ d, long long n) {
+__global__ void k_residual_scaled(const T* __restrict__ b, const T* __restrict__ ax, const T* __restrict__ dinv,
+                                  const double* __restrict__ coef, T* __restrict__ r, T* __restrict__ d, long long n) {
+  const T s = (T)coef[1];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     T ri = b[i] - ax[i];
     r[i] = ri;
@@ -100,7 +107,8 @@ __global__ void k_residual_scaled(const T* __restrict__ b, const T* __restrict__
 // x += d; unless last: r -= ad; d = c1 d + c2 dinv r             (loadpath/mgops.py:334-343)
 template <typename T>
 __global__ void k_cheb(T* __restrict__ x, T* __restrict__ d, T* __restrict__ r, const T* __restrict__ ad,
-                       const T* __restrict__ dinv, T c1, T c2, int last, long long n) {
+                       const T* __restrict__ dinv, const double* __restrict__ coef, int step, int last, long long n) {
+  const T c1 = (T)coef[2 + 2 * step], c2 = (T)coef[3 + 2 * step];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     T di = d[i];
     x[i] += di;
@@ -109,6 +117,29 @@ __global__ void k_cheb(T* __restrict__ x, T* __restrict__ d, T* __restrict__ r, 
       r[i] = ri;
       d[i] = c1 * di + c2 * dinv[i] * ri;
     }
+  }
+}
+
+// lmax and the Chebyshev coefficients from the power iteration's dots (loadpath/mg.py:771-794,
+// :796-821): lmax = safety * max(v.Av of the last step, 1e-12), or 2 when some |v|^2 was 0;
+// the interval is [lmax / 30, lmax]. One thread, float64 throughout.
+__global__ void k_cheb_coef(double* __restrict__ coef, const double* __restrict__ vv, const double* __restrict__ vav,
+                            int its, int degree, double safety) {
+  bool zero = false;
+  for (int k = 0; k < its; ++k) zero = zero || vv[k] == 0.0;
+  const double lam = vav[its - 1];
+  const double hi = zero ? 2.0 : safety * (lam > 1e-12 ? lam : 1e-12);
+  const double lo = hi / 30.0;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+  const double sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  coef[0] = hi;
+  coef[1] = 1.0 / theta;
+  for (int k = 0; k < degree; ++k) {
+    const double rho_new = 1.0 / (2.0 * sigma - rho);
+    coef[2 + 2 * k] = rho_new * rho;
+    coef[3 + 2 * k] = 2.0 * rho_new / delta;
+    rho = rho_new;
   }
 }
 
@@ -248,6 +279,30 @@ __global__ void k_dinv_mask(T* __restrict__ av, const T* __restrict__ dinv, cons
   }
 }
 
+
+// Warm start of the PCG on the device (loadpath/mg.py:878-895), so the solve never waits on
+// the host before its first iteration. sc: [0] b.b, [5] x.Ax, [6] b.x, [7] |rs|^2.
+//   s = b.x / x.Ax when x.Ax > 0, else 0;  rs = b - s Ax
+__device__ __forceinline__ double lp_warm_scale(const double* sc) { return sc[5] > 0.0 ? sc[6] / sc[5] : 0.0; }
+
+__global__ void k_warm_residual(double* __restrict__ rs, const double* __restrict__ b, const double* __restrict__ ax,
+                                const double* __restrict__ sc, long long n) {
+  const double s = lp_warm_scale(sc);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    rs[i] = b[i] - s * ax[i];
+}
+
+// keep the scaled warm start when s > 0 and |rs| < |b| (x = s x, r = rs), else x = 0, r = b
+__global__ void k_warm_select(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ b,
+                              const double* __restrict__ rs, const double* __restrict__ sc, long long n) {
+  const double s = lp_warm_scale(sc);
+  const bool keep = s > 0.0 && sqrt(sc[7]) < sqrt(sc[0]);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] = keep ? x[i] * s : 0.0;
+    r[i] = keep ? rs[i] : b[i];
+  }
+}
+
 }  // namespace
 
 #define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
@@ -346,44 +401,58 @@ int lpb_cast_f32_f64(double* out, const float* a, long long n, void* stream) {
   return LP_OK;
 }
 
-int lpb_cheb_start_f32(const float* b, const float* dinv, float s, float* x, float* r, float* d, long long n,
-                       void* stream) {
-  k_cheb_start<float><<<LP_VEC_GRID(n)>>>(b, dinv, s, x, r, d, n);
+int lpb_cheb_coef(double* coef, const double* vv, const double* vav, int its, int degree, double safety,
+                  void* stream) {
+  if (!coef || !vv || !vav || its < 1 || degree < 1 || degree > LP_CHEB_MAX_DEGREE) return LP_ERR_ARG;
+  k_cheb_coef<<<1, 1, 0, LP_ST>>>(coef, vv, vav, its, degree, safety);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_cheb_start_f64(const double* b, const double* dinv, double s, double* x, double* r, double* d, long long n,
-                       void* stream) {
-  k_cheb_start<double><<<LP_VEC_GRID(n)>>>(b, dinv, s, x, r, d, n);
+int lpb_cheb_start_f32(const float* b, const float* dinv, const double* coef, float* x, float* r, float* d,
+                       long long n, void* stream) {
+  if (!b || !dinv || !coef || !x || !r || !d) return LP_ERR_ARG;
+  k_cheb_start<float><<<LP_VEC_GRID(n)>>>(b, dinv, coef, x, r, d, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, float s, float* r, float* d,
-                            long long n, void* stream) {
-  k_residual_scaled<float><<<LP_VEC_GRID(n)>>>(b, ax, dinv, s, r, d, n);
+int lpb_cheb_start_f64(const double* b, const double* dinv, const double* coef, double* x, double* r, double* d,
+                       long long n, void* stream) {
+  if (!b || !dinv || !coef || !x || !r || !d) return LP_ERR_ARG;
+  k_cheb_start<double><<<LP_VEC_GRID(n)>>>(b, dinv, coef, x, r, d, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, double s, double* r, double* d,
-                            long long n, void* stream) {
-  k_residual_scaled<double><<<LP_VEC_GRID(n)>>>(b, ax, dinv, s, r, d, n);
+int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, const double* coef, float* r,
+                            float* d, long long n, void* stream) {
+  if (!b || !ax || !dinv || !coef || !r || !d) return LP_ERR_ARG;
+  k_residual_scaled<float><<<LP_VEC_GRID(n)>>>(b, ax, dinv, coef, r, d, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, float c1, float c2, int last,
-                 long long n, void* stream) {
-  k_cheb<float><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, c1, c2, last, n);
+int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, const double* coef, double* r,
+                            double* d, long long n, void* stream) {
+  if (!b || !ax || !dinv || !coef || !r || !d) return LP_ERR_ARG;
+  k_residual_scaled<double><<<LP_VEC_GRID(n)>>>(b, ax, dinv, coef, r, d, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
 
-int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, double c1, double c2, int last,
-                 long long n, void* stream) {
-  k_cheb<double><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, c1, c2, last, n);
+int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, const double* coef, int step,
+                 int last, long long n, void* stream) {
+  if (!x || !d || !r || !ad || !dinv || !coef || step < 0 || step >= LP_CHEB_MAX_DEGREE) return LP_ERR_ARG;
+  k_cheb<float><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, coef, step, last, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, const double* coef, int step,
+                 int last, long long n, void* stream) {
+  if (!x || !d || !r || !ad || !dinv || !coef || step < 0 || step >= LP_CHEB_MAX_DEGREE) return LP_ERR_ARG;
+  k_cheb<double><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, coef, step, last, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -484,6 +553,21 @@ int lpb_dinv_mask_f64(double* av, const double* dinv, const uint8_t* m, LP_GRID_
   LpGrid g = LP_GRID;
   long long n = 3 * g.nodes_padded();
   k_dinv_mask<double><<<LP_VEC_GRID(n)>>>(av, dinv, m, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_warm_residual(double* rs, const double* b, const double* ax, const double* sc, long long n, void* stream) {
+  if (!rs || !b || !ax || !sc || n < 0) return LP_ERR_ARG;
+  k_warm_residual<<<LP_VEC_GRID(n)>>>(rs, b, ax, sc, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_warm_select(double* x, double* r, const double* b, const double* rs, const double* sc, long long n,
+                    void* stream) {
+  if (!x || !r || !b || !rs || !sc || n < 0) return LP_ERR_ARG;
+  k_warm_select<<<LP_VEC_GRID(n)>>>(x, r, b, rs, sc, n);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import fem
-from ._lib import LpError, lib
+from ._lib import LpError, add_launches, launches, lib
 from .grid import DevGrid, ptr, stream_handle, torch_dtype
 
 __all__ = ["GridElasticity", "BoxMesh", "LMAX_SAFETY", "STALL"]
@@ -129,8 +129,13 @@ class DevLevel:
         self.pbox = None         # weights: node box of the patch cells (host, 6 ints)
         self.mask = None
         self.dinv = None
-        self.lmax = None
+        self.coef = None         # device: lmax and the Chebyshev coefficients (lpb_cheb_coef)
         self.n_active = 0
+
+    @property
+    def lmax(self):
+        """The smoother's upper eigenvalue bound (read from the device)."""
+        return None if self.coef is None else float(self.coef[0].item())
 
     @property
     def dims(self):
@@ -266,16 +271,28 @@ class GridElasticity:
         self.levels = []
         self.strict = False
         self.last_iters = 0
-        self._lmax_vec = {}
+        self._lmax_init = {}
         self._coarse = None
+        self._plan = None
+        self._patch_plan = None
+        self._mcat_dev = {}
         self._scal = torch.zeros(64, dtype=torch.float64, device=self.device)
+        # device scalars of a build: [0] cells with E > 0, [d] active cells of level d, [31]
+        # patch-flag mismatches, [40 + d] largest diagonal of level d; power-iteration dots
+        # (32 per level) and Chebyshev coefficients (16 per level)
+        self._chk = torch.zeros(64, dtype=torch.float64, device=self.device)
+        self._chk_host = torch.zeros(32, dtype=torch.float64, pin_memory=True)
+        self._info_host = torch.zeros(2, dtype=torch.int32, pin_memory=True)
+        self._pw = torch.zeros(32 * 32, dtype=torch.float64, device=self.device)
+        self._coef = torch.zeros(16 * 32, dtype=torch.float64, device=self.device)
         self._part = torch.zeros(max(lib().lpb_reduce_blocks(), 1024) * 2, dtype=torch.float64, device=self.device)
         self._host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
         self._work = {}
         self._e_dev = None
         # CUDA graphs for the CG iteration (captured once per solve)
         self.use_graphs = True
-        self._graphs = None
+        self._gcache = {}
+        self._gen = 0            # bumped whenever a work buffer is (re)allocated
         self._cap_stream = torch.cuda.Stream(device=self.device)
 
     # --- layout conversion (loadpath/mg.py:495-511) -----------------------------------
@@ -303,6 +320,7 @@ class GridElasticity:
         if t is None or t.dtype != dtype or t.numel() < n:
             t = torch.zeros(max(n, 1), dtype=dtype, device=self.device)
             self._work[key] = t
+            self._gen += 1
         return t
 
     def _buf(self, key, grid: DevGrid, dtype):
@@ -310,6 +328,7 @@ class GridElasticity:
         if t is None or t.dtype != dtype or tuple(t.shape) != (3, grid.NX, grid.NY, grid.pz):
             t = grid.node_field(dtype)
             self._work[key] = t
+            self._gen += 1
         return t
 
     # --- hierarchy (loadpath/mg.py:515-754) --------------------------------------------
@@ -320,93 +339,174 @@ class GridElasticity:
         e_dev = self.g0.cells_to_dev(self.cell_grid(e), torch.float64)
         self.set_moduli_device(e_dev)
 
+    def _tbuf(self, key, shape, dtype, fill=0):
+        """A persistent device buffer (stable address across rebuilds), filled when created."""
+        t = self._work.get(key)
+        if t is None or t.dtype != dtype or tuple(t.shape) != tuple(shape):
+            t = torch.full(tuple(shape), fill, dtype=dtype, device=self.device)
+            self._work[key] = t
+            self._gen += 1
+        return t
+
     def set_moduli_device(self, e_dev: torch.Tensor):
-        """Moduli already on the device as a padded (nx, ny, pz) float64 cell field."""
+        """Moduli already on the device as a padded (nx, ny, pz) float64 cell field.
+
+        The host decisions of a build (how many levels, which level-1 cells carry patch
+        matrices, the coarsest factor's success) depend on the design only through which cells
+        are non-void, so the first build makes them with host reads and records them; a
+        rebuild with the same record runs without any host read and checks every decision in
+        one copy at the end (active-cell counts, patch flags, factor status), redoing the
+        build from scratch when one differs."""
         self._e_dev = e_dev
+        plan = self._plan
+        if plan is not None and plan["strict"] == self.strict and plan["shape"] == tuple(e_dev.shape):
+            if self._build(e_dev, plan):
+                return
+        self._plan = None
+        self._build(e_dev, None)
+
+    def _build(self, e_dev, plan):
+        """One hierarchy build (loadpath/mg.py:515-591). plan None: discovery (host reads,
+        records a plan). Returns False when a planned build's checks fail."""
         L = lib()
         st = stream_handle()
         g0 = self.g0
         dt = self.tdtype
+        chk = self._chk
+        part = self._part
+        if plan is None:
+            self._gen += 1       # captured graphs may hold launch parameters of the last structure
         l0 = DevLevel("scaled", g0, torch.float64)
-        l0.e = e_dev
+        # the moduli in a buffer of this solver's own, so captured graphs can keep its address
+        l0.e = self._tbuf("e0_64", e_dev.shape, torch.float64)
+        if e_dev.data_ptr() != l0.e.data_ptr():
+            L.lpb_memcpy_async(l0.e.data_ptr(), e_dev.data_ptr(), 8 * e_dev.numel(), st)
+        e_dev = self._e_dev = l0.e
         l0.ke = self.ke64
         l0.kmodal = self.kmodal
         l0.err = self._err
         d0 = self._buf("diag0", g0, torch.float64)
         L.lpb_diag_scaled_f64(d0.data_ptr(), e_dev.data_ptr(), self.ke64.data_ptr(), *g0.args, st)
-        l0.mask = g0.mask_field()
-        l0.dinv = g0.node_field(torch.float64)
-        dinv32 = g0.node_field(torch.float32) if dt == torch.float32 else None
+        l0.mask = self._tbuf("mask0", g0.mask_field().shape, torch.uint8)
+        l0.dinv = self._buf("dinv0_64", g0, torch.float64)
+        dinv32 = self._buf("dinv0_32", g0, torch.float32) if dt == torch.float32 else None
         L.lpb_masks(l0.mask.data_ptr(), l0.dinv.data_ptr(), ptr(dinv32), d0.data_ptr(), self.fixed_bits.data_ptr(),
-                    None, *g0.args, 1e-300, 1e-300, st)
-        self.levels = [l0]
+                    None, *g0.args, 1e-300, 1e-300, None, st)
+        levels = [l0]
         if dt == torch.float32:
             s = DevLevel("scaled", g0, torch.float32)
-            s.e = g0.cell_field(torch.float32)
+            s.e = self._tbuf("e0_32", e_dev.shape, torch.float32)
             L.lpb_cast_f64_f32(s.e.data_ptr(), e_dev.data_ptr(), g0.n_cell_field, st)
             s.ke = self.ke32
             s.kmodal = self.kmodal
             s.err = self._err
             s.mask = l0.mask
             s.dinv = dinv32
-            self._l0s = s
+            l0s = s
         else:
-            self._l0s = l0
+            l0s = l0
+        L.lpb_count_positive_f64(e_dev.data_ptr(), e_dev.numel(), part.data_ptr(), chk[0:].data_ptr(), st)
+        counts = [None if plan else int(chk[0].item())]
         fine = l0
-        n_active = int((e_dev > 0).sum().item())
         depth = 0
         held = None
         if self.strict:
-            held = g0.mask_field()
+            held = self._tbuf("held0", l0.mask.shape, torch.uint8)
             L.lpb_held0(held.data_ptr(), l0.mask.data_ptr(), self.fixed_bits.data_ptr(), held.numel(), st)
-        while n_active > self.coarse_cells and min(fine.dims) >= 2:
-            coarse = self._coarsen(fine, first=(depth == 0))
+
+        def more():
+            if plan is not None:
+                return depth < plan["depth"]
+            return counts[-1] > self.coarse_cells and min(fine.dims) >= 2
+
+        while more():
             depth += 1
+            if depth >= 30:
+                raise RuntimeError("hierarchy deeper than 30 levels")
+            coarse = self._coarsen(fine, depth, plan)
             gc = coarse.grid
             d = self._buf(f"diag{depth}", gc, torch.float64)
             coarse.diagonal(d)
-            L.lpb_max_f64(d.data_ptr(), d.numel(), self._part.data_ptr(), self._scal[40:].data_ptr(), st)
-            dmax = float(self._scal[40].item())
-            thr = 1e-12 * max(dmax, 1e-300)
+            L.lpb_max_f64(d.data_ptr(), d.numel(), part.data_ptr(), chk[40 + depth:].data_ptr(), st)
             held_c = kept = None
             if self.strict:
-                held_c = gc.mask_field()
-                kept = gc.node_field(torch.float32)
+                held_c = self._tbuf(f"held{depth}", gc.mask_field().shape, torch.uint8)
+                kept = self._buf(f"kept{depth}", gc, torch.float32)
                 L.lpb_strict_held_kept(held_c.data_ptr(), kept.data_ptr(), held.data_ptr(), fine.mask.data_ptr(),
                                        *fine.grid.args, *gc.args, st)
                 held = held_c
-            coarse.mask = gc.mask_field()
-            coarse.dinv = gc.node_field(dt)
-            if dt == torch.float32:
-                L.lpb_masks(coarse.mask.data_ptr(), None, coarse.dinv.data_ptr(), d.data_ptr(), ptr(held_c),
-                            ptr(kept), *gc.args, thr, thr, st)
-            else:
-                L.lpb_masks(coarse.mask.data_ptr(), coarse.dinv.data_ptr(), None, d.data_ptr(), ptr(held_c),
-                            ptr(kept), *gc.args, thr, thr, st)
-            n_active = self._active_cells(coarse)
-            self.levels.append(coarse)
+            coarse.mask = self._tbuf(f"mask{depth}", gc.mask_field().shape, torch.uint8)
+            coarse.dinv = self._buf(f"dinv{depth}", gc, dt)
+            d64 = coarse.dinv if dt == torch.float64 else None
+            d32 = coarse.dinv if dt == torch.float32 else None
+            # live = d > 1e-12 max(dmax, 1e-300), dmax read on the device
+            L.lpb_masks(coarse.mask.data_ptr(), ptr(d64), ptr(d32), d.data_ptr(), ptr(held_c), ptr(kept), *gc.args,
+                        1e-12, 1e-12, chk[40 + depth:].data_ptr(), st)
+            self._count_active(coarse, chk[depth:])
+            counts.append(None if plan else int(chk[depth].item()))
+            levels.append(coarse)
             fine = coarse
-        ok = self._build_coarse(self.levels[-1])
-        if not ok:
-            if self.strict:
-                raise RuntimeError("coarsest-level factor is singular in the strict hierarchy")
-            self.strict = True
-            return self.set_moduli_device(e_dev)
-        for i in range(len(self.levels)):
-            self._op(i).lmax = self._estimate_lmax(i)
+        self.levels = levels
+        self._l0s = l0s
+        info = self._build_coarse(levels[-1])
+        for i in range(len(levels)):
+            self._estimate_lmax(i)
+        if plan is None:
+            if info is not None:
+                st_pivot, st_barrier = (int(v) for v in info.cpu().numpy())
+                if st_barrier:
+                    raise RuntimeError("coarsest-level factorisation: a grid-barrier wait gave up")
+                if st_pivot:
+                    return self._singular()
+            self._plan = {"strict": self.strict, "shape": tuple(e_dev.shape), "depth": depth,
+                          "counts": counts, "patch": self._patch_plan}
+            return True
+        # one copy back: every count the plan's decisions rest on, the patch-flag mismatches
+        # and the coarse factor's status
+        hc = self._chk_host
+        L.lpb_memcpy_async(hc.data_ptr(), chk.data_ptr(), 8 * 32, st)
+        if info is not None:
+            L.lpb_memcpy_async(self._info_host.data_ptr(), info.data_ptr(), 8, st)
+        torch.cuda.current_stream().synchronize()
+        # the same decisions as discovery's: coarsen while the active cells exceed
+        # coarse_cells, and the same level-1 patch cells
+        n_act = [int(hc[i]) for i in range(depth + 1)]
+        if any(c <= self.coarse_cells for c in n_act[:depth]):
+            return False
+        if n_act[depth] > self.coarse_cells and min(levels[-1].dims) >= 2:
+            return False
+        if depth >= 1 and int(hc[31]) != 0:
+            return False
+        if info is not None:
+            if int(self._info_host[1]) != 0:
+                raise RuntimeError("coarsest-level factorisation: a grid-barrier wait gave up")
+            if int(self._info_host[0]) != 0:
+                return self._singular()
+        return True
 
-    def _active_cells(self, lv):
-        """(loadpath/mg.py:593-599)"""
+    def _singular(self):
+        """The coarsest factor failed (loadpath/mg.py:586-591): take the strict hierarchy."""
+        if self.strict:
+            raise RuntimeError("coarsest-level factor is singular in the strict hierarchy")
+        self.strict = True
+        self._plan = None
+        self._build(self._e_dev, None)
+        return True
+
+    def _count_active(self, lv, out):
+        """Active cells of a coarse level into a device scalar (loadpath/mg.py:593-599)."""
+        L = lib()
         g = lv.grid
+        sfx = "f32" if lv.dtype == torch.float32 else "f64"
         if lv.kind == "weights":
-            act = (lv.w[:, :, :, :g.nz] != 0).any(dim=0)
-            if lv.npatch:
-                act = act | (lv.patch_id[:, :, :g.nz] >= 0)
-            return int(act.sum().item())
-        k = lv.k.view(g.nx, g.ny, g.cpz, 576)[:, :, :g.nz]
-        return int((k != 0).any(dim=-1).sum().item())
+            getattr(L, f"lpb_count_active_weights_{sfx}")(lv.w.data_ptr(), ptr(lv.patch_id) if lv.npatch else None,
+                                                          *g.args, self._part.data_ptr(), out.data_ptr(),
+                                                          stream_handle())
+        else:
+            getattr(L, f"lpb_count_active_explicit_{sfx}")(lv.k.data_ptr(), *g.args, self._part.data_ptr(),
+                                                           out.data_ptr(), stream_handle())
 
-    def _coarsen(self, fine: DevLevel, first: bool) -> DevLevel:
+    def _coarsen(self, fine: DevLevel, depth: int, plan) -> DevLevel:
         """Galerkin coarse level (loadpath/mg.py:601-677)."""
         L = lib()
         st = stream_handle()
@@ -417,18 +517,41 @@ class GridElasticity:
         cdims = tuple(h + h % 2 if h > 1 else h for h in half)
         gc = DevGrid(cdims, self.device)
         gf = fine.grid
-        if first:
+        ncp = gc.nx * gc.ny * gc.cpz
+        if depth == 1:
             lv = DevLevel("weights", gc, dt)
-            lv.w = torch.zeros((8, gc.nx, gc.ny, gc.cpz), dtype=dt, device=self.device)
+            lv.w = self._tbuf("w1", (8, gc.nx, gc.ny, gc.cpz), dt)
             getattr(L, f"lpb_weights_from_e_f64_{sfx}")(lv.w.data_ptr(), fine.e.data_ptr(), *gf.args, *gc.args, st)
-            lv.mcat = torch.tensor(self._mcat.reshape(-1), dtype=dt, device=self.device)
-            flag = torch.zeros((gc.nx, gc.ny, gc.cpz), dtype=torch.uint8, device=self.device)
+            lv.mcat = self._mcat_dev.get(dt)
+            if lv.mcat is None:
+                lv.mcat = torch.tensor(self._mcat.reshape(-1), dtype=dt, device=self.device)
+                self._mcat_dev[dt] = lv.mcat
+            flag = self._tbuf("pflag_new" if plan else "pflag", (gc.nx, gc.ny, gc.cpz), torch.uint8)
             L.lpb_patch_flags(flag.data_ptr(), fine.e.data_ptr(), fine.mask.data_ptr(), *gf.args, *gc.args, st)
-            pcells = torch.nonzero(flag.reshape(-1)).reshape(-1).to(torch.int64).contiguous()
-            lv.npatch = int(pcells.numel())
-            lv.patch_id = torch.full((gc.nx, gc.ny, gc.cpz), -1, dtype=torch.int32, device=self.device)
+            if plan is not None:
+                pp = plan["patch"]
+                L.lpb_count_ne_u8(flag.data_ptr(), self._work["pflag"].data_ptr(), flag.numel(),
+                                  self._part.data_ptr(), self._chk[31:].data_ptr(), st)
+                pcells, lv.npatch, lv.pbox = pp["cells"], pp["n"], pp["box"]
+            else:
+                pcells = torch.nonzero(flag.reshape(-1)).reshape(-1).to(torch.int64).contiguous()
+                lv.npatch = int(pcells.numel())
+                lv.pbox = np.zeros(6, np.int32)
+                if lv.npatch:
+                    z = pcells % gc.cpz
+                    yx = pcells // gc.cpz
+                    y = yx % gc.ny
+                    x = yx // gc.ny
+                    lo = torch.stack([x.min(), y.min(), z.min()]).cpu().numpy()
+                    hi = torch.stack([x.max(), y.max(), z.max()]).cpu().numpy() + 2   # nodes of the last cell
+                    lv.pbox[:3] = lo
+                    lv.pbox[3:] = hi - lo
+                self._patch_plan = {"cells": pcells, "n": lv.npatch, "box": lv.pbox}
+            lv.patch_id = self._tbuf("patch_id", (gc.nx, gc.ny, gc.cpz), torch.int32, -1)
+            if plan is None:
+                lv.patch_id.fill_(-1)
             if lv.npatch:
-                lv.patch_k = torch.zeros((lv.npatch, 576), dtype=dt, device=self.device)
+                lv.patch_k = self._tbuf("patch_k", (lv.npatch, 576), dt)
                 getattr(L, f"lpb_patch_matrices_{sfx}")(lv.patch_k.data_ptr(), lv.w.data_ptr(), lv.patch_id.data_ptr(),
                                                         pcells.data_ptr(), lv.npatch, fine.e.data_ptr(),
                                                         self.ke64.data_ptr(), fine.mask.data_ptr(), *gf.args,
@@ -437,19 +560,9 @@ class GridElasticity:
                 lv.patch_k = None
             lv.patch_cells = pcells
             lv.g1 = self.g1
-            lv.pbox = np.zeros(6, np.int32)
-            if lv.npatch:
-                z = pcells % gc.cpz
-                yx = pcells // gc.cpz
-                y = yx % gc.ny
-                x = yx // gc.ny
-                lo = torch.stack([x.min(), y.min(), z.min()]).cpu().numpy()
-                hi = torch.stack([x.max(), y.max(), z.max()]).cpu().numpy() + 2   # nodes of the last cell
-                lv.pbox[:3] = lo
-                lv.pbox[3:] = hi - lo
             return lv
         lv = DevLevel("explicit", gc, dt)
-        lv.k = torch.zeros((gc.nx * gc.ny * gc.cpz, 576), dtype=dt, device=self.device)
+        lv.k = self._tbuf(f"k{depth}", (ncp, 576), dt)
         if fine.kind == "weights":
             getattr(L, f"lpb_galerkin_explicit_{sfx}")(lv.k.data_ptr(), 1, fine.w.data_ptr(), fine.mcat.data_ptr(),
                                                        ptr(fine.patch_id), ptr(fine.patch_k), None,
@@ -457,50 +570,58 @@ class GridElasticity:
         else:
             getattr(L, f"lpb_galerkin_explicit_{sfx}")(lv.k.data_ptr(), 2, None, None, None, None, fine.k.data_ptr(),
                                                        fine.mask.data_ptr(), int(self.strict), *gf.args, *gc.args, st)
-        ncp = gc.nx * gc.ny * gc.cpz
-        lv.kp = torch.empty((300, ncp), dtype=dt, device=self.device)
+        lv.kp = self._tbuf(f"kp{depth}", (300, ncp), dt)
         getattr(L, f"lpb_pack_sym_{sfx}")(lv.kp.data_ptr(), lv.k.data_ptr(), ncp, st)
-        lv.ft = torch.empty((24, ncp), dtype=dt, device=self.device)
+        lv.ft = self._tbuf(f"ft{depth}", (24, ncp), dt)
         return lv
 
-    def _build_coarse(self, lv: DevLevel) -> bool:
-        """Dense factor of the coarsest level (loadpath/mg.py:708-754). False when singular."""
+    def _build_coarse(self, lv: DevLevel):
+        """Direct solve of the coarsest level (loadpath/mg.py:708-754): its operator as a band,
+        a tiled band Cholesky and the dense inverse from it, all on the device, once per
+        hierarchy; the V-cycle then applies the inverse with one GEMV. Returns the device status
+        pair (0 0 when fine; [0]: a non-positive pivot, the operator is singular; [1]: a
+        grid-barrier wait of the factorisation gave up), or None when there is no coarse solve."""
+        self._coarse = None
         if lv is self.levels[0]:
-            self._coarse = None
-            return True
+            return None
         g = lv.grid
         n = 3 * g.NX * g.NY * g.NZ
         if n > DENSE_COARSE_MAX:
-            self._coarse = None
-            return True
+            return None
         L = lib()
         st = stream_handle()
         dt = self.tdtype
         sfx = "f32" if dt == torch.float32 else "f64"
-        a = torch.empty((n, n), dtype=torch.float64, device=self.device)
+        dims = np.zeros(4, np.int64)
+        ntiles = int(L.lpb_band_dims(g.nx, g.ny, g.nz, dims.ctypes.data))
+        nt = int(dims[1])
+        npad = 32 * nt
+        t = self._tbuf("band_t", (ntiles * 1024,), torch.float64)
         if lv.kind == "weights":
-            getattr(L, f"lpb_coarse_dense_{sfx}")(a.data_ptr(), 1, lv.w.data_ptr(), lv.mcat.data_ptr(),
-                                                  ptr(lv.patch_id), ptr(lv.patch_k), None, lv.mask.data_ptr(),
-                                                  *g.args, st)
+            getattr(L, f"lpb_coarse_band_{sfx}")(t.data_ptr(), 1, lv.w.data_ptr(), lv.mcat.data_ptr(),
+                                                 ptr(lv.patch_id), ptr(lv.patch_k), None, lv.mask.data_ptr(),
+                                                 *g.args, st)
         else:
-            getattr(L, f"lpb_coarse_dense_{sfx}")(a.data_ptr(), 2, None, None, None, None, lv.k.data_ptr(),
-                                                  lv.mask.data_ptr(), *g.args, st)
-        # the dense inverse on the device, once per hierarchy (cuSOLVER potrf + potri); the
-        # V-cycle applies it with this package's GEMV kernel
-        lw = int(L.lpb_coarse_inverse_work(n))
-        work = self._flat_buf("coarse_work", lw, torch.float64)
-        info = self._flat_buf("coarse_info", 2, torch.int32)
-        L.lpb_coarse_inverse(a.data_ptr(), n, work.data_ptr(), lw, info.data_ptr(), st)
-        if bool((info[:2] != 0).any().item()):
-            return False
-        self._coarse = {"ainv": a, "v": torch.zeros(n, dtype=torch.float64, device=self.device), "n": n}
-        return True
+            getattr(L, f"lpb_coarse_band_{sfx}")(t.data_ptr(), 2, None, None, None, None, lv.k.data_ptr(),
+                                                 lv.mask.data_ptr(), *g.args, st)
+        linv = self._tbuf("band_linv", (nt * 1024,), torch.float64)
+        info = self._tbuf("band_info", (2,), torch.int32)
+        bar = self._tbuf("band_bar", (64,), torch.int32)
+        L.lpb_memset_async(info.data_ptr(), 0, 8, st)
+        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
+                          *g.args, st)
+        ainv = self._tbuf("band_ainv", (npad, npad), torch.float64)
+        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *g.args, st)
+        self._coarse = {"ainv": ainv, "v": self._tbuf("coarse_v", (npad,), torch.float64), "n": n}
+        return info
 
     def _op(self, i):
         return self._l0s if i == 0 else self.levels[i]
 
     def _estimate_lmax(self, i, its=12):
-        """Largest eigenvalue of D^-1 A by power iteration, times 1.3 (loadpath/mg.py:771-794)."""
+        """Largest eigenvalue of D^-1 A by power iteration, times 1.3, and the Chebyshev
+        coefficients from it, all on the device (loadpath/mg.py:771-794). The vector is
+        warm-started from the last hierarchy's, as the reference does."""
         L = lib()
         st = stream_handle()
         lv = self._op(i)
@@ -509,30 +630,29 @@ class GridElasticity:
         sfx = "f32" if dt == torch.float32 else "f64"
         v = self._buf(f"pw_v{i}", g, dt)
         av = self._buf(f"pw_av{i}", g, dt)
-        prev = self._lmax_vec.get(i)
-        if prev is not None and prev.shape == v.shape and prev.dtype == dt:
-            src = prev
-        else:
+        keep = self._buf(f"pw_keep{i}", g, dt)
+        if self._lmax_init.get(i) != (tuple(keep.shape), dt):
             rng = np.random.default_rng(i)
             host = (rng.random(lv.node_shape) - 0.5).astype(np.float32 if dt == torch.float32 else np.float64)
-            src = g.nodes_to_dev(host, dt)
-        getattr(L, f"lpb_mask_field_{sfx}")(v.data_ptr(), src.data_ptr(), lv.mask.data_ptr(), *g.args, 0, st)
+            g.nodes_to_dev(host, dt, out=keep)
+            self._lmax_init[i] = (tuple(keep.shape), dt)
+        getattr(L, f"lpb_mask_field_{sfx}")(v.data_ptr(), keep.data_ptr(), lv.mask.data_ptr(), *g.args, 0, st)
         n = g.n_node_field
-        sc = self._scal
+        pw = self._pw[32 * i:32 * (i + 1)]
         for it in range(its):
             getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), v.data_ptr(), n, self._part.data_ptr(),
-                                         sc[it].data_ptr(), st)
-            getattr(L, f"lpb_scale_rsqrt_{sfx}")(v.data_ptr(), n, sc[it].data_ptr(), st)
+                                         pw[it:].data_ptr(), st)
+            getattr(L, f"lpb_scale_rsqrt_{sfx}")(v.data_ptr(), n, pw[it:].data_ptr(), st)
             lv.apply(av, v)
             getattr(L, f"lpb_dinv_mask_{sfx}")(av.data_ptr(), lv.dinv.data_ptr(), lv.mask.data_ptr(), *g.args, st)
             getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), av.data_ptr(), n, self._part.data_ptr(),
-                                         sc[16 + it].data_ptr(), st)
+                                         pw[16 + it:].data_ptr(), st)
             v, av = av, v
-        vals = sc[:32].cpu().numpy()
-        self._lmax_vec[i] = v.clone()
-        if np.any(vals[:its] == 0):
-            return 2.0
-        return LMAX_SAFETY * max(float(vals[16 + its - 1]), 1e-12)
+        # the final vector is kept for the next hierarchy (already masked)
+        getattr(L, f"lpb_mask_field_{sfx}")(keep.data_ptr(), v.data_ptr(), lv.mask.data_ptr(), *g.args, 0, st)
+        lv.coef = self._coef[16 * i:16 * (i + 1)]
+        L.lpb_cheb_coef(lv.coef.data_ptr(), pw.data_ptr(), pw[16:].data_ptr(), its, max(self.degree, 1),
+                        LMAX_SAFETY, st)
 
     # --- V-cycle (loadpath/mg.py:796-864) -----------------------------------------------
     def _smooth(self, i, b, x, from_zero):
@@ -557,27 +677,20 @@ class GridElasticity:
                     getattr(L, f"lpb_jacobi_{sfx}")(x.data_ptr(), b.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(), om,
                                                     0, n, st)
             return x
-        hi = lv.lmax
-        lo = hi / 30.0
-        theta = 0.5 * (hi + lo)
-        delta = 0.5 * (hi - lo)
-        sigma = theta / delta
-        rho = 1.0 / sigma
+        coef = lv.coef.data_ptr()
         if from_zero:
-            getattr(L, f"lpb_cheb_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), 1.0 / theta, x.data_ptr(),
-                                                r.data_ptr(), d.data_ptr(), n, st)
+            getattr(L, f"lpb_cheb_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), coef, x.data_ptr(), r.data_ptr(),
+                                                d.data_ptr(), n, st)
         else:
             lv.apply(t, x)
-            getattr(L, f"lpb_residual_scaled_{sfx}")(b.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(), 1.0 / theta,
+            getattr(L, f"lpb_residual_scaled_{sfx}")(b.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(), coef,
                                                      r.data_ptr(), d.data_ptr(), n, st)
         for it in range(self.degree):
             last = it + 1 == self.degree
             if not last:
                 lv.apply(t, d)
-            rho_new = 1.0 / (2.0 * sigma - rho)
             getattr(L, f"lpb_cheb_{sfx}")(x.data_ptr(), d.data_ptr(), r.data_ptr(), (d if last else t).data_ptr(),
-                                          lv.dinv.data_ptr(), rho_new * rho, 2.0 * rho_new / delta, int(last), n, st)
-            rho = rho_new
+                                          lv.dinv.data_ptr(), coef, it, int(last), n, st)
         return x
 
     def _vcycle(self, i, b):
@@ -592,8 +705,8 @@ class GridElasticity:
         if i == len(self.levels) - 1:
             if self._coarse is not None:
                 c = self._coarse
-                getattr(L, f"lpb_coarse_solve_{sfx}")(x.data_ptr(), b.data_ptr(), c["ainv"].data_ptr(),
-                                                      c["v"].data_ptr(), *g.args, st)
+                getattr(L, f"lpb_band_solve_{sfx}")(x.data_ptr(), b.data_ptr(), c["ainv"].data_ptr(),
+                                                    c["v"].data_ptr(), *g.args, st)
                 return x
             self._smooth(i, b, x, True)
             return self._smooth(i, b, x, False)
@@ -633,122 +746,177 @@ class GridElasticity:
         lib().lpb_dot_f64(a.data_ptr(), b.data_ptr(), a.numel(), self._part.data_ptr(),
                           self._scal[slot].data_ptr(), stream_handle())
 
-    def _pcg_device(self, b, x0):
-        """float64 PCG on padded device fields. Returns (x, iterations, converged)."""
+    def _solve_buffers(self):
+        """Every buffer a solve's launches name, created before any capture (a capture must
+        not allocate) and then reused, so captured graphs stay valid across solves."""
+        g = self.g0
+        for k in ("cg_x", "cg_r", "cg_p", "cg_ap", "cg_z", "cg_rs"):
+            self._buf(k, g, torch.float64)
+        if self.tdtype == torch.float32:
+            self._buf("cg_r32", g, torch.float32)
+        self._buf("b0", g, self.tdtype)
+        for i in range(len(self.levels)):
+            gi = self._op(i).grid
+            for k in ("x", "r", "d", "t"):
+                self._buf(f"{k}{i}", gi, self.tdtype)
+            if i + 1 < len(self.levels):
+                self._buf(f"b{i + 1}", self._op(i + 1).grid, self.tdtype)
+
+    def _graph(self, key, fn):
+        """fn's launches captured as one CUDA graph, kept until a buffer it names is replaced
+        (a new allocation or a new hierarchy structure) or the probe changes. Returns
+        (exec, probe event pairs recorded by each replay)."""
         L = lib()
-        st = stream_handle()
+        cache = self._gcache
+        probe = _PROBE[0]
+        sig = (self._gen, id(probe))
+        if cache.get("sig") != sig:
+            self._free_graphs()
+            cache["sig"] = sig
+        if key not in cache:
+            pairs = []
+            if probe is not None:
+                probe.capture = pairs
+            gen = self._gen
+            c0 = launches()
+            # captured on a side stream (the legacy default stream cannot be captured), launched
+            # on the working stream
+            with torch.cuda.stream(self._cap_stream):
+                st0 = stream_handle()
+                L.lpb_capture_begin(st0)
+                try:
+                    fn()
+                finally:
+                    exec_ = ctypes.c_void_p()
+                    L.lpb_capture_end(st0, ctypes.byref(exec_))
+                    if probe is not None:
+                        probe.capture = None
+            nk = launches() - c0
+            add_launches(-nk)              # recorded, not run
+            if self._gen != gen:
+                L.lpb_graph_free(exec_)
+                raise RuntimeError("a buffer was allocated during a graph capture")
+            cache[key] = (exec_, pairs, nk)
+        return cache[key]
+
+    def _replay(self, entry):
+        """Launch a cached graph on the working stream (its kernels join the launch count)."""
+        lib().lpb_graph_launch(entry[0], stream_handle())
+        add_launches(entry[2])
+
+    def _pcg_device(self, b, x0):
+        """float64 PCG on padded device fields (loadpath/mg.py:872-926). Returns (x, iterations,
+        converged). Nothing waits on the host before the first iteration: the warm-start
+        choice is made on the device, and |b| reaches the host with the first iteration's
+        scalars. With graphs on, the set-up, the CG head (A p, alpha, x, r, |r|^2) and the CG
+        tail (V-cycle, beta, p) are each one graph launch."""
+        L = lib()
         g = self.g0
         n = g.n_node_field
         a = self.levels[0]
         sc = self._scal
+        self._solve_buffers()
         x = self._buf("cg_x", g, torch.float64)
         r = self._buf("cg_r", g, torch.float64)
         p = self._buf("cg_p", g, torch.float64)
         ap = self._buf("cg_ap", g, torch.float64)
         z = self._buf("cg_z", g, torch.float64)
-        self._dot64(b, b, 0)
-        bnorm = math.sqrt(float(sc[0].item()))
-        if bnorm == 0:
-            x.zero_()
-            return x, 0, True
-        r.copy_(b)
-        if x0 is not None:
-            x.copy_(x0)
-            a.apply(ap, x)
-            self._dot64(x, ap, 5)
-            self._dot64(b, x, 6)
-            xax, bx = (float(v) for v in sc[5:7].cpu().numpy())
-            s = bx / xax if xax > 0 else 0.0
-            if s > 0:
-                L.lpb_axpby_f64(z.data_ptr(), 1.0, b.data_ptr(), -s, ap.data_ptr(), n, st)
-                self._dot64(z, z, 7)
-                if math.sqrt(float(sc[7].item())) < bnorm:
-                    L.lpb_axpby_f64(x.data_ptr(), s, x.data_ptr(), 0.0, None, n, st)
-                    r.copy_(z)
-                else:
-                    x.zero_()
-            else:
-                x.zero_()
-        else:
-            x.zero_()
-        self.precondition_device(r, z)
-        p.copy_(z)
-        self._dot64(r, z, 1)
-        tol = self.rtol * bnorm
+        rs = self._buf("cg_rs", g, torch.float64)
         r32 = self._buf("cg_r32", g, torch.float32) if self.tdtype == torch.float32 else None
         host = self._host
+        nb = 8 * n
+        src = self._buf("cg_b", g, torch.float64)
+        if b.data_ptr() != src.data_ptr():
+            L.lpb_memcpy_async(src.data_ptr(), b.data_ptr(), nb, stream_handle())
+        if x0 is not None:
+            L.lpb_memcpy_async(x.data_ptr(), x0.data_ptr(), nb, stream_handle())
+
+        def pre(warm):
+            st = stream_handle()
+            self._dot64(src, src, 0)
+            if warm:
+                a.apply(ap, x)
+                self._dot64(x, ap, 5)
+                self._dot64(src, x, 6)
+                L.lpb_warm_residual(rs.data_ptr(), src.data_ptr(), ap.data_ptr(), sc.data_ptr(), n, st)
+                self._dot64(rs, rs, 7)
+                L.lpb_warm_select(x.data_ptr(), r.data_ptr(), src.data_ptr(), rs.data_ptr(), sc.data_ptr(), n, st)
+            else:
+                L.lpb_memset_async(x.data_ptr(), 0, nb, st)
+                L.lpb_memcpy_async(r.data_ptr(), src.data_ptr(), nb, st)
+            self.precondition_device(r, z)
+            L.lpb_memcpy_async(p.data_ptr(), z.data_ptr(), nb, st)
+            self._dot64(r, z, 1)
 
         def head():
             # ap = A p; pap; x += alpha p; r -= alpha ap (and its float32 copy); |r|^2; scalars out
+            st = stream_handle()
             a.apply(ap, p)
             self._dot64(p, ap, 3)
             L.lpb_cg_step(x.data_ptr(), r.data_ptr(), p.data_ptr(), ap.data_ptr(), ptr(r32), n,
-                          sc[1].data_ptr(), sc[3].data_ptr(), self._part.data_ptr(), sc[4].data_ptr(),
-                          stream_handle())
-            L.lpb_memcpy_async(host.data_ptr(), sc[3:5].data_ptr(), 16, stream_handle())
+                          sc[1].data_ptr(), sc[3].data_ptr(), self._part.data_ptr(), sc[4].data_ptr(), st)
+            L.lpb_memcpy_async(host.data_ptr(), sc[3:5].data_ptr(), 16, st)
+            L.lpb_memcpy_async(host[2:].data_ptr(), sc[0:1].data_ptr(), 8, st)
 
         def tail():
             # z = V(r); rz_new; p = z + (rz_new / rz) p; rz = rz_new
+            st = stream_handle()
             if r32 is not None:
                 xv = self._vcycle(0, r32)
-                L.lpb_dot_f64_f32(r.data_ptr(), xv.data_ptr(), n, self._part.data_ptr(), sc[2].data_ptr(),
-                                  stream_handle())
-                L.lpb_xpby_f32(p.data_ptr(), xv.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), stream_handle())
+                L.lpb_dot_f64_f32(r.data_ptr(), xv.data_ptr(), n, self._part.data_ptr(), sc[2].data_ptr(), st)
+                L.lpb_xpby_f32(p.data_ptr(), xv.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), st)
             else:
                 self.precondition_device(r, z)
                 self._dot64(r, z, 2)
-                L.lpb_xpby_f64(p.data_ptr(), z.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), stream_handle())
-            L.lpb_memcpy_async(sc[1:2].data_ptr(), sc[2:3].data_ptr(), 8, stream_handle())
+                L.lpb_xpby_f64(p.data_ptr(), z.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), st)
+            L.lpb_memcpy_async(sc[1:2].data_ptr(), sc[2:3].data_ptr(), 8, st)
 
-        graphs = None
+        warm = x0 is not None
         probe = _PROBE[0]
-        gpairs = [[], []]
-        if self.use_graphs and self.maxiter > 1:
-            # one capture per solve: buffers and smoother coefficients are fixed within it
-            self._free_graphs()
-            graphs = []
-            # captured on a side stream (the legacy default stream cannot be captured), launched
-            # on the working stream
-            for gi, fn in enumerate((head, tail)):
-                if probe is not None:
-                    probe.capture = gpairs[gi]
-                with torch.cuda.stream(self._cap_stream):
-                    st0 = stream_handle()
-                    L.lpb_capture_begin(st0)
-                    try:
-                        fn()
-                    finally:
-                        exec_ = ctypes.c_void_p()
-                        L.lpb_capture_end(st0, ctypes.byref(exec_))
-                        if probe is not None:
-                            probe.capture = None
-                graphs.append(exec_)
-            self._graphs = graphs      # freed at the next capture
+        graphed = self.use_graphs and self.maxiter > 1
+        if graphed:
+            g_pre = self._graph(("pre", warm), lambda: pre(warm))
+            g_head = self._graph("head", head)
+            g_tail = self._graph("tail", tail)
+            pre_pairs, head_pairs, tail_pairs = g_pre[1], g_head[1], g_tail[1]
+            self._replay(g_pre)
+        else:
+            pre(warm)
         ev = torch.cuda.Event()
 
         def finish(result):
-            if graphs is not None and probe is not None:
+            if graphed and probe is not None:
                 torch.cuda.current_stream().synchronize()
-                probe.harvest(gpairs[1])          # the last (speculative) tail replay
+                probe.harvest(tail_pairs)          # the last (speculative) tail replay
             return result
 
+        tol = None
         for it in range(1, self.maxiter + 1):
-            if graphs is not None:
-                L.lpb_graph_launch(graphs[0], stream_handle())
+            if graphed:
+                self._replay(g_head)
             else:
                 head()
             ev.record()
             # the next preconditioner step is queued before the host looks at |r|: the
             # device never waits on the convergence test (a converged solve discards it)
-            if graphs is not None:
-                L.lpb_graph_launch(graphs[1], stream_handle())
+            if graphed:
+                self._replay(g_tail)
             else:
                 tail()
             ev.synchronize()
-            if graphs is not None and probe is not None:
+            if graphed and probe is not None:
                 # this head replay is complete and the next is not launched yet; a tail replay
                 # may be re-recording its events now, so tails are read once, at the end
-                probe.harvest(gpairs[0])
+                if it == 1:
+                    probe.harvest(pre_pairs)
+                probe.harvest(head_pairs)
+            if tol is None:
+                bb = float(host[2])
+                if bb == 0.0:
+                    torch.cuda.current_stream().synchronize()
+                    L.lpb_memset_async(x.data_ptr(), 0, nb, stream_handle())
+                    return finish((x, 0, True))
+                tol = self.rtol * math.sqrt(bb)
             pap, rr = float(host[0]), float(host[1])
             if not pap > 0:
                 return finish((x, it, False))
@@ -780,7 +948,7 @@ class GridElasticity:
         st = stream_handle()
         g = self.g0
         m = self.levels[0].mask
-        bm = self._buf("solve_b", g, torch.float64)
+        bm = self._buf("cg_b", g, torch.float64)
         L.lpb_mask_field_f64(bm.data_ptr(), b.data_ptr(), m.data_ptr(), *g.args, 0, st)
         x0m = None
         if x0 is not None:
@@ -845,11 +1013,12 @@ class GridElasticity:
         return se[tuple(self.elem_ijk.T)]
 
     def _free_graphs(self):
-        if self._graphs:
+        execs = [v[0] for k, v in self._gcache.items() if k != "sig"]
+        if execs:
             torch.cuda.current_stream().synchronize()
-            for gexec in self._graphs:
+            for gexec in execs:
                 lib().lpb_graph_free(gexec)
-        self._graphs = None
+        self._gcache = {}
 
     def __del__(self):
         try:

@@ -59,3 +59,17 @@ def test_modal_ke_pattern_host_only():
         raise AssertionError("a matrix outside the pattern must be rejected")
     except RuntimeError:
         pass
+
+
+def test_band_layout_host_only():
+    """lpb_band_dims (host code): the coarsest level's band numbering puts the longest node axis
+    slowest, so the half-bandwidth is 3 (N1 N2 + N2 + 1) + 2 over the two shorter extents."""
+    L = lib()
+    for cells, (n1, n2) in (((16, 8, 8), (9, 9)), ((8, 16, 8), (9, 9)), ((6, 4, 10), (7, 5)), ((1, 1, 1), (2, 2))):
+        out = np.zeros(4, np.int64)
+        ntiles = L.lpb_band_dims(*cells, out.ctypes.data)
+        n = 3 * int(np.prod(np.asarray(cells) + 1))
+        bw = 3 * (n1 * n2 + n2 + 1) + 2
+        nt, d = (n + 31) // 32, (bw + 31) // 32
+        assert tuple(int(v) for v in out) == (n, nt, d, bw)
+        assert ntiles == nt * (d + 1)

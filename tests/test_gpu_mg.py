@@ -162,3 +162,57 @@ def ge_fixed(mesh, fixed_grid):
     for i in range(3):
         out[i::3] = flat[i]
     return out
+
+
+@pytest.mark.parametrize("name", ["deep_im", "odd_plain"])
+def test_band_direct_solve_matches_dense(name):
+    """The coarsest level's band Cholesky + inverse against numpy on the dense operator the same
+    level assembles (lpb_coarse_dense_*), float64 to 1e-10 relative."""
+    from loadpath_b200._lib import lib
+    from loadpath_b200.grid import ptr, stream_handle
+
+    g, ge = _ge(name)
+    lv = ge.levels[-1]
+    gr = lv.grid
+    L = lib()
+    n = 3 * gr.NX * gr.NY * gr.NZ
+    a = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    sfx = "f32"
+    if lv.kind == "weights":
+        L.lpb_coarse_dense_f32(a.data_ptr(), 1, lv.w.data_ptr(), lv.mcat.data_ptr(), ptr(lv.patch_id),
+                               ptr(lv.patch_k), None, lv.mask.data_ptr(), *gr.args, stream_handle())
+    else:
+        L.lpb_coarse_dense_f32(a.data_ptr(), 2, None, None, None, None, lv.k.data_ptr(), lv.mask.data_ptr(),
+                               *gr.args, stream_handle())
+    dense = a.cpu().numpy()
+    rng = np.random.default_rng(3)
+    for _ in range(2):
+        b = rng.standard_normal(gr.node_shape).astype(np.float32)
+        bd = gr.nodes_to_dev(b, torch.float32)
+        xd = gr.node_field(torch.float32)
+        c = ge._coarse
+        getattr(L, f"lpb_band_solve_{sfx}")(xd.data_ptr(), bd.data_ptr(), c["ainv"].data_ptr(), c["v"].data_ptr(),
+                                           *gr.args, stream_handle())
+        got = gr.nodes_to_host(xd).astype(np.float64).reshape(-1)
+        want = np.linalg.solve(dense, b.astype(np.float64).reshape(-1))
+        np.testing.assert_allclose(got, want, rtol=2e-6, atol=2e-6 * np.abs(want).max())
+    # the inverse itself, in float64
+    c = ge._coarse
+    ainv = c["ainv"].cpu().numpy()
+    dims = np.zeros(4, np.int64)
+    L.lpb_band_dims(gr.nx, gr.ny, gr.nz, dims.ctypes.data)
+    # band numbering -> the dense (component-major) numbering
+    ext = np.array([gr.NX, gr.NY, gr.NZ])
+    perm = np.argsort(-ext, kind="stable")
+    idx = np.arange(n)
+    node_b, comp = idx // 3, idx % 3
+    p2 = node_b % ext[perm[2]]
+    q = node_b // ext[perm[2]]
+    p1, p0 = q % ext[perm[1]], q // ext[perm[1]]
+    coords = np.zeros((3, n), np.int64)
+    coords[perm[0]], coords[perm[1]], coords[perm[2]] = p0, p1, p2
+    dense_idx = comp * (gr.NX * gr.NY * gr.NZ) + (coords[0] * gr.NY + coords[1]) * gr.NZ + coords[2]
+    inv_dense = np.linalg.inv(dense)
+    got_inv = ainv[:n, :n]
+    want_inv = inv_dense[np.ix_(dense_idx, dense_idx)]
+    np.testing.assert_allclose(got_inv, want_inv, rtol=1e-9, atol=1e-10 * np.abs(want_inv).max())
