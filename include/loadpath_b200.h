@@ -58,6 +58,15 @@ int lpb_modal_ke(const double* ke, double* kmodal_out);
 int lpb_modal_g1(const double* ke, double* g1_out);
 int lpb_apply_weights_march_f32(float* out, const float* u, const float* w, const int* patch_id, const float* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, const int* patch_id, const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* level 1, TMA-staged: the Walsh coefficients c = H w of each cell's child moduli in the
+ * layout (nx, ny, cpz/4, 8, 4) from lpb_walsh_chunks_* (once per hierarchy, after the patch
+ * cells' weights are zeroed), then the march with u arriving by TMA box loads into a 3-stage
+ * mbarrier ring and outputs leaving by TMA stores; g1, pbox HOST; err: device int, set when a
+ * bounded wait gave up (or to an alignment code 20..25) */
+int lpb_walsh_chunks_f32(float* wc, const float* w, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_walsh_chunks_f64(double* wc, const double* w, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_weights_tma_f32(float* out, const float* u, const float* wc, const int* patch_id, const float* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_apply_weights_tma_f64(double* out, const double* u, const double* wc, const int* patch_id, const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* lpb_apply_explicit_sym_f32 for callers that cannot allocate device memory (a host that owns
@@ -105,6 +114,11 @@ int lpb_patch_matrices_f32(float* pk, float* w, int* patch_id, const long long* 
 int lpb_patch_matrices_f64(double* pk, double* w, int* patch_id, const long long* pcells, int npatch, const double* e, const double* ke, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
 int lpb_galerkin_explicit_f32(float* kout, int fine_kind, const float* fw, const float* mcat, const int* patch_id, const float* patch_k, const float* fk, const uint8_t* mf, int strict, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
 int lpb_galerkin_explicit_f64(double* kout, int fine_kind, const double* fw, const double* mcat, const int* patch_id, const double* patch_k, const double* fk, const uint8_t* mf, int strict, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+/* level-2 Galerkin matrices from level-1 weights in the plain hierarchy, as 64 fixed products:
+ * K(C) = sum_(k,q) w_(k,q) N_(k,q), N_(k,q) = P_k^T M_q P_k (nkq: 64 x 576, index 8k + q); children
+ * with a patch matrix add P_k^T patch P_k (patch_id / patch_k NULL when there are none) */
+int lpb_galerkin_w2_f32(float* kout, const float* w1, const float* nkq, const int* patch_id, const float* patch_k, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
+int lpb_galerkin_w2_f64(double* kout, const double* w1, const double* nkq, const int* patch_id, const double* patch_k, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
 /* strict hierarchy: held dofs injected down a level and restrict(fine mask) (loadpath/mg.py:562-574) */
 int lpb_strict_held_kept(uint8_t* held_c, float* kept, const uint8_t* held_f, const uint8_t* mf, int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz, void* stream);
 int lpb_held0(uint8_t* held, const uint8_t* mask0, const uint8_t* fixed_bits, long long n, void* stream);
@@ -145,6 +159,16 @@ int lpb_residual_scaled_f32(const float* b, const float* ax, const float* dinv, 
 int lpb_residual_scaled_f64(const double* b, const double* ax, const double* dinv, const double* coef, double* r, double* d, long long n, void* stream);
 int lpb_cheb_f32(float* x, float* d, float* r, const float* ad, const float* dinv, const double* coef, int step, int last, long long n, void* stream);
 int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double* dinv, const double* coef, int step, int last, long long n, void* stream);
+/* degree-2 Chebyshev in two passes per smoothing (same bits as two lpb_cheb_* steps): from
+ * zero, lpb_cheb_d_start (d = s dinv b), then with ad = A d lpb_cheb2_zero (x = d + d');
+ * otherwise after lpb_residual_scaled and ad = A d, lpb_cheb2 (x = (x + d) + d'), where
+ * d' = c1 d + c2 dinv (r - ad) with step 0's coefficients */
+int lpb_cheb_d_start_f32(const float* b, const float* dinv, const double* coef, float* d, long long n, void* stream);
+int lpb_cheb_d_start_f64(const double* b, const double* dinv, const double* coef, double* d, long long n, void* stream);
+int lpb_cheb2_zero_f32(float* x, const float* b, const float* ad, const float* d, const float* dinv, const double* coef, long long n, void* stream);
+int lpb_cheb2_zero_f64(double* x, const double* b, const double* ad, const double* d, const double* dinv, const double* coef, long long n, void* stream);
+int lpb_cheb2_f32(float* x, const float* d, const float* r, const float* ad, const float* dinv, const double* coef, long long n, void* stream);
+int lpb_cheb2_f64(double* x, const double* d, const double* r, const double* ad, const double* dinv, const double* coef, long long n, void* stream);
 int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero, long long n, void* stream);
 int lpb_jacobi_f64(double* x, const double* b, const double* ax, const double* dinv, double omega, int from_zero, long long n, void* stream);
 

@@ -16,6 +16,7 @@
 // Two passes: a cell pass forms the 24 corner forces f_c = K_c u_c into a caller-provided
 // (24, cells) buffer, a node pass sums each node's eight cells' rows and applies the mask.
 #include "lp_common.cuh"
+#include "lp_tma.cuh"
 
 #include <mutex>
 
@@ -209,6 +210,203 @@ __device__ __forceinline__ void g1_product(const G1<T>& g, const T (&c)[8], cons
          + c[7] * (g.c[277] * v[15] + g.c[278] * v[19]);
 }
 
+// row r of the level-1 modal product (the rows g1_product forms together), so a caller can
+// consume each row as it is produced
+template <int R, typename T>
+__device__ __forceinline__ T g1_row(const G1<T>& g, const T (&c)[8], const T (&v)[24]);
+template <>
+__device__ __forceinline__ float g1_row<0, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return 0.0f;
+}
+template <>
+__device__ __forceinline__ double g1_row<0, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return 0.0;
+}
+template <>
+__device__ __forceinline__ float g1_row<1, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return 0.0f;
+}
+template <>
+__device__ __forceinline__ double g1_row<1, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return 0.0;
+}
+template <>
+__device__ __forceinline__ float g1_row<2, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return 0.0f;
+}
+template <>
+__device__ __forceinline__ double g1_row<2, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return 0.0;
+}
+template <>
+__device__ __forceinline__ float g1_row<3, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[0] * v[3] + g.c[1] * v[7] + g.c[2] * v[14]) + c[1] * (g.c[3] * v[10] + g.c[4] * v[17]) + c[2] * (g.c[5] * v[9] + g.c[6] * v[20]) + c[3] * (g.c[7] * v[23]) + c[4] * (g.c[8] * v[15] + g.c[9] * v[19]) + c[5] * (g.c[10] * v[22]) + c[6] * (g.c[11] * v[21]);
+}
+template <>
+__device__ __forceinline__ double g1_row<3, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[0] * v[3] + g.c[1] * v[7] + g.c[2] * v[14]) + c[1] * (g.c[3] * v[10] + g.c[4] * v[17]) + c[2] * (g.c[5] * v[9] + g.c[6] * v[20]) + c[3] * (g.c[7] * v[23]) + c[4] * (g.c[8] * v[15] + g.c[9] * v[19]) + c[5] * (g.c[10] * v[22]) + c[6] * (g.c[11] * v[21]);
+}
+template <>
+__device__ __forceinline__ float g1_row<4, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[12] * v[4] + g.c[13] * v[6]) + c[1] * (g.c[14] * v[9]) + c[2] * (g.c[15] * v[10]) + c[4] * (g.c[16] * v[16] + g.c[17] * v[18]) + c[5] * (g.c[18] * v[21]) + c[6] * (g.c[19] * v[22]);
+}
+template <>
+__device__ __forceinline__ double g1_row<4, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[12] * v[4] + g.c[13] * v[6]) + c[1] * (g.c[14] * v[9]) + c[2] * (g.c[15] * v[10]) + c[4] * (g.c[16] * v[16] + g.c[17] * v[18]) + c[5] * (g.c[18] * v[21]) + c[6] * (g.c[19] * v[22]);
+}
+template <>
+__device__ __forceinline__ float g1_row<5, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[20] * v[5] + g.c[21] * v[12]) + c[1] * (g.c[22] * v[15]) + c[2] * (g.c[23] * v[11] + g.c[24] * v[18]) + c[3] * (g.c[25] * v[21]) + c[4] * (g.c[26] * v[17]) + c[6] * (g.c[27] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<5, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[20] * v[5] + g.c[21] * v[12]) + c[1] * (g.c[22] * v[15]) + c[2] * (g.c[23] * v[11] + g.c[24] * v[18]) + c[3] * (g.c[25] * v[21]) + c[4] * (g.c[26] * v[17]) + c[6] * (g.c[27] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<6, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[28] * v[4] + g.c[29] * v[6]) + c[1] * (g.c[30] * v[9]) + c[2] * (g.c[31] * v[10]) + c[4] * (g.c[32] * v[16] + g.c[33] * v[18]) + c[5] * (g.c[34] * v[21]) + c[6] * (g.c[35] * v[22]);
+}
+template <>
+__device__ __forceinline__ double g1_row<6, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[28] * v[4] + g.c[29] * v[6]) + c[1] * (g.c[30] * v[9]) + c[2] * (g.c[31] * v[10]) + c[4] * (g.c[32] * v[16] + g.c[33] * v[18]) + c[5] * (g.c[34] * v[21]) + c[6] * (g.c[35] * v[22]);
+}
+template <>
+__device__ __forceinline__ float g1_row<7, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[36] * v[3] + g.c[37] * v[7] + g.c[38] * v[14]) + c[1] * (g.c[39] * v[10] + g.c[40] * v[17]) + c[2] * (g.c[41] * v[9] + g.c[42] * v[20]) + c[3] * (g.c[43] * v[23]) + c[4] * (g.c[44] * v[15] + g.c[45] * v[19]) + c[5] * (g.c[46] * v[22]) + c[6] * (g.c[47] * v[21]);
+}
+template <>
+__device__ __forceinline__ double g1_row<7, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[36] * v[3] + g.c[37] * v[7] + g.c[38] * v[14]) + c[1] * (g.c[39] * v[10] + g.c[40] * v[17]) + c[2] * (g.c[41] * v[9] + g.c[42] * v[20]) + c[3] * (g.c[43] * v[23]) + c[4] * (g.c[44] * v[15] + g.c[45] * v[19]) + c[5] * (g.c[46] * v[22]) + c[6] * (g.c[47] * v[21]);
+}
+template <>
+__device__ __forceinline__ float g1_row<8, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[48] * v[8] + g.c[49] * v[13]) + c[1] * (g.c[50] * v[11] + g.c[51] * v[16]) + c[2] * (g.c[52] * v[19]) + c[3] * (g.c[53] * v[22]) + c[4] * (g.c[54] * v[20]) + c[5] * (g.c[55] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<8, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[48] * v[8] + g.c[49] * v[13]) + c[1] * (g.c[50] * v[11] + g.c[51] * v[16]) + c[2] * (g.c[52] * v[19]) + c[3] * (g.c[53] * v[22]) + c[4] * (g.c[54] * v[20]) + c[5] * (g.c[55] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<9, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[56] * v[9] + g.c[57] * v[20]) + c[1] * (g.c[58] * v[4] + g.c[59] * v[6] + g.c[60] * v[23]) + c[2] * (g.c[61] * v[3] + g.c[62] * v[7] + g.c[63] * v[14]) + c[3] * (g.c[64] * v[10] + g.c[65] * v[17]) + c[4] * (g.c[66] * v[21]) + c[5] * (g.c[67] * v[16] + g.c[68] * v[18]) + c[6] * (g.c[69] * v[15] + g.c[70] * v[19]) + c[7] * (g.c[71] * v[22]);
+}
+template <>
+__device__ __forceinline__ double g1_row<9, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[56] * v[9] + g.c[57] * v[20]) + c[1] * (g.c[58] * v[4] + g.c[59] * v[6] + g.c[60] * v[23]) + c[2] * (g.c[61] * v[3] + g.c[62] * v[7] + g.c[63] * v[14]) + c[3] * (g.c[64] * v[10] + g.c[65] * v[17]) + c[4] * (g.c[66] * v[21]) + c[5] * (g.c[67] * v[16] + g.c[68] * v[18]) + c[6] * (g.c[69] * v[15] + g.c[70] * v[19]) + c[7] * (g.c[71] * v[22]);
+}
+template <>
+__device__ __forceinline__ float g1_row<10, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[72] * v[10] + g.c[73] * v[17]) + c[1] * (g.c[74] * v[3] + g.c[75] * v[7] + g.c[76] * v[14]) + c[2] * (g.c[77] * v[4] + g.c[78] * v[6] + g.c[79] * v[23]) + c[3] * (g.c[80] * v[9] + g.c[81] * v[20]) + c[4] * (g.c[82] * v[22]) + c[5] * (g.c[83] * v[15] + g.c[84] * v[19]) + c[6] * (g.c[85] * v[16] + g.c[86] * v[18]) + c[7] * (g.c[87] * v[21]);
+}
+template <>
+__device__ __forceinline__ double g1_row<10, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[72] * v[10] + g.c[73] * v[17]) + c[1] * (g.c[74] * v[3] + g.c[75] * v[7] + g.c[76] * v[14]) + c[2] * (g.c[77] * v[4] + g.c[78] * v[6] + g.c[79] * v[23]) + c[3] * (g.c[80] * v[9] + g.c[81] * v[20]) + c[4] * (g.c[82] * v[22]) + c[5] * (g.c[83] * v[15] + g.c[84] * v[19]) + c[6] * (g.c[85] * v[16] + g.c[86] * v[18]) + c[7] * (g.c[87] * v[21]);
+}
+template <>
+__device__ __forceinline__ float g1_row<11, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[88] * v[11] + g.c[89] * v[16] + g.c[90] * v[18]) + c[1] * (g.c[91] * v[8] + g.c[92] * v[13] + g.c[93] * v[21]) + c[2] * (g.c[94] * v[5] + g.c[95] * v[12] + g.c[96] * v[22]) + c[3] * (g.c[97] * v[15] + g.c[98] * v[19]) + c[4] * (g.c[99] * v[23]) + c[5] * (g.c[100] * v[20]) + c[6] * (g.c[101] * v[17]);
+}
+template <>
+__device__ __forceinline__ double g1_row<11, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[88] * v[11] + g.c[89] * v[16] + g.c[90] * v[18]) + c[1] * (g.c[91] * v[8] + g.c[92] * v[13] + g.c[93] * v[21]) + c[2] * (g.c[94] * v[5] + g.c[95] * v[12] + g.c[96] * v[22]) + c[3] * (g.c[97] * v[15] + g.c[98] * v[19]) + c[4] * (g.c[99] * v[23]) + c[5] * (g.c[100] * v[20]) + c[6] * (g.c[101] * v[17]);
+}
+template <>
+__device__ __forceinline__ float g1_row<12, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[102] * v[5] + g.c[103] * v[12]) + c[1] * (g.c[104] * v[15]) + c[2] * (g.c[105] * v[11] + g.c[106] * v[18]) + c[3] * (g.c[107] * v[21]) + c[4] * (g.c[108] * v[17]) + c[6] * (g.c[109] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<12, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[102] * v[5] + g.c[103] * v[12]) + c[1] * (g.c[104] * v[15]) + c[2] * (g.c[105] * v[11] + g.c[106] * v[18]) + c[3] * (g.c[107] * v[21]) + c[4] * (g.c[108] * v[17]) + c[6] * (g.c[109] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<13, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[110] * v[8] + g.c[111] * v[13]) + c[1] * (g.c[112] * v[11] + g.c[113] * v[16]) + c[2] * (g.c[114] * v[19]) + c[3] * (g.c[115] * v[22]) + c[4] * (g.c[116] * v[20]) + c[5] * (g.c[117] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<13, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[110] * v[8] + g.c[111] * v[13]) + c[1] * (g.c[112] * v[11] + g.c[113] * v[16]) + c[2] * (g.c[114] * v[19]) + c[3] * (g.c[115] * v[22]) + c[4] * (g.c[116] * v[20]) + c[5] * (g.c[117] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<14, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[118] * v[3] + g.c[119] * v[7] + g.c[120] * v[14]) + c[1] * (g.c[121] * v[10] + g.c[122] * v[17]) + c[2] * (g.c[123] * v[9] + g.c[124] * v[20]) + c[3] * (g.c[125] * v[23]) + c[4] * (g.c[126] * v[15] + g.c[127] * v[19]) + c[5] * (g.c[128] * v[22]) + c[6] * (g.c[129] * v[21]);
+}
+template <>
+__device__ __forceinline__ double g1_row<14, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[118] * v[3] + g.c[119] * v[7] + g.c[120] * v[14]) + c[1] * (g.c[121] * v[10] + g.c[122] * v[17]) + c[2] * (g.c[123] * v[9] + g.c[124] * v[20]) + c[3] * (g.c[125] * v[23]) + c[4] * (g.c[126] * v[15] + g.c[127] * v[19]) + c[5] * (g.c[128] * v[22]) + c[6] * (g.c[129] * v[21]);
+}
+template <>
+__device__ __forceinline__ float g1_row<15, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[130] * v[15] + g.c[131] * v[19]) + c[1] * (g.c[132] * v[5] + g.c[133] * v[12] + g.c[134] * v[22]) + c[2] * (g.c[135] * v[21]) + c[3] * (g.c[136] * v[11] + g.c[137] * v[18]) + c[4] * (g.c[138] * v[3] + g.c[139] * v[7] + g.c[140] * v[14]) + c[5] * (g.c[141] * v[10] + g.c[142] * v[17]) + c[6] * (g.c[143] * v[9] + g.c[144] * v[20]) + c[7] * (g.c[145] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<15, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[130] * v[15] + g.c[131] * v[19]) + c[1] * (g.c[132] * v[5] + g.c[133] * v[12] + g.c[134] * v[22]) + c[2] * (g.c[135] * v[21]) + c[3] * (g.c[136] * v[11] + g.c[137] * v[18]) + c[4] * (g.c[138] * v[3] + g.c[139] * v[7] + g.c[140] * v[14]) + c[5] * (g.c[141] * v[10] + g.c[142] * v[17]) + c[6] * (g.c[143] * v[9] + g.c[144] * v[20]) + c[7] * (g.c[145] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<16, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[146] * v[11] + g.c[147] * v[16] + g.c[148] * v[18]) + c[1] * (g.c[149] * v[8] + g.c[150] * v[13] + g.c[151] * v[21]) + c[2] * (g.c[152] * v[22]) + c[3] * (g.c[153] * v[19]) + c[4] * (g.c[154] * v[4] + g.c[155] * v[6] + g.c[156] * v[23]) + c[5] * (g.c[157] * v[9] + g.c[158] * v[20]) + c[6] * (g.c[159] * v[10]);
+}
+template <>
+__device__ __forceinline__ double g1_row<16, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[146] * v[11] + g.c[147] * v[16] + g.c[148] * v[18]) + c[1] * (g.c[149] * v[8] + g.c[150] * v[13] + g.c[151] * v[21]) + c[2] * (g.c[152] * v[22]) + c[3] * (g.c[153] * v[19]) + c[4] * (g.c[154] * v[4] + g.c[155] * v[6] + g.c[156] * v[23]) + c[5] * (g.c[157] * v[9] + g.c[158] * v[20]) + c[6] * (g.c[159] * v[10]);
+}
+template <>
+__device__ __forceinline__ float g1_row<17, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[160] * v[10] + g.c[161] * v[17]) + c[1] * (g.c[162] * v[3] + g.c[163] * v[7] + g.c[164] * v[14]) + c[2] * (g.c[165] * v[23]) + c[3] * (g.c[166] * v[9] + g.c[167] * v[20]) + c[4] * (g.c[168] * v[5] + g.c[169] * v[12] + g.c[170] * v[22]) + c[5] * (g.c[171] * v[15] + g.c[172] * v[19]) + c[6] * (g.c[173] * v[11] + g.c[174] * v[18]) + c[7] * (g.c[175] * v[21]);
+}
+template <>
+__device__ __forceinline__ double g1_row<17, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[160] * v[10] + g.c[161] * v[17]) + c[1] * (g.c[162] * v[3] + g.c[163] * v[7] + g.c[164] * v[14]) + c[2] * (g.c[165] * v[23]) + c[3] * (g.c[166] * v[9] + g.c[167] * v[20]) + c[4] * (g.c[168] * v[5] + g.c[169] * v[12] + g.c[170] * v[22]) + c[5] * (g.c[171] * v[15] + g.c[172] * v[19]) + c[6] * (g.c[173] * v[11] + g.c[174] * v[18]) + c[7] * (g.c[175] * v[21]);
+}
+template <>
+__device__ __forceinline__ float g1_row<18, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[176] * v[11] + g.c[177] * v[16] + g.c[178] * v[18]) + c[1] * (g.c[179] * v[21]) + c[2] * (g.c[180] * v[5] + g.c[181] * v[12] + g.c[182] * v[22]) + c[3] * (g.c[183] * v[15]) + c[4] * (g.c[184] * v[4] + g.c[185] * v[6] + g.c[186] * v[23]) + c[5] * (g.c[187] * v[9]) + c[6] * (g.c[188] * v[10] + g.c[189] * v[17]);
+}
+template <>
+__device__ __forceinline__ double g1_row<18, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[176] * v[11] + g.c[177] * v[16] + g.c[178] * v[18]) + c[1] * (g.c[179] * v[21]) + c[2] * (g.c[180] * v[5] + g.c[181] * v[12] + g.c[182] * v[22]) + c[3] * (g.c[183] * v[15]) + c[4] * (g.c[184] * v[4] + g.c[185] * v[6] + g.c[186] * v[23]) + c[5] * (g.c[187] * v[9]) + c[6] * (g.c[188] * v[10] + g.c[189] * v[17]);
+}
+template <>
+__device__ __forceinline__ float g1_row<19, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[190] * v[15] + g.c[191] * v[19]) + c[1] * (g.c[192] * v[22]) + c[2] * (g.c[193] * v[8] + g.c[194] * v[13] + g.c[195] * v[21]) + c[3] * (g.c[196] * v[11] + g.c[197] * v[16]) + c[4] * (g.c[198] * v[3] + g.c[199] * v[7] + g.c[200] * v[14]) + c[5] * (g.c[201] * v[10] + g.c[202] * v[17]) + c[6] * (g.c[203] * v[9] + g.c[204] * v[20]) + c[7] * (g.c[205] * v[23]);
+}
+template <>
+__device__ __forceinline__ double g1_row<19, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[190] * v[15] + g.c[191] * v[19]) + c[1] * (g.c[192] * v[22]) + c[2] * (g.c[193] * v[8] + g.c[194] * v[13] + g.c[195] * v[21]) + c[3] * (g.c[196] * v[11] + g.c[197] * v[16]) + c[4] * (g.c[198] * v[3] + g.c[199] * v[7] + g.c[200] * v[14]) + c[5] * (g.c[201] * v[10] + g.c[202] * v[17]) + c[6] * (g.c[203] * v[9] + g.c[204] * v[20]) + c[7] * (g.c[205] * v[23]);
+}
+template <>
+__device__ __forceinline__ float g1_row<20, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[206] * v[9] + g.c[207] * v[20]) + c[1] * (g.c[208] * v[23]) + c[2] * (g.c[209] * v[3] + g.c[210] * v[7] + g.c[211] * v[14]) + c[3] * (g.c[212] * v[10] + g.c[213] * v[17]) + c[4] * (g.c[214] * v[8] + g.c[215] * v[13] + g.c[216] * v[21]) + c[5] * (g.c[217] * v[11] + g.c[218] * v[16]) + c[6] * (g.c[219] * v[15] + g.c[220] * v[19]) + c[7] * (g.c[221] * v[22]);
+}
+template <>
+__device__ __forceinline__ double g1_row<20, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[206] * v[9] + g.c[207] * v[20]) + c[1] * (g.c[208] * v[23]) + c[2] * (g.c[209] * v[3] + g.c[210] * v[7] + g.c[211] * v[14]) + c[3] * (g.c[212] * v[10] + g.c[213] * v[17]) + c[4] * (g.c[214] * v[8] + g.c[215] * v[13] + g.c[216] * v[21]) + c[5] * (g.c[217] * v[11] + g.c[218] * v[16]) + c[6] * (g.c[219] * v[15] + g.c[220] * v[19]) + c[7] * (g.c[221] * v[22]);
+}
+template <>
+__device__ __forceinline__ float g1_row<21, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[222] * v[21]) + c[1] * (g.c[223] * v[11] + g.c[224] * v[16] + g.c[225] * v[18]) + c[2] * (g.c[226] * v[15] + g.c[227] * v[19]) + c[3] * (g.c[228] * v[5] + g.c[229] * v[12] + g.c[230] * v[22]) + c[4] * (g.c[231] * v[9] + g.c[232] * v[20]) + c[5] * (g.c[233] * v[4] + g.c[234] * v[6] + g.c[235] * v[23]) + c[6] * (g.c[236] * v[3] + g.c[237] * v[7] + g.c[238] * v[14]) + c[7] * (g.c[239] * v[10] + g.c[240] * v[17]);
+}
+template <>
+__device__ __forceinline__ double g1_row<21, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[222] * v[21]) + c[1] * (g.c[223] * v[11] + g.c[224] * v[16] + g.c[225] * v[18]) + c[2] * (g.c[226] * v[15] + g.c[227] * v[19]) + c[3] * (g.c[228] * v[5] + g.c[229] * v[12] + g.c[230] * v[22]) + c[4] * (g.c[231] * v[9] + g.c[232] * v[20]) + c[5] * (g.c[233] * v[4] + g.c[234] * v[6] + g.c[235] * v[23]) + c[6] * (g.c[236] * v[3] + g.c[237] * v[7] + g.c[238] * v[14]) + c[7] * (g.c[239] * v[10] + g.c[240] * v[17]);
+}
+template <>
+__device__ __forceinline__ float g1_row<22, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[241] * v[22]) + c[1] * (g.c[242] * v[15] + g.c[243] * v[19]) + c[2] * (g.c[244] * v[11] + g.c[245] * v[16] + g.c[246] * v[18]) + c[3] * (g.c[247] * v[8] + g.c[248] * v[13] + g.c[249] * v[21]) + c[4] * (g.c[250] * v[10] + g.c[251] * v[17]) + c[5] * (g.c[252] * v[3] + g.c[253] * v[7] + g.c[254] * v[14]) + c[6] * (g.c[255] * v[4] + g.c[256] * v[6] + g.c[257] * v[23]) + c[7] * (g.c[258] * v[9] + g.c[259] * v[20]);
+}
+template <>
+__device__ __forceinline__ double g1_row<22, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[241] * v[22]) + c[1] * (g.c[242] * v[15] + g.c[243] * v[19]) + c[2] * (g.c[244] * v[11] + g.c[245] * v[16] + g.c[246] * v[18]) + c[3] * (g.c[247] * v[8] + g.c[248] * v[13] + g.c[249] * v[21]) + c[4] * (g.c[250] * v[10] + g.c[251] * v[17]) + c[5] * (g.c[252] * v[3] + g.c[253] * v[7] + g.c[254] * v[14]) + c[6] * (g.c[255] * v[4] + g.c[256] * v[6] + g.c[257] * v[23]) + c[7] * (g.c[258] * v[9] + g.c[259] * v[20]);
+}
+template <>
+__device__ __forceinline__ float g1_row<23, float>(const G1<float>& g, const float (&c)[8], const float (&v)[24]) {
+  return c[0] * (g.c[260] * v[23]) + c[1] * (g.c[261] * v[9] + g.c[262] * v[20]) + c[2] * (g.c[263] * v[10] + g.c[264] * v[17]) + c[3] * (g.c[265] * v[3] + g.c[266] * v[7] + g.c[267] * v[14]) + c[4] * (g.c[268] * v[11] + g.c[269] * v[16] + g.c[270] * v[18]) + c[5] * (g.c[271] * v[8] + g.c[272] * v[13] + g.c[273] * v[21]) + c[6] * (g.c[274] * v[5] + g.c[275] * v[12] + g.c[276] * v[22]) + c[7] * (g.c[277] * v[15] + g.c[278] * v[19]);
+}
+template <>
+__device__ __forceinline__ double g1_row<23, double>(const G1<double>& g, const double (&c)[8], const double (&v)[24]) {
+  return c[0] * (g.c[260] * v[23]) + c[1] * (g.c[261] * v[9] + g.c[262] * v[20]) + c[2] * (g.c[263] * v[10] + g.c[264] * v[17]) + c[3] * (g.c[265] * v[3] + g.c[266] * v[7] + g.c[267] * v[14]) + c[4] * (g.c[268] * v[11] + g.c[269] * v[16] + g.c[270] * v[18]) + c[5] * (g.c[271] * v[8] + g.c[272] * v[13] + g.c[273] * v[21]) + c[6] * (g.c[274] * v[5] + g.c[275] * v[12] + g.c[276] * v[22]) + c[7] * (g.c[277] * v[15] + g.c[278] * v[19]);
+}
+
 // modes 1, s (per axis) of a pair: (a, b) -> (a + b, b - a)
 template <typename T>
 __device__ __forceinline__ void fwht8(const T (&w)[8], T (&c)[8]) {
@@ -365,6 +563,244 @@ k_weights_march(T* __restrict__ out, const T* __restrict__ u, const T* __restric
     }
     __syncthreads();
   }
+}
+
+// ---- level 1, TMA-staged march -------------------------------------------------------------
+// The chunked Walsh layout: c = H w per cell (the coefficients of the eight G_t), stored
+// (nx, ny, cpz / 4, 8, 4) so one cell column's four cells of a z chunk are 128 contiguous
+// bytes. Formed once per hierarchy (after the patch cells' weights are zeroed).
+template <typename T>
+__global__ void k_walsh_chunks(T* __restrict__ wc, const T* __restrict__ w, LpGrid g) {
+  const long long ncp = g.cells_padded();
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncp; c += (long long)gridDim.x * blockDim.x) {
+    T wk[8], cw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) wk[k] = w[k * ncp + c];
+    fwht8(wk, cw);
+    const long long col = c / g.cpz;
+    const int z = (int)(c % g.cpz);
+    T* dst = wc + (col * (g.cpz / 4) + z / 4) * 32 + (z & 3);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst[k * 4] = cw[k];
+  }
+}
+
+constexpr int WSTAGE = 3;
+constexpr int WBOX = TXC + 1;
+
+template <typename T, int N>
+struct alignas(128) WSlot {
+  T v[(N * sizeof(T) + 127) / 128 * 128 / sizeof(T)];
+};
+
+template <typename T>
+struct WSmem {
+  WSlot<T, 3 * WBOX * WBOX * 4> u[WSTAGE];            // node values [comp][x][y][z]
+  WSlot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store
+  T red[3][4][TXC * TYC];                             // corners 01 + 11 (to y + 1)
+  T own[3][4][TXC * TYC];                             // corners 00 + 10 with the -x neighbour's
+  alignas(8) uint64_t full[WSTAGE];
+};
+
+template <typename T>
+struct WMaps {
+  CUtensorMap u;    // (pz, NY, NX, 3), box (4, 17, 17, 3)
+  CUtensorMap out;  // (pz, NY, NX, 3), box (4, 15, 15, 3)
+};
+
+// node-plane forces of one cell: rows (3q + cc, 3(q + 4) + cc) of the modal product give the
+// lower face (f0 - f1) and upper face (f0 + f1) of mode (q, cc); fp = carry + lower face and the
+// upper face becomes the next carry, row pair by row pair
+template <int Q, int CC, typename T>
+__device__ __forceinline__ void fold_pair(const G1<T>& g, const T (&c)[8], const T (&v)[24], T (&fp)[4][3],
+                                          T (&up)[4][3]) {
+  const T f0 = g1_row<3 * Q + CC, T>(g, c, v), f1 = g1_row<3 * (Q + 4) + CC, T>(g, c, v);
+  fp[Q][CC] = up[Q][CC] + (f0 - f1);
+  up[Q][CC] = f0 + f1;
+}
+
+template <typename T>
+__device__ __forceinline__ void fold_rows(const G1<T>& g, const T (&c)[8], const T (&v)[24], T (&fp)[4][3],
+                                          T (&up)[4][3]) {
+  fold_pair<0, 0>(g, c, v, fp, up); fold_pair<0, 1>(g, c, v, fp, up); fold_pair<0, 2>(g, c, v, fp, up);
+  fold_pair<1, 0>(g, c, v, fp, up); fold_pair<1, 1>(g, c, v, fp, up); fold_pair<1, 2>(g, c, v, fp, up);
+  fold_pair<2, 0>(g, c, v, fp, up); fold_pair<2, 1>(g, c, v, fp, up); fold_pair<2, 2>(g, c, v, fp, up);
+  fold_pair<3, 0>(g, c, v, fp, up); fold_pair<3, 1>(g, c, v, fp, up); fold_pair<3, 2>(g, c, v, fp, up);
+}
+
+// x-y modes of plane zz of this thread's four node columns, from a staged slot
+template <typename T>
+__device__ __forceinline__ void slot_modes(const T* __restrict__ slot, int i, int j, int zz, T (&a)[4][3]) {
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const T* b = slot + cc * WBOX * WBOX * 4 + zz;
+    T m[4];
+    xy4(b[(i * WBOX + j) * 4], b[((i + 1) * WBOX + j) * 4], b[(i * WBOX + j + 1) * 4],
+        b[((i + 1) * WBOX + j + 1) * 4], m);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q][cc] = m[q];
+  }
+}
+
+// level-1 operator, u zero on masked dofs: out = m K u (the patch cells' rows are added by
+// k_patch_add). One block per SM: the modal product keeps ~230 registers busy, and capping it at
+// 168 or 128 (two blocks) spills and runs slower (65 us against 47 us at 128 x 64 x 64 cells).
+// A block owns 15 x 15 node columns over a z segment and runs 16 x 16 threads,
+// one per cell column plus a one-cell halo; u arrives by TMA into a 3-stage mbarrier ring
+// (box 4 x 17 x 17 x 3), the Walsh coefficients by 128-byte loads per cell column and chunk,
+// the outputs leave by TMA stores. Waits are bounded and a block that gives up sets *err.
+template <typename T>
+__global__ void __launch_bounds__(TXC * TYC, 1)
+k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, const uint8_t* __restrict__ mask,
+              const G1<T> gc, LpGrid g, int zch, int nchunks, int* __restrict__ err) {
+  extern __shared__ unsigned char wsm_raw[];
+  const uint32_t raw_off = lp_smem_addr(wsm_raw);
+  WSmem<T>& sm = *reinterpret_cast<WSmem<T>*>(wsm_raw + ((128u - (raw_off & 127u)) & 127u));
+  const int tid = threadIdx.x;
+  const int i = tid % TXC, j = tid / TXC;
+  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
+  const int c_begin = blockIdx.z * zch;
+  const int c_end = min(c_begin + zch, nchunks);
+  if (c_begin >= c_end) return;
+  const int cstart = c_begin > 0 ? c_begin - 1 : 0;
+  const int nload = min(c_end + 1, nchunks) - cstart;
+  const int nproc = c_end - cstart;
+  const bool own = i >= 1 && j >= 1;
+  const int cx = x0 - 1 + i, cy = y0 - 1 + j;
+  const bool cell_ok = cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny;
+  const T* wcol = wc + (cell_ok ? ((long long)cx * g.ny + cy) * (g.cpz / 4) * 32 : 0);
+  constexpr uint32_t UBYTES = 3 * WBOX * WBOX * 4 * sizeof(T);
+  __shared__ int bad;
+  if (tid == 0) {
+    int code = 0;
+    uint32_t so = 0;
+    for (int s = 0; s < WSTAGE; ++s) so |= lp_smem_addr(sm.u[s].v);
+    so |= lp_smem_addr(sm.o[0].v) | lp_smem_addr(sm.o[1].v);
+    if (so & 127) code = 20;
+    else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 21;
+    else if (reinterpret_cast<uintptr_t>(&maps.out) & 63) code = 22;
+    else if (lp_smem_addr(&sm.full[0]) & 7) code = 23;
+    else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 24;
+    else if (reinterpret_cast<uintptr_t>(wc) & 15) code = 25;
+    bad = code;
+    if (code) atomicExch(err, code);
+  }
+  __syncthreads();
+  if (bad) return;
+  if (tid == 0) {
+    for (int s = 0; s < WSTAGE; ++s) lp_mbar_init(&sm.full[s], 1);
+    lp_fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    const int s = k % WSTAGE;
+    lp_mbar_expect_tx(&sm.full[s], UBYTES);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (cstart + k), y0 - 1, x0 - 1, 0, &sm.full[s]);
+  };
+  if (tid == 0) {
+    issue(0);
+    if (nload > 1) issue(1);
+  }
+  T up_carry[4][3], a_lo[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) up_carry[q][c] = a_lo[q][c] = T(0);
+
+  for (int k = 0; k < nproc; ++k) {
+    const int c = cstart + k;
+    const bool halo = c < c_begin;
+    const int s = k % WSTAGE;
+    if (tid == 0) {
+      if (k + 2 < nload) issue(k + 2);
+      lp_bulk_wait_read<1>();
+    }
+    bool ok = lp_mbar_wait(&sm.full[s], (k / WSTAGE) & 1);
+    const bool has_next = k + 1 < nload;
+    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % WSTAGE], ((k + 1) / WSTAGE) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        for (int kk = k; kk < min(k + 3, nload); ++kk) lp_mbar_wait(&sm.full[kk % WSTAGE], (kk / WSTAGE) & 1);
+      }
+      break;
+    }
+    const T* us = sm.u[s].v;
+    const T* un = sm.u[(k + 1) % WSTAGE].v;
+    if (k == 0) slot_modes(us, i, j, halo ? 3 : 0, a_lo);
+    const T* wch = wcol + (long long)c * 32;   // this chunk's Walsh run (128 bytes in float32)
+#pragma unroll 1
+    for (int t = halo ? 3 : 0; t < 4; ++t) {
+      T a_hi[4][3];
+      if (t < 3) {
+        slot_modes(us, i, j, t + 1, a_hi);
+      } else if (has_next) {
+        slot_modes(un, i, j, 0, a_hi);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) a_hi[q][cc] = T(0);
+      }
+      T v[24], cw[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const T lo = a_lo[q][cc], hi = a_hi[q][cc];
+          v[3 * q + cc] = lo + hi;
+          v[3 * (q + 4) + cc] = hi - lo;
+          a_lo[q][cc] = hi;
+        }
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk) cw[kk] = cell_ok ? __ldg(wch + kk * 4 + t) : T(0);
+      T fp[4][3];
+      fold_rows<T>(gc, cw, v, fp, up_carry);
+      if (!halo) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const T t0 = fp[0][cc] - fp[2][cc], t1 = fp[1][cc] - fp[3][cc];
+          const T t2 = fp[0][cc] + fp[2][cc], t3 = fp[1][cc] + fp[3][cc];
+          const T c10 = __shfl_up_sync(0xffffffffu, t0 + t1, 1, TXC);
+          const T c11 = __shfl_up_sync(0xffffffffu, t2 + t3, 1, TXC);
+          sm.own[cc][t][tid] = (t0 - t1) + c10;
+          sm.red[cc][t][tid] = (t2 - t3) + c11;
+        }
+      }
+    }
+    if (halo) {
+      __syncthreads();
+      continue;
+    }
+    __syncthreads();
+    if (own) {
+      const bool inside = cx < g.NX() && cy < g.NY();
+      uint8_t mbs[4] = {0, 0, 0, 0};
+      if (inside) {
+        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + g.node(cx, cy, 0) + 4 * c);
+        mbs[0] = mb.x; mbs[1] = mb.y; mbs[2] = mb.z; mbs[3] = mb.w;
+      }
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        T o[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const T v = sm.own[cc][t][tid] + sm.red[cc][t][tid - TXC];
+          o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
+        }
+        T* dst = &sm.o[k & 1].v[((cc * (TXC - 1) + (i - 1)) * (TYC - 1) + (j - 1)) * 4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) dst[t] = o[t];
+      }
+    }
+    lp_fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      lp_tma_store_4d(&maps.out, 4 * c, y0, x0, 0, sm.o[k & 1].v);
+      lp_bulk_commit();
+    }
+  }
+  if (tid == 0) lp_bulk_wait_all();
 }
 
 // patch cells (weights zero, an explicit masked matrix): out += m * sum of their rows times
@@ -540,6 +976,50 @@ static int launch_weights(T* out, const T* u, const T* w, const int* pid, const 
 }
 
 template <typename T>
+static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, const T* pk, const uint8_t* mask,
+                              const double* g1_host, const int* pbox, int* err, LpGrid g, cudaStream_t st) {
+  if (!lp_grid_ok(g) || g.pz % 4 || g.cpz != g.pz || !out || !u || !wc || !mask || !g1_host || !err || out == u)
+    return LP_ERR_ARG;
+  G1<T> gc;
+  for (int i = 0; i < 279; ++i) gc.c[i] = (T)g1_host[i];
+  WMaps<T> maps;
+  const uint64_t nd[4] = {(uint64_t)g.pz, (uint64_t)g.NY(), (uint64_t)g.NX(), 3};
+  const uint32_t bin[4] = {4, WBOX, WBOX, 3};
+  const uint32_t bout[4] = {4, TXC - 1, TYC - 1, 3};
+  if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
+    return LP_ERR_ARG;
+  const int smem = (int)sizeof(WSmem<T>) + 128;
+  static long long slots = 0;   // resident blocks on the device (queried once per process)
+  if (!slots) {
+    if (cudaFuncSetAttribute(k_weights_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return LP_ERR_LAUNCH;
+    int per_sm = 1, dev = 0, nsm = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weights_tma<T>, TXC * TYC, smem);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    slots = (long long)(per_sm > 0 ? per_sm : 1) * nsm;
+  }
+  const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
+  const int nchunks = g.pz / 4;
+  int best = nchunks;
+  double bc = 1e30;
+  for (int zch = 1; zch <= nchunks; ++zch) {
+    const long long nseg = (nchunks + zch - 1) / zch, units = (long long)gx * gy * nseg;
+    const double cost = (double)((units + slots - 1) / slots) * (zch + (nseg > 1 ? 0.3 : 0.0));
+    if (cost < bc - 1e-9) { bc = cost; best = zch; }
+  }
+  dim3 grid(gx, gy, (nchunks + best - 1) / best);
+  k_weights_tma<T><<<grid, TXC * TYC, smem, st>>>(maps, wc, mask, gc, g, best, nchunks, err);
+  if (pid && pk && pbox && pbox[3] > 0 && pbox[4] > 0 && pbox[5] > 0) {
+    const long long nb = (long long)pbox[3] * pbox[4] * pbox[5];
+    k_patch_add<T><<<lp_blocks(nb * 32, 256), 256, 0, st>>>(out, u, pid, pk, mask, g, pbox[0], pbox[1], pbox[2],
+                                                            pbox[3], pbox[4], pbox[5]);
+  }
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+template <typename T>
 static int launch_explicit(T* out, const T* u, const T* kp, T* ft, const uint8_t* mask, LpGrid g, cudaStream_t st) {
   if (!lp_grid_ok(g) || !out || !u || !kp || !ft || !mask || out == u) return LP_ERR_ARG;
   const long long ncell = (long long)g.nx * g.ny * g.nz;
@@ -645,6 +1125,39 @@ int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, c
                                 const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox,
                                 LP_GRID_ARGS, void* stream) {
   return launch_weights<double>(out, u, w, patch_id, patch_k, mask, g1, pbox, LP_GRID, LP_ST);
+}
+
+// the level-1 Walsh coefficients in the chunked layout (nx, ny, cpz / 4, 8, 4), from the
+// weights (8, cells) after the patch cells' weights are zeroed; cpz % 4 == 0
+int lpb_walsh_chunks_f32(float* wc, const float* w, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || g.cpz % 4 || !wc || !w) return LP_ERR_ARG;
+  k_walsh_chunks<float><<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(wc, w, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_walsh_chunks_f64(double* wc, const double* w, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || g.cpz % 4 || !wc || !w) return LP_ERR_ARG;
+  k_walsh_chunks<double><<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(wc, w, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// level-1 apply, TMA-staged (same result as lpb_apply_weights_march_*): wc from
+// lpb_walsh_chunks_*; g1 and pbox are HOST arrays; err: a device int set when a wait gave up
+// (or to an alignment code, 20..25)
+int lpb_apply_weights_tma_f32(float* out, const float* u, const float* wc, const int* patch_id, const float* patch_k,
+                              const uint8_t* mask, const double* g1, const int* pbox, int* err, LP_GRID_ARGS,
+                              void* stream) {
+  return launch_weights_tma<float>(out, u, wc, patch_id, patch_k, mask, g1, pbox, err, LP_GRID, LP_ST);
+}
+
+int lpb_apply_weights_tma_f64(double* out, const double* u, const double* wc, const int* patch_id,
+                              const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int* err,
+                              LP_GRID_ARGS, void* stream) {
+  return launch_weights_tma<double>(out, u, wc, patch_id, patch_k, mask, g1, pbox, err, LP_GRID, LP_ST);
 }
 
 int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask,

@@ -346,6 +346,115 @@ __global__ void k_coarse_band(double* __restrict__ t, int kind, const Tw* __rest
   }
 }
 
+// Level-2 Galerkin matrices from level-1 weights, plain hierarchy (loadpath/mg.py:639-663 with a
+// weights fine level): K(C) = sum_k P_k^T (sum_q w_(k,q) M_q) P_k = sum_(k,q) w_(k,q) N_(k,q) with
+// the 64 fixed products N_(k,q) = P_k^T M_q P_k (nkq: (64, 576), index 8 k + q), w_(k,q) the
+// weight q of child k. A thread owns one of the 576 entries and keeps its 64 coefficients in
+// registers; a block walks CB cells at a time (float64 accumulation). Children that carry a
+// patch matrix (weights zero) are added by k_galerkin_patch_add.
+template <typename Tw>
+__global__ void __launch_bounds__(288, 1) k_galerkin_w2(Tw* __restrict__ kout, const Tw* __restrict__ w1,
+                                                        const Tw* __restrict__ nkq, LpGrid gf, LpGrid gc) {
+  constexpr int CB = 4;
+  __shared__ __align__(16) double ws[CB][64];   // float64 here: the inner loop converts nothing
+  const int e = blockIdx.y * 288 + threadIdx.x;
+  double nr[64];
+#pragma unroll
+  for (int kq = 0; kq < 64; ++kq) nr[kq] = (double)__ldg(nkq + kq * 576 + e);
+  const long long ncell = (long long)gc.nx * gc.ny * gc.nz;
+  const long long ncp1 = gf.cells_padded();
+  const int hx = gf.nx / 2, hy = gf.ny / 2, hz = gf.nz / 2;
+  for (long long c0 = (long long)blockIdx.x * CB; c0 < ncell; c0 += (long long)gridDim.x * CB) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < CB * 64; i += blockDim.x) {
+      const int cb = i >> 6, kq = i & 63, k = kq >> 3, q = kq & 7;
+      const long long cid = c0 + cb;
+      double v = 0.0;
+      if (cid < ncell) {
+        const int Z = (int)(cid % gc.nz);
+        const long long r = cid / gc.nz;
+        const int Y = (int)(r % gc.ny), X = (int)(r / gc.ny);
+        if (X < hx && Y < hy && Z < hz)
+          v = (double)w1[q * ncp1 + gf.cell(2 * X + cx_(k), 2 * Y + cy_(k), 2 * Z + cz_(k))];
+      }
+      ws[cb][kq] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int cb = 0; cb < CB; ++cb) {
+      const long long cid = c0 + cb;
+      if (cid >= ncell) break;
+      double a0 = 0.0, a1 = 0.0;
+      const double2* w2 = reinterpret_cast<const double2*>(ws[cb]);
+#pragma unroll
+      for (int kk = 0; kk < 32; ++kk) {
+        const double2 wv = w2[kk];
+        a0 += nr[2 * kk] * wv.x;
+        a1 += nr[2 * kk + 1] * wv.y;
+      }
+      const int Z = (int)(cid % gc.nz);
+      const long long r = cid / gc.nz;
+      const int Y = (int)(r % gc.ny), X = (int)(r / gc.ny);
+      kout[gc.cell(X, Y, Z) * 576 + e] = (Tw)(a0 + a1);
+    }
+  }
+}
+
+// adds P_k^T patch P_k for every child k of coarse cell C that carries a patch matrix (after
+// k_galerkin_w2); one block per coarse cell, most return at once
+template <typename Tw>
+__global__ void k_galerkin_patch_add(Tw* __restrict__ kout, const int* __restrict__ patch_id,
+                                     const Tw* __restrict__ patch_k, LpGrid gf, LpGrid gc) {
+  __shared__ double kf[576];
+  __shared__ double tt[576];
+  __shared__ int pids[8];
+  const long long bid = blockIdx.x;
+  const long long ncell = (long long)gc.nx * gc.ny * gc.nz;
+  if (bid >= ncell) return;
+  const int Z = (int)(bid % gc.nz);
+  const long long q0 = bid / gc.nz;
+  const int Y = (int)(q0 % gc.ny), X = (int)(q0 / gc.ny);
+  const int hx = gf.nx / 2, hy = gf.ny / 2, hz = gf.nz / 2;
+  if (!(X < hx && Y < hy && Z < hz)) return;
+  if (threadIdx.x < 8) {
+    const int k = threadIdx.x;
+    pids[k] = patch_id[gf.cell(2 * X + cx_(k), 2 * Y + cy_(k), 2 * Z + cz_(k))];
+  }
+  __syncthreads();
+  bool any = false;
+  for (int k = 0; k < 8; ++k) any = any || pids[k] >= 0;
+  if (!any) return;
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  for (int k = 0; k < 8; ++k) {
+    const int p = pids[k];
+    if (p < 0) continue;
+    for (int i = threadIdx.x; i < 576; i += blockDim.x) kf[i] = (double)patch_k[(long long)p * 576 + i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < 576; i += blockDim.x) {
+      const int a = i / 24, j = i % 24, r = j / 3, cc = j % 3;
+      double sacc = 0.0;
+      for (int qq = 0; qq < 8; ++qq) sacc += kf[a * 24 + 3 * qq + cc] * pw(k, qq, r);
+      tt[i] = sacc;
+    }
+    __syncthreads();
+    for (int sidx = 0; sidx < 3; ++sidx) {
+      const int i = threadIdx.x + sidx * 256;
+      if (i >= 576) break;
+      const int ii = i / 24, j = i % 24, r = ii / 3, cc = ii % 3;
+      double v = 0.0;
+      for (int qq = 0; qq < 8; ++qq) v += pw(k, qq, r) * tt[(3 * qq + cc) * 24 + j];
+      if (sidx == 0) acc0 += v; else if (sidx == 1) acc1 += v; else acc2 += v;
+    }
+    __syncthreads();
+  }
+  const long long C = gc.cell(X, Y, Z);
+  for (int sidx = 0; sidx < 3; ++sidx) {
+    const int i = threadIdx.x + sidx * 256;
+    if (i >= 576) break;
+    kout[C * 576 + i] += (Tw)(sidx == 0 ? acc0 : sidx == 1 ? acc1 : acc2);
+  }
+}
+
 }  // namespace
 
 #define LP_FC_ARGS int fnx, int fny, int fnz, int fpz, int fcpz, int cnx, int cny, int cnz, int cpz_, int ccpz
@@ -403,6 +512,25 @@ int lpb_patch_matrices_f64(double* pk, double* w, int* patch_id, const long long
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
+
+// level-2 Galerkin matrices from level-1 weights, plain hierarchy: nkq (64 x 576, index 8k + q)
+// = P_k^T M_q P_k; patch_id / patch_k may be NULL when the fine level has no patch cells
+#define LP_GAL_W2(T, SFX)                                                                                      \
+  int lpb_galerkin_w2_##SFX(T* kout, const T* w1, const T* nkq, const int* patch_id, const T* patch_k,      \
+                            LP_FC_ARGS, void* stream) {                                                      \
+    LpGrid gf = LP_GF, gc = LP_GC;                                                                          \
+    if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !kout || !w1 || !nkq) return LP_ERR_ARG;                   \
+    const long long ncell = (long long)gc.nx * gc.ny * gc.nz;                                               \
+    long long nb = (ncell + 3) / 4;                                                                         \
+    if (nb > 148 * 8) nb = 148 * 8;                                                                         \
+    k_galerkin_w2<T><<<dim3((unsigned)nb, 2), 288, 0, LP_ST>>>(kout, w1, nkq, gf, gc);                      \
+    if (patch_id && patch_k)                                                                                \
+      k_galerkin_patch_add<T><<<(unsigned)ncell, 256, 0, LP_ST>>>(kout, patch_id, patch_k, gf, gc);          \
+    LP_LAUNCH_CHECK();                                                                                      \
+    return LP_OK;                                                                                           \
+  }
+LP_GAL_W2(float, f32)
+LP_GAL_W2(double, f64)
 
 int lpb_galerkin_explicit_f32(float* kout, int fine_kind, const float* fw, const float* mcat, const int* patch_id,
                               const float* patch_k, const float* fk, const uint8_t* mf, int strict, LP_FC_ARGS,

@@ -143,6 +143,45 @@ __global__ void k_cheb_coef(double* __restrict__ coef, const double* __restrict_
   }
 }
 
+// Degree-2 Chebyshev in two passes per smoothing (the reference's default degree). With
+// d' = c1 d + c2 dinv (r - A d) (step 0's update) the two steps give x + d + d', formed here in
+// the reference's order ((x + d) + d', and 0 + d = d exactly), so the result is the same bits as
+// the step-by-step form while r and d are never rewritten.
+// from zero, pass 1: d = (dinv b) s                               (loadpath/mgops.py:321-328)
+template <typename T>
+__global__ void k_cheb_d_start(const T* __restrict__ b, const T* __restrict__ dinv, const double* __restrict__ coef,
+                               T* __restrict__ d, long long n) {
+  const T s = (T)coef[1];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    d[i] = (dinv[i] * b[i]) * s;
+}
+
+// from zero, pass 2 (ad = A d): x = d + (c1 d + c2 dinv (b - ad))
+template <typename T>
+__global__ void k_cheb2_zero(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ad,
+                             const T* __restrict__ d, const T* __restrict__ dinv, const double* __restrict__ coef,
+                             long long n) {
+  const T c1 = (T)coef[2], c2 = (T)coef[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T di = d[i];
+    const T ri = b[i] - ad[i];
+    x[i] = di + (c1 * di + c2 * dinv[i] * ri);
+  }
+}
+
+// from x (after lpb_residual_scaled: r = b - A x, d = s dinv r; ad = A d):
+// x = (x + d) + (c1 d + c2 dinv (r - ad))
+template <typename T>
+__global__ void k_cheb2(T* __restrict__ x, const T* __restrict__ d, const T* __restrict__ r, const T* __restrict__ ad,
+                        const T* __restrict__ dinv, const double* __restrict__ coef, long long n) {
+  const T c1 = (T)coef[2], c2 = (T)coef[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T di = d[i];
+    const T ri = r[i] - ad[i];
+    x[i] = (x[i] + di) + (c1 * di + c2 * dinv[i] * ri);
+  }
+}
+
 // damped Jacobi: x += omega dinv (b - ax), x = 0 start handled by the caller
 template <typename T>
 __global__ void k_jacobi(T* __restrict__ x, const T* __restrict__ b, const T* __restrict__ ax,
@@ -456,6 +495,30 @@ int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
+
+#define LP_CHEB2_ENTRIES(T, SFX)                                                                            \
+  int lpb_cheb_d_start_##SFX(const T* b, const T* dinv, const double* coef, T* d, long long n, void* stream) { \
+    if (!b || !dinv || !coef || !d) return LP_ERR_ARG;                                                   \
+    k_cheb_d_start<T><<<LP_VEC_GRID(n)>>>(b, dinv, coef, d, n);                                          \
+    LP_LAUNCH_CHECK();                                                                                    \
+    return LP_OK;                                                                                         \
+  }                                                                                                       \
+  int lpb_cheb2_zero_##SFX(T* x, const T* b, const T* ad, const T* d, const T* dinv, const double* coef,  \
+                           long long n, void* stream) {                                                  \
+    if (!x || !b || !ad || !d || !dinv || !coef) return LP_ERR_ARG;                                     \
+    k_cheb2_zero<T><<<LP_VEC_GRID(n)>>>(x, b, ad, d, dinv, coef, n);                                     \
+    LP_LAUNCH_CHECK();                                                                                    \
+    return LP_OK;                                                                                         \
+  }                                                                                                       \
+  int lpb_cheb2_##SFX(T* x, const T* d, const T* r, const T* ad, const T* dinv, const double* coef,       \
+                      long long n, void* stream) {                                                       \
+    if (!x || !d || !r || !ad || !dinv || !coef) return LP_ERR_ARG;                                     \
+    k_cheb2<T><<<LP_VEC_GRID(n)>>>(x, d, r, ad, dinv, coef, n);                                          \
+    LP_LAUNCH_CHECK();                                                                                    \
+    return LP_OK;                                                                                         \
+  }
+LP_CHEB2_ENTRIES(float, f32)
+LP_CHEB2_ENTRIES(double, f64)
 
 int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero,
                    long long n, void* stream) {

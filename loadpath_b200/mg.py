@@ -126,6 +126,7 @@ class DevLevel:
         self.kp = None           # explicit: packed symmetric (300, cells)
         self.ft = None           # explicit: (24, cells) scratch of the cell pass
         self.g1 = None           # weights: 279 corner-parity coefficients (host)
+        self.wc = None           # weights: Walsh coefficients (nx, ny, cpz/4, 8, 4)
         self.pbox = None         # weights: node box of the patch cells (host, 6 ints)
         self.mask = None
         self.dinv = None
@@ -176,11 +177,11 @@ class DevLevel:
                                                        int(mask_in), 1, st)
         elif self.kind == "weights":
             if fine_kernel and not mask_in:
-                getattr(L, f"lpb_apply_weights_march_{sfx}")(out.data_ptr(), u.data_ptr(), self.w.data_ptr(),
-                                                              ptr(self.patch_id) if self.npatch else None,
-                                                              ptr(self.patch_k) if self.npatch else None,
-                                                              self.mask.data_ptr(), self.g1.ctypes.data,
-                                                              self.pbox.ctypes.data, *g.args, st)
+                getattr(L, f"lpb_apply_weights_tma_{sfx}")(out.data_ptr(), u.data_ptr(), self.wc.data_ptr(),
+                                                            ptr(self.patch_id) if self.npatch else None,
+                                                            ptr(self.patch_k) if self.npatch else None,
+                                                            self.mask.data_ptr(), self.g1.ctypes.data,
+                                                            self.pbox.ctypes.data, self.err.data_ptr(), *g.args, st)
             else:
                 getattr(L, f"lpb_apply_weights_{sfx}")(out.data_ptr(), u.data_ptr(), self.w.data_ptr(),
                                                         self.mcat.data_ptr(), ptr(self.patch_id),
@@ -264,6 +265,9 @@ class GridElasticity:
         self.ke32 = self.ke64.float()
         pk = fem.child_prolongations()
         self._mcat = np.einsum("kai,ab,kbj->kij", pk, self.ke, pk).reshape(8, 576)
+        # level 2 from level 1: N_(k,q) = P_k^T M_q P_k, 64 x 576 (index 8 k + q)
+        self._nkq = np.einsum("kai,qab,kbj->kqij", pk, self._mcat.reshape(8, 24, 24), pk).reshape(64, 576)
+        self._nkq_dev = {}
         g1 = np.zeros(279)
         if lib().lpb_modal_g1(np.ascontiguousarray(self.ke).ctypes.data, g1.ctypes.data) != 279:
             raise LpError("the level-1 Galerkin matrices are not in the corner-parity pattern of the kernel")
@@ -560,10 +564,23 @@ class GridElasticity:
                 lv.patch_k = None
             lv.patch_cells = pcells
             lv.g1 = self.g1
+            # the Walsh coefficients of each cell's child moduli, chunked for the march kernel
+            lv.wc = self._tbuf("wc1", (gc.nx, gc.ny, gc.cpz // 4, 8, 4), dt)
+            getattr(L, f"lpb_walsh_chunks_{sfx}")(lv.wc.data_ptr(), lv.w.data_ptr(), *gc.args, st)
+            lv.err = self._err
             return lv
         lv = DevLevel("explicit", gc, dt)
         lv.k = self._tbuf(f"k{depth}", (ncp, 576), dt)
-        if fine.kind == "weights":
+        if fine.kind == "weights" and not self.strict:
+            # the 64 products N_(k,q) = P_k^T M_q P_k: each coarse entry is a 64-term sum
+            nkq = self._nkq_dev.get(dt)
+            if nkq is None:
+                nkq = torch.tensor(self._nkq, dtype=dt, device=self.device)
+                self._nkq_dev[dt] = nkq
+            getattr(L, f"lpb_galerkin_w2_{sfx}")(lv.k.data_ptr(), fine.w.data_ptr(), nkq.data_ptr(),
+                                                 ptr(fine.patch_id) if fine.npatch else None,
+                                                 ptr(fine.patch_k) if fine.npatch else None, *gf.args, *gc.args, st)
+        elif fine.kind == "weights":
             getattr(L, f"lpb_galerkin_explicit_{sfx}")(lv.k.data_ptr(), 1, fine.w.data_ptr(), fine.mcat.data_ptr(),
                                                        ptr(fine.patch_id), ptr(fine.patch_k), None,
                                                        fine.mask.data_ptr(), int(self.strict), *gf.args, *gc.args, st)
@@ -678,6 +695,21 @@ class GridElasticity:
                                                     0, n, st)
             return x
         coef = lv.coef.data_ptr()
+        if self.degree == 2:
+            # the two Chebyshev steps in two passes (same bits as the step-by-step form)
+            if from_zero:
+                getattr(L, f"lpb_cheb_d_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), coef, d.data_ptr(), n, st)
+                lv.apply(t, d)
+                getattr(L, f"lpb_cheb2_zero_{sfx}")(x.data_ptr(), b.data_ptr(), t.data_ptr(), d.data_ptr(),
+                                                    lv.dinv.data_ptr(), coef, n, st)
+            else:
+                lv.apply(t, x)
+                getattr(L, f"lpb_residual_scaled_{sfx}")(b.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(), coef,
+                                                         r.data_ptr(), d.data_ptr(), n, st)
+                lv.apply(t, d)
+                getattr(L, f"lpb_cheb2_{sfx}")(x.data_ptr(), d.data_ptr(), r.data_ptr(), t.data_ptr(),
+                                               lv.dinv.data_ptr(), coef, n, st)
+            return x
         if from_zero:
             getattr(L, f"lpb_cheb_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), coef, x.data_ptr(), r.data_ptr(),
                                                 d.data_ptr(), n, st)
