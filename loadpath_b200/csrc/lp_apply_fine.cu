@@ -23,6 +23,9 @@
 // Requirements (checked by the host entry): pz % 4 == 0 and cpz == pz; u, e and the mask
 // hold zeros in the z padding; u is zero on dofs whose mask bit is 0, so the identity rows
 // (1 - m) u of the masked operator vanish and the kernel writes m * K u.
+#include <cstring>
+#include <mutex>
+
 #include "lp_common.cuh"
 #include "lp_tma.cuh"
 
@@ -334,9 +337,372 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
   if (tid == 0) lp_bulk_wait_all();
 }
 
+// ---- float32: pairs of cells in packed float32x2 arithmetic ------------------------------------
+// The float32 kernel forms cells (z, z+1) and (z+2, z+3) of a chunk as pairs: a 128-bit load of
+// a node column's four planes is two register pairs, the x-y modes and the modal product run on
+// pairs (add / sub / mul / fma .f32x2), and the two steps that shift by one plane (lower plane +
+// upper plane of a cell, face forces into node planes) are scalar operations writing pair
+// halves. Same arithmetic as the scalar kernel, half the floating-point instructions.
+typedef unsigned long long f2_t;
+
+__device__ __forceinline__ f2_t pk2(float lo, float hi) {
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float lo2(f2_t v) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+  return a;
+}
+__device__ __forceinline__ float hi2(f2_t v) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+  return b;
+}
+__device__ __forceinline__ f2_t add2(f2_t a, f2_t b) {
+  f2_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t sub2(f2_t a, f2_t b) {
+  f2_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) {
+  f2_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) {
+  f2_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+struct KModal2 {
+  f2_t c[45];   // each coefficient in both lanes
+};
+
+// the modal product of lpb_modal_ke's pattern on a pair of cells (rows 0..2 are zero)
+__device__ __forceinline__ void modal_product2(const KModal2& km, const f2_t (&v)[24], f2_t (&f)[24]) {
+  f[3] = fma2(km.c[2], v[14], fma2(km.c[1], v[7], mul2(km.c[0], v[3])));
+  f[4] = fma2(km.c[4], v[6], mul2(km.c[3], v[4]));
+  f[5] = fma2(km.c[6], v[12], mul2(km.c[5], v[5]));
+  f[6] = fma2(km.c[8], v[6], mul2(km.c[7], v[4]));
+  f[7] = fma2(km.c[11], v[14], fma2(km.c[10], v[7], mul2(km.c[9], v[3])));
+  f[8] = fma2(km.c[13], v[13], mul2(km.c[12], v[8]));
+  f[9] = fma2(km.c[15], v[20], mul2(km.c[14], v[9]));
+  f[10] = fma2(km.c[17], v[17], mul2(km.c[16], v[10]));
+  f[11] = fma2(km.c[20], v[18], fma2(km.c[19], v[16], mul2(km.c[18], v[11])));
+  f[12] = fma2(km.c[22], v[12], mul2(km.c[21], v[5]));
+  f[13] = fma2(km.c[24], v[13], mul2(km.c[23], v[8]));
+  f[14] = fma2(km.c[27], v[14], fma2(km.c[26], v[7], mul2(km.c[25], v[3])));
+  f[15] = fma2(km.c[29], v[19], mul2(km.c[28], v[15]));
+  f[16] = fma2(km.c[32], v[18], fma2(km.c[31], v[16], mul2(km.c[30], v[11])));
+  f[17] = fma2(km.c[34], v[17], mul2(km.c[33], v[10]));
+  f[18] = fma2(km.c[37], v[18], fma2(km.c[36], v[16], mul2(km.c[35], v[11])));
+  f[19] = fma2(km.c[39], v[19], mul2(km.c[38], v[15]));
+  f[20] = fma2(km.c[41], v[20], mul2(km.c[40], v[9]));
+  f[21] = mul2(km.c[42], v[21]);
+  f[22] = mul2(km.c[43], v[22]);
+  f[23] = mul2(km.c[44], v[23]);
+}
+
+__device__ __forceinline__ void xy_modes2(const f2_t (&v)[4], f2_t (&a)[4]) {
+  const f2_t sx0 = add2(v[0], v[1]), dx0 = sub2(v[1], v[0]), sx1 = add2(v[2], v[3]), dx1 = sub2(v[3], v[2]);
+  a[0] = add2(sx0, sx1);
+  a[1] = add2(dx0, dx1);
+  a[2] = sub2(sx1, sx0);
+  a[3] = sub2(dx1, dx0);
+}
+
+// One pair of cells (lower cell planes lo.., upper ..): forms the pair's modal vectors from the
+// x-y modes of three consecutive planes (m0, m1 as a pair and m2), applies E and K^, and returns
+// the two node-plane forces as a pair (carry + lower face of the first cell, upper face of the
+// first + lower face of the second) and the second cell's upper face as the next carry.
+__device__ __forceinline__ void cell_pair(const KModal2& km, const f2_t (&m01)[4][3], const float (&m2)[4][3], f2_t e,
+                                          float (&carry)[4][3], f2_t (&fp)[4][3]) {
+  f2_t v[24], f[24];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const float a0 = lo2(m01[q][cc]), a1 = hi2(m01[q][cc]), a2 = m2[q][cc];
+      v[3 * q + cc] = mul2(pk2(a0 + a1, a1 + a2), e);
+      v[3 * (q + 4) + cc] = mul2(pk2(a1 - a0, a2 - a1), e);
+    }
+  modal_product2(km, v, f);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const f2_t f1 = f[3 * (q + 4) + cc];
+      f2_t lw, up;
+      if (q == 0) {
+        lw = sub2(0ull, f1);   // rows 0..2 (the constant mode) are zero
+        up = f1;
+      } else {
+        const f2_t f0 = f[3 * q + cc];
+        lw = sub2(f0, f1);
+        up = add2(f0, f1);
+      }
+      fp[q][cc] = pk2(carry[q][cc] + lo2(lw), lo2(up) + hi2(lw));
+      carry[q][cc] = hi2(up);
+    }
+}
+
+// corner forces of one pair of node planes: own corner pair (00 + the -x neighbour's 10) kept,
+// the y + 1 corners (01 + 11 of the -x neighbour) to shared memory
+__device__ __forceinline__ void plane_corners2(const f2_t (&fp)[4][3], f2_t (&s0v)[3], float2* red, int tid) {
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const f2_t t0 = sub2(fp[0][cc], fp[2][cc]), t1 = sub2(fp[1][cc], fp[3][cc]);
+    const f2_t t2 = add2(fp[0][cc], fp[2][cc]), t3 = add2(fp[1][cc], fp[3][cc]);
+    const f2_t a = add2(t0, t1), b = add2(t2, t3);
+    const f2_t ca = pk2(__shfl_up_sync(0xffffffffu, lo2(a), 1, TXC), __shfl_up_sync(0xffffffffu, hi2(a), 1, TXC));
+    const f2_t cb = pk2(__shfl_up_sync(0xffffffffu, lo2(b), 1, TXC), __shfl_up_sync(0xffffffffu, hi2(b), 1, TXC));
+    s0v[cc] = add2(sub2(t0, t1), ca);
+    const f2_t r = add2(sub2(t2, t3), cb);
+    red[cc * TXC * TYC + tid] = make_float2(lo2(r), hi2(r));
+  }
+}
+
+constexpr int NST2 = 3;   // TMA ring depth of the float32 kernel (loads run NST2 - 1 chunks ahead)
+
+struct FineSmem2 {
+  Slot<float, 3 * BOX * BOX * 4> u[NST2];
+  Slot<float, BOX * BOX * 4> e[NST2];
+  float2 red[2][2][3][TXC * TYC];                 // [chunk parity][plane pair][component][thread]
+  alignas(8) uint64_t full[NST2];
+};
+
+__device__ __forceinline__ const float* u_at2(const FineSmem2& sm, int s, int c, int x, int y) {
+  return &sm.u[s].v[((c * BOX + x) * BOX + y) * 4];
+}
+
+// One barrier per chunk: each thread waits for its stage, computes, publishes its y-corner
+// forces into the exchange buffer of the chunk's parity, and the block meets once (which also
+// settles a wait that gave up); the owners then add their -y neighbour's corners and store
+// their four node planes with 16-byte stores. The exchange is double-buffered, so the next
+// chunk's writes never meet this chunk's reads. A chunk runs in two phases that keep the
+// register footprint to one pair of cells: (A) planes 0..2 -> cells 0, 1; (B) planes 2..4 ->
+// cells 2, 3 (plane 2's modes formed in both).
+__global__ void __launch_bounds__(TXC * TYC, 2)
+k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict__ out,
+                const uint8_t* __restrict__ mask, const KModal2 km2, const KModal<float> km, LpGrid g, int zch,
+                int nchunks, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw2[];
+  const uint32_t raw_off = lp_smem_addr(smem_raw2);
+  FineSmem2& sm = *reinterpret_cast<FineSmem2*>(smem_raw2 + ((128u - (raw_off & 127u)) & 127u));
+  const int tid = threadIdx.x;
+  const int i = tid % TXC, j = tid / TXC;
+  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
+  const int c_begin = blockIdx.z * zch;
+  const int c_end = min(c_begin + zch, nchunks);
+  if (c_begin >= c_end) return;
+  const int cstart = c_begin > 0 ? c_begin - 1 : 0;
+  const int nload = min(c_end + 1, nchunks) - cstart;
+  const int nproc = c_end - cstart;
+  const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
+  const bool writer = i >= 1 && j >= 1 && nx_ < g.NX() && ny_ < g.NY();
+  const long long obase = writer ? g.node(nx_, ny_, 0) : 0;
+  const long long cs = g.comp_stride();
+  constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(float);
+  constexpr uint32_t EBYTES = BOX * BOX * 4 * sizeof(float);
+  __shared__ int bad;
+  if (tid == 0) {
+    int code = 0;
+    uint32_t so = 0;
+    for (int s = 0; s < NST2; ++s) so |= lp_smem_addr(sm.u[s].v) | lp_smem_addr(sm.e[s].v);
+    if (so & 127) code = 10;
+    else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 11;
+    else if (reinterpret_cast<uintptr_t>(&maps.e) & 63) code = 12;
+    else if (reinterpret_cast<uintptr_t>(out) & 15) code = 13;
+    else if (lp_smem_addr(&sm.full[0]) & 7) code = 15;
+    else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 16;
+    bad = code;
+    if (code) atomicExch(err, code);
+  }
+  __syncthreads();
+  if (bad) return;
+  if (tid == 0) {
+    for (int s = 0; s < NST2; ++s) lp_mbar_init(&sm.full[s], 1);
+    lp_fence_barrier_init();
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    const int s = k % NST2;
+    const int z = 4 * (cstart + k);
+    lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, z, y0 - 1, x0 - 1, 0, &sm.full[s]);
+    lp_tma_load_3d(sm.e[s].v, &maps.e, z, y0 - 1, x0 - 1, &sm.full[s]);
+  };
+  if (tid == 0)
+    for (int kk = 0; kk < NST2 - 1 && kk < nload; ++kk) issue(kk);
+  float carry[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) carry[q][c] = 0.0f;
+
+  for (int k = 0; k < nproc; ++k) {
+    const int c = cstart + k;
+    const bool halo = c < c_begin;
+    const int s = k % NST2;
+    // the stage refilled here was last read in the previous chunk, before its barrier
+    if (tid == 0 && k + NST2 - 1 < nload) issue(k + NST2 - 1);
+    const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + 4 * c)) : 0u;
+    bool ok = lp_mbar_wait(&sm.full[s], (k / NST2) & 1);
+    const bool has_next = k + 1 < nload;
+    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NST2], ((k + 1) / NST2) & 1);
+    // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
+    const float* ecol = &sm.e[s].v[(i * BOX + j) * 4];
+    f2_t m23[4][3];
+    float m4[4][3];
+    auto load_b = [&]() {
+      f2_t p23[4][3];
+      float p4[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const float2 v = *reinterpret_cast<const float2*>(u_at2(sm, s, cc, i + (q & 1), j + (q >> 1)) + 2);
+          p23[q][cc] = pk2(v.x, v.y);
+          p4[q][cc] = has_next ? *u_at2(sm, (k + 1) % NST2, cc, i + (q & 1), j + (q >> 1)) : 0.0f;
+        }
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        f2_t v23[4] = {p23[0][cc], p23[1][cc], p23[2][cc], p23[3][cc]}, a23[4];
+        float v4[4] = {p4[0][cc], p4[1][cc], p4[2][cc], p4[3][cc]}, a4[4];
+        xy_modes2(v23, a23);
+        xy_modes(v4, a4);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          m23[q][cc] = a23[q];
+          m4[q][cc] = a4[q];
+        }
+      }
+    };
+    if (halo) {
+      // only the chunk's last cell: its upper face starts the carry of the segment
+      load_b();
+      const float ew = ecol[3];
+      float v[24], f[24];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const float lo = hi2(m23[q][cc]), hi = m4[q][cc];
+          v[3 * q + cc] = (lo + hi) * ew;
+          v[3 * (q + 4) + cc] = (hi - lo) * ew;
+        }
+      modal_product<float>(km, v, f);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) carry[q][cc] = f[3 * q + cc] + f[3 * (q + 4) + cc];
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(err, 1);
+          for (int kk = k; kk < min(k + NST2, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST2], (kk / NST2) & 1);
+        }
+        break;
+      }
+      continue;
+    }
+    f2_t s0v[2][3];
+    float2(*red)[3][TXC * TYC] = sm.red[k & 1];
+    {
+      f2_t m01[4][3];
+      float m2[4][3];
+      {
+        f2_t p01[4][3];
+        float p2[4][3];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const float4 v = *reinterpret_cast<const float4*>(u_at2(sm, s, cc, i + (q & 1), j + (q >> 1)));
+            p01[q][cc] = pk2(v.x, v.y);
+            p2[q][cc] = v.z;
+          }
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          f2_t v01[4] = {p01[0][cc], p01[1][cc], p01[2][cc], p01[3][cc]}, a01[4];
+          float v2[4] = {p2[0][cc], p2[1][cc], p2[2][cc], p2[3][cc]}, a2[4];
+          xy_modes2(v01, a01);
+          xy_modes(v2, a2);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            m01[q][cc] = a01[q];
+            m2[q][cc] = a2[q];
+          }
+        }
+      }
+      const float2 e01 = *reinterpret_cast<const float2*>(ecol);
+      f2_t fp[4][3];
+      cell_pair(km2, m01, m2, pk2(e01.x, e01.y), carry, fp);
+      plane_corners2(fp, s0v[0], red[0][0], tid);
+    }
+    {
+      load_b();
+      const float2 e23 = *reinterpret_cast<const float2*>(ecol + 2);
+      f2_t fp[4][3];
+      cell_pair(km2, m23, m4, pk2(e23.x, e23.y), carry, fp);
+      plane_corners2(fp, s0v[1], red[1][0], tid);
+    }
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(err, 1);
+        for (int kk = k; kk < min(k + NST2, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST2], (kk / NST2) & 1);
+      }
+      break;
+    }
+    if (writer) {
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const float2 r01 = red[0][cc][tid - TXC], r23 = red[1][cc][tid - TXC];
+        const f2_t o01 = add2(s0v[0][cc], pk2(r01.x, r01.y)), o23 = add2(s0v[1][cc], pk2(r23.x, r23.y));
+        float4 o = make_float4(lo2(o01), hi2(o01), lo2(o23), hi2(o23));
+        if (!((mb4 >> cc) & 1u)) o.x = 0.0f;
+        if (!((mb4 >> (8 + cc)) & 1u)) o.y = 0.0f;
+        if (!((mb4 >> (16 + cc)) & 1u)) o.z = 0.0f;
+        if (!((mb4 >> (24 + cc)) & 1u)) o.w = 0.0f;
+        *reinterpret_cast<float4*>(out + cc * cs + obase + 4 * c) = o;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 static bool fine_args_ok(const LpGrid& g) { return lp_grid_ok(g) && g.pz % 4 == 0 && g.cpz == g.pz; }
+
+// resident blocks of a kernel on this device at the given dynamic shared memory (and the
+// attribute that allows it), looked up once per kernel
+static long long resident_blocks(const void* kfn, int smem) {
+  static std::mutex mu;
+  static const void* keys[8];
+  static long long vals[8];
+  static int n = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < n; ++i)
+    if (keys[i] == kfn) return vals[i];
+  if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
+  int per_sm = 1, dev = 0, nsm = 148;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, TXC * TYC, smem);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long v = (long long)(per_sm > 0 ? per_sm : 1) * nsm;
+  if (n < 8) {
+    keys[n] = kfn;
+    vals[n] = v;
+    ++n;
+  }
+  return v;
+}
 
 template <typename T>
 static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, const double* kmodal_host, int* err,
@@ -344,28 +710,24 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
   if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal_host || !err || out == u) return LP_ERR_ARG;
   KModal<T> km;
   for (int i = 0; i < 45; ++i) km.c[i] = (T)kmodal_host[i];
+  // float32: the packed-pair kernel
+  const bool x2 = sizeof(T) == 4;
+  const uint32_t zc = 4;
   TileMaps<T> maps;
   const uint64_t nd[4] = {(uint64_t)g.pz, (uint64_t)g.NY(), (uint64_t)g.NX(), 3};
   const uint64_t cd[3] = {(uint64_t)g.cpz, (uint64_t)g.ny, (uint64_t)g.nx};
-  const uint32_t bin[4] = {4, BOX, BOX, 3};
-  const uint32_t be[3] = {4, BOX, BOX};
-  const uint32_t bout[4] = {4, TXC - 1, TYC - 1, 3};
+  const uint32_t bin[4] = {zc, BOX, BOX, 3};
+  const uint32_t be[3] = {zc, BOX, BOX};
+  const uint32_t bout[4] = {zc, TXC - 1, TYC - 1, 3};
   if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.e, e, 3, cd, be, sizeof(T)) ||
       !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
     return LP_ERR_ARG;
-  const int smem = (int)sizeof(FineSmem<T>) + 128;
-  static long long slots = 0;   // resident blocks on the device (queried once per process)
-  if (!slots) {
-    if (cudaFuncSetAttribute(k_apply_fine<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-      return LP_ERR_LAUNCH;
-    int per_sm = 1, dev = 0, nsm = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_fine<T>, TXC * TYC, smem);
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    slots = (long long)(per_sm > 0 ? per_sm : 1) * nsm;
-  }
+  const int smem = x2 ? (int)sizeof(FineSmem2) + 128 : (int)sizeof(FineSmem<T>) + 128;
+  const void* kfn = x2 ? (const void*)k_apply_fine_x2 : (const void*)k_apply_fine<T>;
+  const long long slots = resident_blocks(kfn, smem);
+  if (!slots) return LP_ERR_LAUNCH;
   const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
-  const int nchunks = g.pz / 4;
+  const int nchunks = g.pz / (int)zc;
   // z segments: balance the grid over the resident blocks; a segment recomputes one halo cell
   int best_zch = nchunks;
   double best = 1e30;
@@ -378,6 +740,20 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
   }
   const int nseg = (nchunks + best_zch - 1) / best_zch;
   dim3 grid(gx, gy, nseg);
+  if constexpr (sizeof(T) == 4) {
+    if (x2) {
+      KModal2 km2;
+      for (int i = 0; i < 45; ++i) {
+        const float c = (float)kmodal_host[i];
+        uint32_t bits;
+        memcpy(&bits, &c, 4);
+        km2.c[i] = ((unsigned long long)bits << 32) | bits;
+      }
+      k_apply_fine_x2<<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err);
+      LP_LAUNCH_CHECK();
+      return LP_OK;
+    }
+  }
   k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err);
   LP_LAUNCH_CHECK();
   return LP_OK;

@@ -81,6 +81,10 @@ __device__ __forceinline__ void lp_bulk_wait_all() { asm volatile("cp.async.bulk
 // generic-proxy writes to shared memory made visible to the async (TMA) proxy
 __device__ __forceinline__ void lp_fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// byte offset within a 32-byte-swizzled TMA destination (1024-byte aligned): the 16-byte chunk
+// bit (4) flipped by bit 7
+__device__ __forceinline__ uint32_t lp_swz32(uint32_t off) { return off ^ (((off >> 7) & 1u) << 4); }
+
 // ---- host: tensor-map encoding through the runtime's driver entry point ------------------
 static inline PFN_cuTensorMapEncodeTiled_v12000 lp_encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -94,9 +98,11 @@ static inline PFN_cuTensorMapEncodeTiled_v12000 lp_encode_fn() {
   return fn;
 }
 
-// rank-r tiled map over a dense C-order array; dims/box innermost first; elem 4 or 8 bytes
+// rank-r tiled map over a dense C-order array; dims/box innermost first; elem 4 or 8 bytes;
+// swizzle32: the 32-byte swizzle (box rows of exactly 32 bytes; in shared memory byte address
+// bit 4 is XORed with bit 7, see lp_swz32), destinations then 1024-byte aligned
 static inline bool lp_make_map(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
-                               const uint32_t* box, int elem_bytes) {
+                               const uint32_t* box, int elem_bytes, bool swizzle32 = false) {
   auto fn = lp_encode_fn();
   if (!fn) return false;
   if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
@@ -114,9 +120,11 @@ static inline bool lp_make_map(CUtensorMap* map, const void* base, int rank, con
     stride *= dims[i];
   }
   if ((box[0] * (uint32_t)elem_bytes) % 16) return false;
+  if (swizzle32 && box[0] * (uint32_t)elem_bytes != 32) return false;
   CUtensorMapDataType dt = elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   CUresult r = fn(map, dt, (cuuint32_t)rank, const_cast<void*>(base), gd, gs, bx, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
