@@ -43,6 +43,10 @@ int lpb_apply_explicit_f64(double* out, const double* u, const double* k, const 
  * _scatter_into with finish (loadpath/mgops.py:86-103, :181-217). */
 int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* the float64 fine apply that also forms u . out over the level's nodes into *dot (device),
+ * for the PCG's p . A p: per-block partials in part (part_len doubles, -3 when short), summed in
+ * a fixed order */
+int lpb_apply_fine_dot_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int* err, double* part, long long part_len, double* dot, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* the element matrix (24 x 24, float64, host pointer) in the corner-parity basis that
  * lpb_apply_fine_* reads (45 coefficients, host pointer out); returns the count or < 0 */
 int lpb_modal_ke(const double* ke, double* kmodal_out);
@@ -192,6 +196,12 @@ int lpb_dot_f64_f32(const double* a, const float* b, long long n, double* part, 
 int lpb_cg_step(double* x, double* r, const double* p, const double* ap, float* r32, long long n, const double* num, const double* den, double* part, double* rr, void* stream);
 int lpb_xpby_f32(double* p, const float* z, long long n, const double* num, const double* den, void* stream);
 int lpb_xpby_f64(double* p, const double* z, long long n, const double* num, const double* den, void* stream);
+/* the CG update in two passes with x deferred: lpb_cg_step_r moves r (r -= alpha ap, its float32
+ * copy, |r|^2 into *rr) and lpb_xpby_x_* then does x += (rz / pap) p and p = z + (rz_new / rz) p
+ * (loadpath/mg.py:903-925; the same arithmetic, x updated one pass later) */
+int lpb_cg_step_r(double* r, const double* ap, float* r32, long long n, const double* num, const double* den, double* part, double* rr, void* stream);
+int lpb_xpby_x_f32(double* p, double* x, const float* z, long long n, const double* rz, const double* pap, const double* rz_new, void* stream);
+int lpb_xpby_x_f64(double* p, double* x, const double* z, long long n, const double* rz, const double* pap, const double* rz_new, void* stream);
 /* warm start of the PCG on the device (loadpath/mg.py:878-895); sc holds [0] b.b, [5] x.Ax,
  * [6] b.x, [7] |rs|^2 and s = b.x / x.Ax (0 unless x.Ax > 0). lpb_warm_residual: rs = b - s Ax;
  * lpb_warm_select: x = s x, r = rs when s > 0 and |rs| < |b|, else x = 0, r = b. */

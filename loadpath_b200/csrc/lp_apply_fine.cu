@@ -151,7 +151,7 @@ __device__ __forceinline__ void xy_modes(const T (&v)[4], T (&a)[4]) {
 template <typename T>
 __global__ void __launch_bounds__(TXC * TYC, (sizeof(T) == 4 ? 2 : 1))
 k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict__ mask, const KModal<T> km,
-             LpGrid g, int zch, int nchunks, int* __restrict__ err) {
+             LpGrid g, int zch, int nchunks, int* __restrict__ err, double* __restrict__ dotp) {
   extern __shared__ unsigned char smem_raw[];
   // 128-byte alignment in the shared window (what TMA addresses), not in the generic space
   const uint32_t raw_off = lp_smem_addr(smem_raw);
@@ -161,7 +161,11 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
   const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
   const int c_begin = blockIdx.z * zch;
   const int c_end = min(c_begin + zch, nchunks);
-  if (c_begin >= c_end) return;
+  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  if (c_begin >= c_end) {
+    if (dotp && tid == 0) dotp[bid] = 0.0;
+    return;
+  }
   const int cstart = c_begin > 0 ? c_begin - 1 : 0;     // one halo chunk below the segment
   const int nload = min(c_end + 1, nchunks) - cstart;   // + the plane above the last chunk
   const int nproc = c_end - cstart;
@@ -187,7 +191,10 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
     if (code) atomicExch(err, code);
   }
   __syncthreads();
-  if (bad) return;
+  if (bad) {
+    if (dotp && tid == 0) dotp[bid] = 0.0;
+    return;
+  }
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) lp_mbar_init(&sm.full[s], 1);
     lp_fence_barrier_init();
@@ -210,6 +217,7 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
   for (int q = 0; q < 4; ++q)
 #pragma unroll
     for (int c = 0; c < 3; ++c) up_carry[q][c] = T(0);
+  double pacc = 0.0;   // u . (K u) over this thread's own nodes (when dotp is given)
 
   for (int k = 0; k < nproc; ++k) {
     const int c = cstart + k;
@@ -323,6 +331,7 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
         for (int t = 0; t < 4; ++t) {
           T v = s0v[t][cc] + sm.red[cc][t][tid - TXC];
           o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
+          pacc += (double)o[t] * (double)un[0][cc][t];   // this node's u: column q = 0
         }
         Vec4<T>::sts(&sm.o[k & 1].v[((cc * (TXC - 1) + (i - 1)) * (TYC - 1) + (j - 1)) * 4], o);
       }
@@ -335,6 +344,20 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
     }
   }
   if (tid == 0) lp_bulk_wait_all();
+  if (dotp) {
+    __shared__ double sh[32];
+    pacc = lp_block_sum(pacc, sh);
+    if (tid == 0) dotp[bid] = pacc;
+  }
+}
+
+// ordered sum of the per-block partials (the same bits every run)
+__global__ void k_fine_dot_final(const double* __restrict__ part, long long n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // ---- float32: pairs of cells in packed float32x2 arithmetic ------------------------------------
@@ -706,7 +729,8 @@ static long long resident_blocks(const void* kfn, int smem) {
 
 template <typename T>
 static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, const double* kmodal_host, int* err,
-                       LpGrid g, cudaStream_t st) {
+                       LpGrid g, cudaStream_t st, double* part = nullptr, long long part_len = 0,
+                       double* dot_out = nullptr) {
   if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal_host || !err || out == u) return LP_ERR_ARG;
   KModal<T> km;
   for (int i = 0; i < 45; ++i) km.c[i] = (T)kmodal_host[i];
@@ -754,7 +778,14 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
       return LP_OK;
     }
   }
-  k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err);
+  if (part) {
+    const long long nb = (long long)grid.x * grid.y * grid.z;
+    if (nb > part_len) return LP_ERR_SIZE;
+    k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err, part);
+    k_fine_dot_final<<<1, 1024, 0, st>>>(part, nb, dot_out);
+  } else {
+    k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err, nullptr);
+  }
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -808,6 +839,17 @@ int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t
 int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal,
                        int* err, int nx, int ny, int nz, int pz, int cpz, void* stream) {
   return launch_fine<double>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream);
+}
+
+// lpb_apply_fine_f64 that also forms u . out over the level's nodes into *dot (float64, device):
+// per-block partials in part (part_len doubles; -3 when the grid has more blocks), then an
+// ordered sum, so the dot has the same bits every run
+int lpb_apply_fine_dot_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal,
+                           int* err, double* part, long long part_len, double* dot, int nx, int ny, int nz, int pz,
+                           int cpz, void* stream) {
+  if (!part || !dot || part_len <= 0) return LP_ERR_ARG;
+  return launch_fine<double>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream, part,
+                             part_len, dot);
 }
 
 }  // extern "C"

@@ -342,6 +342,38 @@ __global__ void k_warm_select(double* __restrict__ x, double* __restrict__ r, co
   }
 }
 
+// The CG update split for fewer passes over the float64 fields: the step after A p only moves
+// r (and its float32 copy) and forms |r|^2; x += alpha p is deferred to the pass that rebuilds p,
+// which reads p anyway. alpha = rz / pap and beta = rz_new / rz are read on the device.
+__global__ void k_cg_step_r(double* __restrict__ r, const double* __restrict__ ap, float* __restrict__ r32,
+                            long long n, const double* __restrict__ num, const double* __restrict__ den,
+                            double* __restrict__ part) {
+  __shared__ double sh[32];
+  const double alpha = (*num) / (*den);
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double ri = r[i] - alpha * ap[i];
+    r[i] = ri;
+    if (r32) r32[i] = (float)ri;
+    s += ri * ri;
+  }
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// x += (rz / pap) p; p = z + (rz_new / rz) p
+template <typename Tz>
+__global__ void k_xpby_x(double* __restrict__ p, double* __restrict__ x, const Tz* __restrict__ z, long long n,
+                         const double* __restrict__ rz, const double* __restrict__ pap,
+                         const double* __restrict__ rz_new) {
+  const double alpha = (*rz) / (*pap), beta = (*rz_new) / (*rz);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double pi = p[i];
+    x[i] += alpha * pi;
+    p[i] = (double)z[i] + beta * pi;
+  }
+}
+
 }  // namespace
 
 #define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
@@ -519,6 +551,31 @@ int lpb_cheb_f64(double* x, double* d, double* r, const double* ad, const double
   }
 LP_CHEB2_ENTRIES(float, f32)
 LP_CHEB2_ENTRIES(double, f64)
+
+int lpb_cg_step_r(double* r, const double* ap, float* r32, long long n, const double* num, const double* den,
+                  double* part, double* rr, void* stream) {
+  if (!r || !ap || !num || !den || !part || !rr) return LP_ERR_ARG;
+  k_cg_step_r<<<LP_RED_BLOCKS, LP_RED_THREADS, 0, LP_ST>>>(r, ap, r32, n, num, den, part);
+  k_sum_final<<<1, 1024, 0, LP_ST>>>(part, LP_RED_BLOCKS, rr);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_xpby_x_f32(double* p, double* x, const float* z, long long n, const double* rz, const double* pap,
+                   const double* rz_new, void* stream) {
+  if (!p || !x || !z || !rz || !pap || !rz_new) return LP_ERR_ARG;
+  k_xpby_x<float><<<LP_VEC_GRID(n)>>>(p, x, z, n, rz, pap, rz_new);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_xpby_x_f64(double* p, double* x, const double* z, long long n, const double* rz, const double* pap,
+                   const double* rz_new, void* stream) {
+  if (!p || !x || !z || !rz || !pap || !rz_new) return LP_ERR_ARG;
+  k_xpby_x<double><<<LP_VEC_GRID(n)>>>(p, x, z, n, rz, pap, rz_new);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
 
 int lpb_jacobi_f32(float* x, const float* b, const float* ax, const float* dinv, float omega, int from_zero,
                    long long n, void* stream) {

@@ -196,6 +196,27 @@ class DevLevel:
                                                          self.mask.data_ptr(), *g.args, int(mask_in), 1, st)
         return out
 
+    def apply_dot(self, out, u, part, dot):
+        """out = m K u on the float64 fine level (u zero on masked dofs) and *dot = u . out, in one
+        pass (the PCG's A p and p . A p)."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        probe = _PROBE[0]
+        if probe is not None:
+            a, b = probe.take()
+            L.lpb_event_record(a.cuda_event, st)
+        L.lpb_apply_fine_dot_f64(out.data_ptr(), u.data_ptr(), self.e.data_ptr(), self.mask.data_ptr(),
+                                 self.kmodal.ctypes.data, self.err.data_ptr(), part.data_ptr(), part.numel(),
+                                 dot.data_ptr(), *g.args, st)
+        if probe is not None:
+            L.lpb_event_record(b.cuda_event, st)
+            if probe.capture is not None:
+                probe.capture.append((self.dtype, a, b))
+            else:
+                probe.pending.append((self.dtype, a, b))
+        return out
+
     def diagonal(self, d):
         L = lib()
         g = self.grid
@@ -673,6 +694,7 @@ class GridElasticity:
 
     # --- V-cycle (loadpath/mg.py:796-864) -----------------------------------------------
     def _smooth(self, i, b, x, from_zero):
+        """Chebyshev (or damped Jacobi) smoothing of level i."""
         L = lib()
         st = stream_handle()
         lv = self._op(i)
@@ -725,8 +747,9 @@ class GridElasticity:
                                           lv.dinv.data_ptr(), coef, it, int(last), n, st)
         return x
 
-    def _vcycle(self, i, b):
-        """x = V(b) on level i; b and the result live in level-i buffers."""
+    def _vcycle(self, i, b, dot=None):
+        """x = V(b) on level i; b and the result live in level-i buffers. dot = (r64, out): also
+        out = r64 . x (the PCG's r . z)."""
         L = lib()
         st = stream_handle()
         lv = self._op(i)
@@ -739,9 +762,13 @@ class GridElasticity:
                 c = self._coarse
                 getattr(L, f"lpb_band_solve_{sfx}")(x.data_ptr(), b.data_ptr(), c["ainv"].data_ptr(),
                                                     c["v"].data_ptr(), *g.args, st)
-                return x
-            self._smooth(i, b, x, True)
-            return self._smooth(i, b, x, False)
+            else:
+                self._smooth(i, b, x, True)
+                self._smooth(i, b, x, False)
+            if dot is not None:
+                L.lpb_dot_f64_f32(dot[0].data_ptr(), x.data_ptr(), x.numel(), self._part.data_ptr(),
+                                  dot[1].data_ptr(), st)
+            return x
         self._smooth(i, b, x, True)
         t = self._buf(f"t{i}", g, dt)
         lv.apply(t, x)
@@ -753,7 +780,12 @@ class GridElasticity:
         xc = self._vcycle(i + 1, bc)
         getattr(L, f"lpb_prolong_add_{sfx}")(x.data_ptr(), xc.data_ptr(), nxt.mask.data_ptr(), lv.mask.data_ptr(),
                                              *g.args, *gc.args, st)
-        return self._smooth(i, b, x, False)
+        self._smooth(i, b, x, False)
+        if dot is not None:
+            # its own pass: folded into the last smoothing pass it evicts that pass's inputs from
+            # L2 (the float64 r is 103 MB at 256 x 128 x 128) and runs slower than the two
+            L.lpb_dot_f64_f32(dot[0].data_ptr(), x.data_ptr(), x.numel(), self._part.data_ptr(), dot[1].data_ptr(), st)
+        return x
 
     def precondition_device(self, r64, z_out):
         """z = V(r) with the cast to and from the V-cycle precision (loadpath/mg.py:862-864)."""
@@ -881,26 +913,28 @@ class GridElasticity:
             self._dot64(r, z, 1)
 
         def head():
-            # ap = A p; pap; x += alpha p; r -= alpha ap (and its float32 copy); |r|^2; scalars out
+            # ap = A p and pap in one pass; r -= alpha ap (and its float32 copy); |r|^2; scalars
+            # out. x += alpha p waits for the tail's pass over p.
             st = stream_handle()
-            a.apply(ap, p)
-            self._dot64(p, ap, 3)
-            L.lpb_cg_step(x.data_ptr(), r.data_ptr(), p.data_ptr(), ap.data_ptr(), ptr(r32), n,
-                          sc[1].data_ptr(), sc[3].data_ptr(), self._part.data_ptr(), sc[4].data_ptr(), st)
+            a.apply_dot(ap, p, self._part, sc[3])
+            L.lpb_cg_step_r(r.data_ptr(), ap.data_ptr(), ptr(r32), n, sc[1].data_ptr(), sc[3].data_ptr(),
+                            self._part.data_ptr(), sc[4].data_ptr(), st)
             L.lpb_memcpy_async(host.data_ptr(), sc[3:5].data_ptr(), 16, st)
             L.lpb_memcpy_async(host[2:].data_ptr(), sc[0:1].data_ptr(), 8, st)
 
         def tail():
-            # z = V(r); rz_new; p = z + (rz_new / rz) p; rz = rz_new
+            # z = V(r) and rz_new (formed by the V-cycle's last pass); x += alpha p;
+            # p = z + (rz_new / rz) p; rz = rz_new
             st = stream_handle()
             if r32 is not None:
-                xv = self._vcycle(0, r32)
-                L.lpb_dot_f64_f32(r.data_ptr(), xv.data_ptr(), n, self._part.data_ptr(), sc[2].data_ptr(), st)
-                L.lpb_xpby_f32(p.data_ptr(), xv.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), st)
+                xv = self._vcycle(0, r32, dot=(r, sc[2]))
+                L.lpb_xpby_x_f32(p.data_ptr(), x.data_ptr(), xv.data_ptr(), n, sc[1].data_ptr(), sc[3].data_ptr(),
+                                 sc[2].data_ptr(), st)
             else:
                 self.precondition_device(r, z)
                 self._dot64(r, z, 2)
-                L.lpb_xpby_f64(p.data_ptr(), z.data_ptr(), n, sc[2].data_ptr(), sc[1].data_ptr(), st)
+                L.lpb_xpby_x_f64(p.data_ptr(), x.data_ptr(), z.data_ptr(), n, sc[1].data_ptr(), sc[3].data_ptr(),
+                                 sc[2].data_ptr(), st)
             L.lpb_memcpy_async(sc[1:2].data_ptr(), sc[2:3].data_ptr(), 8, st)
 
         warm = x0 is not None
