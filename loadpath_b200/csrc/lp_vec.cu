@@ -15,6 +15,31 @@
 
 namespace {
 
+template <typename T>
+struct V4ld;
+template <>
+struct V4ld<float> {
+  static __device__ __forceinline__ void ld(const float* p, float (&v)[4]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+  static __device__ __forceinline__ void st(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct V4ld<double> {
+  static __device__ __forceinline__ void ld(const double* p, double (&v)[4]) {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+  static __device__ __forceinline__ void st(double* p, const double (&v)[4]) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+  }
+};
+
+
 template <typename Ta, typename Tb>
 __global__ void k_dot_partial(const Ta* __restrict__ a, const Tb* __restrict__ b, long long n,
                               double* __restrict__ part) {
@@ -281,6 +306,152 @@ __global__ void k_prolong_add(T* __restrict__ x, const T* __restrict__ xc, const
 #pragma unroll
     for (int i = 0; i < 3; ++i)
       if ((mb >> i) & 1) x[i * fcs + fn] += acc[i];
+  }
+}
+
+// ---- grid transfers by z chunks (the level fields' z pitch is a multiple of 4) ----------------
+// One thread per (x, y) node column and chunk of four z planes, the column's values moved with
+// 16-byte loads and stores, the trilinear weights applied separably (z inside a column first).
+
+// rc = restrict(((b - ax) * m) zero-padded) * cm for coarse nodes (X, Y, 4C..4C+3): the fine z
+// range 8C - 1 .. 8C + 7 of the nine fine columns around (2X, 2Y)   (loadpath/mgops.py:666-711)
+template <typename T>
+__global__ void k_restrict4(T* __restrict__ rc, const T* __restrict__ b, const T* __restrict__ ax,
+                            const uint8_t* __restrict__ m, const uint8_t* __restrict__ cm, LpGrid gf, LpGrid gc) {
+  const int CX = gc.NX(), CY = gc.NY(), CZ4 = gc.pz / 4;
+  const int FX = gf.NX(), FY = gf.NY();
+  const long long total = (long long)CX * CY * CZ4;
+  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int C = (int)(t % CZ4);
+    const long long q = t / CZ4;
+    const int Y = (int)(q % CY), X = (int)(q / CY);
+    const int z0 = 8 * C;
+    T acc[3][4] = {};
+#pragma unroll 1
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = 2 * X + dx;
+      if (x < 0 || x >= FX) continue;
+      const T wx = dx ? T(0.5) : T(1);
+#pragma unroll 1
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = 2 * Y + dy;
+        if (y < 0 || y >= FY) continue;
+        const T w = wx * (dy ? T(0.5) : T(1));
+        const long long col = gf.node(x, y, 0);
+        // fine planes z0 - 1 .. z0 + 7 of this column: masked b - ax per component
+        // a coarse level padded up past half the fine one reaches beyond the fine pitch: zeros
+        const bool below = z0 >= 1 && z0 - 1 < gf.pz, lo = z0 < gf.pz, hi = z0 + 4 < gf.pz;
+        uint8_t mz[9];
+        mz[0] = below ? m[col + z0 - 1] : 0;
+        const uchar4 ma = lo ? *reinterpret_cast<const uchar4*>(m + col + z0) : make_uchar4(0, 0, 0, 0);
+        const uchar4 mb = hi ? *reinterpret_cast<const uchar4*>(m + col + z0 + 4) : make_uchar4(0, 0, 0, 0);
+        mz[1] = ma.x; mz[2] = ma.y; mz[3] = ma.z; mz[4] = ma.w;
+        mz[5] = mb.x; mz[6] = mb.y; mz[7] = mb.z; mz[8] = mb.w;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const T* bi = b + i * fcs + col;
+          const T* ai = ax + i * fcs + col;
+          T v[9];
+          v[0] = below ? bi[z0 - 1] - ai[z0 - 1] : T(0);
+          T b4[4], a4[4];
+          if (lo) {
+            V4ld<T>::ld(bi + z0, b4);
+            V4ld<T>::ld(ai + z0, a4);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[1 + k] = b4[k] - a4[k];
+          } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[1 + k] = T(0);
+          }
+          if (hi) {
+            V4ld<T>::ld(bi + z0 + 4, b4);
+            V4ld<T>::ld(ai + z0 + 4, a4);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[5 + k] = b4[k] - a4[k];
+          } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[5 + k] = T(0);
+          }
+#pragma unroll
+          for (int k = 0; k < 9; ++k) v[k] = ((mz[k] >> i) & 1) ? v[k] : T(0);
+          // coarse Z = 4C + kk sums fine z = 2Z - 1, 2Z, 2Z + 1 = v[2kk], v[2kk + 1], v[2kk + 2]
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            acc[i][kk] += w * (T(0.5) * v[2 * kk] + v[2 * kk + 1] + T(0.5) * v[2 * kk + 2]);
+        }
+      }
+    }
+    const long long cn = gc.node(X, Y, 4 * C);
+    const uchar4 cmb = *reinterpret_cast<const uchar4*>(cm + cn);
+    const uint8_t cms[4] = {cmb.x, cmb.y, cmb.z, cmb.w};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      T o[4];
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) o[kk] = ((cms[kk] >> i) & 1) ? acc[i][kk] : T(0);
+      V4ld<T>::st(rc + i * ccs + cn, o);
+    }
+  }
+}
+
+// x += prolong(xc * cm) * m for fine nodes (x, y, 4c..4c+3): coarse planes 2c, 2c + 1, 2c + 2 of
+// the one, two or four coarse columns around (x / 2, y / 2)   (loadpath/mgops.py:714-750)
+template <typename T>
+__global__ void k_prolong4(T* __restrict__ xf, const T* __restrict__ xc, const uint8_t* __restrict__ cm,
+                           const uint8_t* __restrict__ m, LpGrid gf, LpGrid gc) {
+  const int FX = gf.NX(), FY = gf.NY(), FZ4 = gf.pz / 4;
+  const long long total = (long long)FX * FY * FZ4;
+  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % FZ4);
+    const long long q = t / FZ4;
+    const int y = (int)(q % FY), x = (int)(q / FY);
+    const long long fn = gf.node(x, y, 4 * c);
+    const uchar4 mb = *reinterpret_cast<const uchar4*>(m + fn);
+    const uint8_t ms[4] = {mb.x, mb.y, mb.z, mb.w};
+    if (((mb.x | mb.y | mb.z | mb.w) & 7) == 0) continue;
+    const int X0 = x >> 1, Y0 = y >> 1, ox = x & 1, oy = y & 1;
+    const int Z0 = 2 * c;
+    const int zmax = gc.pz - 1;
+    T acc[3][4] = {};
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      if (a && !ox) break;
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        if (bb && !oy) break;
+        const T w = (ox ? T(0.5) : T(1)) * (oy ? T(0.5) : T(1));
+        const long long ccol = gc.node(X0 + a, Y0 + bb, 0);
+        uint8_t cmz[3];
+        T cv[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) cmz[k] = cm[ccol + min(Z0 + k, zmax)];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const T v = xc[i * ccs + ccol + min(Z0 + k, zmax)];
+            cv[i][k] = ((cmz[k] >> i) & 1) ? v : T(0);
+          }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          acc[i][0] += w * cv[i][0];
+          acc[i][1] += w * (T(0.5) * (cv[i][0] + cv[i][1]));
+          acc[i][2] += w * cv[i][1];
+          acc[i][3] += w * (T(0.5) * (cv[i][1] + cv[i][2]));
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      T o[4];
+      V4ld<T>::ld(xf + i * fcs + fn, o);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if ((ms[k] >> i) & 1) o[k] += acc[i][k];
+      V4ld<T>::st(xf + i * fcs + fn, o);
+    }
   }
 }
 
@@ -599,6 +770,12 @@ int lpb_restrict_residual_f32(float* rc, const float* b, const float* ax, const 
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
+    const long long t4 = (long long)gc.NX() * gc.NY() * (gc.pz / 4);
+    k_restrict4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+    LP_LAUNCH_CHECK();
+    return LP_OK;
+  }
   long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
   k_restrict_residual<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
@@ -609,6 +786,12 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
+    const long long t4 = (long long)gc.NX() * gc.NY() * (gc.pz / 4);
+    k_restrict4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+    LP_LAUNCH_CHECK();
+    return LP_OK;
+  }
   long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
   k_restrict_residual<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
@@ -618,6 +801,12 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
 int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
+    const long long t4 = (long long)gf.NX() * gf.NY() * (gf.pz / 4);
+    k_prolong4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+    LP_LAUNCH_CHECK();
+    return LP_OK;
+  }
   long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
   k_prolong_add<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
@@ -627,6 +816,12 @@ int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint
 int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
+    const long long t4 = (long long)gf.NX() * gf.NY() * (gf.pz / 4);
+    k_prolong4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+    LP_LAUNCH_CHECK();
+    return LP_OK;
+  }
   long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
   k_prolong_add<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
