@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--micro", choices=["apply"], default=None,
                    help="only the fine-level K*u microbenchmark (config 1: applies on seeded N(0,1) vectors)")
     p.add_argument("--reps", type=int, default=100)
+    p.add_argument("--kernels", type=int, default=0, metavar="N",
+                   help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
+                        "activity trace (torch.profiler); a table, not the JSON line")
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
     a.dims = tuple(int(v) for v in a.dims.split(","))
@@ -151,6 +154,21 @@ def cpu_apply_times(dims, reps64=3, reps32=3):
     return out, cport.threads()
 
 
+# CG iterations of SIMP iterations 1, 2, ... of this (deterministic) workload at 256x128x128,
+# from the mixed-precision GPU path; the reference arm times the CPU operator for the same counts
+CG_ITERS_256 = (17, 25, 15, 16, 20, 25, 39, 57, 78, 208, 118, 114)
+
+
+def fine_applies(cg_iters):
+    """Fine-level applies per SIMP iteration, averaged over iterations with these CG counts:
+    float64 = the CG iterations + the warm-start apply; float32 = four per V-cycle (one per CG
+    iteration and one before the loop) + 12 power iterations."""
+    n = max(len(cg_iters), 1)
+    n64 = sum(c + 1 for c in cg_iters) / n
+    n32 = sum(12 + 4 * (c + 1) for c in cg_iters) / n
+    return int(round(n64)), int(round(n32))
+
+
 def cpu_iteration_estimate(dims, n64, n32):
     t, cores = cpu_apply_times(dims)
     sec = n64 * t["float64"] + n32 * t["float32"]
@@ -166,10 +184,10 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # fine applies per SIMP iteration of the mixed path at this size: 17 CG iterations (the
-    # reference's count at this workload) + the warm-start apply in float64; four per V-cycle
-    # (18 V-cycles) plus 12 power iterations in float32
-    n64, n32 = 18, 4 * 18 + 12
+    # fine applies per SIMP iteration for the CG counts of the same iterations on the GPU path
+    # (iterations warmup + 1 .. warmup + steps of this workload)
+    seq = CG_ITERS_256[args.warmup:args.warmup + args.steps] if tuple(args.dims) == DIMS else ()
+    n64, n32 = fine_applies(seq if len(seq) == args.steps else (17,))
     cb = cpu_iteration_estimate(args.dims, n64, n32)
     vals = []
     for _ in range(args.warmup + args.steps):
@@ -277,7 +295,7 @@ def run_b200(args):
              "phase_ms_per_step": dict(zip(("hierarchy", "solve", "sensitivities", "oc"),
                                            np.round(phases.mean(axis=0), 3).tolist())),
              "fine_apply_f64_us": (fine["f64_ms"] / fine["f64_count"] * 1e3) if fine["f64_count"] else None,
-             "fine_applies_per_step": {"f64": fine["f64_count"] / args.steps, "f32": fine["f32_count"] / args.steps}}
+             "fine_applies_per_step": dict(zip(("f64", "f32"), fine_applies(iters)))}
     del loop
     torch.cuda.empty_cache()
 
@@ -351,8 +369,7 @@ def run_b200(args):
     # ---- CPU baseline (rank 0, N = 1 only) -----------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        n64 = int(round(extra["fine_applies_per_step"]["f64"]))
-        n32 = int(round(extra["fine_applies_per_step"]["f32"]))
+        n64, n32 = fine_applies(iters)
         cpu = cpu_iteration_estimate(dims, n64, n32)
 
     if world > 1:
@@ -427,11 +444,62 @@ def run_micro_apply(args):
     return 0
 
 
+def run_kernels(args):
+    """Per-kernel device time of args.kernels SIMP iterations after args.warmup, from the CUDA
+    activity records (CUPTI through torch.profiler: kernels are not serialised)."""
+    import collections
+    import re
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from loadpath_b200.grid import DevGrid
+    from loadpath_b200.simp import DeviceFilter, Top3dLoop
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    fixed, f = cantilever(dims)
+    g = DevGrid(dims)
+    rng = np.random.default_rng(1)
+    xr = g.cells_to_dev(np.exp(rng.uniform(np.log(1e-3), 0.0, dims)), torch.float64)
+    flt = DeviceFilter(g, 2.0)
+    x0 = g.cells_to_host(flt.apply(g.cell_field(torch.float64), xr, hs_out=flt.hs))
+    loop = Top3dLoop(dims, VOLFRAC, RMIN, fixed, f, rtol=RTOL, dtype=np.float32, x0=x0, penal=PENAL, emin=EMIN,
+                     move=MOVE, element="im")
+    for _ in range(args.warmup):
+        loop.step()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(args.kernels):
+            loop.step()
+        torch.cuda.synchronize()
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type != torch.autograd.DeviceType.CUDA:
+            continue
+        name = re.sub(r"\(.*", "", ev.name.replace("(anonymous namespace)::", "").replace("<unnamed>::", ""))
+        agg[name][0] += 1
+        agg[name][1] += getattr(ev, "device_time_total", 0.0) or ev.cuda_time_total
+    k = args.kernels
+    tot = sum(v[1] for v in agg.values())
+    print(f"{k} SIMP iterations after {args.warmup} warm-up at {dims[0]}x{dims[1]}x{dims[2]}: "
+          f"CG iterations {[h[2] for h in loop.history[-k:]]} (all: {[h[2] for h in loop.history]}), "
+          f"device time {tot / 1e3 / k:.3f} ms per iteration")
+    print(f"{'ms/iter':>9} {'share':>7} {'launches/iter':>13} {'us/launch':>10}  kernel")
+    for name, (c, t) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+        if t / tot < 0.002:
+            continue
+        print(f"{t / 1e3 / k:9.3f} {100 * t / tot:6.2f}% {c / k:13.1f} {t / c:10.1f}  {name[:90]}")
+    return 0
+
+
 def main():
     args = parse()
     sys.path.insert(0, ROOT)
     if args.micro == "apply":
         return run_micro_apply(args)
+    if args.kernels:
+        return run_kernels(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
