@@ -286,7 +286,7 @@ def run_b200(args):
             if tuple(pd.get("dims", ())) == tuple(dims):
                 traffic = pd.get("dram_bytes_per_launch")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "kernel": "k_apply_fine<float>",
+                    "traffic": traffic, "kernel": "k_apply_fine_x2 (float32)",
                     "algorithmic_bytes": b32, "avg_launch_us": avg * 1e6, "launches_timed": fine["f32_count"],
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
     phases = np.array([[a.elapsed_time(b) for a, b in zip(ev[:-1], ev[1:])] for ev in loop.timing])
