@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "lp_common.cuh"
+#include "lp_modal.cuh"
 #include "lp_tma.cuh"
 
 namespace {
@@ -795,30 +796,14 @@ extern "C" {
 // Ke (24 x 24, row-major, float64) -> the 45 coefficients of T Ke T^T / 64 in the fixed
 // pattern the kernel uses; -1 if Ke has weight outside the pattern (not an isotropic brick).
 int lpb_modal_ke(const double* ke, double* kmodal_out) {
-  static const int rows[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
-                               13, 13, 14, 14, 14, 15, 15, 16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21, 22, 23};
-  static const int cols[45] = {3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12,
-                               8, 13, 3, 7, 14, 15, 19, 11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22, 23};
+  static const int rows[LP_MODAL_NNZ] = LP_MODAL_ROWS;
+  static const int cols[LP_MODAL_NNZ] = LP_MODAL_COLS;
   if (!ke || !kmodal_out) return LP_ERR_ARG;
-  // H[m][k] = prod over axes a with bit a of m set of (2 * bit a of k - 1)
-  double h[8][8];
-  for (int m = 0; m < 8; ++m)
-    for (int k = 0; k < 8; ++k) {
-      double v = 1.0;
-      for (int a = 0; a < 3; ++a)
-        if ((m >> a) & 1) v *= ((k >> a) & 1) ? 1.0 : -1.0;
-      h[m][k] = v;
-    }
-  // K^ = T ke T^T / 64 with T = kron(H, I3)
   double kh[24][24];
   double amax = 0.0;
   for (int r = 0; r < 24; ++r)
     for (int c = 0; c < 24; ++c) {
-      int mr = r / 3, cr = r % 3, mc = c / 3, cc = c % 3;
-      double s = 0.0;
-      for (int k1 = 0; k1 < 8; ++k1)
-        for (int k2 = 0; k2 < 8; ++k2) s += h[mr][k1] * ke[(3 * k1 + cr) * 24 + 3 * k2 + cc] * h[mc][k2];
-      kh[r][c] = s / 64.0;
+      kh[r][c] = lp_modal_entry(ke, r, c);
       if (fabs(kh[r][c]) > amax) amax = fabs(kh[r][c]);
     }
   bool in_pattern[24][24] = {};

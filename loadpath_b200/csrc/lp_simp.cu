@@ -3,7 +3,10 @@
 // strain energy u_e^T Ke v_e (loadpath/femops.py:51-78, loadpath/mg.py:975-988), sensitivities
 // (loadpath/benchmarks/reference.py:89-99) and the OC volume pass (reference.py:100-110).
 // All in float64.
+#include <algorithm>
+
 #include "lp_common.cuh"
+#include "lp_modal.cuh"
 
 #define LP_MAX_TAPS 1024
 #define LP_MAX_LAMBDA 64
@@ -62,37 +65,77 @@ __global__ void k_simp_law(double* __restrict__ e, const double* __restrict__ x,
   }
 }
 
-// per-cell u_e^T ke v_e on the node grid (v = u when v is null), float64; also optional
-// compliance partial sum_c e_c * ce_c
+// per-cell u_e^T ke v_e on the node grid (v = u when v is null), float64. The product is taken in
+// the corner-parity basis: u^ = T u_e, v^ = T v_e (eight-point Walsh transforms per component),
+// u_e^T ke v_e = u^T K^ v^ with K^ = T ke T^T / 64 formed by each block from ke. When K^ has
+// weight outside the 45-entry pattern (not an isotropic brick) the block takes the dense
+// 21 x 21 modal product instead.
 template <typename T>
-__global__ void k_element_energy(double* __restrict__ ce, const T* __restrict__ u, const T* __restrict__ v,
-                                 const double* __restrict__ ke, LpGrid g) {
-  __shared__ double sk[576];
-  for (int i = threadIdx.x; i < 576; i += blockDim.x) sk[i] = ke[i];
+__global__ void __launch_bounds__(128) k_element_energy(double* __restrict__ ce, const T* __restrict__ u,
+                                                        const T* __restrict__ v, const double* __restrict__ ke,
+                                                        LpGrid g) {
+  __shared__ double kh[576];
+  __shared__ double wmax[4];
+  constexpr int rows[LP_MODAL_NNZ] = LP_MODAL_ROWS;
+  constexpr int cols[LP_MODAL_NNZ] = LP_MODAL_COLS;
+  double amax = 0.0;
+  for (int i = threadIdx.x; i < 576; i += blockDim.x) {
+    kh[i] = lp_modal_entry(ke, i / 24, i % 24);
+    amax = fmax(amax, fabs(kh[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = amax;
   __syncthreads();
+  amax = fmax(fmax(wmax[0], wmax[1]), fmax(wmax[2], wmax[3]));
+  int off = 0;
+  for (int i = threadIdx.x; i < 576; i += blockDim.x) {
+    bool in = false;
+    for (int j = 0; j < LP_MODAL_NNZ; ++j) in |= (rows[j] * 24 + cols[j] == i);
+    off |= (!in && fabs(kh[i]) > 1e-12 * amax);
+  }
+  const bool dense = __syncthreads_or(off) != 0;
+
   const long long total = (long long)g.nx * g.ny * g.nz;
   const long long cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    int y = (int)(q % g.ny);
-    int x = (int)(q / g.ny);
-    double ue[24], ve[24];
+    const int z = (int)(t % g.nz);
+    const long long q = t / g.nz;
+    const int y = (int)(q % g.ny);
+    const int x = (int)(q / g.ny);
+    double uh[24], vh[24];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      long long n = g.node(x + cx_(k), y + cy_(k), z + cz_(k));
+    for (int c = 0; c < 3; ++c) {
+      double a[8], b[8];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        ue[3 * k + c] = (double)u[c * cs + n];
-        ve[3 * k + c] = v ? (double)v[c * cs + n] : ue[3 * k + c];
+      for (int k = 0; k < 8; ++k) {
+        const long long n = c * cs + g.node(x + cx_(k), y + cy_(k), z + cz_(k));
+        a[k] = (double)u[n];
+        b[k] = v ? (double)v[n] : 0.0;
+      }
+      lp_walsh8(a);
+      lp_walsh8(b);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        uh[3 * m + c] = a[m];
+        vh[3 * m + c] = b[m];
       }
     }
-    // j outer, k inner, (u_j ke_jk) v_k: the reference's summation order
-    double s = 0.0;
-    for (int j = 0; j < 24; ++j) {
-      double uj = ue[j];
+    if (!v) {
 #pragma unroll
-      for (int k = 0; k < 24; ++k) s += uj * sk[j * 24 + k] * ve[k];
+      for (int i = 0; i < 24; ++i) vh[i] = uh[i];
+    }
+    double s = 0.0;
+    if (!dense) {
+#pragma unroll
+      for (int j = 0; j < LP_MODAL_NNZ; ++j) s = fma(uh[rows[j]] * kh[rows[j] * 24 + cols[j]], vh[cols[j]], s);
+    } else {
+#pragma unroll
+      for (int r = 3; r < 24; ++r) {
+        double f = 0.0;
+#pragma unroll
+        for (int c = 3; c < 24; ++c) f = fma(kh[r * 24 + c], vh[c], f);
+        s = fma(uh[r], f, s);
+      }
     }
     ce[g.cell(x, y, z)] = s;
   }
@@ -234,6 +277,7 @@ __global__ void k_sum_final_s(const double* __restrict__ part, int n, double* __
 #define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
 #define LP_ST ((cudaStream_t)stream)
 #define LP_SIMP_BLOCKS 592
+#define LP_ENERGY_BLOCKS 592  // 148 SMs x 4 resident blocks of 128 (128 registers)
 
 extern "C" {
 
@@ -263,7 +307,8 @@ int lpb_element_energy_f64(double* ce, const double* u, const double* v, const d
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
   long long total = (long long)g.nx * g.ny * g.nz;
-  k_element_energy<double><<<lp_blocks(total, 128), 128, 0, LP_ST>>>(ce, u, v, ke, g);
+  k_element_energy<double><<<(int)std::min<long long>(lp_blocks(total, 128), LP_ENERGY_BLOCKS), 128, 0, LP_ST>>>(
+      ce, u, v, ke, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -272,7 +317,8 @@ int lpb_element_energy_f32(double* ce, const float* u, const float* v, const dou
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
   long long total = (long long)g.nx * g.ny * g.nz;
-  k_element_energy<float><<<lp_blocks(total, 128), 128, 0, LP_ST>>>(ce, u, v, ke, g);
+  k_element_energy<float><<<(int)std::min<long long>(lp_blocks(total, 128), LP_ENERGY_BLOCKS), 128, 0, LP_ST>>>(
+      ce, u, v, ke, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -23,7 +23,7 @@ from ._lib import lib
 from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
-__all__ = ["filter_taps", "DeviceFilter", "density_filter", "Top3dLoop", "_project", "_dproject"]
+__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "Top3dLoop", "_project", "_dproject"]
 
 
 def filter_taps(radius: float, pitch: float = 1.0):
@@ -106,6 +106,53 @@ def _dproject(xt, beta, eta):
     return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
 
 
+def oc_bisection(volumes, target, l1=0.0, l2=1e9, tol=1e-3, width=31):
+    """The reference's bisection (loadpath/benchmarks/reference.py:100-110):
+        while (l2 - l1) / (l1 + l2) > tol: lmid = (l1 + l2) / 2; V(lmid) > target ? l1 = lmid : l2 = lmid
+    with V evaluated in batches: `volumes(cands)` returns V at `width` multipliers at once.
+
+    V is non-increasing in the multiplier (every cell's OC step is), so an evaluated
+    V(lam) <= target decides every midpoint >= lam (l2 = lmid) and V(lam) > target every
+    midpoint <= lam (l1 = lmid). The walk decides each midpoint from the evaluations so far and
+    stops at the first one they leave open. While l1 = 0 a batch is the ladder l2 / 2^(2i+1) of
+    the midpoints the walk visits next (exact halvings, so they equal the walk's own midpoints);
+    otherwise it is the `width` midpoints of the next levels of the bisection tree below the
+    open one, breadth first. Returns the last midpoint (the reference's lmid) and the
+    number of batches."""
+    below = math.inf    # smallest multiplier seen with V <= target
+    above = -math.inf   # largest multiplier seen with V > target
+    lmid = None
+    passes = 0
+    while (l2 - l1) / (l1 + l2) > tol:
+        m = 0.5 * (l2 + l1)
+        if m >= below:
+            lmid = l2 = m
+            continue
+        if m <= above:
+            lmid = l1 = m
+            continue
+        if l1 == 0.0:
+            cands = [l2 * 2.0 ** -(2 * i + 1) for i in range(width)]
+        else:
+            nodes, cands = [(l1, l2)], []
+            while len(cands) < width:
+                nxt = []
+                for a, b in nodes:
+                    mm = 0.5 * (b + a)
+                    cands.append(mm)
+                    nxt += [(a, mm), (mm, b)]
+                nodes = nxt
+            cands = cands[:width]
+        vols = volumes(cands)
+        passes += 1
+        for lam, v in zip(cands, vols):
+            if v > target:
+                above = max(above, lam)
+            else:
+                below = min(below, lam)
+    return lmid, passes
+
+
 class Top3dLoop:
     """top3d's SIMP loop with the density filter, on the device
     (loadpath/benchmarks/reference.py:74-117), solved by the device MG-PCG.
@@ -173,41 +220,20 @@ class Top3dLoop:
         self.filter.apply(self.dcf, self.dc, hs_in=self.filter.hs)
 
     def oc(self):
-        """top3d's bisection on the volume multiplier (loadpath/benchmarks/reference.py:100-110),
-        five levels of the bisection tree per pass over the cells."""
+        """top3d's bisection on the volume multiplier (loadpath/benchmarks/reference.py:100-110);
+        the multipliers are evaluated on the device, 31 per pass over the cells."""
         L = lib()
         st = stream_handle()
         g = self.grid
-        target = self.volfrac * self.ncell
-        l1, l2 = 0.0, 1e9
-        lmid = None
-        while (l2 - l1) / (l1 + l2) > 1e-3:
-            # the 31 midpoints the next five bisection levels can reach, breadth first
-            nodes = [(l1, l2)]
-            cands = []
-            for depth in range(5):
-                nxt = []
-                for a, b in nodes:
-                    m = 0.5 * (b + a)
-                    cands.append(m)
-                    nxt += [(a, m), (m, b)]
-                nodes = nxt
+
+        def volumes(cands):
             self._lam.copy_(torch.tensor(cands, dtype=torch.float64))
             L.lpb_oc_volumes(self._vols.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(),
                              self.filter.gv.data_ptr(), self._lam.data_ptr(), 31, self.move, self._part.data_ptr(),
                              *g.args, st)
-            vols = self._vols.cpu().numpy()
-            idx = 0
-            for depth in range(5):
-                if not (l2 - l1) / (l1 + l2) > 1e-3:
-                    break
-                lmid = 0.5 * (l2 + l1)
-                if vols[idx] > target:
-                    l1 = lmid
-                    idx = 2 * idx + 2
-                else:
-                    l2 = lmid
-                    idx = 2 * idx + 1
+            return self._vols.cpu().numpy()
+
+        lmid, self.oc_passes = oc_bisection(volumes, self.volfrac * self.ncell)
         L.lpb_oc_apply(self.xnew.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(), lmid,
                        self.move, self._part.data_ptr(), self._scal[1:].data_ptr(), *g.args, st)
         self.lmid = lmid

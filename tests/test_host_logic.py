@@ -1,0 +1,60 @@
+"""Host-side logic that needs no GPU: the batched OC bisection walk."""
+import numpy as np
+import pytest
+
+from loadpath_b200.simp import oc_bisection
+
+
+def _volume_fn(seed, n=4000, move=0.2):
+    """V(lam) = sum_c clamp(x sqrt(-dc / dv) / sqrt(lam), max(0, x - move), min(1, x + move)) gv,
+    the OC step's filtered volume, on random cells."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, 1.0, n)
+    x[rng.random(n) < 0.1] = 0.0
+    dc = -10.0 ** rng.uniform(-9, 3, n)
+    dv = rng.uniform(0.5, 1.5, n)
+    gv = rng.uniform(0.5, 1.5, n)
+    ts = x * np.sqrt(-dc / dv)
+    lo, hi = np.maximum(0.0, x - move), np.minimum(1.0, x + move)
+
+    def vol(lam):
+        return float(np.sum(np.clip(ts / np.sqrt(lam), lo, hi) * gv))
+
+    return vol, float(np.sum(gv))
+
+
+def _plain(vol, target, l1=0.0, l2=1e9):
+    lmid, n = None, 0
+    while (l2 - l1) / (l1 + l2) > 1e-3:
+        lmid = 0.5 * (l2 + l1)
+        n += 1
+        if vol(lmid) > target:
+            l1 = lmid
+        else:
+            l2 = lmid
+    return lmid, n
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("frac", [0.05, 0.3, 0.6])
+def test_oc_bisection_follows_the_plain_walk(seed, frac):
+    vol, total = _volume_fn(seed)
+    target = frac * total
+    want, steps = _plain(vol, target)
+    got, passes = oc_bisection(lambda cands: [vol(c) for c in cands], target)
+    assert got == want
+    # one ladder pass and at most ceil(remaining levels / 5) tree passes
+    assert passes <= 1 + (steps + 4) // 5
+    assert passes <= 5
+
+
+def test_oc_bisection_plateaus_and_ties():
+    """A step-function V (whole ranges of multipliers give the same volume, one exactly equal to
+    the target) still gives the plain walk's midpoint."""
+    def vol(lam):
+        return float(np.floor(np.log2(1e9 / lam)))
+
+    for target in (0.0, 3.0, 17.0, 40.0, 100.0):
+        want, _ = _plain(vol, target)
+        got, _ = oc_bisection(lambda cands: [vol(c) for c in cands], target)
+        assert got == want
