@@ -423,7 +423,7 @@ def run_micro_apply(args):
     for lv in (ge._l0s, ge.levels[0]):
         gr = lv.grid
         m = torch.stack([((lv.mask >> c) & 1) for c in range(3)]).to(lv.dtype)
-        u = torch.randn((3, gr.NX, gr.NY, gr.pz), generator=torch.Generator(device="cuda").manual_seed(101),
+        u = torch.randn((3, gr.pz // 4, gr.NY, gr.NX, 4), generator=torch.Generator(device="cuda").manual_seed(101),
                         device="cuda", dtype=torch.float64).to(lv.dtype) * m
         o = gr.node_field(lv.dtype)
         for _ in range(3):

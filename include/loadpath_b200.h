@@ -4,11 +4,14 @@
  * legacy default stream) and returns an int status: 0 ok, -1 bad arguments, -2 launch error,
  * -3 size beyond a kernel's limit. Nothing allocates: callers own every buffer.
  *
- * Layouts (C order):
- *   node field  (3, nx+1, ny+1, pz)  pz >= nz+1 is the z pitch in elements
- *   cell field  (nx, ny, cpz)        cpz >= nz
- *   node mask   (nx+1, ny+1, pz) uint8: bits 0..2 solved dof per component (alive and not
- *               held), bits 3..5 alive (carries stiffness) per component
+ * Layouts (C order): z is cut into chunks of four planes, the chunk index slowest, so that a
+ * chunk's four planes of a row of x are contiguous (node (x, y, z) of a component at
+ * ((z / 4 * (ny+1) + y) * (nx+1) + x) * 4 + z % 4):
+ *   node field  (3, pz/4, ny+1, nx+1, 4)  pz >= nz+1, pz % 4 == 0
+ *   cell field  (cpz/4, ny, nx, 4)        cpz >= nz, cpz % 4 == 0
+ *   node mask   (pz/4, ny+1, nx+1, 4) uint8: bits 0..2 solved dof per component (alive and
+ *               not held), bits 3..5 alive (carries stiffness) per component
+ *   z padding (node z > nz, cell z >= nz) holds zeros
  *   cell matrices (cells, 24, 24), rows/cols ordered 3*corner + component, corner k at
  *               (k & 1, k >> 1 & 1, k >> 2 & 1)
  * `LP_GRID` below stands for the five ints  nx, ny, nz, pz, cpz  of one level;
@@ -60,10 +63,8 @@ int lpb_modal_ke(const double* ke, double* kmodal_out);
  * entry-major ((300, cells)); ft is caller scratch of 24 * cells values. Replaces
  * mgops._product_explicit + _scatter_into (loadpath/mgops.py:131-146, 181-217). */
 int lpb_modal_g1(const double* ke, double* g1_out);
-int lpb_apply_weights_march_f32(float* out, const float* u, const float* w, const int* patch_id, const float* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
-int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, const int* patch_id, const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* level 1, TMA-staged: the Walsh coefficients c = H w of each cell's child moduli in the
- * layout (nx, ny, cpz/4, 8, 4) from lpb_walsh_chunks_* (once per hierarchy, after the patch
+ * layout (cpz/4, ny, nx, 8, 4) from lpb_walsh_chunks_* (once per hierarchy, after the patch
  * cells' weights are zeroed), then the march with u arriving by TMA box loads into a 3-stage
  * mbarrier ring and outputs leaving by TMA stores; g1, pbox HOST; err: device int, set when a
  * bounded wait gave up (or to an alignment code 20..25) */

@@ -120,23 +120,25 @@ struct alignas(128) Slot {
 
 template <typename T>
 struct FineSmem {
-  Slot<T, 3 * BOX * BOX * 4> u[NSTAGE];              // node values: [comp][x][y][z]
-  Slot<T, BOX * BOX * 4> e[NSTAGE];                  // cell moduli: [x][y][z] (16 used per side)
-  Slot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store
+  Slot<T, 3 * BOX * BOX * 4> u[NSTAGE];              // node values: [comp][y][x][z]
+  Slot<T, BOX * BOX * 4> e[NSTAGE];                  // cell moduli: [y][x][z] (16 used per side)
+  Slot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store [comp][y][x][z]
   T red[3][4][TXC * TYC];                            // y-neighbour exchange
   alignas(8) uint64_t full[NSTAGE];
 };
 
 template <typename T>
 __device__ __forceinline__ T* u_at(FineSmem<T>& sm, int s, int c, int x, int y) {
-  return &sm.u[s].v[((c * BOX + x) * BOX + y) * 4];
+  return &sm.u[s].v[((c * BOX + y) * BOX + x) * 4];
 }
 
+// The fields as TMA tensors: a chunk's row of x columns (4 z values each) is the inner
+// dimension, so every box row is 16 * (x extent) contiguous bytes.
 template <typename T>
 struct TileMaps {
-  CUtensorMap u;    // (pz, NY, NX, 3), box (4, 17, 17, 3)
-  CUtensorMap e;    // (cpz, ny, nx),    box (4, 17, 17)
-  CUtensorMap out;  // (pz, NY, NX, 3), box (4, 15, 15, 3)
+  CUtensorMap u;    // (4 NX, NY, pz / 4, 3), box (4 * 17, 17, 1, 3)
+  CUtensorMap e;    // (4 nx, ny, cpz / 4),    box (4 * 17, 17, 1)
+  CUtensorMap out;  // (4 NX, NY, pz / 4, 3), box (4 * 15, 15, 1, 3)
 };
 
 template <typename T>
@@ -203,10 +205,9 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
   __syncthreads();
   auto issue = [&](int k) {
     const int s = k % NSTAGE;
-    const int z = 4 * (cstart + k);
     lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
-    lp_tma_load_4d(sm.u[s].v, &maps.u, z, y0 - 1, x0 - 1, 0, &sm.full[s]);
-    lp_tma_load_3d(sm.e[s].v, &maps.e, z, y0 - 1, x0 - 1, &sm.full[s]);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
+    lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, cstart + k, &sm.full[s]);
   };
   if (tid == 0) {
     issue(0);
@@ -252,7 +253,7 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
         un[q][cc][4] = has_next ? *u_at(sm, (k + 1) % NSTAGE, cc, i + (q & 1), j + (q >> 1)) : T(0);
       }
     T ev[4];
-    Vec4<T>::lds(&sm.e[s].v[(i * BOX + j) * 4], ev);
+    Vec4<T>::lds(&sm.e[s].v[(j * BOX + i) * 4], ev);
 
     T a_lo[4][3];
     {
@@ -318,11 +319,10 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
     }
     __syncthreads();
     if (own) {
-      const long long obase = g.node(x0 - 1 + i, y0 - 1 + j, 0);
       const bool inside = x0 - 1 + i < g.NX() && y0 - 1 + j < g.NY();
       uint8_t mbs[4] = {0, 0, 0, 0};
       if (inside) {
-        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + obase + 4 * c);
+        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + g.node(x0 - 1 + i, y0 - 1 + j, 4 * c));
         mbs[0] = mb.x; mbs[1] = mb.y; mbs[2] = mb.z; mbs[3] = mb.w;
       }
 #pragma unroll
@@ -334,13 +334,13 @@ k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict
           o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
           pacc += (double)o[t] * (double)un[0][cc][t];   // this node's u: column q = 0
         }
-        Vec4<T>::sts(&sm.o[k & 1].v[((cc * (TXC - 1) + (i - 1)) * (TYC - 1) + (j - 1)) * 4], o);
+        Vec4<T>::sts(&sm.o[k & 1].v[((cc * (TYC - 1) + (j - 1)) * (TXC - 1) + (i - 1)) * 4], o);
       }
     }
     lp_fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      lp_tma_store_4d(&maps.out, 4 * c, y0, x0, 0, sm.o[k & 1].v);
+      lp_tma_store_4d(&maps.out, 4 * x0, y0, c, 0, sm.o[k & 1].v);
       lp_bulk_commit();
     }
   }
@@ -503,7 +503,7 @@ struct FineSmem2 {
 };
 
 __device__ __forceinline__ const float* u_at2(const FineSmem2& sm, int s, int c, int x, int y) {
-  return &sm.u[s].v[((c * BOX + x) * BOX + y) * 4];
+  return &sm.u[s].v[((c * BOX + y) * BOX + x) * 4];
 }
 
 // One barrier per chunk: each thread waits for its stage, computes, publishes its y-corner
@@ -531,8 +531,8 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
   const int nproc = c_end - cstart;
   const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
   const bool writer = i >= 1 && j >= 1 && nx_ < g.NX() && ny_ < g.NY();
-  const long long obase = writer ? g.node(nx_, ny_, 0) : 0;
-  const long long cs = g.comp_stride();
+  const long long obase = writer ? g.node(nx_, ny_, 0) : 0;   // chunk c at obase + c * zcs
+  const long long cs = g.comp_stride(), zcs = g.node_zc_stride();
   constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(float);
   constexpr uint32_t EBYTES = BOX * BOX * 4 * sizeof(float);
   __shared__ int bad;
@@ -558,10 +558,9 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
   __syncthreads();
   auto issue = [&](int k) {
     const int s = k % NST2;
-    const int z = 4 * (cstart + k);
     lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
-    lp_tma_load_4d(sm.u[s].v, &maps.u, z, y0 - 1, x0 - 1, 0, &sm.full[s]);
-    lp_tma_load_3d(sm.e[s].v, &maps.e, z, y0 - 1, x0 - 1, &sm.full[s]);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
+    lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, cstart + k, &sm.full[s]);
   };
   if (tid == 0)
     for (int kk = 0; kk < NST2 - 1 && kk < nload; ++kk) issue(kk);
@@ -577,12 +576,12 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
     const int s = k % NST2;
     // the stage refilled here was last read in the previous chunk, before its barrier
     if (tid == 0 && k + NST2 - 1 < nload) issue(k + NST2 - 1);
-    const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + 4 * c)) : 0u;
+    const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + c * zcs)) : 0u;
     bool ok = lp_mbar_wait(&sm.full[s], (k / NST2) & 1);
     const bool has_next = k + 1 < nload;
     if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NST2], ((k + 1) / NST2) & 1);
     // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
-    const float* ecol = &sm.e[s].v[(i * BOX + j) * 4];
+    const float* ecol = &sm.e[s].v[(j * BOX + i) * 4];
     f2_t m23[4][3];
     float m4[4][3];
     auto load_b = [&]() {
@@ -694,7 +693,7 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
         if (!((mb4 >> (8 + cc)) & 1u)) o.y = 0.0f;
         if (!((mb4 >> (16 + cc)) & 1u)) o.z = 0.0f;
         if (!((mb4 >> (24 + cc)) & 1u)) o.w = 0.0f;
-        *reinterpret_cast<float4*>(out + cc * cs + obase + 4 * c) = o;
+        *reinterpret_cast<float4*>(out + cc * cs + obase + c * zcs) = o;
       }
     }
   }
@@ -739,11 +738,11 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
   const bool x2 = sizeof(T) == 4;
   const uint32_t zc = 4;
   TileMaps<T> maps;
-  const uint64_t nd[4] = {(uint64_t)g.pz, (uint64_t)g.NY(), (uint64_t)g.NX(), 3};
-  const uint64_t cd[3] = {(uint64_t)g.cpz, (uint64_t)g.ny, (uint64_t)g.nx};
-  const uint32_t bin[4] = {zc, BOX, BOX, 3};
-  const uint32_t be[3] = {zc, BOX, BOX};
-  const uint32_t bout[4] = {zc, TXC - 1, TYC - 1, 3};
+  const uint64_t nd[4] = {zc * (uint64_t)g.NX(), (uint64_t)g.NY(), (uint64_t)g.pz / zc, 3};
+  const uint64_t cd[3] = {zc * (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.cpz / zc};
+  const uint32_t bin[4] = {zc * BOX, BOX, 1, 3};
+  const uint32_t be[3] = {zc * BOX, BOX, 1};
+  const uint32_t bout[4] = {zc * (TXC - 1), TYC - 1, 1, 3};
   if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.e, e, 3, cd, be, sizeof(T)) ||
       !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
     return LP_ERR_ARG;

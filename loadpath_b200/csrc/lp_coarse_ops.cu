@@ -29,31 +29,6 @@ struct G1 {
   T c[279];
 };
 
-template <typename T>
-struct V4;
-template <>
-struct V4<float> {
-  static __device__ __forceinline__ void ld(const float* p, float (&v)[4]) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
-  static __device__ __forceinline__ void st(float* p, const float (&v)[4]) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  }
-};
-template <>
-struct V4<double> {
-  static __device__ __forceinline__ void ld(const double* p, double (&v)[4]) {
-    double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-  static __device__ __forceinline__ void st(double* p, const double (&v)[4]) {
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
-  }
-};
-
 // f = sum_t c_t G^_t v on the corner-parity modes (index 3 * mode + component)
 template <typename T>
 __device__ __forceinline__ void g1_product(const G1<T>& g, const T (&c)[8], const T (&v)[24], T (&f)[24]) {
@@ -431,144 +406,11 @@ __device__ __forceinline__ void xy4(T u00, T u10, T u01, T u11, T (&a)[4]) {
   a[3] = dx1 - dx0;
 }
 
-// x-y modes of node plane z of the four columns around cell column (cx, cy), one component
-template <typename T>
-__device__ __forceinline__ void plane_modes(const T* __restrict__ u, const long long (&col)[4], const bool (&ok)[4],
-                                            long long cs, int z, int pz, T (&a)[4][3]) {
-#pragma unroll
-  for (int cc = 0; cc < 3; ++cc) {
-    T v[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = (ok[q] && z < pz) ? __ldg(u + cc * cs + col[q] + z) : T(0);
-    T m[4];
-    xy4(v[0], v[1], v[2], v[3], m);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) a[q][cc] = m[q];
-  }
-}
-
-// one cell's modal forces from the x-y modes of its lower and upper node planes
-template <typename T>
-__device__ __forceinline__ void weights_cell(const G1<T>& gc, const T (&a_lo)[4][3], const T (&a_hi)[4][3],
-                                             const T (&wk)[8], T (&f)[24]) {
-  T v[24], cw[8];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int cc = 0; cc < 3; ++cc) {
-      const T lo = a_lo[q][cc], hi = a_hi[q][cc];
-      v[3 * q + cc] = lo + hi;
-      v[3 * (q + 4) + cc] = hi - lo;
-    }
-  fwht8(wk, cw);
-  g1_product<T>(gc, cw, v, f);
-}
-
-// level-1 operator, u zero on masked dofs: out = m K u
-template <typename T>
-__global__ void __launch_bounds__(TXC * TYC, 1)
-k_weights_march(T* __restrict__ out, const T* __restrict__ u, const T* __restrict__ w,
-                const uint8_t* __restrict__ mask, const G1<T> gc, LpGrid g, int zch, int nchunks) {
-  __shared__ T red[3][4][TXC * TYC];     // corner 01 + 11 (-> y + 1)
-  __shared__ T own_s[3][4][TXC * TYC];   // corner 00 + 10 of the -x neighbour
-  const int tid = threadIdx.x;
-  const int i = tid % TXC, j = tid / TXC;
-  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
-  const int c_begin = blockIdx.z * zch;
-  const int c_end = min(c_begin + zch, nchunks);
-  if (c_begin >= c_end) return;
-  const int cx = x0 - 1 + i, cy = y0 - 1 + j;
-  const int NX = g.NX(), NY = g.NY();
-  const long long cs = g.comp_stride(), ncp = g.cells_padded();
-  const bool cell_ok = cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny;
-  const bool own = i >= 1 && j >= 1 && cx < NX && cy < NY;
-  bool col_ok[4];
-  long long col_base[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int nx_ = cx + (q & 1), ny_ = cy + (q >> 1);
-    col_ok[q] = nx_ >= 0 && nx_ < NX && ny_ >= 0 && ny_ < NY;
-    col_base[q] = col_ok[q] ? g.node(nx_, ny_, 0) : 0;
-  }
-  const long long ebase = cell_ok ? g.cell(cx, cy, 0) : 0;
-  const long long obase = own ? g.node(cx, cy, 0) : 0;
-  T up_carry[4][3], a_lo[4][3];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) up_carry[q][c] = T(0);
-  const int z0 = 4 * c_begin;
-  if (c_begin > 0) {
-    // the cell below the segment: its upper face starts the carry
-    T a_hi[4][3], wk[8], f[24];
-    plane_modes(u, col_base, col_ok, cs, z0 - 1, g.pz, a_lo);
-    plane_modes(u, col_base, col_ok, cs, z0, g.pz, a_hi);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) wk[k] = cell_ok ? __ldg(w + k * ncp + ebase + z0 - 1) : T(0);
-    weights_cell(gc, a_lo, a_hi, wk, f);
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        up_carry[q][cc] = f[3 * q + cc] + f[3 * (q + 4) + cc];
-        a_lo[q][cc] = a_hi[q][cc];
-      }
-  } else {
-    plane_modes(u, col_base, col_ok, cs, 0, g.pz, a_lo);
-  }
-
-  for (int ch = c_begin; ch < c_end; ++ch) {
-    const int z = 4 * ch;
-#pragma unroll 1
-    for (int t = 0; t < 4; ++t) {
-      T a_hi[4][3], wk[8], f[24];
-      plane_modes(u, col_base, col_ok, cs, z + t + 1, g.pz, a_hi);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) wk[k] = cell_ok ? __ldg(w + k * ncp + ebase + z + t) : T(0);
-      weights_cell(gc, a_lo, a_hi, wk, f);
-      T fp[4][3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const T f0 = f[3 * q + cc], f1 = f[3 * (q + 4) + cc];
-          fp[q][cc] = up_carry[q][cc] + (f0 - f1);
-          up_carry[q][cc] = f0 + f1;
-          a_lo[q][cc] = a_hi[q][cc];
-        }
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const T t0 = fp[0][cc] - fp[2][cc], t1 = fp[1][cc] - fp[3][cc];
-        const T t2 = fp[0][cc] + fp[2][cc], t3 = fp[1][cc] + fp[3][cc];
-        const T c10 = __shfl_up_sync(0xffffffffu, t0 + t1, 1, TXC);
-        const T c11 = __shfl_up_sync(0xffffffffu, t2 + t3, 1, TXC);
-        own_s[cc][t][tid] = (t0 - t1) + c10;
-        red[cc][t][tid] = (t2 - t3) + c11;
-      }
-    }
-    __syncthreads();
-    if (own) {
-      const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + obase + z);
-      const uint8_t mbs[4] = {mb.x, mb.y, mb.z, mb.w};
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        T o[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const T sv = own_s[cc][t][tid] + red[cc][t][tid - TXC];
-          o[t] = ((mbs[t] >> cc) & 1) ? sv : T(0);
-        }
-        V4<T>::st(out + cc * cs + obase + z, o);
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ---- level 1, TMA-staged march -------------------------------------------------------------
 // The chunked Walsh layout: c = H w per cell (the coefficients of the eight G_t), stored
-// (nx, ny, cpz / 4, 8, 4) so one cell column's four cells of a z chunk are 128 contiguous
-// bytes. Formed once per hierarchy (after the patch cells' weights are zeroed).
+// (cpz / 4, ny, nx, 8, 4) so one cell column's four cells of a z chunk are 128 contiguous
+// bytes (float32) and a row of x columns is one run. Formed once per hierarchy (after the
+// patch cells' weights are zeroed).
 template <typename T>
 __global__ void k_walsh_chunks(T* __restrict__ wc, const T* __restrict__ w, LpGrid g) {
   const long long ncp = g.cells_padded();
@@ -577,9 +419,7 @@ __global__ void k_walsh_chunks(T* __restrict__ wc, const T* __restrict__ w, LpGr
 #pragma unroll
     for (int k = 0; k < 8; ++k) wk[k] = w[k * ncp + c];
     fwht8(wk, cw);
-    const long long col = c / g.cpz;
-    const int z = (int)(c % g.cpz);
-    T* dst = wc + (col * (g.cpz / 4) + z / 4) * 32 + (z & 3);
+    T* dst = wc + (c >> 2) * 32 + (c & 3);
 #pragma unroll
     for (int k = 0; k < 8; ++k) dst[k * 4] = cw[k];
   }
@@ -595,8 +435,8 @@ struct alignas(128) WSlot {
 
 template <typename T>
 struct WSmem {
-  WSlot<T, 3 * WBOX * WBOX * 4> u[WSTAGE];            // node values [comp][x][y][z]
-  WSlot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store
+  WSlot<T, 3 * WBOX * WBOX * 4> u[WSTAGE];            // node values [comp][y][x][z]
+  WSlot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store [comp][y][x][z]
   T red[3][4][TXC * TYC];                             // corners 01 + 11 (to y + 1)
   T own[3][4][TXC * TYC];                             // corners 00 + 10 with the -x neighbour's
   alignas(8) uint64_t full[WSTAGE];
@@ -604,8 +444,8 @@ struct WSmem {
 
 template <typename T>
 struct WMaps {
-  CUtensorMap u;    // (pz, NY, NX, 3), box (4, 17, 17, 3)
-  CUtensorMap out;  // (pz, NY, NX, 3), box (4, 15, 15, 3)
+  CUtensorMap u;    // (4 NX, NY, pz / 4, 3), box (4 * 17, 17, 1, 3)
+  CUtensorMap out;  // (4 NX, NY, pz / 4, 3), box (4 * 15, 15, 1, 3)
 };
 
 // node-plane forces of one cell: rows (3q + cc, 3(q + 4) + cc) of the modal product give the
@@ -635,8 +475,8 @@ __device__ __forceinline__ void slot_modes(const T* __restrict__ slot, int i, in
   for (int cc = 0; cc < 3; ++cc) {
     const T* b = slot + cc * WBOX * WBOX * 4 + zz;
     T m[4];
-    xy4(b[(i * WBOX + j) * 4], b[((i + 1) * WBOX + j) * 4], b[(i * WBOX + j + 1) * 4],
-        b[((i + 1) * WBOX + j + 1) * 4], m);
+    xy4(b[(j * WBOX + i) * 4], b[(j * WBOX + i + 1) * 4], b[((j + 1) * WBOX + i) * 4],
+        b[((j + 1) * WBOX + i + 1) * 4], m);
 #pragma unroll
     for (int q = 0; q < 4; ++q) a[q][cc] = m[q];
   }
@@ -647,7 +487,8 @@ __device__ __forceinline__ void slot_modes(const T* __restrict__ slot, int i, in
 // 168 or 128 (two blocks) spills and runs slower (65 us against 47 us at 128 x 64 x 64 cells).
 // A block owns 15 x 15 node columns over a z segment and runs 16 x 16 threads,
 // one per cell column plus a one-cell halo; u arrives by TMA into a 3-stage mbarrier ring
-// (box 4 x 17 x 17 x 3), the Walsh coefficients by 128-byte loads per cell column and chunk,
+// (one chunk of 17 x 17 node columns x 3 components), the Walsh coefficients by 128-byte loads
+// per cell column and chunk,
 // the outputs leave by TMA stores. Waits are bounded and a block that gives up sets *err.
 template <typename T>
 __global__ void __launch_bounds__(TXC * TYC, 1)
@@ -668,7 +509,8 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
   const bool own = i >= 1 && j >= 1;
   const int cx = x0 - 1 + i, cy = y0 - 1 + j;
   const bool cell_ok = cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny;
-  const T* wcol = wc + (cell_ok ? ((long long)cx * g.ny + cy) * (g.cpz / 4) * 32 : 0);
+  const long long wstride = 32LL * g.nx * g.ny;   // one chunk of Walsh runs to the next
+  const T* wcol = wc + (cell_ok ? ((long long)cy * g.nx + cx) * 32 : 0);
   constexpr uint32_t UBYTES = 3 * WBOX * WBOX * 4 * sizeof(T);
   __shared__ int bad;
   if (tid == 0) {
@@ -695,7 +537,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
   auto issue = [&](int k) {
     const int s = k % WSTAGE;
     lp_mbar_expect_tx(&sm.full[s], UBYTES);
-    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (cstart + k), y0 - 1, x0 - 1, 0, &sm.full[s]);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
   };
   if (tid == 0) {
     issue(0);
@@ -728,7 +570,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
     const T* us = sm.u[s].v;
     const T* un = sm.u[(k + 1) % WSTAGE].v;
     if (k == 0) slot_modes(us, i, j, halo ? 3 : 0, a_lo);
-    const T* wch = wcol + (long long)c * 32;   // this chunk's Walsh run (128 bytes in float32)
+    const T* wch = wcol + (long long)c * wstride;   // this chunk's Walsh run (128 bytes in float32)
 #pragma unroll 1
     for (int t = halo ? 3 : 0; t < 4; ++t) {
       T a_hi[4][3];
@@ -777,7 +619,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
       const bool inside = cx < g.NX() && cy < g.NY();
       uint8_t mbs[4] = {0, 0, 0, 0};
       if (inside) {
-        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + g.node(cx, cy, 0) + 4 * c);
+        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + g.node(cx, cy, 4 * c));
         mbs[0] = mb.x; mbs[1] = mb.y; mbs[2] = mb.z; mbs[3] = mb.w;
       }
 #pragma unroll
@@ -788,7 +630,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
           const T v = sm.own[cc][t][tid] + sm.red[cc][t][tid - TXC];
           o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
         }
-        T* dst = &sm.o[k & 1].v[((cc * (TXC - 1) + (i - 1)) * (TYC - 1) + (j - 1)) * 4];
+        T* dst = &sm.o[k & 1].v[((cc * (TYC - 1) + (j - 1)) * (TXC - 1) + (i - 1)) * 4];
 #pragma unroll
         for (int t = 0; t < 4; ++t) dst[t] = o[t];
       }
@@ -796,7 +638,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
     lp_fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      lp_tma_store_4d(&maps.out, 4 * c, y0, x0, 0, sm.o[k & 1].v);
+      lp_tma_store_4d(&maps.out, 4 * x0, y0, c, 0, sm.o[k & 1].v);
       lp_bulk_commit();
     }
   }
@@ -805,7 +647,7 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
 
 // patch cells (weights zero, an explicit masked matrix): out += m * sum of their rows times
 // u, node by node over the box of nodes they touch (one warp per node: the lanes split the
-// 8 cells x 24 columns); runs after k_weights_march
+// 8 cells x 24 columns); runs after k_weights_tma
 template <typename T>
 __global__ void k_patch_add(T* __restrict__ out, const T* __restrict__ u, const int* __restrict__ pid,
                             const T* __restrict__ pk, const uint8_t* __restrict__ mask, LpGrid g, int bx0, int by0,
@@ -853,49 +695,55 @@ __host__ __device__ __forceinline__ int sym_index(int i, int j) {  // i <= j
   return i * 24 - (i * (i - 1)) / 2 + (j - i);
 }
 
+// One thread per cell, its 300 matrix entries streamed (entry p of consecutive cells coalesced).
+// The kernel is bound by how many of those loads are in flight: under a (128, 4) register bound
+// the compiler hoists them (a few spilled bytes), which measured 1.3x faster at 64 x 32 x 32
+// cells than the unbounded build (96 registers, loads issued as used) and 2x faster than a
+// grid-stride form.
 template <typename T>
-__global__ void k_explicit_cells(T* __restrict__ ft, const T* __restrict__ u, const T* __restrict__ kp, LpGrid g) {
-  const long long ncell = (long long)g.nx * g.ny * g.nz;
+__global__ void __launch_bounds__(128, 4)
+k_explicit_cells(T* __restrict__ ft, const T* __restrict__ u, const T* __restrict__ kp, LpGrid g) {
   const long long ncp = g.cells_padded();
   const long long cs = g.comp_stride();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncell; t += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(t % g.nz);
-    const long long q = t / g.nz;
-    const int y = (int)(q % g.ny), x = (int)(q / g.ny);
-    const long long c = g.cell(x, y, z);
-    T uc[24], f[24];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= ncp) return;
+  int x, y, z;
+  if (!g.cell_at(t, x, y, z)) return;
+  const long long c = t;
+  // corner k at n0 + x step (4) + y step (4 NX) + z step (1, or to the next chunk)
+  const long long n0 = g.node(x, y, z);
+  const long long oy = 4LL * g.NX(), oz = (z & 3) == 3 ? g.node_zc_stride() - 3 : 1;
+  T uc[24], f[24];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const long long n = g.node(x + cx_(k), y + cy_(k), z + cz_(k));
+  for (int k = 0; k < 8; ++k) {
+    const long long n = n0 + (k & 1 ? 4 : 0) + (k & 2 ? oy : 0) + (k & 4 ? oz : 0);
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) uc[3 * k + cc] = u[cc * cs + n];
-    }
-#pragma unroll
-    for (int r = 0; r < 24; ++r) f[r] = T(0);
-#pragma unroll
-    for (int a = 0; a < 24; ++a) {
-#pragma unroll
-      for (int b = a; b < 24; ++b) {
-        const T kab = __ldg(kp + (long long)sym_index(a, b) * ncp + c);
-        f[a] += kab * uc[b];
-        if (b != a) f[b] += kab * uc[a];
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < 24; ++r) ft[(long long)r * ncp + c] = f[r];
+    for (int cc = 0; cc < 3; ++cc) uc[3 * k + cc] = u[cc * cs + n];
   }
+#pragma unroll
+  for (int r = 0; r < 24; ++r) f[r] = T(0);
+  const T* kc = kp + c;
+#pragma unroll
+  for (int a = 0; a < 24; ++a) {
+#pragma unroll
+    for (int b = a; b < 24; ++b) {
+      const T kab = __ldg(kc + (long long)sym_index(a, b) * ncp);
+      f[a] += kab * uc[b];
+      if (b != a) f[b] += kab * uc[a];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 24; ++r) ft[(long long)r * ncp + c] = f[r];
 }
 
 template <typename T>
 __global__ void k_explicit_gather(T* __restrict__ out, const T* __restrict__ ft, const uint8_t* __restrict__ mask,
                                   LpGrid g) {
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long total = (long long)NX * NY * NZ;
+  const long long total = g.nodes_padded();
   const long long ncp = g.cells_padded(), cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(t % NZ);
-    const long long q = t / NZ;
-    const int y = (int)(q % NY), x = (int)(q / NY);
+    int x, y, z;
+    if (!g.node_at(t, x, y, z)) continue;
     T a[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -946,36 +794,6 @@ static const int G1_TS[279] = {0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6, 0, 0, 1, 2, 4
 static const int G1_COLS[279] = {3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 4, 6, 9, 10, 16, 18, 21, 22, 5, 12, 15, 11, 18, 21, 17, 23, 4, 6, 9, 10, 16, 18, 21, 22, 3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 8, 13, 11, 16, 19, 22, 20, 23, 9, 20, 4, 6, 23, 3, 7, 14, 10, 17, 21, 16, 18, 15, 19, 22, 10, 17, 3, 7, 14, 4, 6, 23, 9, 20, 22, 15, 19, 16, 18, 21, 11, 16, 18, 8, 13, 21, 5, 12, 22, 15, 19, 23, 20, 17, 5, 12, 15, 11, 18, 21, 17, 23, 8, 13, 11, 16, 19, 22, 20, 23, 3, 7, 14, 10, 17, 9, 20, 23, 15, 19, 22, 21, 15, 19, 5, 12, 22, 21, 11, 18, 3, 7, 14, 10, 17, 9, 20, 23, 11, 16, 18, 8, 13, 21, 22, 19, 4, 6, 23, 9, 20, 10, 10, 17, 3, 7, 14, 23, 9, 20, 5, 12, 22, 15, 19, 11, 18, 21, 11, 16, 18, 21, 5, 12, 22, 15, 4, 6, 23, 9, 10, 17, 15, 19, 22, 8, 13, 21, 11, 16, 3, 7, 14, 10, 17, 9, 20, 23, 9, 20, 23, 3, 7, 14, 10, 17, 8, 13, 21, 11, 16, 15, 19, 22, 21, 11, 16, 18, 15, 19, 5, 12, 22, 9, 20, 4, 6, 23, 3, 7, 14, 10, 17, 22, 15, 19, 11, 16, 18, 8, 13, 21, 10, 17, 3, 7, 14, 4, 6, 23, 9, 20, 23, 9, 20, 10, 17, 3, 7, 14, 11, 16, 18, 8, 13, 21, 5, 12, 22, 15, 19};
 
 template <typename T>
-static int launch_weights(T* out, const T* u, const T* w, const int* pid, const T* pk, const uint8_t* mask,
-                          const double* g1_host, const int* pbox, LpGrid g, cudaStream_t st) {
-  if (!lp_grid_ok(g) || g.pz % 4 || g.cpz != g.pz || !out || !u || !w || !mask || !g1_host || out == u)
-    return LP_ERR_ARG;
-  G1<T> gc;
-  for (int i = 0; i < 279; ++i) gc.c[i] = (T)g1_host[i];
-  const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
-  const int nchunks = g.pz / 4;
-  int dev = 0, nsm = 148;  // one resident block per SM
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  int best = nchunks;
-  double bc = 1e30;
-  for (int zch = 2; zch <= nchunks; ++zch) {
-    const long long nseg = (nchunks + zch - 1) / zch, units = (long long)gx * gy * nseg;
-    const double cost = (double)((units + nsm - 1) / nsm) * (zch + (nseg > 1 ? 0.3 : 0.0));
-    if (cost < bc - 1e-9) { bc = cost; best = zch; }
-  }
-  dim3 grid(gx, gy, (nchunks + best - 1) / best);
-  k_weights_march<T><<<grid, TXC * TYC, 0, st>>>(out, u, w, mask, gc, g, best, nchunks);
-  if (pid && pk && pbox && pbox[3] > 0 && pbox[4] > 0 && pbox[5] > 0) {
-    const long long nb = (long long)pbox[3] * pbox[4] * pbox[5];
-    k_patch_add<T><<<lp_blocks(nb * 32, 256), 256, 0, st>>>(out, u, pid, pk, mask, g, pbox[0], pbox[1], pbox[2],
-                                                            pbox[3], pbox[4], pbox[5]);
-  }
-  LP_LAUNCH_CHECK();
-  return LP_OK;
-}
-
-template <typename T>
 static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, const T* pk, const uint8_t* mask,
                               const double* g1_host, const int* pbox, int* err, LpGrid g, cudaStream_t st) {
   if (!lp_grid_ok(g) || g.pz % 4 || g.cpz != g.pz || !out || !u || !wc || !mask || !g1_host || !err || out == u)
@@ -983,9 +801,9 @@ static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, c
   G1<T> gc;
   for (int i = 0; i < 279; ++i) gc.c[i] = (T)g1_host[i];
   WMaps<T> maps;
-  const uint64_t nd[4] = {(uint64_t)g.pz, (uint64_t)g.NY(), (uint64_t)g.NX(), 3};
-  const uint32_t bin[4] = {4, WBOX, WBOX, 3};
-  const uint32_t bout[4] = {4, TXC - 1, TYC - 1, 3};
+  const uint64_t nd[4] = {4 * (uint64_t)g.NX(), (uint64_t)g.NY(), (uint64_t)g.pz / 4, 3};
+  const uint32_t bin[4] = {4 * WBOX, WBOX, 1, 3};
+  const uint32_t bout[4] = {4 * (TXC - 1), TYC - 1, 1, 3};
   if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
     return LP_ERR_ARG;
   const int smem = (int)sizeof(WSmem<T>) + 128;
@@ -1022,10 +840,8 @@ static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, c
 template <typename T>
 static int launch_explicit(T* out, const T* u, const T* kp, T* ft, const uint8_t* mask, LpGrid g, cudaStream_t st) {
   if (!lp_grid_ok(g) || !out || !u || !kp || !ft || !mask || out == u) return LP_ERR_ARG;
-  const long long ncell = (long long)g.nx * g.ny * g.nz;
-  const long long nn = (long long)g.NX() * g.NY() * g.NZ();
-  k_explicit_cells<T><<<lp_blocks(ncell, 128), 128, 0, st>>>(ft, u, kp, g);
-  k_explicit_gather<T><<<lp_blocks(nn, 256), 256, 0, st>>>(out, ft, mask, g);
+  k_explicit_cells<T><<<lp_blocks(g.cells_padded(), 128), 128, 0, st>>>(ft, u, kp, g);
+  k_explicit_gather<T><<<lp_blocks(g.nodes_padded(), 256), 256, 0, st>>>(out, ft, mask, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -1116,19 +932,6 @@ int lpb_modal_g1(const double* ke, double* g1_out) {
 }
 
 // pbox (host, 6 ints): node box x0, y0, z0, nx, ny, nz holding every node a patch cell touches
-int lpb_apply_weights_march_f32(float* out, const float* u, const float* w, const int* patch_id, const float* patch_k,
-                                const uint8_t* mask, const double* g1, const int* pbox, LP_GRID_ARGS, void* stream) {
-  return launch_weights<float>(out, u, w, patch_id, patch_k, mask, g1, pbox, LP_GRID, LP_ST);
-}
-
-int lpb_apply_weights_march_f64(double* out, const double* u, const double* w, const int* patch_id,
-                                const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox,
-                                LP_GRID_ARGS, void* stream) {
-  return launch_weights<double>(out, u, w, patch_id, patch_k, mask, g1, pbox, LP_GRID, LP_ST);
-}
-
-// the level-1 Walsh coefficients in the chunked layout (nx, ny, cpz / 4, 8, 4), from the
-// weights (8, cells) after the patch cells' weights are zeroed; cpz % 4 == 0
 int lpb_walsh_chunks_f32(float* wc, const float* w, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || g.cpz % 4 || !wc || !w) return LP_ERR_ARG;

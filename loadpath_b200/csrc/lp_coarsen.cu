@@ -24,13 +24,11 @@ __device__ __forceinline__ double pw(int k, int q, int r) {
 // w[k, C] = e[2C + CORNERS[k]] for C inside the fine grid's half, else 0 (loadpath/mg.py:617-620)
 template <typename Te, typename Tw>
 __global__ void k_weights_from_e(Tw* __restrict__ w, const Te* __restrict__ e, LpGrid gf, LpGrid gc) {
-  const long long total = (long long)gc.nx * gc.ny * gc.nz;
+  const long long total = gc.cells_padded();
   const int hx = gf.nx / 2, hy = gf.ny / 2, hz = gf.nz / 2;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int Z = (int)(t % gc.nz);
-    long long q = t / gc.nz;
-    int Y = (int)(q % gc.ny);
-    int X = (int)(q / gc.ny);
+    int X, Y, Z;
+    if (!gc.cell_at(t, X, Y, Z)) continue;
     long long c = gc.cell(X, Y, Z);
     bool in = X < hx && Y < hy && Z < hz;
     for (int k = 0; k < 8; ++k) {
@@ -46,13 +44,11 @@ __global__ void k_weights_from_e(Tw* __restrict__ w, const Te* __restrict__ e, L
 template <typename Te>
 __global__ void k_patch_flags(uint8_t* __restrict__ flag, const Te* __restrict__ e, const uint8_t* __restrict__ mf,
                               LpGrid gf, LpGrid gc) {
-  const long long total = (long long)gc.nx * gc.ny * gc.nz;
+  const long long total = gc.cells_padded();
   const int hx = gf.nx / 2, hy = gf.ny / 2, hz = gf.nz / 2;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int Z = (int)(t % gc.nz);
-    long long q = t / gc.nz;
-    int Y = (int)(q % gc.ny);
-    int X = (int)(q / gc.ny);
+    int X, Y, Z;
+    if (!gc.cell_at(t, X, Y, Z)) continue;
     uint8_t f = 0;
     if (X < hx && Y < hy && Z < hz) {
       for (int k = 0; k < 8 && !f; ++k) {
@@ -80,11 +76,9 @@ __global__ void k_patch_matrices(Tw* __restrict__ pk, Tw* __restrict__ w, int* _
   __shared__ double dm[24];
   int p = blockIdx.x;
   if (p >= npatch) return;
-  long long C = pcells[p];
-  int Z = (int)(C % gc.cpz);
-  long long q0 = C / gc.cpz;
-  int Y = (int)(q0 % gc.ny);
-  int X = (int)(q0 / gc.ny);
+  const long long C = pcells[p];
+  int X, Y, Z;
+  gc.cell_at(C, X, Y, Z);
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;  // thread t handles outputs t, t+256, t+512
   for (int k = 0; k < 8; ++k) {
     int x = 2 * X + cx_(k), y = 2 * Y + cy_(k), z = 2 * Z + cz_(k);
@@ -202,16 +196,13 @@ __global__ void k_galerkin_explicit(Tw* __restrict__ kout, int fine_kind, const 
 __global__ void k_strict_held_kept(uint8_t* __restrict__ held_c, float* __restrict__ kept,
                                    const uint8_t* __restrict__ held_f, const uint8_t* __restrict__ mf, LpGrid gf,
                                    LpGrid gc) {
-  const int CX = gc.NX(), CY = gc.NY(), CZ = gc.NZ();
   const int FX = gf.NX(), FY = gf.NY(), FZ = gf.NZ();
-  const long long total = (long long)CX * CY * CZ;
+  const long long total = gc.nodes_padded();
   const long long ccs = gc.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int Z = (int)(t % CZ);
-    long long q = t / CZ;
-    int Y = (int)(q % CY);
-    int X = (int)(q / CY);
-    long long cn = gc.node(X, Y, Z);
+    int X, Y, Z;
+    if (!gc.node_at(t, X, Y, Z)) continue;
+    const long long cn = t;
     uint8_t h = 0;
     if (2 * X < FX && 2 * Y < FY && 2 * Z < FZ) h = held_f[gf.node(2 * X, 2 * Y, 2 * Z)] & 7;
     held_c[cn] = h;
@@ -469,7 +460,7 @@ extern "C" {
 int lpb_weights_from_e_f64_f32(float* w, const double* e, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !w || !e) return LP_ERR_ARG;
-  long long total = (long long)gc.nx * gc.ny * gc.nz;
+  long long total = gc.cells_padded();
   k_weights_from_e<double, float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(w, e, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -478,7 +469,7 @@ int lpb_weights_from_e_f64_f32(float* w, const double* e, LP_FC_ARGS, void* stre
 int lpb_weights_from_e_f64_f64(double* w, const double* e, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !w || !e) return LP_ERR_ARG;
-  long long total = (long long)gc.nx * gc.ny * gc.nz;
+  long long total = gc.cells_padded();
   k_weights_from_e<double, double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(w, e, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -487,7 +478,7 @@ int lpb_weights_from_e_f64_f64(double* w, const double* e, LP_FC_ARGS, void* str
 int lpb_patch_flags(uint8_t* flag, const double* e, const uint8_t* mf, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !flag || !e || !mf) return LP_ERR_ARG;
-  long long total = (long long)gc.nx * gc.ny * gc.nz;
+  long long total = gc.cells_padded();
   k_patch_flags<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(flag, e, mf, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -564,7 +555,7 @@ int lpb_strict_held_kept(uint8_t* held_c, float* kept, const uint8_t* held_f, co
                          void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !held_c || !kept || !held_f || !mf) return LP_ERR_ARG;
-  long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
+  long long total = gc.nodes_padded();
   k_strict_held_kept<<<lp_blocks(total, 256), 256, 0, LP_ST>>>(held_c, kept, held_f, mf, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;

@@ -1,10 +1,14 @@
 // Shared definitions for the loadpath_b200 CUDA kernels (sm_100a).
 //
-// Layouts (all C order):
-//   node field  (3, NX, NY, PZ)   NX = nx + 1, NY = ny + 1, PZ >= nz + 1 (z pitch, elements)
-//   cell field  (nx, ny, CPZ)     CPZ >= nz
-//   node mask   (NX, NY, PZ) uint8: bits 0..2 = dof is solved for (alive and not held) per
+// Layouts (all C order). A level's z extent is cut into chunks of four planes, and the chunk
+// index is the slowest axis, so one chunk's four planes of a row of x are contiguous:
+//   node field  (3, PZ/4, NY, NX, 4)   NX = nx + 1, NY = ny + 1, PZ >= nz + 1, PZ % 4 == 0
+//   cell field  (CPZ/4, ny, nx, 4)     CPZ >= nz, CPZ % 4 == 0
+//   node mask   (PZ/4, NY, NX, 4) uint8: bits 0..2 = dof is solved for (alive and not held) per
 //               component; bits 3..5 = dof carries stiffness (alive) per component.
+// Node (x, y, z) sits at ((z / 4 * NY + y) * NX + x) * 4 + z % 4 of its component; a tile of
+// node columns moves as rows of 16 * (x extent) bytes, and the z padding (z > nz for nodes,
+// z >= nz for cells) holds zeros.
 // Corner k of a cell sits at (k & 1, k >> 1 & 1, k >> 2 & 1); a cell's 24 dofs are ordered
 // 3 * corner + component (loadpath/fem.py:30, loadpath/fem.py:127-145).
 #pragma once
@@ -25,13 +29,33 @@ struct LpGrid {
   __host__ __device__ int NZ() const { return nz + 1; }
   __host__ __device__ long long comp_stride() const { return (long long)(nx + 1) * (ny + 1) * pz; }
   __host__ __device__ long long node(int x, int y, int z) const {
-    return ((long long)x * (ny + 1) + y) * pz + z;
+    return (((long long)(z >> 2) * (ny + 1) + y) * (nx + 1) + x) * 4 + (z & 3);
   }
   __host__ __device__ long long cell(int x, int y, int z) const {
-    return ((long long)x * ny + y) * cpz + z;
+    return (((long long)(z >> 2) * ny + y) * nx + x) * 4 + (z & 3);
   }
+  // index step from one z chunk of a column to the next
+  __host__ __device__ long long node_zc_stride() const { return 4LL * (nx + 1) * (ny + 1); }
+  __host__ __device__ long long cell_zc_stride() const { return 4LL * nx * ny; }
   __host__ __device__ long long nodes_padded() const { return (long long)(nx + 1) * (ny + 1) * pz; }
   __host__ __device__ long long cells_padded() const { return (long long)nx * ny * cpz; }
+  // the node / cell at index t of a field (memory order); false on the z padding
+  __host__ __device__ bool node_at(long long t, int& x, int& y, int& z) const {
+    long long r = t >> 2;
+    x = (int)(r % (nx + 1));
+    r /= (nx + 1);
+    y = (int)(r % (ny + 1));
+    z = 4 * (int)(r / (ny + 1)) + (int)(t & 3);
+    return z <= nz;
+  }
+  __host__ __device__ bool cell_at(long long t, int& x, int& y, int& z) const {
+    long long r = t >> 2;
+    x = (int)(r % nx);
+    r /= nx;
+    y = (int)(r % ny);
+    z = 4 * (int)(r / ny) + (int)(t & 3);
+    return z < nz;
+  }
 };
 
 static inline LpGrid lp_grid(int nx, int ny, int nz, int pz, int cpz) {
@@ -41,7 +65,8 @@ static inline LpGrid lp_grid(int nx, int ny, int nz, int pz, int cpz) {
 }
 
 static inline bool lp_grid_ok(const LpGrid& g) {
-  return g.nx >= 1 && g.ny >= 1 && g.nz >= 1 && g.pz >= g.nz + 1 && g.cpz >= g.nz;
+  return g.nx >= 1 && g.ny >= 1 && g.nz >= 1 && g.pz >= g.nz + 1 && g.cpz >= g.nz && g.pz % 4 == 0 &&
+         g.cpz % 4 == 0;
 }
 
 static inline int lp_blocks(long long n, int threads) {

@@ -58,15 +58,12 @@ __global__ void k_apply_level(T* __restrict__ out, const T* __restrict__ u, cons
     for (int i = threadIdx.x; i < 8 * 576; i += blockDim.x) sm[i] = a.mcat[i];
   }
   __syncthreads();
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long total = (long long)NX * NY * NZ;
+  const long long total = g.nodes_padded();
   const long long cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % NZ);
-    long long r = t / NZ;
-    int y = (int)(r % NY);
-    int x = (int)(r / NY);
+    int x, y, z;
+    if (!g.node_at(t, x, y, z)) continue;
     T acc[3] = {T(0), T(0), T(0)};
 #pragma unroll 1
     for (int kk = 0; kk < 8; ++kk) {
@@ -148,7 +145,7 @@ int launch_apply(T* out, const T* u, const uint8_t* mask, LpGrid g, LevelArgs<T>
   if (smem > 48 * 1024) {
     cudaFuncSetAttribute(k_apply_level<T, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
-  long long total = (long long)g.NX() * g.NY() * g.NZ();
+  long long total = g.nodes_padded();
   int threads = 256;
   int blocks = lp_blocks(total, threads);
   if (blocks > 148 * 64) blocks = 148 * 64;
@@ -160,15 +157,12 @@ int launch_apply(T* out, const T* u, const uint8_t* mask, LpGrid g, LevelArgs<T>
 // diagonal of the unmasked K, float64 (3, nodes)
 template <typename T, int KIND>
 __global__ void k_diag_level(double* __restrict__ d, LpGrid g, LevelArgs<T> a) {
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long total = (long long)NX * NY * NZ;
+  const long long total = g.nodes_padded();
   const long long cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % NZ);
-    long long r = t / NZ;
-    int y = (int)(r % NY);
-    int x = (int)(r / NY);
+    int x, y, z;
+    if (!g.node_at(t, x, y, z)) continue;
     double acc[3] = {0.0, 0.0, 0.0};
     for (int kk = 0; kk < 8; ++kk) {
       int cx = x - cx_(kk), cy = y - cy_(kk), cz = z - cz_(kk);
@@ -198,7 +192,7 @@ __global__ void k_diag_level(double* __restrict__ d, LpGrid g, LevelArgs<T> a) {
 template <typename T, int KIND>
 int launch_diag(double* d, LpGrid g, LevelArgs<T> a, cudaStream_t st) {
   if (!lp_grid_ok(g) || !d) return LP_ERR_ARG;
-  long long total = (long long)g.NX() * g.NY() * g.NZ();
+  long long total = g.nodes_padded();
   k_diag_level<T, KIND><<<lp_blocks(total, 256), 256, 0, st>>>(d, g, a);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -219,15 +213,12 @@ __global__ void k_masks(uint8_t* __restrict__ mask, double* __restrict__ dinv64,
     alive_thr *= sc;
     live_thr *= sc;
   }
-  const int NX = g.NX(), NY = g.NY(), NZ = g.NZ();
-  const long long total = (long long)NX * NY * NZ;
+  const long long total = g.nodes_padded();
   const long long cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % NZ);
-    long long r = t / NZ;
-    int y = (int)(r % NY);
-    int x = (int)(r / NY);
+    int x, y, z;
+    if (!g.node_at(t, x, y, z)) continue;
     long long n = g.node(x, y, z);
     uint8_t hb = held_bits ? held_bits[n] : 0;
     uint8_t mb = 0;
@@ -302,13 +293,13 @@ __global__ void k_count_pos(const double* __restrict__ e, long long n, double* _
 template <typename T>
 __global__ void k_count_weights(const T* __restrict__ w, const int* __restrict__ patch_id, LpGrid g,
                                 double* __restrict__ part) {
-  const long long total = (long long)g.nx * g.ny * g.nz, ncp = g.cells_padded();
+  const long long ncp = g.cells_padded();
   double c = 0.0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncp;
        t += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(t % g.nz);
-    const long long q = t / g.nz;
-    const long long cell = g.cell((int)(q / g.ny), (int)(q % g.ny), z);
+    int x, y, z;
+    if (!g.cell_at(t, x, y, z)) continue;
+    const long long cell = t;
     bool act = patch_id && patch_id[cell] >= 0;
     for (int k = 0; k < 8 && !act; ++k) act = w[k * ncp + cell] != T(0);
     c += act ? 1.0 : 0.0;
@@ -319,14 +310,14 @@ __global__ void k_count_weights(const T* __restrict__ w, const int* __restrict__
 // explicit-level cells whose 24 x 24 matrix has a non-zero entry; one warp per cell
 template <typename T>
 __global__ void k_count_explicit(const T* __restrict__ k, LpGrid g, double* __restrict__ part) {
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   const int lane = threadIdx.x & 31;
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   double c = 0.0;
   for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < total; t += warps) {
-    const int z = (int)(t % g.nz);
-    const long long q = t / g.nz;
-    const T* kc = k + g.cell((int)(q / g.ny), (int)(q % g.ny), z) * 576;
+    int x, y, z;
+    if (!g.cell_at(t, x, y, z)) continue;
+    const T* kc = k + t * 576;
     bool nz = false;
     for (int i = lane; i < 576; i += 32) nz = nz || kc[i] != T(0);
     if (__any_sync(0xffffffffu, nz) && lane == 0) c += 1.0;
@@ -448,7 +439,7 @@ int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, con
               void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !mask || !d) return LP_ERR_ARG;
-  long long total = (long long)g.NX() * g.NY() * g.NZ();
+  long long total = g.nodes_padded();
   k_masks<<<lp_blocks(total, 256), 256, 0, (cudaStream_t)stream>>>(mask, dinv64, dinv32, d, held_bits, kept, g,
                                                                    alive_thr, live_thr, thr_scale);
   LP_LAUNCH_CHECK();

@@ -32,12 +32,10 @@ __global__ void k_filter(double* __restrict__ out, const double* __restrict__ v,
     sw[i] = tw[i];
   }
   __syncthreads();
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    int y = (int)(q % g.ny);
-    int x = (int)(q / g.ny);
+    int x, y, z;
+    if (!g.cell_at(t, x, y, z)) continue;
     double s = 0.0;
     for (int i = 0; i < ntaps; ++i) {
       int xx = x + so[3 * i], yy = y + so[3 * i + 1], zz = z + so[3 * i + 2];
@@ -56,11 +54,11 @@ __global__ void k_filter(double* __restrict__ out, const double* __restrict__ v,
 
 // e = emin + x^p (1 - emin) on the grid's cells (padding untouched)
 __global__ void k_simp_law(double* __restrict__ e, const double* __restrict__ x, double penal, double emin, LpGrid g) {
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    long long c = g.cell((int)(q / g.ny), (int)(q % g.ny), z);
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const long long c = t;
     e[c] = emin + pow(x[c], penal) * (1.0 - emin);
   }
 }
@@ -95,34 +93,34 @@ __global__ void __launch_bounds__(128) k_element_energy(double* __restrict__ ce,
   }
   const bool dense = __syncthreads_or(off) != 0;
 
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   const long long cs = g.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(t % g.nz);
-    const long long q = t / g.nz;
-    const int y = (int)(q % g.ny);
-    const int x = (int)(q / g.ny);
+    int x, y, z;
+    if (!g.cell_at(t, x, y, z)) continue;
+    long long nk[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) nk[k] = g.node(x + cx_(k), y + cy_(k), z + cz_(k));
     double uh[24], vh[24];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      double a[8], b[8];
+      double a[8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const long long n = c * cs + g.node(x + cx_(k), y + cy_(k), z + cz_(k));
-        a[k] = (double)u[n];
-        b[k] = v ? (double)v[n] : 0.0;
-      }
+      for (int k = 0; k < 8; ++k) a[k] = (double)u[c * cs + nk[k]];
       lp_walsh8(a);
-      lp_walsh8(b);
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        uh[3 * m + c] = a[m];
-        vh[3 * m + c] = b[m];
-      }
+      for (int m = 0; m < 8; ++m) uh[3 * m + c] = vh[3 * m + c] = a[m];
     }
-    if (!v) {
+    if (v) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) vh[i] = uh[i];
+      for (int c = 0; c < 3; ++c) {
+        double a[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = (double)v[c * cs + nk[k]];
+        lp_walsh8(a);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) vh[3 * m + c] = a[m];
+      }
     }
     double s = 0.0;
     if (!dense) {
@@ -147,14 +145,12 @@ __global__ void k_sensitivity(double* __restrict__ dc, const double* __restrict_
                               const double* __restrict__ e, double penal, double emin, double scale, int accumulate,
                               LpGrid g, double* __restrict__ part) {
   __shared__ double sh[32];
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   double acc = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    int y = (int)(q % g.ny);
-    int x = (int)(q / g.ny);
-    long long c = g.cell(x, y, z);
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const long long c = t;
     double xv = xphys[c];
     double d = -penal * (1.0 - emin) * pow(xv, penal - 1.0) * ce[c] * scale;
     dc[c] = accumulate ? dc[c] + d : d;
@@ -182,13 +178,11 @@ __global__ void __launch_bounds__(256) k_oc_volumes(const double* __restrict__ x
   double acc[NL];
 #pragma unroll
   for (int j = 0; j < NL; ++j) acc[j] = 0.0;
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    int y = (int)(q % g.ny);
-    int xx = (int)(q / g.ny);
-    long long c = g.cell(xx, y, z);
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const long long c = t;
     double xv = x[c], gw = gv[c];
     double ts = xv * sqrt(-dc[c] / dv[c]);
     double lo = fmax(0.0, xv - move), hi = fmin(1.0, xv + move);
@@ -225,14 +219,12 @@ __global__ void k_oc_apply(double* __restrict__ xnew, const double* __restrict__
                            const double* __restrict__ dv, double lam, double move, LpGrid g,
                            double* __restrict__ part) {
   __shared__ double sh[32];
-  const long long total = (long long)g.nx * g.ny * g.nz;
+  const long long total = g.cells_padded();
   double mx = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int z = (int)(t % g.nz);
-    long long q = t / g.nz;
-    int y = (int)(q % g.ny);
-    int xx = (int)(q / g.ny);
-    long long c = g.cell(xx, y, z);
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const long long c = t;
     double xv = x[c];
     double xn = xv * sqrt(-dc[c] / dv[c] / lam);
     xn = fmax(0.0, fmax(xv - move, fmin(1.0, fmin(xv + move, xn))));
@@ -287,7 +279,7 @@ int lpb_filter(double* out, const double* v, const int* toff, const double* tw, 
   if (!lp_grid_ok(g) || !out || !v || !toff || !tw || ntaps < 1 || ntaps > LP_MAX_TAPS) return LP_ERR_ARG;
   if (out == v) return LP_ERR_ARG;
   size_t smem = ((3 * ntaps * sizeof(int) + 15) & ~(size_t)15) + ntaps * sizeof(double);
-  long long total = (long long)g.nx * g.ny * g.nz;
+  long long total = g.cells_padded();
   k_filter<<<lp_blocks(total, 256), 256, smem, LP_ST>>>(out, v, toff, tw, ntaps, hs_in, hs_out, e_out, penal, emin, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -296,7 +288,7 @@ int lpb_filter(double* out, const double* v, const int* toff, const double* tw, 
 int lpb_simp_law(double* e, const double* x, double penal, double emin, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !e || !x) return LP_ERR_ARG;
-  long long total = (long long)g.nx * g.ny * g.nz;
+  long long total = g.cells_padded();
   k_simp_law<<<lp_blocks(total, 256), 256, 0, LP_ST>>>(e, x, penal, emin, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
@@ -306,7 +298,7 @@ int lpb_element_energy_f64(double* ce, const double* u, const double* v, const d
                            void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
-  long long total = (long long)g.nx * g.ny * g.nz;
+  long long total = g.cells_padded();
   k_element_energy<double><<<(int)std::min<long long>(lp_blocks(total, 128), LP_ENERGY_BLOCKS), 128, 0, LP_ST>>>(
       ce, u, v, ke, g);
   LP_LAUNCH_CHECK();
@@ -316,7 +308,7 @@ int lpb_element_energy_f64(double* ce, const double* u, const double* v, const d
 int lpb_element_energy_f32(double* ce, const float* u, const float* v, const double* ke, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !ce || !u || !ke) return LP_ERR_ARG;
-  long long total = (long long)g.nx * g.ny * g.nz;
+  long long total = g.cells_padded();
   k_element_energy<float><<<(int)std::min<long long>(lp_blocks(total, 128), LP_ENERGY_BLOCKS), 128, 0, LP_ST>>>(
       ce, u, v, ke, g);
   LP_LAUNCH_CHECK();

@@ -219,145 +219,62 @@ __global__ void k_jacobi(T* __restrict__ x, const T* __restrict__ b, const T* __
   }
 }
 
-// rc = restrict(((b - ax) * m) zero-padded) * cm, one coarse node per thread
-// (loadpath/mgops.py:666-711)
-template <typename T>
-__global__ void k_restrict_residual(T* __restrict__ rc, const T* __restrict__ b, const T* __restrict__ ax,
-                                    const uint8_t* __restrict__ m, const uint8_t* __restrict__ cm, LpGrid gf,
-                                    LpGrid gc) {
-  const int CX = gc.NX(), CY = gc.NY(), CZ = gc.NZ();
-  const int FX = gf.NX(), FY = gf.NY(), FZ = gf.NZ();
-  const long long total = (long long)CX * CY * CZ;
-  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    int Z = (int)(t % CZ);
-    long long q = t / CZ;
-    int Y = (int)(q % CY);
-    int X = (int)(q / CY);
-    long long cn = gc.node(X, Y, Z);
-    uint8_t cmb = cm[cn];
-    T acc[3] = {T(0), T(0), T(0)};
-    for (int a = -1; a <= 1; ++a) {
-      int x = 2 * X + a;
-      if (x < 0 || x >= FX) continue;
-      T wa = a ? T(0.5) : T(1);
-      for (int bb = -1; bb <= 1; ++bb) {
-        int y = 2 * Y + bb;
-        if (y < 0 || y >= FY) continue;
-        T wb = wa * (bb ? T(0.5) : T(1));
-        for (int e = -1; e <= 1; ++e) {
-          int z = 2 * Z + e;
-          if (z < 0 || z >= FZ) continue;
-          T we = wb * (e ? T(0.5) : T(1));
-          long long fn = gf.node(x, y, z);
-          uint8_t mb = m[fn];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            if ((mb >> i) & 1) acc[i] += (b[i * fcs + fn] - ax[i * fcs + fn]) * we;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) rc[i * ccs + cn] = ((cmb >> i) & 1) ? acc[i] : T(0);
-  }
-}
+// ---- grid transfers by z chunks -----------------------------------------------------------
+// One thread per (x, y) node column and chunk of four z planes (x fastest across threads), the
+// chunk's values moved with 16-byte loads and stores, the trilinear weights applied separably
+// (z inside a column first).
 
-// x += prolong(xc * cm)[fine nodes] * m, one fine node per thread (loadpath/mgops.py:714-750).
-// Every node reads the 2 x 2 x 2 coarse corners around it; on an even coordinate the two
-// taps of that axis coincide and the second gets weight zero, so the loop has no branches.
-template <typename T>
-__global__ void k_prolong_add(T* __restrict__ x, const T* __restrict__ xc, const uint8_t* __restrict__ cm,
-                              const uint8_t* __restrict__ m, LpGrid gf, LpGrid gc) {
-  const int FX = gf.NX(), FY = gf.NY(), FZ = gf.NZ();
-  const long long total = (long long)FX * FY * FZ;
-  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(t % FZ);
-    const long long q = t / FZ;
-    const int y = (int)(q % FY);
-    const int xx = (int)(q / FY);
-    const long long fn = gf.node(xx, y, z);
-    const uint8_t mb = m[fn];
-    if ((mb & 7) == 0) continue;
-    const int x0 = xx >> 1, y0 = y >> 1, z0 = z >> 1;
-    const int ox = xx & 1, oy = y & 1, oz = z & 1;
-    const T wx[2] = {ox ? T(0.5) : T(1), ox ? T(0.5) : T(0)};
-    const T wy[2] = {oy ? T(0.5) : T(1), oy ? T(0.5) : T(0)};
-    const T wz[2] = {oz ? T(0.5) : T(1), oz ? T(0.5) : T(0)};
-    T acc[3] = {T(0), T(0), T(0)};
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const long long cn = gc.node(x0 + a * ox, y0 + bb * oy, z0 + e * oz);
-          const uint8_t cmb = cm[cn];
-          const T w = wx[a] * wy[bb] * wz[e];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            const T v = ((cmb >> i) & 1) ? xc[i * ccs + cn] : T(0);
-            acc[i] += w * v;
-          }
-        }
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-      if ((mb >> i) & 1) x[i * fcs + fn] += acc[i];
-  }
-}
+// rc = restrict(((b - ax) * m) zero-padded) * cm (loadpath/mgops.py:666-711). One warp per 15
+// coarse columns X0..X0+14 of one coarse row Y and chunk C (coarse planes 4C..4C+3): lane l
+// reads fine column x = 2 X0 - 1 + l (rows 2Y - 1 .. 2Y + 1, fine planes 8C - 1 .. 8C + 7), so a
+// warp's loads are 32 consecutive 16-byte chunk rows; the lane restricts z and y in registers,
+// and the odd lanes (x = 2X) finish x with their two neighbours' sums by shuffles and store.
+constexpr int R4_COLS = 15;   // coarse columns per warp
 
-// ---- grid transfers by z chunks (the level fields' z pitch is a multiple of 4) ----------------
-// One thread per (x, y) node column and chunk of four z planes, the column's values moved with
-// 16-byte loads and stores, the trilinear weights applied separably (z inside a column first).
-
-// rc = restrict(((b - ax) * m) zero-padded) * cm for coarse nodes (X, Y, 4C..4C+3): the fine z
-// range 8C - 1 .. 8C + 7 of the nine fine columns around (2X, 2Y)   (loadpath/mgops.py:666-711)
 template <typename T>
 __global__ void k_restrict4(T* __restrict__ rc, const T* __restrict__ b, const T* __restrict__ ax,
                             const uint8_t* __restrict__ m, const uint8_t* __restrict__ cm, LpGrid gf, LpGrid gc) {
   const int CX = gc.NX(), CY = gc.NY(), CZ4 = gc.pz / 4;
   const int FX = gf.NX(), FY = gf.NY();
-  const long long total = (long long)CX * CY * CZ4;
-  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int C = (int)(t % CZ4);
-    const long long q = t / CZ4;
-    const int Y = (int)(q % CY), X = (int)(q / CY);
+  const int ngx = (CX + R4_COLS - 1) / R4_COLS;
+  const long long nwarps = (long long)ngx * CY * CZ4;
+  const long long fcs = gf.comp_stride(), ccs = gc.comp_stride(), fzs = gf.node_zc_stride();
+  const int lane = threadIdx.x & 31;
+  const long long wstep = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < nwarps; w += wstep) {
+    const int gx = (int)(w % ngx);
+    const long long q = w / ngx;
+    const int Y = (int)(q % CY), C = (int)(q / CY);
+    const int X0 = gx * R4_COLS;
+    const int x = 2 * X0 - 1 + lane;
     const int z0 = 8 * C;
+    // a coarse level padded up past half the fine one reaches beyond the fine pitch: zeros
+    const bool below = z0 >= 1 && z0 - 1 < gf.pz, lo = z0 < gf.pz, hi = z0 + 4 < gf.pz;
     T acc[3][4] = {};
-#pragma unroll 1
-    for (int dx = -1; dx <= 1; ++dx) {
-      const int x = 2 * X + dx;
-      if (x < 0 || x >= FX) continue;
-      const T wx = dx ? T(0.5) : T(1);
+    if (x >= 0 && x < FX) {
 #pragma unroll 1
       for (int dy = -1; dy <= 1; ++dy) {
         const int y = 2 * Y + dy;
         if (y < 0 || y >= FY) continue;
-        const T w = wx * (dy ? T(0.5) : T(1));
-        const long long col = gf.node(x, y, 0);
-        // fine planes z0 - 1 .. z0 + 7 of this column: masked b - ax per component
-        // a coarse level padded up past half the fine one reaches beyond the fine pitch: zeros
-        const bool below = z0 >= 1 && z0 - 1 < gf.pz, lo = z0 < gf.pz, hi = z0 + 4 < gf.pz;
+        const T wy = dy ? T(0.5) : T(1);
+        const long long n_lo = lo ? gf.node(x, y, z0) : 0, n_hi = n_lo + fzs;
+        const long long n_below = below ? gf.node(x, y, z0 - 1) : 0;
         uint8_t mz[9];
-        mz[0] = below ? m[col + z0 - 1] : 0;
-        const uchar4 ma = lo ? *reinterpret_cast<const uchar4*>(m + col + z0) : make_uchar4(0, 0, 0, 0);
-        const uchar4 mb = hi ? *reinterpret_cast<const uchar4*>(m + col + z0 + 4) : make_uchar4(0, 0, 0, 0);
+        mz[0] = below ? m[n_below] : 0;
+        const uchar4 ma = lo ? *reinterpret_cast<const uchar4*>(m + n_lo) : make_uchar4(0, 0, 0, 0);
+        const uchar4 mb = hi ? *reinterpret_cast<const uchar4*>(m + n_hi) : make_uchar4(0, 0, 0, 0);
         mz[1] = ma.x; mz[2] = ma.y; mz[3] = ma.z; mz[4] = ma.w;
         mz[5] = mb.x; mz[6] = mb.y; mz[7] = mb.z; mz[8] = mb.w;
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-          const T* bi = b + i * fcs + col;
-          const T* ai = ax + i * fcs + col;
+          const T* bi = b + i * fcs;
+          const T* ai = ax + i * fcs;
           T v[9];
-          v[0] = below ? bi[z0 - 1] - ai[z0 - 1] : T(0);
+          v[0] = below ? bi[n_below] - ai[n_below] : T(0);
           T b4[4], a4[4];
           if (lo) {
-            V4ld<T>::ld(bi + z0, b4);
-            V4ld<T>::ld(ai + z0, a4);
+            V4ld<T>::ld(bi + n_lo, b4);
+            V4ld<T>::ld(ai + n_lo, a4);
 #pragma unroll
             for (int k = 0; k < 4; ++k) v[1 + k] = b4[k] - a4[k];
           } else {
@@ -365,8 +282,8 @@ __global__ void k_restrict4(T* __restrict__ rc, const T* __restrict__ b, const T
             for (int k = 0; k < 4; ++k) v[1 + k] = T(0);
           }
           if (hi) {
-            V4ld<T>::ld(bi + z0 + 4, b4);
-            V4ld<T>::ld(ai + z0 + 4, a4);
+            V4ld<T>::ld(bi + n_hi, b4);
+            V4ld<T>::ld(ai + n_hi, a4);
 #pragma unroll
             for (int k = 0; k < 4; ++k) v[5 + k] = b4[k] - a4[k];
           } else {
@@ -378,19 +295,33 @@ __global__ void k_restrict4(T* __restrict__ rc, const T* __restrict__ b, const T
           // coarse Z = 4C + kk sums fine z = 2Z - 1, 2Z, 2Z + 1 = v[2kk], v[2kk + 1], v[2kk + 2]
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk)
-            acc[i][kk] += w * (T(0.5) * v[2 * kk] + v[2 * kk + 1] + T(0.5) * v[2 * kk + 2]);
+            acc[i][kk] += wy * (T(0.5) * v[2 * kk] + v[2 * kk + 1] + T(0.5) * v[2 * kk + 2]);
         }
       }
     }
-    const long long cn = gc.node(X, Y, 4 * C);
-    const uchar4 cmb = *reinterpret_cast<const uchar4*>(cm + cn);
-    const uint8_t cms[4] = {cmb.x, cmb.y, cmb.z, cmb.w};
+    // x: coarse X = X0 + (lane - 1) / 2 on the odd lanes, from fine x - 1, x, x + 1
+    const int X = X0 + ((lane - 1) >> 1);
+    const bool out = (lane & 1) && lane <= 2 * R4_COLS - 1 && X < CX;
+    T o[3][4];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      T o[4];
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) o[kk] = ((cms[kk] >> i) & 1) ? acc[i][kk] : T(0);
-      V4ld<T>::st(rc + i * ccs + cn, o);
+      for (int kk = 0; kk < 4; ++kk) {
+        const T l = __shfl_up_sync(0xffffffffu, acc[i][kk], 1);
+        const T r = __shfl_down_sync(0xffffffffu, acc[i][kk], 1);
+        o[i][kk] = T(0.5) * l + acc[i][kk] + T(0.5) * r;
+      }
+    if (out) {
+      const long long cn = gc.node(X, Y, 4 * C);
+      const uchar4 cmb = *reinterpret_cast<const uchar4*>(cm + cn);
+      const uint8_t cms[4] = {cmb.x, cmb.y, cmb.z, cmb.w};
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        T ov[4];
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) ov[kk] = ((cms[kk] >> i) & 1) ? o[i][kk] : T(0);
+        V4ld<T>::st(rc + i * ccs + cn, ov);
+      }
     }
   }
 }
@@ -400,14 +331,13 @@ __global__ void k_restrict4(T* __restrict__ rc, const T* __restrict__ b, const T
 template <typename T>
 __global__ void k_prolong4(T* __restrict__ xf, const T* __restrict__ xc, const uint8_t* __restrict__ cm,
                            const uint8_t* __restrict__ m, LpGrid gf, LpGrid gc) {
-  const int FX = gf.NX(), FY = gf.NY(), FZ4 = gf.pz / 4;
-  const long long total = (long long)FX * FY * FZ4;
+  const long long total = gf.nodes_padded() / 4;
   const long long fcs = gf.comp_stride(), ccs = gc.comp_stride();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t % FZ4);
-    const long long q = t / FZ4;
-    const int y = (int)(q % FY), x = (int)(q / FY);
-    const long long fn = gf.node(x, y, 4 * c);
+    int x, y, c;
+    gf.node_at(4 * t, x, y, c);
+    c >>= 2;
+    const long long fn = 4 * t;
     const uchar4 mb = *reinterpret_cast<const uchar4*>(m + fn);
     const uint8_t ms[4] = {mb.x, mb.y, mb.z, mb.w};
     if (((mb.x | mb.y | mb.z | mb.w) & 7) == 0) continue;
@@ -422,16 +352,19 @@ __global__ void k_prolong4(T* __restrict__ xf, const T* __restrict__ xc, const u
       for (int bb = 0; bb < 2; ++bb) {
         if (bb && !oy) break;
         const T w = (ox ? T(0.5) : T(1)) * (oy ? T(0.5) : T(1));
-        const long long ccol = gc.node(X0 + a, Y0 + bb, 0);
+        long long cn[3];
         uint8_t cmz[3];
         T cv[3][3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) cmz[k] = cm[ccol + min(Z0 + k, zmax)];
+        for (int k = 0; k < 3; ++k) {
+          cn[k] = gc.node(X0 + a, Y0 + bb, min(Z0 + k, zmax));
+          cmz[k] = cm[cn[k]];
+        }
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
-            const T v = xc[i * ccs + ccol + min(Z0 + k, zmax)];
+            const T v = xc[i * ccs + cn[k]];
             cv[i][k] = ((cmz[k] >> i) & 1) ? v : T(0);
           }
 #pragma unroll
@@ -770,14 +703,8 @@ int lpb_restrict_residual_f32(float* rc, const float* b, const float* ax, const 
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
-  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
-    const long long t4 = (long long)gc.NX() * gc.NY() * (gc.pz / 4);
-    k_restrict4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
-    LP_LAUNCH_CHECK();
-    return LP_OK;
-  }
-  long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
-  k_restrict_residual<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+  const long long nw = (long long)((gc.NX() + R4_COLS - 1) / R4_COLS) * gc.NY() * (gc.pz / 4);
+  k_restrict4<float><<<lp_blocks(32 * nw, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -786,14 +713,8 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
-  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
-    const long long t4 = (long long)gc.NX() * gc.NY() * (gc.pz / 4);
-    k_restrict4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
-    LP_LAUNCH_CHECK();
-    return LP_OK;
-  }
-  long long total = (long long)gc.NX() * gc.NY() * gc.NZ();
-  k_restrict_residual<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
+  const long long nw = (long long)((gc.NX() + R4_COLS - 1) / R4_COLS) * gc.NY() * (gc.pz / 4);
+  k_restrict4<double><<<lp_blocks(32 * nw, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -801,14 +722,8 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
 int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
-  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
-    const long long t4 = (long long)gf.NX() * gf.NY() * (gf.pz / 4);
-    k_prolong4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
-    LP_LAUNCH_CHECK();
-    return LP_OK;
-  }
-  long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
-  k_prolong_add<float><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+  const long long t4 = gf.nodes_padded() / 4;
+  k_prolong4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -816,14 +731,8 @@ int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint
 int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
-  if (gf.pz % 4 == 0 && gc.pz % 4 == 0) {
-    const long long t4 = (long long)gf.NX() * gf.NY() * (gf.pz / 4);
-    k_prolong4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
-    LP_LAUNCH_CHECK();
-    return LP_OK;
-  }
-  long long total = (long long)gf.NX() * gf.NY() * gf.NZ();
-  k_prolong_add<double><<<lp_blocks(total, 256), 256, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
+  const long long t4 = gf.nodes_padded() / 4;
+  k_prolong4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -126,7 +126,7 @@ class DevLevel:
         self.kp = None           # explicit: packed symmetric (300, cells)
         self.ft = None           # explicit: (24, cells) scratch of the cell pass
         self.g1 = None           # weights: 279 corner-parity coefficients (host)
-        self.wc = None           # weights: Walsh coefficients (nx, ny, cpz/4, 8, 4)
+        self.wc = None           # weights: Walsh coefficients (cpz/4, ny, nx, 8, 4)
         self.pbox = None         # weights: node box of the patch cells (host, 6 ints)
         self.mask = None
         self.dinv = None
@@ -350,7 +350,7 @@ class GridElasticity:
 
     def _buf(self, key, grid: DevGrid, dtype):
         t = self._work.get(key)
-        if t is None or t.dtype != dtype or tuple(t.shape) != (3, grid.NX, grid.NY, grid.pz):
+        if t is None or t.dtype != dtype or tuple(t.shape) != (3, grid.pz // 4, grid.NY, grid.NX, 4):
             t = grid.node_field(dtype)
             self._work[key] = t
             self._gen += 1
@@ -374,7 +374,7 @@ class GridElasticity:
         return t
 
     def set_moduli_device(self, e_dev: torch.Tensor):
-        """Moduli already on the device as a padded (nx, ny, pz) float64 cell field.
+        """Moduli already on the device as a float64 cell field of the fine level.
 
         The host decisions of a build (how many levels, which level-1 cells carry patch
         matrices, the coarsest factor's success) depend on the design only through which cells
@@ -545,13 +545,13 @@ class GridElasticity:
         ncp = gc.nx * gc.ny * gc.cpz
         if depth == 1:
             lv = DevLevel("weights", gc, dt)
-            lv.w = self._tbuf("w1", (8, gc.nx, gc.ny, gc.cpz), dt)
+            lv.w = self._tbuf("w1", (8, gc.cpz // 4, gc.ny, gc.nx, 4), dt)
             getattr(L, f"lpb_weights_from_e_f64_{sfx}")(lv.w.data_ptr(), fine.e.data_ptr(), *gf.args, *gc.args, st)
             lv.mcat = self._mcat_dev.get(dt)
             if lv.mcat is None:
                 lv.mcat = torch.tensor(self._mcat.reshape(-1), dtype=dt, device=self.device)
                 self._mcat_dev[dt] = lv.mcat
-            flag = self._tbuf("pflag_new" if plan else "pflag", (gc.nx, gc.ny, gc.cpz), torch.uint8)
+            flag = self._tbuf("pflag_new" if plan else "pflag", (gc.cpz // 4, gc.ny, gc.nx, 4), torch.uint8)
             L.lpb_patch_flags(flag.data_ptr(), fine.e.data_ptr(), fine.mask.data_ptr(), *gf.args, *gc.args, st)
             if plan is not None:
                 pp = plan["patch"]
@@ -563,16 +563,16 @@ class GridElasticity:
                 lv.npatch = int(pcells.numel())
                 lv.pbox = np.zeros(6, np.int32)
                 if lv.npatch:
-                    z = pcells % gc.cpz
-                    yx = pcells // gc.cpz
-                    y = yx % gc.ny
-                    x = yx // gc.ny
+                    col = pcells // 4          # cell index -> (x, y, z), chunked layout
+                    x = col % gc.nx
+                    y = (col // gc.nx) % gc.ny
+                    z = 4 * (col // (gc.nx * gc.ny)) + pcells % 4
                     lo = torch.stack([x.min(), y.min(), z.min()]).cpu().numpy()
                     hi = torch.stack([x.max(), y.max(), z.max()]).cpu().numpy() + 2   # nodes of the last cell
                     lv.pbox[:3] = lo
                     lv.pbox[3:] = hi - lo
                 self._patch_plan = {"cells": pcells, "n": lv.npatch, "box": lv.pbox}
-            lv.patch_id = self._tbuf("patch_id", (gc.nx, gc.ny, gc.cpz), torch.int32, -1)
+            lv.patch_id = self._tbuf("patch_id", (gc.cpz // 4, gc.ny, gc.nx, 4), torch.int32, -1)
             if plan is None:
                 lv.patch_id.fill_(-1)
             if lv.npatch:
@@ -586,7 +586,7 @@ class GridElasticity:
             lv.patch_cells = pcells
             lv.g1 = self.g1
             # the Walsh coefficients of each cell's child moduli, chunked for the march kernel
-            lv.wc = self._tbuf("wc1", (gc.nx, gc.ny, gc.cpz // 4, 8, 4), dt)
+            lv.wc = self._tbuf("wc1", (gc.cpz // 4, gc.ny, gc.nx, 8, 4), dt)
             getattr(L, f"lpb_walsh_chunks_{sfx}")(lv.wc.data_ptr(), lv.w.data_ptr(), *gc.args, st)
             lv.err = self._err
             return lv
@@ -1056,7 +1056,7 @@ class GridElasticity:
 
     def live_dofs(self):
         """Bool per mesh dof: carries stiffness (loadpath/mg.py:967-973)."""
-        m = self.levels[0].mask[:, :, :self.g0.NZ].cpu().numpy()
+        m = self.g0.node_grid(self.levels[0].mask).cpu().numpy()
         a = np.stack([(m >> (3 + c)) & 1 for c in range(3)]).astype(bool).reshape(3, -1)
         out = np.empty(3 * len(self.node_flat), bool)
         for i in range(3):

@@ -49,12 +49,10 @@ class DeviceFilter:
         self.toff = torch.tensor([list(d) for d, _ in taps], dtype=torch.int32, device=grid.device).reshape(-1)
         self.tw = torch.tensor([w for _, w in taps], dtype=torch.float64, device=grid.device)
         self.full = float(sum(w for _, w in taps))
-        ones = grid.cell_field(torch.float64)
-        ones[:, :, :grid.nz] = 1.0
+        ones = grid.set_cells(grid.cell_field(torch.float64), 1.0)
         self.rowsum = self.apply(grid.cell_field(torch.float64), ones)
         if pad:
-            self.hs = grid.cell_field(torch.float64)
-            self.hs[:, :, :grid.nz] = self.full
+            self.hs = grid.set_cells(grid.cell_field(torch.float64), self.full)
         else:
             self.hs = self.rowsum
         # H (1 / hs): the filtered volume's weights, and top3d's dv = H (1 / hs)
@@ -181,10 +179,11 @@ class Top3dLoop:
         self.f = g.nodes_to_dev(np.asarray(f_grid, np.float64), torch.float64)
         self.x = g.cell_field(torch.float64)
         if x0 is None:
-            self.x[:, :, :g.nz] = self.volfrac
+            g.set_cells(self.x, self.volfrac)
         else:
             g.cells_to_dev(np.asarray(x0, np.float64), torch.float64, out=self.x)
         self.xphys = self.x.clone()
+        self._x_stage = None     # step_host: the design in grid order on the device
         self.xnew = g.cell_field(torch.float64)
         self.e = g.cell_field(torch.float64)
         self.ce = g.cell_field(torch.float64)
@@ -274,10 +273,13 @@ class Top3dLoop:
         formed on the device, and the updated design comes back in out_host. Returns
         (compliance, change)."""
         g = self.grid
-        self.x[:, :, :g.nz].copy_(x_host, non_blocking=True)
+        if self._x_stage is None:
+            self._x_stage = torch.empty(g.cells, dtype=torch.float64, device=g.device)
+        self._x_stage.copy_(x_host, non_blocking=True)
+        g.set_cells(self.x, self._x_stage)
         self.filter.apply(self.xphys, self.x, hs_out=self.filter.hs, e_out=self.e, penal=self.penal, emin=self.emin)
         c, change = self.step()
-        out_host.copy_(self.x[:, :, :g.nz], non_blocking=True)
+        out_host.copy_(g.cell_grid(self.x), non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return c, change
 

@@ -24,12 +24,11 @@ def _inputs(dims, seed):
     ncp = g.nx * g.ny * g.cpz
     a = torch.randn((ncp, 24, 24), generator=gen, device="cuda")
     k = (a + a.transpose(1, 2)).contiguous()
-    cells = torch.zeros((g.nx, g.ny, g.cpz), device="cuda")
-    cells[:, :, :g.nz] = 1.0
+    cells = g.set_cells(g.cell_field(torch.float32), 1.0)   # zero on the z padding
     k *= cells.reshape(-1, 1, 1)
-    mask = torch.randint(0, 8, (g.NX, g.NY, g.pz), generator=gen, device="cuda", dtype=torch.uint8)
-    mask[:, :, g.NZ:] = 0
-    u = torch.randn((3, g.NX, g.NY, g.pz), generator=gen, device="cuda")
+    mask = g.set_nodes(g.mask_field(), torch.randint(0, 8, (g.NX, g.NY, g.NZ), generator=gen, device="cuda",
+                                                     dtype=torch.uint8))
+    u = torch.randn(g.node_field(torch.float32).shape, generator=gen, device="cuda")
     bits = torch.stack([((mask >> c) & 1) for c in range(3)]).float()
     u *= bits
     return g, k, u, mask
