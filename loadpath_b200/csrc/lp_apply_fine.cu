@@ -10,12 +10,13 @@
 // brings the operator under the HBM roofline on CUDA cores.
 //
 // Work layout. A block owns a 15 x 15 patch of node columns and runs 16 x 16 threads, one per
-// cell column of the patch plus a one-cell halo on the low x and y sides. Each thread marches
-// its column along z four cells at a time: it loads four z-planes of its four node columns
-// with 16-byte loads (and the fifth plane with a scalar load), forms per plane the x-y modes
-// (4 per component), combines consecutive
-// planes into the cell's z modes, applies E_c K^ in the modal basis and transforms back to
-// the cell's two faces. A node plane's modal force is the upper face of the cell below plus
+// cell column of the patch plus a one-cell halo on the low x and y sides, lanes along x. It
+// marches along z one chunk of four planes at a time: TMA brings the chunk's 17 x 17 node
+// columns (and cell moduli) into a ring of shared-memory stages; in the z-chunked field layout
+// each box row is 17 columns x 4 planes, one contiguous run. A thread reads its four node
+// columns' four planes (and the next chunk's first), forms per plane the x-y modes
+// (4 per component), combines consecutive planes into the cell's z modes, applies E_c K^ in
+// the modal basis and transforms back to the cell's two faces. A node plane's modal force is the upper face of the cell below plus
 // the lower face of the cell above, both in this thread, so z needs no exchange; the four cell
 // columns around a node column exchange their corner forces through shared memory.
 // No atomics, no scatter: every output is written once by its owner.
