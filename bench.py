@@ -46,7 +46,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--micro", choices=["apply"], default=None,
-                   help="only the fine-level K*u microbenchmark (config 1: applies on seeded N(0,1) vectors)")
+                   help="only the K*u microbenchmarks (fine level in both precisions, then the level-1 "
+                        "weights operator; applies on seeded N(0,1) vectors)")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--kernels", type=int, default=0, metavar="N",
                    help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
@@ -440,6 +441,31 @@ def run_micro_apply(args):
         gbs = apply_bytes(dims, isz) / (us * 1e-6) / 1e9
         out["f32" if isz == 4 else "f64"] = {"us_per_apply": us, "GBps": gbs, "frac_of_peak": gbs / peaks()[0]}
     ge.check_device()
+    # the level-1 (weights) operator of the solver's own hierarchy, float32
+    ge1 = GridElasticity(mesh, 0.3, fx, element="im")
+    ge1.set_moduli_device(e)
+    lv = ge1._op(1)
+    if lv.kind == "weights":
+        gr = lv.grid
+        m = torch.stack([((lv.mask >> c) & 1) for c in range(3)]).to(lv.dtype)
+        u = torch.randn((3, gr.pz // 4, gr.NY, gr.NX, 4), generator=torch.Generator(device="cuda").manual_seed(102),
+                        device="cuda", dtype=torch.float64).to(lv.dtype) * m
+        o = gr.node_field(lv.dtype)
+        for _ in range(3):
+            lv.apply(o, u)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.reps):
+            lv.apply(o, u)
+        b.record()
+        torch.cuda.synchronize()
+        us = a.elapsed_time(b) / args.reps * 1e3
+        isz = 4 if lv.dtype == torch.float32 else 8
+        nb = (2 * 3 * gr.NX * gr.NY * gr.NZ + 8 * gr.nx * gr.ny * gr.nz) * isz
+        out["level1"] = {"dims": list(gr.cells), "us_per_apply": us, "GBps": nb / (us * 1e-6) / 1e9,
+                         "patch_cells": int(lv.npatch)}
+        ge1.check_device()
     print(json.dumps({"micro": "fine K*u apply", "dims": list(dims), "reps": args.reps, **out}))
     return 0
 

@@ -319,6 +319,10 @@ class GridElasticity:
         self._gcache = {}
         self._gen = 0            # bumped whenever a work buffer is (re)allocated
         self._cap_stream = torch.cuda.Stream(device=self.device)
+        self._side = torch.cuda.Stream(device=self.device, priority=-1)   # coarsest factorisation
+        self._ev_fork = torch.cuda.Event()
+        self._ev_join = torch.cuda.Event()
+        self._joined = True
 
     # --- layout conversion (loadpath/mg.py:495-511) -----------------------------------
     def to_grid(self, v, dtype=np.float64):
@@ -476,6 +480,7 @@ class GridElasticity:
         info = self._build_coarse(levels[-1])
         for i in range(len(levels)):
             self._estimate_lmax(i)
+        self._join_coarse()
         if plan is None:
             if info is not None:
                 st_pivot, st_barrier = (int(v) for v in info.cpu().numpy())
@@ -645,13 +650,28 @@ class GridElasticity:
         linv = self._tbuf("band_linv", (nt * 1024,), torch.float64)
         info = self._tbuf("band_info", (2,), torch.int32)
         bar = self._tbuf("band_bar", (64,), torch.int32)
-        L.lpb_memset_async(info.data_ptr(), 0, 8, st)
-        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
-                          *g.args, st)
         ainv = self._tbuf("band_ainv", (npad, npad), torch.float64)
-        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *g.args, st)
         self._coarse = {"ainv": ainv, "v": self._tbuf("coarse_v", (npad,), torch.float64), "n": n}
+        # The factorisation and the inverse are latency-bound chains on a fraction of the SMs;
+        # they run on a high-priority side stream, overlapped with the power iterations the
+        # caller issues next on the main stream, which joins before anything reads them.
+        main = torch.cuda.current_stream()
+        self._ev_fork.record(main)
+        self._side.wait_event(self._ev_fork)
+        ss = self._side.cuda_stream
+        L.lpb_memset_async(info.data_ptr(), 0, 8, ss)
+        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
+                          *g.args, ss)
+        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *g.args, ss)
+        self._ev_join.record(self._side)
+        self._joined = False
         return info
+
+    def _join_coarse(self):
+        """The main stream waits for the side stream's factorisation and inverse."""
+        if not self._joined:
+            torch.cuda.current_stream().wait_event(self._ev_join)
+            self._joined = True
 
     def _op(self, i):
         return self._l0s if i == 0 else self.levels[i]
