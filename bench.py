@@ -45,9 +45,10 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--micro", choices=["apply"], default=None,
-                   help="only the K*u microbenchmarks (fine level in both precisions, then the level-1 "
-                        "weights operator; applies on seeded N(0,1) vectors)")
+    p.add_argument("--micro", choices=["apply", "band"], default=None,
+                   help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
+                        "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
+                        "coarsest level's band assembly, factorisation and inverse")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--kernels", type=int, default=0, metavar="N",
                    help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
@@ -470,6 +471,74 @@ def run_micro_apply(args):
     return 0
 
 
+def run_micro_band(args):
+    """args.reps rebuilds of the coarsest level's direct solve alone, on the main stream: the band
+    assembly, the tiled Cholesky (k_band_factor) and the dense inverse (k_band_inverse), each timed
+    with CUDA events; one JSON line."""
+    import torch
+
+    from loadpath_b200._lib import lib
+    from loadpath_b200.grid import DevGrid, stream_handle
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from loadpath_b200.simp import DeviceFilter
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    g = DevGrid(dims)
+    rng = np.random.default_rng(1)
+    flt = DeviceFilter(g, 2.0)
+    xr = g.cells_to_dev(np.exp(rng.uniform(np.log(1e-3), 0.0, dims)), torch.float64)
+    x = flt.apply(g.cell_field(torch.float64), xr, hs_out=flt.hs)
+    e = g.cell_field(torch.float64)
+    L = lib()
+    st = stream_handle()
+    L.lpb_simp_law(e.data_ptr(), x.data_ptr(), PENAL, EMIN, *g.args, st)
+    fixed, _ = cantilever(dims)
+    mesh = BoxMesh(dims)
+    fx = np.empty(mesh.n_dof, bool)
+    for i in range(3):
+        fx[i::3] = fixed[i].reshape(-1)
+    ge = GridElasticity(mesh, 0.3, fx, element="im")
+    ge.set_moduli_device(e)
+    torch.cuda.synchronize()
+    lv = ge.levels[-1]
+    gr = lv.grid
+    w = ge._work
+    t, linv, info, bar, ainv = (w[k] for k in ("band_t", "band_linv", "band_info", "band_bar", "band_ainv"))
+    sfx = "f32" if lv.dtype == torch.float32 else "f64"
+
+    def ptr_or_none(a):
+        return None if a is None else a.data_ptr()
+
+    times = {"assemble": [], "factor": [], "inverse": []}
+    for r in range(args.reps + 3):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        if lv.kind == "weights":
+            getattr(L, f"lpb_coarse_band_{sfx}")(t.data_ptr(), 1, lv.w.data_ptr(), lv.mcat.data_ptr(),
+                                                 ptr_or_none(lv.patch_id), ptr_or_none(lv.patch_k), None,
+                                                 lv.mask.data_ptr(), *gr.args, st)
+        else:
+            getattr(L, f"lpb_coarse_band_{sfx}")(t.data_ptr(), 2, None, None, None, None, lv.k.data_ptr(),
+                                                 lv.mask.data_ptr(), *gr.args, st)
+        L.lpb_memset_async(info.data_ptr(), 0, 8, st)
+        ev[1].record()
+        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
+                          *gr.args, st)
+        ev[2].record()
+        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *gr.args, st)
+        ev[3].record()
+        torch.cuda.synchronize()
+        if r >= 3:
+            for k, (a, b) in zip(times, zip(ev[:-1], ev[1:])):
+                times[k].append(a.elapsed_time(b) * 1e3)
+    status = [int(v) for v in info.cpu().numpy()]
+    out = {k: float(np.median(v)) for k, v in times.items()}
+    print(json.dumps({"micro": "coarsest direct solve rebuild", "dims": list(dims),
+                      "coarsest_nodes": [gr.NX, gr.NY, gr.NZ], "reps": args.reps, "us": out, "status": status}))
+    return 0
+
+
 def run_kernels(args):
     """Per-kernel device time of args.kernels SIMP iterations after args.warmup, from the CUDA
     activity records (CUPTI through torch.profiler: kernels are not serialised)."""
@@ -524,6 +593,8 @@ def main():
     sys.path.insert(0, ROOT)
     if args.micro == "apply":
         return run_micro_apply(args)
+    if args.micro == "band":
+        return run_micro_band(args)
     if args.kernels:
         return run_kernels(args)
     if args.impl == "reference":

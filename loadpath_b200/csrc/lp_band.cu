@@ -77,7 +77,8 @@ __device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv
     for (int j = 0; j < 32; ++j) {
       const double p = __shfl_sync(0xffffffffu, a[j], j);
       if (!(p > 0.0) && bad == 0) bad = (int)(row0 + j + 1);
-      const double d = sqrt(p), rd = 1.0 / d;
+      // one reciprocal square root per pivot on the chain (not a square root and a division)
+      const double rd = rsqrt(p), d = p * rd;
       const double l = i > j ? a[j] * rd : (i == j ? d : 0.0);
       a[j] = l;
 #pragma unroll
