@@ -238,10 +238,30 @@ int lpb_graph_free(void* exec);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
 int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 
-/* ---- coarsest level: inverse of the dense SPD operator in place (cuSOLVER potrf + potri, then
- * the triangle mirrored); info: two device ints (factorization, inversion), nonzero when the
- * matrix is not positive definite (the reference then rebuilds the hierarchy strict,
- * loadpath/mg.py:580-586) */
+/* ---- MMA (loadpath/mma.py:31-214, MMA.update and MMA._subsolv): the n-sized work of one
+ * update over n variables and m <= 8 constraints, float64, device arrays; P, Q, df are (m, n)
+ * row-major. `part` is scratch of lpb_mma_part_len(m) doubles; each reduction writes its values to
+ * `out` / `bsum` (device) with M = m rounded up to 1, 2, 4 or 8 entries per m-sized group.
+ * lam / dlam are HOST pointers to m doubles. The host runs the interior-point loops and the
+ * (m + 1) x (m + 1) Newton system (loadpath/mma.py:127-214). */
+long long lpb_mma_part_len(int m);
+/* sanitise x, df0, df in place (non-finite values as the reference reads them), move the
+ * asymptotes (init: the first two iterations), alfa/beta, p0 q0 P Q; bsum[i] = sum_j P_ij / (upp_j -
+ * x_j) + Q_ij / (x_j - low_j)   (loadpath/mma.py:57-103) */
+int lpb_mma_prepare(long long n, int m, double* x, const double* xmin, const double* xmax, double* low, double* upp, const double* xold1, const double* xold2, int init, double asyinit, double asyincr, double asydecr, double move, double* df0, double* df, double* alfa, double* beta, double* p0, double* q0, double* P, double* Q, double* part, double* bsum, void* stream);
+/* the subsolver's start: x = (alfa + beta) / 2, xsi = max(1 / (x - alfa), 1), eta = max(1 / (beta - x), 1) */
+int lpb_mma_sub_init(long long n, const double* alfa, const double* beta, double* xs, double* xsi, double* eta, void* stream);
+/* a Newton step's n-sized terms: delx, diagx; out = [gvec (M), GG (delx / diagx) (M),
+ * (GG / diagx) GG^T upper triangle row by row (M (M + 1) / 2)] */
+int lpb_mma_newton_a(long long n, int m, const double* low, const double* upp, const double* alfa, const double* beta, const double* p0, const double* q0, const double* P, const double* Q, const double* xs, const double* xsi, const double* eta, const double* lam, double epsi, double* delx, double* diagx, double* part, double* out, void* stream);
+/* dx, dxsi, deta from dlam; out = [max -1.01 dxsi / xsi, max -1.01 deta / eta,
+ * max -1.01 dx / (x - alfa), max 1.01 dx / (beta - x)] */
+int lpb_mma_newton_b(long long n, int m, const double* low, const double* upp, const double* alfa, const double* beta, const double* P, const double* Q, const double* xs, const double* xsi, const double* eta, const double* delx, const double* diagx, const double* dlam, double epsi, double* dx, double* dxsi, double* deta, double* part, double* out, void* stream);
+/* (xs, xsi, eta) = (xs0, xsi0, eta0) + steg (dx, dxsi, deta) (dx NULL: evaluate at xs0 only);
+ * out = [sum of squares, largest magnitude of the residual's n-sized rows, gvec (M)] */
+int lpb_mma_trial(long long n, int m, const double* low, const double* upp, const double* alfa, const double* beta, const double* p0, const double* q0, const double* P, const double* Q, const double* xs0, const double* xsi0, const double* eta0, const double* dx, const double* dxsi, const double* deta, double steg, const double* lam, double epsi, double* xs, double* xsi, double* eta, double* part, double* out, void* stream);
+/* xnew = clip(finite(xs) ? xs : x, alfa, beta)   (loadpath/mma.py:104-108) */
+int lpb_mma_finish(long long n, const double* xs, const double* x, const double* alfa, const double* beta, double* xnew, void* stream);
 
 #ifdef __cplusplus
 }
