@@ -229,6 +229,18 @@ int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const dou
 /* volumes[j] of the clipped OC step at nl = 31 multipliers lam[j] (device), weights gv = H (1 / hs) */
 int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv, const double* lam, int nl, double move, double* part, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* dv, double lam, double move, double* part, double* change, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* loadpath's own design update; flags: uint8 per cell, bit 0 passive solid, bit 1 passive void
+ * (NULL: none). lpb_project: xp = (tanh(b eta) + tanh(b (xt - eta))) / den and its derivative dxp
+ * (either NULL to skip), held cells 1 / 0 with derivative 0, and *vol = sum xp w when w is given
+ * (part: 592 doubles)   (loadpath/simp.py:1443-1450 _project/_dproject, :1779-1785 physical,
+ * :1809-1814 eroded) */
+int lpb_project(double* xp, double* dxp, const double* xt, double beta, double eta, const uint8_t* flags, const double* w, double* part, double* vol, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* xn = clip(x sqrt(-dc / dv) / sqrt(lm), max(0, x - move), min(1, x + move)), held cells 1 / 0
+ * (loadpath/simp.py:2314-2318, the optimality-criteria step at one volume multiplier) */
+int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* dv, double lm, double move, const uint8_t* flags, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* out = a * b (b NULL: a), 0 on held cells, then min(out, 0) when clip0: the products the filter
+ * chain rule feeds to H^T (loadpath/simp.py:2001, :2077, :2191) */
+int lpb_cell_product(double* out, const double* a, const double* b, const uint8_t* flags, int clip0, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
 /* ---- CUDA graphs of a stream's work (the solver records one CG iteration per solve) */
 int lpb_capture_begin(void* stream);

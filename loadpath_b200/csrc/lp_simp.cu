@@ -263,6 +263,76 @@ __global__ void k_sum_final_s(const double* __restrict__ part, int n, double* __
   if (threadIdx.x == 0) *out = s;
 }
 
+
+// ---- loadpath's own design update (loadpath/simp.py:1443-1450, :1775-1814, :2249-2376) --------
+// Cell flags: bit 0 passive solid (pres: design and projection held at 1, derivative 0), bit 1
+// passive void (held at 0).
+
+// xp = (tanh(b eta) + tanh(b (xt - eta))) / den, den = tanh(b eta) + tanh(b (1 - eta)); dxp its
+// derivative b (1 - tanh(b (xt - eta))^2) / den; held cells as the flags say; partial sums of
+// xp * w into part[block] (w given)
+__global__ void k_project(double* __restrict__ xp, double* __restrict__ dxp, const double* __restrict__ xt,
+                          double beta, double eta, double tbe, double den, const uint8_t* __restrict__ flags,
+                          const double* __restrict__ w, LpGrid g, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const long long total = g.cells_padded();
+  double acc = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const uint8_t fl = flags ? flags[t] : 0;
+    const double th = tanh(beta * (xt[t] - eta));
+    double p = (tbe + th) / den, dp = beta * (1.0 - th * th) / den;
+    if (fl & 1) {
+      p = 1.0;
+      dp = 0.0;
+    } else if (fl & 2) {
+      p = 0.0;
+      dp = 0.0;
+    }
+    if (xp) xp[t] = p;
+    if (dxp) dxp[t] = dp;
+    if (w) acc += p * w[t];
+  }
+  if (part) {
+    acc = lp_block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  }
+}
+
+// the OC step at multiplier lm: xn = clip(x sqrt(-dc / dv) / sqrt(lm), max(0, x - move),
+// min(1, x + move)), held cells as the flags say
+__global__ void k_oc_stepped(double* __restrict__ xn, const double* __restrict__ x, const double* __restrict__ dc,
+                             const double* __restrict__ dv, double lm, double move, const uint8_t* __restrict__ flags,
+                             LpGrid g) {
+  const double sl = sqrt(lm);
+  const long long total = g.cells_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    const double xv = x[t];
+    double v = fmin(fmax(xv * sqrt(-dc[t] / dv[t]) / sl, fmax(0.0, xv - move)), fmin(1.0, xv + move));
+    const uint8_t fl = flags ? flags[t] : 0;
+    if (fl & 1) v = 1.0;
+    else if (fl & 2) v = 0.0;
+    xn[t] = v;
+  }
+}
+
+// out = a * b (zero where the flags hold a cell); with clip0, out = min(out, 0)
+__global__ void k_cell_product(double* __restrict__ out, const double* __restrict__ a, const double* __restrict__ b,
+                               const uint8_t* __restrict__ flags, int clip0, LpGrid g) {
+  const long long total = g.cells_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int x_, y_, z;
+    if (!g.cell_at(t, x_, y_, z)) continue;
+    double v = b ? a[t] * b[t] : a[t];
+    if (flags && (flags[t] & 3)) v = 0.0;
+    if (clip0) v = fmin(v, 0.0);
+    out[t] = v;
+  }
+}
+
 }  // namespace
 
 #define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
@@ -345,6 +415,38 @@ int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* 
   if (!lp_grid_ok(g) || !xnew || !x || !dc || !dv || !part || !change) return LP_ERR_ARG;
   k_oc_apply<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xnew, x, dc, dv, lam, move, g, part);
   k_max_final2<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, change);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// xp, dxp (either may be NULL) of the projection at (beta, eta); *vol = sum xp * w when w and vol
+// are given (part: LP_SIMP_BLOCKS doubles)
+int lpb_project(double* xp, double* dxp, const double* xt, double beta, double eta, const uint8_t* flags,
+                const double* w, double* part, double* vol, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !xt || (w && (!part || !vol))) return LP_ERR_ARG;
+  const double tbe = tanh(beta * eta), den = tbe + tanh(beta * (1.0 - eta));
+  k_project<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xp, dxp, xt, beta, eta, tbe, den, flags, w, g, w ? part : nullptr);
+  if (w) k_sum_final_s<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, vol);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* dv, double lm, double move,
+                   const uint8_t* flags, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !xn || !x || !dc || !dv || !(lm > 0.0)) return LP_ERR_ARG;
+  k_oc_stepped<<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(xn, x, dc, dv, lm, move, flags, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// out = a * b (b NULL: a), zero on flagged cells, then min(., 0) when clip0
+int lpb_cell_product(double* out, const double* a, const double* b, const uint8_t* flags, int clip0, LP_GRID_ARGS,
+                     void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !out || !a) return LP_ERR_ARG;
+  k_cell_product<<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(out, a, b, flags, clip0, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -23,7 +23,8 @@ from ._lib import lib
 from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
-__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "Top3dLoop", "_project", "_dproject"]
+__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "ProjectedDesign", "Top3dLoop",
+           "_project", "_dproject"]
 
 
 def filter_taps(radius: float, pitch: float = 1.0):
@@ -102,6 +103,128 @@ def _dproject(xt, beta, eta):
     """its derivative (loadpath/simp.py:1448-1450)."""
     den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
     return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+VOLUME_RTOL = 1e-13   # the volume multiplier's stopping tolerance (loadpath/simp.py:1234)
+
+
+class ProjectedDesign:
+    """loadpath's own design update on the device: the filtered and projected physical density
+    (loadpath/simp.py:1775-1786 `physical`, :1809-1814 `eroded`), the filter chain rule of a
+    gradient through the projection (loadpath/simp.py:1995-2001, :2077), and the optimality-
+    criteria step whose volume multiplier is solved to rounding (loadpath/simp.py:2249-2376): bracket
+    the root outward from the last step's multiplier in log space, then false position with the
+    Illinois modification, every trial measured on the physical density's volume.
+
+    flt: the grid's DeviceFilter (H symmetric, as the reference's cone filter); w: volume weight per
+    cell (float64 cell field; None: 1 on every cell); flags: uint8 cell field, bit 0 passive solid
+    (held at 1), bit 1 passive void (held at 0), or None. The reference's mirror symmetry, column
+    extrusion, printed-hook and blockage terms are not part of this step."""
+
+    def __init__(self, flt: DeviceFilter, w=None, flags=None):
+        g = flt.grid
+        self.flt, self.grid, self.flags = flt, g, flags
+        self.w = w if w is not None else g.set_cells(g.cell_field(torch.float64), 1.0)
+        self.xt = g.cell_field(torch.float64)
+        self.xp = g.cell_field(torch.float64)
+        self.xn = g.cell_field(torch.float64)
+        self._tmp = g.cell_field(torch.float64)
+        self._part = torch.zeros(592, dtype=torch.float64, device=g.device)
+        self._vol = torch.zeros(1, dtype=torch.float64, device=g.device)
+        self.lam_last = None
+        self.n_eval = 0
+
+    def physical(self, x, beta, eta, xp=None, dxp=None):
+        """xt = H x / hs into self.xt, its projection into xp (default self.xp) and the derivative
+        into dxp (if given); returns the projected volume sum xp w."""
+        L = lib()
+        g = self.grid
+        self.flt.apply(self.xt, x, hs_out=self.flt.hs)
+        xp = self.xp if xp is None else xp
+        L.lpb_project(xp.data_ptr(), ptr(dxp), self.xt.data_ptr(), float(beta), float(eta), ptr(self.flags),
+                      self.w.data_ptr(), self._part.data_ptr(), self._vol.data_ptr(), *g.args, stream_handle())
+        return float(self._vol.item())
+
+    def chain(self, out, grad, dxp, clip=False):
+        """out = H^T (grad dxp / hs) (zero on held cells), then min(out, 0) with clip."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        L.lpb_cell_product(self._tmp.data_ptr(), grad.data_ptr(), ptr(dxp), ptr(self.flags), 0, *g.args, st)
+        self.flt.apply(out, self._tmp, hs_in=self.flt.hs)
+        if clip:
+            L.lpb_cell_product(out.data_ptr(), out.data_ptr(), None, None, 1, *g.args, st)
+        return out
+
+    def oc_step(self, x, dc, dv, move, beta, eta, target):
+        """The step x -> clip(x sqrt(-dc / dv / lm), x -+ move) with the multiplier lm that puts the
+        physical volume on target (loadpath/simp.py:2320-2376). Returns (x_new, lm, held): x_new is
+        self.xn (the last trial), held False when the move limits kept the volume off target."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        n_eval = [0]
+
+        def stepped(lm_):
+            n_eval[0] += 1
+            L.lpb_oc_stepped(self.xn.data_ptr(), x.data_ptr(), dc.data_ptr(), dv.data_ptr(), float(lm_), float(move),
+                             ptr(self.flags), *g.args, st)
+            return self.physical(self.xn, beta, eta) - target
+
+        l1, l2 = 1e-12, 1e12
+        s_lo, s_hi = np.log(l1), np.log(l2)
+        lam_last = self.lam_last
+        sm = min(max(np.log(lam_last), s_lo), s_hi) if lam_last else 0.0
+        f = stepped(float(np.exp(sm)))
+        lm = float(np.exp(sm))
+        s1 = s2 = sm
+        f1 = f2 = None
+        if f > 0:
+            f1 = f
+        else:
+            f2 = f
+        reach = 0.25
+        while (f1 is None or f2 is None) and f != 0.0:
+            if f1 is None:
+                if s1 <= s_lo:
+                    break
+                s1 = max(s1 - reach, s_lo)
+                sm = s1
+            else:
+                if s2 >= s_hi:
+                    break
+                s2 = min(s2 + reach, s_hi)
+                sm = s2
+            reach *= 4.0
+            lm = float(np.exp(sm))
+            f = stepped(lm)
+            if f > 0:
+                f1, s1 = f, sm
+            else:
+                f2, s2 = f, sm
+        if f1 is not None and f2 is not None:
+            side = 0
+            for _ in range(60):
+                if abs(f) <= VOLUME_RTOL * target or f2 == f1 or s2 - s1 <= 4e-16 * max(abs(s1), abs(s2), 1.0):
+                    break
+                sm = (s1 * f2 - s2 * f1) / (f2 - f1)
+                if not s1 < sm < s2:
+                    sm = 0.5 * (s1 + s2)
+                lm = float(np.exp(sm))
+                f = stepped(lm)
+                if f > 0:
+                    s1, f1 = sm, f
+                    if side == 1:
+                        f2 *= 0.5
+                    side = 1
+                else:
+                    s2, f2 = sm, f
+                    if side == -1:
+                        f1 *= 0.5
+                    side = -1
+        self.lam_last = lm
+        self.n_eval = n_eval[0]
+        return self.xn, lm, f1 is not None and f2 is not None
 
 
 def oc_bisection(volumes, target, l1=0.0, l2=1e9, tol=1e-3, width=31):

@@ -683,6 +683,104 @@ def oc_top3d(x, dc, dv, volfrac, h_apply, hs, move=0.2):
     return xnew, xphys
 
 
+def project(xt, beta, eta):
+    """tanh Heaviside projection (loadpath/simp.py:1443-1446)."""
+    den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+    return (np.tanh(beta * eta) + np.tanh(beta * (xt - eta))) / den
+
+
+def dproject(xt, beta, eta):
+    """its derivative in xt (loadpath/simp.py:1448-1450)."""
+    den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
+    return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+VOLUME_RTOL = 1e-13   # loadpath/simp.py:1234
+
+
+def oc_loadpath_step(x, dc, dv, move, beta, eta, h_apply, hs, w, target, pres=None, void=None,
+                     lam_last=None):
+    """loadpath's optimality-criteria step (loadpath/simp.py:2249-2376, the volume-constrained
+    path: no thermal swing constraint, mirror, extrusion or blockage term). The step
+    x sqrt(-dc / dv / lm) clipped to [max(0, x - move), min(1, x + move)] (passive cells held),
+    measured on the physical volume sum(project(H x / hs) w); the multiplier is bracketed outward
+    from lam_last in log space (reach 0.25, x4 per try, range 1e-12..1e12), then found by false
+    position with the Illinois halving, to |f| <= 1e-13 target. Returns (x_new, lm, n_eval, held)."""
+    lo_x = np.maximum(0.0, x - move)
+    hi_x = np.minimum(1.0, x + move)
+    ratio = np.sqrt(-dc / dv)
+    n_eval = [0]
+
+    def physical(xv):
+        xp = project(h_apply(xv) / hs, beta, eta)
+        if pres is not None:
+            xp[pres] = 1.0
+        if void is not None:
+            xp[void] = 0.0
+        return xp
+
+    def stepped(lm_):
+        n_eval[0] += 1
+        xn = np.clip(x * ratio / np.sqrt(lm_), lo_x, hi_x)
+        if pres is not None:
+            xn[pres] = 1.0
+        if void is not None:
+            xn[void] = 0.0
+        return xn, float(np.sum(physical(xn) * w)) - target
+
+    l1, l2 = 1e-12, 1e12
+    s_lo, s_hi = np.log(l1), np.log(l2)
+    sm = min(max(np.log(lam_last), s_lo), s_hi) if lam_last else 0.0
+    x_new, f = stepped(float(np.exp(sm)))
+    lm = float(np.exp(sm))
+    s1 = s2 = sm
+    f1 = f2 = None
+    if f > 0:
+        f1 = f
+    else:
+        f2 = f
+    reach = 0.25
+    while (f1 is None or f2 is None) and f != 0.0:
+        if f1 is None:
+            if s1 <= s_lo:
+                break
+            s1 = max(s1 - reach, s_lo)
+            sm = s1
+        else:
+            if s2 >= s_hi:
+                break
+            s2 = min(s2 + reach, s_hi)
+            sm = s2
+        reach *= 4.0
+        lm = float(np.exp(sm))
+        x_new, f = stepped(lm)
+        if f > 0:
+            f1, s1 = f, sm
+        else:
+            f2, s2 = f, sm
+    if f1 is not None and f2 is not None:
+        side = 0
+        for _ in range(60):
+            if abs(f) <= VOLUME_RTOL * target or f2 == f1 or s2 - s1 <= 4e-16 * max(abs(s1), abs(s2), 1.0):
+                break
+            sm = (s1 * f2 - s2 * f1) / (f2 - f1)
+            if not s1 < sm < s2:
+                sm = 0.5 * (s1 + s2)
+            lm = float(np.exp(sm))
+            x_new, f = stepped(lm)
+            if f > 0:
+                s1, f1 = sm, f
+                if side == 1:
+                    f2 *= 0.5
+                side = 1
+            else:
+                s2, f2 = sm, f
+                if side == -1:
+                    f1 *= 0.5
+                side = -1
+    return x_new, lm, n_eval[0], f1 is not None and f2 is not None
+
+
 # --------------------------------------------------------------------------
 # assembled direct solve for tiny grids (loadpath/benchmarks/evaluate.py:111-117)
 # --------------------------------------------------------------------------

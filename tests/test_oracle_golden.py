@@ -191,3 +191,38 @@ def test_c_port_apply_matches_golden(name):
     op32 = cport.MaskedApply(l0.ke, l0.e, l0.mask, np.float32)
     want = g["L0_apply"]
     np.testing.assert_allclose(op32(g["L0_u"]), want, rtol=2e-5, atol=2e-5 * np.abs(want).max())
+
+
+def test_projection_matches_reference():
+    g = _load("filter.npz")
+    for beta in (1.0, 8.0):
+        np.testing.assert_allclose(R.project(g["proj_x"], beta, 0.5), g[f"proj_{beta}"], rtol=1e-15, atol=0)
+        np.testing.assert_allclose(R.dproject(g["proj_x"], beta, 0.5), g[f"dproj_{beta}"], rtol=1e-15, atol=0)
+
+
+@pytest.mark.parametrize("beta,lam_last", [(1.0, None), (8.0, None), (4.0, 3e-3)])
+def test_oracle_oc_loadpath_step_lands_on_the_volume(beta, lam_last):
+    """The restated step (the reference's closure inside simp.optimize is not callable alone)
+    lands the projected volume on target to the reference's tolerance, moves no cell past its
+    move limit and keeps the passive cells."""
+    rng = np.random.default_rng(5)
+    dims = (14, 9, 7)
+    taps = R.filter_taps(2.0)
+    hs = R.filter_row_sums(dims, taps)
+    x = 0.2 + 0.6 * rng.random(dims)
+    dc = -np.exp(rng.uniform(-3, 1, dims))
+    dv = R.grid_filter(np.ones(dims) * R.dproject(R.grid_filter(x, taps) / hs, beta, 0.5) / hs, taps)
+    pres = np.zeros(dims, bool)
+    pres[0, :, :2] = True
+    void = np.zeros(dims, bool)
+    void[-1, :, -2:] = True
+    w = np.ones(dims)
+    target = 0.45 * x.size
+    xn, lm, n_eval, held = R.oc_loadpath_step(x, dc, dv, 0.2, beta, 0.5, lambda v: R.grid_filter(v, taps), hs, w,
+                                              target, pres, void, lam_last)
+    assert held and n_eval < 40
+    vol = np.sum(np.where(pres, 1.0, np.where(void, 0.0, R.project(R.grid_filter(xn, taps) / hs, beta, 0.5))))
+    assert abs(vol - target) <= 1e-12 * target
+    free = ~pres & ~void
+    assert np.all(np.abs(xn - x)[free] <= 0.2 + 1e-15)
+    assert np.all(xn[pres] == 1.0) and np.all(xn[void] == 0.0)
