@@ -250,6 +250,19 @@ int lpb_graph_free(void* exec);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
 int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 
+/* ---- live-cell reduction (loadpath/simp.py:725 the alive set, :263-289 _connected, :795-826
+ * _solve_mg): state (uint8 cell field) 0 dead, 1 alive, 2 alive and 26-connected to an alive cell
+ * touching a support. flags: bit 0 the cell touches a support, bit 1 an anchor (alive whatever its
+ * density). lpb_live_seed sets alive = xp > alive_thr or anchor and seeds the support cells
+ * (*n_alive: the alive count, device); lpb_live_flood spreads the reached state one pass (the
+ * caller zeroes *changed and repeats while a pass sets it); lpb_live_moduli keeps e on reached
+ * cells only; lpb_dead_loads counts loaded dofs without stiffness (the reference then solves
+ * the full grid). part: 592 doubles. */
+int lpb_live_seed(uint8_t* state, const double* xp, const uint8_t* flags, double alive_thr, double* part, double* n_alive, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_live_flood(uint8_t* state, int* changed, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_live_moduli(double* e_out, const double* e, const uint8_t* state, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_dead_loads(const double* f, const uint8_t* mask, double* part, double* count, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
 /* ---- MMA (loadpath/mma.py:31-214, MMA.update and MMA._subsolv): the n-sized work of one
  * update over n variables and m <= 8 constraints, float64, device arrays; P, Q, df are (m, n)
  * row-major. `part` is scratch of lpb_mma_part_len(m) doubles; each reduction writes its values to

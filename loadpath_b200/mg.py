@@ -1112,6 +1112,30 @@ class GridElasticity:
         except Exception:
             pass
 
+    def set_moduli_live(self, e_dev, live, xp_dev, loads=()):
+        """set_moduli with the live-cell reduction (loadpath/simp.py:795-806): the moduli of the
+        cells `live` (simp.LiveCells) does not keep for the projected densities xp_dev are zeroed;
+        if that leaves a load on a dof without stiffness (loads: float64 device node fields), the
+        full grid is solved instead. Returns True when the reduced grid was kept."""
+        keep = live.keep(xp_dev)
+        if keep is None:
+            self.set_moduli_device(e_dev)
+            return False
+        er = self._tbuf("e_live", e_dev.shape, torch.float64)
+        live.moduli(e_dev, er)
+        self.set_moduli_device(er)
+        L = lib()
+        st = stream_handle()
+        g = self.g0
+        cnt = self._tbuf("dead_cnt", (1,), torch.float64)
+        for f in loads:
+            L.lpb_dead_loads(f.data_ptr(), self.levels[0].mask.data_ptr(), self._part.data_ptr(), cnt.data_ptr(),
+                             *g.args, st)
+            if float(cnt.item()) > 0:
+                self.set_moduli_device(e_dev)
+                return False
+        return True
+
     def check_device(self):
         """Raise if a tiled fine-apply launch flagged a shared-memory wait that gave up."""
         if int(self._err.item()) != 0:

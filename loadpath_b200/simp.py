@@ -23,7 +23,7 @@ from ._lib import lib
 from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
-__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "ProjectedDesign", "Top3dLoop",
+__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "LiveCells", "ProjectedDesign", "Top3dLoop",
            "_project", "_dproject"]
 
 
@@ -103,6 +103,61 @@ def _dproject(xt, beta, eta):
     """its derivative (loadpath/simp.py:1448-1450)."""
     den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
     return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+ALIVE = 1e-3          # cells at or below this projected density leave the solve (loadpath/simp.py:59)
+REDUCE_BELOW = 0.8    # ...once fewer than this share of the cells are alive (loadpath/simp.py:61)
+
+
+class LiveCells:
+    """The solve's live-cell reduction on the device (loadpath/simp.py:725 the alive set, :263-289
+    `_connected`, :795-826 `_solve_mg`): alive = projected density above ALIVE or an anchor cell
+    (touching a support or a load, or preserved); when fewer than REDUCE_BELOW of the cells are
+    alive, the solve keeps the alive cells 26-connected to an alive cell touching a support and
+    the others get modulus 0 on the fixed grid. The components are found by a flood fill from
+    those support cells (lp_live.cu), the union the reference's labelling keeps.
+
+    support_touch, anchor: bool (nx, ny, nz) host arrays in grid order."""
+
+    def __init__(self, grid: DevGrid, support_touch, anchor):
+        self.grid = grid
+        st = np.asarray(support_touch, bool)
+        an = np.asarray(anchor, bool)
+        bits = torch.from_numpy((st.astype(np.uint8) | (an.astype(np.uint8) << 1)))
+        self.flags = grid.set_cells(grid.cell_field(torch.uint8), bits)
+        self.state = grid.cell_field(torch.uint8)
+        self._part = torch.zeros(592, dtype=torch.float64, device=grid.device)
+        self._cnt = torch.zeros(1, dtype=torch.float64, device=grid.device)
+        self._changed = torch.zeros(1, dtype=torch.int32, device=grid.device)
+        self.n_cells = grid.nx * grid.ny * grid.nz
+        self.alive_share = 1.0
+        self.passes = 0
+
+    def keep(self, xp, max_passes=1 << 20):
+        """The kept cells (self.state == 2) for projected densities xp (float64 cell field), or
+        None when REDUCE_BELOW or more of the cells are alive (the reference keeps them all)."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        L.lpb_live_seed(self.state.data_ptr(), xp.data_ptr(), self.flags.data_ptr(), ALIVE, self._part.data_ptr(),
+                        self._cnt.data_ptr(), *g.args, st)
+        self.alive_share = float(self._cnt.item()) / self.n_cells
+        self.passes = 0
+        if self.alive_share >= REDUCE_BELOW:
+            return None
+        while self.passes < max_passes:
+            L.lpb_memset_async(self._changed.data_ptr(), 0, 4, st)
+            for _ in range(4):   # a few passes between reads of the flag
+                L.lpb_live_flood(self.state.data_ptr(), self._changed.data_ptr(), *g.args, st)
+                self.passes += 1
+            if int(self._changed.item()) == 0:
+                return self.state
+        raise RuntimeError("live-cell flood fill did not settle")
+
+    def moduli(self, e, out):
+        """out = e on the kept cells, 0 elsewhere (after keep())."""
+        lib().lpb_live_moduli(out.data_ptr(), e.data_ptr(), self.state.data_ptr(), *self.grid.args, stream_handle())
+        return out
 
 
 VOLUME_RTOL = 1e-13   # the volume multiplier's stopping tolerance (loadpath/simp.py:1234)

@@ -781,6 +781,21 @@ def oc_loadpath_step(x, dc, dv, move, beta, eta, h_apply, hs, w, target, pres=No
     return x_new, lm, n_eval[0], f1 is not None and f2 is not None
 
 
+ALIVE = 1e-3          # loadpath/simp.py:59
+REDUCE_BELOW = 0.8    # loadpath/simp.py:61
+
+
+def connected_keep(alive, support_touch):
+    """The cells the solve keeps (loadpath/simp.py:263-289 `_connected`): alive cells in a
+    26-connected component (scipy.ndimage.label, as the reference) holding an alive cell that
+    touches a support. Grid-order bool arrays."""
+    from scipy import ndimage
+
+    lbl, _ = ndimage.label(alive, structure=np.ones((3, 3, 3), bool))
+    keep_l = np.unique(lbl[alive & support_touch])
+    return alive & np.isin(lbl, keep_l[keep_l > 0])
+
+
 # --------------------------------------------------------------------------
 # assembled direct solve for tiny grids (loadpath/benchmarks/evaluate.py:111-117)
 # --------------------------------------------------------------------------
