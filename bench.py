@@ -504,7 +504,8 @@ def run_micro_band(args):
     lv = ge.levels[-1]
     gr = lv.grid
     w = ge._work
-    t, linv, info, bar, ainv = (w[k] for k in ("band_t", "band_linv", "band_info", "band_bar", "band_ainv"))
+    t, linv, sgn, info, bar, ainv = (w[k] for k in ("band_t", "band_linv", "band_sgn", "band_info", "band_bar",
+                                                    "band_ainv"))
     sfx = "f32" if lv.dtype == torch.float32 else "f64"
 
     def ptr_or_none(a):
@@ -523,10 +524,11 @@ def run_micro_band(args):
                                                  lv.mask.data_ptr(), *gr.args, st)
         L.lpb_memset_async(info.data_ptr(), 0, 8, st)
         ev[1].record()
-        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
+        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), sgn.data_ptr(), info.data_ptr(), bar.data_ptr(),
+                          info[1:].data_ptr(),
                           *gr.args, st)
         ev[2].record()
-        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *gr.args, st)
+        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), sgn.data_ptr(), *gr.args, st)
         ev[3].record()
         torch.cuda.synchronize()
         if r >= 3:

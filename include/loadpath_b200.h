@@ -138,16 +138,18 @@ int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mca
  * the lower band is stored as 32 x 32 tiles, tile (R, d) = rows 32R.., columns 32(R-d)..,
  * row-major at t + (R (D + 1) + d) * 1024, padding dofs past n as identity rows.
  * lpb_band_dims: out = {n, nt, D, bw}, returns the tile count nt (D + 1).
- * lpb_band_factor: in-place tiled Cholesky (one cooperative launch; bounded grid barrier);
- *   linv: nt * 1024 doubles; info: 0 or the 1-based band dof of the first non-positive pivot;
- *   bar: 64 device words of scratch; err: set when a barrier wait gave up.
+ * lpb_band_factor: in-place tiled signed Cholesky A = L S L^T, S = diag(+-1) (a symmetric LU
+ *   without pivoting, as the reference's SuperLU in symmetric mode; one cooperative launch,
+ *   bounded grid barrier); linv: nt * 1024 doubles; sgn: 32 nt doubles, the pivot signs; info: 0
+ *   or the 1-based band dof of the first exactly zero (or non-finite) pivot; bar: 64 device words
+ *   of scratch; err: set when a barrier wait gave up.
  * lpb_band_inverse: ainv (32 nt x 32 nt, row-major, band numbering) = A^-1 from the factor.
  * lpb_band_solve_*: f_out = A^-1 f_in through the band numbering; v: 32 nt doubles scratch. */
 int lpb_coarse_band_f32(double* t, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_coarse_band_f64(double* t, int kind, const double* w, const double* mcat, const int* patch_id, const double* patch_k, const double* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 long long lpb_band_dims(int nx, int ny, int nz, long long* out);
-int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
-int lpb_band_inverse(double* ainv, const double* t, const double* linv, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_factor(double* t, double* linv, double* sgn, int* info, unsigned* bar, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_inverse(double* ainv, const double* t, const double* linv, const double* sgn, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_band_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_band_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
 

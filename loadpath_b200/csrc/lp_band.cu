@@ -1,11 +1,14 @@
 // The coarsest level's direct solve (loadpath/mg.py:708-766: the reference factors D K D + (I - D)
-// with SuperLU on the host). Here the operator is a band (a 27-point block stencil whose nodes
-// are numbered longest axis slowest, half-bandwidth 3 (N1 N2 + N2 + 1) + 2 dofs), so:
-//   1. k_band_factor: Cholesky of the band stored as 32 x 32 tiles (tile (R, d) = rows 32R..,
+// with SuperLU on the host, in symmetric mode without pivoting). Here the operator is a band (a
+// 27-point block stencil whose nodes are numbered longest axis slowest, half-bandwidth
+// 3 (N1 N2 + N2 + 1) + 2 dofs), so:
+//   1. k_band_factor: signed Cholesky A = L S L^T (S = diag(+-1): a symmetric LU without pivoting,
+//      failing only on an exactly zero pivot, as SuperLU does) of the band stored as 32 x 32
+//      tiles (tile (R, d) = rows 32R..,
 //      columns 32(R - d)..), right-looking by tile columns; one cooperative launch whose blocks
 //      meet at a bounded grid barrier twice per tile column. A tile column's diagonal block is
 //      factored (and its lower-triangular inverse formed) by one warp in registers.
-//   2. k_band_inverse: A^-1 = L^-T L^-1 applied to the identity, eight columns per block: a
+//   2. k_band_inverse: A^-1 = L^-T S L^-1 applied to the identity, 32 columns per block: a
 //      forward then a backward block substitution over the band tiles. Only the lower triangle
 //      is needed (rows >= the block's first column); k_sym_lower copies it across.
 //   3. per V-cycle: gather the level's field into the band numbering, one GEMV with the dense
@@ -62,11 +65,14 @@ __device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int
 
 // Tiles another block wrote are read with ld.global.cg (L2, not a possibly stale L1 line).
 
-// Cholesky of one 32 x 32 diagonal tile (lower part read) by warp 0: lane i holds row i in
-// registers. Writes L (upper part zero) over the tile and L^-1 (row-major) to linv. A pivot
-// that is not positive records its dof (1-based) in *info; the arithmetic continues.
-__device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv, long long row0, int* info,
-                            double (*sm)[33]) {
+// Signed Cholesky A = L S L^T (S = diag(+-1)) of one 32 x 32 diagonal tile (lower part read) by
+// warp 0: lane i holds row i in registers. Each pivot p gives L_jj = sqrt|p| and S_j = sign(p),
+// so negative pivots are factored as they are: a symmetric LU without pivoting, as the
+// reference's SuperLU in symmetric mode (loadpath/mg.py:744-747). Writes L (upper part zero) over
+// the tile, L^-1 (row-major) to linv and S to sg[0..31]. A pivot that is exactly zero (or not
+// finite) records its dof (1-based) in *info: the operator is singular; the arithmetic continues.
+__device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv, double* __restrict__ sg,
+                            long long row0, int* info, double (*sm)[33]) {
   if (threadIdx.x < 32) {
     const int i = threadIdx.x;
     double a[32];
@@ -76,15 +82,18 @@ __device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const double p = __shfl_sync(0xffffffffu, a[j], j);
-      if (!(p > 0.0) && bad == 0) bad = (int)(row0 + j + 1);
+      if (!(fabs(p) > 0.0) && bad == 0) bad = (int)(row0 + j + 1);
+      const double sj = p < 0.0 ? -1.0 : 1.0, ap = fabs(p);
+      if (i == j) sg[j] = sj;
       // one reciprocal square root per pivot on the chain (not a square root and a division)
-      const double rd = rsqrt(p), d = p * rd;
-      const double l = i > j ? a[j] * rd : (i == j ? d : 0.0);
+      const double rd = rsqrt(ap), d = ap * rd;
+      const double l = i > j ? a[j] * rd * sj : (i == j ? d : 0.0);
+      const double ls = l * sj;
       a[j] = l;
 #pragma unroll
       for (int t = j + 1; t < 32; ++t) {   // entries above the diagonal of row i take garbage
         const double lt = __shfl_sync(0xffffffffu, l, t);   // here; a[t] is zeroed before use
-        a[t] -= l * lt;                                      // (l = 0 at pivot t > i)
+        a[t] -= ls * lt;                                     // (l = 0 at pivot t > i)
       }
     }
     if (i == 0 && bad) atomicCAS(info, 0, bad);
@@ -113,10 +122,10 @@ __device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv
   }
 }
 
-// a (32 x 32 tile, global, in place) = a * li^T with li lower triangular (the panel solve
-// L_a = A_a L_kk^-T)
-__device__ void panel_tile(double* __restrict__ a, const double* __restrict__ li, double (*sa)[33],
-                           double (*sl)[33]) {
+// a (32 x 32 tile, global, in place) = a * li^T * S with li lower triangular (the panel solve
+// L_a = A_a L_kk^-T S_k)
+__device__ void panel_tile(double* __restrict__ a, const double* __restrict__ li, const double* __restrict__ sg,
+                           double (*sa)[33], double (*sl)[33]) {
   for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
     sa[e >> 5][e & 31] = __ldcg(a + e);
     sl[e >> 5][e & 31] = __ldcg(li + e);
@@ -132,17 +141,17 @@ __device__ void panel_tile(double* __restrict__ a, const double* __restrict__ li
       s2 += sa[r][m + 2] * sl[c][m + 2];
       s3 += sa[r][m + 3] * sl[c][m + 3];
     }
-    a[e] = (s0 + s1) + (s2 + s3);
+    a[e] = ((s0 + s1) + (s2 + s3)) * __ldcg(sg + c);
   }
   __syncthreads();
 }
 
-// x (32 x 32 tile, global, in place) -= la * lc^T
+// x (32 x 32 tile, global, in place) -= la * S * lc^T
 __device__ void update_tile(double* __restrict__ x, const double* __restrict__ la, const double* __restrict__ lc,
-                            double (*sa)[33], double (*sl)[33]) {
+                            const double* __restrict__ sg, double (*sa)[33], double (*sl)[33]) {
   for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
     sa[e >> 5][e & 31] = __ldcg(la + e);
-    sl[e >> 5][e & 31] = __ldcg(lc + e);
+    sl[e >> 5][e & 31] = __ldcg(lc + e) * __ldcg(sg + (e & 31));
   }
   __syncthreads();
   for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
@@ -165,28 +174,32 @@ __device__ void update_tile(double* __restrict__ x, const double* __restrict__ l
 // (k + a, k + c), 1 <= c <= a <= D, numbered u = a (a - 1) / 2 + c - 1, go to block u mod gridDim;
 // block 0 (which owns u = 0, tile (k + 1, k + 1)) then factors that tile. bar: two zeroed words;
 // err: set when a barrier wait gave up.
-__global__ void __launch_bounds__(256, 1) k_band_factor(double* __restrict__ t, double* __restrict__ linv, LpBand bd,
-                                                        int* __restrict__ info, unsigned* __restrict__ bar,
-                                                        int* __restrict__ err) {
+__global__ void __launch_bounds__(256, 1) k_band_factor(double* __restrict__ t, double* __restrict__ linv,
+                                                        double* __restrict__ sg, LpBand bd, int* __restrict__ info,
+                                                        unsigned* __restrict__ bar, int* __restrict__ err) {
   __shared__ double sa[32][33];
   __shared__ double sl[32][33];
   unsigned gen = 0;
   const unsigned nb = gridDim.x;
   const int b = blockIdx.x;
   const int nu = bd.D * (bd.D + 1) / 2;
-  if (b == 0) factor_diag(tile_at(t, bd, 0, 0), linv, 0, info, sa);
+  if (b == 0) factor_diag(tile_at(t, bd, 0, 0), linv, sg, 0, info, sa);
   if (!grid_barrier(bar, nb, gen, err)) return;
   for (int k = 0; k + 1 < bd.nt; ++k) {
     for (int a = 1 + b; a <= bd.D && k + a < bd.nt; a += nb)
-      panel_tile(tile_at(t, bd, k + a, a), linv + (long long)k * 1024, sa, sl);
+      panel_tile(tile_at(t, bd, k + a, a), linv + (long long)k * 1024, sg + 32LL * k, sa, sl);
     if (!grid_barrier(bar, nb, gen, err)) return;
     for (int u = b; u < nu; u += nb) {
       int a = 1;
       while ((a + 1) * a / 2 <= u) ++a;         // u in [a (a - 1) / 2, a (a + 1) / 2)
       const int c = u - a * (a - 1) / 2 + 1;
-      if (k + a < bd.nt) update_tile(tile_at(t, bd, k + a, a - c), tile_at(t, bd, k + a, a), tile_at(t, bd, k + c, c), sa, sl);
+      if (k + a < bd.nt)
+        update_tile(tile_at(t, bd, k + a, a - c), tile_at(t, bd, k + a, a), tile_at(t, bd, k + c, c), sg + 32LL * k,
+                    sa, sl);
     }
-    if (b == 0) factor_diag(tile_at(t, bd, k + 1, 0), linv + (long long)(k + 1) * 1024, 32LL * (k + 1), info, sa);
+    if (b == 0)
+      factor_diag(tile_at(t, bd, k + 1, 0), linv + (long long)(k + 1) * 1024, sg + 32LL * (k + 1), 32LL * (k + 1), info,
+                  sa);
     if (!grid_barrier(bar, nb, gen, err)) return;
   }
 }
@@ -200,19 +213,20 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 }
 
 // Columns j0..j0+31 of A^-1 (rows >= the first column's tile row) into ainv (n_pad x n_pad,
-// row-major): Y = L^-1 E by forward substitution, then X = L^-T Y backwards, one tile row per
+// row-major), A = L S L^T: Y = L^-1 E by forward substitution, then X = L^-T S Y backwards, one tile row per
 // step. A step stages, in chunks of at most `chunk` pairs, its band tiles (8 KB each) with the
 // matching earlier result blocks (read back from ainv through L2) in shared memory; each of 16
 // warps forms one 8 x 8 block of the 32 x 32 result with FP64 MMAs:
 //   forward  S = E - sum_d T_(k,d) Y_(k-d),      Y_k = L_kk^-1 S
-//   backward S = Y_k - sum_d T_(k+d,d)^T X_(k+d), X_k = L_kk^-T S
+//   backward S = S_k Y_k - sum_d T_(k+d,d)^T X_(k+d), X_k = L_kk^-T S   (S_k: the pivot signs)
 // Shared row strides of 36 doubles spread each MMA operand load over all banks.
 constexpr int INV_COLS = 32;
 constexpr int INV_LD = 36;
 constexpr int INV_TILE = 32 * INV_LD;   // doubles per staged 32 x 32 block
 
 __global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ainv, const double* __restrict__ t,
-                                                         const double* __restrict__ linv, LpBand bd, int chunk) {
+                                                         const double* __restrict__ linv, const double* __restrict__ sg,
+                                                         LpBand bd, int chunk) {
   extern __shared__ double sm_inv[];
   double* tiles = sm_inv;                           // chunk band tiles
   double* blks = sm_inv + (long long)chunk * INV_TILE;  // chunk result blocks
@@ -277,8 +291,9 @@ __global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ai
         tmp[orow * INV_LD + ocol + 1] = (gr == j0 + ocol + 1 ? 1.0 : 0.0) - (p1 + r1);
       } else {
         const double2 yk = __ldcg(reinterpret_cast<const double2*>(out));
-        tmp[orow * INV_LD + ocol] = yk.x - (p0 + r0);
-        tmp[orow * INV_LD + ocol + 1] = yk.y - (p1 + r1);
+        const double sr = __ldg(sg + 32LL * k + orow);
+        tmp[orow * INV_LD + ocol] = sr * yk.x - (p0 + r0);
+        tmp[orow * INV_LD + ocol + 1] = sr * yk.y - (p1 + r1);
       }
       __syncthreads();
       double y0 = 0.0, y1 = 0.0;
@@ -379,13 +394,14 @@ long long lpb_band_dims(int nx, int ny, int nz, long long* out) {
   return (long long)bd.nt * (bd.D + 1);
 }
 
-// Cholesky of the band in t (from lpb_coarse_band_*), in place; linv: nt x 1024 doubles (the
-// inverses of the diagonal factor tiles); info: one device int, 0 or the first dof (1-based)
-// whose pivot was not positive; bar: 64 device words of scratch; err: one device int, set when
+// Signed Cholesky of the band in t (from lpb_coarse_band_*), in place; linv: nt x 1024 doubles
+// (the inverses of the diagonal factor tiles); sgn: 32 nt doubles, the pivot signs; info: one
+// device int, 0 or the first dof (1-based) whose pivot was exactly zero (or not finite); bar: 64 device words of scratch; err: one device int, set when
 // a barrier wait gave up. One cooperative launch of max(D, D (D + 1) / 2) blocks.
-int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err, LP_GRID_ARGS, void* stream) {
+int lpb_band_factor(double* t, double* linv, double* sgn, int* info, unsigned* bar, int* err, LP_GRID_ARGS,
+                    void* stream) {
   LpGrid g = LP_GRID;
-  if (!lp_grid_ok(g) || !t || !linv || !info || !bar || !err) return LP_ERR_ARG;
+  if (!lp_grid_ok(g) || !t || !linv || !sgn || !info || !bar || !err) return LP_ERR_ARG;
   LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
   int dev = 0, nsm = 0, per_sm = 0, coop = 0;
   cudaGetDevice(&dev);
@@ -400,7 +416,7 @@ int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err,
   if (!coop || nblocks < 1) return LP_ERR_SIZE;
   if (cudaMemsetAsync(bar, 0, 64 * sizeof(unsigned), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
   if (cudaMemsetAsync(info, 0, sizeof(int), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
-  void* args[] = {&t, &linv, &bd, &info, &bar, &err};
+  void* args[] = {&t, &linv, &sgn, &bd, &info, &bar, &err};
   if (cudaLaunchCooperativeKernel((const void*)k_band_factor, dim3((unsigned)nblocks), dim3(256), args, 0, LP_ST) !=
       cudaSuccess)
     return LP_ERR_LAUNCH;
@@ -409,9 +425,10 @@ int lpb_band_factor(double* t, double* linv, int* info, unsigned* bar, int* err,
 }
 
 // ainv (32 nt x 32 nt doubles, row-major, band numbering) = A^-1 from the factor
-int lpb_band_inverse(double* ainv, const double* t, const double* linv, LP_GRID_ARGS, void* stream) {
+int lpb_band_inverse(double* ainv, const double* t, const double* linv, const double* sgn, LP_GRID_ARGS,
+                     void* stream) {
   LpGrid g = LP_GRID;
-  if (!lp_grid_ok(g) || !ainv || !t || !linv) return LP_ERR_ARG;
+  if (!lp_grid_ok(g) || !ainv || !t || !linv || !sgn) return LP_ERR_ARG;
   const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
   const long long np = 32LL * bd.nt;
   // as many (tile, block) pairs per chunk as fit in 227 KB next to the diagonal inverse and S
@@ -421,7 +438,7 @@ int lpb_band_inverse(double* ainv, const double* t, const double* linv, LP_GRID_
   const long long smem = (2LL * chunk + 2) * INV_TILE * sizeof(double);
   if (cudaFuncSetAttribute(k_band_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return LP_ERR_SIZE;
-  k_band_inverse<<<(unsigned)(np / INV_COLS), 512, (size_t)smem, LP_ST>>>(ainv, t, linv, bd, chunk);
+  k_band_inverse<<<(unsigned)(np / INV_COLS), 512, (size_t)smem, LP_ST>>>(ainv, t, linv, sgn, bd, chunk);
   k_sym_lower<<<dim3(bd.nt, bd.nt), 256, 0, LP_ST>>>(ainv, np);
   LP_LAUNCH_CHECK();
   return LP_OK;

@@ -651,6 +651,7 @@ class GridElasticity:
         info = self._tbuf("band_info", (2,), torch.int32)
         bar = self._tbuf("band_bar", (64,), torch.int32)
         ainv = self._tbuf("band_ainv", (npad, npad), torch.float64)
+        sgn = self._tbuf("band_sgn", (npad,), torch.float64)
         self._coarse = {"ainv": ainv, "v": self._tbuf("coarse_v", (npad,), torch.float64), "n": n}
         # The factorisation and the inverse are latency-bound chains on a fraction of the SMs;
         # they run on a high-priority side stream, overlapped with the power iterations the
@@ -660,9 +661,9 @@ class GridElasticity:
         self._side.wait_event(self._ev_fork)
         ss = self._side.cuda_stream
         L.lpb_memset_async(info.data_ptr(), 0, 8, ss)
-        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), info.data_ptr(), bar.data_ptr(), info[1:].data_ptr(),
-                          *g.args, ss)
-        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), *g.args, ss)
+        L.lpb_band_factor(t.data_ptr(), linv.data_ptr(), sgn.data_ptr(), info.data_ptr(), bar.data_ptr(),
+                          info[1:].data_ptr(), *g.args, ss)
+        L.lpb_band_inverse(ainv.data_ptr(), t.data_ptr(), linv.data_ptr(), sgn.data_ptr(), *g.args, ss)
         self._ev_join.record(self._side)
         self._joined = False
         return info

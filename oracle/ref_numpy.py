@@ -358,7 +358,7 @@ class Hierarchy:
             fine = coarse
         try:
             self.build_coarse(self.levels[-1])
-        except np.linalg.LinAlgError:
+        except RuntimeError:                     # "Factor is exactly singular"
             if self.strict:
                 raise
             self.strict = True
@@ -433,9 +433,10 @@ class Hierarchy:
 
     def build_coarse(self, lv):
         """Assemble the coarsest level over the dofs of its active cells, as
-        D K D + (I - D), symmetrised, and factor it (loadpath/mg.py:708-754).
-        The reference factors with SuperLU in SPD mode; the same operator is
-        factored here by a dense Cholesky (an exact solve of the same system)."""
+        D K D + (I - D), symmetrised, and factor it (loadpath/mg.py:708-754)
+        with the reference's own call: SuperLU in symmetric mode without pivoting
+        (scipy.sparse.linalg.splu, MMD_AT_PLUS_A, diag_pivot_thresh 0), which raises
+        RuntimeError on an exactly singular factor."""
         if lv is self.levels[0]:
             self.coarse = None
             return
@@ -466,16 +467,19 @@ class Hierarchy:
         m = lv.mask.reshape(-1)[gdof].astype(np.float64)
         kd = m[:, None] * kd * m[None, :] + np.diag(1.0 - m)
         kd = 0.5 * (kd + kd.T)
-        chol = np.linalg.cholesky(kd)
-        self.coarse = {"gdof": gdof, "chol": chol, "n": n}
+        import scipy.sparse as sp
+        from scipy.sparse.linalg import splu
+
+        lu = splu(sp.csc_matrix(kd), permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0,
+                  options={"SymmetricMode": True})
+        self.coarse = {"gdof": gdof, "lu": lu, "n": n}
 
     def coarse_solve(self, b):
         """(loadpath/mg.py:756-766)"""
         c = self.coarse
         flat = b.reshape(-1)
         rhs = flat[c["gdof"]].astype(np.float64)
-        y = np.linalg.solve(c["chol"], rhs)
-        x = np.linalg.solve(c["chol"].T, y)
+        x = c["lu"].solve(rhs)
         out = np.zeros_like(flat)
         out[c["gdof"]] = x
         return out.reshape(b.shape)
