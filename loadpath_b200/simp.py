@@ -23,7 +23,8 @@ from ._lib import lib
 from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
-__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "LiveCells", "ProjectedDesign", "Top3dLoop",
+__all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "case_compliance", "adjoint_sensitivity",
+           "LiveCells", "ProjectedDesign", "Top3dLoop",
            "_project", "_dproject"]
 
 
@@ -103,6 +104,36 @@ def _dproject(xt, beta, eta):
     """its derivative (loadpath/simp.py:1448-1450)."""
     den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
     return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+def case_compliance(f, u, part=None):
+    """f . u on float64 device node fields: a load case's compliance, the single-direction case of
+    loadpath/directions.py:167-180 (`collapse`, whose energy terms are then [(1.0, u)])."""
+    L = lib()
+    g_n = f.numel()
+    part = part if part is not None else torch.zeros(2048, dtype=torch.float64, device=f.device)
+    out = torch.zeros(1, dtype=torch.float64, device=f.device)
+    L.lpb_dot_f64(f.data_ptr(), u.data_ptr(), g_n, part.data_ptr(), out.data_ptr(), stream_handle())
+    return float(out.item())
+
+
+def adjoint_sensitivity(ge, pairs, xp, dproj, out, modulus=1.0, penal=3.0, emin=1e-9):
+    """The compliant-mechanism output's sensitivity (loadpath/mechanism.py:156-165):
+    out = -sum over (u, lam) pairs of lam_e . k_e u_e, times modulus p (1 - emin) xp^(p - 1) and
+    dproj, with K lam = l the adjoint solve of the output functional l (ge.solve_device(l)).
+    pairs: [(u, lam)] float64 device node fields; xp, dproj, out: float64 cell fields of ge's fine
+    grid."""
+    L = lib()
+    g = ge.g0
+    st = stream_handle()
+    ce = ge._tbuf("adj_ce", out.shape, torch.float64)
+    part = ge._tbuf("adj_part", (4096,), torch.float64)
+    for k, (u, lam) in enumerate(pairs):
+        ge.strain_energy_device(lam, u, out=ce)
+        L.lpb_sensitivity(out.data_ptr(), xp.data_ptr(), ce.data_ptr(), None, float(penal), float(emin),
+                          float(modulus), int(k > 0), part.data_ptr(), None, *g.args, st)
+    L.lpb_cell_product(out.data_ptr(), out.data_ptr(), dproj.data_ptr(), None, 0, *g.args, st)
+    return out
 
 
 ALIVE = 1e-3          # cells at or below this projected density leave the solve (loadpath/simp.py:59)
