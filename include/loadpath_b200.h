@@ -252,6 +252,16 @@ int lpb_graph_free(void* exec);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
 int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 
+/* ---- the float32-only solve's pieces (loadpath/gpu.py:119-149 _two_sum/_rigid_free, :233-258
+ * apply_rf, :429-481 solve_fp32). lpb_apply_rf_f32: out = m K (h + l) + (1 - m) h on the fine
+ * level (float32 moduli e, float32 ke 24 x 24 on the device), each cell's matrix applied to its
+ * corner displacements less the corner-0 translation and the mean rotation, formed in pair
+ * (error-free) arithmetic; l may be NULL; ft: scratch of 24 * cells floats.
+ * lpb_pair_residual_f32: r = (bh - ax) + bl. lpb_pair_add_f32: (xh, xl) += d in pair arithmetic. */
+int lpb_apply_rf_f32(float* out, const float* h, const float* l, const uint8_t* mask, const float* e, const float* ke, float* ft, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_pair_residual_f32(float* r, const float* bh, const float* ax, const float* bl, long long n, void* stream);
+int lpb_pair_add_f32(float* xh, float* xl, const float* d, long long n, void* stream);
+
 /* ---- live-cell reduction (loadpath/simp.py:725 the alive set, :263-289 _connected, :795-826
  * _solve_mg): state (uint8 cell field) 0 dead, 1 alive, 2 alive and 26-connected to an alive cell
  * touching a support. flags: bit 0 the cell touches a support, bit 1 an anchor (alive whatever its

@@ -1113,6 +1113,133 @@ class GridElasticity:
         except Exception:
             pass
 
+    # --- float32-only solve (loadpath/gpu.py:399-481, TorchMG._pcg32 / solve_fp32) -------------
+    def apply_rf(self, out, h, l=None):
+        """out = m K (h + l) + (1 - m) h on the fine level in float32, each cell's matrix applied to
+        its rigid-motion-free deformation formed in pair arithmetic (loadpath/gpu.py:119-149,
+        :233-258); h, l, out: float32 device node fields (l None: h alone)."""
+        lv = self._l0s
+        g = self.g0
+        if lv.dtype != torch.float32:
+            raise ValueError("apply_rf needs the float32 fine level (dtype=np.float32)")
+        ft = self._tbuf("rf_ft", (24, g.n_cell_field), torch.float32)
+        lib().lpb_apply_rf_f32(out.data_ptr(), h.data_ptr(), ptr(l), lv.mask.data_ptr(), lv.e.data_ptr(),
+                               self.ke32.data_ptr(), ft.data_ptr(), *g.args, stream_handle())
+        return out
+
+    def _dot32(self, a, b):
+        out = self._tbuf("dot32", (1,), torch.float64)
+        lib().lpb_dot_f32(a.data_ptr(), b.data_ptr(), a.numel(), self._part.data_ptr(), out.data_ptr(),
+                          stream_handle())
+        return float(out.item())
+
+    def _pcg32(self, r, tol, maxiter):
+        """Plain float32 PCG on the fine level's rigid-free operator for a correction K d = r to
+        tol relative (loadpath/gpu.py:399-427). Returns (d, iterations); r is not changed."""
+        L = lib()
+        st = stream_handle()
+        g = self.g0
+        n = g.n_node_field
+        f32 = torch.float32
+        d = self._buf("rf_d", g, f32)
+        d.zero_()
+        rnorm = self._dot32(r, r) ** 0.5
+        if rnorm == 0:
+            return d, 0
+        rr = self._buf("rf_r", g, f32)
+        rr.copy_(r)
+        p = self._buf("rf_p", g, f32)
+        ap = self._buf("rf_ap", g, f32)
+        z = self._vcycle(0, rr)
+        p.copy_(z)
+        rz = self._dot32(rr, z)
+        for it in range(1, maxiter + 1):
+            self.apply_rf(ap, p)
+            pap = self._dot32(p, ap)
+            if pap <= 0:
+                return d, it
+            alpha = rz / pap
+            L.lpb_axpby_f32(d.data_ptr(), 1.0, d.data_ptr(), alpha, p.data_ptr(), n, st)
+            L.lpb_axpby_f32(rr.data_ptr(), 1.0, rr.data_ptr(), -alpha, ap.data_ptr(), n, st)
+            if self._dot32(rr, rr) ** 0.5 <= tol * rnorm:
+                return d, it
+            z = self._vcycle(0, rr)
+            rz_new = self._dot32(rr, z)
+            L.lpb_axpby_f32(p.data_ptr(), rz_new / rz, p.data_ptr(), 1.0, z.data_ptr(), n, st)
+            rz = rz_new
+        return d, maxiter
+
+    def solve_fp32_device(self, b, x0=None, inner_rtol=3e-3, inner_max=50, outer_max=40):
+        """The float32-only solve (loadpath/gpu.py:429-481): iterative refinement on the pair
+        x = hi + lo. Each outer step forms the residual with the rigid-free operator from the pair,
+        solves the correction with float32 PCG to inner_rtol and adds it in pair arithmetic;
+        converged when the correction's energy |d . r| is under rtol^2 of x . b. b, x0: float64
+        device node fields (b masked by the caller). Returns (x float64 device field, V-cycles,
+        converged). For devices without fast float64; the mixed solve is the default."""
+        L = lib()
+        st = stream_handle()
+        g = self.g0
+        n = g.n_node_field
+        f32, f64 = torch.float32, torch.float64
+        out = g.node_field(f64)
+        if float(torch.count_nonzero(b)) == 0:
+            return out, 0, True
+        bh, bl = self._buf("rf_bh", g, f32), self._buf("rf_bl", g, f32)
+        t64 = self._buf("rf_t64", g, f64)
+        L.lpb_cast_f64_f32(bh.data_ptr(), b.data_ptr(), n, st)
+        L.lpb_cast_f32_f64(t64.data_ptr(), bh.data_ptr(), n, st)
+        L.lpb_axpby_f64(t64.data_ptr(), 1.0, b.data_ptr(), -1.0, t64.data_ptr(), n, st)
+        L.lpb_cast_f64_f32(bl.data_ptr(), t64.data_ptr(), n, st)
+        xh, xl = self._buf("rf_xh", g, f32), self._buf("rf_xl", g, f32)
+        xh.zero_()
+        xl.zero_()
+        ax, r = self._buf("rf_ax", g, f32), self._buf("rf_res", g, f32)
+
+        def split(x64):   # float64 field -> (hi, lo) float32 pair in xh, xl
+            L.lpb_cast_f64_f32(xh.data_ptr(), x64.data_ptr(), n, st)
+            L.lpb_cast_f32_f64(t64.data_ptr(), xh.data_ptr(), n, st)
+            L.lpb_axpby_f64(t64.data_ptr(), 1.0, x64.data_ptr(), -1.0, t64.data_ptr(), n, st)
+            L.lpb_cast_f64_f32(xl.data_ptr(), t64.data_ptr(), n, st)
+
+        if x0 is not None and float(torch.count_nonzero(x0)) > 0:
+            # the energy-optimal multiple of x0, or zero if even that is worse
+            split(x0)
+            self.apply_rf(ax, xh, xl)
+            xax = self._dot32(xh, ax) + self._dot32(xl, ax)
+            sc = (self._dot32(bh, xh) + self._dot32(bh, xl)) / xax if xax > 0 else 0.0
+            keep = False
+            if sc > 0:
+                L.lpb_axpby_f32(r.data_ptr(), 1.0, bh.data_ptr(), -sc, ax.data_ptr(), n, st)
+                keep = self._dot32(r, r) < self._dot32(bh, bh)
+            if keep:
+                xs = self._buf("rf_xs", g, f64)
+                L.lpb_axpby_f64(xs.data_ptr(), sc, x0.data_ptr(), 0.0, x0.data_ptr(), n, st)
+                split(xs)
+            else:
+                xh.zero_()
+                xl.zero_()
+        tol2 = self.rtol ** 2
+        total = 0
+        ok = False
+        for _ in range(outer_max):
+            self.apply_rf(ax, xh, xl)
+            L.lpb_pair_residual_f32(r.data_ptr(), bh.data_ptr(), ax.data_ptr(), bl.data_ptr(), n, st)
+            d, it = self._pcg32(r, inner_rtol, inner_max)
+            total += it
+            L.lpb_pair_add_f32(xh.data_ptr(), xl.data_ptr(), d.data_ptr(), n, st)
+            de = abs(self._dot32(d, r))
+            xe = self._dot32(xh, bh)
+            if xe <= 0 or not np.isfinite(de):
+                break
+            if de <= tol2 * xe:
+                ok = True
+                break
+        L.lpb_cast_f32_f64(out.data_ptr(), xh.data_ptr(), n, st)
+        L.lpb_cast_f32_f64(t64.data_ptr(), xl.data_ptr(), n, st)
+        L.lpb_axpby_f64(out.data_ptr(), 1.0, out.data_ptr(), 1.0, t64.data_ptr(), n, st)
+        self.last_iters = total
+        return out, total, ok
+
     def set_moduli_live(self, e_dev, live, xp_dev, loads=()):
         """set_moduli with the live-cell reduction (loadpath/simp.py:795-806): the moduli of the
         cells `live` (simp.LiveCells) does not keep for the projected densities xp_dev are zeroed;
