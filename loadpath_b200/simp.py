@@ -24,6 +24,7 @@ from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
 __all__ = ["filter_taps", "DeviceFilter", "density_filter", "oc_bisection", "case_compliance", "adjoint_sensitivity",
+           "LoadCaseShards",
            "LiveCells", "ProjectedDesign", "Top3dLoop",
            "_project", "_dproject"]
 
@@ -104,6 +105,38 @@ def _dproject(xt, beta, eta):
     """its derivative (loadpath/simp.py:1448-1450)."""
     den = np.tanh(beta * eta) + np.tanh(beta * (1 - eta))
     return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den
+
+
+class LoadCaseShards:
+    """Load cases split over the ranks of a torch.distributed group (one process per GPU): rank r
+    solves cases r, r + world, ...; after each rank has summed its cases' compliance and
+    sensitivity, one all-reduce (sum) gives every rank the totals, and every rank then takes the
+    same design step, so the designs stay identical without being sent. The only exchange per
+    SIMP iteration is that one reduction of a cell field plus one scalar (NCCL on CUDA tensors,
+    gloo on CPU tensors)."""
+
+    def __init__(self, n_cases, group=None):
+        import torch.distributed as dist
+
+        self.n_cases = int(n_cases)
+        self.group = group
+        self.dist = dist if dist.is_available() and dist.is_initialized() else None
+        self.rank = self.dist.get_rank(group) if self.dist else 0
+        self.world = self.dist.get_world_size(group) if self.dist else 1
+
+    def mine(self):
+        """This rank's case indices."""
+        return list(range(self.rank, self.n_cases, self.world))
+
+    def reduce(self, dc, comp):
+        """dc (a cell field, summed in place over the ranks) and comp (this rank's compliance
+        sum) -> the total compliance."""
+        if self.dist is None or self.world == 1:
+            return float(comp)
+        c = torch.tensor([float(comp)], dtype=dc.dtype, device=dc.device)
+        self.dist.all_reduce(dc, group=self.group)
+        self.dist.all_reduce(c, group=self.group)
+        return float(c.item())
 
 
 def case_compliance(f, u, part=None):
