@@ -72,6 +72,15 @@ int lpb_walsh_chunks_f32(float* wc, const float* w, int nx, int ny, int nz, int 
 int lpb_walsh_chunks_f64(double* wc, const double* w, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_weights_tma_f32(float* out, const float* u, const float* wc, const int* patch_id, const float* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_weights_tma_f64(double* out, const double* u, const double* wc, const int* patch_id, const double* patch_k, const uint8_t* mask, const double* g1, const int* pbox, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* explicit levels in the cell's corner-parity basis: K^ = T K T^T / 64 has the level-1 pattern
+ * (150 upper entries) at every level of the plain hierarchy; lpb_pack_modal_f32 stores them
+ * (km: (150, cells)) and lists the cells with off-pattern weight (children with masked patch
+ * matrices; glist: up to `cells` ints, *gcount device int) with their 300 node-basis entries
+ * (kpc: up to 300 * cells floats, cell-major by list slot); lpb_apply_explicit_modal_f32 applies
+ * f = T^T K^ T u on the others and the node-basis entries on the listed ones (half the bytes of
+ * lpb_apply_explicit_sym_f32). Same operator as loadpath/mgops.py:131-146 + 181-217. */
+int lpb_pack_modal_f32(float* km, int* glist, int* gcount, float* kpc, const float* k, long long ncells, double tol, void* stream);
+int lpb_apply_explicit_modal_f32(float* out, const float* u, const float* km, const float* kpc, const int* glist, const int* gcount, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* lpb_apply_explicit_sym_f32 for callers that cannot allocate device memory (a host that owns

@@ -736,6 +736,196 @@ k_explicit_cells(T* __restrict__ ft, const T* __restrict__ u, const T* __restric
   for (int r = 0; r < 24; ++r) ft[(long long)r * ncp + c] = f[r];
 }
 
+// ---- explicit levels in the corner-parity basis ------------------------------------------------
+// A Galerkin level's cell matrix K, in the modes of its cell (K^ = T K T^T / 64, T = kron(H, I3)),
+// has the level-1 pattern: 279 non-zeros, 150 in the upper triangle, at every level of the plain
+// hierarchy (the pattern is kept by the child Galerkin product). Those cells are stored as the
+// 150 entries (entry-major, (150, cells)) and applied as f = T^T (K^ (T u)): half the bytes of the
+// 300-entry node-basis form. Cells with weight off the pattern (children carrying masked patch
+// matrices) are listed and applied from the node-basis form.
+constexpr int MODAL_UP = 150;
+__constant__ int c_mup_r[MODAL_UP] = {3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 4, 4, 4, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 5, 5, 5, 6, 6, 6, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 8, 8, 8, 8, 8, 8, 8, 8, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 12, 12, 12, 12, 12, 12, 13, 13, 13, 13, 13, 13, 14, 14, 14, 14, 14, 14, 14, 14, 15, 15, 15, 15, 15, 15, 15, 15, 16, 16, 16, 16, 16, 16, 16, 17, 17, 17, 17, 17, 17, 17, 18, 18, 18, 18, 19, 19, 19, 19, 19, 20, 20, 20, 20, 21, 21, 21, 22, 22, 23};
+__constant__ int c_mup_c[MODAL_UP] = {3, 7, 9, 10, 14, 15, 17, 19, 20, 21, 22, 23, 4, 6, 9, 10, 16, 18, 21, 22, 5, 11, 12, 15, 17, 18, 21, 23, 6, 9, 10, 16, 18, 21, 22, 7, 9, 10, 14, 15, 17, 19, 20, 21, 22, 23, 8, 11, 13, 16, 19, 20, 22, 23, 9, 10, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 10, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 11, 12, 13, 15, 16, 17, 18, 19, 20, 21, 22, 23, 12, 15, 17, 18, 21, 23, 13, 16, 19, 20, 22, 23, 14, 15, 17, 19, 20, 21, 22, 23, 15, 17, 18, 19, 20, 21, 22, 23, 16, 18, 19, 20, 21, 22, 23, 17, 18, 19, 20, 21, 22, 23, 18, 21, 22, 23, 19, 20, 21, 22, 23, 20, 21, 22, 23, 21, 22, 23, 22, 23, 23};
+// bit i % 32 of word i / 32: entry i = 24 r + c of K^ is on the pattern
+__constant__ unsigned c_mpat[18] = {0x00000000u, 0x00000000u, 0xfac68800u, 0x20650650u, 0x0650a698u, 0xfac68865u, 0xd8d92900u, 0xc6d8ffc6u, 0xffb920ffu, 0x00a69820u, 0xc688d929u, 0xfedea8fau, 0xa8fd2f50u, 0x9e70fedeu, 0xfbef88e7u, 0xf8fbef88u, 0xefd8ffdeu, 0xffffa8ffu};
+#define MUP_ROWS {3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 3, 4, 4, 4, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 5, 5, 5, 6, 6, 6, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 8, 8, 8, 8, 8, 8, 8, 8, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 12, 12, 12, 12, 12, 12, 13, 13, 13, 13, 13, 13, 14, 14, 14, 14, 14, 14, 14, 14, 15, 15, 15, 15, 15, 15, 15, 15, 16, 16, 16, 16, 16, 16, 16, 17, 17, 17, 17, 17, 17, 17, 18, 18, 18, 18, 19, 19, 19, 19, 19, 20, 20, 20, 20, 21, 21, 21, 22, 22, 23}
+#define MUP_COLS {3, 7, 9, 10, 14, 15, 17, 19, 20, 21, 22, 23, 4, 6, 9, 10, 16, 18, 21, 22, 5, 11, 12, 15, 17, 18, 21, 23, 6, 9, 10, 16, 18, 21, 22, 7, 9, 10, 14, 15, 17, 19, 20, 21, 22, 23, 8, 11, 13, 16, 19, 20, 22, 23, 9, 10, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 10, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 11, 12, 13, 15, 16, 17, 18, 19, 20, 21, 22, 23, 12, 15, 17, 18, 21, 23, 13, 16, 19, 20, 22, 23, 14, 15, 17, 19, 20, 21, 22, 23, 15, 17, 18, 19, 20, 21, 22, 23, 16, 18, 19, 20, 21, 22, 23, 17, 18, 19, 20, 21, 22, 23, 18, 21, 22, 23, 19, 20, 21, 22, 23, 20, 21, 22, 23, 21, 22, 23, 22, 23, 23}
+
+__device__ __forceinline__ float walsh_h(int m, int k) {
+  float v = 1.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    if ((m >> a) & 1) v *= ((k >> a) & 1) ? 1.0f : -1.0f;
+  return v;
+}
+
+// one warp per cell: K^ of the cell's (24 x 24) matrix in float64, its symmetric part on the
+// pattern into km; a cell with off-pattern weight above tol of its largest entry is listed
+template <typename Ti>
+__global__ void __launch_bounds__(128) k_pack_modal(float* __restrict__ km, int* __restrict__ glist,
+                                                    int* __restrict__ gcount, float* __restrict__ kpc,
+                                                    const Ti* __restrict__ k, long long ncp, double tol) {
+  __shared__ double sk[4][576];
+  __shared__ double sa[4][576];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* K = sk[w];
+  double* A = sa[w];
+  for (long long cell = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; cell < ncp;
+       cell += (long long)gridDim.x * (blockDim.x >> 5)) {
+    for (int i = lane; i < 576; i += 32) K[i] = (double)k[cell * 576 + i];
+    __syncwarp();
+    // A = T K
+    for (int i = lane; i < 576; i += 32) {
+      const int r = i / 24, c = i % 24, mr = r / 3, cr = r % 3;
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s += (double)walsh_h(mr, q) * K[(3 * q + cr) * 24 + c];
+      A[i] = s;
+    }
+    __syncwarp();
+    // K^ = A T^T / 64 into K (reused)
+    double amax = 0.0, off = 0.0;
+    for (int i = lane; i < 576; i += 32) {
+      const int r = i / 24, c = i % 24, mc = c / 3, cc = c % 3;
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s += A[r * 24 + 3 * q + cc] * (double)walsh_h(mc, q);
+      s /= 64.0;
+      K[i] = s;
+      amax = fmax(amax, fabs(s));
+    }
+    __syncwarp();
+    for (int i = lane; i < 576; i += 32)
+      if (!((c_mpat[i >> 5] >> (i & 31)) & 1u)) off = fmax(off, fabs(K[i]));
+    for (int o = 16; o > 0; o >>= 1) {
+      amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      off = fmax(off, __shfl_xor_sync(0xffffffffu, off, o));
+    }
+    const bool general = off > tol * amax;
+    for (int p = lane; p < MODAL_UP; p += 32) {
+      const int r = c_mup_r[p], c = c_mup_c[p];
+      km[(long long)p * ncp + cell] = general ? 0.0f : (float)(0.5 * (K[r * 24 + c] + K[c * 24 + r]));
+    }
+    if (general) {   // listed: the node-basis symmetric part, cell-major, at the cell's slot
+      int slot = 0;
+      if (lane == 0) slot = atomicAdd(gcount, 1);
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if (lane == 0) glist[slot] = (int)cell;
+      for (int p = lane; p < 300; p += 32) {
+        int a = 0, rem = p;
+        while (rem >= 24 - a) { rem -= 24 - a; ++a; }
+        const int b2 = a + rem;
+        kpc[(long long)slot * 300 + p] =
+            (float)(0.5 * ((double)k[cell * 576 + a * 24 + b2] + (double)k[cell * 576 + b2 * 24 + a]));
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// in-place a[k] <- sum_m H[m][k] a[m] (the transpose of lp's Walsh transform H a)
+__device__ __forceinline__ void walsh8t(float (&a)[8]) {
+#pragma unroll
+  for (int b = 1; b < 8; b <<= 1)
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (!(k & b)) {
+        const float lo = a[k], hi = a[k | b];
+        a[k] = lo - hi;
+        a[k | b] = lo + hi;
+      }
+}
+
+__device__ __forceinline__ void walsh8(float (&a)[8]) {
+#pragma unroll
+  for (int b = 1; b < 8; b <<= 1)
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (!(k & b)) {
+        const float lo = a[k], hi = a[k | b];
+        a[k] = lo + hi;
+        a[k | b] = hi - lo;
+      }
+}
+
+// ft (24, cells) = T^T (K^ (T u_c)) for every cell (listed cells are rewritten afterwards)
+__global__ void __launch_bounds__(128, 4) k_modal_cells(float* __restrict__ ft, const float* __restrict__ u,
+                                                       const float* __restrict__ km, LpGrid g) {
+  const long long ncp = g.cells_padded();
+  const long long cs = g.comp_stride();
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= ncp) return;
+  int x, y, z;
+  if (!g.cell_at(t, x, y, z)) return;
+  const long long n0 = g.node(x, y, z);
+  const long long oy = 4LL * g.NX(), oz = (z & 3) == 3 ? g.node_zc_stride() - 3 : 1;
+  constexpr int MUP_R[MODAL_UP] = MUP_ROWS;
+  constexpr int MUP_C[MODAL_UP] = MUP_COLS;
+  float uh[24], fh[24];
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    float a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      a[q] = u[cc * cs + n0 + (q & 1 ? 4 : 0) + (q & 2 ? oy : 0) + (q & 4 ? oz : 0)];
+    walsh8(a);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) uh[3 * m + cc] = a[m];
+  }
+#pragma unroll
+  for (int r = 0; r < 24; ++r) fh[r] = 0.0f;
+  const float* kc = km + t;
+#pragma unroll
+  for (int p = 0; p < MODAL_UP; ++p) {
+    const float v = __ldg(kc + (long long)p * ncp);
+    fh[MUP_R[p]] += v * uh[MUP_C[p]];
+    if (MUP_R[p] != MUP_C[p]) fh[MUP_C[p]] += v * uh[MUP_R[p]];
+  }
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    float a[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) a[m] = fh[3 * m + cc];
+    walsh8t(a);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) ft[(long long)(3 * q + cc) * ncp + t] = a[q];
+  }
+}
+
+// the listed cells from their node-basis entries (kpc: 300 per listed cell, cell-major): one warp
+// per cell, its 300 entries and 24 corner values staged in shared memory, lane r < 24 forms row r
+__global__ void __launch_bounds__(128) k_listed_cells(float* __restrict__ ft, const float* __restrict__ u,
+                                                      const float* __restrict__ kpc, const int* __restrict__ glist,
+                                                      const int* __restrict__ gcount, LpGrid g) {
+  __shared__ float sk[4][300];
+  __shared__ float su[4][24];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long ncp = g.cells_padded();
+  const long long cs = g.comp_stride();
+  const int cnt = *gcount;
+  for (int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; slot < cnt; slot += (gridDim.x * blockDim.x) >> 5) {
+    const long long c = glist[slot];
+    int x, y, z;
+    g.cell_at(c, x, y, z);
+    for (int p = lane; p < 300; p += 32) sk[w][p] = __ldg(kpc + (long long)slot * 300 + p);
+    if (lane < 24) {
+      const int q = lane / 3, cc = lane % 3;
+      su[w][lane] = u[cc * cs + g.node(x + cx_(q), y + cy_(q), z + cz_(q))];
+    }
+    __syncwarp();
+    if (lane < 24) {
+      float f = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 24; ++b) {
+        const int lo = lane < b ? lane : b, hi = lane < b ? b : lane;
+        f += sk[w][sym_index(lo, hi)] * su[w][b];
+      }
+      ft[(long long)lane * ncp + c] = f;
+    }
+    __syncwarp();
+  }
+}
+
 template <typename T>
 __global__ void k_explicit_gather(T* __restrict__ out, const T* __restrict__ ft, const uint8_t* __restrict__ mask,
                                   LpGrid g) {
@@ -987,6 +1177,34 @@ int lpb_apply_explicit_sym_noalloc_f32(float* out, const float* u, const float* 
   float* ft = explicit_scratch_address();
   if (!ft) return LP_ERR_LAUNCH;
   return launch_explicit<float>(out, u, kp, ft, mask, g, LP_ST);
+}
+
+// km (150, ncells) = the pattern entries of each cell's K^ = T K T^T / 64 (symmetric part); cells
+// with off-pattern weight above tol of their largest entry get zeros and are listed in glist
+// (*gcount of them), their 300 node-basis symmetric entries in kpc at their list slot (glist and
+// kpc hold up to ncells cells)
+int lpb_pack_modal_f32(float* km, int* glist, int* gcount, float* kpc, const float* k, long long ncells, double tol,
+                       void* stream) {
+  if (!km || !glist || !gcount || !kpc || !k || ncells < 1) return LP_ERR_ARG;
+  if (cudaMemsetAsync(gcount, 0, sizeof(int), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
+  const long long blocks = (ncells + 3) / 4;
+  k_pack_modal<float><<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 128, 0, LP_ST>>>(km, glist, gcount, kpc,
+                                                                                          k, ncells, tol);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// out = m K u on an explicit level from the modal form km and, for the listed cells, their
+// node-basis entries kpc (both from lpb_pack_modal_f32); ft: 24 * cells scratch
+int lpb_apply_explicit_modal_f32(float* out, const float* u, const float* km, const float* kpc, const int* glist,
+                                 const int* gcount, float* ft, const uint8_t* mask, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !out || !u || !km || !kpc || !glist || !gcount || !ft || !mask || out == u) return LP_ERR_ARG;
+  k_modal_cells<<<lp_blocks(g.cells_padded(), 128), 128, 0, LP_ST>>>(ft, u, km, g);
+  k_listed_cells<<<148 * 4, 128, 0, LP_ST>>>(ft, u, kpc, glist, gcount, g);
+  k_explicit_gather<float><<<lp_blocks(g.nodes_padded(), 256), 256, 0, LP_ST>>>(out, ft, mask, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
 }
 
 int lpb_pack_sym_f32(float* kp, const float* k, long long ncells, void* stream) {

@@ -37,6 +37,9 @@ __all__ = ["GridElasticity", "BoxMesh", "LMAX_SAFETY", "STALL"]
 LMAX_SAFETY = 1.3          # loadpath/mg.py:81
 STALL = 100                # loadpath/mg.py:930
 DENSE_COARSE_MAX = 12_000  # dofs of the coarsest level solved by the dense factor (1.2 GB)
+# off-pattern weight (relative to a cell's largest corner-parity entry) above which an explicit
+# cell is applied from its node-basis matrix; float32 storage leaves ~1e-7 on pattern cells
+MODAL_TOL = 1e-5
 
 
 class BoxMesh:
@@ -124,6 +127,8 @@ class DevLevel:
         self.npatch = 0
         self.k = None
         self.kp = None           # explicit: packed symmetric (300, cells)
+        self.km = None           # explicit, plain hierarchy: corner-parity pattern entries (150, cells)
+        self.glist = self.gcount = self.kpc = None   # ...and the cells applied from node-basis entries
         self.ft = None           # explicit: (24, cells) scratch of the cell pass
         self.g1 = None           # weights: 279 corner-parity coefficients (host)
         self.wc = None           # weights: Walsh coefficients (cpz/4, ny, nx, 8, 4)
@@ -188,7 +193,11 @@ class DevLevel:
                                                         ptr(self.patch_k), self.mask.data_ptr(), *g.args,
                                                         int(mask_in), 1, st)
         else:
-            if fine_kernel and not mask_in:
+            if fine_kernel and not mask_in and self.km is not None:
+                L.lpb_apply_explicit_modal_f32(out.data_ptr(), u.data_ptr(), self.km.data_ptr(), self.kpc.data_ptr(),
+                                               self.glist.data_ptr(), self.gcount.data_ptr(), self.ft.data_ptr(),
+                                               self.mask.data_ptr(), *g.args, st)
+            elif fine_kernel and not mask_in:
                 getattr(L, f"lpb_apply_explicit_sym_{sfx}")(out.data_ptr(), u.data_ptr(), self.kp.data_ptr(),
                                                              self.ft.data_ptr(), self.mask.data_ptr(), *g.args, st)
             else:
@@ -613,9 +622,19 @@ class GridElasticity:
         else:
             getattr(L, f"lpb_galerkin_explicit_{sfx}")(lv.k.data_ptr(), 2, None, None, None, None, fine.k.data_ptr(),
                                                        fine.mask.data_ptr(), int(self.strict), *gf.args, *gc.args, st)
-        lv.kp = self._tbuf(f"kp{depth}", (300, ncp), dt)
-        getattr(L, f"lpb_pack_sym_{sfx}")(lv.kp.data_ptr(), lv.k.data_ptr(), ncp, st)
         lv.ft = self._tbuf(f"ft{depth}", (24, ncp), dt)
+        lv.km = lv.kp = None
+        if dt != torch.float32 or self.strict:
+            lv.kp = self._tbuf(f"kp{depth}", (300, ncp), dt)
+            getattr(L, f"lpb_pack_sym_{sfx}")(lv.kp.data_ptr(), lv.k.data_ptr(), ncp, st)
+        else:
+            # the plain hierarchy's cell matrices keep the corner-parity pattern: half the bytes
+            lv.km = self._tbuf(f"km{depth}", (150, ncp), dt)
+            lv.glist = self._tbuf(f"glist{depth}", (ncp,), torch.int32)
+            lv.gcount = self._tbuf(f"gcount{depth}", (1,), torch.int32)
+            lv.kpc = self._tbuf(f"kpc{depth}", (ncp, 300), dt)
+            L.lpb_pack_modal_f32(lv.km.data_ptr(), lv.glist.data_ptr(), lv.gcount.data_ptr(), lv.kpc.data_ptr(),
+                                 lv.k.data_ptr(), ncp, MODAL_TOL, st)
         return lv
 
     def _build_coarse(self, lv: DevLevel):
@@ -964,17 +983,22 @@ class GridElasticity:
         if graphed:
             g_pre = self._graph(("pre", warm), lambda: pre(warm))
             g_head = self._graph("head", head)
-            g_tail = self._graph("tail", tail)
-            pre_pairs, head_pairs, tail_pairs = g_pre[1], g_head[1], g_tail[1]
+            # with the probe set, two instances of the tail take turns: the one replayed at
+            # iteration it - 1 is complete (and not replayed again) when iteration it's head is
+            g_tails = [self._graph("tail", tail)]
+            if probe is not None:
+                g_tails.append(self._graph("tail2", tail))
+            pre_pairs, head_pairs = g_pre[1], g_head[1]
             self._replay(g_pre)
         else:
             pre(warm)
         ev = torch.cuda.Event()
+        last_tail = [None]
 
         def finish(result):
             if graphed and probe is not None:
                 torch.cuda.current_stream().synchronize()
-                probe.harvest(tail_pairs)          # the last (speculative) tail replay
+                probe.harvest(last_tail[0][1])     # the last (speculative) tail replay
             return result
 
         tol = None
@@ -986,16 +1010,20 @@ class GridElasticity:
             ev.record()
             # the next preconditioner step is queued before the host looks at |r|: the
             # device never waits on the convergence test (a converged solve discards it)
+            prev_tail = last_tail[0]
             if graphed:
-                self._replay(g_tail)
+                last_tail[0] = g_tails[it % len(g_tails)]
+                self._replay(last_tail[0])
             else:
                 tail()
             ev.synchronize()
             if graphed and probe is not None:
-                # this head replay is complete and the next is not launched yet; a tail replay
-                # may be re-recording its events now, so tails are read once, at the end
+                # this head replay and the previous tail replay are complete, and neither graph
+                # instance is queued again before the next harvest
                 if it == 1:
                     probe.harvest(pre_pairs)
+                else:
+                    probe.harvest(prev_tail[1])
                 probe.harvest(head_pairs)
             if tol is None:
                 bb = float(host[2])

@@ -299,3 +299,35 @@ def test_coarse_factor_takes_roundoff_negative_pivots():
     c, c_ref = float(np.vdot(f, u)), float(np.vdot(f, u_ref))
     assert abs(c - c_ref) <= 1e-9 * abs(c_ref)
     assert np.linalg.norm(u - u_ref) <= 1e-5 * np.linalg.norm(u_ref)
+
+
+def test_explicit_levels_modal_form_matches_node_basis():
+    """The explicit levels' corner-parity storage (150 pattern entries per cell, listed cells from
+    the node-basis form) gives the general kernel's operator; the supports' patch cells make some
+    cells listed, so both paths run."""
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from oracle import ref_numpy as R
+
+    dims = (32, 16, 16)
+    x = R.log_uniform_density(dims, 5)
+    e = R.simp_moduli(x)
+    fixed, f = R.cantilever_bc(dims)
+    mesh = BoxMesh(dims)
+    ge = GridElasticity(mesh, 0.3, ge_fixed(mesh, fixed), coarse_cells=20, element="im")
+    ge.set_moduli(e.reshape(-1))
+    explicit = [lv for lv in ge.levels[1:] if lv.kind == "explicit" and lv.km is not None]
+    assert explicit
+    listed = 0
+    rng = np.random.default_rng(2)
+    for lv in explicit:
+        gr = lv.grid
+        listed += int(lv.gcount.item())
+        m = gr.mask_to_host(lv.mask)
+        u = (rng.standard_normal(gr.node_shape) * m).astype(np.float32)
+        ud = gr.nodes_to_dev(u, torch.float32)
+        a, b = gr.node_field(torch.float32), gr.node_field(torch.float32)
+        lv.apply(a, ud)
+        lv.apply(b, ud, fine_kernel=False)
+        ga, gb = gr.nodes_to_host(a), gr.nodes_to_host(b)
+        np.testing.assert_allclose(ga, gb, rtol=2e-5, atol=2e-5 * np.abs(gb).max())
+    assert listed > 0
