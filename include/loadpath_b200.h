@@ -161,6 +161,11 @@ int lpb_band_factor(double* t, double* linv, double* sgn, int* info, unsigned* b
 int lpb_band_inverse(double* ainv, const double* t, const double* linv, const double* sgn, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_band_solve_f32(float* f_out, const float* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_band_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* The same for ncol right-hand sides of a block solve (no reference counterpart: the reference
+ * solves its load cases one at a time, loadpath/mg.py:932-949): column c of f_in / f_out at element
+ * offset c * cstride; the inverse is read once per 8 columns; v: 32 nt * ncol doubles. */
+int lpb_band_solve_cols_f32(float* f_out, const float* f_in, long long cstride, int ncol, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_band_solve_cols_f64(double* f_out, const double* f_in, long long cstride, int ncol, const double* ainv, double* v, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
 /* ---- Chebyshev smoother (loadpath/mg.py:771-821, loadpath/mgops.py:312-343) with its
  * coefficients in device memory: lpb_cheb_coef turns the power iteration's dots (vv[k] = |v|^2

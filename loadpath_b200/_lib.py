@@ -34,6 +34,10 @@ _KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_m
             "lpb_mma_part_len": 0, "lpb_mma_prepare": 2, "lpb_mma_newton_a": 2, "lpb_mma_newton_b": 2,
             "lpb_mma_trial": 2, "lpb_project": 2, "lpb_live_seed": 2,
             "lpb_dead_loads": 2, "lpb_apply_rf_f32": 2, "lpb_apply_explicit_modal_f32": 3}
+# entries whose kernel count depends on their arguments
+_VARIABLE = {"lpb_sensitivity": lambda a: 1 + (a[9] is not None),
+             "lpb_band_solve_cols_f32": lambda a: a[3] + (a[3] + 7) // 8,
+             "lpb_band_solve_cols_f64": lambda a: a[3] + (a[3] + 7) // 8}
 _COUNT = [0]
 
 
@@ -99,9 +103,10 @@ class _Lib:
             raise AttributeError(name)
 
         nk = _KERNELS.get(name, 1)
+        var = _VARIABLE.get(name)
 
         def call(*args):
-            _COUNT[0] += nk + (1 if name == "lpb_sensitivity" and args[9] is not None else 0)
+            _COUNT[0] += var(args) if var is not None else nk
             st = fn(*args)
             if st is not None and st < 0:
                 raise LpError(f"{name}: {_STATUS.get(st, 'error')} (status {st})")

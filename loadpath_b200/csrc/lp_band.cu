@@ -361,6 +361,70 @@ __global__ void k_band_gemv_to_field(T* __restrict__ f, const double* __restrict
   }
 }
 
+// k right-hand sides at once (fields at column stride cstride, band vectors at stride np): one
+// warp per row reads the row of ainv once for all k columns; each column's sum runs in the
+// single-column kernel's order, so a column's result has the same bits as a lone solve
+template <typename T, int K>
+__global__ void k_band_gemm_to_field(T* __restrict__ f, long long cstride, const double* __restrict__ a,
+                                     const double* __restrict__ v, LpGrid g, LpBand bd) {
+  const long long np = 32LL * bd.nt;
+  const int lane = threadIdx.x & 31;
+  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (row >= bd.n) return;
+  const double* ar = a + row * np;
+  double s[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) s[c] = 0.0;
+  for (long long j = lane; j < np; j += 32) {
+    const double aj = ar[j];
+#pragma unroll
+    for (int c = 0; c < K; ++c) s[c] += aj * v[c * np + j];
+  }
+#pragma unroll
+  for (int c = 0; c < K; ++c)
+    for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_down_sync(0xffffffffu, s[c], o);
+  if (lane == 0) {
+    int nx_, ny_, nz_;
+    bd.coords(row / 3, nx_, ny_, nz_);
+    const long long at = (row % 3) * g.comp_stride() + g.node(nx_, ny_, nz_);
+#pragma unroll
+    for (int c = 0; c < K; ++c) f[c * cstride + at] = (T)s[c];
+  }
+}
+
+template <typename T, int K>
+void band_gemm_launch(T* f_out, long long cstride, const double* ainv, const double* v, LpGrid g, LpBand bd,
+                      cudaStream_t st) {
+  k_band_gemm_to_field<T, K><<<lp_blocks(bd.n * 32, 256), 256, 0, st>>>(f_out, cstride, ainv, v, g, bd);
+}
+
+template <typename T>
+int band_solve_cols(T* f_out, const T* f_in, long long cstride, int ncol, const double* ainv, double* v, LpGrid g,
+                    cudaStream_t st) {
+  if (!lp_grid_ok(g) || !f_out || !f_in || !ainv || !v || ncol < 1 || cstride < g.comp_stride() * 3) return LP_ERR_ARG;
+  const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
+  const long long np = 32LL * bd.nt;
+  for (int c = 0; c < ncol; ++c)
+    k_field_to_band<T><<<lp_blocks(np, 256), 256, 0, st>>>(v + c * np, f_in + c * cstride, g, bd);
+  for (int c0 = 0; c0 < ncol; c0 += 8) {
+    const int k = ncol - c0 < 8 ? ncol - c0 : 8;
+    T* fo = f_out + c0 * cstride;
+    const double* vc = v + c0 * np;
+    switch (k) {
+      case 1: band_gemm_launch<T, 1>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 2: band_gemm_launch<T, 2>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 3: band_gemm_launch<T, 3>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 4: band_gemm_launch<T, 4>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 5: band_gemm_launch<T, 5>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 6: band_gemm_launch<T, 6>(fo, cstride, ainv, vc, g, bd, st); break;
+      case 7: band_gemm_launch<T, 7>(fo, cstride, ainv, vc, g, bd, st); break;
+      default: band_gemm_launch<T, 8>(fo, cstride, ainv, vc, g, bd, st); break;
+    }
+  }
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
 template <typename T>
 int band_solve(T* f_out, const T* f_in, const double* ainv, double* v, LpGrid g, cudaStream_t st) {
   if (!lp_grid_ok(g) || !f_out || !f_in || !ainv || !v) return LP_ERR_ARG;
@@ -453,6 +517,18 @@ int lpb_band_solve_f32(float* f_out, const float* f_in, const double* ainv, doub
 int lpb_band_solve_f64(double* f_out, const double* f_in, const double* ainv, double* v, LP_GRID_ARGS,
                        void* stream) {
   return band_solve<double>(f_out, f_in, ainv, v, LP_GRID, LP_ST);
+}
+
+// ncol right-hand sides at once: column c of f_in / f_out at element offset c * cstride (whole
+// node fields, cstride >= 3 * the component stride); v: 32 nt * ncol doubles scratch
+int lpb_band_solve_cols_f32(float* f_out, const float* f_in, long long cstride, int ncol, const double* ainv,
+                            double* v, LP_GRID_ARGS, void* stream) {
+  return band_solve_cols<float>(f_out, f_in, cstride, ncol, ainv, v, LP_GRID, LP_ST);
+}
+
+int lpb_band_solve_cols_f64(double* f_out, const double* f_in, long long cstride, int ncol, const double* ainv,
+                            double* v, LP_GRID_ARGS, void* stream) {
+  return band_solve_cols<double>(f_out, f_in, cstride, ncol, ainv, v, LP_GRID, LP_ST);
 }
 
 }  // extern "C"

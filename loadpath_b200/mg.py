@@ -1094,6 +1094,270 @@ class GridElasticity:
         self.last_iters = iters
         return out
 
+    # --- k right-hand sides as one block ----------------------------------------------------
+    # The reference solves its load cases one after another (loadpath/mg.py:932-949). Here k
+    # columns advance together: one traversal of the hierarchy per PCG iteration runs every
+    # column's smoothing, transfers and operator applies level by level (so a level's
+    # coefficients - moduli, level-1 weights, explicit matrices - are read from L2 by the
+    # columns after the first), one kernel solves the coarsest level for all columns (its
+    # dense inverse read once per eight), and the host reads every column's scalars with one
+    # copy per iteration. Each column keeps its own scalars and stopping test and runs the
+    # same kernels on the same data as a lone solve, so a column's answer has the same bits.
+    def _blk(self, key, k, grid: DevGrid, dtype):
+        """k node fields of a level as one (k, field) tensor; [j] is column j's field."""
+        return self._tbuf(key, (k, 3, grid.pz // 4, grid.NY, grid.NX, 4), dtype)
+
+    def _block_buffers(self, k):
+        g = self.g0
+        bufs = {key: self._blk(f"bcg_{key}", k, g, torch.float64) for key in ("x", "r", "p", "ap", "rs", "b")}
+        for i in range(len(self.levels)):
+            lv = self._op(i)
+            self._blk(f"bx{i}", k, lv.grid, self.tdtype)
+            self._blk(f"bb{i}", k, lv.grid, self.tdtype)
+            for key in ("r", "d", "t"):
+                self._buf(f"{key}{i}", lv.grid, self.tdtype)
+        if self._coarse is not None:
+            self._flat_buf("band_vcols", k * self._coarse["v"].numel(), torch.float64)
+        bufs["sc"] = self._tbuf("bcg_sc", (k, 8), torch.float64)
+        if getattr(self, "_bhost", None) is None or self._bhost.shape[0] != k:
+            self._bhost = torch.zeros((k, 8), dtype=torch.float64, pin_memory=True)
+            self._gen += 1               # graphs that copy into the old one are not replayed again
+        return bufs
+
+    def _vcycle_cols(self, i, bb, dots=None):
+        """The V-cycle of level i for every column of bb (a (k, field) level-i block); returns
+        the level's x block. dots: [(r64, out)] per column, out = r64 . x."""
+        L = lib()
+        st = stream_handle()
+        lv = self._op(i)
+        g = lv.grid
+        dt = lv.dtype
+        sfx = "f32" if dt == torch.float32 else "f64"
+        k = bb.shape[0]
+        xb = self._blk(f"bx{i}", k, g, dt)
+        if i == len(self.levels) - 1:
+            if self._coarse is not None:
+                c = self._coarse
+                v = self._flat_buf("band_vcols", k * c["v"].numel(), torch.float64)
+                getattr(L, f"lpb_band_solve_cols_{sfx}")(xb.data_ptr(), bb.data_ptr(), xb[0].numel(), k,
+                                                         c["ainv"].data_ptr(), v.data_ptr(), *g.args, st)
+            else:
+                for j in range(k):
+                    self._smooth(i, bb[j], xb[j], True)
+                    self._smooth(i, bb[j], xb[j], False)
+        else:
+            t = self._buf(f"t{i}", g, dt)
+            nxt = self._op(i + 1)
+            gc = nxt.grid
+            bc = self._blk(f"bb{i + 1}", k, gc, dt)
+            for j in range(k):
+                self._smooth(i, bb[j], xb[j], True)
+                lv.apply(t, xb[j])
+                getattr(L, f"lpb_restrict_residual_{sfx}")(bc[j].data_ptr(), bb[j].data_ptr(), t.data_ptr(),
+                                                           lv.mask.data_ptr(), nxt.mask.data_ptr(), *g.args,
+                                                           *gc.args, st)
+            xc = self._vcycle_cols(i + 1, bc)
+            for j in range(k):
+                getattr(L, f"lpb_prolong_add_{sfx}")(xb[j].data_ptr(), xc[j].data_ptr(), nxt.mask.data_ptr(),
+                                                     lv.mask.data_ptr(), *g.args, *gc.args, st)
+                self._smooth(i, bb[j], xb[j], False)
+        if dots is not None:
+            dot = L.lpb_dot_f64_f32 if dt == torch.float32 else L.lpb_dot_f64
+            for j, (r64, out) in enumerate(dots):
+                dot(r64.data_ptr(), xb[j].data_ptr(), xb[j].numel(), self._part.data_ptr(), out.data_ptr(), st)
+        return xb
+
+    def _pcg_block(self, bs, x0s, outs):
+        """float64 PCG on k columns at once (the per-column algorithm of _pcg_device). bs, x0s:
+        lists of masked padded fields (x0s entries may be None); outs: the k result fields, each
+        written once its column has converged. Returns (iterations, converged) per column."""
+        L = lib()
+        g = self.g0
+        n = g.n_node_field
+        k = len(bs)
+        a = self.levels[0]
+        probe = _PROBE[0]
+        _PROBE[0] = None                 # the block path records no fine-apply events
+        try:
+            B = self._block_buffers(k)
+            x, r, p, ap, rs, src, sc = B["x"], B["r"], B["p"], B["ap"], B["rs"], B["b"], B["sc"]
+            host = self._bhost
+            nb = 8 * n
+            f32 = self.tdtype == torch.float32
+            bb0 = self._blk("bb0", k, g, self.tdtype)
+            for j in range(k):
+                L.lpb_memcpy_async(src[j].data_ptr(), bs[j].data_ptr(), nb, stream_handle())
+                if x0s[j] is not None:
+                    L.lpb_memcpy_async(x[j].data_ptr(), x0s[j].data_ptr(), nb, stream_handle())
+            warm = tuple(x0 is not None for x0 in x0s)
+
+            def dot(u, v, out):
+                L.lpb_dot_f64(u.data_ptr(), v.data_ptr(), n, self._part.data_ptr(), out.data_ptr(), stream_handle())
+
+            def precondition_all():
+                # z = V(r) for every column, z left in the level-0 x block
+                st = stream_handle()
+                for j in range(k):
+                    if f32:
+                        L.lpb_cast_f64_f32(bb0[j].data_ptr(), r[j].data_ptr(), n, st)
+                    else:
+                        L.lpb_memcpy_async(bb0[j].data_ptr(), r[j].data_ptr(), nb, st)
+                return self._vcycle_cols(0, bb0)
+
+            def pre():
+                st = stream_handle()
+                for j in range(k):
+                    s = sc[j]
+                    dot(src[j], src[j], s[0])
+                    if warm[j]:
+                        a.apply(ap[j], x[j])
+                        dot(x[j], ap[j], s[5])
+                        dot(src[j], x[j], s[6])
+                        L.lpb_warm_residual(rs[j].data_ptr(), src[j].data_ptr(), ap[j].data_ptr(), s.data_ptr(), n,
+                                            st)
+                        dot(rs[j], rs[j], s[7])
+                        L.lpb_warm_select(x[j].data_ptr(), r[j].data_ptr(), src[j].data_ptr(), rs[j].data_ptr(),
+                                          s.data_ptr(), n, st)
+                    else:
+                        L.lpb_memset_async(x[j].data_ptr(), 0, nb, st)
+                        L.lpb_memcpy_async(r[j].data_ptr(), src[j].data_ptr(), nb, st)
+                z = precondition_all()
+                for j in range(k):
+                    if f32:
+                        L.lpb_cast_f32_f64(p[j].data_ptr(), z[j].data_ptr(), n, st)
+                    else:
+                        L.lpb_memcpy_async(p[j].data_ptr(), z[j].data_ptr(), nb, st)
+                    dot(r[j], p[j], sc[j][1])
+
+            def head():
+                st = stream_handle()
+                for j in range(k):
+                    s = sc[j]
+                    a.apply_dot(ap[j], p[j], self._part, s[3])
+                    L.lpb_cg_step_r(r[j].data_ptr(), ap[j].data_ptr(), bb0[j].data_ptr() if f32 else None, n,
+                                    s[1].data_ptr(), s[3].data_ptr(), self._part.data_ptr(), s[4].data_ptr(), st)
+                L.lpb_memcpy_async(host.data_ptr(), sc.data_ptr(), 8 * 8 * k, st)
+
+            def tail():
+                st = stream_handle()
+                if f32:
+                    # cg_step_r left each column's float32 residual in the level-0 b block
+                    z = self._vcycle_cols(0, bb0, dots=[(r[j], sc[j][2]) for j in range(k)])
+                else:
+                    z = precondition_all()
+                    for j in range(k):
+                        dot(r[j], z[j], sc[j][2])
+                for j in range(k):
+                    s = sc[j]
+                    getattr(L, "lpb_xpby_x_f32" if f32 else "lpb_xpby_x_f64")(
+                        p[j].data_ptr(), x[j].data_ptr(), z[j].data_ptr(), n, s[1].data_ptr(), s[3].data_ptr(),
+                        s[2].data_ptr(), st)
+                    L.lpb_memcpy_async(s[1].data_ptr(), s[2].data_ptr(), 8, st)
+
+            graphed = self.use_graphs and self.maxiter > 1
+            if graphed:
+                g_pre = self._graph(("bpre", k, warm), pre)
+                g_head = self._graph(("bhead", k), head)
+                g_tail = self._graph(("btail", k), tail)
+                self._replay(g_pre)
+            else:
+                pre()
+            ev = torch.cuda.Event()
+            iters = [0] * k
+            ok = [False] * k
+            done = [False] * k
+            tol = [None] * k
+            for it in range(1, self.maxiter + 1):
+                if graphed:
+                    self._replay(g_head)
+                else:
+                    head()
+                ev.record()
+                if graphed:
+                    self._replay(g_tail)
+                else:
+                    tail()
+                ev.synchronize()
+                hv = host.numpy()
+                for j in range(k):
+                    if done[j]:
+                        continue
+                    if tol[j] is None:
+                        bbj = float(hv[j, 0])
+                        if bbj == 0.0:
+                            L.lpb_memset_async(outs[j].data_ptr(), 0, nb, stream_handle())
+                            done[j], ok[j], iters[j] = True, True, 0
+                            continue
+                        tol[j] = self.rtol * math.sqrt(bbj)
+                    pap, rr = float(hv[j, 3]), float(hv[j, 4])
+                    if not pap > 0:
+                        done[j], iters[j] = True, it
+                    elif math.sqrt(rr) <= tol[j]:
+                        # this iteration's tail (already queued) completes x; its masked copy
+                        # follows it
+                        L.lpb_mask_field_f64(outs[j].data_ptr(), x[j].data_ptr(), a.mask.data_ptr(), *g.args, 0,
+                                             stream_handle())
+                        done[j], ok[j], iters[j] = True, True, it
+                if all(done):
+                    break
+            for j in range(k):
+                if not done[j]:
+                    iters[j] = self.maxiter
+            return iters, ok
+        finally:
+            _PROBE[0] = probe
+
+    def solve_block_device(self, bs, x0s=None):
+        """Solve for k right-hand sides at once (padded float64 device fields); b and x0 are
+        masked here. Returns a list of new device fields (masked); self.last_iters is the list of
+        per-column iteration counts. A column not converged within the stall limit switches the
+        hierarchy to strict and is solved again with the rest that failed (loadpath/mg.py:951-965).
+        Raises RuntimeError when a column does not converge."""
+        L = lib()
+        st = stream_handle()
+        g = self.g0
+        m = self.levels[0].mask
+        k = len(bs)
+        x0s = list(x0s) if x0s is not None else [None] * k
+        bm, x0m, outs = [], [], []
+        for j in range(k):
+            b = g.node_field(torch.float64)
+            L.lpb_mask_field_f64(b.data_ptr(), bs[j].data_ptr(), m.data_ptr(), *g.args, 0, st)
+            bm.append(b)
+            if x0s[j] is not None:
+                x0 = g.node_field(torch.float64)
+                L.lpb_mask_field_f64(x0.data_ptr(), x0s[j].data_ptr(), m.data_ptr(), *g.args, 0, st)
+                x0m.append(x0)
+            else:
+                x0m.append(None)
+            outs.append(g.node_field(torch.float64))
+        todo = list(range(k))
+        iters = [0] * k
+        stall = not (self.strict or len(self.levels) < 2)
+        full = self.maxiter
+        if stall:
+            self.maxiter = min(full, STALL)
+        try:
+            its, ok = self._pcg_block([bm[j] for j in todo], [x0m[j] for j in todo], [outs[j] for j in todo])
+        finally:
+            self.maxiter = full
+        for j, it_ in zip(todo, its):
+            iters[j] += it_
+        todo = [j for j, o in zip(todo, ok) if not o]
+        if todo and stall:
+            self.strict = True
+            self.set_moduli_device(self._e_dev)
+            its, ok = self._pcg_block([bm[j] for j in todo], [x0m[j] for j in todo], [outs[j] for j in todo])
+            for j, it_ in zip(todo, its):
+                iters[j] += it_
+            todo = [j for j, o in zip(todo, ok) if not o]
+        self.last_iters = iters
+        self.check_device()
+        if todo:
+            raise RuntimeError(f"linear solve did not converge ({max(iters[j] for j in todo)} iterations); "
+                               "the structure may be a mechanism (check supports)")
+        return outs
+
     # --- other reference methods ----------------------------------------------------------
     def apply(self, u):
         """The float64 operator on a host node-grid field (loadpath/mg.py:868-870)."""
