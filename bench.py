@@ -31,6 +31,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 DIMS = (256, 128, 128)
+CASE_DIMS = (192, 96, 96)
 VOLFRAC, RMIN, RTOL, PENAL, EMIN, MOVE = 0.3, 2.0, 1e-6, 3.0, 1e-9, 0.2
 METRIC = "SIMP iter/s & K*u GB/s at 12.7M DOF: mixed-prec vs FP64 GPU, <=1e-6 rel err"
 
@@ -45,17 +46,21 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--micro", choices=["apply", "band"], default=None,
+    p.add_argument("--micro", choices=["apply", "band", "cases"], default=None,
                    help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
                         "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
-                        "coarsest level's band assembly, factorisation and inverse")
+                        "coarsest level's band assembly, factorisation and inverse; cases: the batched "
+                        "load-case SIMP iteration (8 point loads at 192x96x96 unless --dims is given), "
+                        "the cases solved as one block and one after another")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--kernels", type=int, default=0, metavar="N",
                    help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
                         "activity trace (torch.profiler); a table, not the JSON line")
     a = p.parse_args()
     a.warmup = max(a.warmup, 3)
-    a.dims = tuple(int(v) for v in a.dims.split(","))
+    if a.micro == "cases" and a.dims == ",".join(str(d) for d in DIMS):
+        a.dims = CASE_DIMS
+    a.dims = tuple(int(v) for v in a.dims.split(",")) if isinstance(a.dims, str) else a.dims
     return a
 
 
@@ -244,14 +249,8 @@ def run_b200(args):
 
     # ---- device-resident timing -----------------------------------------------------------
     loop = new_loop(np.float32)
-    # the probe is set through the warm-up, so the graphs that record its events are captured
-    # there, and its totals restart with the timed region
-    probe = mg.FineApplyProbe()
-    mg.set_probe(probe)
     for _ in range(args.warmup):
         loop.step()
-    probe.summary()
-    probe.totals = dict.fromkeys(probe.totals, 0)
     barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
@@ -267,7 +266,7 @@ def run_b200(args):
         iters.append(loop.ge.last_iters)
     t1.record()
     torch.cuda.synchronize()
-    mg.set_probe(None)
+    timing, loop.timing = loop.timing, None
     barrier()
     clocks = clk.stop()
     launches = _lib.launches() - calls0
@@ -277,6 +276,14 @@ def run_b200(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * args.steps / (ms / 1e3)
+    # the fine kernel's launch times: CUDA events around every fine-level apply over a second
+    # pass of as many SIMP iterations, right after the timed one (events cannot sit inside the
+    # device-side CG loop's graph, so this pass tests convergence on the host)
+    probe = mg.FineApplyProbe()
+    mg.set_probe(probe)
+    for _ in range(args.steps):
+        loop.step()
+    mg.set_probe(None)
     fine = probe.summary()
     peak, peak_kind = peaks()
     b32 = apply_bytes(dims, 4)
@@ -294,11 +301,12 @@ def run_b200(args):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "kernel": "k_apply_fine_x2 (float32)",
                     "algorithmic_bytes": b32, "avg_launch_us": avg * 1e6, "launches_timed": fine["f32_count"],
+                    "timed_over": f"{args.steps} SIMP iterations after the timed region, CUDA events around "
+                                  "each fine-level float32 apply on its stream",
                     "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured"
                                     else "fallback (6.65 TB/s copy measured earlier on this pool's B200s)")}
-    phases = np.array([[a.elapsed_time(b) for a, b in zip(ev[:-1], ev[1:])] for ev in loop.timing])
-    loop.timing = None
-    extra = {"cg_iterations": iters, "compliance": loop.history[-1][0],
+    phases = np.array([[a.elapsed_time(b) for a, b in zip(ev[:-1], ev[1:])] for ev in timing])
+    extra = {"cg_iterations": iters, "compliance": loop.history[args.warmup + args.steps - 1][0],
              "phase_ms_per_step": dict(zip(("hierarchy", "solve", "sensitivities", "oc"),
                                            np.round(phases.mean(axis=0), 3).tolist())),
              "fine_apply_f64_us": (fine["f64_ms"] / fine["f64_count"] * 1e3) if fine["f64_count"] else None,
@@ -318,7 +326,7 @@ def run_b200(args):
             lp.u = None
             lp.solve()
             lp.sensitivities()
-            return float(lp._scal[0].item()), lp.u.clone(), lp.dcf.clone()
+            return float(lp._scal[8].item()), lp.u.clone(), lp.dcf.clone()
 
         c32, u32, dc32 = first(mix, RTOL)
         c64, _, _ = first(ref, RTOL)
@@ -546,6 +554,60 @@ def run_micro_band(args):
     return 0
 
 
+def case_loads(dims, k=8, seed=3):
+    """k unit point forces at nodes (nx, j, kk) of the free face, j and kk from
+    default_rng(seed).integers, each direction a normalised standard_normal(3)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(k):
+        j, kk = int(rng.integers(0, dims[1] + 1)), int(rng.integers(0, dims[2] + 1))
+        d = rng.standard_normal(3)
+        f = np.zeros((3,) + tuple(n + 1 for n in dims))
+        f[:, dims[0], j, kk] = d / np.linalg.norm(d)
+        out.append(f)
+    return out
+
+
+def run_micro_cases(args):
+    """The batched load-case SIMP iteration: 8 cases, x = 0 face held, uniform start at volume
+    fraction 0.2, filter r = 2, mixed precision; SIMP iterations per second with the cases solved
+    as one block of right-hand sides and one after another, CUDA-event timed."""
+    import torch
+
+    from loadpath_b200.simp import Top3dLoop
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    fixed, _ = cantilever(dims)
+    loads = case_loads(dims)
+    out = {}
+    for block in (True, False):
+        loop = Top3dLoop(dims, 0.2, 2.0, fixed, loads, rtol=RTOL, dtype=np.float32, penal=PENAL, emin=EMIN,
+                         move=MOVE, element="im", block_cases=block)
+        for _ in range(args.warmup):
+            loop.step()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            loop.step()
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / args.steps
+        out["block" if block else "one_by_one"] = {
+            "simp_iter_per_s": 1e3 / ms, "ms_per_step": ms,
+            "cg_iterations": [list(map(int, h[2])) for h in loop.history[-args.steps:]],
+            "compliance": [h[0] for h in loop.history[-args.steps:]]}
+        del loop
+        torch.cuda.empty_cache()
+    same = out["block"]["compliance"] == out["one_by_one"]["compliance"]
+    print(json.dumps({"micro": "load cases", "dims": list(dims), "cases": len(loads), "steps": args.steps,
+                      "warmup": args.warmup, "dtype": "f32+f64", "data": "synthetic (seeded point loads)",
+                      "block_over_one_by_one": out["block"]["simp_iter_per_s"] / out["one_by_one"]["simp_iter_per_s"],
+                      "same_compliance_bits": same, **out}))
+    return 0
+
+
 def run_kernels(args):
     """Per-kernel device time of args.kernels SIMP iterations after args.warmup, from the CUDA
     activity records (CUPTI through torch.profiler: kernels are not serialised)."""
@@ -602,6 +664,8 @@ def main():
         return run_micro_apply(args)
     if args.micro == "band":
         return run_micro_band(args)
+    if args.micro == "cases":
+        return run_micro_cases(args)
     if args.kernels:
         return run_kernels(args)
     if args.impl == "reference":

@@ -263,6 +263,14 @@ int lpb_capture_begin(void* stream);
 int lpb_capture_end(void* stream, void** exec);
 int lpb_graph_launch(void* exec, void* stream);
 int lpb_graph_free(void* exec);
+/* A device-side loop (no reference counterpart: loadpath/mg.py:872-926 tests convergence on the
+ * host each iteration): lpb_while_begin starts capturing the body of a graph's WHILE node into
+ * the stream, lpb_while_end instantiates it (an exec for lpb_graph_launch); the body's
+ * lpb_cg_continue (sc: the PCG scalars, [0] |b|^2, [3] p.Ap, [4] |r|^2; state: iterations,
+ * status) ends the loop once |r| <= rtol |b|, p.Ap <= 0, b = 0 or maxiter iterations ran. */
+int lpb_while_begin(void* stream, long long* handle, void** graph);
+int lpb_while_end(void* stream, void* graph, void** exec);
+int lpb_cg_continue(long long handle, const double* sc, long long* state, double rtol, long long maxiter, void* stream);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
 int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 

@@ -1,11 +1,91 @@
 // Host-side plumbing kept out of Python's way: CUDA graph capture of a stream (begin /
 // end+instantiate / launch / free), so the solver records its set-up, CG head and CG tail once
 // and replays each with one launch; capturable asynchronous copies and fills.
+#include <cstring>
+
 #include "lp_common.cuh"
 
 #define LP_ST ((cudaStream_t)stream)
 
+namespace {
+
+// The PCG's stopping test on the device (loadpath/mg.py:872-926, as the host loop makes it):
+// sc[0] = |b|^2, sc[3] = p.Ap, sc[4] = |r|^2 after this iteration's head; state[0] counts
+// iterations, state[1] is left 1 converged, 2 zero right-hand side, 3 p.Ap not positive, 0
+// otherwise. The loop continues while the test fails and fewer than maxiter iterations ran.
+__global__ void k_cg_continue(cudaGraphConditionalHandle handle, const double* __restrict__ sc,
+                              long long* __restrict__ state, double rtol, long long maxiter) {
+  const long long it = state[0] + 1;
+  state[0] = it;
+  const double bb = sc[0], pap = sc[3], rr = sc[4];
+  long long status = 0;
+  if (bb == 0.0) status = 2;
+  else if (!(pap > 0.0)) status = 3;
+  else if (sqrt(rr) <= rtol * sqrt(bb)) status = 1;
+  state[1] = status;
+  cudaGraphSetConditional(handle, (status == 0 && it < maxiter) ? 1u : 0u);
+}
+
+}  // namespace
+
 extern "C" {
+
+// Starts recording the body of a device-side while loop: a graph with one conditional WHILE node
+// (its condition 1 at each launch of the graph), the stream capturing into the node's body.
+// *handle: the condition's handle (for lpb_cg_continue); *graph: the outer graph, for
+// lpb_while_end.
+int lpb_while_begin(void* stream, long long* handle, void** graph) {
+  if (!handle || !graph) return LP_ERR_ARG;
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return LP_ERR_LAUNCH;
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return LP_ERR_LAUNCH;
+  }
+  // a zeroed parameter block (the struct's union makes its default constructor deleted)
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& p = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, nullptr, 0, &p) != cudaSuccess ||
+      cudaStreamBeginCaptureToGraph(LP_ST, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return LP_ERR_LAUNCH;
+  }
+  *handle = (long long)h;
+  *graph = (void*)g;
+  return LP_OK;
+}
+
+// Ends the body's capture and instantiates the outer graph; *exec receives a cudaGraphExec_t
+int lpb_while_end(void* stream, void* graph, void** exec) {
+  if (!graph || !exec) return LP_ERR_ARG;
+  cudaGraph_t g = (cudaGraph_t)graph;
+  cudaGraph_t body = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(LP_ST, &body);
+  cudaGraphExec_t ge = nullptr;
+  const cudaError_t ei = ec == cudaSuccess ? cudaGraphInstantiate(&ge, g, 0) : ec;
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return LP_ERR_LAUNCH;
+  *exec = (void*)ge;
+  return LP_OK;
+}
+
+// The loop's stopping test (k_cg_continue) as one launch in the body: sc the solve's scalars,
+// state two device long longs (iterations, status), zeroed before the loop's launch
+int lpb_cg_continue(long long handle, const double* sc, long long* state, double rtol, long long maxiter,
+                    void* stream) {
+  if (!sc || !state || maxiter < 1) return LP_ERR_ARG;
+  k_cg_continue<<<1, 1, 0, LP_ST>>>((cudaGraphConditionalHandle)handle, sc, state, rtol, maxiter);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
 
 int lpb_capture_begin(void* stream) {
   return cudaStreamBeginCapture(LP_ST, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? LP_OK : LP_ERR_LAUNCH;

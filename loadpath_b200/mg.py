@@ -321,6 +321,10 @@ class GridElasticity:
         self._coef = torch.zeros(16 * 32, dtype=torch.float64, device=self.device)
         self._part = torch.zeros(max(lib().lpb_reduce_blocks(), 1024) * 2, dtype=torch.float64, device=self.device)
         self._host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
+        # the device-side CG loop: its stopping test's state (iterations, status) and its copy
+        self._loop_state = torch.zeros(2, dtype=torch.int64, device=self.device)
+        self._loop_out = torch.zeros(2, dtype=torch.int64, pin_memory=True)
+        self.device_loop = True  # graphed solves test convergence on the device (no host read per iteration)
         self._work = {}
         self._e_dev = None
         # CUDA graphs for the CG iteration (captured once per solve)
@@ -866,10 +870,11 @@ class GridElasticity:
             if i + 1 < len(self.levels):
                 self._buf(f"b{i + 1}", self._op(i + 1).grid, self.tdtype)
 
-    def _graph(self, key, fn):
+    def _graph(self, key, fn, loop=False):
         """fn's launches captured as one CUDA graph, kept until a buffer it names is replaced
         (a new allocation or a new hierarchy structure) or the probe changes. Returns
-        (exec, probe event pairs recorded by each replay)."""
+        (exec, probe event pairs recorded by each replay, kernels per replay). loop: fn(handle)
+        records the body of a device-side while loop whose condition handle it is given."""
         L = lib()
         cache = self._gcache
         probe = _PROBE[0]
@@ -887,12 +892,19 @@ class GridElasticity:
             # on the working stream
             with torch.cuda.stream(self._cap_stream):
                 st0 = stream_handle()
-                L.lpb_capture_begin(st0)
+                if loop:
+                    handle, outer = ctypes.c_longlong(), ctypes.c_void_p()
+                    L.lpb_while_begin(st0, ctypes.byref(handle), ctypes.byref(outer))
+                else:
+                    L.lpb_capture_begin(st0)
                 try:
-                    fn()
+                    fn(handle.value) if loop else fn()
                 finally:
                     exec_ = ctypes.c_void_p()
-                    L.lpb_capture_end(st0, ctypes.byref(exec_))
+                    if loop:
+                        L.lpb_while_end(st0, outer, ctypes.byref(exec_))
+                    else:
+                        L.lpb_capture_end(st0, ctypes.byref(exec_))
                     if probe is not None:
                         probe.capture = None
             nk = launches() - c0
@@ -980,6 +992,35 @@ class GridElasticity:
         warm = x0 is not None
         probe = _PROBE[0]
         graphed = self.use_graphs and self.maxiter > 1
+        if graphed and self.device_loop and probe is None:
+            # the whole iteration loop as one graph launch: head, the stopping test, tail per
+            # iteration, the test on the device (the graph's WHILE node); the host reads the
+            # outcome once
+            st = stream_handle()
+            state = self._loop_state
+            rtol, maxiter = float(self.rtol), int(self.maxiter)
+
+            def body(handle):
+                stb = stream_handle()
+                a.apply_dot(ap, p, self._part, sc[3])
+                L.lpb_cg_step_r(r.data_ptr(), ap.data_ptr(), ptr(r32), n, sc[1].data_ptr(), sc[3].data_ptr(),
+                                self._part.data_ptr(), sc[4].data_ptr(), stb)
+                L.lpb_cg_continue(handle, sc.data_ptr(), state.data_ptr(), rtol, maxiter, stb)
+                tail()
+
+            g_pre = self._graph(("pre", warm), lambda: pre(warm))
+            g_loop = self._graph(("loop", rtol, maxiter), body, loop=True)
+            L.lpb_memset_async(state.data_ptr(), 0, 16, st)
+            self._replay(g_pre)
+            self._replay(g_loop)
+            L.lpb_memcpy_async(self._loop_out.data_ptr(), state.data_ptr(), 16, st)
+            torch.cuda.current_stream().synchronize()
+            it, status = int(self._loop_out[0]), int(self._loop_out[1])
+            add_launches(g_loop[2] * (it - 1))          # the body ran `it` times
+            if status == 2:
+                L.lpb_memset_async(x.data_ptr(), 0, nb, st)
+                return x, 0, True
+            return x, it, status == 1
         if graphed:
             g_pre = self._graph(("pre", warm), lambda: pre(warm))
             g_head = self._graph("head", head)

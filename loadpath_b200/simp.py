@@ -398,11 +398,13 @@ class Top3dLoop:
     (loadpath/benchmarks/reference.py:74-117), solved by the device MG-PCG.
 
     dims: cells (even counts); fixed_grid: bool (3, nx+1, ny+1, nz+1); f_grid: float64 loads on
-    the same grid; x0: optional initial density (cells), default volfrac everywhere."""
+    the same grid, or a list of them (load cases: the objective is their equally weighted
+    compliance sum, the cases solved as one block of right-hand sides); x0: optional initial
+    density (cells), default volfrac everywhere."""
 
     def __init__(self, dims, volfrac, rmin, fixed_grid, f_grid, nu=0.3, element=None, penal=3.0, emin=1e-9,
                  move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=500,
-                 smoother="chebyshev", warm_start=True, device="cuda"):
+                 smoother="chebyshev", warm_start=True, block_cases=True, device="cuda"):
         dims = tuple(int(d) for d in dims)
         if any(d % 2 for d in dims):
             raise ValueError("the device SIMP loop takes even cell counts (the multigrid pads odd ones)")
@@ -418,7 +420,9 @@ class Top3dLoop:
         g = self.ge.g0
         self.grid = g
         self.filter = DeviceFilter(g, rmin, pad=False)
-        self.f = g.nodes_to_dev(np.asarray(f_grid, np.float64), torch.float64)
+        cases = f_grid if isinstance(f_grid, (list, tuple)) else [f_grid]
+        self.fs = [g.nodes_to_dev(np.asarray(fk, np.float64), torch.float64) for fk in cases]
+        self.f = self.fs[0]
         self.x = g.cell_field(torch.float64)
         if x0 is None:
             g.set_cells(self.x, self.volfrac)
@@ -432,9 +436,12 @@ class Top3dLoop:
         self.dc = g.cell_field(torch.float64)
         self.dcf = g.cell_field(torch.float64)
         self.u = None
+        self.us = None           # the load cases' displacements (several cases)
+        self.block_cases = block_cases   # False: the cases one solve after another
         self.warm_start = warm_start
         self.ncell = dims[0] * dims[1] * dims[2]
-        self._scal = torch.zeros(64, dtype=torch.float64, device=g.device)
+        # [0] compliance, [1] change, [8 + k] case k's compliance
+        self._scal = torch.zeros(8 + max(len(self.fs), 56), dtype=torch.float64, device=g.device)
         self._part = torch.zeros(31 * 592 + 1024, dtype=torch.float64, device=g.device)
         self._lam = torch.zeros(31, dtype=torch.float64, device=g.device)
         self._vols = torch.zeros(31, dtype=torch.float64, device=g.device)
@@ -444,20 +451,40 @@ class Top3dLoop:
         lib().lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, stream_handle())
 
     # ---- one iteration -------------------------------------------------------------------
+    def _solve_cases(self):
+        if len(self.fs) == 1:
+            x0 = self.u if (self.warm_start and self.u is not None) else None
+            self.u = self.ge.solve_device(self.f, x0)
+            self.us = [self.u]
+        else:
+            x0s = self.us if (self.warm_start and self.us is not None) else [None] * len(self.fs)
+            if self.block_cases:
+                self.us = self.ge.solve_block_device(self.fs, x0s)
+            else:
+                us, its = [], []
+                for f, x0 in zip(self.fs, x0s):
+                    us.append(self.ge.solve_device(f, x0))
+                    its.append(self.ge.last_iters)
+                self.us = us
+                self.ge.last_iters = its
+            self.u = self.us[0]
+
     def solve(self):
         self.ge.set_moduli_device(self.e)
-        x0 = self.u if (self.warm_start and self.u is not None) else None
-        self.u = self.ge.solve_device(self.f, x0)
+        self._solve_cases()
         return self.u
 
     def sensitivities(self):
-        """ce, compliance (device scalar), dc = H (dc_raw / hs) (loadpath/benchmarks/reference.py:91-99)."""
+        """ce, compliance (device scalar), dc = H (dc_raw / hs) (loadpath/benchmarks/reference.py:91-99);
+        with several load cases the sums of the cases' compliances and raw sensitivities."""
         L = lib()
         st = stream_handle()
         g = self.grid
-        self.ge.strain_energy_device(self.u, out=self.ce)
-        L.lpb_sensitivity(self.dc.data_ptr(), self.xphys.data_ptr(), self.ce.data_ptr(), self.e.data_ptr(),
-                          self.penal, self.emin, 1.0, 0, self._part.data_ptr(), self._scal[0:].data_ptr(), *g.args, st)
+        for k, u in enumerate(self.us):
+            self.ge.strain_energy_device(u, out=self.ce)
+            L.lpb_sensitivity(self.dc.data_ptr(), self.xphys.data_ptr(), self.ce.data_ptr(), self.e.data_ptr(),
+                              self.penal, self.emin, 1.0, int(k > 0), self._part.data_ptr(),
+                              self._scal[8 + k:].data_ptr(), *g.args, st)
         self.filter.apply(self.dcf, self.dc, hs_in=self.filter.hs)
 
     def oc(self):
@@ -489,8 +516,7 @@ class Top3dLoop:
             ev[0].record()
             self.ge.set_moduli_device(self.e)
             ev[1].record()
-            x0 = self.u if (self.warm_start and self.u is not None) else None
-            self.u = self.ge.solve_device(self.f, x0)
+            self._solve_cases()
             ev[2].record()
             self.sensitivities()
             ev[3].record()
@@ -505,7 +531,8 @@ class Top3dLoop:
         self.filter.apply(self.xphys, self.xnew, hs_out=self.filter.hs, e_out=self.e, penal=self.penal,
                           emin=self.emin)
         self.x, self.xnew = self.xnew, self.x
-        c, change = (float(v) for v in self._scal[:2].cpu().numpy())
+        vals = self._scal[:8 + len(self.fs)].cpu().numpy()
+        c, change = float(vals[8:].sum()) if len(self.fs) > 1 else float(vals[8]), float(vals[1])
         self.history.append((c, change, self.ge.last_iters))
         return c, change
 

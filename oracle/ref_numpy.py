@@ -832,8 +832,15 @@ def assembled_solve(ke, e_grid, fixed_grid, f_grid):
 def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, emin=1e-9, move=0.2,
                solve=None):
     """top3d's loop with the density filter (loadpath/benchmarks/reference.py:74-117).
-    Returns (x, xphys, compliance history, change history)."""
-    solve = solve or (lambda e: assembled_solve(ke, e, fixed_grid, f_grid))
+    Returns (x, xphys, compliance history, change history). f_grid may be a list of load cases:
+    the objective is then their equally weighted compliance sum, and its sensitivity the sum of
+    the cases' (the reference's loop has one load; its sums over cases are those of
+    loadpath/simp.py:1901-1904 applied per case). solve(e) returns u, or a list of u per case."""
+    if solve is None:
+        if isinstance(f_grid, (list, tuple)):
+            solve = lambda e: [assembled_solve(ke, e, fixed_grid, fk) for fk in f_grid]
+        else:
+            solve = lambda e: assembled_solve(ke, e, fixed_grid, f_grid)
     taps = filter_taps(rmin)
     hs = filter_row_sums(dims, taps)
     hap = lambda v: grid_filter(v, taps)
@@ -842,10 +849,14 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
     hist_c, hist_ch = [], []
     for _ in range(iters):
         e = simp_moduli(xphys, penal, emin)
-        u = solve(e)
-        g = gather_cells(u, dims).reshape(24, -1)
-        ce = np.einsum("in,in->n", g, ke @ g).reshape(dims)
-        c = float(np.sum(e * ce))
+        us = solve(e)
+        ce = np.zeros(dims)
+        c = 0.0
+        for u in (us if isinstance(us, list) else [us]):
+            g = gather_cells(u, dims).reshape(24, -1)
+            ce_k = np.einsum("in,in->n", g, ke @ g).reshape(dims)
+            c += float(np.sum(e * ce_k))
+            ce += ce_k
         dc = -penal * (1 - emin) * xphys ** (penal - 1) * ce
         dc = hap(dc / hs)
         dv = hap(np.ones(dims) / hs)

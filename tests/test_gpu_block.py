@@ -71,3 +71,22 @@ def test_block_warm_starts_and_zero_column():
         want = ge.solve_device(bs[j], x0s[j])
         assert ge.last_iters == its[j]
         np.testing.assert_array_equal(g.nodes_to_host(xs[j]), g.nodes_to_host(want))
+
+
+def test_load_case_simp_loop_matches_oracle():
+    """The batched load-case SIMP loop (Top3dLoop with a list of loads, solved as one block) against
+    the oracle's top3d loop on the compliance sum, with its direct sparse solves."""
+    from loadpath_b200.simp import Top3dLoop
+    from oracle import ref_numpy as R
+
+    dims = (16, 8, 8)
+    fixed, _ = R.cantilever_bc(dims)
+    loads = _point_loads(dims, 4, 7)
+    iters = 6
+    _, xp_ref, hc, hch = R.top3d_loop(dims, 0.2, 2.0, R.hex8_ke(0.3, "plain"), fixed, loads, iters)
+    loop = Top3dLoop(dims, 0.2, 2.0, fixed, loads, rtol=1e-10, element="plain", coarse_cells=20)
+    got = [loop.step() for _ in range(iters)]
+    np.testing.assert_allclose([c for c, _ in got], hc, rtol=1e-7)
+    np.testing.assert_allclose([ch for _, ch in got], hch, rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(loop.xphys_host(), xp_ref, rtol=1e-6, atol=1e-8)
+    assert len(loop.history[-1][2]) == 4
