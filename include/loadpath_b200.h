@@ -271,6 +271,11 @@ int lpb_graph_free(void* exec);
 int lpb_while_begin(void* stream, long long* handle, void** graph);
 int lpb_while_end(void* stream, void* graph, void** exec);
 int lpb_cg_continue(long long handle, const double* sc, long long* state, double rtol, long long maxiter, void* stream);
+/* The block solve's loop (k columns; sc (k, 8); state (k + 1, 2): per column the iteration it
+ * stopped at and its status, then the iteration count): the loop runs while a column does;
+ * lpb_snapshot_converged writes m x of column col into out in the iteration it converges. */
+int lpb_cg_continue_cols(long long handle, const double* sc, long long* state, int k, double rtol, long long maxiter, void* stream);
+int lpb_snapshot_converged(double* out, const double* x, const uint8_t* mask, const long long* state, int col, int k, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_memcpy_async(void* dst, const void* src, long long bytes, void* stream);
 int lpb_memset_async(void* dst, int value, long long bytes, void* stream);
 

@@ -26,7 +26,48 @@ __global__ void k_cg_continue(cudaGraphConditionalHandle handle, const double* _
   cudaGraphSetConditional(handle, (status == 0 && it < maxiter) ? 1u : 0u);
 }
 
+// The same test for the k columns of a block solve: sc (k, 8) their scalars; state (k + 1, 2):
+// row j the iteration at which column j stopped and its status (0 while it runs), row k the
+// iteration count. The loop continues while a column runs and fewer than maxiter iterations ran.
+__global__ void k_cg_continue_cols(cudaGraphConditionalHandle handle, const double* __restrict__ sc,
+                                   long long* __restrict__ state, int k, double rtol, long long maxiter) {
+  const long long it = state[2 * k] + 1;
+  state[2 * k] = it;
+  bool running = false;
+  for (int j = 0; j < k; ++j) {
+    if (state[2 * j + 1] != 0) continue;
+    const double* s = sc + 8 * j;
+    const double bb = s[0], pap = s[3], rr = s[4];
+    long long status = 0;
+    if (bb == 0.0) status = 2;
+    else if (!(pap > 0.0)) status = 3;
+    else if (sqrt(rr) <= rtol * sqrt(bb)) status = 1;
+    if (status) {
+      state[2 * j] = it;
+      state[2 * j + 1] = status;
+    } else {
+      running = true;
+    }
+  }
+  cudaGraphSetConditional(handle, (running && it < maxiter) ? 1u : 0u);
+}
+
+// out = m x (the solved bits) when column col converged at this iteration (state as above)
+__global__ void k_snapshot_converged(double* __restrict__ out, const double* __restrict__ x,
+                                     const uint8_t* __restrict__ m, const long long* __restrict__ state, int col,
+                                     int k, LpGrid g) {
+  if (state[2 * col + 1] != 1 || state[2 * col] != state[2 * k]) return;
+  const long long nn = g.nodes_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / nn);
+    out[t] = ((m[t - c * nn] >> c) & 1) ? x[t] : 0.0;
+  }
+}
+
 }  // namespace
+
+#define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
+#define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
 
 extern "C" {
 
@@ -124,6 +165,25 @@ int lpb_memset_async(void* dst, int value, long long bytes, void* stream) {
 int lpb_graph_free(void* exec) {
   if (!exec) return LP_OK;
   return cudaGraphExecDestroy((cudaGraphExec_t)exec) == cudaSuccess ? LP_OK : LP_ERR_LAUNCH;
+}
+
+// the block solve's test: k columns, sc (k, 8), state (k + 1, 2) zeroed before the loop
+int lpb_cg_continue_cols(long long handle, const double* sc, long long* state, int k, double rtol, long long maxiter,
+                         void* stream) {
+  if (!sc || !state || k < 1 || maxiter < 1) return LP_ERR_ARG;
+  k_cg_continue_cols<<<1, 1, 0, LP_ST>>>((cudaGraphConditionalHandle)handle, sc, state, k, rtol, maxiter);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// out = m x if column col of a block solve converged at the current iteration (else nothing)
+int lpb_snapshot_converged(double* out, const double* x, const uint8_t* mask, const long long* state, int col, int k,
+                           LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !out || !x || !mask || !state || col < 0 || col >= k || out == x) return LP_ERR_ARG;
+  k_snapshot_converged<<<lp_blocks(3 * g.nodes_padded(), 256), 256, 0, LP_ST>>>(out, x, mask, state, col, k, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
 }
 
 }  // extern "C"

@@ -1148,9 +1148,17 @@ class GridElasticity:
         """k node fields of a level as one (k, field) tensor; [j] is column j's field."""
         return self._tbuf(key, (k, 3, grid.pz // 4, grid.NY, grid.NX, 4), dtype)
 
+    def _tbuf_host(self, key, shape, dtype):
+        """A persistent pinned host buffer (for copies a solve makes once)."""
+        t = self._work.get(key)
+        if t is None or t.dtype != dtype or tuple(t.shape) != tuple(shape):
+            t = torch.zeros(tuple(shape), dtype=dtype, pin_memory=True)
+            self._work[key] = t
+        return t
+
     def _block_buffers(self, k):
         g = self.g0
-        bufs = {key: self._blk(f"bcg_{key}", k, g, torch.float64) for key in ("x", "r", "p", "ap", "rs", "b")}
+        bufs = {key: self._blk(f"bcg_{key}", k, g, torch.float64) for key in ("x", "r", "p", "ap", "rs", "b", "snap")}
         for i in range(len(self.levels)):
             lv = self._op(i)
             self._blk(f"bx{i}", k, lv.grid, self.tdtype)
@@ -1270,14 +1278,15 @@ class GridElasticity:
                         L.lpb_memcpy_async(p[j].data_ptr(), z[j].data_ptr(), nb, st)
                     dot(r[j], p[j], sc[j][1])
 
-            def head():
+            def head(to_host=True):
                 st = stream_handle()
                 for j in range(k):
                     s = sc[j]
                     a.apply_dot(ap[j], p[j], self._part, s[3])
                     L.lpb_cg_step_r(r[j].data_ptr(), ap[j].data_ptr(), bb0[j].data_ptr() if f32 else None, n,
                                     s[1].data_ptr(), s[3].data_ptr(), self._part.data_ptr(), s[4].data_ptr(), st)
-                L.lpb_memcpy_async(host.data_ptr(), sc.data_ptr(), 8 * 8 * k, st)
+                if to_host:
+                    L.lpb_memcpy_async(host.data_ptr(), sc.data_ptr(), 8 * 8 * k, st)
 
             def tail():
                 st = stream_handle()
@@ -1296,6 +1305,49 @@ class GridElasticity:
                     L.lpb_memcpy_async(s[1].data_ptr(), s[2].data_ptr(), 8, st)
 
             graphed = self.use_graphs and self.maxiter > 1
+            if graphed and self.device_loop:
+                # the loop on the device (as in _pcg_device): per iteration every column's head,
+                # the columns' stopping test, every tail, and the masked copy of each column that
+                # converged in this iteration
+                st = stream_handle()
+                state = self._tbuf("bloop_state", (k + 1, 2), torch.int64)
+                rtol, maxiter = float(self.rtol), int(self.maxiter)
+                mk = a.mask.data_ptr()
+
+                snap = B["snap"]
+
+                def body(handle):
+                    stb = stream_handle()
+                    head(to_host=False)
+                    L.lpb_cg_continue_cols(handle, sc.data_ptr(), state.data_ptr(), k, rtol, maxiter, stb)
+                    tail()
+                    for j in range(k):
+                        L.lpb_snapshot_converged(snap[j].data_ptr(), x[j].data_ptr(), mk, state.data_ptr(), j, k,
+                                                 *g.args, stb)
+
+                g_pre = self._graph(("bpre", k, warm), pre)
+                g_loop = self._graph(("bloop", k, rtol, maxiter), body, loop=True)
+                L.lpb_memset_async(state.data_ptr(), 0, state.numel() * 8, st)
+                self._replay(g_pre)
+                self._replay(g_loop)
+                hs = self._tbuf_host("bloop_host", (k + 1, 2), torch.int64)
+                L.lpb_memcpy_async(hs.data_ptr(), state.data_ptr(), state.numel() * 8, st)
+                torch.cuda.current_stream().synchronize()
+                sv = hs.numpy().copy()
+                it_all = int(sv[k, 0])
+                add_launches(g_loop[2] * (it_all - 1))
+                iters, ok = [], []
+                for j in range(k):
+                    done_at, status = int(sv[j, 0]), int(sv[j, 1])
+                    if status == 2:
+                        L.lpb_memset_async(outs[j].data_ptr(), 0, nb, st)
+                        iters.append(0)
+                    else:
+                        if status == 1:
+                            L.lpb_memcpy_async(outs[j].data_ptr(), snap[j].data_ptr(), nb, st)
+                        iters.append(done_at if status else self.maxiter)
+                    ok.append(status in (1, 2))
+                return iters, ok
             if graphed:
                 g_pre = self._graph(("bpre", k, warm), pre)
                 g_head = self._graph(("bhead", k), head)
