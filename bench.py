@@ -32,6 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 DIMS = (256, 128, 128)
 CASE_DIMS = (192, 96, 96)
+FULL_DIMS = (384, 192, 192)
 VOLFRAC, RMIN, RTOL, PENAL, EMIN, MOVE = 0.3, 2.0, 1e-6, 3.0, 1e-9, 0.2
 METRIC = "SIMP iter/s & K*u GB/s at 12.7M DOF: mixed-prec vs FP64 GPU, <=1e-6 rel err"
 
@@ -46,12 +47,15 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--micro", choices=["apply", "band", "cases"], default=None,
+    p.add_argument("--micro", choices=["apply", "band", "cases", "full"], default=None,
                    help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
                         "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
                         "coarsest level's band assembly, factorisation and inverse; cases: the batched "
                         "load-case SIMP iteration (8 point loads at 192x96x96 unless --dims is given), "
-                        "the cases solved as one block and one after another")
+                        "the cases solved as one block and one after another; full: the full-scale MMA "
+                        "SIMP run (384x192x192 unless --dims is given, --iters iterations) in mixed "
+                        "precision and on the plain FP64 GPU path, final compliance and design compared")
+    p.add_argument("--iters", type=int, default=100, help="SIMP iterations of --micro full")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--kernels", type=int, default=0, metavar="N",
                    help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
@@ -60,6 +64,8 @@ def parse():
     a.warmup = max(a.warmup, 3)
     if a.micro == "cases" and a.dims == ",".join(str(d) for d in DIMS):
         a.dims = CASE_DIMS
+    if a.micro == "full" and a.dims == ",".join(str(d) for d in DIMS):
+        a.dims = FULL_DIMS
     a.dims = tuple(int(v) for v in a.dims.split(",")) if isinstance(a.dims, str) else a.dims
     return a
 
@@ -608,6 +614,48 @@ def run_micro_cases(args):
     return 0
 
 
+def run_micro_full(args):
+    """The full-scale SIMP run: cantilever, uniform start at volume fraction 0.25, filter r = 3,
+    penalty ramped 1 -> 3 over 20 iterations, MMA, sensitivities from the autograd path; the same
+    run in mixed precision (rtol 1e-6) and on the plain FP64 GPU path, CUDA-event timed, with the
+    final compliance and filtered design compared."""
+    import torch
+
+    from loadpath_b200.optimize import MMALoop
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    fixed, f = cantilever(dims)
+    out, designs = {}, {}
+    for name, dtype in (("mixed", np.float32), ("fp64", np.float64)):
+        loop = MMALoop(dims, 0.25, 3.0, fixed, f, penal=3.0, penal0=1.0, ramp=20, rtol=RTOL, dtype=dtype)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record()
+        loop.run(args.iters)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / args.iters
+        h = loop.history
+        out[name] = {"simp_iter_per_s": 1e3 / ms, "ms_per_iteration": ms, "final_compliance": h[-1][0],
+                     "final_volume_fraction": h[-1][1], "final_change": h[-1][2],
+                     "cg_iterations_total": int(sum(r[4] for r in h)), "levels": len(loop.problem.ge.levels),
+                     "compliance_every_10": [h[i][0] for i in range(0, len(h), 10)]}
+        designs[name] = loop.problem.xphys.clone()
+        del loop
+        torch.cuda.empty_cache()
+    a, b = designs["mixed"], designs["fp64"]
+    print(json.dumps({"micro": "full-scale MMA SIMP", "dims": list(dims), "iterations": args.iters,
+                      "dtype": "f32+f64", "data": "synthetic (uniform start, cantilever)",
+                      "mixed_over_fp64": out["mixed"]["simp_iter_per_s"] / out["fp64"]["simp_iter_per_s"],
+                      "rel_err_vs_fp64_path": {
+                          "compliance": abs(out["mixed"]["final_compliance"] - out["fp64"]["final_compliance"])
+                          / abs(out["fp64"]["final_compliance"]),
+                          "design_max_abs": float((a - b).abs().max()),
+                          "design_l2": float((a - b).norm() / b.norm())}, **out}))
+    return 0
+
+
 def run_kernels(args):
     """Per-kernel device time of args.kernels SIMP iterations after args.warmup, from the CUDA
     activity records (CUPTI through torch.profiler: kernels are not serialised)."""
@@ -666,6 +714,8 @@ def main():
         return run_micro_band(args)
     if args.micro == "cases":
         return run_micro_cases(args)
+    if args.micro == "full":
+        return run_micro_full(args)
     if args.kernels:
         return run_kernels(args)
     if args.impl == "reference":

@@ -342,11 +342,15 @@ static MVec mvec(const double* h, int m) {
 
 extern "C" {
 
-// part: scratch of at least lpb_mma_part_len(m) doubles
+// part: scratch of at least lpb_mma_part_len(m) doubles: LP_MMA_BLOCKS partials for each value
+// of the widest reduction any pass makes (prepare M, newton_a 2M + M(M+1)/2, newton_b 4,
+// trial 2 + M, M = m rounded up to 1, 2, 4 or 8)
 long long lpb_mma_part_len(int m) {
   const int M = mma_m_template(m);
-  const int K = 2 * M + M * (M + 1) / 2;
-  return (long long)(K > 2 + M ? K : 2 + M) * LP_MMA_BLOCKS;
+  int K = 2 * M + M * (M + 1) / 2;
+  if (K < 4) K = 4;
+  if (K < 2 + M) K = 2 + M;
+  return (long long)K * LP_MMA_BLOCKS;
 }
 
 int lpb_mma_prepare(long long n, int m, double* x, const double* xmin, const double* xmax, double* low, double* upp,

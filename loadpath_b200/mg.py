@@ -319,7 +319,12 @@ class GridElasticity:
         self._info_host = torch.zeros(2, dtype=torch.int32, pin_memory=True)
         self._pw = torch.zeros(32 * 32, dtype=torch.float64, device=self.device)
         self._coef = torch.zeros(16 * 32, dtype=torch.float64, device=self.device)
-        self._part = torch.zeros(max(lib().lpb_reduce_blocks(), 1024) * 2, dtype=torch.float64, device=self.device)
+        # reduction partials: the vector kernels' blocks, and one per block of the fine float64
+        # apply with p . A p (15 x 15 node columns by z segments of at least two chunks)
+        g0 = self.g0
+        fine_blocks = ((g0.NX + 14) // 15) * ((g0.NY + 14) // 15) * (g0.pz // 4)
+        self._part = torch.zeros(max(lib().lpb_reduce_blocks() * 2, 2048, fine_blocks), dtype=torch.float64,
+                                 device=self.device)
         self._host = torch.zeros(8, dtype=torch.float64, pin_memory=True)
         # the device-side CG loop: its stopping test's state (iterations, status) and its copy
         self._loop_state = torch.zeros(2, dtype=torch.int64, device=self.device)

@@ -1002,6 +1002,41 @@ class MMA:
         return x
 
 
+
+def mma_simp_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, penal0=1.0, ramp=20,
+                  move=0.2, emin=1e-9, solve=None):
+    """SIMP with the MMA update (m = 1, volume of the filtered design), the penalty ramped from
+    penal0 to penal over `ramp` iterations and the objective scaled by the first compliance: the
+    sensitivities of loadpath/simp.py:1901-1904 chained through the filter (loadpath/simp.py:2001),
+    one MMA step per iteration (loadpath/mma.py:57-112). Returns (x, xphys, history) with history
+    rows (compliance, volume fraction, change)."""
+    solve = solve or (lambda e: assembled_solve(ke, e, fixed_grid, f_grid))
+    taps = filter_taps(rmin)
+    hs = filter_row_sums(dims, taps)
+    hap = lambda v: grid_filter(v, taps)
+    n = int(np.prod(dims))
+    x = np.full(dims, volfrac)
+    dg = (hap(np.ones(dims) / hs) / (n * volfrac)).reshape(1, -1)
+    opt = MMA(n, 1, 0.0, 1.0, move)
+    c0 = None
+    hist = []
+    for k in range(iters):
+        p = penal0 + (penal - penal0) * min(k, ramp) / ramp
+        xphys = hap(x) / hs
+        e = simp_moduli(xphys, p, emin)
+        u = solve(e)
+        g = gather_cells(u, dims).reshape(24, -1)
+        ce = np.einsum("in,in->n", g, ke @ g).reshape(dims)
+        c = float(np.sum(e * ce))
+        dc = hap(-p * (1 - emin) * xphys ** (p - 1) * ce / hs)
+        c0 = c0 if c0 is not None else (abs(c) if c != 0 else 1.0)
+        vol = float(xphys.sum()) / n
+        xnew = opt.update(x.reshape(-1), c / c0, dc.reshape(-1) / c0, np.array([vol / volfrac - 1.0]), dg)
+        xnew = np.asarray(xnew).reshape(dims)
+        hist.append((c, vol, float(np.abs(xnew - x).max())))
+        x = xnew
+    return x, hap(x) / hs, hist
+
 # --------------------------------------------------------------------------
 # problem builders shared by the tests and the CPU baseline
 # --------------------------------------------------------------------------

@@ -73,3 +73,15 @@ def test_band_layout_host_only():
         nt, d = (n + 31) // 32, (bw + 31) // 32
         assert tuple(int(v) for v in out) == (n, nt, d, bw)
         assert ntiles == nt * (d + 1)
+
+
+def test_mma_scratch_covers_every_reduction():
+    """lpb_mma_part_len(m) holds 592 partials for each value of the widest reduction the MMA's
+    passes make (prepare M, newton_a 2M + M(M+1)/2, newton_b 4, trial 2 + M): the m = 1 size once
+    missed newton_b's four maxima and its partials overran the buffer."""
+    from loadpath_b200._lib import lib
+
+    for m in range(1, 9):
+        M = 1 if m <= 1 else 2 if m <= 2 else 4 if m <= 4 else 8
+        need = 592 * max(M, 2 * M + M * (M + 1) // 2, 4, 2 + M)
+        assert lib().lpb_mma_part_len(m) >= need
