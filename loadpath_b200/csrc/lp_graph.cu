@@ -59,7 +59,7 @@ __global__ void k_snapshot_converged(double* __restrict__ out, const double* __r
   if (state[2 * col + 1] != 1 || state[2 * col] != state[2 * k]) return;
   const long long nn = g.nodes_padded();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t / nn);
+    const int c = t >= nn ? (t >= 2 * nn ? 2 : 1) : 0;
     out[t] = ((m[t - c * nn] >> c) & 1) ? x[t] : 0.0;
   }
 }

@@ -388,15 +388,23 @@ __global__ void k_prolong4(T* __restrict__ xf, const T* __restrict__ xc, const u
   }
 }
 
-// out = u * mask (per component bit)
+// out = u * mask (per component bit); four nodes per step (the padded node count is a multiple
+// of 4), the component found by comparison, not by a 64-bit division
 template <typename T>
 __global__ void k_mask_field(T* __restrict__ out, const T* __restrict__ u, const uint8_t* __restrict__ m, LpGrid g,
                              int bitshift) {
-  const long long nn = g.nodes_padded();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
-    int c = (int)(t / nn);
-    long long n = t - c * nn;
-    out[t] = ((m[n] >> (c + bitshift)) & 1) ? u[t] : T(0);
+  const long long nq = g.nodes_padded() >> 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3 * nq; i += (long long)gridDim.x * blockDim.x) {
+    const int c = i >= nq ? (i >= 2 * nq ? 2 : 1) : 0;
+    const uchar4 mb = reinterpret_cast<const uchar4*>(m)[i - c * nq];
+    const int sh = c + bitshift;
+    T v[4];
+    V4ld<T>::ld(u + 4 * i, v);
+    if (!((mb.x >> sh) & 1)) v[0] = T(0);
+    if (!((mb.y >> sh) & 1)) v[1] = T(0);
+    if (!((mb.z >> sh) & 1)) v[2] = T(0);
+    if (!((mb.w >> sh) & 1)) v[3] = T(0);
+    V4ld<T>::st(out + 4 * i, v);
   }
 }
 
@@ -411,14 +419,21 @@ __global__ void k_scale_rsqrt(T* __restrict__ v, long long n, const double* __re
   (void)f;
 }
 
-// av = dinv * av * mask
+// av = dinv * av * mask, four nodes per step as k_mask_field
 template <typename T>
 __global__ void k_dinv_mask(T* __restrict__ av, const T* __restrict__ dinv, const uint8_t* __restrict__ m, LpGrid g) {
-  const long long nn = g.nodes_padded();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * nn; t += (long long)gridDim.x * blockDim.x) {
-    int c = (int)(t / nn);
-    long long n = t - c * nn;
-    av[t] = ((m[n] >> c) & 1) ? dinv[t] * av[t] : T(0);
+  const long long nq = g.nodes_padded() >> 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3 * nq; i += (long long)gridDim.x * blockDim.x) {
+    const int c = i >= nq ? (i >= 2 * nq ? 2 : 1) : 0;
+    const uchar4 mb = reinterpret_cast<const uchar4*>(m)[i - c * nq];
+    T v[4], d[4];
+    V4ld<T>::ld(av + 4 * i, v);
+    V4ld<T>::ld(dinv + 4 * i, d);
+    v[0] = ((mb.x >> c) & 1) ? d[0] * v[0] : T(0);
+    v[1] = ((mb.y >> c) & 1) ? d[1] * v[1] : T(0);
+    v[2] = ((mb.z >> c) & 1) ? d[2] * v[2] : T(0);
+    v[3] = ((mb.w >> c) & 1) ? d[3] * v[3] : T(0);
+    V4ld<T>::st(av + 4 * i, v);
   }
 }
 
@@ -740,7 +755,7 @@ int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const ui
 int lpb_mask_field_f32(float* out, const float* u, const uint8_t* m, LP_GRID_ARGS, int bitshift, void* stream) {
   LpGrid g = LP_GRID;
   long long n = 3 * g.nodes_padded();
-  k_mask_field<float><<<LP_VEC_GRID(n)>>>(out, u, m, g, bitshift);
+  k_mask_field<float><<<LP_VEC_GRID(n / 4)>>>(out, u, m, g, bitshift);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -748,7 +763,7 @@ int lpb_mask_field_f32(float* out, const float* u, const uint8_t* m, LP_GRID_ARG
 int lpb_mask_field_f64(double* out, const double* u, const uint8_t* m, LP_GRID_ARGS, int bitshift, void* stream) {
   LpGrid g = LP_GRID;
   long long n = 3 * g.nodes_padded();
-  k_mask_field<double><<<LP_VEC_GRID(n)>>>(out, u, m, g, bitshift);
+  k_mask_field<double><<<LP_VEC_GRID(n / 4)>>>(out, u, m, g, bitshift);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -768,7 +783,7 @@ int lpb_scale_rsqrt_f64(double* v, long long n, const double* nrm2, void* stream
 int lpb_dinv_mask_f32(float* av, const float* dinv, const uint8_t* m, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   long long n = 3 * g.nodes_padded();
-  k_dinv_mask<float><<<LP_VEC_GRID(n)>>>(av, dinv, m, g);
+  k_dinv_mask<float><<<LP_VEC_GRID(n / 4)>>>(av, dinv, m, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -776,7 +791,7 @@ int lpb_dinv_mask_f32(float* av, const float* dinv, const uint8_t* m, LP_GRID_AR
 int lpb_dinv_mask_f64(double* av, const double* dinv, const uint8_t* m, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   long long n = 3 * g.nodes_padded();
-  k_dinv_mask<double><<<LP_VEC_GRID(n)>>>(av, dinv, m, g);
+  k_dinv_mask<double><<<LP_VEC_GRID(n / 4)>>>(av, dinv, m, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -340,6 +340,10 @@ class GridElasticity:
         self._side = torch.cuda.Stream(device=self.device, priority=-1)   # coarsest factorisation
         self._ev_fork = torch.cuda.Event()
         self._ev_join = torch.cuda.Event()
+        self._pw_stream = torch.cuda.Stream(device=self.device)             # coarse power iterations
+        self._ev_pw_fork = torch.cuda.Event()
+        self._ev_pw_join = torch.cuda.Event()
+        self._part_pw = torch.zeros(lib().lpb_reduce_blocks() * 2, dtype=torch.float64, device=self.device)
         self._joined = True
 
     # --- layout conversion (loadpath/mg.py:495-511) -----------------------------------
@@ -496,8 +500,7 @@ class GridElasticity:
         self.levels = levels
         self._l0s = l0s
         info = self._build_coarse(levels[-1])
-        for i in range(len(levels)):
-            self._estimate_lmax(i)
+        self._all_lmax(len(levels))
         self._join_coarse()
         if plan is None:
             if info is not None:
@@ -705,16 +708,12 @@ class GridElasticity:
     def _op(self, i):
         return self._l0s if i == 0 else self.levels[i]
 
-    def _estimate_lmax(self, i, its=12):
-        """Largest eigenvalue of D^-1 A by power iteration, times 1.3, and the Chebyshev
-        coefficients from it, all on the device (loadpath/mg.py:771-794). The vector is
-        warm-started from the last hierarchy's, as the reference does."""
-        L = lib()
-        st = stream_handle()
+    def _lmax_vectors(self, i):
+        """The power iteration's buffers of level i; the start vector is drawn once per level
+        shape and then warm-started from the last hierarchy's, as the reference does."""
         lv = self._op(i)
         g = lv.grid
         dt = lv.dtype
-        sfx = "f32" if dt == torch.float32 else "f64"
         v = self._buf(f"pw_v{i}", g, dt)
         av = self._buf(f"pw_av{i}", g, dt)
         keep = self._buf(f"pw_keep{i}", g, dt)
@@ -723,23 +722,62 @@ class GridElasticity:
             host = (rng.random(lv.node_shape) - 0.5).astype(np.float32 if dt == torch.float32 else np.float64)
             g.nodes_to_dev(host, dt, out=keep)
             self._lmax_init[i] = (tuple(keep.shape), dt)
+        return v, av, keep
+
+    def _estimate_lmax(self, i, its=12, part=None):
+        """Largest eigenvalue of D^-1 A by power iteration, times 1.3, and the Chebyshev
+        coefficients from it, all on the device (loadpath/mg.py:771-794). Launches only (the
+        buffers come from _lmax_vectors), so a level's iterations can be one graph."""
+        L = lib()
+        st = stream_handle()
+        part = self._part if part is None else part
+        lv = self._op(i)
+        g = lv.grid
+        dt = lv.dtype
+        sfx = "f32" if dt == torch.float32 else "f64"
+        v, av, keep = self._lmax_vectors(i)
         getattr(L, f"lpb_mask_field_{sfx}")(v.data_ptr(), keep.data_ptr(), lv.mask.data_ptr(), *g.args, 0, st)
         n = g.n_node_field
         pw = self._pw[32 * i:32 * (i + 1)]
         for it in range(its):
-            getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), v.data_ptr(), n, self._part.data_ptr(),
+            getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), v.data_ptr(), n, part.data_ptr(),
                                          pw[it:].data_ptr(), st)
             getattr(L, f"lpb_scale_rsqrt_{sfx}")(v.data_ptr(), n, pw[it:].data_ptr(), st)
             lv.apply(av, v)
             getattr(L, f"lpb_dinv_mask_{sfx}")(av.data_ptr(), lv.dinv.data_ptr(), lv.mask.data_ptr(), *g.args, st)
-            getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), av.data_ptr(), n, self._part.data_ptr(),
+            getattr(L, f"lpb_dot_{sfx}")(v.data_ptr(), av.data_ptr(), n, part.data_ptr(),
                                          pw[16 + it:].data_ptr(), st)
             v, av = av, v
         # the final vector is kept for the next hierarchy (already masked)
         getattr(L, f"lpb_mask_field_{sfx}")(keep.data_ptr(), v.data_ptr(), lv.mask.data_ptr(), *g.args, 0, st)
-        lv.coef = self._coef[16 * i:16 * (i + 1)]
-        L.lpb_cheb_coef(lv.coef.data_ptr(), pw.data_ptr(), pw[16:].data_ptr(), its, max(self.degree, 1),
-                        LMAX_SAFETY, st)
+        L.lpb_cheb_coef(self._coef[16 * i:].data_ptr(), pw.data_ptr(), pw[16:].data_ptr(), its,
+                        max(self.degree, 1), LMAX_SAFETY, st)
+
+    def _all_lmax(self, nl):
+        """λmax of every level. The levels are independent: the fine two run on the working
+        stream, the coarse ones (chains of small kernels) on a stream of their own beside them;
+        with graphs on, each level's twelve iterations are one graph launch."""
+        for i in range(nl):
+            self._op(i).coef = self._coef[16 * i:16 * (i + 1)]
+            self._lmax_vectors(i)
+
+        def run(i, part):
+            if self.use_graphs:
+                self._replay(self._graph(("lmax", i, nl), lambda: self._estimate_lmax(i, part=part)))
+            else:
+                self._estimate_lmax(i, part=part)
+
+        if nl > 2:
+            self._ev_pw_fork.record()
+        for i in range(min(nl, 2)):
+            run(i, self._part)
+        if nl > 2:
+            with torch.cuda.stream(self._pw_stream):
+                self._pw_stream.wait_event(self._ev_pw_fork)
+                for i in range(2, nl):
+                    run(i, self._part_pw)
+                self._ev_pw_join.record()
+            torch.cuda.current_stream().wait_event(self._ev_pw_join)
 
     # --- V-cycle (loadpath/mg.py:796-864) -----------------------------------------------
     def _smooth(self, i, b, x, from_zero):
@@ -886,6 +924,7 @@ class GridElasticity:
         sig = (self._gen, id(probe))
         if cache.get("sig") != sig:
             self._free_graphs()
+            cache = self._gcache          # the new, empty cache
             cache["sig"] = sig
         if key not in cache:
             pairs = []

@@ -58,3 +58,45 @@ def test_oc_bisection_plateaus_and_ties():
         want, _ = _plain(vol, target)
         got, _ = oc_bisection(lambda cands: [vol(c) for c in cands], target)
         assert got == want
+
+
+def test_graph_cache_keeps_graphs_across_calls(monkeypatch):
+    """GridElasticity._graph captures a key once per buffer generation: a second call with the
+    same key and generation reuses the first capture (no GPU: capture and free are stubbed)."""
+    import loadpath_b200.mg as mg
+
+    class FakeLib:
+        def __init__(self):
+            self.captured = 0
+            self.freed = 0
+
+        def lpb_capture_begin(self, st):
+            self.captured += 1
+
+        def lpb_capture_end(self, st, out):
+            out._obj.value = 1000 + self.captured
+
+        def lpb_graph_free(self, g):
+            self.freed += 1
+
+    fake = FakeLib()
+    monkeypatch.setattr(mg, "lib", lambda: fake)
+    monkeypatch.setattr(mg, "stream_handle", lambda: 0)
+
+    class Stream:
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *a):
+            return False
+
+    monkeypatch.setattr(mg.torch.cuda, "stream", lambda s: Stream())
+    monkeypatch.setattr(mg.torch.cuda, "current_stream", lambda: type("S", (), {"synchronize": lambda self: None})())
+    ge = object.__new__(mg.GridElasticity)
+    ge._gcache, ge._gen, ge._cap_stream = {}, 0, None
+    a = ge._graph("head", lambda: None)
+    b = ge._graph("head", lambda: None)
+    assert fake.captured == 1 and a is b
+    ge._gen += 1                               # a buffer was replaced: the graphs go
+    ge._graph("head", lambda: None)
+    assert fake.captured == 2 and fake.freed == 1
