@@ -268,6 +268,13 @@ int lpb_graph_free(void* exec);
  * the stream, lpb_while_end instantiates it (an exec for lpb_graph_launch); the body's
  * lpb_cg_continue (sc: the PCG scalars, [0] |b|^2, [3] p.Ap, [4] |r|^2; state: iterations,
  * status) ends the loop once |r| <= rtol |b|, p.Ap <= 0, b = 0 or maxiter iterations ran. */
+/* Launch-geometry tuning (no reference counterpart): the z-segment length, in chunks of four
+ * planes, of the fine float32 (knob 1) and float64 (2) apply and of the level-1 float32 (3) and
+ * float64 (4) apply, per grid of nx x ny x nz cells; 0 clears it (the launcher's cost model
+ * decides). Set by loadpath_b200.tune from timed candidates; results are the same operator, the
+ * last bit of a float32 sum can differ at segment boundaries. */
+int lpb_tune_set(int knob, int nx, int ny, int nz, int value);
+int lpb_tune_get(int knob, int nx, int ny, int nz);
 int lpb_while_begin(void* stream, long long* handle, void** graph);
 int lpb_while_end(void* stream, void* graph, void** exec);
 int lpb_cg_continue(long long handle, const double* sc, long long* state, double rtol, long long maxiter, void* stream);

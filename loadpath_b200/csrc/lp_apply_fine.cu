@@ -763,6 +763,8 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
     const double cost = (double)waves * (zch + (nseg > 1 ? 0.3 : 0.0));
     if (cost < best - 1e-9) { best = cost; best_zch = zch; }
   }
+  const int tuned = lp_tune_lookup(sizeof(T) == 4 ? LP_KNOB_FINE_F32 : LP_KNOB_FINE_F64, g.nx, g.ny, g.nz);
+  if (tuned >= 2 && tuned <= nchunks) best_zch = tuned;
   const int nseg = (nchunks + best_zch - 1) / best_zch;
   dim3 grid(gx, gy, nseg);
   if constexpr (sizeof(T) == 4) {

@@ -804,7 +804,9 @@ __global__ void __launch_bounds__(128) k_pack_modal(float* __restrict__ km, int*
     const bool general = off > tol * amax;
     for (int p = lane; p < MODAL_UP; p += 32) {
       const int r = c_mup_r[p], c = c_mup_c[p];
-      km[(long long)p * ncp + cell] = general ? 0.0f : (float)(0.5 * (K[r * 24 + c] + K[c * 24 + r]));
+      // a listed cell's entries are zero, its entry 0 a NaN marker the apply skips it by
+      km[(long long)p * ncp + cell] =
+          general ? (p == 0 ? __int_as_float(0x7fc00001) : 0.0f) : (float)(0.5 * (K[r * 24 + c] + K[c * 24 + r]));
     }
     if (general) {   // listed: the node-basis symmetric part, cell-major, at the cell's slot
       int slot = 0;
@@ -849,14 +851,14 @@ __device__ __forceinline__ void walsh8(float (&a)[8]) {
 }
 
 // ft (24, cells) = T^T (K^ (T u_c)) for every cell (listed cells are rewritten afterwards)
-__global__ void __launch_bounds__(128, 4) k_modal_cells(float* __restrict__ ft, const float* __restrict__ u,
-                                                       const float* __restrict__ km, LpGrid g) {
+__device__ __forceinline__ void modal_cell(float* __restrict__ ft, const float* __restrict__ u,
+                                           const float* __restrict__ km, const LpGrid& g, long long t) {
   const long long ncp = g.cells_padded();
   const long long cs = g.comp_stride();
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= ncp) return;
   int x, y, z;
   if (!g.cell_at(t, x, y, z)) return;
+  if (isnan(__ldg(km + t))) return;                // a listed cell (its entry 0 holds the marker)
   const long long n0 = g.node(x, y, z);
   const long long oy = 4LL * g.NX(), oz = (z & 3) == 3 ? g.node_zc_stride() - 3 : 1;
   constexpr int MUP_R[MODAL_UP] = MUP_ROWS;
@@ -894,16 +896,15 @@ __global__ void __launch_bounds__(128, 4) k_modal_cells(float* __restrict__ ft, 
 
 // the listed cells from their node-basis entries (kpc: 300 per listed cell, cell-major): one warp
 // per cell, its 300 entries and 24 corner values staged in shared memory, lane r < 24 forms row r
-__global__ void __launch_bounds__(128) k_listed_cells(float* __restrict__ ft, const float* __restrict__ u,
-                                                      const float* __restrict__ kpc, const int* __restrict__ glist,
-                                                      const int* __restrict__ gcount, LpGrid g) {
-  __shared__ float sk[4][300];
-  __shared__ float su[4][24];
+__device__ __forceinline__ void listed_cells(float* __restrict__ ft, const float* __restrict__ u,
+                                             const float* __restrict__ kpc, const int* __restrict__ glist,
+                                             const int* __restrict__ gcount, const LpGrid& g, int block, int nblocks,
+                                             float (*sk)[300], float (*su)[24]) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long long ncp = g.cells_padded();
   const long long cs = g.comp_stride();
   const int cnt = *gcount;
-  for (int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; slot < cnt; slot += (gridDim.x * blockDim.x) >> 5) {
+  for (int slot = (block * blockDim.x + threadIdx.x) >> 5; slot < cnt; slot += (nblocks * blockDim.x) >> 5) {
     const long long c = glist[slot];
     int x, y, z;
     g.cell_at(c, x, y, z);
@@ -923,6 +924,23 @@ __global__ void __launch_bounds__(128) k_listed_cells(float* __restrict__ ft, co
       ft[(long long)lane * ncp + c] = f;
     }
     __syncwarp();
+  }
+}
+
+// the cell rows of an explicit level in one launch: blocks below modal_blocks apply the modal
+// form to one cell per thread (listed cells skipped), the blocks past them the listed cells
+__global__ void __launch_bounds__(128, 4) k_explicit_modal_cells(float* __restrict__ ft, const float* __restrict__ u,
+                                                                const float* __restrict__ km,
+                                                                const float* __restrict__ kpc,
+                                                                const int* __restrict__ glist,
+                                                                const int* __restrict__ gcount, LpGrid g,
+                                                                int modal_blocks) {
+  __shared__ float sk[4][300];
+  __shared__ float su[4][24];
+  if ((int)blockIdx.x < modal_blocks) {
+    modal_cell(ft, u, km, g, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  } else {
+    listed_cells(ft, u, kpc, glist, gcount, g, blockIdx.x - modal_blocks, gridDim.x - modal_blocks, sk, su);
   }
 }
 
@@ -1016,6 +1034,8 @@ static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, c
     const double cost = (double)((units + slots - 1) / slots) * (zch + (nseg > 1 ? 0.3 : 0.0));
     if (cost < bc - 1e-9) { bc = cost; best = zch; }
   }
+  const int tuned = lp_tune_lookup(sizeof(T) == 4 ? LP_KNOB_L1_F32 : LP_KNOB_L1_F64, g.nx, g.ny, g.nz);
+  if (tuned >= 1 && tuned <= nchunks) best = tuned;
   dim3 grid(gx, gy, (nchunks + best - 1) / best);
   k_weights_tma<T><<<grid, TXC * TYC, smem, st>>>(maps, wc, mask, gc, g, best, nchunks, err);
   if (pid && pk && pbox && pbox[3] > 0 && pbox[4] > 0 && pbox[5] > 0) {
@@ -1200,8 +1220,8 @@ int lpb_apply_explicit_modal_f32(float* out, const float* u, const float* km, co
                                  const int* gcount, float* ft, const uint8_t* mask, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !out || !u || !km || !kpc || !glist || !gcount || !ft || !mask || out == u) return LP_ERR_ARG;
-  k_modal_cells<<<lp_blocks(g.cells_padded(), 128), 128, 0, LP_ST>>>(ft, u, km, g);
-  k_listed_cells<<<148 * 4, 128, 0, LP_ST>>>(ft, u, kpc, glist, gcount, g);
+  const int modal_blocks = lp_blocks(g.cells_padded(), 128);
+  k_explicit_modal_cells<<<modal_blocks + 148, 128, 0, LP_ST>>>(ft, u, km, kpc, glist, gcount, g, modal_blocks);
   k_explicit_gather<float><<<lp_blocks(g.nodes_padded(), 256), 256, 0, LP_ST>>>(out, ft, mask, g);
   LP_LAUNCH_CHECK();
   return LP_OK;

@@ -69,6 +69,12 @@ static inline bool lp_grid_ok(const LpGrid& g) {
          g.cpz % 4 == 0;
 }
 
+// Launch-geometry tuning table (lp_graph.cu): a value set for (knob, grid) by lpb_tune_set, or 0
+// when none is (the launcher's own cost model then decides). Knobs: the z-segment length in
+// chunks of the fine float32 / float64 apply and of the level-1 float32 / float64 apply.
+enum { LP_KNOB_FINE_F32 = 1, LP_KNOB_FINE_F64 = 2, LP_KNOB_L1_F32 = 3, LP_KNOB_L1_F64 = 4, LP_KNOB_MAX = 4 };
+int lp_tune_lookup(int knob, int nx, int ny, int nz);
+
 static inline int lp_blocks(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;

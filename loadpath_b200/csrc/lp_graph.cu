@@ -2,6 +2,7 @@
 // end+instantiate / launch / free), so the solver records its set-up, CG head and CG tail once
 // and replays each with one launch; capturable asynchronous copies and fills.
 #include <cstring>
+#include <mutex>
 
 #include "lp_common.cuh"
 
@@ -69,7 +70,46 @@ __global__ void k_snapshot_converged(double* __restrict__ out, const double* __r
 #define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
 #define LP_GRID lp_grid(nx, ny, nz, pz, cpz)
 
+namespace {
+struct TuneEntry {
+  int knob, nx, ny, nz, value;
+};
+std::mutex g_tune_mu;
+TuneEntry g_tune[256];
+int g_ntune = 0;
+}  // namespace
+
+int lp_tune_lookup(int knob, int nx, int ny, int nz) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  for (int i = 0; i < g_ntune; ++i)
+    if (g_tune[i].knob == knob && g_tune[i].nx == nx && g_tune[i].ny == ny && g_tune[i].nz == nz)
+      return g_tune[i].value;
+  return 0;
+}
+
 extern "C" {
+
+// Sets (value > 0) or clears (value 0) the tuned launch geometry of a knob for one grid; the
+// launchers read it on their next call. -3 when the table is full.
+int lpb_tune_set(int knob, int nx, int ny, int nz, int value) {
+  if (knob < 1 || knob > LP_KNOB_MAX || nx < 1 || ny < 1 || nz < 1 || value < 0) return LP_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  for (int i = 0; i < g_ntune; ++i)
+    if (g_tune[i].knob == knob && g_tune[i].nx == nx && g_tune[i].ny == ny && g_tune[i].nz == nz) {
+      g_tune[i].value = value;
+      return LP_OK;
+    }
+  if (value == 0) return LP_OK;
+  if (g_ntune >= 256) return LP_ERR_SIZE;
+  g_tune[g_ntune++] = TuneEntry{knob, nx, ny, nz, value};
+  return LP_OK;
+}
+
+// the tuned value of a knob for a grid, 0 when none is set
+int lpb_tune_get(int knob, int nx, int ny, int nz) {
+  if (knob < 1 || knob > LP_KNOB_MAX) return LP_ERR_ARG;
+  return lp_tune_lookup(knob, nx, ny, nz);
+}
 
 // Starts recording the body of a device-side while loop: a graph with one conditional WHILE node
 // (its condition 1 at each launch of the graph), the stream capturing into the node's body.

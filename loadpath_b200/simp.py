@@ -404,7 +404,7 @@ class Top3dLoop:
 
     def __init__(self, dims, volfrac, rmin, fixed_grid, f_grid, nu=0.3, element=None, penal=3.0, emin=1e-9,
                  move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=500,
-                 smoother="chebyshev", warm_start=True, block_cases=True, device="cuda"):
+                 smoother="chebyshev", warm_start=True, block_cases=True, autotune=True, device="cuda"):
         dims = tuple(int(d) for d in dims)
         if any(d % 2 for d in dims):
             raise ValueError("the device SIMP loop takes even cell counts (the multigrid pads odd ones)")
@@ -438,6 +438,7 @@ class Top3dLoop:
         self.u = None
         self.us = None           # the load cases' displacements (several cases)
         self.block_cases = block_cases   # False: the cases one solve after another
+        self.autotune = autotune         # time the applies' launch geometry after the first build
         self.warm_start = warm_start
         self.ncell = dims[0] * dims[1] * dims[2]
         # [0] compliance, [1] change, [8 + k] case k's compliance
@@ -469,8 +470,16 @@ class Top3dLoop:
                 self.ge.last_iters = its
             self.u = self.us[0]
 
-    def solve(self):
+    def _set_moduli(self):
         self.ge.set_moduli_device(self.e)
+        if self.autotune:
+            from .tune import autotune
+
+            autotune(self.ge)
+            self.autotune = False
+
+    def solve(self):
+        self._set_moduli()
         self._solve_cases()
         return self.u
 
@@ -514,7 +523,7 @@ class Top3dLoop:
         if t is not None:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
             ev[0].record()
-            self.ge.set_moduli_device(self.e)
+            self._set_moduli()
             ev[1].record()
             self._solve_cases()
             ev[2].record()

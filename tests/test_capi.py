@@ -6,6 +6,7 @@ import re
 import subprocess
 
 import numpy as np
+import pytest
 
 from loadpath_b200 import build
 from loadpath_b200._lib import HEADER, LIB_PATH, lib, parse_header
@@ -85,3 +86,28 @@ def test_mma_scratch_covers_every_reduction():
         M = 1 if m <= 1 else 2 if m <= 2 else 4 if m <= 4 else 8
         need = 592 * max(M, 2 * M + M * (M + 1) // 2, 4, 2 + M)
         assert lib().lpb_mma_part_len(m) >= need
+
+
+def test_tuning_table_host_only():
+    """lpb_tune_set / lpb_tune_get keep one value per (knob, grid) and clear with 0."""
+    from loadpath_b200._lib import LpError, lib
+
+    L = lib()
+    assert L.lpb_tune_get(1, 33, 17, 9) == 0
+    L.lpb_tune_set(1, 33, 17, 9, 6)
+    L.lpb_tune_set(3, 33, 17, 9, 2)
+    assert L.lpb_tune_get(1, 33, 17, 9) == 6 and L.lpb_tune_get(3, 33, 17, 9) == 2
+    assert L.lpb_tune_get(2, 33, 17, 9) == 0 and L.lpb_tune_get(1, 33, 17, 10) == 0
+    L.lpb_tune_set(1, 33, 17, 9, 0)
+    assert L.lpb_tune_get(1, 33, 17, 9) == 0
+    L.lpb_tune_set(3, 33, 17, 9, 0)
+    with pytest.raises(LpError):
+        L.lpb_tune_set(9, 33, 17, 9, 1)
+
+
+def test_tune_candidates():
+    from loadpath_b200.tune import candidates
+
+    c = candidates(65, 2)
+    assert c[0] == 0 and c[-1] == 65 and all(2 <= z <= 65 for z in c[1:]) and len(c) < 20
+    assert candidates(1, 1) == [0, 1]
