@@ -57,6 +57,9 @@ def parse():
                         "precision and on the plain FP64 GPU path, final compliance and design compared")
     p.add_argument("--iters", type=int, default=100, help="SIMP iterations of --micro full")
     p.add_argument("--reps", type=int, default=100)
+    p.add_argument("--eager", action="store_true",
+                   help="launch every kernel eagerly (no CUDA graphs, convergence tested on the host): the same "
+                        "kernels in the same order, for profilers that do not follow graph launches")
     p.add_argument("--kernels", type=int, default=0, metavar="N",
                    help="device time per kernel over N SIMP iterations (after the warm-up), from the CUDA "
                         "activity trace (torch.profiler); a table, not the JSON line")
@@ -255,6 +258,9 @@ def run_b200(args):
 
     # ---- device-resident timing -----------------------------------------------------------
     loop = new_loop(np.float32)
+    if args.eager:
+        loop.ge.use_graphs = False
+        loop.ge.device_loop = False
     for _ in range(args.warmup):
         loop.step()
     barrier()
@@ -265,12 +271,14 @@ def run_b200(args):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     loop.timing = []
+    torch.cuda.nvtx.range_push("timed")        # the region a profiler can be limited to
     t0.record()
     iters = []
     for _ in range(args.steps):
         loop.step()
         iters.append(loop.ge.last_iters)
     t1.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     timing, loop.timing = loop.timing, None
     barrier()
