@@ -220,6 +220,16 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 //   forward  S = E - sum_d T_(k,d) Y_(k-d),      Y_k = L_kk^-1 S
 //   backward S = S_k Y_k - sum_d T_(k+d,d)^T X_(k+d), X_k = L_kk^-T S   (S_k: the pivot signs)
 // Shared row strides of 36 doubles spread each MMA operand load over all banks.
+// 16-byte asynchronous copies global -> shared through L2 (cp.async.cg): a step issues all its
+// loads at once and waits once, instead of a chain of dependent load rounds
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 constexpr int INV_COLS = 32;
 constexpr int INV_LD = 36;
 constexpr int INV_TILE = 32 * INV_LD;   // doubles per staged 32 x 32 block
@@ -227,7 +237,7 @@ constexpr int INV_TILE = 32 * INV_LD;   // doubles per staged 32 x 32 block
 __global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ainv, const double* __restrict__ t,
                                                          const double* __restrict__ linv, const double* __restrict__ sg,
                                                          LpBand bd, int chunk) {
-  extern __shared__ double sm_inv[];
+  extern __shared__ __align__(16) double sm_inv[];
   double* tiles = sm_inv;                           // chunk band tiles
   double* blks = sm_inv + (long long)chunk * INV_TILE;  // chunk result blocks
   double* diag = blks + (long long)chunk * INV_TILE;    // L_kk^-1
@@ -248,16 +258,19 @@ __global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ai
       double p0 = 0.0, p1 = 0.0, r0 = 0.0, r1 = 0.0;
       for (int d0 = 1; d0 <= dm; d0 += chunk) {
         const int nc = min(chunk, dm - d0 + 1);
-        for (int e = threadIdx.x; e < nc * 1024; e += blockDim.x) {
-          const int d = d0 + (e >> 10), rr = (e >> 5) & 31, cc = e & 31;
+        // pairs of doubles: every offset below is a multiple of 16 bytes (row strides of 32 and
+        // 36 doubles, n_pad a multiple of 32, j0 a multiple of 32, cc even)
+        for (int e = threadIdx.x; e < nc * 512; e += blockDim.x) {
+          const int d = d0 + (e >> 9), rr = (e >> 4) & 31, cc = 2 * (e & 15);
           const long long tk = fwd ? k : k + d;   // band tile (tk, d)
           const long long bk = fwd ? k - d : k + d;   // earlier result block
-          tiles[(e >> 10) * INV_TILE + rr * INV_LD + cc] = __ldg(t + (tk * R1 + d) * 1024 + rr * 32 + cc);
-          blks[(e >> 10) * INV_TILE + rr * INV_LD + cc] = __ldcg(ainv + (32 * bk + rr) * np + j0 + cc);
+          cp_async16(tiles + (e >> 9) * INV_TILE + rr * INV_LD + cc, t + (tk * R1 + d) * 1024 + rr * 32 + cc);
+          cp_async16(blks + (e >> 9) * INV_TILE + rr * INV_LD + cc, ainv + (32 * bk + rr) * np + j0 + cc);
         }
         if (d0 == 1)
-          for (int e = threadIdx.x; e < 1024; e += blockDim.x)
-            diag[(e >> 5) * INV_LD + (e & 31)] = __ldg(linv + (long long)k * 1024 + e);
+          for (int e = threadIdx.x; e < 512; e += blockDim.x)
+            cp_async16(diag + (e >> 4) * INV_LD + 2 * (e & 15), linv + (long long)k * 1024 + 2 * e);
+        cp_async_wait_all();
         __syncthreads();
         for (int c = 0; c < nc; ++c) {
           const double* tc = tiles + c * INV_TILE;
