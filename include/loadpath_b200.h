@@ -240,6 +240,10 @@ int lpb_dinv_mask_f64(double* av, const double* dinv, const uint8_t* m, int nx, 
 int lpb_filter(double* out, const double* v, const int* toff, const double* tw, int ntaps, const double* hs_in, const double* hs_out, double* e_out, double penal, double emin, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_simp_law(double* e, const double* x, double penal, double emin, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_element_energy_f64(double* ce, const double* u, const double* v, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* femops.element_energy (loadpath/femops.py:236-242) on a general mesh: ce[e] = u_e^T ke v_e with
+ * u_e = u[edof[e, 0..23]] (int64 indices, each < the vectors' length, checked by the caller);
+ * v NULL: v = u; ke 24 x 24 float64 (device). */
+int lpb_element_energy_edof(double* ce, const double* u, const double* v, const long long* edof, const double* ke, long long ne, void* stream);
 int lpb_element_energy_f32(double* ce, const float* u, const float* v, const double* ke, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const double* e, double penal, double emin, double scale, int accumulate, double* part, double* comp, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* volumes[j] of the clipped OC step at nl = 31 multipliers lam[j] (device), weights gv = H (1 / hs) */

@@ -333,6 +333,34 @@ __global__ void k_cell_product(double* __restrict__ out, const double* __restric
   }
 }
 
+// ce[e] = u_e^T ke v_e over a general mesh, u_e the 24 values at edof[e, :] (femops.element_energy,
+// loadpath/femops.py:236-242); v NULL: v = u. One thread per element, ke in shared memory; the
+// caller has checked every index against the vectors' length.
+__global__ void k_energy_edof(double* __restrict__ ce, const double* __restrict__ u, const double* __restrict__ v,
+                              const long long* __restrict__ edof, const double* __restrict__ ke, long long ne) {
+  __shared__ double sk[576];
+  for (int i = threadIdx.x; i < 576; i += blockDim.x) sk[i] = ke[i];
+  __syncthreads();
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne; e += (long long)gridDim.x * blockDim.x) {
+    double ue[24], ve[24];
+#pragma unroll
+    for (int a = 0; a < 24; ++a) {
+      const long long d = edof[e * 24 + a];
+      ue[a] = u[d];
+      ve[a] = v ? v[d] : ue[a];
+    }
+    double acc = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < 24; ++j) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 24; ++k) s += sk[j * 24 + k] * ve[k];
+      acc += ue[j] * s;
+    }
+    ce[e] = acc;
+  }
+}
+
 }  // namespace
 
 #define LP_GRID_ARGS int nx, int ny, int nz, int pz, int cpz
@@ -360,6 +388,15 @@ int lpb_simp_law(double* e, const double* x, double penal, double emin, LP_GRID_
   if (!lp_grid_ok(g) || !e || !x) return LP_ERR_ARG;
   long long total = g.cells_padded();
   k_simp_law<<<lp_blocks(total, 256), 256, 0, LP_ST>>>(e, x, penal, emin, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_element_energy_edof(double* ce, const double* u, const double* v, const long long* edof, const double* ke,
+                            long long ne, void* stream) {
+  if (!ce || !u || !edof || !ke || ne < 0) return LP_ERR_ARG;
+  if (ne == 0) return LP_OK;
+  k_energy_edof<<<lp_blocks(ne, 128), 128, 0, LP_ST>>>(ce, u, v, edof, ke, ne);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -714,10 +714,20 @@ int lpb_jacobi_f64(double* x, const double* b, const double* ax, const double* d
 #define LP_GF lp_grid(fnx, fny, fnz, fpz, fcpz)
 #define LP_GC lp_grid(cnx, cny, cnz, cpz_, ccpz)
 
+// a fine level and the level below it: on each axis the coarse cells are ceil(fine cells / 2),
+// or one more when the coarse count is padded to even (loadpath/mg.py:607); the prolongation
+// reads coarse nodes up to ceil(fine / 2), the restriction checks its fine reads against the fine
+// grid
+static bool lp_axis_ok(int f, int c) { return c >= (f + 1) / 2 && c <= (f + 1) / 2 + 1; }
+static bool lp_pair_ok(const LpGrid& gf, const LpGrid& gc) {
+  return lp_axis_ok(gf.nx, gc.nx) && lp_axis_ok(gf.ny, gc.ny) && lp_axis_ok(gf.nz, gc.nz);
+}
+
 int lpb_restrict_residual_f32(float* rc, const float* b, const float* ax, const uint8_t* m, const uint8_t* cm,
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  if (!lp_pair_ok(gf, gc)) return LP_ERR_ARG;
   const long long nw = (long long)((gc.NX() + R4_COLS - 1) / R4_COLS) * gc.NY() * (gc.pz / 4);
   k_restrict4<float><<<lp_blocks(32 * nw, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
@@ -728,6 +738,7 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
                               LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !rc || !b || !ax || !m || !cm) return LP_ERR_ARG;
+  if (!lp_pair_ok(gf, gc)) return LP_ERR_ARG;
   const long long nw = (long long)((gc.NX() + R4_COLS - 1) / R4_COLS) * gc.NY() * (gc.pz / 4);
   k_restrict4<double><<<lp_blocks(32 * nw, 128), 128, 0, LP_ST>>>(rc, b, ax, m, cm, gf, gc);
   LP_LAUNCH_CHECK();
@@ -737,6 +748,7 @@ int lpb_restrict_residual_f64(double* rc, const double* b, const double* ax, con
 int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  if (!lp_pair_ok(gf, gc)) return LP_ERR_ARG;
   const long long t4 = gf.nodes_padded() / 4;
   k_prolong4<float><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
@@ -746,6 +758,7 @@ int lpb_prolong_add_f32(float* x, const float* xc, const uint8_t* cm, const uint
 int lpb_prolong_add_f64(double* x, const double* xc, const uint8_t* cm, const uint8_t* m, LP_FC_ARGS, void* stream) {
   LpGrid gf = LP_GF, gc = LP_GC;
   if (!lp_grid_ok(gf) || !lp_grid_ok(gc) || !x || !xc || !m || !cm) return LP_ERR_ARG;
+  if (!lp_pair_ok(gf, gc)) return LP_ERR_ARG;
   const long long t4 = gf.nodes_padded() / 4;
   k_prolong4<double><<<lp_blocks(t4, 128), 128, 0, LP_ST>>>(x, xc, cm, m, gf, gc);
   LP_LAUNCH_CHECK();
