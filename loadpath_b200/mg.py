@@ -32,7 +32,23 @@ from . import fem
 from ._lib import LpError, add_launches, launches, lib
 from .grid import DevGrid, ptr, stream_handle, torch_dtype
 
-__all__ = ["GridElasticity", "BoxMesh", "LMAX_SAFETY", "STALL"]
+__all__ = ["GridElasticity", "BoxMesh", "LMAX_SAFETY", "STALL", "prolong", "restrict"]
+
+
+def prolong(c):
+    """Trilinear prolongation of a (3, n0, n1, n2) node field to (3, 2n0-1, 2n1-1, 2n2-1)
+    (loadpath/mg.py:84-108), on the device."""
+    from .mgops import prolong as _prolong
+
+    return _prolong(c)
+
+
+def restrict(f):
+    """Full-weighting restriction, the transpose of prolong (loadpath/mg.py:111-132), on the
+    device."""
+    from .mgops import restrict as _restrict
+
+    return _restrict(f)
 
 LMAX_SAFETY = 1.3          # loadpath/mg.py:81
 STALL = 100                # loadpath/mg.py:930

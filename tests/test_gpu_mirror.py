@@ -73,6 +73,10 @@ def test_transfers_cast_dot():
     np.testing.assert_allclose(mgops.restrict(f), R.restrict(f), rtol=1e-13, atol=1e-13)
     c = rng.standard_normal((3, 4, 3, 5))
     np.testing.assert_allclose(mgops.prolong(c), R.prolong(c), rtol=1e-13, atol=1e-13)
+    from loadpath_b200 import mg
+
+    np.testing.assert_array_equal(mg.prolong(c), mgops.prolong(c))
+    np.testing.assert_array_equal(mg.restrict(f), mgops.restrict(f))
     fine = (3, 8, 6, 10)                              # 7 x 5 x 9 cells: a padded coarse level
     coarse = (3, 5, 4, 6)
     b, ax = rng.standard_normal(fine), rng.standard_normal(fine)
