@@ -89,7 +89,12 @@ class _HostFilter:
 
 
 def density_filter(dims, radius, pad=True, pitch=1.0, device="cuda"):
-    """(H, hs) of the cone filter on a full box of cells in C order (loadpath/simp.py:1181-1228)."""
+    """(H, hs) of the cone filter on a full box of cells in C order (loadpath/simp.py:1181-1228).
+    dims: the cell counts, or a domain with `.dims` and `.pitch` as the reference takes (a full
+    box: every cell a design cell)."""
+    if hasattr(dims, "dims"):
+        pitch = float(getattr(dims, "pitch", pitch))
+        dims = tuple(int(d) for d in dims.dims)
     g = DevGrid(dims, device)
     f = DeviceFilter(g, radius, pitch, pad)
     return _HostFilter(f), g.cells_to_host(f.hs).reshape(-1)
