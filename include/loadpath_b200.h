@@ -64,7 +64,7 @@ int lpb_modal_ke(const double* ke, double* kmodal_out);
  * mgops._product_explicit + _scatter_into (loadpath/mgops.py:131-146, 181-217). */
 int lpb_modal_g1(const double* ke, double* g1_out);
 /* level 1, TMA-staged: the Walsh coefficients c = H w of each cell's child moduli in the
- * layout (cpz/4, ny, nx, 8, 4) from lpb_walsh_chunks_* (once per hierarchy, after the patch
+ * layout (cpz/4, ny, nx, 4, 8) from lpb_walsh_chunks_* (once per hierarchy, after the patch
  * cells' weights are zeroed), then the march with u arriving by TMA box loads into a 3-stage
  * mbarrier ring and outputs leaving by TMA stores; g1, pbox HOST; err: device int, set when a
  * bounded wait gave up (or to an alignment code 20..25) */

@@ -15,6 +15,8 @@
 // in entry-major order (entry p of consecutive cells contiguous, so a warp's loads coalesce).
 // Two passes: a cell pass forms the 24 corner forces f_c = K_c u_c into a caller-provided
 // (24, cells) buffer, a node pass sums each node's eight cells' rows and applies the mask.
+#include <cstring>
+
 #include "lp_common.cuh"
 #include "lp_tma.cuh"
 
@@ -408,9 +410,9 @@ __device__ __forceinline__ void xy4(T u00, T u10, T u01, T u11, T (&a)[4]) {
 
 // ---- level 1, TMA-staged march -------------------------------------------------------------
 // The chunked Walsh layout: c = H w per cell (the coefficients of the eight G_t), stored
-// (cpz / 4, ny, nx, 8, 4) so one cell column's four cells of a z chunk are 128 contiguous
-// bytes (float32) and a row of x columns is one run. Formed once per hierarchy (after the
-// patch cells' weights are zeroed).
+// (cpz / 4, ny, nx, 4, 8) so one cell column's four cells of a z chunk are 128 contiguous bytes
+// (float32), each cell's eight coefficients 32 of them, and a row of x columns is one run.
+// Formed once per hierarchy (after the patch cells' weights are zeroed).
 template <typename T>
 __global__ void k_walsh_chunks(T* __restrict__ wc, const T* __restrict__ w, LpGrid g) {
   const long long ncp = g.cells_padded();
@@ -419,9 +421,9 @@ __global__ void k_walsh_chunks(T* __restrict__ wc, const T* __restrict__ w, LpGr
 #pragma unroll
     for (int k = 0; k < 8; ++k) wk[k] = w[k * ncp + c];
     fwht8(wk, cw);
-    T* dst = wc + (c >> 2) * 32 + (c & 3);
+    T* dst = wc + (c >> 2) * 32 + (c & 3) * 8;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) dst[k * 4] = cw[k];
+    for (int k = 0; k < 8; ++k) dst[k] = cw[k];
   }
 }
 
@@ -433,8 +435,17 @@ struct alignas(128) WSlot {
   T v[(N * sizeof(T) + 127) / 128 * 128 / sizeof(T)];
 };
 
+// float32: the Walsh coefficients of the block's 16 x 16 cell columns arrive by TMA with the
+// node values, one 128-byte row per column in the 128-byte swizzle (a warp's 16-byte reads of
+// eight consecutive rows then meet no bank twice); float64 reads them from global memory
+template <typename T>
+struct WCoef {
+  static constexpr int N = sizeof(T) == 4 ? 32 * TXC * TYC : 32;
+};
+
 template <typename T>
 struct WSmem {
+  alignas(1024) T w[WSTAGE][WCoef<T>::N];            // Walsh coefficients [y][x][cell][t] (float32)
   WSlot<T, 3 * WBOX * WBOX * 4> u[WSTAGE];            // node values [comp][y][x][z]
   WSlot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store [comp][y][x][z]
   T red[3][4][TXC * TYC];                             // corners 01 + 11 (to y + 1)
@@ -446,6 +457,7 @@ template <typename T>
 struct WMaps {
   CUtensorMap u;    // (4 NX, NY, pz / 4, 3), box (4 * 17, 17, 1, 3)
   CUtensorMap out;  // (4 NX, NY, pz / 4, 3), box (4 * 15, 15, 1, 3)
+  CUtensorMap w;    // float32 Walsh coefficients (32, nx, ny, cpz / 4), box (32, 16, 16, 1), 128-byte swizzle
 };
 
 // node-plane forces of one cell: rows (3q + cc, 3(q + 4) + cc) of the modal product give the
@@ -496,7 +508,8 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
               const G1<T> gc, LpGrid g, int zch, int nchunks, int* __restrict__ err) {
   extern __shared__ unsigned char wsm_raw[];
   const uint32_t raw_off = lp_smem_addr(wsm_raw);
-  WSmem<T>& sm = *reinterpret_cast<WSmem<T>*>(wsm_raw + ((128u - (raw_off & 127u)) & 127u));
+  WSmem<T>& sm = *reinterpret_cast<WSmem<T>*>(wsm_raw + ((1024u - (raw_off & 1023u)) & 1023u));
+  constexpr bool staged_w = sizeof(T) == 4;
   const int tid = threadIdx.x;
   const int i = tid % TXC, j = tid / TXC;
   const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
@@ -512,13 +525,18 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
   const long long wstride = 32LL * g.nx * g.ny;   // one chunk of Walsh runs to the next
   const T* wcol = wc + (cell_ok ? ((long long)cy * g.nx + cx) * 32 : 0);
   constexpr uint32_t UBYTES = 3 * WBOX * WBOX * 4 * sizeof(T);
+  constexpr uint32_t WBYTES = staged_w ? 32 * TXC * TYC * sizeof(T) : 0;
   __shared__ int bad;
   if (tid == 0) {
     int code = 0;
-    uint32_t so = 0;
-    for (int s = 0; s < WSTAGE; ++s) so |= lp_smem_addr(sm.u[s].v);
+    uint32_t so = 0, sw = 0;
+    for (int s = 0; s < WSTAGE; ++s) {
+      so |= lp_smem_addr(sm.u[s].v);
+      sw |= lp_smem_addr(sm.w[s]);
+    }
     so |= lp_smem_addr(sm.o[0].v) | lp_smem_addr(sm.o[1].v);
-    if (so & 127) code = 20;
+    if ((so & 127) || (staged_w && (sw & 1023))) code = 20;
+    else if (staged_w && (reinterpret_cast<uintptr_t>(&maps.w) & 63)) code = 26;
     else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 21;
     else if (reinterpret_cast<uintptr_t>(&maps.out) & 63) code = 22;
     else if (lp_smem_addr(&sm.full[0]) & 7) code = 23;
@@ -536,8 +554,9 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
   __syncthreads();
   auto issue = [&](int k) {
     const int s = k % WSTAGE;
-    lp_mbar_expect_tx(&sm.full[s], UBYTES);
+    lp_mbar_expect_tx(&sm.full[s], UBYTES + WBYTES);
     lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
+    if constexpr (staged_w) lp_tma_load_4d(sm.w[s], &maps.w, 0, x0 - 1, y0 - 1, cstart + k, &sm.full[s]);
   };
   if (tid == 0) {
     issue(0);
@@ -594,8 +613,20 @@ k_weights_tma(const __grid_constant__ WMaps<T> maps, const T* __restrict__ wc, c
           v[3 * (q + 4) + cc] = hi - lo;
           a_lo[q][cc] = hi;
         }
+      if constexpr (staged_w) {
+        // this cell's eight coefficients: two 16-byte reads of the column's swizzled row
+        const uint32_t row = (uint32_t)(j * TXC + i);
+        const unsigned char* wb = reinterpret_cast<const unsigned char*>(sm.w[s]);
+        const float4 c0 = *reinterpret_cast<const float4*>(wb + lp_swz128(row * 128u + (uint32_t)t * 32u));
+        const float4 c1 = *reinterpret_cast<const float4*>(wb + lp_swz128(row * 128u + (uint32_t)t * 32u + 16u));
+        cw[0] = c0.x; cw[1] = c0.y; cw[2] = c0.z; cw[3] = c0.w;
+        cw[4] = c1.x; cw[5] = c1.y; cw[6] = c1.z; cw[7] = c1.w;
 #pragma unroll
-      for (int kk = 0; kk < 8; ++kk) cw[kk] = cell_ok ? __ldg(wch + kk * 4 + t) : T(0);
+        for (int kk = 0; kk < 8; ++kk) cw[kk] = cell_ok ? cw[kk] : T(0);
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) cw[kk] = cell_ok ? __ldg(wch + t * 8 + kk) : T(0);
+      }
       T fp[4][3];
       fold_rows<T>(gc, cw, v, fp, up_carry);
       if (!halo) {
@@ -1014,7 +1045,13 @@ static int launch_weights_tma(T* out, const T* u, const T* wc, const int* pid, c
   const uint32_t bout[4] = {4 * (TXC - 1), TYC - 1, 1, 3};
   if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
     return LP_ERR_ARG;
-  const int smem = (int)sizeof(WSmem<T>) + 128;
+  memset(&maps.w, 0, sizeof(maps.w));
+  if (sizeof(T) == 4) {
+    const uint64_t wd[4] = {32, (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.cpz / 4};
+    const uint32_t wb[4] = {32, TXC, TYC, 1};
+    if (!lp_make_map(&maps.w, wc, 4, wd, wb, sizeof(T), 128)) return LP_ERR_ARG;
+  }
+  const int smem = (int)sizeof(WSmem<T>) + 1024;
   static long long slots = 0;   // resident blocks on the device (queried once per process)
   if (!slots) {
     if (cudaFuncSetAttribute(k_weights_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)

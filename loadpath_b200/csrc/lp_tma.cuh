@@ -84,6 +84,8 @@ __device__ __forceinline__ void lp_fence_proxy_async() { asm volatile("fence.pro
 // byte offset within a 32-byte-swizzled TMA destination (1024-byte aligned): the 16-byte chunk
 // bit (4) flipped by bit 7
 __device__ __forceinline__ uint32_t lp_swz32(uint32_t off) { return off ^ (((off >> 7) & 1u) << 4); }
+// byte offset (from a 1024-byte aligned base) of a 128-byte-swizzled TMA destination
+__device__ __forceinline__ uint32_t lp_swz128(uint32_t off) { return off ^ (((off >> 7) & 7u) << 4); }
 
 // ---- host: tensor-map encoding through the runtime's driver entry point ------------------
 static inline PFN_cuTensorMapEncodeTiled_v12000 lp_encode_fn() {
@@ -99,10 +101,11 @@ static inline PFN_cuTensorMapEncodeTiled_v12000 lp_encode_fn() {
 }
 
 // rank-r tiled map over a dense C-order array; dims/box innermost first; elem 4 or 8 bytes;
-// swizzle32: the 32-byte swizzle (box rows of exactly 32 bytes; in shared memory byte address
-// bit 4 is XORed with bit 7, see lp_swz32), destinations then 1024-byte aligned
+// swizzle: 0, or 32 (box rows of exactly 32 bytes; in shared memory byte address bit 4 is XORed
+// with bit 7, see lp_swz32) or 128 (box rows of exactly 128 bytes; bits 4-6 XORed with bits
+// 7-9, see lp_swz128), destinations then 1024-byte aligned
 static inline bool lp_make_map(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
-                               const uint32_t* box, int elem_bytes, bool swizzle32 = false) {
+                               const uint32_t* box, int elem_bytes, int swizzle = 0) {
   auto fn = lp_encode_fn();
   if (!fn) return false;
   if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
@@ -120,10 +123,13 @@ static inline bool lp_make_map(CUtensorMap* map, const void* base, int rank, con
     stride *= dims[i];
   }
   if ((box[0] * (uint32_t)elem_bytes) % 16) return false;
-  if (swizzle32 && box[0] * (uint32_t)elem_bytes != 32) return false;
+  if (swizzle && box[0] * (uint32_t)elem_bytes != (uint32_t)swizzle) return false;
+  if (swizzle != 0 && swizzle != 32 && swizzle != 128) return false;
   CUtensorMapDataType dt = elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   CUresult r = fn(map, dt, (cuuint32_t)rank, const_cast<void*>(base), gd, gs, bx, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  swizzle == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                 : (swizzle == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE),
                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;

@@ -147,7 +147,7 @@ class DevLevel:
         self.glist = self.gcount = self.kpc = None   # ...and the cells applied from node-basis entries
         self.ft = None           # explicit: (24, cells) scratch of the cell pass
         self.g1 = None           # weights: 279 corner-parity coefficients (host)
-        self.wc = None           # weights: Walsh coefficients (cpz/4, ny, nx, 8, 4)
+        self.wc = None           # weights: Walsh coefficients (cpz/4, ny, nx, 4, 8)
         self.pbox = None         # weights: node box of the patch cells (host, 6 ints)
         self.mask = None
         self.dinv = None
@@ -628,7 +628,7 @@ class GridElasticity:
             lv.patch_cells = pcells
             lv.g1 = self.g1
             # the Walsh coefficients of each cell's child moduli, chunked for the march kernel
-            lv.wc = self._tbuf("wc1", (gc.cpz // 4, gc.ny, gc.nx, 8, 4), dt)
+            lv.wc = self._tbuf("wc1", (gc.cpz // 4, gc.ny, gc.nx, 4, 8), dt)
             getattr(L, f"lpb_walsh_chunks_{sfx}")(lv.wc.data_ptr(), lv.w.data_ptr(), *gc.args, st)
             lv.err = self._err
             return lv
