@@ -318,7 +318,7 @@ def run_b200(args):
                     "timed_over": f"{args.steps} SIMP iterations after the timed region, CUDA events around "
                                   "each fine-level float32 apply on its stream",
                     "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured"
-                                    else "fallback (6.65 TB/s copy measured earlier on this pool's B200s)")}
+                                    else "fallback (6.65 TB/s, a copy measured on B200)")}
     phases = np.array([[a.elapsed_time(b) for a, b in zip(ev[:-1], ev[1:])] for ev in timing])
     extra = {"cg_iterations": iters, "compliance": loop.history[args.warmup + args.steps - 1][0],
              "phase_ms_per_step": dict(zip(("hierarchy", "solve", "sensitivities", "oc"),
