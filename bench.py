@@ -73,6 +73,14 @@ def parse():
     return a
 
 
+def workload_config(dims, world):
+    """The `config` both arms print: the bench workload and its sizes."""
+    return {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, dims))} hex8 "
+                        f"({3 * math.prod(d + 1 for d in dims)} DOF), MG-PCG rtol {RTOL}, "
+                        "V-cycle float32, CG float64",
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (fields of 51-103 MB)"}
+
+
 def cantilever(dims):
     nx, ny, nz = dims
     fixed = np.zeros((3, nx + 1, ny + 1, nz + 1), bool)
@@ -212,8 +220,8 @@ def run_reference(args):
     v = statistics.median(vals[args.warmup:])
     line = {"metric": METRIC, "value": v, "unit": "SIMP iter/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-            "config": {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, args.dims))} hex8"},
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": workload_config(args.dims, args.gpus),
             "impl": "reference", "cpu_baseline": dict(cb, value=v),
             "e2e": {"value": v, "unit": "SIMP iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -411,10 +419,7 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded log-uniform density smoothed by the r=2 filter; cantilever loads)",
-            "config": {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, dims))} hex8 "
-                                   f"({3 * math.prod(d + 1 for d in dims)} DOF), MG-PCG rtol {RTOL}, "
-                                   "V-cycle float32, CG float64",
-                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (fields of 51-103 MB)"},
+            "config": workload_config(dims, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "fp64_gpu_path": fp64, "detail": extra}
     print(json.dumps(line))
