@@ -691,6 +691,10 @@ __global__ void k_patch_add(T* __restrict__ out, const T* __restrict__ u, const 
   const int z = bz0 + (int)(warp % bnz);
   const long long q = warp / bnz;
   const int y = by0 + (int)(q % bny), x = bx0 + (int)(q / bny);
+  // a node with no solved component keeps its output (the held nodes of a support face are
+  // half of a patch box): the whole warp leaves
+  const uint8_t mb0 = mask[g.node(x, y, z)];
+  if (!(mb0 & 7)) return;
   // lane -> (cell corner kk = lane / 4, column block of 6 = lane % 4)
   const int kk = lane >> 2, cb = lane & 3;
   T a[3] = {T(0), T(0), T(0)};
@@ -714,10 +718,9 @@ __global__ void k_patch_add(T* __restrict__ out, const T* __restrict__ u, const 
     for (int o = 16; o > 0; o >>= 1) a[cc] += __shfl_down_sync(0xffffffffu, a[cc], o);
   if (lane == 0) {
     const long long n = g.node(x, y, z);
-    const uint8_t mb = mask[n];
 #pragma unroll
     for (int cc = 0; cc < 3; ++cc)
-      if ((mb >> cc) & 1) out[cc * cs + n] += a[cc];
+      if ((mb0 >> cc) & 1) out[cc * cs + n] += a[cc];
   }
 }
 
