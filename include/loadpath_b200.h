@@ -81,6 +81,11 @@ int lpb_apply_weights_tma_f64(double* out, const double* u, const double* wc, co
  * lpb_apply_explicit_sym_f32). Same operator as loadpath/mgops.py:131-146 + 181-217. */
 int lpb_pack_modal_f32(float* km, int* glist, int* gcount, float* kpc, const float* k, long long ncells, double tol, void* stream);
 int lpb_apply_explicit_modal_f32(float* out, const float* u, const float* km, const float* kpc, const int* glist, const int* gcount, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* The same with a degree-2 Chebyshev update formed in its gather (the smoothing of
+ * loadpath/mgops.py:312-343 as lpb_cheb2_zero / lpb_residual_scaled / lpb_cheb2 apply it):
+ * mode 1 (u = d) x = d + (c1 d + c2 dinv (b - A d)); mode 2 (u = x) r = b - A x, d = s dinv r;
+ * mode 3 (u = d) x = (x + d) + (c1 d + c2 dinv (r - A d)); coef: the level's coefficients. */
+int lpb_apply_explicit_modal_cheb_f32(int mode, float* x, float* r, float* d, const float* u, const float* b, const float* dinv, const double* coef, const float* km, const float* kpc, const int* glist, const int* gcount, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f32(float* out, const float* u, const float* kp, float* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, double* ft, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* lpb_apply_explicit_sym_f32 for callers that cannot allocate device memory (a host that owns

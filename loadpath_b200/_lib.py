@@ -34,7 +34,8 @@ _KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_m
             "lpb_while_end": 0,
             "lpb_mma_part_len": 0, "lpb_mma_prepare": 2, "lpb_mma_newton_a": 2, "lpb_mma_newton_b": 2,
             "lpb_mma_trial": 2, "lpb_project": 2, "lpb_live_seed": 2,
-            "lpb_dead_loads": 2, "lpb_apply_rf_f32": 2, "lpb_apply_explicit_modal_f32": 2}
+            "lpb_dead_loads": 2, "lpb_apply_rf_f32": 2, "lpb_apply_explicit_modal_f32": 2,
+            "lpb_apply_explicit_modal_cheb_f32": 2}
 # entries whose kernel count depends on their arguments
 _VARIABLE = {"lpb_sensitivity": lambda a: 1 + (a[9] is not None),
              "lpb_band_solve_cols_f32": lambda a: a[3] + (a[3] + 7) // 8,

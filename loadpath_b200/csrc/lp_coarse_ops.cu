@@ -1002,6 +1002,56 @@ __global__ void k_explicit_gather(T* __restrict__ out, const T* __restrict__ ft,
   }
 }
 
+// The explicit gather with a degree-2 Chebyshev update applied to each node's A u as it is formed
+// (the standalone kernels' expressions): mode 1 x = d + (c1 d + c2 dinv (b - A d)); mode 2 r = b - A x,
+// d = s dinv r; mode 3 x = (x + d) + (c1 d + c2 dinv (r - A d)). Padding is left as it is (zero).
+struct ChebArgs {
+  float* x;
+  float* r;
+  float* d;
+  const float* b;
+  const float* dinv;
+  const double* coef;
+};
+
+template <int MODE>
+__global__ void k_explicit_gather_cheb(const float* __restrict__ ft, const uint8_t* __restrict__ mask, LpGrid g,
+                                       ChebArgs a) {
+  const long long total = g.nodes_padded();
+  const long long ncp = g.cells_padded(), cs = g.comp_stride();
+  const float s = (float)a.coef[1], c1 = (float)a.coef[2], c2 = (float)a.coef[3];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    if (!g.node_at(t, x, y, z)) continue;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int cx = x - cx_(k), cy = y - cy_(k), cz = z - cz_(k);
+      if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz) continue;
+      const long long c = g.cell(cx, cy, cz);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) acc[cc] += ft[(long long)(3 * k + cc) * ncp + c];
+    }
+    const long long n = g.node(x, y, z);
+    const uint8_t mb = mask[n];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      const long long i = cc * cs + n;
+      const float adi = ((mb >> cc) & 1) ? acc[cc] : 0.0f;
+      if (MODE == 1) {
+        a.x[i] = lp_cheb2_zero_v(a.d[i], a.b[i], adi, a.dinv[i], c1, c2);
+      } else if (MODE == 2) {
+        float ri, di;
+        lp_residual_scaled_v(a.b[i], adi, a.dinv[i], s, ri, di);
+        a.r[i] = ri;
+        a.d[i] = di;
+      } else {
+        a.x[i] = lp_cheb2_v(a.x[i], a.d[i], a.r[i], adi, a.dinv[i], c1, c2);
+      }
+    }
+  }
+}
+
 // full (cells, 576) matrices -> packed symmetric entry-major (the average of K and K^T)
 template <typename Ti, typename To>
 __global__ void k_pack_sym(To* __restrict__ kp, const Ti* __restrict__ k, long long ncp) {
@@ -1263,6 +1313,31 @@ int lpb_apply_explicit_modal_f32(float* out, const float* u, const float* km, co
   const int modal_blocks = lp_blocks(g.cells_padded(), 128);
   k_explicit_modal_cells<<<modal_blocks + 148, 128, 0, LP_ST>>>(ft, u, km, kpc, glist, gcount, g, modal_blocks);
   k_explicit_gather<float><<<lp_blocks(g.nodes_padded(), 256), 256, 0, LP_ST>>>(out, ft, mask, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// the explicit level's A u (modal form, as lpb_apply_explicit_modal_f32) with a degree-2 Chebyshev
+// update in its gather: mode 1 (u = d) x = d + (c1 d + c2 dinv (b - A d)); mode 2 (u = x)
+// r = b - A x, d = s dinv r; mode 3 (u = d) x = (x + d) + (c1 d + c2 dinv (r - A d)); the fields
+// a mode does not name may be NULL; coef: the level's Chebyshev coefficients (device)
+int lpb_apply_explicit_modal_cheb_f32(int mode, float* x, float* r, float* d, const float* u, const float* b,
+                                      const float* dinv, const double* coef, const float* km, const float* kpc,
+                                      const int* glist, const int* gcount, float* ft, const uint8_t* mask,
+                                      LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !u || !km || !kpc || !glist || !gcount || !ft || !mask || !dinv || !coef) return LP_ERR_ARG;
+  if (mode == 1 && (!x || !d || !b || u != d || x == d)) return LP_ERR_ARG;
+  if (mode == 2 && (!r || !d || !b || u == r || u == d || r == d)) return LP_ERR_ARG;
+  if (mode == 3 && (!x || !d || !r || u != d || x == d)) return LP_ERR_ARG;
+  if (mode < 1 || mode > 3) return LP_ERR_ARG;
+  const int modal_blocks = lp_blocks(g.cells_padded(), 128);
+  k_explicit_modal_cells<<<modal_blocks + 148, 128, 0, LP_ST>>>(ft, u, km, kpc, glist, gcount, g, modal_blocks);
+  const ChebArgs a{x, r, d, b, dinv, coef};
+  const int nb = lp_blocks(g.nodes_padded(), 256);
+  if (mode == 1) k_explicit_gather_cheb<1><<<nb, 256, 0, LP_ST>>>(ft, mask, g, a);
+  else if (mode == 2) k_explicit_gather_cheb<2><<<nb, 256, 0, LP_ST>>>(ft, mask, g, a);
+  else k_explicit_gather_cheb<3><<<nb, 256, 0, LP_ST>>>(ft, mask, g, a);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -75,6 +75,25 @@ static inline bool lp_grid_ok(const LpGrid& g) {
 enum { LP_KNOB_FINE_F32 = 1, LP_KNOB_FINE_F64 = 2, LP_KNOB_L1_F32 = 3, LP_KNOB_L1_F64 = 4, LP_KNOB_MAX = 4 };
 int lp_tune_lookup(int knob, int nx, int ny, int nz);
 
+// The degree-2 Chebyshev updates, one definition for the standalone vector kernels and the
+// explicit levels' gather that applies them as it forms A u (the same expression, so the same bits)
+template <typename T>
+__device__ __forceinline__ T lp_cheb2_zero_v(T di, T bi, T adi, T dinvi, T c1, T c2) {
+  const T ri = bi - adi;
+  return di + (c1 * di + c2 * dinvi * ri);
+}
+template <typename T>
+__device__ __forceinline__ T lp_cheb2_v(T xi, T di, T rin, T adi, T dinvi, T c1, T c2) {
+  const T ri = rin - adi;
+  return (xi + di) + (c1 * di + c2 * dinvi * ri);
+}
+template <typename T>
+__device__ __forceinline__ void lp_residual_scaled_v(T bi, T axi, T dinvi, T s, T& r, T& d) {
+  const T ri = bi - axi;
+  r = ri;
+  d = s * dinvi * ri;
+}
+
 static inline int lp_blocks(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b < 1) b = 1;

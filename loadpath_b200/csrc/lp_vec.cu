@@ -123,9 +123,10 @@ __global__ void k_residual_scaled(const T* __restrict__ b, const T* __restrict__
                                   const double* __restrict__ coef, T* __restrict__ r, T* __restrict__ d, long long n) {
   const T s = (T)coef[1];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    T ri = b[i] - ax[i];
+    T ri, di;
+    lp_residual_scaled_v(b[i], ax[i], dinv[i], s, ri, di);
     r[i] = ri;
-    d[i] = s * dinv[i] * ri;
+    d[i] = di;
   }
 }
 
@@ -187,11 +188,8 @@ __global__ void k_cheb2_zero(T* __restrict__ x, const T* __restrict__ b, const T
                              const T* __restrict__ d, const T* __restrict__ dinv, const double* __restrict__ coef,
                              long long n) {
   const T c1 = (T)coef[2], c2 = (T)coef[3];
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const T di = d[i];
-    const T ri = b[i] - ad[i];
-    x[i] = di + (c1 * di + c2 * dinv[i] * ri);
-  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = lp_cheb2_zero_v(d[i], b[i], ad[i], dinv[i], c1, c2);
 }
 
 // from x (after lpb_residual_scaled: r = b - A x, d = s dinv r; ad = A d):
@@ -200,11 +198,8 @@ template <typename T>
 __global__ void k_cheb2(T* __restrict__ x, const T* __restrict__ d, const T* __restrict__ r, const T* __restrict__ ad,
                         const T* __restrict__ dinv, const double* __restrict__ coef, long long n) {
   const T c1 = (T)coef[2], c2 = (T)coef[3];
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const T di = d[i];
-    const T ri = r[i] - ad[i];
-    x[i] = (x[i] + di) + (c1 * di + c2 * dinv[i] * ri);
-  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = lp_cheb2_v(x[i], d[i], r[i], ad[i], dinv[i], c1, c2);
 }
 
 // damped Jacobi: x += omega dinv (b - ax), x = 0 start handled by the caller

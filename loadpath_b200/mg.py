@@ -820,6 +820,20 @@ class GridElasticity:
                                                     0, n, st)
             return x
         coef = lv.coef.data_ptr()
+        if self.degree == 2 and lv.kind == "explicit" and lv.km is not None:
+            # the explicit levels form each update in the gather of A u (the same expressions)
+            def fused(mode, u):
+                L.lpb_apply_explicit_modal_cheb_f32(mode, x.data_ptr(), r.data_ptr(), d.data_ptr(), u.data_ptr(),
+                                                    b.data_ptr(), lv.dinv.data_ptr(), coef, lv.km.data_ptr(),
+                                                    lv.kpc.data_ptr(), lv.glist.data_ptr(), lv.gcount.data_ptr(),
+                                                    lv.ft.data_ptr(), lv.mask.data_ptr(), *g.args, st)
+            if from_zero:
+                getattr(L, f"lpb_cheb_d_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), coef, d.data_ptr(), n, st)
+                fused(1, d)
+            else:
+                fused(2, x)
+                fused(3, d)
+            return x
         if self.degree == 2:
             # the two Chebyshev steps in two passes (same bits as the step-by-step form)
             if from_zero:
