@@ -97,6 +97,20 @@ def apply_bytes(dims, itemsize):
     return 2 * 3 * n * itemsize + nx * ny * nz * itemsize
 
 
+# the float32 fine apply's Chebyshev-update forms (lpb_apply_fine_cheb_f32), as extra node fields
+# moved beyond the plain apply's u in / A u out: 1 reads b and dinv (u is d); 2 reads b and dinv
+# and writes r and d; 3 reads x, r and dinv and writes x (u is d)
+CHEB_FORMS = {"f32c1": 2, "f32c2": 3, "f32c3": 3}
+
+
+def form_bytes(dims, form):
+    """Algorithmic bytes of one float32 fine apply in the given form ("f32" plain, or a
+    CHEB_FORMS key)."""
+    nx, ny, nz = dims
+    field = 3 * (nx + 1) * (ny + 1) * (nz + 1) * 4
+    return apply_bytes(dims, 4) + CHEB_FORMS.get(form, 0) * field
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -308,21 +322,33 @@ def run_b200(args):
     mg.set_probe(None)
     fine = probe.summary()
     peak, peak_kind = peaks()
-    b32 = apply_bytes(dims, 4)
     roofline = None
-    if fine["f32_count"]:
-        avg = fine["f32_ms"] / fine["f32_count"] / 1e3
-        achieved = b32 / avg / 1e9
+    forms = [f for f in ("f32",) + tuple(CHEB_FORMS) if fine[f + "_count"]]
+    if forms:
+        # every float32 fine launch (the plain apply and its Chebyshev-update forms): their
+        # algorithmic bytes over their event time
+        count = sum(fine[f + "_count"] for f in forms)
+        sec = sum(fine[f + "_ms"] for f in forms) / 1e3
+        nbytes = sum(form_bytes(dims, f) * fine[f + "_count"] for f in forms)
+        avg = sec / count
+        achieved = nbytes / sec / 1e9
         traffic = None
         prof = os.path.join(ROOT, "profiles", "fine_apply_f32_traffic.json")
         if os.path.exists(prof):
             with open(prof) as fh:
                 pd = json.load(fh)
-            if tuple(pd.get("dims", ())) == tuple(dims):
-                traffic = pd.get("dram_bytes_per_launch")
+            per = pd.get("forms", {})
+            if tuple(pd.get("dims", ())) == tuple(dims) and all(f in per for f in forms):
+                traffic = sum(per[f] * fine[f + "_count"] for f in forms) / count
+        by_form = {f: {"launches": fine[f + "_count"], "avg_us": fine[f + "_ms"] / fine[f + "_count"] * 1e3,
+                       "algorithmic_bytes": form_bytes(dims, f),
+                       "GBps": form_bytes(dims, f) / (fine[f + "_ms"] / fine[f + "_count"] / 1e3) / 1e9}
+                   for f in forms}
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "kernel": "k_apply_fine_x2 (float32)",
-                    "algorithmic_bytes": b32, "avg_launch_us": avg * 1e6, "launches_timed": fine["f32_count"],
+                    "traffic": traffic, "kernel": "k_apply_fine_x2 (float32: plain A u and the Chebyshev-update "
+                                              "forms f32c1..3)",
+                    "algorithmic_bytes": nbytes / count, "avg_launch_us": avg * 1e6, "launches_timed": count,
+                    "forms": by_form,
                     "timed_over": f"{args.steps} SIMP iterations after the timed region, CUDA events around "
                                   "each fine-level float32 apply on its stream",
                     "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak_kind == "measured"
@@ -426,6 +452,43 @@ def run_b200(args):
     return 0
 
 
+def time_cheb_forms(lv, u, m, dims, reps):
+    """The three Chebyshev-update forms of the float32 fine apply on seeded fields (held dofs
+    zero, as in the V-cycle), each warmed once and timed over reps launches."""
+    import torch
+
+    from loadpath_b200._lib import lib
+    from loadpath_b200.grid import stream_handle
+
+    L, st, gr = lib(), stream_handle(), lv.grid
+    gen = torch.Generator(device="cuda").manual_seed(103)
+
+    def fld():
+        return (torch.randn(u.shape, generator=gen, device="cuda", dtype=torch.float32) * m).contiguous()
+
+    x, r, b, dinv, d = fld(), fld(), fld(), fld().abs(), u.clone()
+    coef = torch.tensor([0.0, 0.5, 0.3, 0.2] + [0.0] * 12, dtype=torch.float64, device="cuda")
+    srcs = {1: d, 2: x, 3: d}
+    res = {}
+    for mode in (1, 2, 3):
+        def call():
+            L.lpb_apply_fine_cheb_f32(mode, x.data_ptr(), r.data_ptr(), d.data_ptr(), srcs[mode].data_ptr(),
+                                      b.data_ptr(), dinv.data_ptr(), coef.data_ptr(), lv.e.data_ptr(),
+                                      lv.mask.data_ptr(), lv.kmodal.ctypes.data, lv.err.data_ptr(), *gr.args, st)
+        call()
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            call()
+        e.record()
+        torch.cuda.synchronize()
+        us = a.elapsed_time(e) / reps * 1e3
+        gbs = form_bytes(dims, f"f32c{mode}") / (us * 1e-6) / 1e9
+        res[f"mode{mode}"] = {"us_per_apply": us, "GBps": gbs, "frac_of_peak": gbs / peaks()[0]}
+    return res
+
+
 def run_micro_apply(args):
     """args.reps fine-level applies (float32 and float64) on seeded N(0,1) vectors at the bench's
     density, timed with CUDA events; one JSON line."""
@@ -474,6 +537,8 @@ def run_micro_apply(args):
         isz = 4 if lv.dtype == torch.float32 else 8
         gbs = apply_bytes(dims, isz) / (us * 1e-6) / 1e9
         out["f32" if isz == 4 else "f64"] = {"us_per_apply": us, "GBps": gbs, "frac_of_peak": gbs / peaks()[0]}
+        if isz == 4:
+            out["f32_cheb_forms"] = time_cheb_forms(lv, u, m, dims, args.reps)
     ge.check_device()
     # the level-1 (weights) operator of the solver's own hierarchy, float32
     ge1 = GridElasticity(mesh, 0.3, fx, element="im")

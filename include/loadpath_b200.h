@@ -45,6 +45,11 @@ int lpb_apply_explicit_f64(double* out, const double* u, const double* k, const 
  * Needs pz % 4 == 0, cpz == pz and 16-byte aligned fields. Replaces mgops._product_scaled +
  * _scatter_into with finish (loadpath/mgops.py:86-103, :181-217). */
 int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* lpb_apply_fine_f32 with a degree-2 Chebyshev update formed where A u is stored (the V-cycle
+ * smoothing of loadpath/mgops.py:312-343 as lpb_cheb2_zero / lpb_residual_scaled / lpb_cheb2
+ * apply it, same bits): mode 1 (u = d) x = d + (c1 d + c2 dinv (b - A d)); mode 2 (u = x)
+ * r = b - A x, d = s dinv r; mode 3 (u = d) x = (x + d) + (c1 d + c2 dinv (r - A d)). */
+int lpb_apply_fine_cheb_f32(int mode, float* x, float* r, float* d, const float* u, const float* b, const float* dinv, const double* coef, const float* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal, int* err, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* the float64 fine apply that also forms u . out over the level's nodes into *dot (device),
  * for the PCG's p . A p: per-block partials in part (part_len doubles, -3 when short), summed in

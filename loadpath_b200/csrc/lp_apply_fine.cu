@@ -507,17 +507,68 @@ __device__ __forceinline__ const float* u_at2(const FineSmem2& sm, int s, int c,
   return &sm.u[s].v[((c * BOX + y) * BOX + x) * 4];
 }
 
+// The degree-2 Chebyshev update formed where A u is stored (the vector kernels' expressions, so
+// the same bits): mode 1 (u = d) x = d + (c1 d + c2 dinv (b - A d)); mode 2 (u = x) r = b - A x,
+// d = s dinv r; mode 3 (u = d) x = (x + d) + (c1 d + c2 dinv (r - A d)).
+struct FineCheb {
+  float* x;
+  float* r;
+  float* d;
+  const float* b;
+  const float* dinv;
+  const double* coef;
+};
+
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+template <int MODE>
+__device__ __forceinline__ void cheb_store(const FineCheb& ch, long long i, const float4 ad4, float s, float c1,
+                                           float c2) {
+  const float4 dv4 = ldg4(ch.dinv + i);
+  const float* ad = &ad4.x;
+  const float* dv = &dv4.x;
+  if constexpr (MODE == 1) {
+    const float4 d4 = ldg4(ch.d + i), b4 = ldg4(ch.b + i);
+    const float *d = &d4.x, *b = &b4.x;
+    float4 x4;
+    float* x = &x4.x;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) x[t] = lp_cheb2_zero_v(d[t], b[t], ad[t], dv[t], c1, c2);
+    *reinterpret_cast<float4*>(ch.x + i) = x4;
+  } else if constexpr (MODE == 2) {
+    const float4 b4 = ldg4(ch.b + i);
+    const float* b = &b4.x;
+    float4 r4, d4;
+    float *r = &r4.x, *d = &d4.x;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) lp_residual_scaled_v(b[t], ad[t], dv[t], s, r[t], d[t]);
+    *reinterpret_cast<float4*>(ch.r + i) = r4;
+    *reinterpret_cast<float4*>(ch.d + i) = d4;
+  } else {
+    const float4 x4 = *reinterpret_cast<const float4*>(ch.x + i);   // read, then written, by this thread
+    const float4 d4 = ldg4(ch.d + i), r4 = ldg4(ch.r + i);
+    const float *x = &x4.x, *d = &d4.x, *r = &r4.x;
+    float4 o4;
+    float* o = &o4.x;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) o[t] = lp_cheb2_v(x[t], d[t], r[t], ad[t], dv[t], c1, c2);
+    *reinterpret_cast<float4*>(ch.x + i) = o4;
+  }
+}
+
 // One barrier per chunk: each thread waits for its stage, computes, publishes its y-corner
 // forces into the exchange buffer of the chunk's parity, and the block meets once (which also
 // settles a wait that gave up); the owners then add their -y neighbour's corners and store
 // their four node planes with 16-byte stores. The exchange is double-buffered, so the next
 // chunk's writes never meet this chunk's reads. A chunk runs in two phases that keep the
 // register footprint to one pair of cells: (A) planes 0..2 -> cells 0, 1; (B) planes 2..4 ->
-// cells 2, 3 (plane 2's modes formed in both).
+// cells 2, 3 (plane 2's modes formed in both). MODE 0 stores A u in out; modes 1..3 store a
+// Chebyshev update instead (cheb_store; out unused).
+template <int MODE>
 __global__ void __launch_bounds__(TXC * TYC, 2)
 k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict__ out,
                 const uint8_t* __restrict__ mask, const KModal2 km2, const KModal<float> km, LpGrid g, int zch,
-                int nchunks, int* __restrict__ err) {
+                int nchunks, int* __restrict__ err, const FineCheb ch) {
   extern __shared__ unsigned char smem_raw2[];
   const uint32_t raw_off = lp_smem_addr(smem_raw2);
   FineSmem2& sm = *reinterpret_cast<FineSmem2*>(smem_raw2 + ((128u - (raw_off & 127u)) & 127u));
@@ -544,7 +595,10 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
     if (so & 127) code = 10;
     else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 11;
     else if (reinterpret_cast<uintptr_t>(&maps.e) & 63) code = 12;
-    else if (reinterpret_cast<uintptr_t>(out) & 15) code = 13;
+    else if (MODE == 0 && (reinterpret_cast<uintptr_t>(out) & 15)) code = 13;
+    else if (MODE != 0 && ((reinterpret_cast<uintptr_t>(ch.x) | reinterpret_cast<uintptr_t>(ch.r) |
+                            reinterpret_cast<uintptr_t>(ch.d) | reinterpret_cast<uintptr_t>(ch.b) |
+                            reinterpret_cast<uintptr_t>(ch.dinv)) & 15)) code = 14;
     else if (lp_smem_addr(&sm.full[0]) & 7) code = 15;
     else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 16;
     bad = code;
@@ -552,6 +606,12 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
   }
   __syncthreads();
   if (bad) return;
+  float cs_s = 0.0f, cs_c1 = 0.0f, cs_c2 = 0.0f;
+  if constexpr (MODE != 0) {
+    cs_s = (float)ch.coef[1];
+    cs_c1 = (float)ch.coef[2];
+    cs_c2 = (float)ch.coef[3];
+  }
   if (tid == 0) {
     for (int s = 0; s < NST2; ++s) lp_mbar_init(&sm.full[s], 1);
     lp_fence_barrier_init();
@@ -694,7 +754,8 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
         if (!((mb4 >> (8 + cc)) & 1u)) o.y = 0.0f;
         if (!((mb4 >> (16 + cc)) & 1u)) o.z = 0.0f;
         if (!((mb4 >> (24 + cc)) & 1u)) o.w = 0.0f;
-        *reinterpret_cast<float4*>(out + cc * cs + obase + c * zcs) = o;
+        if constexpr (MODE == 0) *reinterpret_cast<float4*>(out + cc * cs + obase + c * zcs) = o;
+        else cheb_store<MODE>(ch, cc * cs + obase + c * zcs, o, cs_s, cs_c1, cs_c2);
       }
     }
   }
@@ -731,12 +792,13 @@ static long long resident_blocks(const void* kfn, int smem) {
 template <typename T>
 static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, const double* kmodal_host, int* err,
                        LpGrid g, cudaStream_t st, double* part = nullptr, long long part_len = 0,
-                       double* dot_out = nullptr) {
+                       double* dot_out = nullptr, int mode = 0, const FineCheb* ch = nullptr) {
   if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal_host || !err || out == u) return LP_ERR_ARG;
   KModal<T> km;
   for (int i = 0; i < 45; ++i) km.c[i] = (T)kmodal_host[i];
   // float32: the packed-pair kernel
   const bool x2 = sizeof(T) == 4;
+  if (mode != 0 && (!x2 || !ch || mode < 0 || mode > 3)) return LP_ERR_ARG;
   const uint32_t zc = 4;
   TileMaps<T> maps;
   const uint64_t nd[4] = {zc * (uint64_t)g.NX(), (uint64_t)g.NY(), (uint64_t)g.pz / zc, 3};
@@ -748,7 +810,11 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
       !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
     return LP_ERR_ARG;
   const int smem = x2 ? (int)sizeof(FineSmem2) + 128 : (int)sizeof(FineSmem<T>) + 128;
-  const void* kfn = x2 ? (const void*)k_apply_fine_x2 : (const void*)k_apply_fine<T>;
+  const void* x2fn = mode == 1   ? (const void*)k_apply_fine_x2<1>
+                     : mode == 2 ? (const void*)k_apply_fine_x2<2>
+                     : mode == 3 ? (const void*)k_apply_fine_x2<3>
+                                 : (const void*)k_apply_fine_x2<0>;
+  const void* kfn = x2 ? x2fn : (const void*)k_apply_fine<T>;
   const long long slots = resident_blocks(kfn, smem);
   if (!slots) return LP_ERR_LAUNCH;
   const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
@@ -776,7 +842,12 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
         memcpy(&bits, &c, 4);
         km2.c[i] = ((unsigned long long)bits << 32) | bits;
       }
-      k_apply_fine_x2<<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err);
+      const FineCheb none{};
+      const FineCheb& c = ch ? *ch : none;
+      if (mode == 1) k_apply_fine_x2<1><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
+      else if (mode == 2) k_apply_fine_x2<2><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
+      else if (mode == 3) k_apply_fine_x2<3><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
+      else k_apply_fine_x2<0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
       LP_LAUNCH_CHECK();
       return LP_OK;
     }
@@ -826,6 +897,24 @@ int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t
 int lpb_apply_fine_f64(double* out, const double* u, const double* e, const uint8_t* mask, const double* kmodal,
                        int* err, int nx, int ny, int nz, int pz, int cpz, void* stream) {
   return launch_fine<double>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream);
+}
+
+// lpb_apply_fine_f32 with a degree-2 Chebyshev update formed where A u is stored: mode 1 (u = d)
+// x = d + (c1 d + c2 dinv (b - A d)); mode 2 (u = x) r = b - A x, d = s dinv r; mode 3 (u = d)
+// x = (x + d) + (c1 d + c2 dinv (r - A d)); coef: the level's Chebyshev coefficients (device);
+// the fields a mode does not name may be NULL
+int lpb_apply_fine_cheb_f32(int mode, float* x, float* r, float* d, const float* u, const float* b, const float* dinv,
+                            const double* coef, const float* e, const uint8_t* mask, const double* kmodal, int* err,
+                            int nx, int ny, int nz, int pz, int cpz, void* stream) {
+  if (!u || !dinv || !coef) return LP_ERR_ARG;
+  float* out = nullptr;
+  if (mode == 1 && x && d && b && u == d && x != d) out = x;
+  if (mode == 2 && r && d && b && u == x && r != u && d != u && r != d) out = r;
+  if (mode == 3 && x && d && r && u == d && x != d && r != d && r != x) out = x;
+  if (!out) return LP_ERR_ARG;
+  const FineCheb ch{x, r, d, b, dinv, coef};
+  return launch_fine<float>(out, u, e, mask, kmodal, err, lp_grid(nx, ny, nz, pz, cpz), (cudaStream_t)stream, nullptr,
+                            0, nullptr, mode, &ch);
 }
 
 // lpb_apply_fine_f64 that also forms u . out over the level's nodes into *dot (float64, device):

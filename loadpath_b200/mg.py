@@ -88,7 +88,10 @@ class FineApplyProbe:
     def __init__(self, n=512):
         self.pending = []        # eager launches, read at summary()
         self.capture = None      # pairs recorded while a graph is being captured
-        self.totals = {"f32_ms": 0.0, "f32_count": 0, "f64_ms": 0.0, "f64_count": 0}
+        # f32 / f64: the plain applies; f32c1..f32c3: the float32 applies that form a Chebyshev
+        # update as they store (modes 1..3 of lpb_apply_fine_cheb_f32)
+        self.totals = {f"{k}_{v}": (0.0 if v == "ms" else 0) for k in ("f32", "f64", "f32c1", "f32c2", "f32c3")
+                       for v in ("ms", "count")}
         self.pool = []
         self._grow(n)
 
@@ -110,7 +113,7 @@ class FineApplyProbe:
 
     def harvest(self, pairs, recycle=False):
         for dt, a, b in pairs:
-            k = "f32" if dt == torch.float32 else "f64"
+            k = dt if isinstance(dt, str) else ("f32" if dt == torch.float32 else "f64")
             self.totals[k + "_ms"] += a.elapsed_time(b)
             self.totals[k + "_count"] += 1
             if recycle:
@@ -820,6 +823,26 @@ class GridElasticity:
                                                     0, n, st)
             return x
         coef = lv.coef.data_ptr()
+        if self.degree == 2 and lv.kind == "scaled" and dt == torch.float32:
+            # the fine float32 level forms each update where its tiled apply stores A u
+            def fused(mode, u):
+                probe = _PROBE[0]
+                if probe is not None:
+                    ea, eb = probe.take()
+                    L.lpb_event_record(ea.cuda_event, st)
+                L.lpb_apply_fine_cheb_f32(mode, x.data_ptr(), r.data_ptr(), d.data_ptr(), u.data_ptr(), b.data_ptr(),
+                                          lv.dinv.data_ptr(), coef, lv.e.data_ptr(), lv.mask.data_ptr(),
+                                          lv.kmodal.ctypes.data, lv.err.data_ptr(), *g.args, st)
+                if probe is not None:
+                    L.lpb_event_record(eb.cuda_event, st)
+                    (probe.capture if probe.capture is not None else probe.pending).append((f"f32c{mode}", ea, eb))
+            if from_zero:
+                getattr(L, f"lpb_cheb_d_start_{sfx}")(b.data_ptr(), lv.dinv.data_ptr(), coef, d.data_ptr(), n, st)
+                fused(1, d)
+            else:
+                fused(2, x)
+                fused(3, d)
+            return x
         if self.degree == 2 and lv.kind == "explicit" and lv.km is not None:
             # the explicit levels form each update in the gather of A u (the same expressions)
             def fused(mode, u):
