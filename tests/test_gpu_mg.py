@@ -331,3 +331,77 @@ def test_explicit_levels_modal_form_matches_node_basis():
         ga, gb = gr.nodes_to_host(a), gr.nodes_to_host(b)
         np.testing.assert_allclose(ga, gb, rtol=2e-5, atol=2e-5 * np.abs(gb).max())
     assert listed > 0
+
+
+def test_smoothing_forms_match_two_launch_form():
+    """The applies that form a Chebyshev update where they store A u (the fine float32 stencil
+    kernel and the explicit levels' gather, modes 1-3) give the bits of the plain apply followed
+    by the vector kernel of the same step (lpb_cheb2_zero / lpb_residual_scaled / lpb_cheb2)."""
+    from loadpath_b200._lib import lib
+    from loadpath_b200.grid import stream_handle
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from oracle import ref_numpy as R
+
+    dims = (32, 16, 16)
+    x = R.log_uniform_density(dims, 6)
+    e = R.simp_moduli(x)
+    fixed, _ = R.cantilever_bc(dims)
+    mesh = BoxMesh(dims)
+    ge = GridElasticity(mesh, 0.3, ge_fixed(mesh, fixed), coarse_cells=20, element="im")
+    ge.set_moduli(e.reshape(-1))
+    L, st = lib(), stream_handle()
+    coef = torch.tensor([0.0, 0.7, 0.3, 0.2] + [0.0] * 12, dtype=torch.float64, device="cuda")
+    levels = [ge._l0s] + [lv for lv in ge.levels[1:] if lv.kind == "explicit" and lv.km is not None]
+    assert levels[0].kind == "scaled" and levels[0].dtype == torch.float32 and len(levels) > 1
+    rng = np.random.default_rng(7)
+    for lv in levels:
+        gr = lv.grid
+        n = gr.n_node_field
+        m = gr.mask_to_host(lv.mask)
+
+        def fld():
+            return gr.nodes_to_dev((rng.standard_normal(gr.node_shape) * m).astype(np.float32), torch.float32)
+
+        b0, d0, x0, r0 = fld(), fld(), fld(), fld()
+
+        def fused(mode, xx, rr, dd, u):
+            if lv.kind == "scaled":
+                rc = L.lpb_apply_fine_cheb_f32(mode, xx.data_ptr(), rr.data_ptr(), dd.data_ptr(), u.data_ptr(),
+                                               b0.data_ptr(), lv.dinv.data_ptr(), coef.data_ptr(), lv.e.data_ptr(),
+                                               lv.mask.data_ptr(), lv.kmodal.ctypes.data, lv.err.data_ptr(),
+                                               *gr.args, st)
+            else:
+                rc = L.lpb_apply_explicit_modal_cheb_f32(mode, xx.data_ptr(), rr.data_ptr(), dd.data_ptr(),
+                                                         u.data_ptr(), b0.data_ptr(), lv.dinv.data_ptr(),
+                                                         coef.data_ptr(), lv.km.data_ptr(), lv.kpc.data_ptr(),
+                                                         lv.glist.data_ptr(), lv.gcount.data_ptr(), lv.ft.data_ptr(),
+                                                         lv.mask.data_ptr(), *gr.args, st)
+            assert rc == 0
+
+        t = gr.node_field(torch.float32)
+        # mode 1: x = d + (c1 d + c2 dinv (b - A d))
+        xa = x0.clone()
+        fused(1, xa, r0.clone(), d0, d0)
+        xb = x0.clone()
+        lv.apply(t, d0)
+        L.lpb_cheb2_zero_f32(xb.data_ptr(), b0.data_ptr(), t.data_ptr(), d0.data_ptr(), lv.dinv.data_ptr(),
+                             coef.data_ptr(), n, st)
+        assert torch.equal(xa, xb)
+        # mode 2: r = b - A x, d = s dinv r
+        ra, da = r0.clone(), d0.clone()
+        fused(2, x0, ra, da, x0)
+        rb, db = r0.clone(), d0.clone()
+        lv.apply(t, x0)
+        L.lpb_residual_scaled_f32(b0.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(), coef.data_ptr(), rb.data_ptr(),
+                                  db.data_ptr(), n, st)
+        assert torch.equal(ra, rb) and torch.equal(da, db)
+        # mode 3: x = (x + d) + (c1 d + c2 dinv (r - A d))
+        xa = x0.clone()
+        fused(3, xa, r0, d0, d0)
+        xb = x0.clone()
+        lv.apply(t, d0)
+        L.lpb_cheb2_f32(xb.data_ptr(), d0.data_ptr(), r0.data_ptr(), t.data_ptr(), lv.dinv.data_ptr(),
+                        coef.data_ptr(), n, st)
+        assert torch.equal(xa, xb)
+        assert float(xa.abs().max()) > 0
+    ge.check_device()
