@@ -2,15 +2,22 @@
 """SIMP iterations per second at 256x128x128 hex8 (12.8M DOF) on B200, mixed precision,
 with the plain FP64 GPU path and the K*u apply's HBM roofline beside it.
 
-One step = one SIMP iteration of the plain top3d loop on the device: SIMP law, Galerkin
-multigrid hierarchy build, MG-PCG solve to rtol 1e-6 (warm-started), element energies,
-compliance and sensitivities, density-filter chain rule, OC bisection, filtered densities.
+One step = one SIMP iteration of the plain top3d loop on the device, from the same seeded
+design every step: SIMP law, Galerkin multigrid hierarchy build, MG-PCG solve to rtol 1e-6 from
+zero, element energies, compliance and sensitivities, density-filter chain rule, OC bisection,
+filtered densities and moduli of the new design. Each step does identical work whatever --steps
+is (the solve takes the reference's 17 CG iterations on this design).
 Workload (synthetic, seeded): cantilever with the x = 0 face held and a unit -z load spread over
-the bottom edge at x = nx; initial density log-uniform in [1e-3, 1] (seed 1) smoothed by the
-r = 2 cone filter; E0 = 1, Emin = 1e-9, nu = 0.3, p = 3, volume fraction 0.3, filter r = 2,
-move 0.2, incompatible-mode hex8, 5-level hierarchy (coarse_cells 2000).
+the bottom edge at x = nx; density log-uniform in [1e-3, 1] (seed 1) smoothed by the r = 2 cone
+filter (row-normalised); E0 = 1, Emin = 1e-9, nu = 0.3, p = 3, volume fraction 0.3, filter
+r = 2, move 0.2, incompatible-mode hex8, 5-level hierarchy (coarse_cells 2000).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--evolve runs the loop instead (each step's design is the last step's output, warm-started
+solves) and reports its CG counts; the designs of that loop sharpen into 1e9 stiffness contrasts
+that the multigrid takes hundreds of CG iterations on (the reference's SIMP driver leaves the
+multigrid past 60 CG iterations for a factorisation or AMG-CG, loadpath/simp.py:85, 735).
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of the workload
 (the loop does not shard: replicas only), the step time is the max over ranks.
@@ -40,13 +47,16 @@ METRIC = "SIMP iter/s & K*u GB/s at 12.7M DOF: mixed-prec vs FP64 GPU, <=1e-6 re
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--dims", default=",".join(str(d) for d in DIMS))
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 GPU comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--evolve", action="store_true",
+                   help="step the evolving SIMP loop (each step from the last step's design, warm-started "
+                        "solves) instead of the fixed-work iteration from the seeded design")
     p.add_argument("--micro", choices=["apply", "band", "cases", "full"], default=None,
                    help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
                         "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
@@ -73,12 +83,18 @@ def parse():
     return a
 
 
-def workload_config(dims, world):
+def workload_config(dims, world, evolve=False):
     """The `config` both arms print: the bench workload and its sizes."""
-    return {"workload": f"plain SIMP iteration, cantilever {'x'.join(map(str, dims))} hex8 "
-                        f"({3 * math.prod(d + 1 for d in dims)} DOF), MG-PCG rtol {RTOL}, "
-                        "V-cycle float32, CG float64",
-            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (fields of 51-103 MB)"}
+    dof = 3 * math.prod(d + 1 for d in dims)
+    if evolve:
+        what = (f"evolving plain SIMP loop (warm-started solves), cantilever {'x'.join(map(str, dims))} hex8 "
+                f"({dof} DOF), MG-PCG rtol {RTOL}, V-cycle float32, CG float64")
+    else:
+        what = (f"plain SIMP iteration from the seeded config-1 design (log-uniform density, seed 1, r=2 smoothed), "
+                f"cantilever {'x'.join(map(str, dims))} hex8 ({dof} DOF): hierarchy build, MG-PCG from zero to rtol "
+                f"{RTOL} (V-cycle float32, CG float64), sensitivities, filter chain rule, OC; same design every step")
+    return {"workload": what, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (fields of 51-103 MB)"}
 
 
 def cantilever(dims):
@@ -192,18 +208,20 @@ def cpu_apply_times(dims, reps64=3, reps32=3):
     return out, cport.threads()
 
 
-# CG iterations of SIMP iterations 1, 2, ... of this (deterministic) workload at 256x128x128,
-# from the mixed-precision GPU path; the reference arm times the CPU operator for the same counts
-CG_ITERS_256 = (17, 25, 15, 16, 20, 25, 39, 57, 78, 208, 118, 114)
+# CG iterations of the reference's own solve (loadpath/mg.py GridElasticity, float32 V-cycle,
+# rtol 1e-6, from zero) on the bench's design at 256x128x128: C = 257.0077140996013 in 17
+CG_REFERENCE_256 = 17
+C_REFERENCE_256 = 257.0077140996013
 
 
 def fine_applies(cg_iters):
-    """Fine-level applies per SIMP iteration, averaged over iterations with these CG counts:
-    float64 = the CG iterations + the warm-start apply; float32 = four per V-cycle (one per CG
-    iteration and one before the loop) + 12 power iterations."""
+    """Fine-level applies of SIMP iterations whose solves start from zero, averaged over
+    iterations with these CG counts (loadpath/mg.py:872-926): float64 = one per CG iteration;
+    float32 = four per V-cycle (one V-cycle before the loop and one after every iteration but
+    the last) + 12 power iterations."""
     n = max(len(cg_iters), 1)
-    n64 = sum(c + 1 for c in cg_iters) / n
-    n32 = sum(12 + 4 * (c + 1) for c in cg_iters) / n
+    n64 = sum(c for c in cg_iters) / n
+    n32 = sum(12 + 4 * c for c in cg_iters) / n
     return int(round(n64)), int(round(n32))
 
 
@@ -211,32 +229,64 @@ def cpu_iteration_estimate(dims, n64, n32):
     t, cores = cpu_apply_times(dims)
     sec = n64 * t["float64"] + n32 * t["float32"]
     return {"value": 1.0 / sec, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
-            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) on {cores} threads: "
-                       f"{t['float64'] * 1e3:.1f} ms per float64 and {t['float32'] * 1e3:.1f} ms per float32 "
-                       f"fine-level apply at {dims[0]}x{dims[1]}x{dims[2]}, times the {n64} float64 + {n32} float32 "
-                       "fine applies one SIMP iteration makes; coarse levels, setup, filter and OC not counted "
-                       "(a lower bound on the CPU iteration time)")}
+            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) on {cores} threads, "
+                       f"3 applies per precision: {t['float64'] * 1e3:.1f} ms per float64 and "
+                       f"{t['float32'] * 1e3:.1f} ms per float32 fine-level apply at {dims[0]}x{dims[1]}x{dims[2]}, "
+                       f"scaled to the {n64} float64 + {n32} float32 fine applies one SIMP iteration makes; coarse "
+                       "levels, setup, filter and OC not counted (a lower bound on the CPU iteration time)")}
 
 
 def run_reference(args):
+    """The reference arm: every fine-level apply one SIMP iteration of the workload makes
+    (its solve's float64 CG applies and float32 V-cycle and power-iteration applies), executed
+    by the oracle's C port of the reference's CPU operator on all host cores, per step. Coarse
+    levels, setup, filter and OC are not run (a lower bound on the reference's CPU time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # fine applies per SIMP iteration for the CG counts of the same iterations on the GPU path
-    # (iterations warmup + 1 .. warmup + steps of this workload)
-    seq = CG_ITERS_256[args.warmup:args.warmup + args.steps] if tuple(args.dims) == DIMS else ()
-    n64, n32 = fine_applies(seq if len(seq) == args.steps else (17,))
-    cb = cpu_iteration_estimate(args.dims, n64, n32)
-    vals = []
-    for _ in range(args.warmup + args.steps):
-        t, _ = cpu_apply_times(args.dims, 1, 1)
-        vals.append(1.0 / (n64 * t["float64"] + n32 * t["float32"]))
-    v = statistics.median(vals[args.warmup:])
+    from oracle import cport
+    from oracle import ref_numpy as R
+
+    dims = tuple(args.dims)
+    n64, n32 = fine_applies((CG_REFERENCE_256,))
+    nx, ny, nz = dims
+    rng = np.random.default_rng(101)
+    e = R.simp_moduli(R.log_uniform_density(dims, 1))
+    m = np.ones((3, nx + 1, ny + 1, nz + 1))
+    m[:, 0] = 0.0
+    ke = R.hex8_ke(0.3, "im")
+    u = rng.standard_normal(m.shape) * m
+    ops = {}
+    for dt in (np.float64, np.float32):
+        op = cport.MaskedApply(ke, e, m, dt)
+        uu = u.astype(dt)
+        ops[dt] = (op, uu, np.empty_like(uu))
+
+    def step():
+        for dt, n in ((np.float64, n64), (np.float32, n32)):
+            op, uu, o = ops[dt]
+            for _ in range(n):
+                op(uu, o)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    sec = (time.perf_counter() - t0) / args.steps
+    v = 1.0 / sec
+    cores = cport.threads()
+    cb = {"value": v, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
+          "sample": (f"per step, the {n64} float64 + {n32} float32 fine-level applies one SIMP iteration of the "
+                     f"workload makes ({CG_REFERENCE_256} CG iterations, the reference's own count on this design), "
+                     f"executed by the C port of the reference's two-pass CPU operator (loadpath/mgops.py) on "
+                     f"{cores} threads at {nx}x{ny}x{nz}; coarse levels, setup, filter and OC not run (a lower "
+                     "bound on the CPU iteration time)")}
     line = {"metric": METRIC, "value": v, "unit": "SIMP iter/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": workload_config(args.dims, args.gpus),
-            "impl": "reference", "cpu_baseline": dict(cb, value=v),
+            "config": workload_config(dims, args.gpus, args.evolve),
+            "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "SIMP iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -278,13 +328,20 @@ def run_b200(args):
         if world > 1:
             dist.barrier()
 
+    def one_step(lp):
+        # the fixed-work step starts every iteration from the seeded design (device copies and
+        # the SIMP law, inside the timed region); --evolve steps the loop on
+        if not args.evolve:
+            lp.restart()
+        return lp.step()
+
     # ---- device-resident timing -----------------------------------------------------------
     loop = new_loop(np.float32)
     if args.eager:
         loop.ge.use_graphs = False
         loop.ge.device_loop = False
     for _ in range(args.warmup):
-        loop.step()
+        one_step(loop)
     barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
@@ -297,7 +354,7 @@ def run_b200(args):
     t0.record()
     iters = []
     for _ in range(args.steps):
-        loop.step()
+        one_step(loop)
         iters.append(loop.ge.last_iters)
     t1.record()
     torch.cuda.nvtx.range_pop()
@@ -318,7 +375,7 @@ def run_b200(args):
     probe = mg.FineApplyProbe()
     mg.set_probe(probe)
     for _ in range(args.steps):
-        loop.step()
+        one_step(loop)
     mg.set_probe(None)
     fine = probe.summary()
     peak, peak_kind = peaks()
@@ -384,20 +441,28 @@ def run_b200(args):
         del u32, dc32, u_or, dc_or
         ref.ge.rtol = RTOL
         for _ in range(args.warmup - 1):
-            ref.step()
+            one_step(ref)
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record()
+        it64 = []
         for _ in range(args.steps):
-            ref.step()
+            one_step(ref)
+            it64.append(ref.ge.last_iters)
         a1.record()
         torch.cuda.synchronize()
         v64 = args.steps / (a0.elapsed_time(a1) / 1e3)
-        fp64 = {"value": v64, "unit": "SIMP iter/s", "mixed_over_fp64": value / world / v64,
+        fp64 = {"value": v64, "unit": "SIMP iter/s", "mixed_over_fp64": value / world / v64, "cg_iterations": it64,
                 "rel_err_vs_fp64_oracle": {"compliance": abs(c32 - c_or) / abs(c_or),
                                            "compliance_fp64_path": abs(c64 - c_or) / abs(c_or),
-                                           "displacement": du, "sensitivity": dsens}}
+                                           "displacement": du, "sensitivity": dsens},
+                "fp64_oracle_compliance": c_or, "mixed_compliance": c32}
+        if tuple(dims) == DIMS:
+            # the reference's own solve of this design (loadpath/mg.py GridElasticity on the CPU,
+            # rtol 1e-6, 17 CG iterations)
+            fp64["rel_diff_vs_reference_cpu_solve"] = {"mixed": abs(c32 - C_REFERENCE_256) / C_REFERENCE_256,
+                                                       "fp64_oracle": abs(c_or - C_REFERENCE_256) / C_REFERENCE_256}
         del ref, mix
         torch.cuda.empty_cache()
 
@@ -407,17 +472,22 @@ def run_b200(args):
         loop = new_loop(np.float32)
         x_host = torch.from_numpy(np.ascontiguousarray(x0_host)).pin_memory()
         out_host = torch.empty_like(x_host).pin_memory()
-        # the same warm-up as the device-timed loop, so both time the same SIMP iterations
-        # each step's output design is the next step's input: the two pinned buffers swap roles
+        # the same warm-up as the device-timed loop, so both time the same SIMP iterations; with
+        # --evolve each step's output design is the next step's input (the pinned buffers swap
+        # roles), else every step takes the seeded design in again
         for _ in range(args.warmup):
-            loop.step_host(x_host, out_host)
-            x_host, out_host = out_host, x_host
+            loop.step_host(x_host, out_host, restart=not args.evolve)
+            if args.evolve:
+                x_host, out_host = out_host, x_host
         barrier()
         torch.cuda.synchronize()
         w0 = time.perf_counter()
+        e2e_iters = []
         for _ in range(args.steps):
-            c, _ = loop.step_host(x_host, out_host)
-            x_host, out_host = out_host, x_host
+            c, _ = loop.step_host(x_host, out_host, restart=not args.evolve)
+            e2e_iters.append(loop.ge.last_iters)
+            if args.evolve:
+                x_host, out_host = out_host, x_host
         torch.cuda.synchronize()
         w = time.perf_counter() - w0
         if world > 1:
@@ -426,8 +496,11 @@ def run_b200(args):
             w = float(tt.item())
         nb = int(np.prod(dims)) * 8
         e2e = {"value": world * args.steps / w, "unit": "SIMP iter/s", "h2d_bytes_per_step": nb,
-               "d2h_bytes_per_step": nb + 16,
-               "api": "Top3dLoop.step_host: design in from pinned host memory, filtered design and compliance out"}
+               "d2h_bytes_per_step": nb + 16, "cg_iterations": e2e_iters,
+               "api": ("Top3dLoop.step_host: the design in from pinned host memory (restart: taken as its own "
+                       "physical density), the updated design, compliance and change out"
+                       if not args.evolve else
+                       "Top3dLoop.step_host: design in from pinned host memory, updated design and compliance out")}
         del loop
 
     # ---- CPU baseline (rank 0, N = 1 only) -----------------------------------------------------
@@ -445,7 +518,7 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded log-uniform density smoothed by the r=2 filter; cantilever loads)",
-            "config": workload_config(dims, world),
+            "config": workload_config(dims, world, args.evolve),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "fp64_gpu_path": fp64, "detail": extra}
     print(json.dumps(line))
@@ -766,12 +839,17 @@ def run_kernels(args):
     # the activity trace does not list kernels run inside a graph's conditional (WHILE) node,
     # so the table is taken with the host-tested CG loop: the same kernels in the same order
     loop.ge.device_loop = False
-    for _ in range(args.warmup):
+    def one_step():
+        if not args.evolve:
+            loop.restart()
         loop.step()
+
+    for _ in range(args.warmup):
+        one_step()
     torch.cuda.synchronize()
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         for _ in range(args.kernels):
-            loop.step()
+            one_step()
         torch.cuda.synchronize()
     agg = collections.defaultdict(lambda: [0, 0.0])
     for ev in prof.events():

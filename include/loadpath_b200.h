@@ -96,9 +96,12 @@ int lpb_apply_explicit_sym_f64(double* out, const double* u, const double* kp, d
 /* lpb_apply_explicit_sym_f32 for callers that cannot allocate device memory (a host that owns
  * every device allocation, or a loop that must not call cudaMalloc/cudaFree, which synchronize):
  * the (24, cells) intermediate lives in a 6 MB array inside the library instead of a caller
- * buffer. At most 65,536 padded cells (nx * ny * cpz) per call, else -3. The first call on a
- * device looks the array up and should come before any stream capture; calls that overlap on
- * the GPU share the array and race. No counterpart in the reference. */
+ * buffer. At most 65,536 padded cells (nx * ny * cpz) per call, else -3. The array's address is
+ * looked up for the CURRENT device (cudaGetDevice), so the stream must belong to the current
+ * device. The first call on a device looks the array up and should come before any stream
+ * capture; the address is kept for the life of the process and is not looked up again after a
+ * cudaDeviceReset (do not call this after resetting a device). Calls that overlap on the GPU
+ * share the array and race. No counterpart in the reference. */
 int lpb_apply_explicit_sym_noalloc_f32(float* out, const float* u, const float* kp, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* (cells, 24, 24) matrices -> packed symmetric entry-major (the mean of K and K^T) */
 int lpb_pack_sym_f32(float* kp, const float* k, long long ncells, void* stream);

@@ -1156,7 +1156,9 @@ static int launch_explicit(T* out, const T* u, const T* kp, T* ft, const uint8_t
 #define LP_NOALLOC_MAX_DEVICES 64
 static __device__ __align__(256) float g_explicit_scratch[24 * LP_NOALLOC_MAX_CELLS];
 
-// the array's device address on the current device, looked up once per device
+// the array's device address on the current device, looked up once per device ordinal and kept
+// for the life of the process: the caller's stream must belong to the current device, and a
+// cudaDeviceReset invalidates the kept address (callers must not reset a device they use it on)
 static float* explicit_scratch_address() {
   static std::mutex mu;
   static float* addr[LP_NOALLOC_MAX_DEVICES] = {};

@@ -1022,7 +1022,13 @@ class GridElasticity:
         converged). Nothing waits on the host before the first iteration: the warm-start
         choice is made on the device, and |b| reaches the host with the first iteration's
         scalars. With graphs on, the set-up, the CG head (A p, alpha, x, r, |r|^2) and the CG
-        tail (V-cycle, beta, p) are each one graph launch."""
+        tail (V-cycle, beta, p) are each one graph launch.
+
+        When converged is False, x is undefined: the host-tested loop queues an iteration's
+        tail (which moves x by alpha p) before it reads that iteration's p.Ap, so on the
+        p.Ap <= 0 exit x has taken one step past the iterate the reference returns
+        (loadpath/mg.py:903-905). Callers discard it (solve_device raises, the strict fallback
+        starts again from the caller's x0)."""
         L = lib()
         g = self.g0
         n = g.n_node_field

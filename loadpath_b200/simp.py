@@ -176,6 +176,20 @@ def adjoint_sensitivity(ge, pairs, xp, dproj, out, modulus=1.0, penal=3.0, emin=
 
 ALIVE = 1e-3          # cells at or below this projected density leave the solve (loadpath/simp.py:59)
 REDUCE_BELOW = 0.8    # ...once fewer than this share of the cells are alive (loadpath/simp.py:61)
+MG_SLOW_ITERS = 60    # CG iterations past which the SIMP driver leaves the multigrid (loadpath/simp.py:85)
+MG_MAXITER = 2000     # the SIMP driver's CG cap for its multigrid (loadpath/simp.py:182)
+
+
+def _cells_touching(node_flags):
+    """bool (nx, ny, nz): cells with any of their eight corner nodes set in node_flags
+    (nx+1, ny+1, nz+1)."""
+    n = np.asarray(node_flags, bool)
+    out = np.zeros(tuple(d - 1 for d in n.shape), bool)
+    for i in (0, 1):
+        for j in (0, 1):
+            for k in (0, 1):
+                out |= n[i:i + out.shape[0], j:j + out.shape[1], k:k + out.shape[2]]
+    return out
 
 
 class LiveCells:
@@ -405,11 +419,23 @@ class Top3dLoop:
     dims: cells (even counts); fixed_grid: bool (3, nx+1, ny+1, nz+1); f_grid: float64 loads on
     the same grid, or a list of them (load cases: the objective is their equally weighted
     compliance sum, the cases solved as one block of right-hand sides); x0: optional initial
-    density (cells), default volfrac everywhere."""
+    density (cells), default volfrac everywhere.
+
+    live_cells: solve the way loadpath's SIMP driver runs its multigrid (loadpath/simp.py:720-826,
+    `_solve` / `_solve_mg`): once fewer than REDUCE_BELOW of the cells are alive (physical density
+    above ALIVE, or touching a support or a load), only the alive cells 26-connected to a support
+    keep their moduli; a load left on a dof without stiffness, or a reduced solve that fails, goes
+    back to the full grid. Off (the default), every solve is on the full grid as top3d's direct
+    solve. Either way a solve that takes more than slow_iters CG iterations (the driver's
+    MG_SLOW_ITERS, loadpath/simp.py:85) is recorded in self.slow_solves as (iteration, CG count):
+    the reference's driver then leaves the multigrid for a factorisation or AMG-CG, which this
+    package does not build, so the answer is kept and the caller can see it. maxiter defaults to
+    the driver's own cap (2000, loadpath/simp.py:182)."""
 
     def __init__(self, dims, volfrac, rmin, fixed_grid, f_grid, nu=0.3, element=None, penal=3.0, emin=1e-9,
-                 move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=500,
-                 smoother="chebyshev", warm_start=True, block_cases=True, autotune=True, device="cuda"):
+                 move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=MG_MAXITER,
+                 smoother="chebyshev", warm_start=True, block_cases=True, autotune=True, device="cuda",
+                 live_cells=False, slow_iters=MG_SLOW_ITERS):
         dims = tuple(int(d) for d in dims)
         if any(d % 2 for d in dims):
             raise ValueError("the device SIMP loop takes even cell counts (the multigrid pads odd ones)")
@@ -434,6 +460,7 @@ class Top3dLoop:
         else:
             g.cells_to_dev(np.asarray(x0, np.float64), torch.float64, out=self.x)
         self.xphys = self.x.clone()
+        self._x_start = None     # restart(): the design the loop was constructed with
         self._x_stage = None     # step_host: the design in grid order on the device
         self.xnew = g.cell_field(torch.float64)
         self.e = g.cell_field(torch.float64)
@@ -454,10 +481,57 @@ class Top3dLoop:
         self.loop = 0
         self.history = []
         self.timing = None       # a list to collect per-phase CUDA events into, or None
+        self.slow_iters = int(slow_iters)
+        self.slow_solves = []    # (iteration, CG iterations) of solves above slow_iters
+        self.live = None
+        self.reduced = False     # the last solve ran on the live cells only
+        if live_cells:
+            held = np.asarray(fixed_grid, bool).reshape(g.node_shape).any(axis=0)
+            loaded = np.zeros(g.node_shape[1:], bool)
+            for fk in cases:
+                loaded |= (np.asarray(fk).reshape(g.node_shape) != 0).any(axis=0)
+            self.live = LiveCells(g, _cells_touching(held), _cells_touching(held | loaded))
         lib().lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, stream_handle())
+        self._x_start = self.x.clone()
+
+    def restart(self, x=None):
+        """Put the loop back at a first iteration: the design x (a float64 device cell field in the
+        padded layout; default: the design the loop was constructed with) becomes both the design
+        and its physical density, as top3d starts (loadpath/benchmarks/reference.py:80-82,
+        xPhys = x), the moduli are formed from it and the next solve starts from zero. Device work
+        only: two cell-field copies and the SIMP law."""
+        src = self._x_start if x is None else x
+        L = lib()
+        st = stream_handle()
+        g = self.grid
+        nb = src.numel() * 8
+        for dst in (self.x, self.xphys):
+            if dst.data_ptr() != src.data_ptr():
+                L.lpb_memcpy_async(dst.data_ptr(), src.data_ptr(), nb, st)
+        L.lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, st)
+        self.u = None
+        self.us = None
+        return self
 
     # ---- one iteration -------------------------------------------------------------------
     def _solve_cases(self):
+        try:
+            self._solve_cases_once()
+        except RuntimeError:
+            if not self.reduced:
+                raise
+            # the live cells hang on the rest by an edge or a corner, or a coarse level lost a
+            # thin support: the full grid, void at Emin, holds it (loadpath/simp.py:815-822)
+            self.reduced = False
+            self.ge.set_moduli_device(self.e)
+            self.u = self.us = None
+            self._solve_cases_once()
+        its = self.ge.last_iters
+        worst = max(its) if isinstance(its, (list, tuple)) else its
+        if worst > self.slow_iters:
+            self.slow_solves.append((self.loop, int(worst)))
+
+    def _solve_cases_once(self):
         if len(self.fs) == 1:
             x0 = self.u if (self.warm_start and self.u is not None) else None
             self.u = self.ge.solve_device(self.f, x0)
@@ -476,7 +550,10 @@ class Top3dLoop:
             self.u = self.us[0]
 
     def _set_moduli(self):
-        self.ge.set_moduli_device(self.e)
+        if self.live is not None:
+            self.reduced = self.ge.set_moduli_live(self.e, self.live, self.xphys, self.fs)
+        else:
+            self.ge.set_moduli_device(self.e)
         if self.autotune:
             from .tune import autotune
 
@@ -550,17 +627,23 @@ class Top3dLoop:
         self.history.append((c, change, self.ge.last_iters))
         return c, change
 
-    def step_host(self, x_host, out_host):
+    def step_host(self, x_host, out_host, restart=False):
         """One iteration on a design held in host memory (pinned, so the copies are async):
         the design x (cells, float64) goes in, its physical densities H x / hs and moduli are
-        formed on the device, and the updated design comes back in out_host. Returns
-        (compliance, change)."""
+        formed on the device, and the updated design comes back in out_host. With restart the
+        design is taken as its own physical density and the solve starts from zero (restart()).
+        Returns (compliance, change)."""
         g = self.grid
         if self._x_stage is None:
             self._x_stage = torch.empty(g.cells, dtype=torch.float64, device=g.device)
         self._x_stage.copy_(x_host, non_blocking=True)
-        g.set_cells(self.x, self._x_stage)
-        self.filter.apply(self.xphys, self.x, hs_out=self.filter.hs, e_out=self.e, penal=self.penal, emin=self.emin)
+        if restart:
+            g.set_cells(self.xphys, self._x_stage)
+            self.restart(self.xphys)
+        else:
+            g.set_cells(self.x, self._x_stage)
+            self.filter.apply(self.xphys, self.x, hs_out=self.filter.hs, e_out=self.e, penal=self.penal,
+                              emin=self.emin)
         c, change = self.step()
         out_host.copy_(g.cell_grid(self.x), non_blocking=True)
         torch.cuda.current_stream().synchronize()

@@ -800,13 +800,48 @@ def connected_keep(alive, support_touch):
     return alive & np.isin(lbl, keep_l[keep_l > 0])
 
 
+def cells_touching(node_flags):
+    """Cells with any of their eight corners set in node_flags (nx+1, ny+1, nz+1): the cells
+    touching a support or a load (loadpath/simp.py:150-151, `support_nodes[mesh.enode].any(axis=1)`)."""
+    n = np.asarray(node_flags, bool)
+    dims = tuple(d - 1 for d in n.shape)
+    out = np.zeros(dims, bool)
+    for (i, j, k) in OFFS:
+        out |= n[i:i + dims[0], j:j + dims[1], k:k + dims[2]]
+    return out
+
+
+def live_solve(ke, fixed_grid, f_grid, support_touch, anchor):
+    """solve(e, xphys) with the SIMP driver's live-cell reduction (loadpath/simp.py:725, 795-826):
+    alive = xphys > ALIVE or an anchor cell; when fewer than REDUCE_BELOW of the cells are alive,
+    only the cells connected_keep keeps carry their moduli, dofs left without stiffness are
+    dropped (and are zero in u), and a load on such a dof sends the solve back to the full grid.
+    Direct sparse solves (assembled_solve)."""
+    def solve(e, xphys):
+        alive = (xphys > ALIVE) | anchor
+        if alive.mean() < REDUCE_BELOW:
+            keep = connected_keep(alive, support_touch)
+            er = np.where(keep, e, 0.0)
+            u = assembled_solve(ke, er, fixed_grid, f_grid, drop_dead=True)
+            stiff = np.zeros(tuple(d + 1 for d in e.shape), bool)
+            for (i, j, k) in OFFS:
+                stiff[i:i + e.shape[0], j:j + e.shape[1], k:k + e.shape[2]] |= keep
+            if not np.any(np.asarray(f_grid)[:, ~stiff]):
+                return u
+        return assembled_solve(ke, e, fixed_grid, f_grid)
+    return solve
+
+
 # --------------------------------------------------------------------------
 # assembled direct solve for tiny grids (loadpath/benchmarks/evaluate.py:111-117)
 # --------------------------------------------------------------------------
 
-def assembled_solve(ke, e_grid, fixed_grid, f_grid):
+def assembled_solve(ke, e_grid, fixed_grid, f_grid, drop_dead=False):
     """Direct sparse solve of K(e) u = f on the full node grid, fixed dofs
-    removed (the evaluator's scheme). Returns the node-grid displacement."""
+    removed (the evaluator's scheme). With drop_dead, dofs without stiffness
+    (zero diagonal, cells of modulus 0 only) are removed too and come back as
+    zero, as the multigrid's masks do (loadpath/mg.py:537-550). Returns the
+    node-grid displacement."""
     import scipy.sparse as sp
     import scipy.sparse.linalg as spla
 
@@ -823,19 +858,24 @@ def assembled_solve(ke, e_grid, fixed_grid, f_grid):
     cols = np.tile(dofs, (1, 24)).ravel()
     data = (e_grid[tuple(ijk.T)][:, None, None] * ke[None]).ravel()
     k = sp.csr_matrix((data, (rows, cols)), shape=(3 * nn, 3 * nn))
-    free = np.flatnonzero(~fixed_grid.reshape(-1))
+    keep = ~fixed_grid.reshape(-1)
+    if drop_dead:
+        keep &= k.diagonal() > 1e-300
+    free = np.flatnonzero(keep)
     u = np.zeros(3 * nn)
     u[free] = spla.spsolve(k[free][:, free].tocsc(), f_grid.reshape(-1)[free])
     return u.reshape((3,) + nshape)
 
 
 def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, emin=1e-9, move=0.2,
-               solve=None):
+               solve=None, x0=None, with_xphys=False):
     """top3d's loop with the density filter (loadpath/benchmarks/reference.py:74-117).
     Returns (x, xphys, compliance history, change history). f_grid may be a list of load cases:
     the objective is then their equally weighted compliance sum, and its sensitivity the sum of
     the cases' (the reference's loop has one load; its sums over cases are those of
-    loadpath/simp.py:1901-1904 applied per case). solve(e) returns u, or a list of u per case."""
+    loadpath/simp.py:1901-1904 applied per case). solve(e) returns u, or a list of u per case
+    (solve(e, xphys) with with_xphys). x0: the starting design (default volfrac everywhere),
+    taken as its own physical density as top3d starts."""
     if solve is None:
         if isinstance(f_grid, (list, tuple)):
             solve = lambda e: [assembled_solve(ke, e, fixed_grid, fk) for fk in f_grid]
@@ -844,12 +884,12 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
     taps = filter_taps(rmin)
     hs = filter_row_sums(dims, taps)
     hap = lambda v: grid_filter(v, taps)
-    x = np.full(dims, volfrac)
+    x = np.full(dims, volfrac) if x0 is None else np.array(x0, np.float64)
     xphys = x.copy()
     hist_c, hist_ch = [], []
     for _ in range(iters):
         e = simp_moduli(xphys, penal, emin)
-        us = solve(e)
+        us = solve(e, xphys) if with_xphys else solve(e)
         ce = np.zeros(dims)
         c = 0.0
         for u in (us if isinstance(us, list) else [us]):

@@ -2,7 +2,10 @@
 
 Run in a container that has the loadpath source tree (read-only is fine):
 
-    LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py
+    LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
+
+(names: element transfers femops filter mma hierarchies top3d config0; default all but config0,
+which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
 benchmarks.*), runs them on small seeded inputs and stores inputs and outputs
@@ -19,7 +22,9 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.environ.get("LOADPATH_SRC", "/root/reference")
+SRC = os.environ.get("LOADPATH_SRC")
+if not SRC:
+    raise SystemExit("set LOADPATH_SRC to the loadpath source tree (the folder that holds the loadpath package)")
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "lp_numba_cache"))
 os.environ["LOADPATH_DEVICE"] = "cpu"
 sys.path.insert(0, SRC)
@@ -246,18 +251,38 @@ def make_mma():
     np.savez_compressed(os.path.join(HERE, "mma.npz"), n=n, m=m, steps=len(steps), **out)
 
 
-def main():
-    make_element()
-    make_transfers()
-    make_femops()
-    make_filter()
-    make_mma()
-    make_hierarchy("even_im", (12, 6, 6), "im", 1, 50, 0.02)
-    make_hierarchy("odd_plain", (11, 5, 7), "plain", 2, 30, 0.0)
-    make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0)
-    make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)
-    make_top3d()
+def make_config0():
+    """The 60x20x10 cantilever (top3d's default problem at that size, "im" element) with a unit total
+    load: 20 iterations of the reference's top3d port (SuperLU direct solves), its compliance and
+    change history and the final physical densities."""
+    import dataclasses
+
+    os.environ["LOADPATH_HEX8"] = "im"
+    import loadpath.benchmarks.reference as ref
+    from loadpath.benchmarks.problems import cantilever_3d
+
+    p = cantilever_3d(60, 20, 10, 0.3, 1.5)
+    nodes, comp, val = p.loads[0]
+    p = dataclasses.replace(p, loads=[(nodes, comp, val / (p.dims[1] + 1))])
+    hist = []
+    ref.TOP3D_MAXIT = 20
+    rec = ref.optimize_reference(p, "top3d", on_iter=lambda loop, c, ch: hist.append((c, ch)))
+    ref.TOP3D_MAXIT = 200
+    np.savez_compressed(os.path.join(HERE, "config0.npz"), dims=np.array(p.dims), volfrac=p.volfrac, rmin=p.rmin,
+                        xphys=rec["x"], hist=np.array(hist), load_per_node=val / (p.dims[1] + 1))
+
+
+def main(names=None):
+    gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
+            "mma": make_mma,
+            "hierarchies": lambda: (make_hierarchy("even_im", (12, 6, 6), "im", 1, 50, 0.02),
+                                    make_hierarchy("odd_plain", (11, 5, 7), "plain", 2, 30, 0.0),
+                                    make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
+                                    make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
+            "top3d": make_top3d, "config0": make_config0}
+    for name in names or [k for k in gens if k != "config0"]:
+        gens[name]()
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

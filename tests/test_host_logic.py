@@ -100,3 +100,46 @@ def test_graph_cache_keeps_graphs_across_calls(monkeypatch):
     ge._gen += 1                               # a buffer was replaced: the graphs go
     ge._graph("head", lambda: None)
     assert fake.captured == 2 and fake.freed == 1
+
+
+def test_cells_touching_matches_oracle():
+    """The loop's anchor/support cells (any corner node flagged) against the oracle's restatement
+    of loadpath/simp.py:150-151 on random node flags."""
+    from loadpath_b200.simp import _cells_touching
+    from oracle import ref_numpy as R
+
+    rng = np.random.default_rng(4)
+    flags = rng.random((7, 5, 9)) < 0.05
+    np.testing.assert_array_equal(_cells_touching(flags), R.cells_touching(flags))
+
+
+def test_oracle_live_solve_reduces_and_falls_back():
+    """The oracle's live-cell solve (loadpath/simp.py:795-826): on a design with a floating island
+    the island's dofs come back zero and the answer equals a solve on the kept cells alone; with
+    the load placed on the island it goes back to the full grid."""
+    from oracle import ref_numpy as R
+
+    dims = (8, 3, 3)
+    fixed = np.zeros((3, 9, 4, 4), bool)
+    fixed[:, 0] = True
+    f = np.zeros(fixed.shape)
+    f[2, 3, :, 0] = -0.25
+    x = np.full(dims, 1e-4)
+    x[:4] = 1.0                 # a bar from the support to the load
+    x[6] = 1.0                  # an island, not touching the bar (5 of 8 slabs alive: below 0.8)
+    ke = R.hex8_ke(0.3, "im")
+    e = R.simp_moduli(x)
+    held = fixed.any(axis=0)
+    support = R.cells_touching(held)
+    anchor = R.cells_touching(held | (f != 0).any(axis=0))
+    u = R.live_solve(ke, fixed, f, support, anchor)(e, x)
+    assert np.all(u[:, 6:] == 0.0) and np.any(u[:, 1:4] != 0.0)
+    keep = R.connected_keep((x > R.ALIVE) | anchor, support)
+    assert keep[:4].all() and not keep[4:].any()
+    np.testing.assert_allclose(u, R.assembled_solve(ke, np.where(keep, e, 0.0), fixed, f, drop_dead=True),
+                               rtol=1e-12, atol=1e-14)
+    f2 = np.zeros(fixed.shape)
+    f2[2, 8, 1, 3] = -1.0       # a load on the island: the full grid solves it
+    anchor2 = R.cells_touching(held | (f2 != 0).any(axis=0))
+    u2 = R.live_solve(ke, fixed, f2, support, anchor2)(e, x)
+    np.testing.assert_allclose(u2, R.assembled_solve(ke, e, fixed, f2), rtol=1e-12)
