@@ -57,14 +57,17 @@ def parse():
     p.add_argument("--evolve", action="store_true",
                    help="step the evolving SIMP loop (each step from the last step's design, warm-started "
                         "solves) instead of the fixed-work iteration from the seeded design")
-    p.add_argument("--micro", choices=["apply", "band", "cases", "full"], default=None,
+    p.add_argument("--micro", choices=["apply", "band", "cases", "full", "torchref"], default=None,
                    help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
                         "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
                         "coarsest level's band assembly, factorisation and inverse; cases: the batched "
                         "load-case SIMP iteration (8 point loads at 192x96x96 unless --dims is given), "
                         "the cases solved as one block and one after another; full: the full-scale MMA "
                         "SIMP run (384x192x192 unless --dims is given, --iters iterations) in mixed "
-                        "precision and on the plain FP64 GPU path, final compliance and design compared")
+                        "precision and on the plain FP64 GPU path, final compliance and design compared; torchref: "
+                        "the reference's own torch-CUDA multigrid (loadpath.gpu.TorchMG under "
+                        "mg.GridElasticity(device='cuda'), from the copy installed in baseline/_ref) on the bench's "
+                        "design: hierarchy build and one solve to rtol 1e-6, wall-clock, beside this package's")
     p.add_argument("--iters", type=int, default=100, help="SIMP iterations of --micro full")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--eager", action="store_true",
@@ -814,6 +817,84 @@ def run_micro_full(args):
     return 0
 
 
+def run_micro_torchref(args):
+    """The reference's own GPU path on the bench's design: loadpath.mg.GridElasticity with
+    device='cuda' (its hierarchy built on the host by numba, then loaded into torch tensors; the
+    solve is gpu.TorchMG.solve_mixed: float64 CG and operator on the device, float32 V-cycle, the
+    coarsest level on the host), timed by wall clock (the path synchronises with the host every CG
+    iteration), beside this package's hierarchy build + solve of the same design, CUDA-event timed.
+    Needs the reference installed in baseline/_ref (pip install --target baseline/_ref); prints an
+    `unavailable` line without it."""
+    import torch
+
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "loadpath")):
+        print(json.dumps({"micro": "reference torch-CUDA solve", "unavailable": "baseline/_ref holds no loadpath"}))
+        return 0
+    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "lp_numba_cache"))
+    sys.path.insert(0, ref_dir)
+    from loadpath.fem import HexMesh
+    from loadpath.mg import GridElasticity as RefGE
+
+    from loadpath_b200.grid import DevGrid
+    from loadpath_b200.mg import BoxMesh, GridElasticity
+    from loadpath_b200.simp import case_compliance
+    from oracle import ref_numpy as R
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = tuple(args.dims)
+    x = R.log_uniform_density(dims, 1)
+    e = R.simp_moduli(x)
+    fixed_g, f_g = R.cantilever_bc(dims)
+    mesh = HexMesh(np.argwhere(np.ones(dims, bool)), 1.0, np.zeros(3))
+    fixed = fixed_g.transpose(1, 2, 3, 0).reshape(-1)
+    f = f_g.transpose(1, 2, 3, 0).reshape(-1)
+    out = {"micro": "reference torch-CUDA solve", "dims": list(dims), "rtol": RTOL}
+    ref = RefGE(mesh, 0.3, fixed, rtol=RTOL, device="cuda")
+    runs = []
+    for _ in range(2):       # the first run includes numba compilation
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref.set_moduli(e.reshape(-1))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        u = ref.solve_many([f])[0]
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        runs.append({"set_moduli_s": t1 - t0, "solve_s": t2 - t1, "cg_iterations": int(ref.last_iters),
+                     "compliance": float(f @ u)})
+    out["reference"] = dict(runs[-1], first_run=runs[0], levels=len(ref.levels),
+                            host_threads=int(os.cpu_count() or 1))
+    del ref, u
+    torch.cuda.empty_cache()
+    # this package on the same design
+    bm = BoxMesh(dims)
+    fx = np.empty(bm.n_dof, bool)
+    for i in range(3):
+        fx[i::3] = fixed_g[i].reshape(-1)
+    ge = GridElasticity(bm, 0.3, fx, rtol=RTOL, element="im")
+    dg = DevGrid(dims)
+    ed = dg.cells_to_dev(e, torch.float64)
+    b = dg.nodes_to_dev(f_g, torch.float64)
+    res = []
+    for _ in range(4):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        ge.set_moduli_device(ed)
+        ev[1].record()
+        ud = ge.solve_device(b)
+        ev[2].record()
+        torch.cuda.synchronize()
+        res.append({"set_moduli_s": ev[0].elapsed_time(ev[1]) / 1e3, "solve_s": ev[1].elapsed_time(ev[2]) / 1e3,
+                    "cg_iterations": int(ge.last_iters), "compliance": case_compliance(b, ud)})
+    out["b200"] = res[-1]
+    out["speedup"] = {"solve": out["reference"]["solve_s"] / res[-1]["solve_s"],
+                      "build_and_solve": (out["reference"]["set_moduli_s"] + out["reference"]["solve_s"])
+                      / (res[-1]["set_moduli_s"] + res[-1]["solve_s"])}
+    print(json.dumps(out))
+    return 0
+
+
 def run_kernels(args):
     """Per-kernel device time of args.kernels SIMP iterations after args.warmup, from the CUDA
     activity records (CUPTI through torch.profiler: kernels are not serialised)."""
@@ -882,6 +963,8 @@ def main():
         return run_micro_cases(args)
     if args.micro == "full":
         return run_micro_full(args)
+    if args.micro == "torchref":
+        return run_micro_torchref(args)
     if args.kernels:
         return run_kernels(args)
     if args.impl == "reference":

@@ -430,12 +430,16 @@ class Top3dLoop:
     MG_SLOW_ITERS, loadpath/simp.py:85) is recorded in self.slow_solves as (iteration, CG count):
     the reference's driver then leaves the multigrid for a factorisation or AMG-CG, which this
     package does not build, so the answer is kept and the caller can see it. maxiter defaults to
-    the driver's own cap (2000, loadpath/simp.py:182)."""
+    the driver's own cap (2000, loadpath/simp.py:182).
+
+    shards: a LoadCaseShards over the ranks of a process group (one process per GPU): this
+    rank solves only its cases, and one all-reduce per iteration sums the raw sensitivity and
+    the compliance over the ranks before the filter, so every rank takes the same design step."""
 
     def __init__(self, dims, volfrac, rmin, fixed_grid, f_grid, nu=0.3, element=None, penal=3.0, emin=1e-9,
                  move=0.2, rtol=1e-8, dtype=np.float32, x0=None, coarse_cells=2000, maxiter=MG_MAXITER,
                  smoother="chebyshev", warm_start=True, block_cases=True, autotune=True, device="cuda",
-                 live_cells=False, slow_iters=MG_SLOW_ITERS):
+                 live_cells=False, slow_iters=MG_SLOW_ITERS, shards=None):
         dims = tuple(int(d) for d in dims)
         if any(d % 2 for d in dims):
             raise ValueError("the device SIMP loop takes even cell counts (the multigrid pads odd ones)")
@@ -452,8 +456,11 @@ class Top3dLoop:
         self.grid = g
         self.filter = DeviceFilter(g, rmin, pad=False)
         cases = f_grid if isinstance(f_grid, (list, tuple)) else [f_grid]
-        self.fs = [g.nodes_to_dev(np.asarray(fk, np.float64), torch.float64) for fk in cases]
-        self.f = self.fs[0]
+        self.shards = shards
+        self.c_total = None
+        mine = shards.mine() if shards is not None else range(len(cases))
+        self.fs = [g.nodes_to_dev(np.asarray(cases[i], np.float64), torch.float64) for i in mine]
+        self.f = self.fs[0] if self.fs else None
         self.x = g.cell_field(torch.float64)
         if x0 is None:
             g.set_cells(self.x, self.volfrac)
@@ -491,6 +498,9 @@ class Top3dLoop:
             for fk in cases:
                 loaded |= (np.asarray(fk).reshape(g.node_shape) != 0).any(axis=0)
             self.live = LiveCells(g, _cells_touching(held), _cells_touching(held | loaded))
+            # the dead-load test looks at every case, so all ranks of a sharded loop decide alike
+            self._loads_all = self.fs if shards is None else [
+                g.nodes_to_dev(np.asarray(fk, np.float64), torch.float64) for fk in cases]
         lib().lpb_simp_law(self.e.data_ptr(), self.xphys.data_ptr(), self.penal, self.emin, *g.args, stream_handle())
         self._x_start = self.x.clone()
 
@@ -532,6 +542,10 @@ class Top3dLoop:
             self.slow_solves.append((self.loop, int(worst)))
 
     def _solve_cases_once(self):
+        if not self.fs:          # a rank with no load case of its own (more ranks than cases)
+            self.u, self.us = None, []
+            self.ge.last_iters = 0
+            return
         if len(self.fs) == 1:
             x0 = self.u if (self.warm_start and self.u is not None) else None
             self.u = self.ge.solve_device(self.f, x0)
@@ -551,7 +565,7 @@ class Top3dLoop:
 
     def _set_moduli(self):
         if self.live is not None:
-            self.reduced = self.ge.set_moduli_live(self.e, self.live, self.xphys, self.fs)
+            self.reduced = self.ge.set_moduli_live(self.e, self.live, self.xphys, self._loads_all)
         else:
             self.ge.set_moduli_device(self.e)
         if self.autotune:
@@ -571,11 +585,18 @@ class Top3dLoop:
         L = lib()
         st = stream_handle()
         g = self.grid
-        for k, u in enumerate(self.us):
+        for k, u in enumerate(self.us or ()):
             self.ge.strain_energy_device(u, out=self.ce)
             L.lpb_sensitivity(self.dc.data_ptr(), self.xphys.data_ptr(), self.ce.data_ptr(), self.e.data_ptr(),
                               self.penal, self.emin, 1.0, int(k > 0), self._part.data_ptr(),
                               self._scal[8 + k:].data_ptr(), *g.args, st)
+        if self.shards is not None:
+            # this rank's cases summed; one all-reduce gives every rank the totals, and every rank
+            # then takes the same design step
+            if not self.fs:
+                self.dc.zero_()
+            local = float(self._scal[8:8 + len(self.fs)].sum().item()) if self.fs else 0.0
+            self.c_total = self.shards.reduce(self.dc, local)
         self.filter.apply(self.dcf, self.dc, hs_in=self.filter.hs)
 
     def oc(self):
@@ -623,7 +644,10 @@ class Top3dLoop:
                           emin=self.emin)
         self.x, self.xnew = self.xnew, self.x
         vals = self._scal[:8 + len(self.fs)].cpu().numpy()
-        c, change = float(vals[8:].sum()) if len(self.fs) > 1 else float(vals[8]), float(vals[1])
+        if self.shards is not None:
+            c, change = self.c_total, float(vals[1])
+        else:
+            c, change = float(vals[8:].sum()) if len(self.fs) > 1 else float(vals[8]), float(vals[1])
         self.history.append((c, change, self.ge.last_iters))
         return c, change
 

@@ -868,14 +868,15 @@ def assembled_solve(ke, e_grid, fixed_grid, f_grid, drop_dead=False):
 
 
 def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, emin=1e-9, move=0.2,
-               solve=None, x0=None, with_xphys=False):
+               solve=None, x0=None, with_xphys=False, reduce=None):
     """top3d's loop with the density filter (loadpath/benchmarks/reference.py:74-117).
     Returns (x, xphys, compliance history, change history). f_grid may be a list of load cases:
     the objective is then their equally weighted compliance sum, and its sensitivity the sum of
     the cases' (the reference's loop has one load; its sums over cases are those of
     loadpath/simp.py:1901-1904 applied per case). solve(e) returns u, or a list of u per case
     (solve(e, xphys) with with_xphys). x0: the starting design (default volfrac everywhere),
-    taken as its own physical density as top3d starts."""
+    taken as its own physical density as top3d starts. reduce(ce, c) -> (ce, c): the totals over
+    the load cases other processes solved (the cell energies and compliance summed over ranks)."""
     if solve is None:
         if isinstance(f_grid, (list, tuple)):
             solve = lambda e: [assembled_solve(ke, e, fixed_grid, fk) for fk in f_grid]
@@ -897,6 +898,8 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
             ce_k = np.einsum("in,in->n", g, ke @ g).reshape(dims)
             c += float(np.sum(e * ce_k))
             ce += ce_k
+        if reduce is not None:
+            ce, c = reduce(ce, c)
         dc = -penal * (1 - emin) * xphys ** (penal - 1) * ce
         dc = hap(dc / hs)
         dv = hap(np.ones(dims) / hs)

@@ -90,3 +90,23 @@ def test_load_case_simp_loop_matches_oracle():
     np.testing.assert_allclose([ch for _, ch in got], hch, rtol=1e-5, atol=1e-9)
     np.testing.assert_allclose(loop.xphys_host(), xp_ref, rtol=1e-6, atol=1e-8)
     assert len(loop.history[-1][2]) == 4
+
+
+def test_sharded_loop_single_rank_equals_block_loop():
+    """Top3dLoop with a LoadCaseShards over one rank (no process group: it owns every case) takes the
+    sharded path (compliance summed on the host, the reduction a no-op) and equals the plain
+    load-case loop."""
+    from loadpath_b200.simp import LoadCaseShards, Top3dLoop
+    from oracle import ref_numpy as R
+
+    dims = (16, 8, 8)
+    fixed, _ = R.cantilever_bc(dims)
+    loads = _point_loads(dims, 3, 9)
+    a = Top3dLoop(dims, 0.2, 2.0, fixed, loads, rtol=1e-10, element="plain", coarse_cells=20, autotune=False)
+    b = Top3dLoop(dims, 0.2, 2.0, fixed, loads, rtol=1e-10, element="plain", coarse_cells=20, autotune=False,
+                  shards=LoadCaseShards(len(loads)))
+    ga = [a.step() for _ in range(3)]
+    gb = [b.step() for _ in range(3)]
+    np.testing.assert_allclose([c for c, _ in gb], [c for c, _ in ga], rtol=1e-14)
+    assert [ch for _, ch in gb] == [ch for _, ch in ga]
+    np.testing.assert_array_equal(b.xphys_host(), a.xphys_host())
