@@ -405,7 +405,7 @@ def run_b200(args):
                        "GBps": form_bytes(dims, f) / (fine[f + "_ms"] / fine[f + "_count"] / 1e3) / 1e9}
                    for f in forms}
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "kernel": "k_apply_fine_x2 (float32: plain A u and the Chebyshev-update "
+                    "traffic": traffic, "kernel": "k_apply_fine<float> (plain A u and the Chebyshev-update "
                                               "forms f32c1..3)",
                     "algorithmic_bytes": nbytes / count, "avg_launch_us": avg * 1e6, "launches_timed": count,
                     "forms": by_form,

@@ -58,6 +58,10 @@ int lpb_apply_fine_dot_f64(double* out, const double* u, const double* e, const 
 /* the element matrix (24 x 24, float64, host pointer) in the corner-parity basis that
  * lpb_apply_fine_* reads (45 coefficients, host pointer out); returns the count or < 0 */
 int lpb_modal_ke(const double* ke, double* kmodal_out);
+/* lpb_modal_ke's 45 coefficients -> the seven classes of the unit brick's cubic symmetry the fine
+ * kernel's product uses {a - b, b, d, b2, d2, e2, t} (host pointers); 7, or -1 when the matrix
+ * lacks that symmetry (the reference's element matrices, loadpath/fem.py:191-224, have it). */
+int lpb_modal_sym(const double* kmodal, double* classes_out);
 
 /* ---- coarse levels on the hot path (u zero on masked dofs; out = m K u):
  * level 1: z-marching kernel in the corner-parity basis; g1 is a HOST pointer to the 279

@@ -4,27 +4,39 @@
 //
 // Corner-parity basis. A cell's eight corner values of one component, rewritten in the modes
 // {1, sx, sy, sxsy, sz, sxsz, sysz, sxsysz} (s = +-1 per axis), turn the 24 x 24 element matrix
-// into one with 45 non-zeros (for the plain and the incompatible-mode brick alike, any
-// isotropic nu): three decoupled blocks (linear, bilinear and trilinear modes). The transforms
-// are sums and differences, so a cell costs about 190 flops instead of the dense 1152, which
-// brings the operator under the HBM roofline on CUDA cores.
+// into one with 45 non-zeros (for the plain and the incompatible-mode brick alike, any isotropic
+// nu): three decoupled blocks (linear, bilinear and trilinear modes). The unit brick's cubic
+// symmetry leaves seven coefficient classes in those blocks (lpb_modal_sym), so with the cell's
+// modulus folded into them a cell costs about 140 floating-point operations instead of the dense
+// 1152:
+//   linear normal   {(sx,x), (sy,y), (sz,z)}:      f = (a - b) v + b (v1 + v2 + v3)
+//   linear shear    {(sx,y), (sy,x)} and its two axis permutations: f1 = f2 = d (v1 + v2)
+//                   (the shear strain sees both modes alike: the block has rank one)
+//   bilinear normal {(sxsy,z), (sxsz,y), (sysz,x)}: f = b2 v + b2 (v1 + v2 + v3)
+//   bilinear shear  {(sxsy,x), (sysz,z)} and its two permutations: f1 = d2 v1 + e2 v2, f2 = e2 v1 + d2 v2
+//   trilinear       (sxsysz, c):                  f = t v
 //
 // Work layout. A block owns a 15 x 15 patch of node columns and runs 16 x 16 threads, one per
 // cell column of the patch plus a one-cell halo on the low x and y sides, lanes along x. It
 // marches along z one chunk of four planes at a time: TMA brings the chunk's 17 x 17 node
-// columns (and cell moduli) into a ring of shared-memory stages; in the z-chunked field layout
-// each box row is 17 columns x 4 planes, one contiguous run. A thread reads its four node
-// columns' four planes (and the next chunk's first), forms per plane the x-y modes
-// (4 per component), combines consecutive planes into the cell's z modes, applies E_c K^ in
-// the modal basis and transforms back to the cell's two faces. A node plane's modal force is the upper face of the cell below plus
-// the lower face of the cell above, both in this thread, so z needs no exchange; the four cell
-// columns around a node column exchange their corner forces through shared memory.
-// No atomics, no scatter: every output is written once by its owner.
+// columns and 16 x 16 cell moduli into a ring of shared-memory stages; in the z-chunked field
+// layout every box row is one contiguous run of columns x 4 planes. A thread forms its cells two
+// at a time, cells (0, 1) then (2, 3) of the chunk, as pairs of values: the x-y modes of planes
+// (0, 1) and (2, 3) come from one two-plane load per node column, the next chunk's planes (0, 1)
+// are formed once and carried, and a pair of cells takes its upper planes (1, 2) or (3, 4) from
+// those. A node plane's modal force is the upper face of the cell below plus the lower face of
+// the cell above, both in this thread (a carry between chunks), so z needs no exchange; the four
+// cell columns around a node column meet through warp shuffles (x) and shared memory (y), one
+// block barrier per chunk. No atomics, no scatter: every output is written once by its owner.
+// The pairs are plain registers and scalar instructions: a packed f32x2 form measured slower on
+// B200 (58.8 against 55.3 us at 256 x 128 x 128), its repacking between pairs costing more issue
+// slots than the packing saves.
 //
 // Requirements (checked by the host entry): pz % 4 == 0 and cpz == pz; u, e and the mask
 // hold zeros in the z padding; u is zero on dofs whose mask bit is 0, so the identity rows
 // (1 - m) u of the masked operator vanish and the kernel writes m * K u.
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 
 #include "lp_common.cuh"
@@ -33,478 +45,180 @@
 
 namespace {
 
-constexpr int TXC = 16;   // cell columns per block in x (15 owned node columns)
-constexpr int TYC = 16;   // in y
+constexpr int TXC = 16;         // cell columns per block in x (15 owned node columns)
+constexpr int TYC = 16;         // in y
+constexpr int BOX = TXC + 1;    // 17 node columns per side in a loaded box
+constexpr int NST = 3;          // TMA ring depth (chunks of four z planes; loads run NST - 1 ahead)
 
-template <typename T>
-struct KModal {
-  T c[45];
-};
-
-template <typename T>
-struct Vec4;
-template <>
-struct Vec4<float> {
-  static __device__ __forceinline__ void load(const float* p, float (&v)[4]) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
-  static __device__ __forceinline__ void store(float* p, const float (&v)[4]) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  }
-  static __device__ __forceinline__ void lds(const float* p, float (&v)[4]) {
-    float4 a = *reinterpret_cast<const float4*>(p);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
-  static __device__ __forceinline__ void sts(float* p, const float (&v)[4]) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  }
-};
-template <>
-struct Vec4<double> {
-  static __device__ __forceinline__ void load(const double* p, double (&v)[4]) {
-    double2 a = __ldg(reinterpret_cast<const double2*>(p));
-    double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-  static __device__ __forceinline__ void store(double* p, const double (&v)[4]) {
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
-  }
-  static __device__ __forceinline__ void lds(const double* p, double (&v)[4]) {
-    double2 a = *reinterpret_cast<const double2*>(p);
-    double2 b = *reinterpret_cast<const double2*>(p + 2);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
-  static __device__ __forceinline__ void sts(double* p, const double (&v)[4]) {
-    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-    *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
-  }
-};
-
-// f = K^ v on the 21 non-constant modes (index 3 * mode + component, mode = mx + 2 my + 4 mz);
-// the pattern is fixed, the 45 values come from lpb_modal_ke
-template <typename T>
-__device__ __forceinline__ void modal_product(const KModal<T>& km, const T (&v)[24], T (&f)[24]) {
-  f[0] = f[1] = f[2] = T(0);
-  f[3] = km.c[0] * v[3] + km.c[1] * v[7] + km.c[2] * v[14];
-  f[4] = km.c[3] * v[4] + km.c[4] * v[6];
-  f[5] = km.c[5] * v[5] + km.c[6] * v[12];
-  f[6] = km.c[7] * v[4] + km.c[8] * v[6];
-  f[7] = km.c[9] * v[3] + km.c[10] * v[7] + km.c[11] * v[14];
-  f[8] = km.c[12] * v[8] + km.c[13] * v[13];
-  f[9] = km.c[14] * v[9] + km.c[15] * v[20];
-  f[10] = km.c[16] * v[10] + km.c[17] * v[17];
-  f[11] = km.c[18] * v[11] + km.c[19] * v[16] + km.c[20] * v[18];
-  f[12] = km.c[21] * v[5] + km.c[22] * v[12];
-  f[13] = km.c[23] * v[8] + km.c[24] * v[13];
-  f[14] = km.c[25] * v[3] + km.c[26] * v[7] + km.c[27] * v[14];
-  f[15] = km.c[28] * v[15] + km.c[29] * v[19];
-  f[16] = km.c[30] * v[11] + km.c[31] * v[16] + km.c[32] * v[18];
-  f[17] = km.c[33] * v[10] + km.c[34] * v[17];
-  f[18] = km.c[35] * v[11] + km.c[36] * v[16] + km.c[37] * v[18];
-  f[19] = km.c[38] * v[15] + km.c[39] * v[19];
-  f[20] = km.c[40] * v[9] + km.c[41] * v[20];
-  f[21] = km.c[42] * v[21];
-  f[22] = km.c[43] * v[22];
-  f[23] = km.c[44] * v[23];
-}
-
-constexpr int NSTAGE = 3;           // TMA ring depth (chunks of four z-planes)
-constexpr int BOX = TXC + 1;         // 17 node columns per side in a loaded box
-
-// every TMA destination / source starts on a 128-byte boundary
+// every TMA destination starts on a 128-byte boundary
 template <typename T, int N>
 struct alignas(128) Slot {
   T v[(N * sizeof(T) + 127) / 128 * 128 / sizeof(T)];
 };
 
+// The fields as TMA tensors: a chunk's row of x columns (4 z values each) is the inner
+// dimension, so every box row is one contiguous run.
+struct FineMaps {
+  CUtensorMap u;    // (4 NX, NY, pz / 4, 3), box (4 * 17, 17, 1, 3)
+  CUtensorMap e;    // (4 nx, ny, cpz / 4),    box (4 * 16, 16, 1)
+};
+
+// two values of a field (two cells, or two planes of a node column) carried together
+template <typename T>
+struct Pair {
+  T a, b;
+};
+
+template <typename T>
+struct PairOps {
+  typedef Pair<T> P;
+  static __device__ __forceinline__ P mk(T a, T b) { return P{a, b}; }
+  static __device__ __forceinline__ P add(P x, P y) { return P{x.a + y.a, x.b + y.b}; }
+  static __device__ __forceinline__ P sub(P x, P y) { return P{x.a - y.a, x.b - y.b}; }
+  static __device__ __forceinline__ P mul(P x, P y) { return P{x.a * y.a, x.b * y.b}; }
+  static __device__ __forceinline__ P fma(P x, P y, P z) { return P{fmr(x.a, y.a, z.a), fmr(x.b, y.b, z.b)}; }
+  static __device__ __forceinline__ P zero() { return P{T(0), T(0)}; }
+  static __device__ __forceinline__ P shfl_up1(P v) {
+    return P{__shfl_up_sync(0xffffffffu, v.a, 1, TXC), __shfl_up_sync(0xffffffffu, v.b, 1, TXC)};
+  }
+  // two consecutive values (an even offset into a 4-plane column)
+  static __device__ __forceinline__ P lds2(const T* p);
+  static __device__ __forceinline__ void sts(P* p, P v);
+  static __device__ __forceinline__ float fmr(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ double fmr(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+template <>
+__device__ __forceinline__ PairOps<float>::P PairOps<float>::lds2(const float* p) {
+  const float2 v = *reinterpret_cast<const float2*>(p);
+  return P{v.x, v.y};
+}
+template <>
+__device__ __forceinline__ PairOps<double>::P PairOps<double>::lds2(const double* p) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  return P{v.x, v.y};
+}
+template <>
+__device__ __forceinline__ void PairOps<float>::sts(P* p, P v) {
+  *reinterpret_cast<float2*>(p) = make_float2(v.a, v.b);
+}
+template <>
+__device__ __forceinline__ void PairOps<double>::sts(P* p, P v) {
+  *reinterpret_cast<double2*>(p) = make_double2(v.a, v.b);
+}
+
+// the seven coefficient classes of the symmetric product
+template <typename T>
+struct KSym {
+  T c[7];   // a - b, b, d, b2, d2, e2, t
+};
+
 template <typename T>
 struct FineSmem {
-  Slot<T, 3 * BOX * BOX * 4> u[NSTAGE];              // node values: [comp][y][x][z]
-  Slot<T, BOX * BOX * 4> e[NSTAGE];                  // cell moduli: [y][x][z] (16 used per side)
-  Slot<T, 3 * (TXC - 1) * (TYC - 1) * 4> o[2];       // outputs staged for the TMA store [comp][y][x][z]
-  T red[3][4][TXC * TYC];                            // y-neighbour exchange
-  alignas(8) uint64_t full[NSTAGE];
+  Slot<T, 3 * BOX * BOX * 4> u[NST];                 // node values [comp][y][x][z]
+  Slot<T, TXC * TYC * 4> e[NST];                     // cell moduli [y][x][z]
+  Pair<T> red[2][2][3][TXC * TYC];                   // y exchange [chunk parity][plane pair][comp][thread]
+  alignas(8) uint64_t full[NST];
 };
 
 template <typename T>
-__device__ __forceinline__ T* u_at(FineSmem<T>& sm, int s, int c, int x, int y) {
+__device__ __forceinline__ const T* col_at(const FineSmem<T>& sm, int s, int c, int x, int y) {
   return &sm.u[s].v[((c * BOX + y) * BOX + x) * 4];
 }
 
-// The fields as TMA tensors: a chunk's row of x columns (4 z values each) is the inner
-// dimension, so every box row is 16 * (x extent) contiguous bytes.
+// x-y modes of two consecutive planes (zo = 0: planes 0, 1; zo = 2: planes 2, 3) of the thread's
+// four node columns 00, 10, 01, 11: m[q][c], q = const, sx, sy, sxsy
 template <typename T>
-struct TileMaps {
-  CUtensorMap u;    // (4 NX, NY, pz / 4, 3), box (4 * 17, 17, 1, 3)
-  CUtensorMap e;    // (4 nx, ny, cpz / 4),    box (4 * 17, 17, 1)
-  CUtensorMap out;  // (4 NX, NY, pz / 4, 3), box (4 * 15, 15, 1, 3)
-};
-
-template <typename T>
-__device__ __forceinline__ void xy_modes(const T (&v)[4], T (&a)[4]) {
-  // v: node columns 00, 10, 01, 11 -> modes 1, sx, sy, sxsy
-  T sx0 = v[0] + v[1], dx0 = v[1] - v[0], sx1 = v[2] + v[3], dx1 = v[3] - v[2];
-  a[0] = sx0 + sx1;
-  a[1] = dx0 + dx1;
-  a[2] = sx1 - sx0;
-  a[3] = dx1 - dx0;
+__device__ __forceinline__ void plane_modes(const FineSmem<T>& sm, int s, int i, int j, int zo, Pair<T> (&m)[4][3]) {
+  typedef PairOps<T> O;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Pair<T> v0 = O::lds2(col_at(sm, s, c, i, j) + zo), v1 = O::lds2(col_at(sm, s, c, i + 1, j) + zo);
+    const Pair<T> v2 = O::lds2(col_at(sm, s, c, i, j + 1) + zo), v3 = O::lds2(col_at(sm, s, c, i + 1, j + 1) + zo);
+    const Pair<T> sx0 = O::add(v0, v1), dx0 = O::sub(v1, v0), sx1 = O::add(v2, v3), dx1 = O::sub(v3, v2);
+    m[0][c] = O::add(sx0, sx1);
+    m[1][c] = O::add(dx0, dx1);
+    m[2][c] = O::sub(sx1, sx0);
+    m[3][c] = O::sub(dx1, dx0);
+  }
 }
 
+// One pair of cells: lower-plane modes lo, upper-plane modes hi, moduli E -> the node plane
+// pair's forces in the x-y mode basis, F[q][c] = (carry + lower face of the first cell, upper
+// face of the first + lower face of the second); carry becomes the second cell's upper face.
 template <typename T>
-__global__ void __launch_bounds__(TXC * TYC, (sizeof(T) == 4 ? 2 : 1))
-k_apply_fine(const __grid_constant__ TileMaps<T> maps, const uint8_t* __restrict__ mask, const KModal<T> km,
-             LpGrid g, int zch, int nchunks, int* __restrict__ err, double* __restrict__ dotp) {
-  extern __shared__ unsigned char smem_raw[];
-  // 128-byte alignment in the shared window (what TMA addresses), not in the generic space
-  const uint32_t raw_off = lp_smem_addr(smem_raw);
-  FineSmem<T>& sm = *reinterpret_cast<FineSmem<T>*>(smem_raw + ((128u - (raw_off & 127u)) & 127u));
-  const int tid = threadIdx.x;
-  const int i = tid % TXC, j = tid / TXC;
-  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
-  const int c_begin = blockIdx.z * zch;
-  const int c_end = min(c_begin + zch, nchunks);
-  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-  if (c_begin >= c_end) {
-    if (dotp && tid == 0) dotp[bid] = 0.0;
-    return;
-  }
-  const int cstart = c_begin > 0 ? c_begin - 1 : 0;     // one halo chunk below the segment
-  const int nload = min(c_end + 1, nchunks) - cstart;   // + the plane above the last chunk
-  const int nproc = c_end - cstart;
-  const bool own = i >= 1 && j >= 1;
-  constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(T);
-  constexpr uint32_t EBYTES = BOX * BOX * 4 * sizeof(T);
-
-  // alignment contract of every TMA operand and vector access, checked once per block: a
-  // violation is recorded in *err (codes 10..16) and the block returns without touching memory
-  __shared__ int bad;
-  if (tid == 0) {
-    int code = 0;
-    uint32_t so = 0;
-    for (int s = 0; s < NSTAGE; ++s) so |= lp_smem_addr(sm.u[s].v) | lp_smem_addr(sm.e[s].v);
-    so |= lp_smem_addr(sm.o[0].v) | lp_smem_addr(sm.o[1].v);
-    if (so & 127) code = 10;
-    else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 11;
-    else if (reinterpret_cast<uintptr_t>(&maps.e) & 63) code = 12;
-    else if (reinterpret_cast<uintptr_t>(&maps.out) & 63) code = 13;
-    else if (lp_smem_addr(&sm.full[0]) & 7) code = 15;
-    else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 16;
-    bad = code;
-    if (code) atomicExch(err, code);
-  }
-  __syncthreads();
-  if (bad) {
-    if (dotp && tid == 0) dotp[bid] = 0.0;
-    return;
-  }
-  if (tid == 0) {
-    for (int s = 0; s < NSTAGE; ++s) lp_mbar_init(&sm.full[s], 1);
-    lp_fence_barrier_init();
-  }
-  __syncthreads();
-  auto issue = [&](int k) {
-    const int s = k % NSTAGE;
-    lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
-    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
-    lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, cstart + k, &sm.full[s]);
-  };
-  if (tid == 0) {
-    issue(0);
-    if (nload > 1) issue(1);
-  }
-
-  T up_carry[4][3];
+__device__ __forceinline__ void cell_pair_sym(const KSym<T>& ks, const Pair<T> (&lo)[4][3], const Pair<T> (&hi)[4][3],
+                                              Pair<T> E, T (&carry)[4][3], Pair<T> (&F)[4][3]) {
+  typedef PairOps<T> O;
+  typedef Pair<T> P;
+  // z step: S[q][c] = lo + hi (q = 1..3; the constant mode carries no force), D[q][c] = hi - lo
+  P S[4][3], D[4][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) up_carry[q][c] = T(0);
-  double pacc = 0.0;   // u . (K u) over this thread's own nodes (when dotp is given)
-
-  for (int k = 0; k < nproc; ++k) {
-    const int c = cstart + k;
-    const bool halo = c < c_begin;
-    const int s = k % NSTAGE;
-    if (tid == 0) {
-      if (k + 2 < nload) issue(k + 2);
-      lp_bulk_wait_read<1>();   // the store from two chunks ago has read its staging buffer
+    for (int c = 0; c < 3; ++c) {
+      if (q > 0) S[q][c] = O::add(lo[q][c], hi[q][c]);
+      D[q][c] = O::sub(hi[q][c], lo[q][c]);
     }
-    bool ok = lp_mbar_wait(&sm.full[s], (k / NSTAGE) & 1);
-    const bool has_next = k + 1 < nload;
-    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NSTAGE], ((k + 1) / NSTAGE) & 1);
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicExch(err, 1);
-        // let the loads already issued land before the block exits (bounded as well)
-        for (int kk = k; kk < min(k + 3, nload); ++kk) lp_mbar_wait(&sm.full[kk % NSTAGE], (kk / NSTAGE) & 1);
-      }
-      break;
-    }
-    // ---- this thread's four node columns: planes z..z+3 and plane z+4
-    T un[4][3][5];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const T* col = u_at(sm, s, cc, i + (q & 1), j + (q >> 1));
-        T v4[4];
-        Vec4<T>::lds(col, v4);
-        un[q][cc][0] = v4[0]; un[q][cc][1] = v4[1]; un[q][cc][2] = v4[2]; un[q][cc][3] = v4[3];
-        un[q][cc][4] = has_next ? *u_at(sm, (k + 1) % NSTAGE, cc, i + (q & 1), j + (q >> 1)) : T(0);
-      }
-    T ev[4];
-    Vec4<T>::lds(&sm.e[s].v[(j * BOX + i) * 4], ev);
-
-    T a_lo[4][3];
-    {
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        T v[4], a[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) v[q] = halo ? un[q][cc][3] : un[q][cc][0];
-        xy_modes(v, a);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a_lo[q][cc] = a[q];
-      }
-    }
-    T s0v[4][3];   // this node column's force from its own and its -x neighbour's cells
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      if (halo && t < 3) continue;
-      T a_hi[4][3];
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        T v[4] = {un[0][cc][t + 1], un[1][cc][t + 1], un[2][cc][t + 1], un[3][cc][t + 1]}, a[4];
-        xy_modes(v, a);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a_hi[q][cc] = a[q];
-      }
-      const T ec = ev[t];
-      T v[24], f[24];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          T lo = a_lo[q][cc], hi = a_hi[q][cc];
-          v[3 * q + cc] = (lo + hi) * ec;
-          v[3 * (q + 4) + cc] = (hi - lo) * ec;
-        }
-      modal_product<T>(km, v, f);
-      T fp[4][3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          T f0 = f[3 * q + cc], f1 = f[3 * (q + 4) + cc];
-          fp[q][cc] = up_carry[q][cc] + (f0 - f1);
-          up_carry[q][cc] = f0 + f1;
-          a_lo[q][cc] = a_hi[q][cc];
-        }
-      if (!halo) {
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          T t0 = fp[0][cc] - fp[2][cc], t1 = fp[1][cc] - fp[3][cc];
-          T t2 = fp[0][cc] + fp[2][cc], t3 = fp[1][cc] + fp[3][cc];
-          // corners 00, 10 (-> x+1), 01 (-> y+1), 11 (-> x+1, y+1); x through shuffles
-          T c10 = __shfl_up_sync(0xffffffffu, t0 + t1, 1, TXC);
-          T c11 = __shfl_up_sync(0xffffffffu, t2 + t3, 1, TXC);
-          s0v[t][cc] = (t0 - t1) + c10;
-          sm.red[cc][t][tid] = (t2 - t3) + c11;
-        }
-      }
-    }
-    if (halo) {           // uniform across the block: the halo chunk only sets up_carry
-      __syncthreads();    // its stage is refilled next iteration: every thread is done reading
-      continue;
-    }
-    __syncthreads();
-    if (own) {
-      const bool inside = x0 - 1 + i < g.NX() && y0 - 1 + j < g.NY();
-      uint8_t mbs[4] = {0, 0, 0, 0};
-      if (inside) {
-        const uchar4 mb = *reinterpret_cast<const uchar4*>(mask + g.node(x0 - 1 + i, y0 - 1 + j, 4 * c));
-        mbs[0] = mb.x; mbs[1] = mb.y; mbs[2] = mb.z; mbs[3] = mb.w;
-      }
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        T o[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          T v = s0v[t][cc] + sm.red[cc][t][tid - TXC];
-          o[t] = ((mbs[t] >> cc) & 1) ? v : T(0);
-          pacc += (double)o[t] * (double)un[0][cc][t];   // this node's u: column q = 0
-        }
-        Vec4<T>::sts(&sm.o[k & 1].v[((cc * (TYC - 1) + (j - 1)) * (TXC - 1) + (i - 1)) * 4], o);
-      }
-    }
-    lp_fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      lp_tma_store_4d(&maps.out, 4 * x0, y0, c, 0, sm.o[k & 1].v);
-      lp_bulk_commit();
-    }
+  auto scaled = [&](T c) { return P{E.a * c, E.b * c}; };
+  const P A = scaled(ks.c[0]), B = scaled(ks.c[1]), Dd = scaled(ks.c[2]), B2 = scaled(ks.c[3]);
+  const P D2 = scaled(ks.c[4]), E2 = scaled(ks.c[5]), Tt = scaled(ks.c[6]);
+  // fc[q][c]: force on mode (q, z-const) (q = 1..3); fo[q][c]: on mode (q, sz)
+  P fc[4][3], fo[4][3];
+  {  // linear normal: (sx,x) = S[1][0], (sy,y) = S[2][1], (sz,z) = D[0][2]
+    const P bs = O::mul(B, O::add(O::add(S[1][0], S[2][1]), D[0][2]));
+    fc[1][0] = O::fma(A, S[1][0], bs);
+    fc[2][1] = O::fma(A, S[2][1], bs);
+    fo[0][2] = O::fma(A, D[0][2], bs);
   }
-  if (tid == 0) lp_bulk_wait_all();
-  if (dotp) {
-    __shared__ double sh[32];
-    pacc = lp_block_sum(pacc, sh);
-    if (tid == 0) dotp[bid] = pacc;
+  // linear shear: {(sx,y), (sy,x)}, {(sx,z), (sz,x)}, {(sy,z), (sz,y)}
+  fc[1][1] = fc[2][0] = O::mul(Dd, O::add(S[1][1], S[2][0]));
+  fc[1][2] = fo[0][0] = O::mul(Dd, O::add(S[1][2], D[0][0]));
+  fc[2][2] = fo[0][1] = O::mul(Dd, O::add(S[2][2], D[0][1]));
+  {  // bilinear normal: (sxsy,z) = S[3][2], (sxsz,y) = D[1][1], (sysz,x) = D[2][0]
+    const P bs = O::mul(B2, O::add(O::add(S[3][2], D[1][1]), D[2][0]));
+    fc[3][2] = O::fma(B2, S[3][2], bs);
+    fo[1][1] = O::fma(B2, D[1][1], bs);
+    fo[2][0] = O::fma(B2, D[2][0], bs);
+  }
+  // bilinear shear: {(sxsy,x), (sysz,z)}, {(sxsy,y), (sxsz,z)}, {(sxsz,x), (sysz,y)}
+  fc[3][0] = O::fma(D2, S[3][0], O::mul(E2, D[2][2]));
+  fo[2][2] = O::fma(D2, D[2][2], O::mul(E2, S[3][0]));
+  fc[3][1] = O::fma(D2, S[3][1], O::mul(E2, D[1][2]));
+  fo[1][2] = O::fma(D2, D[1][2], O::mul(E2, S[3][1]));
+  fo[1][0] = O::fma(D2, D[1][0], O::mul(E2, D[2][1]));
+  fo[2][1] = O::fma(D2, D[2][1], O::mul(E2, D[1][0]));
+  // trilinear
+#pragma unroll
+  for (int c = 0; c < 3; ++c) fo[3][c] = O::mul(Tt, D[3][c]);
+  // back along z: a cell's lower face is fc - fo, its upper face fc + fo (fc = 0 for q = 0)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    F[0][c] = O::sub(O::mk(carry[0][c], fo[0][c].a), fo[0][c]);
+    carry[0][c] = fo[0][c].b;
+#pragma unroll
+    for (int q = 1; q < 4; ++q) {
+      const P lw = O::sub(fc[q][c], fo[q][c]), up = O::add(fc[q][c], fo[q][c]);
+      F[q][c] = O::add(O::mk(carry[q][c], up.a), lw);
+      carry[q][c] = up.b;
+    }
   }
 }
 
-// ordered sum of the per-block partials (the same bits every run)
-__global__ void k_fine_dot_final(const double* __restrict__ part, long long n, double* __restrict__ out) {
-  __shared__ double sh[32];
-  double s = 0.0;
-  for (long long i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
-  s = lp_block_sum(s, sh);
-  if (threadIdx.x == 0) *out = s;
-}
-
-// ---- float32: pairs of cells in packed float32x2 arithmetic ------------------------------------
-// The float32 kernel forms cells (z, z+1) and (z+2, z+3) of a chunk as pairs: a 128-bit load of
-// a node column's four planes is two register pairs, the x-y modes and the modal product run on
-// pairs (add / sub / mul / fma .f32x2), and the two steps that shift by one plane (lower plane +
-// upper plane of a cell, face forces into node planes) are scalar operations writing pair
-// halves. Same arithmetic as the scalar kernel, half the floating-point instructions.
-typedef unsigned long long f2_t;
-
-__device__ __forceinline__ f2_t pk2(float lo, float hi) {
-  f2_t r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ float lo2(f2_t v) {
-  float a, b;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-  return a;
-}
-__device__ __forceinline__ float hi2(f2_t v) {
-  float a, b;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-  return b;
-}
-__device__ __forceinline__ f2_t add2(f2_t a, f2_t b) {
-  f2_t r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2_t sub2(f2_t a, f2_t b) {
-  f2_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) {
-  f2_t r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
-__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) {
-  f2_t r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-  return r;
-}
-
-struct KModal2 {
-  f2_t c[45];   // each coefficient in both lanes
-};
-
-// the modal product of lpb_modal_ke's pattern on a pair of cells (rows 0..2 are zero)
-__device__ __forceinline__ void modal_product2(const KModal2& km, const f2_t (&v)[24], f2_t (&f)[24]) {
-  f[3] = fma2(km.c[2], v[14], fma2(km.c[1], v[7], mul2(km.c[0], v[3])));
-  f[4] = fma2(km.c[4], v[6], mul2(km.c[3], v[4]));
-  f[5] = fma2(km.c[6], v[12], mul2(km.c[5], v[5]));
-  f[6] = fma2(km.c[8], v[6], mul2(km.c[7], v[4]));
-  f[7] = fma2(km.c[11], v[14], fma2(km.c[10], v[7], mul2(km.c[9], v[3])));
-  f[8] = fma2(km.c[13], v[13], mul2(km.c[12], v[8]));
-  f[9] = fma2(km.c[15], v[20], mul2(km.c[14], v[9]));
-  f[10] = fma2(km.c[17], v[17], mul2(km.c[16], v[10]));
-  f[11] = fma2(km.c[20], v[18], fma2(km.c[19], v[16], mul2(km.c[18], v[11])));
-  f[12] = fma2(km.c[22], v[12], mul2(km.c[21], v[5]));
-  f[13] = fma2(km.c[24], v[13], mul2(km.c[23], v[8]));
-  f[14] = fma2(km.c[27], v[14], fma2(km.c[26], v[7], mul2(km.c[25], v[3])));
-  f[15] = fma2(km.c[29], v[19], mul2(km.c[28], v[15]));
-  f[16] = fma2(km.c[32], v[18], fma2(km.c[31], v[16], mul2(km.c[30], v[11])));
-  f[17] = fma2(km.c[34], v[17], mul2(km.c[33], v[10]));
-  f[18] = fma2(km.c[37], v[18], fma2(km.c[36], v[16], mul2(km.c[35], v[11])));
-  f[19] = fma2(km.c[39], v[19], mul2(km.c[38], v[15]));
-  f[20] = fma2(km.c[41], v[20], mul2(km.c[40], v[9]));
-  f[21] = mul2(km.c[42], v[21]);
-  f[22] = mul2(km.c[43], v[22]);
-  f[23] = mul2(km.c[44], v[23]);
-}
-
-__device__ __forceinline__ void xy_modes2(const f2_t (&v)[4], f2_t (&a)[4]) {
-  const f2_t sx0 = add2(v[0], v[1]), dx0 = sub2(v[1], v[0]), sx1 = add2(v[2], v[3]), dx1 = sub2(v[3], v[2]);
-  a[0] = add2(sx0, sx1);
-  a[1] = add2(dx0, dx1);
-  a[2] = sub2(sx1, sx0);
-  a[3] = sub2(dx1, dx0);
-}
-
-// One pair of cells (lower cell planes lo.., upper ..): forms the pair's modal vectors from the
-// x-y modes of three consecutive planes (m0, m1 as a pair and m2), applies E and K^, and returns
-// the two node-plane forces as a pair (carry + lower face of the first cell, upper face of the
-// first + lower face of the second) and the second cell's upper face as the next carry.
-__device__ __forceinline__ void cell_pair(const KModal2& km, const f2_t (&m01)[4][3], const float (&m2)[4][3], f2_t e,
-                                          float (&carry)[4][3], f2_t (&fp)[4][3]) {
-  f2_t v[24], f[24];
+// a node plane pair's x-y mode forces -> this thread's node column's share (own) and the share
+// of the node column at y + 1 (published for that thread in red); x through shuffles
+template <typename T>
+__device__ __forceinline__ void plane_pair_back(const Pair<T> (&F)[4][3], Pair<T> (&own)[3], Pair<T>* red, int tid) {
+  typedef PairOps<T> O;
+  typedef Pair<T> P;
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int cc = 0; cc < 3; ++cc) {
-      const float a0 = lo2(m01[q][cc]), a1 = hi2(m01[q][cc]), a2 = m2[q][cc];
-      v[3 * q + cc] = mul2(pk2(a0 + a1, a1 + a2), e);
-      v[3 * (q + 4) + cc] = mul2(pk2(a1 - a0, a2 - a1), e);
-    }
-  modal_product2(km, v, f);
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int cc = 0; cc < 3; ++cc) {
-      const f2_t f1 = f[3 * (q + 4) + cc];
-      f2_t lw, up;
-      if (q == 0) {
-        lw = sub2(0ull, f1);   // rows 0..2 (the constant mode) are zero
-        up = f1;
-      } else {
-        const f2_t f0 = f[3 * q + cc];
-        lw = sub2(f0, f1);
-        up = add2(f0, f1);
-      }
-      fp[q][cc] = pk2(carry[q][cc] + lo2(lw), lo2(up) + hi2(lw));
-      carry[q][cc] = hi2(up);
-    }
-}
-
-// corner forces of one pair of node planes: own corner pair (00 + the -x neighbour's 10) kept,
-// the y + 1 corners (01 + 11 of the -x neighbour) to shared memory
-__device__ __forceinline__ void plane_corners2(const f2_t (&fp)[4][3], f2_t (&s0v)[3], float2* red, int tid) {
-#pragma unroll
-  for (int cc = 0; cc < 3; ++cc) {
-    const f2_t t0 = sub2(fp[0][cc], fp[2][cc]), t1 = sub2(fp[1][cc], fp[3][cc]);
-    const f2_t t2 = add2(fp[0][cc], fp[2][cc]), t3 = add2(fp[1][cc], fp[3][cc]);
-    const f2_t a = add2(t0, t1), b = add2(t2, t3);
-    const f2_t ca = pk2(__shfl_up_sync(0xffffffffu, lo2(a), 1, TXC), __shfl_up_sync(0xffffffffu, hi2(a), 1, TXC));
-    const f2_t cb = pk2(__shfl_up_sync(0xffffffffu, lo2(b), 1, TXC), __shfl_up_sync(0xffffffffu, hi2(b), 1, TXC));
-    s0v[cc] = add2(sub2(t0, t1), ca);
-    const f2_t r = add2(sub2(t2, t3), cb);
-    red[cc * TXC * TYC + tid] = make_float2(lo2(r), hi2(r));
+  for (int c = 0; c < 3; ++c) {
+    // corner (dx, dy) = P(dx) + sy(dy) Q(dx): P(0) = F0 - F1, P(1) = F0 + F1, Q likewise from F2, F3
+    const P p0 = O::sub(F[0][c], F[1][c]), p1 = O::add(F[0][c], F[1][c]);
+    const P q0 = O::sub(F[2][c], F[3][c]), q1 = O::add(F[2][c], F[3][c]);
+    const P pn = O::add(p0, O::shfl_up1(p1)), qn = O::add(q0, O::shfl_up1(q1));
+    own[c] = O::sub(pn, qn);
+    O::sts(&red[c * TXC * TYC + tid], O::add(pn, qn));
   }
-}
-
-constexpr int NST2 = 3;   // TMA ring depth of the float32 kernel (loads run NST2 - 1 chunks ahead)
-
-struct FineSmem2 {
-  Slot<float, 3 * BOX * BOX * 4> u[NST2];
-  Slot<float, BOX * BOX * 4> e[NST2];
-  float2 red[2][2][3][TXC * TYC];                 // [chunk parity][plane pair][component][thread]
-  alignas(8) uint64_t full[NST2];
-};
-
-__device__ __forceinline__ const float* u_at2(const FineSmem2& sm, int s, int c, int x, int y) {
-  return &sm.u[s].v[((c * BOX + y) * BOX + x) * 4];
 }
 
 // The degree-2 Chebyshev update formed where A u is stored (the vector kernels' expressions, so
@@ -556,42 +270,58 @@ __device__ __forceinline__ void cheb_store(const FineCheb& ch, long long i, cons
   }
 }
 
-// One barrier per chunk: each thread waits for its stage, computes, publishes its y-corner
-// forces into the exchange buffer of the chunk's parity, and the block meets once (which also
-// settles a wait that gave up); the owners then add their -y neighbour's corners and store
-// their four node planes with 16-byte stores. The exchange is double-buffered, so the next
-// chunk's writes never meet this chunk's reads. A chunk runs in two phases that keep the
-// register footprint to one pair of cells: (A) planes 0..2 -> cells 0, 1; (B) planes 2..4 ->
-// cells 2, 3 (plane 2's modes formed in both). MODE 0 stores A u in out; modes 1..3 store a
-// Chebyshev update instead (cheb_store; out unused).
-template <int MODE>
-__global__ void __launch_bounds__(TXC * TYC, 2)
-k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict__ out,
-                const uint8_t* __restrict__ mask, const KModal2 km2, const KModal<float> km, LpGrid g, int zch,
-                int nchunks, int* __restrict__ err, const FineCheb ch) {
-  extern __shared__ unsigned char smem_raw2[];
-  const uint32_t raw_off = lp_smem_addr(smem_raw2);
-  FineSmem2& sm = *reinterpret_cast<FineSmem2*>(smem_raw2 + ((128u - (raw_off & 127u)) & 127u));
+__device__ __forceinline__ void store4(float* p, const float (&o)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double (&o)[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(o[2], o[3]);
+}
+
+// One barrier per chunk: each thread waits for its stages, forms its two pairs of cells, publishes
+// its y shares into the exchange buffer of the chunk's parity, and the block meets once (which
+// also settles a wait that gave up); the owners then add their -y neighbour's shares and store
+// their four node planes. The exchange is double-buffered, so the next chunk's writes never meet
+// this chunk's reads. MODE 0 stores A u in out (float64: and, with dotp, the block's share of
+// u . A u); modes 1..3 (float32) store a Chebyshev update instead (cheb_store; out unused).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(TXC * TYC, (sizeof(T) == 4 ? 2 : 1))
+k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const uint8_t* __restrict__ mask,
+             const KSym<T> ks, LpGrid g, int zch, int nchunks, int* __restrict__ err, const FineCheb ch,
+             double* __restrict__ dotp) {
+  typedef PairOps<T> O;
+  typedef Pair<T> P;
+  extern __shared__ unsigned char smem_raw[];
+  // 128-byte alignment in the shared window (what TMA addresses), not in the generic space
+  const uint32_t raw_off = lp_smem_addr(smem_raw);
+  FineSmem<T>& sm = *reinterpret_cast<FineSmem<T>*>(smem_raw + ((128u - (raw_off & 127u)) & 127u));
   const int tid = threadIdx.x;
   const int i = tid % TXC, j = tid / TXC;
   const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
   const int c_begin = blockIdx.z * zch;
   const int c_end = min(c_begin + zch, nchunks);
-  if (c_begin >= c_end) return;
-  const int cstart = c_begin > 0 ? c_begin - 1 : 0;
-  const int nload = min(c_end + 1, nchunks) - cstart;
+  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  if (c_begin >= c_end) {
+    if (dotp && tid == 0) dotp[bid] = 0.0;
+    return;
+  }
+  const int cstart = c_begin > 0 ? c_begin - 1 : 0;     // one halo chunk below the segment
+  const int nload = min(c_end + 1, nchunks) - cstart;   // + the chunk above the last one
   const int nproc = c_end - cstart;
   const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
   const bool writer = i >= 1 && j >= 1 && nx_ < g.NX() && ny_ < g.NY();
   const long long obase = writer ? g.node(nx_, ny_, 0) : 0;   // chunk c at obase + c * zcs
   const long long cs = g.comp_stride(), zcs = g.node_zc_stride();
-  constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(float);
-  constexpr uint32_t EBYTES = BOX * BOX * 4 * sizeof(float);
+  constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(T);
+  constexpr uint32_t EBYTES = TXC * TYC * 4 * sizeof(T);
+
+  // alignment contract of every TMA operand and vector access, checked once per block: a
+  // violation is recorded in *err (codes 10..17) and the block returns without touching memory
   __shared__ int bad;
   if (tid == 0) {
     int code = 0;
     uint32_t so = 0;
-    for (int s = 0; s < NST2; ++s) so |= lp_smem_addr(sm.u[s].v) | lp_smem_addr(sm.e[s].v);
+    for (int s = 0; s < NST; ++s) so |= lp_smem_addr(sm.u[s].v) | lp_smem_addr(sm.e[s].v);
     if (so & 127) code = 10;
     else if (reinterpret_cast<uintptr_t>(&maps.u) & 63) code = 11;
     else if (reinterpret_cast<uintptr_t>(&maps.e) & 63) code = 12;
@@ -601,11 +331,15 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
                             reinterpret_cast<uintptr_t>(ch.dinv)) & 15)) code = 14;
     else if (lp_smem_addr(&sm.full[0]) & 7) code = 15;
     else if (reinterpret_cast<uintptr_t>(mask) & 3) code = 16;
+    else if (lp_smem_addr(&sm.red[0][0][0][0]) & 15) code = 17;
     bad = code;
     if (code) atomicExch(err, code);
   }
   __syncthreads();
-  if (bad) return;
+  if (bad) {
+    if (dotp && tid == 0) dotp[bid] = 0.0;
+    return;
+  }
   float cs_s = 0.0f, cs_c1 = 0.0f, cs_c2 = 0.0f;
   if constexpr (MODE != 0) {
     cs_s = (float)ch.coef[1];
@@ -613,152 +347,137 @@ k_apply_fine_x2(const __grid_constant__ TileMaps<float> maps, float* __restrict_
     cs_c2 = (float)ch.coef[3];
   }
   if (tid == 0) {
-    for (int s = 0; s < NST2; ++s) lp_mbar_init(&sm.full[s], 1);
+    for (int s = 0; s < NST; ++s) lp_mbar_init(&sm.full[s], 1);
     lp_fence_barrier_init();
   }
   __syncthreads();
   auto issue = [&](int k) {
-    const int s = k % NST2;
+    const int s = k % NST;
     lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
     lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
     lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, cstart + k, &sm.full[s]);
   };
   if (tid == 0)
-    for (int kk = 0; kk < NST2 - 1 && kk < nload; ++kk) issue(kk);
-  float carry[4][3];
+    for (int kk = 0; kk < NST - 1 && kk < nload; ++kk) issue(kk);
+  T carry[4][3];
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) carry[q][c] = 0.0f;
+    for (int c = 0; c < 3; ++c) carry[q][c] = T(0);
+  double pacc = 0.0;
+  // modes of planes (0, 1) of the chunk in hand, formed by the iteration before
+  P m01[4][3];
+  bool ok = lp_mbar_wait(&sm.full[0], 0);
+  plane_modes<T>(sm, 0, i, j, 0, m01);
 
   for (int k = 0; k < nproc; ++k) {
     const int c = cstart + k;
     const bool halo = c < c_begin;
-    const int s = k % NST2;
+    const int s = k % NST;
     // the stage refilled here was last read in the previous chunk, before its barrier
-    if (tid == 0 && k + NST2 - 1 < nload) issue(k + NST2 - 1);
+    if (tid == 0 && k + NST - 1 < nload) issue(k + NST - 1);
     const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + c * zcs)) : 0u;
-    bool ok = lp_mbar_wait(&sm.full[s], (k / NST2) & 1);
+    ok = ok && lp_mbar_wait(&sm.full[s], (k / NST) & 1);
     const bool has_next = k + 1 < nload;
-    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NST2], ((k + 1) / NST2) & 1);
+    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NST], ((k + 1) / NST) & 1);
     // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
-    const float* ecol = &sm.e[s].v[(j * BOX + i) * 4];
-    f2_t m23[4][3];
-    float m4[4][3];
-    auto load_b = [&]() {
-      f2_t p23[4][3];
-      float p4[4][3];
+    const T* ecol = &sm.e[s].v[(j * TXC + i) * 4];
+    P m23[4][3];
+    plane_modes<T>(sm, s, i, j, 2, m23);
+    P(*red)[3][TXC * TYC] = sm.red[k & 1];
+    P own[2][3];
+    T ucol[3][4];   // this node column's u (float64 dot), read before the barrier frees the stage
+    if constexpr (MODE == 0 && sizeof(T) == 8) {
+      if (dotp != nullptr && writer && !halo) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+        for (int cc = 0; cc < 3; ++cc)
 #pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const float2 v = *reinterpret_cast<const float2*>(u_at2(sm, s, cc, i + (q & 1), j + (q >> 1)) + 2);
-          p23[q][cc] = pk2(v.x, v.y);
-          p4[q][cc] = has_next ? *u_at2(sm, (k + 1) % NST2, cc, i + (q & 1), j + (q >> 1)) : 0.0f;
-        }
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        f2_t v23[4] = {p23[0][cc], p23[1][cc], p23[2][cc], p23[3][cc]}, a23[4];
-        float v4[4] = {p4[0][cc], p4[1][cc], p4[2][cc], p4[3][cc]}, a4[4];
-        xy_modes2(v23, a23);
-        xy_modes(v4, a4);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          m23[q][cc] = a23[q];
-          m4[q][cc] = a4[q];
-        }
+          for (int t = 0; t < 4; ++t) ucol[cc][t] = col_at(sm, s, cc, i, j)[t];
       }
-    };
-    if (halo) {
-      // only the chunk's last cell: its upper face starts the carry of the segment
-      load_b();
-      const float ew = ecol[3];
-      float v[24], f[24];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          const float lo = hi2(m23[q][cc]), hi = m4[q][cc];
-          v[3 * q + cc] = (lo + hi) * ew;
-          v[3 * (q + 4) + cc] = (hi - lo) * ew;
-        }
-      modal_product<float>(km, v, f);
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) carry[q][cc] = f[3 * q + cc] + f[3 * (q + 4) + cc];
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicExch(err, 1);
-          for (int kk = k; kk < min(k + NST2, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST2], (kk / NST2) & 1);
-        }
-        break;
-      }
-      continue;
     }
-    f2_t s0v[2][3];
-    float2(*red)[3][TXC * TYC] = sm.red[k & 1];
+    // cells (0, 1): planes (0, 1) and (1, 2). In a halo chunk only cell 3 matters (its upper face
+    // starts the segment's carry), so the first pair is skipped there.
+    if (!halo) {
+      P hi[4][3], F[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m01[q][cc].b, m23[q][cc].a);
+      cell_pair_sym<T>(ks, m01, hi, O::lds2(ecol), carry, F);
+      plane_pair_back<T>(F, own[0], &red[0][0][0], tid);
+    }
+    // the next chunk's planes (0, 1), kept for the next iteration
+    if (has_next) {
+      plane_modes<T>(sm, (k + 1) % NST, i, j, 0, m01);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) m01[q][cc] = O::zero();
+    }
     {
-      f2_t m01[4][3];
-      float m2[4][3];
-      {
-        f2_t p01[4][3];
-        float p2[4][3];
+      // cells (2, 3): planes (2, 3) and (3, 4)
+      P hi[4][3], F[4][3];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m23[q][cc].b, m01[q][cc].a);
+      if (halo) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int cc = 0; cc < 3; ++cc) {
-            const float4 v = *reinterpret_cast<const float4*>(u_at2(sm, s, cc, i + (q & 1), j + (q >> 1)));
-            p01[q][cc] = pk2(v.x, v.y);
-            p2[q][cc] = v.z;
-          }
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          f2_t v01[4] = {p01[0][cc], p01[1][cc], p01[2][cc], p01[3][cc]}, a01[4];
-          float v2[4] = {p2[0][cc], p2[1][cc], p2[2][cc], p2[3][cc]}, a2[4];
-          xy_modes2(v01, a01);
-          xy_modes(v2, a2);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            m01[q][cc] = a01[q];
-            m2[q][cc] = a2[q];
-          }
-        }
+          for (int cc = 0; cc < 3; ++cc) carry[q][cc] = T(0);
       }
-      const float2 e01 = *reinterpret_cast<const float2*>(ecol);
-      f2_t fp[4][3];
-      cell_pair(km2, m01, m2, pk2(e01.x, e01.y), carry, fp);
-      plane_corners2(fp, s0v[0], red[0][0], tid);
-    }
-    {
-      load_b();
-      const float2 e23 = *reinterpret_cast<const float2*>(ecol + 2);
-      f2_t fp[4][3];
-      cell_pair(km2, m23, m4, pk2(e23.x, e23.y), carry, fp);
-      plane_corners2(fp, s0v[1], red[1][0], tid);
+      cell_pair_sym<T>(ks, m23, hi, O::lds2(ecol + 2), carry, F);
+      if (!halo) plane_pair_back<T>(F, own[1], &red[1][0][0], tid);
     }
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(err, 1);
-        for (int kk = k; kk < min(k + NST2, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST2], (kk / NST2) & 1);
+        // let the loads already issued land before the block exits (bounded as well)
+        for (int kk = k; kk < min(k + NST, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST], (kk / NST) & 1);
       }
       break;
     }
+    if (halo) continue;   // uniform across the block
     if (writer) {
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
-        const float2 r01 = red[0][cc][tid - TXC], r23 = red[1][cc][tid - TXC];
-        const f2_t o01 = add2(s0v[0][cc], pk2(r01.x, r01.y)), o23 = add2(s0v[1][cc], pk2(r23.x, r23.y));
-        float4 o = make_float4(lo2(o01), hi2(o01), lo2(o23), hi2(o23));
-        if (!((mb4 >> cc) & 1u)) o.x = 0.0f;
-        if (!((mb4 >> (8 + cc)) & 1u)) o.y = 0.0f;
-        if (!((mb4 >> (16 + cc)) & 1u)) o.z = 0.0f;
-        if (!((mb4 >> (24 + cc)) & 1u)) o.w = 0.0f;
-        if constexpr (MODE == 0) *reinterpret_cast<float4*>(out + cc * cs + obase + c * zcs) = o;
-        else cheb_store<MODE>(ch, cc * cs + obase + c * zcs, o, cs_s, cs_c1, cs_c2);
+        const P a = O::add(own[0][cc], red[0][cc][tid - TXC]);
+        const P b = O::add(own[1][cc], red[1][cc][tid - TXC]);
+        T o[4] = {a.a, a.b, b.a, b.b};
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if (!((mb4 >> (8 * t + cc)) & 1u)) o[t] = T(0);
+        const long long idx = cc * cs + obase + c * zcs;
+        if constexpr (MODE == 0) {
+          store4(out + idx, o);
+          if constexpr (sizeof(T) == 8) {
+            if (dotp) {
+#pragma unroll
+              for (int t = 0; t < 4; ++t) pacc += o[t] * ucol[cc][t];
+            }
+          }
+        } else if constexpr (sizeof(T) == 4) {
+          cheb_store<MODE>(ch, idx, make_float4(o[0], o[1], o[2], o[3]), cs_s, cs_c1, cs_c2);
+        }
       }
     }
   }
+  if (dotp) {
+    __shared__ double sh[32];
+    pacc = lp_block_sum(pacc, sh);
+    if (tid == 0) dotp[bid] = pacc;
+  }
+}
+
+// ordered sum of the per-block partials (the same bits every run)
+__global__ void k_fine_dot_final(const double* __restrict__ part, long long n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = lp_block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace
@@ -789,37 +508,97 @@ static long long resident_blocks(const void* kfn, int smem) {
   return v;
 }
 
+// The seven coefficient classes of the cubic-symmetric modal matrix from lpb_modal_ke's 45
+// values: {a - b, b, d, b2, d2, e2, t}. False when an entry strays from its class by more than
+// 1e-9 of the largest, or the exact identities of the isotropic unit brick (the linear shear block
+// has rank one, e = d; the bilinear normal block is b2 (I + 1 1^T), a2 = 2 b2) do not hold.
+static bool modal_sym_classes(const double* km, double out[7]) {
+  static const int rows[LP_MODAL_NNZ] = LP_MODAL_ROWS;
+  static const int cols[LP_MODAL_NNZ] = LP_MODAL_COLS;
+  auto in = [](int v, std::initializer_list<int> s) {
+    for (int w : s)
+      if (w == v) return true;
+    return false;
+  };
+  auto pair_of = [](int v) -> int {   // the shear pairs: an id per pair, -1 when v is in none
+    const int pl[3][2] = {{4, 6}, {5, 12}, {8, 13}}, pb[3][2] = {{9, 20}, {10, 17}, {15, 19}};
+    for (int p = 0; p < 3; ++p) {
+      if (v == pl[p][0] || v == pl[p][1]) return p;
+      if (v == pb[p][0] || v == pb[p][1]) return 3 + p;
+    }
+    return -1;
+  };
+  // classes: 0 a, 1 b, 2 d, 3 e, 4 a2, 5 b2, 6 d2, 7 e2, 8 t
+  double sum[9] = {}, lo[9], hi[9];
+  int cnt[9] = {};
+  for (int k = 0; k < 9; ++k) {
+    lo[k] = 1e300;
+    hi[k] = -1e300;
+  }
+  double amax = 0.0;
+  for (int n = 0; n < LP_MODAL_NNZ; ++n) {
+    const int r = rows[n], c = cols[n];
+    int cl = -1;
+    if (in(r, {3, 7, 14}) && in(c, {3, 7, 14})) cl = r == c ? 0 : 1;
+    else if (in(r, {11, 16, 18}) && in(c, {11, 16, 18})) cl = r == c ? 4 : 5;
+    else if (r >= 21 && r == c) cl = 8;
+    else if (pair_of(r) >= 0 && pair_of(r) == pair_of(c)) cl = (pair_of(r) < 3 ? 2 : 6) + (r == c ? 0 : 1);
+    if (cl < 0) return false;
+    sum[cl] += km[n];
+    cnt[cl] += 1;
+    lo[cl] = fmin(lo[cl], km[n]);
+    hi[cl] = fmax(hi[cl], km[n]);
+    amax = fmax(amax, fabs(km[n]));
+  }
+  double m[9];
+  for (int k = 0; k < 9; ++k) {
+    if (!cnt[k] || hi[k] - lo[k] > 1e-9 * amax) return false;
+    m[k] = sum[k] / cnt[k];
+  }
+  if (fabs(m[3] - m[2]) > 1e-9 * amax || fabs(m[4] - 2.0 * m[5]) > 1e-9 * amax) return false;
+  out[0] = m[0] - m[1];
+  out[1] = m[1];
+  out[2] = m[2];
+  out[3] = m[5];
+  out[4] = m[6];
+  out[5] = m[7];
+  out[6] = m[8];
+  return true;
+}
+
 template <typename T>
 static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, const double* kmodal_host, int* err,
                        LpGrid g, cudaStream_t st, double* part = nullptr, long long part_len = 0,
                        double* dot_out = nullptr, int mode = 0, const FineCheb* ch = nullptr) {
   if (!fine_args_ok(g) || !out || !u || !e || !mask || !kmodal_host || !err || out == u) return LP_ERR_ARG;
-  KModal<T> km;
-  for (int i = 0; i < 45; ++i) km.c[i] = (T)kmodal_host[i];
-  // float32: the packed-pair kernel
-  const bool x2 = sizeof(T) == 4;
-  if (mode != 0 && (!x2 || !ch || mode < 0 || mode > 3)) return LP_ERR_ARG;
+  if (mode != 0 && (sizeof(T) != 4 || !ch || mode < 0 || mode > 3)) return LP_ERR_ARG;
+  double cls[7];
+  if (!modal_sym_classes(kmodal_host, cls)) return LP_ERR_ARG;
+  KSym<T> ks;
+  for (int n = 0; n < 7; ++n) ks.c[n] = (T)cls[n];
   const uint32_t zc = 4;
-  TileMaps<T> maps;
+  FineMaps maps;
   const uint64_t nd[4] = {zc * (uint64_t)g.NX(), (uint64_t)g.NY(), (uint64_t)g.pz / zc, 3};
   const uint64_t cd[3] = {zc * (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.cpz / zc};
   const uint32_t bin[4] = {zc * BOX, BOX, 1, 3};
-  const uint32_t be[3] = {zc * BOX, BOX, 1};
-  const uint32_t bout[4] = {zc * (TXC - 1), TYC - 1, 1, 3};
-  if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.e, e, 3, cd, be, sizeof(T)) ||
-      !lp_make_map(&maps.out, out, 4, nd, bout, sizeof(T)))
+  const uint32_t be[3] = {zc * TXC, TYC, 1};
+  if (!lp_make_map(&maps.u, u, 4, nd, bin, sizeof(T)) || !lp_make_map(&maps.e, e, 3, cd, be, sizeof(T)))
     return LP_ERR_ARG;
-  const int smem = x2 ? (int)sizeof(FineSmem2) + 128 : (int)sizeof(FineSmem<T>) + 128;
-  const void* x2fn = mode == 1   ? (const void*)k_apply_fine_x2<1>
-                     : mode == 2 ? (const void*)k_apply_fine_x2<2>
-                     : mode == 3 ? (const void*)k_apply_fine_x2<3>
-                                 : (const void*)k_apply_fine_x2<0>;
-  const void* kfn = x2 ? x2fn : (const void*)k_apply_fine<T>;
+  const int smem = (int)sizeof(FineSmem<T>) + 128;
+  const void* kfn;
+  if constexpr (sizeof(T) == 4) {
+    kfn = mode == 1   ? (const void*)k_apply_fine<float, 1>
+          : mode == 2 ? (const void*)k_apply_fine<float, 2>
+          : mode == 3 ? (const void*)k_apply_fine<float, 3>
+                      : (const void*)k_apply_fine<float, 0>;
+  } else {
+    kfn = (const void*)k_apply_fine<double, 0>;
+  }
   const long long slots = resident_blocks(kfn, smem);
   if (!slots) return LP_ERR_LAUNCH;
   const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
   const int nchunks = g.pz / (int)zc;
-  // z segments: balance the grid over the resident blocks; a segment recomputes one halo cell
+  // z segments: balance the grid over the resident blocks; a segment recomputes one halo chunk
   int best_zch = nchunks;
   double best = 1e30;
   for (int zch = 2; zch <= nchunks; ++zch) {
@@ -827,39 +606,36 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
     const long long units = (long long)gx * gy * nseg;
     const long long waves = (units + slots - 1) / slots;
     const double cost = (double)waves * (zch + (nseg > 1 ? 0.3 : 0.0));
-    if (cost < best - 1e-9) { best = cost; best_zch = zch; }
+    if (cost < best - 1e-9) {
+      best = cost;
+      best_zch = zch;
+    }
   }
   const int tuned = lp_tune_lookup(sizeof(T) == 4 ? LP_KNOB_FINE_F32 : LP_KNOB_FINE_F64, g.nx, g.ny, g.nz);
   if (tuned >= 2 && tuned <= nchunks) best_zch = tuned;
   const int nseg = (nchunks + best_zch - 1) / best_zch;
   dim3 grid(gx, gy, nseg);
-  if constexpr (sizeof(T) == 4) {
-    if (x2) {
-      KModal2 km2;
-      for (int i = 0; i < 45; ++i) {
-        const float c = (float)kmodal_host[i];
-        uint32_t bits;
-        memcpy(&bits, &c, 4);
-        km2.c[i] = ((unsigned long long)bits << 32) | bits;
-      }
-      const FineCheb none{};
-      const FineCheb& c = ch ? *ch : none;
-      if (mode == 1) k_apply_fine_x2<1><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
-      else if (mode == 2) k_apply_fine_x2<2><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
-      else if (mode == 3) k_apply_fine_x2<3><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
-      else k_apply_fine_x2<0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, km2, km, g, best_zch, nchunks, err, c);
-      LP_LAUNCH_CHECK();
-      return LP_OK;
-    }
-  }
+  const FineCheb none{};
+  const FineCheb& c = ch ? *ch : none;
+  double* dp = nullptr;
+  const long long nb = (long long)grid.x * grid.y * grid.z;
   if (part) {
-    const long long nb = (long long)grid.x * grid.y * grid.z;
     if (nb > part_len) return LP_ERR_SIZE;
-    k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err, part);
-    k_fine_dot_final<<<1, 1024, 0, st>>>(part, nb, dot_out);
-  } else {
-    k_apply_fine<T><<<grid, TXC * TYC, smem, st>>>(maps, mask, km, g, best_zch, nchunks, err, nullptr);
+    dp = part;
   }
+  if constexpr (sizeof(T) == 4) {
+    if (mode == 1)
+      k_apply_fine<float, 1><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+    else if (mode == 2)
+      k_apply_fine<float, 2><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+    else if (mode == 3)
+      k_apply_fine<float, 3><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+    else
+      k_apply_fine<float, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+  } else {
+    k_apply_fine<double, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, dp);
+  }
+  if (dp) k_fine_dot_final<<<1, 1024, 0, st>>>(dp, nb, dot_out);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
@@ -888,6 +664,12 @@ int lpb_modal_ke(const double* ke, double* kmodal_out) {
   return 45;
 }
 
+// lpb_modal_ke's 45 coefficients -> the seven classes the fine kernel's product uses
+// {a - b, b, d, b2, d2, e2, t}; 7, or -1 when the coefficients lack the unit brick's symmetry
+int lpb_modal_sym(const double* kmodal, double* classes_out) {
+  if (!kmodal || !classes_out) return LP_ERR_ARG;
+  return modal_sym_classes(kmodal, classes_out) ? 7 : -1;
+}
 
 int lpb_apply_fine_f32(float* out, const float* u, const float* e, const uint8_t* mask, const double* kmodal,
                        int* err, int nx, int ny, int nz, int pz, int cpz, void* stream) {

@@ -111,3 +111,47 @@ def test_tune_candidates():
     c = candidates(65, 2)
     assert c[0] == 0 and c[-1] == 65 and all(2 <= z <= 65 for z in c[1:]) and len(c) < 20
     assert candidates(1, 1) == [0, 1]
+
+
+def test_modal_symmetry_classes_host_only():
+    """lpb_modal_sym (host code): the seven classes the fine kernel's product uses rebuild all 45
+    corner-parity coefficients of the reference's bricks (plain and incompatible-mode, several
+    nu), and the kernel's block formulas give K^ v; coefficients without the symmetry are refused."""
+    from loadpath_b200.fem import hex8_ke
+
+    rows = [3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12, 13, 13, 14, 14, 14, 15, 15,
+            16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21, 22, 23]
+    cols = [3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12, 8, 13, 3, 7, 14, 15, 19,
+            11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22, 23]
+    rng = np.random.default_rng(3)
+    for el in ("im", "plain"):
+        for nu in (0.2, 0.3, 0.45):
+            ke = np.ascontiguousarray(hex8_ke(nu, el))
+            km = np.zeros(45)
+            lib().lpb_modal_ke(ke.ctypes.data, km.ctypes.data)
+            cl = np.zeros(7)
+            assert lib().lpb_modal_sym(km.ctypes.data, cl.ctypes.data) == 7
+            khat = np.zeros((24, 24))
+            khat[rows, cols] = km
+            amb, b, d, b2, d2, e2, t = cl
+            v = rng.standard_normal(24)
+            f = np.zeros(24)
+            s1 = v[3] + v[7] + v[14]
+            for k in (3, 7, 14):
+                f[k] = amb * v[k] + b * s1
+            for p, q in ((4, 6), (5, 12), (8, 13)):
+                f[p] = f[q] = d * (v[p] + v[q])
+            s2 = v[11] + v[16] + v[18]
+            for k in (11, 16, 18):
+                f[k] = b2 * v[k] + b2 * s2
+            for p, q in ((9, 20), (10, 17), (15, 19)):
+                f[p], f[q] = d2 * v[p] + e2 * v[q], e2 * v[p] + d2 * v[q]
+            f[21:] = t * v[21:]
+            np.testing.assert_allclose(f, khat @ v, rtol=1e-13, atol=1e-15 * np.abs(khat).max())
+    bad = km.copy()
+    bad[0] *= 1.01          # one diagonal of the linear normal block off its class
+    try:
+        lib().lpb_modal_sym(bad.ctypes.data, cl.ctypes.data)
+        raise AssertionError("coefficients without the brick's symmetry must be refused")
+    except RuntimeError:
+        pass
