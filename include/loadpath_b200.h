@@ -165,10 +165,11 @@ int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mca
  * row-major at t + (R (D + 1) + d) * 1024, padding dofs past n as identity rows.
  * lpb_band_dims: out = {n, nt, D, bw}, returns the tile count nt (D + 1).
  * lpb_band_factor: in-place tiled signed Cholesky A = L S L^T, S = diag(+-1) (a symmetric LU
- *   without pivoting, as the reference's SuperLU in symmetric mode; one cooperative launch,
- *   bounded grid barrier); linv: nt * 1024 doubles; sgn: 32 nt doubles, the pivot signs; info: 0
- *   or the 1-based band dof of the first exactly zero (or non-finite) pivot; bar: 64 device words
- *   of scratch; err: set when a barrier wait gave up.
+ *   without pivoting, as the reference's SuperLU in symmetric mode; one cooperative launch, tile
+ *   rows owned by blocks that wait on each other's progress counts, bounded waits); linv:
+ *   nt * 1024 doubles; sgn: 32 nt doubles, the pivot signs; info: 0 or the 1-based band dof of the
+ *   first exactly zero (or non-finite) pivot; bar: max(64, nt) device words of scratch; err: set
+ *   when a wait gave up.
  * lpb_band_inverse: ainv (32 nt x 32 nt, row-major, band numbering) = A^-1 from the factor.
  * lpb_band_solve_*: f_out = A^-1 f_in through the band numbering; v: 32 nt doubles scratch. */
 int lpb_coarse_band_f32(double* t, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
@@ -354,6 +355,46 @@ int lpb_mma_newton_b(long long n, int m, const double* low, const double* upp, c
 int lpb_mma_trial(long long n, int m, const double* low, const double* upp, const double* alfa, const double* beta, const double* p0, const double* q0, const double* P, const double* Q, const double* xs0, const double* xsi0, const double* eta0, const double* dx, const double* dxsi, const double* deta, double steg, const double* lam, double epsi, double* xs, double* xsi, double* eta, double* part, double* out, void* stream);
 /* xnew = clip(finite(xs) ? xs : x, alfa, beta)   (loadpath/mma.py:104-108) */
 int lpb_mma_finish(long long n, const double* xs, const double* x, const double* alfa, const double* beta, double* xnew, void* stream);
+
+
+/* ---- the solver behind an opaque handle (loadpath/mg.py:411-988: GridElasticity(...),
+ * .set_moduli, .solve_many), for hosts that are not Python. Fields are float64 device arrays in
+ * the layout below; the handle owns its device memory (freed by lpb_mg_destroy) and must not be
+ * used from two host threads at once. Given the same element matrix, a solve has the bits of
+ * loadpath_b200.mg.GridElasticity.solve_device with convergence tested on the host.
+ * lpb_mg_create: nx, ny, nz even cell counts; fixed: uint8 (NX, NY, NZ) host array in grid order,
+ *   bit c set when component c of the node is held; ke: 24 x 24 element matrix at E = 1 (times the
+ *   pitch), host; single: 1 for the float32 V-cycle (the mixed solve), 0 for float64; rtol,
+ *   maxiter, coarse_cells as GridElasticity; *status 0 or < 0. Returns the handle or NULL.
+ * lpb_mg_set_moduli: e, the fine cells' moduli (layout of lpb_layout_cells_f64): builds the
+ *   hierarchy (the strict one when the coarsest factor is singular, loadpath/mg.py:586-591).
+ * lpb_mg_solve: x = A^-1 b, b and x0 (may be NULL) masked first; the strict hierarchy when the
+ *   plain one stalls (STALL = 100 CG iterations, loadpath/mg.py:951-965); returns 0, 1 when CG did
+ *   not converge (loadpath/mg.py:945-946 raises there), < 0 on an error; *iters the CG count.
+ * lpb_mg_levels / lpb_mg_strict: the depth and strictness of the current hierarchy. */
+void* lpb_mg_create(int nx, int ny, int nz, const uint8_t* fixed, const double* ke, int single, double rtol, int maxiter, long long coarse_cells, int* status);
+int lpb_mg_set_moduli(void* h, const double* e, void* stream);
+int lpb_mg_solve(void* h, const double* b, const double* x0, double* x, int* iters, void* stream);
+int lpb_mg_levels(void* h);
+int lpb_mg_strict(void* h);
+void lpb_mg_destroy(void* h);
+/* host helpers of the handle (and of the Python class, which shares their bits):
+ * lpb_hex8_ke: the hex8 element matrix at E = 1 on the unit cube (loadpath/fem.py:191-224),
+ *   incompatible = 1 for Wilson's incompatible modes condensed ("im"), 0 for the plain brick;
+ * lpb_level1_products: mcat (8 x 576) = P_k^T Ke P_k and nkq (64 x 576, 8 k + q) = P_k^T mcat_q P_k,
+ *   P_k the child prolongations (loadpath/mg.py:57-75, 601-677);
+ * lpb_uniform_numpy: numpy.random.default_rng(seed).random(n) (the power iteration's start,
+ *   loadpath/mg.py:779-781);
+ * lpb_layout_dims: {pz, cpz, node field entries, cell field entries, mask entries} of the layout;
+ * lpb_layout_nodes_f64 / lpb_unlayout_nodes_f64 / lpb_layout_cells_f64: grid order (3, NX, NY, NZ)
+ *   or (nx, ny, nz) <-> the device layout, host arrays. */
+int lpb_hex8_ke(double nu, int incompatible, double* ke_out);
+int lpb_level1_products(const double* ke, double* mcat, double* nkq);
+int lpb_uniform_numpy(long long seed, long long n, double* out);
+int lpb_layout_dims(int nx, int ny, int nz, long long* out);
+int lpb_layout_nodes_f64(const double* grid, double* out, int nx, int ny, int nz);
+int lpb_unlayout_nodes_f64(const double* dev_layout, double* grid, int nx, int ny, int nz);
+int lpb_layout_cells_f64(const double* grid, double* out, int nx, int ny, int nz);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,7 @@ _CTYPES = {
     "float": ctypes.c_float,
     "double": ctypes.c_double,
     "void": None,
+    "void*": ctypes.c_void_p,
 }
 _STATUS = {-1: "bad arguments", -2: "kernel launch failed", -3: "size beyond the kernel's limit"}
 # kernels each entry point launches (1 when not listed; 0 for host-only entries)
@@ -35,7 +36,12 @@ _KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_m
             "lpb_mma_part_len": 0, "lpb_mma_prepare": 2, "lpb_mma_newton_a": 2, "lpb_mma_newton_b": 2,
             "lpb_mma_trial": 2, "lpb_project": 2, "lpb_live_seed": 2,
             "lpb_dead_loads": 2, "lpb_apply_rf_f32": 2, "lpb_apply_explicit_modal_f32": 2,
-            "lpb_apply_explicit_modal_cheb_f32": 2}
+            "lpb_apply_explicit_modal_cheb_f32": 2, "lpb_modal_sym": 0, "lpb_hex8_ke": 0,
+            "lpb_level1_products": 0, "lpb_uniform_numpy": 0, "lpb_layout_dims": 0, "lpb_layout_nodes_f64": 0,
+            "lpb_unlayout_nodes_f64": 0, "lpb_layout_cells_f64": 0, "lpb_mg_levels": 0, "lpb_mg_strict": 0,
+            "lpb_mg_destroy": 0,
+            # the handle's entries launch on its own stream; their kernels are not counted here
+            "lpb_mg_create": 0, "lpb_mg_set_moduli": 0, "lpb_mg_solve": 0}
 # entries whose kernel count depends on their arguments
 _VARIABLE = {"lpb_sensitivity": lambda a: 1 + (a[9] is not None),
              "lpb_band_solve_cols_f32": lambda a: a[3] + (a[3] + 7) // 8,
@@ -64,8 +70,8 @@ def parse_header(path: str = HEADER):
     text = open(path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     out = []
-    for m in re.finditer(r"\b(int|void|long long)\s+(lpb_\w+)\s*\(([^)]*)\)\s*;", text):
-        ret, name, args = m.group(1), m.group(2), m.group(3).strip()
+    for m in re.finditer(r"\b(int|void\s*\*|void|long long)\s*(lpb_\w+)\s*\(([^)]*)\)\s*;", text):
+        ret, name, args = re.sub(r"\s+", "", m.group(1)) if "*" in m.group(1) else m.group(1), m.group(2), m.group(3).strip()
         types = []
         if args and args != "void":
             for a in args.split(","):

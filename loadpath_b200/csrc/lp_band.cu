@@ -4,10 +4,10 @@
 // 3 (N1 N2 + N2 + 1) + 2 dofs), so:
 //   1. k_band_factor: signed Cholesky A = L S L^T (S = diag(+-1): a symmetric LU without pivoting,
 //      failing only on an exactly zero pivot, as SuperLU does) of the band stored as 32 x 32
-//      tiles (tile (R, d) = rows 32R..,
-//      columns 32(R - d)..), right-looking by tile columns; one cooperative launch whose blocks
-//      meet at a bounded grid barrier twice per tile column. A tile column's diagonal block is
-//      factored (and its lower-triangular inverse formed) by one warp in registers.
+//      tiles (tile (R, d) = rows 32R.., columns 32(R - d)..), left-looking by tile rows as a
+//      dataflow: each block owns tile rows and waits only on the progress counts of the rows it
+//      reads (no grid-wide barrier). A diagonal tile is factored by one warp in registers; its
+//      lower-triangular inverse (for step 2) is formed after the row is published.
 //   2. k_band_inverse: A^-1 = L^-T S L^-1 applied to the identity, 32 columns per block: a
 //      forward then a backward block substitution over the band tiles. Only the lower triangle
 //      is needed (rows >= the block's first column); k_sym_lower copies it across.
@@ -17,7 +17,7 @@
 // level of a 256 x 128 x 128 grid, n = 4131 and bw = 275.
 #include "lp_common.cuh"
 
-#define LP_BAR_LIMIT (1u << 22)   // polls before a grid-barrier wait gives up and flags an error
+#define LP_BAR_LIMIT (1u << 22)   // polls before a progress wait gives up and flags an error
 
 namespace {
 
@@ -31,36 +31,47 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
-// bounded sense-counting barrier over all blocks of a cooperative launch; false when a wait
-// gave up (the caller stops and the error flag is set)
-__device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int* err) {
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Block-wide: wait until prog[row] > need (thread 0 polls with acquire loads, bounded); seen
+// keeps the last value read (the same in every thread), so a later wait on the same row with a
+// smaller need returns at once. False when a wait gave up (err is set).
+__device__ bool wait_row(const unsigned* prog, int row, unsigned need, unsigned& seen, int* err) {
   __shared__ int ok_s;
-  __syncthreads();
+  __shared__ unsigned seen_s;
+  if (seen > need) return true;
   if (threadIdx.x == 0) {
     int ok = 1;
-    __threadfence();
-    const unsigned g = gen;
-    if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicExch(&bar[32], g + 1u);
-    } else {
-      unsigned it = 0;
-      while (ld_acquire(&bar[32]) == g) {
-        if (++it > LP_BAR_LIMIT) {
-          ok = 0;
-          atomicExch(err, 1);
-          break;
-        }
-        if (it > 64) __nanosleep(32);
+    unsigned v = ld_acquire(prog + row), it = 0;
+    while (v <= need) {
+      if (++it > LP_BAR_LIMIT) {
+        ok = 0;
+        atomicExch(err, 1);
+        break;
       }
+      if (it > 64) __nanosleep(32);
+      v = ld_acquire(prog + row);
     }
-    __threadfence();
     ok_s = ok;
+    seen_s = v;
   }
   __syncthreads();
-  gen += 1u;
-  return ok_s != 0;
+  seen = seen_s;
+  const bool ok = ok_s != 0;
+  __syncthreads();   // ok_s / seen_s are rewritten by the next wait
+  return ok;
+}
+
+// row R of the factor now has its first v tile columns: tiles stored by every thread of the
+// block are made visible before the count
+__device__ __forceinline__ void publish_row(unsigned* prog, int row, unsigned v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(prog + row, v);
+  }
 }
 
 // Tiles another block wrote are read with ld.global.cg (L2, not a possibly stale L1 line).
@@ -69,10 +80,10 @@ __device__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen, int
 // warp 0: lane i holds row i in registers. Each pivot p gives L_jj = sqrt|p| and S_j = sign(p),
 // so negative pivots are factored as they are: a symmetric LU without pivoting, as the
 // reference's SuperLU in symmetric mode (loadpath/mg.py:744-747). Writes L (upper part zero) over
-// the tile, L^-1 (row-major) to linv and S to sg[0..31]. A pivot that is exactly zero (or not
-// finite) records its dof (1-based) in *info: the operator is singular; the arithmetic continues.
-__device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv, double* __restrict__ sg,
-                            long long row0, int* info, double (*sm)[33]) {
+// the tile and into sm, and S to sg[0..31]. A pivot that is exactly zero (or not finite) records
+// its dof (1-based) in *info: the operator is singular; the arithmetic continues.
+__device__ void factor_diag(double* __restrict__ tile, double* __restrict__ sg, long long row0, int* info,
+                            double (*sm)[33]) {
   if (threadIdx.x < 32) {
     const int i = threadIdx.x;
     double a[32];
@@ -104,8 +115,15 @@ __device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv
       sm[i][m] = v;
     }
     __syncwarp();
-    // lane c: column c of L^-1, right-looking (the 32 row updates of a step are independent)
-    const int c = i;
+  }
+}
+
+// linv (row-major) = L^-1 of the diagonal factor in sm (factor_diag's copy), by warp 0: lane c
+// forms column c, right-looking (the 32 row updates of a step are independent). The inverse is
+// for k_band_inverse; the factorisation itself solves its panels against L.
+__device__ void diag_inverse(double* __restrict__ linv, const double (*sm)[33]) {
+  if (threadIdx.x < 32) {
+    const int c = threadIdx.x;
     const double rd = 1.0 / sm[c][c];
     double x[32];
 #pragma unroll
@@ -122,85 +140,130 @@ __device__ void factor_diag(double* __restrict__ tile, double* __restrict__ linv
   }
 }
 
-// a (32 x 32 tile, global, in place) = a * li^T * S with li lower triangular (the panel solve
-// L_a = A_a L_kk^-T S_k)
-__device__ void panel_tile(double* __restrict__ a, const double* __restrict__ li, const double* __restrict__ sg,
-                           double (*sa)[33], double (*sl)[33]) {
+// This thread's four entries x[q] of a 32 x 32 tile (entry e = threadIdx.x + 256 q, row e / 32,
+// column e % 32) -= a S b^T, with a, b tiles in global memory (read through L2) and S the
+// pivot signs of their column block.
+__device__ void sub_product(double (&x)[4], const double* __restrict__ a, const double* __restrict__ b,
+                            const double* __restrict__ sg, double (*sa)[33], double (*sb)[33]) {
+  __syncthreads();   // the previous product is done with sa / sb
   for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
     sa[e >> 5][e & 31] = __ldcg(a + e);
-    sl[e >> 5][e & 31] = __ldcg(li + e);
+    sb[e >> 5][e & 31] = __ldcg(b + e) * __ldcg(sg + (e & 31));
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
-    const int r = e >> 5, c = e & 31;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-    for (int m = 0; m < 32; m += 4) {   // sl[c][m] = 0 for m > c (lower triangular)
-      s0 += sa[r][m] * sl[c][m];
-      s1 += sa[r][m + 1] * sl[c][m + 1];
-      s2 += sa[r][m + 2] * sl[c][m + 2];
-      s3 += sa[r][m + 3] * sl[c][m + 3];
-    }
-    a[e] = ((s0 + s1) + (s2 + s3)) * __ldcg(sg + c);
-  }
-  __syncthreads();
-}
-
-// x (32 x 32 tile, global, in place) -= la * S * lc^T
-__device__ void update_tile(double* __restrict__ x, const double* __restrict__ la, const double* __restrict__ lc,
-                            const double* __restrict__ sg, double (*sa)[33], double (*sl)[33]) {
-  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
-    sa[e >> 5][e & 31] = __ldcg(la + e);
-    sl[e >> 5][e & 31] = __ldcg(lc + e) * __ldcg(sg + (e & 31));
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
-    const int r = e >> 5, c = e & 31;
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + 256 * q, r = e >> 5, c = e & 31;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
     for (int m = 0; m < 32; m += 4) {
-      s0 += sa[r][m] * sl[c][m];
-      s1 += sa[r][m + 1] * sl[c][m + 1];
-      s2 += sa[r][m + 2] * sl[c][m + 2];
-      s3 += sa[r][m + 3] * sl[c][m + 3];
+      s0 += sa[r][m] * sb[c][m];
+      s1 += sa[r][m + 1] * sb[c][m + 1];
+      s2 += sa[r][m + 2] * sb[c][m + 2];
+      s3 += sa[r][m + 3] * sb[c][m + 3];
     }
-    x[e] = __ldcg(x + e) - ((s0 + s1) + (s2 + s3));
+    x[q] -= (s0 + s1) + (s2 + s3);
   }
-  __syncthreads();
 }
 
-// Right-looking tiled band Cholesky over tile columns k. Panel phase: tile (k + a, k),
-// a = 1..D, goes to block (a - 1) mod gridDim. Update phase: the D (D + 1) / 2 trailing tiles
-// (k + a, k + c), 1 <= c <= a <= D, numbered u = a (a - 1) / 2 + c - 1, go to block u mod gridDim;
-// block 0 (which owns u = 0, tile (k + 1, k + 1)) then factors that tile. bar: two zeroed words;
-// err: set when a barrier wait gave up.
+// y -= l S l^T for the tile l this block holds in registers (four entries per thread, as x)
+__device__ void sub_self_product(double (&y)[4], const double (&l)[4], const double* __restrict__ sg,
+                                 double (*sa)[33], double (*sb)[33]) {
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    sa[e >> 5][e & 31] = l[q];
+    sb[e >> 5][e & 31] = l[q] * __ldcg(sg + (e & 31));
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + 256 * q, r = e >> 5, c = e & 31;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; m += 4) {
+      s0 += sa[r][m] * sb[c][m];
+      s1 += sa[r][m + 1] * sb[c][m + 1];
+      s2 += sa[r][m + 2] * sb[c][m + 2];
+      s3 += sa[r][m + 3] * sb[c][m + 3];
+    }
+    y[q] -= (s0 + s1) + (s2 + s3);
+  }
+}
+
+// x = x L_cc^-T S_c (the panel solve L_Rc = X L_cc^-T S_c) by forward substitution against the
+// diagonal factor tile lc: warp w holds rows w, w + 8, w + 16, w + 24 of x (x[q], the lane is the
+// column), so each step is a shuffle and a multiply-add per row, no inverse on the chain.
+__device__ void solve_panel(double (&x)[4], const double* __restrict__ lc, const double* __restrict__ sg,
+                            double (*sb)[33]) {
+  __syncthreads();
+  for (int e = threadIdx.x; e < 1024; e += blockDim.x) sb[e >> 5][e & 31] = __ldcg(lc + e);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const double rd = 1.0 / sb[lane][lane];
+  double y[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int m = 0; m < 32; ++m) {
+    const double rm = __shfl_sync(0xffffffffu, rd, m);
+    const double lm = sb[lane][m];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double ym = __shfl_sync(0xffffffffu, x[q], m) * rm;
+      if (lane == m) y[q] = ym;
+      if (lane > m) x[q] -= ym * lm;
+    }
+  }
+  const double s = __ldcg(sg + lane);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) x[q] = y[q] * s;
+}
+
+// Left-looking band factorisation by tile rows, as a dataflow: block b owns tile rows
+// R = b, b + gridDim.x, ... and works through each row's tiles left to right,
+//   L_Rc = (A_Rc - sum_j L_Rj S_j L_cj^T) L_cc^-T S_c     (c = R - D .. R - 1, j = max(R, c) - D .. c - 1)
+//   L_RR S_R L_RR^T = A_RR - sum_j L_Rj S_j L_Rj^T         (factored by warp 0, factor_diag)
+// publishing prog[R] = the number of tile columns of row R done after each tile. A tile waits
+// only for the rows it reads (prog[c] > j for L_cj, prog[c] > c for L_cc^-1), so the chain from
+// one row to the next is one panel solve (forward substitution against L_cc), one product and
+// one diagonal factor; the diagonal tile's other terms are summed as the row's tiles come out. prog: nt zeroed words; every block
+// must be resident (a cooperative launch); err: set when a wait gave up.
 __global__ void __launch_bounds__(256, 1) k_band_factor(double* __restrict__ t, double* __restrict__ linv,
                                                         double* __restrict__ sg, LpBand bd, int* __restrict__ info,
-                                                        unsigned* __restrict__ bar, int* __restrict__ err) {
+                                                        unsigned* __restrict__ prog, int* __restrict__ err) {
   __shared__ double sa[32][33];
-  __shared__ double sl[32][33];
-  unsigned gen = 0;
-  const unsigned nb = gridDim.x;
-  const int b = blockIdx.x;
-  const int nu = bd.D * (bd.D + 1) / 2;
-  if (b == 0) factor_diag(tile_at(t, bd, 0, 0), linv, sg, 0, info, sa);
-  if (!grid_barrier(bar, nb, gen, err)) return;
-  for (int k = 0; k + 1 < bd.nt; ++k) {
-    for (int a = 1 + b; a <= bd.D && k + a < bd.nt; a += nb)
-      panel_tile(tile_at(t, bd, k + a, a), linv + (long long)k * 1024, sg + 32LL * k, sa, sl);
-    if (!grid_barrier(bar, nb, gen, err)) return;
-    for (int u = b; u < nu; u += nb) {
-      int a = 1;
-      while ((a + 1) * a / 2 <= u) ++a;         // u in [a (a - 1) / 2, a (a + 1) / 2)
-      const int c = u - a * (a - 1) / 2 + 1;
-      if (k + a < bd.nt)
-        update_tile(tile_at(t, bd, k + a, a - c), tile_at(t, bd, k + a, a), tile_at(t, bd, k + c, c), sg + 32LL * k,
-                    sa, sl);
+  __shared__ double sb[32][33];
+  for (int R = blockIdx.x; R < bd.nt; R += gridDim.x) {
+    const int c0 = R - bd.D > 0 ? R - bd.D : 0;
+    double y[4];   // the diagonal tile, its terms subtracted as the row's tiles are formed
+    const double* tr0 = tile_at(t, bd, R, 0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y[q] = __ldcg(tr0 + threadIdx.x + 256 * q);
+    for (int c = c0; c < R; ++c) {
+      double* trc = tile_at(t, bd, R, R - c);
+      double x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = __ldcg(trc + threadIdx.x + 256 * q);
+      unsigned seen = 0;
+      const int j0 = c - bd.D > c0 ? c - bd.D : c0;
+      for (int j = j0; j < c; ++j) {
+        if (!wait_row(prog, c, (unsigned)j, seen, err)) return;   // row c has its column j
+        sub_product(x, tile_at(t, bd, R, R - j), tile_at(t, bd, c, c - j), sg + 32LL * j, sa, sb);
+      }
+      if (!wait_row(prog, c, (unsigned)c, seen, err)) return;     // row c's diagonal factor
+      solve_panel(x, tile_at(t, bd, c, 0), sg + 32LL * c, sb);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) trc[threadIdx.x + 256 * q] = x[q];
+      publish_row(prog, R, (unsigned)(c + 1));
+      sub_self_product(y, x, sg + 32LL * c, sa, sb);
     }
-    if (b == 0)
-      factor_diag(tile_at(t, bd, k + 1, 0), linv + (long long)(k + 1) * 1024, sg + 32LL * (k + 1), 32LL * (k + 1), info,
-                  sa);
-    if (!grid_barrier(bar, nb, gen, err)) return;
+    double* tr0w = tile_at(t, bd, R, 0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tr0w[threadIdx.x + 256 * q] = y[q];
+    __syncthreads();
+    factor_diag(tr0w, sg + 32LL * R, 32LL * R, info, sa);
+    publish_row(prog, R, (unsigned)(R + 1));
+    diag_inverse(linv + 1024LL * R, sa);   // off the chain: the next rows only need L
   }
 }
 
@@ -473,8 +536,9 @@ long long lpb_band_dims(int nx, int ny, int nz, long long* out) {
 
 // Signed Cholesky of the band in t (from lpb_coarse_band_*), in place; linv: nt x 1024 doubles
 // (the inverses of the diagonal factor tiles); sgn: 32 nt doubles, the pivot signs; info: one
-// device int, 0 or the first dof (1-based) whose pivot was exactly zero (or not finite); bar: 64 device words of scratch; err: one device int, set when
-// a barrier wait gave up. One cooperative launch of max(D, D (D + 1) / 2) blocks.
+// device int, 0 or the first dof (1-based) whose pivot was exactly zero (or not finite); bar:
+// max(64, nt) device words of scratch (the rows' progress counts); err: one device int, set when
+// a wait gave up. One cooperative launch of up to 2 (D + 1) blocks, each owning tile rows.
 int lpb_band_factor(double* t, double* linv, double* sgn, int* info, unsigned* bar, int* err, LP_GRID_ARGS,
                     void* stream) {
   LpGrid g = LP_GRID;
@@ -485,13 +549,15 @@ int lpb_band_factor(double* t, double* linv, double* sgn, int* info, unsigned* b
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band_factor, 256, 0);
-  // one block per trailing tile while they all fit at once (a cooperative launch needs every
-  // block resident), fewer blocks with several tiles each beyond that
-  long long nblocks = (long long)bd.D * (bd.D + 1) / 2;
+  // D + 1 rows in flight hide each row's own products behind the chain from row to row; twice
+  // that gives each block a row's worth of slack
+  long long nblocks = 2LL * (bd.D + 1);
+  if (nblocks > bd.nt) nblocks = bd.nt;
   const long long cap = (long long)per_sm * nsm;
   if (nblocks > cap) nblocks = cap;
   if (!coop || nblocks < 1) return LP_ERR_SIZE;
-  if (cudaMemsetAsync(bar, 0, 64 * sizeof(unsigned), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
+  const long long words = bd.nt > 64 ? bd.nt : 64;
+  if (cudaMemsetAsync(bar, 0, words * sizeof(unsigned), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
   if (cudaMemsetAsync(info, 0, sizeof(int), LP_ST) != cudaSuccess) return LP_ERR_LAUNCH;
   void* args[] = {&t, &linv, &sgn, &bd, &info, &bar, &err};
   if (cudaLaunchCooperativeKernel((const void*)k_band_factor, dim3((unsigned)nblocks), dim3(256), args, 0, LP_ST) !=

@@ -39,21 +39,23 @@ struct LpGrid {
   __host__ __device__ long long cell_zc_stride() const { return 4LL * nx * ny; }
   __host__ __device__ long long nodes_padded() const { return (long long)(nx + 1) * (ny + 1) * pz; }
   __host__ __device__ long long cells_padded() const { return (long long)nx * ny * cpz; }
-  // the node / cell at index t of a field (memory order); false on the z padding
+  // the node / cell at index t of a field (memory order); false on the z padding. The column
+  // index t / 4 is taken in 32-bit unsigned arithmetic (a field of one component holds fewer
+  // than 2^34 entries), which divides several times faster than 64-bit.
   __host__ __device__ bool node_at(long long t, int& x, int& y, int& z) const {
-    long long r = t >> 2;
-    x = (int)(r % (nx + 1));
-    r /= (nx + 1);
-    y = (int)(r % (ny + 1));
-    z = 4 * (int)(r / (ny + 1)) + (int)(t & 3);
+    const unsigned r = (unsigned)(t >> 2), NXu = (unsigned)(nx + 1), NYu = (unsigned)(ny + 1);
+    const unsigned q = r / NXu, w = q / NYu;
+    x = (int)(r - q * NXu);
+    y = (int)(q - w * NYu);
+    z = 4 * (int)w + (int)(t & 3);
     return z <= nz;
   }
   __host__ __device__ bool cell_at(long long t, int& x, int& y, int& z) const {
-    long long r = t >> 2;
-    x = (int)(r % nx);
-    r /= nx;
-    y = (int)(r % ny);
-    z = 4 * (int)(r / ny) + (int)(t & 3);
+    const unsigned r = (unsigned)(t >> 2), nxu = (unsigned)nx, nyu = (unsigned)ny;
+    const unsigned q = r / nxu, w = q / nyu;
+    x = (int)(r - q * nxu);
+    y = (int)(q - w * nyu);
+    z = 4 * (int)w + (int)(t & 3);
     return z < nz;
   }
 };

@@ -94,17 +94,3 @@ def hex8_ke(nu: float, element: str | None = None) -> np.ndarray:
             raise ValueError(element)
         _CACHE[key] = 0.5 * (k + k.T)
     return _CACHE[key].copy()
-
-
-def child_prolongations() -> np.ndarray:
-    """P_k (8, 24, 24): coarse-cell dofs -> dofs of child k (loadpath/mg.py:57-75)."""
-    out = np.zeros((8, 24, 24))
-    for k in range(8):
-        for q in range(8):
-            p = (CORNERS[k] + CORNERS[q]) * 0.5
-            for r in range(8):
-                w = float(np.prod(np.where(CORNERS[r] == 1, p, 1.0 - p)))
-                if w:
-                    for i in range(3):
-                        out[k, 3 * q + i, 3 * r + i] = w
-    return out

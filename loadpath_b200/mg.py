@@ -312,10 +312,13 @@ class GridElasticity:
         self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.ke64 = torch.tensor(self.ke.reshape(-1), dtype=torch.float64, device=self.device)
         self.ke32 = self.ke64.float()
-        pk = fem.child_prolongations()
-        self._mcat = np.einsum("kai,ab,kbj->kij", pk, self.ke, pk).reshape(8, 576)
-        # level 2 from level 1: N_(k,q) = P_k^T M_q P_k, 64 x 576 (index 8 k + q)
-        self._nkq = np.einsum("kai,qab,kbj->kqij", pk, self._mcat.reshape(8, 24, 24), pk).reshape(64, 576)
+        # level 1: M_k = P_k^T Ke P_k (8 x 576); level 2 from level 1: N_(k,q) = P_k^T M_q P_k
+        # (64 x 576, index 8 k + q); formed by the library, so the C-ABI solver handle
+        # (lpb_mg_create) shares their bits
+        self._mcat = np.zeros((8, 576))
+        self._nkq = np.zeros((64, 576))
+        lib().lpb_level1_products(np.ascontiguousarray(self.ke).ctypes.data, self._mcat.ctypes.data,
+                                  self._nkq.ctypes.data)
         self._nkq_dev = {}
         g1 = np.zeros(279)
         if lib().lpb_modal_g1(np.ascontiguousarray(self.ke).ctypes.data, g1.ctypes.data) != 279:
@@ -699,7 +702,7 @@ class GridElasticity:
                                                  lv.mask.data_ptr(), *g.args, st)
         linv = self._tbuf("band_linv", (nt * 1024,), torch.float64)
         info = self._tbuf("band_info", (2,), torch.int32)
-        bar = self._tbuf("band_bar", (64,), torch.int32)
+        bar = self._tbuf("band_bar", (max(64, nt),), torch.int32)
         ainv = self._tbuf("band_ainv", (npad, npad), torch.float64)
         sgn = self._tbuf("band_sgn", (npad,), torch.float64)
         self._coarse = {"ainv": ainv, "v": self._tbuf("coarse_v", (npad,), torch.float64), "n": n}

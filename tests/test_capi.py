@@ -30,8 +30,14 @@ def test_library_builds_and_exports_every_declared_symbol():
 def test_header_is_plain_c():
     text = open(HEADER).read()
     assert "torch" not in text and "at::" not in text and "std::" not in text
+    # status codes and sizes, the solver handle (an opaque pointer) and its destructor
     for name, ret, types in parse_header():
-        assert ret in (ctypes.c_int, ctypes.c_longlong), name
+        if name == "lpb_mg_create":
+            assert ret is ctypes.c_void_p
+        elif name == "lpb_mg_destroy":
+            assert ret is None
+        else:
+            assert ret in (ctypes.c_int, ctypes.c_longlong), name
 
 
 def test_modal_ke_pattern_host_only():
@@ -155,3 +161,51 @@ def test_modal_symmetry_classes_host_only():
         raise AssertionError("coefficients without the brick's symmetry must be refused")
     except RuntimeError:
         pass
+
+
+def test_handle_host_helpers_host_only():
+    """The host code the solver handle shares with the Python class: numpy's default_rng(seed).random()
+    restated (the power iteration's start), the hex8 element, the level-1 Galerkin products and the
+    device layout of node and cell fields."""
+    import torch
+
+    from loadpath_b200.fem import hex8_ke
+    from loadpath_b200.grid import DevGrid
+    from oracle import ref_numpy as R
+
+    for seed in (0, 1, 2, 7, 4095):
+        got = np.zeros(1000)
+        lib().lpb_uniform_numpy(seed, 1000, got.ctypes.data)
+        np.testing.assert_array_equal(got, np.random.default_rng(seed).random(1000))
+    for inc, el in ((1, "im"), (0, "plain")):
+        for nu in (0.2, 0.3, 0.45):
+            ke = np.zeros((24, 24))
+            lib().lpb_hex8_ke(nu, inc, ke.ctypes.data)
+            ref = hex8_ke(nu, el)
+            np.testing.assert_allclose(ke, ref, rtol=0, atol=1e-14 * np.abs(ref).max())
+            np.testing.assert_array_equal(ke, ke.T)
+    ke = np.ascontiguousarray(hex8_ke(0.3, "im"))
+    mcat, nkq = np.zeros((8, 576)), np.zeros((64, 576))
+    lib().lpb_level1_products(ke.ctypes.data, mcat.ctypes.data, nkq.ctypes.data)
+    pk = R.child_prolongations()
+    want_m = np.einsum("kai,ab,kbj->kij", pk, ke, pk)
+    np.testing.assert_allclose(mcat.reshape(8, 24, 24), want_m, rtol=0, atol=1e-14 * np.abs(want_m).max())
+    want_n = np.einsum("kai,qab,kbj->kqij", pk, want_m, pk)
+    np.testing.assert_allclose(nkq.reshape(8, 8, 24, 24), want_n, rtol=0, atol=1e-14 * np.abs(want_n).max())
+    dims = (6, 4, 10)
+    g = DevGrid(dims, device="cpu")
+    rng = np.random.default_rng(0)
+    nodes = rng.standard_normal(g.node_shape)
+    out = np.zeros(g.n_node_field)
+    lib().lpb_layout_nodes_f64(np.ascontiguousarray(nodes).ctypes.data, out.ctypes.data, *dims)
+    np.testing.assert_array_equal(out, g.nodes_to_dev(nodes, torch.float64).reshape(-1).numpy())
+    back = np.zeros(g.node_shape)
+    lib().lpb_unlayout_nodes_f64(out.ctypes.data, back.ctypes.data, *dims)
+    np.testing.assert_array_equal(back, nodes)
+    cells = rng.standard_normal(dims)
+    cout = np.zeros(g.cpz // 4 * dims[1] * dims[0] * 4)
+    lib().lpb_layout_cells_f64(np.ascontiguousarray(cells).ctypes.data, cout.ctypes.data, *dims)
+    np.testing.assert_array_equal(cout, g.cells_to_dev(cells, torch.float64).reshape(-1).numpy())
+    sizes = np.zeros(5, np.int64)
+    lib().lpb_layout_dims(*dims, sizes.ctypes.data)
+    assert list(sizes) == [g.pz, g.cpz, g.n_node_field, g.cpz // 4 * dims[1] * dims[0] * 4, g.pz * g.NY * g.NX]
