@@ -4,7 +4,7 @@ Run in a container that has the loadpath source tree (read-only is fine):
 
     LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
 
-(names: element transfers femops filter mma hierarchies top3d config0; default all but config0,
+(names: element transfers femops filter mma hierarchies top3d config0 oc_step; default all but config0,
 which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
@@ -272,6 +272,64 @@ def make_config0():
                         xphys=rec["x"], hist=np.array(hist), load_per_node=val / (p.dims[1] + 1))
 
 
+def make_oc_step():
+    """loadpath's design step as a whole (loadpath/simp.py:2249-2376: the optimality-criteria step
+    whose volume multiplier is bracketed outward from the last step's in log space, then found by
+    false position with the Illinois halving), captured from the reference's own optimize on the
+    12x4x6 cantilever of its benchmarks (domain_for: load and support cells pinned, padded filter,
+    default options) for its first three iterations. numpy inside loadpath.simp is replaced by a
+    pass-through whose clip, called by the step's trial function, records the trial's inputs (the
+    design x, ratio = sqrt(-dc / dv), the move limits, beta, the volume target, the last step's
+    multiplier) and outputs from the calling frames; the accepted step is the last trial of an
+    iteration."""
+    os.environ["LOADPATH_HEX8"] = "im"
+    import loadpath.simp as S
+    from loadpath.benchmarks.problems import cantilever_3d
+    from loadpath.benchmarks.run import NU, design_volfrac, domain_for
+
+    p = cantilever_3d(12, 4, 6, 0.3, 1.5)
+    dom, _ = domain_for(p)
+    opts = S.SimpOptions(volume_fraction=design_volfrac(p, dom), filter_radius=p.rmin, max_iterations=3)
+    real_np = S.np
+    trials = []
+
+    class _Numpy:
+        def __getattr__(self, k):
+            return getattr(real_np, k)
+
+        def clip(self, a, lo, hi, *args, **kw):
+            out = real_np.clip(a, lo, hi, *args, **kw)
+            f1 = sys._getframe(1)
+            if f1.f_code.co_name == "stepped":
+                l1, l2 = f1.f_locals, f1.f_back.f_locals
+                trials.append(dict(it=int(l2["it"]), x=l1["x"].copy(), ratio=l1["ratio"].copy(), move=float(l2["move"]),
+                                   beta=float(l1["beta"]), target=float(l1["target"]),
+                                   lam_last=float(l2["lam_last"]) if l2["lam_last"] is not None else float("nan"),
+                                   lm=float(l1["lm_"]), xn=out.copy(), pres=l1["pres"].copy(),
+                                   wdesign=l1["wdesign"].copy(), void=l1["void"]))
+            return out
+
+    S.np = _Numpy()
+    try:
+        S.optimize(dom, NU, opts)
+    finally:
+        S.np = real_np
+    its = sorted({t["it"] for t in trials})
+    out = dict(dims=np.array(dom.dims), pitch=float(dom.mesh.pitch), radius=float(opts.filter_radius),
+               pad=bool(S._pad(opts)), eta=float(opts.eta), elem_ijk=dom.mesh.elem_ijk, iterations=np.array(its))
+    for k, it in enumerate(its):
+        mine = [t for t in trials if t["it"] == it]
+        first, last = mine[0], mine[-1]
+        assert first["void"] is None
+        xn = last["xn"].copy()
+        xn[first["pres"]] = 1.0
+        out.update({f"x{k}": first["x"], f"ratio{k}": first["ratio"], f"move{k}": first["move"],
+                    f"beta{k}": first["beta"], f"target{k}": first["target"], f"lam_last{k}": first["lam_last"],
+                    f"pres{k}": first["pres"], f"w{k}": first["wdesign"], f"x_new{k}": xn, f"lm{k}": last["lm"],
+                    f"n_eval{k}": len(mine)})
+    np.savez_compressed(os.path.join(HERE, "oc_step.npz"), **out)
+
+
 def main(names=None):
     gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
             "mma": make_mma,
@@ -279,7 +337,7 @@ def main(names=None):
                                     make_hierarchy("odd_plain", (11, 5, 7), "plain", 2, 30, 0.0),
                                     make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
                                     make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
-            "top3d": make_top3d, "config0": make_config0}
+            "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step}
     for name in names or [k for k in gens if k != "config0"]:
         gens[name]()
 

@@ -87,3 +87,39 @@ def test_chain_rule_matches_oracle():
     pd.chain(out, g.cells_to_dev(grad, torch.float64), dxp, clip=True)
     want = np.minimum(R.grid_filter(grad * want_d / hs, taps), 0.0)
     np.testing.assert_allclose(g.cells_to_host(out), want, rtol=1e-12, atol=1e-14 * np.abs(want).max())
+
+
+def test_oc_step_matches_reference_run():
+    """The device step against the step the reference's own optimize took in its first three
+    iterations on the 12x4x6 cantilever (tests/golden/oc_step.npz, captured from loadpath.simp's
+    trial function): the accepted design, the multiplier and the number of trial steps."""
+    from loadpath_b200.grid import DevGrid
+    from loadpath_b200.simp import DeviceFilter, ProjectedDesign
+
+    gold = np.load(os.path.join(GOLD, "oc_step.npz"))
+    dims = tuple(int(d) for d in gold["dims"])
+    ijk = gold["elem_ijk"]
+
+    def grid(v):
+        out = np.zeros(dims, v.dtype)
+        out[tuple(ijk.T)] = v
+        return out
+
+    g = DevGrid(dims)
+    flt = DeviceFilter(g, float(gold["radius"]), float(gold["pitch"]), pad=bool(gold["pad"]))
+    for k in range(len(gold["iterations"])):
+        pres = grid(gold[f"pres{k}"])
+        flags = g.set_cells(g.cell_field(torch.uint8), torch.from_numpy(pres.astype(np.uint8)))
+        pd = ProjectedDesign(flt, w=g.cells_to_dev(grid(gold[f"w{k}"]), torch.float64), flags=flags)
+        lam_last = float(gold[f"lam_last{k}"])
+        pd.lam_last = None if np.isnan(lam_last) else lam_last
+        ratio = grid(gold[f"ratio{k}"])
+        xd = g.cells_to_dev(grid(gold[f"x{k}"]), torch.float64)
+        dcd = g.cells_to_dev(-ratio ** 2, torch.float64)
+        dvd = g.cells_to_dev(np.ones(dims), torch.float64)
+        xn, lm, held = pd.oc_step(xd, dcd, dvd, float(gold[f"move{k}"]), float(gold[f"beta{k}"]), float(gold["eta"]),
+                                  float(gold[f"target{k}"]))
+        assert held
+        assert pd.n_eval == int(gold[f"n_eval{k}"])
+        np.testing.assert_allclose(lm, float(gold[f"lm{k}"]), rtol=1e-10)
+        np.testing.assert_allclose(g.cells_to_host(xn), grid(gold[f"x_new{k}"]), rtol=0, atol=1e-11)

@@ -226,3 +226,34 @@ def test_oracle_oc_loadpath_step_lands_on_the_volume(beta, lam_last):
     free = ~pres & ~void
     assert np.all(np.abs(xn - x)[free] <= 0.2 + 1e-15)
     assert np.all(xn[pres] == 1.0) and np.all(xn[void] == 0.0)
+
+
+def _oc_golden():
+    g = np.load(os.path.join(GOLD, "oc_step.npz"))
+    dims = tuple(int(d) for d in g["dims"])
+    ijk = g["elem_ijk"]
+
+    def grid(v):
+        out = np.zeros(dims, v.dtype)
+        out[tuple(ijk.T)] = v
+        return out
+    return g, dims, grid
+
+
+def test_oracle_oc_loadpath_step_matches_reference_run():
+    """The oracle's restatement of loadpath's design step against the step the reference's own
+    optimize took in its first three iterations on the 12x4x6 cantilever (tests/golden/oc_step.npz):
+    the accepted design, the multiplier and the number of trial steps."""
+    g, dims, grid = _oc_golden()
+    taps = R.filter_taps(float(g["radius"]), float(g["pitch"]))
+    hs = np.full(dims, sum(w for _, w in taps)) if bool(g["pad"]) else R.filter_row_sums(dims, taps)
+    for k in range(len(g["iterations"])):
+        ratio = grid(g[f"ratio{k}"])
+        lam_last = float(g[f"lam_last{k}"])
+        xn, lm, n_eval, held = R.oc_loadpath_step(
+            grid(g[f"x{k}"]), -ratio ** 2, np.ones(dims), float(g[f"move{k}"]), float(g[f"beta{k}"]), float(g["eta"]),
+            lambda v: R.grid_filter(v, taps), hs, grid(g[f"w{k}"]), float(g[f"target{k}"]), grid(g[f"pres{k}"]), None,
+            None if np.isnan(lam_last) else lam_last)
+        assert n_eval == int(g[f"n_eval{k}"])
+        np.testing.assert_allclose(lm, float(g[f"lm{k}"]), rtol=1e-12)
+        np.testing.assert_allclose(xn, grid(g[f"x_new{k}"]), rtol=0, atol=1e-13)
