@@ -267,6 +267,16 @@ int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const dou
 /* volumes[j] of the clipped OC step at nl = 31 multipliers lam[j] (device), weights gv = H (1 / hs) */
 int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv, const double* lam, int nl, double move, double* part, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* dv, double lam, double move, double* part, double* change, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* top3d's bisection on the multiplier (loadpath/benchmarks/reference.py:100-110) walked on the
+ * device, the host walk of simp.oc_bisection restated: state (7 doubles) = {l1, l2, below, above,
+ * lmid, passes, done}; lpb_oc_walk_init starts it at (0, l2) and writes the first 31 candidates;
+ * after each lpb_oc_volumes pass over the candidates lpb_oc_walk folds the volumes in, decides
+ * what they decide and writes the next candidates, or finishes (done = 1, lmid the step's
+ * multiplier). handle: a graph WHILE node's conditional (the loop runs while candidates are
+ * open) or 0. lpb_oc_apply_at is lpb_oc_apply at a multiplier in device memory (state + 4). */
+int lpb_oc_walk_init(double* state, double* cands, double l2, double target, double tol, void* stream);
+int lpb_oc_walk(long long handle, double* state, const double* vols, double* cands, double target, double tol, void* stream);
+int lpb_oc_apply_at(double* xnew, const double* x, const double* dc, const double* dv, const double* lam, double move, double* part, double* change, int nx, int ny, int nz, int pz, int cpz, void* stream);
 /* loadpath's own design update; flags: uint8 per cell, bit 0 passive solid, bit 1 passive void
  * (NULL: none). lpb_project: xp = (tanh(b eta) + tanh(b (xt - eta))) / den and its derivative dxp
  * (either NULL to skip), held cells 1 / 0 with derivative 0, and *vol = sum xp w when w is given

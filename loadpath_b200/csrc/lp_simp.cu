@@ -214,11 +214,87 @@ __global__ void k_oc_final(const double* __restrict__ part, int nblocks, int nl,
   }
 }
 
-// the OC step at one multiplier: xnew and the change max|xnew - x| partials
+// The top3d bisection on the volume multiplier walked on the device (the walk of
+// loadpath_b200.simp.oc_bisection, loadpath/benchmarks/reference.py:100-110): state = {l1, l2,
+// below (smallest multiplier seen with volume <= target), above (largest seen with volume >
+// target), lmid, passes, done}. With absorb the 31 volumes of the last candidates are folded into
+// below / above first; the walk then decides every midpoint the evaluations decide and stops at
+// the first one they leave open, writing the next 31 candidates (the ladder l2 / 2^(2i+1) while l1 =
+// 0, else the next five levels of the bisection tree below the open interval, breadth first), or
+// finishes (done = 1, lmid the last midpoint). With a conditional handle (a graph WHILE node) the
+// loop goes on while candidates are open.
+__global__ void k_oc_walk(cudaGraphConditionalHandle handle, int use_handle, double* __restrict__ state,
+                          const double* __restrict__ vols, double* __restrict__ cands, double target, double tol,
+                          int absorb) {
+  double l1 = state[0], l2 = state[1], below = state[2], above = state[3], lmid = state[4], passes = state[5];
+  if (absorb) {
+    for (int j = 0; j < 31; ++j) {
+      if (vols[j] > target) above = fmax(above, cands[j]);
+      else below = fmin(below, cands[j]);
+    }
+    passes += 1.0;
+  }
+  unsigned need = 0;
+  while ((l2 - l1) / (l1 + l2) > tol) {
+    const double m = 0.5 * (l2 + l1);
+    if (m >= below) {
+      lmid = l2 = m;
+      continue;
+    }
+    if (m <= above) {
+      lmid = l1 = m;
+      continue;
+    }
+    if (l1 == 0.0) {
+      for (int i = 0; i < 31; ++i) cands[i] = ldexp(l2, -(2 * i + 1));
+    } else {
+      double qa[63], qb[63];
+      int head = 0, tail = 1;
+      qa[0] = l1;
+      qb[0] = l2;
+      for (int n = 0; n < 31; ++n) {
+        const double a = qa[head], b = qb[head];
+        ++head;
+        const double mm = 0.5 * (b + a);
+        cands[n] = mm;
+        qa[tail] = a;
+        qb[tail] = mm;
+        ++tail;
+        qa[tail] = mm;
+        qb[tail] = b;
+        ++tail;
+      }
+    }
+    need = 1;
+    break;
+  }
+  state[0] = l1;
+  state[1] = l2;
+  state[2] = below;
+  state[3] = above;
+  state[4] = lmid;
+  state[5] = passes;
+  state[6] = need ? 0.0 : 1.0;
+  if (use_handle) cudaGraphSetConditional(handle, need);
+}
+
+__global__ void k_oc_walk_init(double* __restrict__ state, double l2) {
+  state[0] = 0.0;
+  state[1] = l2;
+  state[2] = __longlong_as_double(0x7ff0000000000000LL);    // +inf
+  state[3] = -__longlong_as_double(0x7ff0000000000000LL);   // -inf
+  state[4] = __longlong_as_double(0x7ff8000000000000LL);    // no midpoint yet
+  state[5] = 0.0;
+  state[6] = 0.0;
+}
+
+// the OC step at one multiplier (lam, or *lam_dev when given): xnew and the change max|xnew - x|
+// partials
 __global__ void k_oc_apply(double* __restrict__ xnew, const double* __restrict__ x, const double* __restrict__ dc,
-                           const double* __restrict__ dv, double lam, double move, LpGrid g,
-                           double* __restrict__ part) {
+                           const double* __restrict__ dv, double lam_h, const double* __restrict__ lam_dev,
+                           double move, LpGrid g, double* __restrict__ part) {
   __shared__ double sh[32];
+  const double lam = lam_dev ? *lam_dev : lam_h;
   const long long total = g.cells_padded();
   double mx = 0.0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -433,6 +509,24 @@ int lpb_sensitivity(double* dc, const double* xphys, const double* ce, const dou
   return LP_OK;
 }
 
+// the device walk of the bisection (k_oc_walk): init (state: 7 doubles, the first candidates in
+// cands) and one step after a volumes pass; handle: the conditional of a graph WHILE node or 0
+int lpb_oc_walk_init(double* state, double* cands, double l2, double target, double tol, void* stream) {
+  if (!state || !cands || !(l2 > 0.0)) return LP_ERR_ARG;
+  k_oc_walk_init<<<1, 1, 0, LP_ST>>>(state, l2);
+  k_oc_walk<<<1, 1, 0, LP_ST>>>(cudaGraphConditionalHandle{}, 0, state, nullptr, cands, target, tol, 0);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+int lpb_oc_walk(long long handle, double* state, const double* vols, double* cands, double target, double tol,
+                void* stream) {
+  if (!state || !vols || !cands) return LP_ERR_ARG;
+  k_oc_walk<<<1, 1, 0, LP_ST>>>((cudaGraphConditionalHandle)handle, handle != 0, state, vols, cands, target, tol, 1);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
 // volumes[j] = sum_c xnew(lam[j])_c gv_c for nl = 31 multipliers; part: nl * 592 doubles
 int lpb_oc_volumes(double* volumes, const double* x, const double* dc, const double* dv, const double* gv,
                    const double* lam, int nl, double move, double* part, LP_GRID_ARGS, void* stream) {
@@ -450,7 +544,18 @@ int lpb_oc_apply(double* xnew, const double* x, const double* dc, const double* 
                  double* part, double* change, LP_GRID_ARGS, void* stream) {
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !xnew || !x || !dc || !dv || !part || !change) return LP_ERR_ARG;
-  k_oc_apply<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xnew, x, dc, dv, lam, move, g, part);
+  k_oc_apply<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xnew, x, dc, dv, lam, nullptr, move, g, part);
+  k_max_final2<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, change);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// lpb_oc_apply at the multiplier *lam (device), e.g. the walk's lmid (state + 4)
+int lpb_oc_apply_at(double* xnew, const double* x, const double* dc, const double* dv, const double* lam,
+                    double move, double* part, double* change, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !xnew || !x || !dc || !dv || !lam || !part || !change) return LP_ERR_ARG;
+  k_oc_apply<<<LP_SIMP_BLOCKS, 256, 0, LP_ST>>>(xnew, x, dc, dv, 0.0, lam, move, g, part);
   k_max_final2<<<1, 1024, 0, LP_ST>>>(part, LP_SIMP_BLOCKS, change);
   LP_LAUNCH_CHECK();
   return LP_OK;

@@ -19,7 +19,7 @@ import math
 import numpy as np
 import torch
 
-from ._lib import lib
+from ._lib import add_launches, lib
 from .grid import DevGrid, ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 
@@ -177,6 +177,7 @@ def adjoint_sensitivity(ge, pairs, xp, dproj, out, modulus=1.0, penal=3.0, emin=
 ALIVE = 1e-3          # cells at or below this projected density leave the solve (loadpath/simp.py:59)
 REDUCE_BELOW = 0.8    # ...once fewer than this share of the cells are alive (loadpath/simp.py:61)
 MG_SLOW_ITERS = 60    # CG iterations past which the SIMP driver leaves the multigrid (loadpath/simp.py:85)
+OC_TOL = 1e-3         # top3d's bisection stops at (l2 - l1) / (l1 + l2) <= 1e-3 (loadpath/benchmarks/reference.py:100)
 MG_MAXITER = 2000     # the SIMP driver's CG cap for its multigrid (loadpath/simp.py:182)
 
 
@@ -485,6 +486,9 @@ class Top3dLoop:
         self._part = torch.zeros(31 * 592 + 1024, dtype=torch.float64, device=g.device)
         self._lam = torch.zeros(31, dtype=torch.float64, device=g.device)
         self._vols = torch.zeros(31, dtype=torch.float64, device=g.device)
+        self._oc_state = torch.zeros(8, dtype=torch.float64, device=g.device)
+        self.device_oc = True    # the bisection walked on the device (oc())
+        self._oc_graph = None
         self.loop = 0
         self.history = []
         self.timing = None       # a list to collect per-phase CUDA events into, or None
@@ -601,22 +605,52 @@ class Top3dLoop:
 
     def oc(self):
         """top3d's bisection on the volume multiplier (loadpath/benchmarks/reference.py:100-110);
-        the multipliers are evaluated on the device, 31 per pass over the cells."""
+        the multipliers are evaluated on the device, 31 per pass over the cells. With device_oc
+        (the default) the walk itself runs on the device too (lpb_oc_walk): with graphs the
+        passes are one graph launch whose WHILE node repeats volumes + walk while candidates are
+        open, so the step reads nothing back; the multiplier and the pass count reach the host
+        with the step's scalars. Otherwise the host walks (oc_bisection), reading each pass."""
         L = lib()
         st = stream_handle()
         g = self.grid
+        target = self.volfrac * self.ncell
+        if not self.device_oc:
+            def volumes(cands):
+                self._lam.copy_(torch.tensor(cands, dtype=torch.float64))
+                L.lpb_oc_volumes(self._vols.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(),
+                                 self.filter.gv.data_ptr(), self.filter.gv.data_ptr(), self._lam.data_ptr(), 31,
+                                 self.move, self._part.data_ptr(), *g.args, st)
+                return self._vols.cpu().numpy()
 
-        def volumes(cands):
-            self._lam.copy_(torch.tensor(cands, dtype=torch.float64))
+            lmid, self.oc_passes = oc_bisection(volumes, target)
+            L.lpb_oc_apply(self.xnew.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(),
+                           lmid, self.move, self._part.data_ptr(), self._scal[1:].data_ptr(), *g.args, st)
+            self.lmid = lmid
+            return
+        state = self._oc_state
+        L.lpb_oc_walk_init(state.data_ptr(), self._lam.data_ptr(), 1e9, target, OC_TOL, st)
+
+        def body(handle):
+            stb = stream_handle()
             L.lpb_oc_volumes(self._vols.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(),
                              self.filter.gv.data_ptr(), self._lam.data_ptr(), 31, self.move, self._part.data_ptr(),
-                             *g.args, st)
-            return self._vols.cpu().numpy()
+                             *g.args, stb)
+            L.lpb_oc_walk(handle, state.data_ptr(), self._vols.data_ptr(), self._lam.data_ptr(), target, OC_TOL, stb)
 
-        lmid, self.oc_passes = oc_bisection(volumes, self.volfrac * self.ncell)
-        L.lpb_oc_apply(self.xnew.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(), lmid,
-                       self.move, self._part.data_ptr(), self._scal[1:].data_ptr(), *g.args, st)
-        self.lmid = lmid
+        if self.ge.use_graphs:
+            self._oc_graph = self.ge._graph(("oc_walk", self.x.data_ptr(), target, self.move), body, loop=True)
+            self.ge._replay(self._oc_graph)
+        else:
+            self._oc_graph = None
+            while True:
+                body(0)
+                if float(state[6].item()) != 0.0:
+                    break
+        L.lpb_oc_apply_at(self.xnew.data_ptr(), self.x.data_ptr(), self.dcf.data_ptr(), self.filter.gv.data_ptr(),
+                          state[4:].data_ptr(), self.move, self._part.data_ptr(), self._scal[1:].data_ptr(), *g.args, st)
+        # the multiplier and the pass count, read with the step's scalars
+        L.lpb_memcpy_async(self._scal[2:].data_ptr(), state[4:].data_ptr(), 16, st)
+        self.lmid = None
 
     def step(self):
         """One iteration; returns (compliance, change) as top3d reports them."""
@@ -644,6 +678,10 @@ class Top3dLoop:
                           emin=self.emin)
         self.x, self.xnew = self.xnew, self.x
         vals = self._scal[:8 + len(self.fs)].cpu().numpy()
+        if self.device_oc:
+            self.lmid, self.oc_passes = float(vals[2]), int(vals[3])
+            if self._oc_graph is not None and self.oc_passes > 1:
+                add_launches(self._oc_graph[2] * (self.oc_passes - 1))   # the body ran once per pass
         if self.shards is not None:
             c, change = self.c_total, float(vals[1])
         else:

@@ -50,3 +50,26 @@ def test_smoke_entry():
     import __graft_entry__ as ge
 
     ge.smoke()
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_device_bisection_walk_equals_host_walk(graphs):
+    """The OC bisection walked on the device (lpb_oc_walk, in a graph WHILE loop or looped from
+    the host) takes the host walk's (oc_bisection) candidates, passes and multiplier, so the
+    designs agree bit for bit."""
+    from loadpath_b200.simp import Top3dLoop
+
+    dims = (24, 8, 8)
+    nx, ny, nz = dims
+    fixed = np.zeros((3, nx + 1, ny + 1, nz + 1), bool)
+    fixed[:, 0] = True
+    f = np.zeros(fixed.shape)
+    f[2, nx, :, 0] = -1.0
+    loops = [Top3dLoop(dims, 0.3, 1.5, fixed, f, rtol=1e-10, coarse_cells=40) for _ in range(2)]
+    loops[1].device_oc = False
+    loops[0].ge.use_graphs = graphs
+    for it in range(6):
+        (c0, ch0), (c1, ch1) = loops[0].step(), loops[1].step()
+        assert (c0, ch0) == (c1, ch1), it
+        assert loops[0].lmid == loops[1].lmid and loops[0].oc_passes == loops[1].oc_passes, it
+        assert torch.equal(loops[0].x, loops[1].x), it
