@@ -36,30 +36,38 @@ def available():
 
 
 class Cells:
-    """A level's cells that carry stiffness, x-major; rows[x, y, z] is a cell's index in that list,
-    or -1 (loadpath/mgops.py:220-244: the same fields)."""
+    """The cells of a level that carry stiffness, with the fields the reference's callers read
+    (loadpath/mgops.py:220-244):
+
+    - cells: (n, 3) int64, the (x, y, z) of each listed cell, x-major (C order of the grid);
+    - n: their count; rows: an int64 grid, a listed cell's position in `cells`, -1 elsewhere;
+    - base: (n,) the flat index of each cell's low corner in the node grid (X+1, Y+1, Z+1);
+    - off: (24,) the flat offset of element dof 3k + d from `base` in a (3, X+1, Y+1, Z+1) field:
+      component d's plane plus corner k's step, bit a of k stepping along axis a;
+    - ft(dtype): a (24, n) work array kept per dtype."""
 
     def __init__(self, active: np.ndarray):
-        active = np.asarray(active, bool)
-        ijk = np.argwhere(active)
-        self.active = active
-        self.cells = np.ascontiguousarray(ijk, np.int64)
-        self.n = len(ijk)
-        self.rows = np.full(active.shape, -1, np.int64)
-        self.rows[tuple(ijk.T)] = np.arange(self.n)
-        nshape = tuple(int(d) + 1 for d in active.shape)
-        self.base = np.ascontiguousarray(np.ravel_multi_index(tuple(ijk.T), nshape), np.int64)
-        nn = int(np.prod(nshape))
-        sy, sz = nshape[1] * nshape[2], nshape[2]
-        self.off = np.array([d * nn + (k & 1) * sy + (k >> 1 & 1) * sz + (k >> 2 & 1)
-                             for k in range(8) for d in range(3)], np.int64)
-        self.buffers = {}
+        self.active = np.asarray(active, bool)
+        shape = self.active.shape
+        listed = np.flatnonzero(self.active)
+        self.n = int(listed.size)
+        self.cells = np.ascontiguousarray(np.column_stack(np.unravel_index(listed, shape)), np.int64)
+        rows = np.full(self.active.size, -1, np.int64)
+        rows[listed] = np.arange(self.n, dtype=np.int64)
+        self.rows = rows.reshape(shape)
+        nodes = np.array(shape, np.int64) + 1
+        stride = np.array([nodes[1] * nodes[2], nodes[2], 1], np.int64)
+        self.base = np.ascontiguousarray(self.cells @ stride)
+        bits = (np.arange(8)[:, None] >> np.arange(3)[None, :]) & 1
+        plane = int(np.prod(nodes)) * np.arange(3, dtype=np.int64)
+        self.off = np.ascontiguousarray((bits @ stride)[:, None] + plane[None, :]).reshape(24)
+        self._work = {}
 
     def ft(self, dtype):
-        key = np.dtype(dtype).str
-        if key not in self.buffers:
-            self.buffers[key] = np.empty((24, self.n), dtype)
-        return self.buffers[key]
+        dtype = np.dtype(dtype)
+        if dtype not in self._work:
+            self._work[dtype] = np.empty((24, self.n), dtype)
+        return self._work[dtype]
 
 
 def _sfx(dtype):

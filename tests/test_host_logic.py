@@ -143,3 +143,29 @@ def test_oracle_live_solve_reduces_and_falls_back():
     anchor2 = R.cells_touching(held | (f2 != 0).any(axis=0))
     u2 = R.live_solve(ke, fixed, f2, support, anchor2)(e, x)
     np.testing.assert_allclose(u2, R.assembled_solve(ke, e, fixed, f2), rtol=1e-12)
+
+
+def test_mgops_cells_fields():
+    """mgops.Cells carries the fields the reference's callers read (loadpath/mgops.py:220-244),
+    checked here element by element: the dof at base + off[3k + d] of a (3, X+1, Y+1, Z+1) field
+    is component d of the cell's corner k."""
+    from loadpath_b200.mgops import Cells
+
+    rng = np.random.default_rng(3)
+    shape = (4, 3, 5)
+    active = rng.random(shape) > 0.3
+    c = Cells(active)
+    want = [(x, y, z) for x in range(4) for y in range(3) for z in range(5) if active[x, y, z]]
+    assert c.n == len(want) and c.cells.tolist() == [list(w) for w in want]
+    for i, (x, y, z) in enumerate(want):
+        assert c.rows[x, y, z] == i
+    assert (c.rows[~active] == -1).all()
+    field = np.arange(3 * 5 * 4 * 6).reshape(3, 5, 4, 6)
+    flat = field.reshape(-1)
+    for i, (x, y, z) in enumerate(want):
+        assert flat[c.base[i]] == field[0, x, y, z]
+        for k in range(8):
+            for d in range(3):
+                assert flat[c.base[i] + c.off[3 * k + d]] == field[d, x + (k & 1), y + (k >> 1 & 1), z + (k >> 2 & 1)]
+    assert c.ft(np.float32).shape == (24, c.n) and c.ft(np.float32) is c.ft("float32")
+    assert c.base.dtype == c.off.dtype == c.cells.dtype == np.int64
