@@ -165,11 +165,12 @@ int lpb_coarse_dense_f64(double* a, int kind, const double* w, const double* mca
  * row-major at t + (R (D + 1) + d) * 1024, padding dofs past n as identity rows.
  * lpb_band_dims: out = {n, nt, D, bw}, returns the tile count nt (D + 1).
  * lpb_band_factor: in-place tiled signed Cholesky A = L S L^T, S = diag(+-1) (a symmetric LU
- *   without pivoting, as the reference's SuperLU in symmetric mode; one cooperative launch, tile
- *   rows owned by blocks that wait on each other's progress counts, bounded waits); linv:
- *   nt * 1024 doubles; sgn: 32 nt doubles, the pivot signs; info: 0 or the 1-based band dof of the
- *   first exactly zero (or non-finite) pivot; bar: max(64, nt) device words of scratch; err: set
- *   when a wait gave up.
+ *   without pivoting, as the reference's SuperLU in symmetric mode; one cooperative launch: helper
+ *   blocks own tile rows, a critical block finishes the rows in order, all waiting on each other's
+ *   progress counts with bounded waits); linv: nt * 1024 doubles, the inverses of the diagonal
+ *   factor tiles; sgn: 32 nt doubles, the pivot signs; info: 0 or the 1-based band dof of the first
+ *   exactly zero (or non-finite) pivot; bar: 2 max(64, nt) device words of scratch; err: set when
+ *   a wait gave up.
  * lpb_band_inverse: ainv (32 nt x 32 nt, row-major, band numbering) = A^-1 from the factor.
  * lpb_band_solve_*: f_out = A^-1 f_in through the band numbering; v: 32 nt doubles scratch. */
 int lpb_coarse_band_f32(double* t, int kind, const float* w, const float* mcat, const int* patch_id, const float* patch_k, const float* k, const uint8_t* mask, int nx, int ny, int nz, int pz, int cpz, void* stream);
@@ -300,11 +301,11 @@ int lpb_graph_free(void* exec);
  * the stream, lpb_while_end instantiates it (an exec for lpb_graph_launch); the body's
  * lpb_cg_continue (sc: the PCG scalars, [0] |b|^2, [3] p.Ap, [4] |r|^2; state: iterations,
  * status) ends the loop once |r| <= rtol |b|, p.Ap <= 0, b = 0 or maxiter iterations ran. */
-/* Launch-geometry tuning (no reference counterpart): the z-segment length, in chunks of four
- * planes, of the fine float32 (knob 1) and float64 (2) apply and of the level-1 float32 (3) and
- * float64 (4) apply, per grid of nx x ny x nz cells; 0 clears it (the launcher's cost model
- * decides). Set by loadpath_b200.tune from timed candidates; results are the same operator, the
- * last bit of a float32 sum can differ at segment boundaries. */
+/* Launch-geometry tuning (no reference counterpart), per grid of nx x ny x nz cells: the
+ * persistent blocks per SM of the fine float32 (knob 1) and float64 (2) apply, and the z-segment
+ * length, in chunks of four planes, of the level-1 float32 (3) and float64 (4) apply; 0 clears it
+ * (the launcher decides). Set by loadpath_b200.tune from timed candidates; results are the same
+ * operator, the last bit of a float32 sum can differ at segment boundaries. */
 int lpb_tune_set(int knob, int nx, int ny, int nz, int value);
 int lpb_tune_get(int knob, int nx, int ny, int nz);
 int lpb_while_begin(void* stream, long long* handle, void** graph);

@@ -278,16 +278,39 @@ __device__ __forceinline__ void store4(double* p, const double (&o)[4]) {
   *reinterpret_cast<double2*>(p + 2) = make_double2(o[2], o[3]);
 }
 
-// One barrier per chunk: each thread waits for its stages, forms its two pairs of cells, publishes
-// its y shares into the exchange buffer of the chunk's parity, and the block meets once (which
-// also settles a wait that gave up); the owners then add their -y neighbour's shares and store
-// their four node planes. The exchange is double-buffered, so the next chunk's writes never meet
-// this chunk's reads. MODE 0 stores A u in out (float64: and, with dotp, the block's share of
-// u . A u); modes 1..3 (float32) store a Chebyshev update instead (cheb_store; out unused).
+// The work of a launch: units (tile, chunk), tile-major (tile = x tile + gx * y tile), block b
+// taking units [b U / B, (b + 1) U / B), so every block has the same number of chunks. A run of
+// consecutive chunks [cb, ce) of one tile is a segment; it loads one halo chunk below cb (its top
+// cell starts the z carry) and the chunk above ce - 1 (the upper plane of the last cell).
+struct FineSeg {
+  int tile, cb, ce;
+  int cstart, nload, nproc;   // loads from chunk cstart, nload of them; chunks processed
+};
+
+__device__ __forceinline__ FineSeg fine_seg(long long u, long long u1, int nchunks) {
+  FineSeg s;
+  s.tile = (int)(u / nchunks);
+  s.cb = (int)(u - (long long)s.tile * nchunks);
+  const long long left = u1 - u;
+  s.ce = left < (long long)(nchunks - s.cb) ? s.cb + (int)left : nchunks;
+  s.cstart = s.cb > 0 ? s.cb - 1 : 0;
+  s.nload = min(s.ce + 1, nchunks) - s.cstart;
+  s.nproc = s.ce - s.cstart;
+  return s;
+}
+
+// Persistent blocks, one barrier per chunk: each thread waits for its stages, forms its two pairs
+// of cells, publishes its y shares into the exchange buffer of the chunk's parity, and the block
+// meets once (which also settles a wait that gave up); the owners then add their -y neighbour's
+// shares and store their four node planes. The exchange is double-buffered, so the next chunk's
+// writes never meet this chunk's reads. The TMA ring runs over the block's loads of all its
+// segments in order, so the next segment's first chunks load while this one finishes. MODE 0
+// stores A u in out (float64: and, with dotp, the block's share of u . A u); modes 1..3 (float32)
+// store a Chebyshev update instead (cheb_store; out unused).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(TXC * TYC, (sizeof(T) == 4 ? 2 : 1))
 k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const uint8_t* __restrict__ mask,
-             const KSym<T> ks, LpGrid g, int zch, int nchunks, int* __restrict__ err, const FineCheb ch,
+             const KSym<T> ks, LpGrid g, int nchunks, int* __restrict__ err, const FineCheb ch,
              double* __restrict__ dotp) {
   typedef PairOps<T> O;
   typedef Pair<T> P;
@@ -297,23 +320,16 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
   FineSmem<T>& sm = *reinterpret_cast<FineSmem<T>*>(smem_raw + ((128u - (raw_off & 127u)) & 127u));
   const int tid = threadIdx.x;
   const int i = tid % TXC, j = tid / TXC;
-  const int x0 = blockIdx.x * (TXC - 1), y0 = blockIdx.y * (TYC - 1);
-  const int c_begin = blockIdx.z * zch;
-  const int c_end = min(c_begin + zch, nchunks);
-  const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-  if (c_begin >= c_end) {
-    if (dotp && tid == 0) dotp[bid] = 0.0;
-    return;
-  }
-  const int cstart = c_begin > 0 ? c_begin - 1 : 0;     // one halo chunk below the segment
-  const int nload = min(c_end + 1, nchunks) - cstart;   // + the chunk above the last one
-  const int nproc = c_end - cstart;
-  const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
-  const bool writer = i >= 1 && j >= 1 && nx_ < g.NX() && ny_ < g.NY();
-  const long long obase = writer ? g.node(nx_, ny_, 0) : 0;   // chunk c at obase + c * zcs
+  const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
+  const long long units = (long long)gx * gy * nchunks;
+  const long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
   const long long cs = g.comp_stride(), zcs = g.node_zc_stride();
   constexpr uint32_t UBYTES = 3 * BOX * BOX * 4 * sizeof(T);
   constexpr uint32_t EBYTES = TXC * TYC * 4 * sizeof(T);
+  if (u0 >= u1) {
+    if (dotp && tid == 0) dotp[blockIdx.x] = 0.0;
+    return;
+  }
 
   // alignment contract of every TMA operand and vector access, checked once per block: a
   // violation is recorded in *err (codes 10..17) and the block returns without touching memory
@@ -337,7 +353,7 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
   }
   __syncthreads();
   if (bad) {
-    if (dotp && tid == 0) dotp[bid] = 0.0;
+    if (dotp && tid == 0) dotp[blockIdx.x] = 0.0;
     return;
   }
   float cs_s = 0.0f, cs_c1 = 0.0f, cs_c2 = 0.0f;
@@ -346,128 +362,160 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
     cs_c1 = (float)ch.coef[2];
     cs_c2 = (float)ch.coef[3];
   }
+  // the producer (thread 0) walks the block's loads: its segment, the loads issued in it and in all
+  int total = 0;
+  long long pu = u0;
+  FineSeg ps = fine_seg(u0, u1, nchunks);
+  int pk = 0, issued = 0;
   if (tid == 0) {
+    for (long long u = u0; u < u1;) {
+      const FineSeg q = fine_seg(u, u1, nchunks);
+      total += q.nload;
+      u += q.ce - q.cb;
+    }
     for (int s = 0; s < NST; ++s) lp_mbar_init(&sm.full[s], 1);
     lp_fence_barrier_init();
   }
   __syncthreads();
-  auto issue = [&](int k) {
-    const int s = k % NST;
+  auto issue_next = [&]() {
+    if (pk == ps.nload) {
+      pu += ps.ce - ps.cb;
+      ps = fine_seg(pu, u1, nchunks);
+      pk = 0;
+    }
+    const int s = issued % NST;
+    const int x0 = (ps.tile % gx) * (TXC - 1), y0 = (ps.tile / gx) * (TYC - 1);
     lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
-    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, cstart + k, 0, &sm.full[s]);
-    lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, cstart + k, &sm.full[s]);
+    lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, ps.cstart + pk, 0, &sm.full[s]);
+    lp_tma_load_3d(sm.e[s].v, &maps.e, 4 * (x0 - 1), y0 - 1, ps.cstart + pk, &sm.full[s]);
+    ++pk;
+    ++issued;
   };
   if (tid == 0)
-    for (int kk = 0; kk < NST - 1 && kk < nload; ++kk) issue(kk);
-  T carry[4][3];
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) carry[q][c] = T(0);
+    while (issued < NST - 1 && issued < total) issue_next();
   double pacc = 0.0;
-  // modes of planes (0, 1) of the chunk in hand, formed by the iteration before
-  P m01[4][3];
-  bool ok = lp_mbar_wait(&sm.full[0], 0);
-  plane_modes<T>(sm, 0, i, j, 0, m01);
-
-  for (int k = 0; k < nproc; ++k) {
-    const int c = cstart + k;
-    const bool halo = c < c_begin;
-    const int s = k % NST;
-    // the stage refilled here was last read in the previous chunk, before its barrier
-    if (tid == 0 && k + NST - 1 < nload) issue(k + NST - 1);
-    const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + c * zcs)) : 0u;
-    ok = ok && lp_mbar_wait(&sm.full[s], (k / NST) & 1);
-    const bool has_next = k + 1 < nload;
-    if (has_next) ok = ok && lp_mbar_wait(&sm.full[(k + 1) % NST], ((k + 1) / NST) & 1);
-    // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
-    const T* ecol = &sm.e[s].v[(j * TXC + i) * 4];
-    P m23[4][3];
-    plane_modes<T>(sm, s, i, j, 2, m23);
-    P(*red)[3][TXC * TYC] = sm.red[k & 1];
-    P own[2][3];
-    T ucol[3][4];   // this node column's u (float64 dot), read before the barrier frees the stage
-    if constexpr (MODE == 0 && sizeof(T) == 8) {
-      if (dotp != nullptr && writer && !halo) {
+  bool ok = true, failed = false;
+  int n = 0;    // the block's load in hand (the chunk processed)
+  int it = 0;   // chunks processed: the exchange buffer alternates with it
+  for (long long u = u0; u < u1 && !failed;) {
+    const FineSeg sg = fine_seg(u, u1, nchunks);
+    u += sg.ce - sg.cb;
+    const int x0 = (sg.tile % gx) * (TXC - 1), y0 = (sg.tile / gx) * (TYC - 1);
+    const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
+    const bool writer = i >= 1 && j >= 1 && nx_ < g.NX() && ny_ < g.NY();
+    const long long obase = writer ? g.node(nx_, ny_, 0) : 0;   // chunk c at obase + c * zcs
+    T carry[4][3];
 #pragma unroll
-        for (int cc = 0; cc < 3; ++cc)
+    for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int t = 0; t < 4; ++t) ucol[cc][t] = col_at(sm, s, cc, i, j)[t];
+      for (int c = 0; c < 3; ++c) carry[q][c] = T(0);
+    // modes of planes (0, 1) of the chunk in hand, formed by the iteration before
+    P m01[4][3];
+    ok = ok && lp_mbar_wait(&sm.full[n % NST], (n / NST) & 1);
+    plane_modes<T>(sm, n % NST, i, j, 0, m01);
+    for (int k = 0; k < sg.nproc; ++k, ++n, ++it) {
+      const int c = sg.cstart + k;
+      const bool halo = c < sg.cb;
+      const int s = n % NST;
+      // the stages refilled here were last read before the previous chunk's barrier
+      if (tid == 0)
+        while (issued < n + NST && issued < total) issue_next();
+      const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + c * zcs)) : 0u;
+      ok = ok && lp_mbar_wait(&sm.full[s], (n / NST) & 1);
+      const bool has_next = k + 1 < sg.nload;
+      if (has_next) ok = ok && lp_mbar_wait(&sm.full[(n + 1) % NST], ((n + 1) / NST) & 1);
+      // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
+      const T* ecol = &sm.e[s].v[(j * TXC + i) * 4];
+      P m23[4][3];
+      plane_modes<T>(sm, s, i, j, 2, m23);
+      P(*red)[3][TXC * TYC] = sm.red[it & 1];
+      P own[2][3];
+      T ucol[3][4];   // this node column's u (float64 dot), read before the barrier frees the stage
+      if constexpr (MODE == 0 && sizeof(T) == 8) {
+        if (dotp != nullptr && writer && !halo) {
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) ucol[cc][t] = col_at(sm, s, cc, i, j)[t];
+        }
       }
-    }
-    // cells (0, 1): planes (0, 1) and (1, 2). In a halo chunk only cell 3 matters (its upper face
-    // starts the segment's carry), so the first pair is skipped there.
-    if (!halo) {
-      P hi[4][3], F[4][3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m01[q][cc].b, m23[q][cc].a);
-      cell_pair_sym<T>(ks, m01, hi, O::lds2(ecol), carry, F);
-      plane_pair_back<T>(F, own[0], &red[0][0][0], tid);
-    }
-    // the next chunk's planes (0, 1), kept for the next iteration
-    if (has_next) {
-      plane_modes<T>(sm, (k + 1) % NST, i, j, 0, m01);
-    } else {
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) m01[q][cc] = O::zero();
-    }
-    {
-      // cells (2, 3): planes (2, 3) and (3, 4)
-      P hi[4][3], F[4][3];
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m23[q][cc].b, m01[q][cc].a);
-      if (halo) {
+      // cells (0, 1): planes (0, 1) and (1, 2). In a halo chunk only cell 3 matters (its upper
+      // face starts the segment's carry), so the first pair is skipped there.
+      if (!halo) {
+        P hi[4][3], F[4][3];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int cc = 0; cc < 3; ++cc) carry[q][cc] = T(0);
+          for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m01[q][cc].b, m23[q][cc].a);
+        cell_pair_sym<T>(ks, m01, hi, O::lds2(ecol), carry, F);
+        plane_pair_back<T>(F, own[0], &red[0][0][0], tid);
       }
-      cell_pair_sym<T>(ks, m23, hi, O::lds2(ecol + 2), carry, F);
-      if (!halo) plane_pair_back<T>(F, own[1], &red[1][0][0], tid);
-    }
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicExch(err, 1);
-        // let the loads already issued land before the block exits (bounded as well)
-        for (int kk = k; kk < min(k + NST, nload); ++kk) lp_mbar_wait(&sm.full[kk % NST], (kk / NST) & 1);
+      // the next chunk's planes (0, 1), kept for the next iteration
+      if (has_next) {
+        plane_modes<T>(sm, (n + 1) % NST, i, j, 0, m01);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) m01[q][cc] = O::zero();
       }
-      break;
-    }
-    if (halo) continue;   // uniform across the block
-    if (writer) {
+      {
+        // cells (2, 3): planes (2, 3) and (3, 4)
+        P hi[4][3], F[4][3];
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const P a = O::add(own[0][cc], red[0][cc][tid - TXC]);
-        const P b = O::add(own[1][cc], red[1][cc][tid - TXC]);
-        T o[4] = {a.a, a.b, b.a, b.b};
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int t = 0; t < 4; ++t)
-          if (!((mb4 >> (8 * t + cc)) & 1u)) o[t] = T(0);
-        const long long idx = cc * cs + obase + c * zcs;
-        if constexpr (MODE == 0) {
-          store4(out + idx, o);
-          if constexpr (sizeof(T) == 8) {
-            if (dotp) {
+          for (int cc = 0; cc < 3; ++cc) hi[q][cc] = O::mk(m23[q][cc].b, m01[q][cc].a);
+        if (halo) {
 #pragma unroll
-              for (int t = 0; t < 4; ++t) pacc += o[t] * ucol[cc][t];
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) carry[q][cc] = T(0);
+        }
+        cell_pair_sym<T>(ks, m23, hi, O::lds2(ecol + 2), carry, F);
+        if (!halo) plane_pair_back<T>(F, own[1], &red[1][0][0], tid);
+      }
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(err, 1);
+          // let the loads already issued land before the block exits (bounded as well)
+          for (int kk = n; kk < issued; ++kk) lp_mbar_wait(&sm.full[kk % NST], (kk / NST) & 1);
+        }
+        failed = true;
+        break;
+      }
+      if (halo) continue;   // uniform across the block
+      if (writer) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const P a = O::add(own[0][cc], red[0][cc][tid - TXC]);
+          const P b = O::add(own[1][cc], red[1][cc][tid - TXC]);
+          T o[4] = {a.a, a.b, b.a, b.b};
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            if (!((mb4 >> (8 * t + cc)) & 1u)) o[t] = T(0);
+          const long long idx = cc * cs + obase + c * zcs;
+          if constexpr (MODE == 0) {
+            store4(out + idx, o);
+            if constexpr (sizeof(T) == 8) {
+              if (dotp) {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) pacc += o[t] * ucol[cc][t];
+              }
             }
+          } else if constexpr (sizeof(T) == 4) {
+            cheb_store<MODE>(ch, idx, make_float4(o[0], o[1], o[2], o[3]), cs_s, cs_c1, cs_c2);
           }
-        } else if constexpr (sizeof(T) == 4) {
-          cheb_store<MODE>(ch, idx, make_float4(o[0], o[1], o[2], o[3]), cs_s, cs_c1, cs_c2);
         }
       }
     }
+    // the segment's last load (the chunk above) was only read as the next chunk's planes
+    if (!failed && sg.nload > sg.nproc) ++n;
   }
   if (dotp) {
     __shared__ double sh[32];
     pacc = lp_block_sum(pacc, sh);
-    if (tid == 0) dotp[bid] = pacc;
+    if (tid == 0) dotp[blockIdx.x] = pacc;
   }
 }
 
@@ -598,42 +646,37 @@ static int launch_fine(T* out, const T* u, const T* e, const uint8_t* mask, cons
   if (!slots) return LP_ERR_LAUNCH;
   const int gx = (g.NX() + TXC - 2) / (TXC - 1), gy = (g.NY() + TYC - 2) / (TYC - 1);
   const int nchunks = g.pz / (int)zc;
-  // z segments: balance the grid over the resident blocks; a segment recomputes one halo chunk
-  int best_zch = nchunks;
-  double best = 1e30;
-  for (int zch = 2; zch <= nchunks; ++zch) {
-    const long long nseg = (nchunks + zch - 1) / zch;
-    const long long units = (long long)gx * gy * nseg;
-    const long long waves = (units + slots - 1) / slots;
-    const double cost = (double)waves * (zch + (nseg > 1 ? 0.3 : 0.0));
-    if (cost < best - 1e-9) {
-      best = cost;
-      best_zch = zch;
-    }
-  }
+  // persistent blocks: all resident blocks (or the tuned number per SM), each with an equal share
+  // of the (tile, chunk) units
+  long long nb = slots;
   const int tuned = lp_tune_lookup(sizeof(T) == 4 ? LP_KNOB_FINE_F32 : LP_KNOB_FINE_F64, g.nx, g.ny, g.nz);
-  if (tuned >= 2 && tuned <= nchunks) best_zch = tuned;
-  const int nseg = (nchunks + best_zch - 1) / best_zch;
-  dim3 grid(gx, gy, nseg);
+  if (tuned >= 1) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if ((long long)tuned * nsm < nb) nb = (long long)tuned * nsm;
+  }
+  const long long units = (long long)gx * gy * nchunks;
+  if (nb > units) nb = units;
   const FineCheb none{};
   const FineCheb& c = ch ? *ch : none;
   double* dp = nullptr;
-  const long long nb = (long long)grid.x * grid.y * grid.z;
   if (part) {
     if (nb > part_len) return LP_ERR_SIZE;
     dp = part;
   }
+  const dim3 grid((unsigned)nb);
   if constexpr (sizeof(T) == 4) {
     if (mode == 1)
-      k_apply_fine<float, 1><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+      k_apply_fine<float, 1><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, nchunks, err, c, nullptr);
     else if (mode == 2)
-      k_apply_fine<float, 2><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+      k_apply_fine<float, 2><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, nchunks, err, c, nullptr);
     else if (mode == 3)
-      k_apply_fine<float, 3><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+      k_apply_fine<float, 3><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, nchunks, err, c, nullptr);
     else
-      k_apply_fine<float, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, nullptr);
+      k_apply_fine<float, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, nchunks, err, c, nullptr);
   } else {
-    k_apply_fine<double, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, best_zch, nchunks, err, c, dp);
+    k_apply_fine<double, 0><<<grid, TXC * TYC, smem, st>>>(maps, out, mask, ks, g, nchunks, err, c, dp);
   }
   if (dp) k_fine_dot_final<<<1, 1024, 0, st>>>(dp, nb, dot_out);
   LP_LAUNCH_CHECK();

@@ -534,7 +534,7 @@ void build_coarse(Mg& m, Level& lv) {
                                      m.st));
   double* linv = (double*)m.buf("band_linv", 8 * 1024 * (size_t)nt);
   m.info = (int*)m.buf("band_info", 8);
-  unsigned* bar = (unsigned*)m.buf("band_bar", 4 * (size_t)std::max(64LL, nt));
+  unsigned* bar = (unsigned*)m.buf("band_bar", 8 * (size_t)std::max(64LL, nt));
   m.ainv = (double*)m.buf("band_ainv", 8 * (size_t)npad * npad);
   double* sgn = (double*)m.buf("band_sgn", 8 * (size_t)npad);
   m.cv = (double*)m.buf("coarse_v", 8 * (size_t)npad);

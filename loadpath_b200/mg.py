@@ -702,7 +702,7 @@ class GridElasticity:
                                                  lv.mask.data_ptr(), *g.args, st)
         linv = self._tbuf("band_linv", (nt * 1024,), torch.float64)
         info = self._tbuf("band_info", (2,), torch.int32)
-        bar = self._tbuf("band_bar", (max(64, nt),), torch.int32)
+        bar = self._tbuf("band_bar", (2 * max(64, nt),), torch.int32)
         ainv = self._tbuf("band_ainv", (npad, npad), torch.float64)
         sgn = self._tbuf("band_sgn", (npad,), torch.float64)
         self._coarse = {"ainv": ainv, "v": self._tbuf("coarse_v", (npad,), torch.float64), "n": n}

@@ -1,13 +1,14 @@
 """Launch-geometry autotuner for the stencil applies.
 
-The fine-level and level-1 applies march along z in segments of chunks (four node planes); a
-segment recomputes one halo cell, so short segments fill the GPU's resident blocks at the cost of
-more halo work, long ones the other way round. The launchers pick a segment length by a cost
-model; `autotune(ge)` instead times the applies of a built hierarchy at a set of candidate
-lengths (CUDA events on the working stream, after a warm-up launch) and records the fastest in
-the library's tuning table (`lpb_tune_set`), per grid and precision. Only launch geometry is
-tuned: the smoothing schedule (Chebyshev degree 2, as the reference's V-cycle) is part of the
-algorithm the CG iteration counts are checked against, and stays fixed.
+The level-1 apply marches along z in segments of chunks (four node planes); a segment recomputes
+one halo cell, so short segments fill the GPU's resident blocks at the cost of more halo work, long
+ones the other way round. The fine-level applies run persistent blocks that share the (tile,
+chunk) units out evenly; their knob is the number of blocks per SM (0: all that fit). The
+launchers pick a geometry by a cost model; `autotune(ge)` instead times the applies of a built
+hierarchy at a set of candidates (CUDA events on the working stream, after a warm-up launch) and
+records the fastest in the library's tuning table (`lpb_tune_set`), per grid and precision. Only
+launch geometry is tuned: the smoothing schedule (Chebyshev degree 2, as the reference's V-cycle)
+is part of the algorithm the CG iteration counts are checked against, and stays fixed.
 
 Results are kept for the process (a second hierarchy of the same grid reuses them) and can be
 saved to / loaded from a JSON file.
@@ -25,7 +26,7 @@ from .grid import stream_handle
 __all__ = ["KNOBS", "autotune", "candidates", "save", "load", "tuned"]
 
 KNOBS = {"fine_f32": 1, "fine_f64": 2, "level1_f32": 3, "level1_f64": 4}
-_RESULTS = {}        # (knob name, nx, ny, nz) -> {"best": zch, "us": {zch: time}}
+_RESULTS = {}        # (knob name, nx, ny, nz) -> {"best": value, "us": {value: time}}
 
 
 def candidates(nchunks, lo):
@@ -50,6 +51,9 @@ def _time(fn, reps):
     return a.elapsed_time(b) * 1e3 / reps
 
 
+FINE_CANDIDATES = (0, 1, 2)   # persistent fine-apply blocks per SM (0: all that fit)
+
+
 def _tune_one(name, grid, fn, lo, reps):
     L = lib()
     knob = KNOBS[name]
@@ -58,7 +62,8 @@ def _tune_one(name, grid, fn, lo, reps):
         L.lpb_tune_set(knob, grid.nx, grid.ny, grid.nz, _RESULTS[key]["best"])
         return _RESULTS[key]
     times = {}
-    for z in candidates(grid.pz // 4, lo):
+    cands = FINE_CANDIDATES if name.startswith("fine") else candidates(grid.pz // 4, lo)
+    for z in cands:
         L.lpb_tune_set(knob, grid.nx, grid.ny, grid.nz, z)
         times[z] = _time(fn, reps)
     best = min(times, key=times.get)
@@ -101,7 +106,7 @@ def autotune(ge, reps=5):
 
 
 def tuned():
-    """Every result of this process: {"knob nx ny nz": {"best": zch, "us": {zch: time}}}."""
+    """Every result of this process: {"knob nx ny nz": {"best": value, "us": {value: time}}}."""
     return {" ".join(map(str, k)): v for k, v in _RESULTS.items()}
 
 
