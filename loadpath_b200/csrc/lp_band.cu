@@ -728,6 +728,129 @@ __global__ void __launch_bounds__(512, 1) k_band_inverse(double* __restrict__ ai
   }
 }
 
+// k_band_inverse for CB columns per block (4 CB / 8 warps, one 8 x 8 block of each step's 32 x CB
+// result per warp), with the block's last D + 1 result blocks kept in shared memory (a ring; a
+// step reads D of them) and each step's band tiles, L_kk^-1 and (backward) Y_k loaded by
+// asynchronous copies while the step before finishes, so a step waits on no load of its own. A
+// block's chain is its column's 2 (nt - kb) steps, each bound by the SM's FP64 tensor rate, so
+// narrow column blocks (CB = 16) shorten the longest chain (column 0's). The same products in the
+// same order as k_band_inverse, so the same bits. Bands of at most INV_RING_D tile diagonals.
+constexpr int INV_RING_D = 9;
+constexpr int INV_RING_CB = 16;
+
+template <int CB>
+struct InvRing {
+  static constexpr int LDR = CB + 4;             // result block row stride
+  static constexpr int RB = 32 * LDR;            // doubles per result block
+  static constexpr int NW = 4 * CB / 8;          // warps
+  static size_t smem(int D) {
+    return ((size_t)(D + 1) * RB + (size_t)D * INV_TILE + 2 * (size_t)INV_TILE + 3 * (size_t)RB) * sizeof(double);
+  }
+};
+
+template <int CB>
+__global__ void __launch_bounds__(32 * InvRing<CB>::NW, 1)
+k_band_inverse_ring(double* __restrict__ ainv, const double* __restrict__ t, const double* __restrict__ linv,
+                    const double* __restrict__ sg, LpBand bd) {
+  typedef InvRing<CB> IR;
+  extern __shared__ __align__(16) double sm_inv[];
+  const int D = bd.D, RS = D + 1, R1 = D + 1;
+  double* ring = sm_inv;                   // result block k in slot k % RS
+  double* tiles = ring + RS * IR::RB;      // the step's band tiles, d = 1 .. D
+  double* diag = tiles + D * INV_TILE;     // L_kk^-1, by step parity
+  double* ykb = diag + 2 * INV_TILE;       // Y_k of a backward step, by step parity
+  double* tmp = ykb + 2 * IR::RB;          // S
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int row0 = 8 * (w / (CB / 8)), col0 = 8 * (w % (CB / 8));
+  const int orow = row0 + g, ocol = col0 + 2 * q;   // this lane's two outputs: (orow, ocol + i)
+  const long long np = 32LL * bd.nt;
+  const int j0 = CB * blockIdx.x;
+  const int kb = j0 >> 5;
+  const int nfwd = bd.nt - kb, total = 2 * nfwd;
+  const int nthr = 32 * IR::NW;
+  // step s: forward k = kb + s (s < nfwd), backward k = nt - 1 - (s - nfwd)
+  auto step_k = [&](int s) { return s < nfwd ? kb + s : bd.nt - 1 - (s - nfwd); };
+  auto step_dm = [&](int s, int k) { return s < nfwd ? min(D, k - kb) : min(D, bd.nt - 1 - k); };
+  // Y_k of a backward step is still in the ring when no later forward step reused its slot
+  auto y_in_ring = [&](int k) { return k >= bd.nt - RS; };
+  auto issue = [&](int s) {
+    const bool fwd = s < nfwd;
+    const int k = step_k(s), dm = step_dm(s, k);
+    for (int e = threadIdx.x; e < dm * 512; e += nthr) {
+      const int d = 1 + (e >> 9), rr = (e >> 4) & 31, cc = 2 * (e & 15);
+      const long long tk = fwd ? k : k + d;   // band tile (tk, d)
+      cp_async16(tiles + (d - 1) * INV_TILE + rr * INV_LD + cc, t + (tk * R1 + d) * 1024 + rr * 32 + cc);
+    }
+    for (int e = threadIdx.x; e < 512; e += nthr)
+      cp_async16(diag + (s & 1) * INV_TILE + (e >> 4) * INV_LD + 2 * (e & 15), linv + (long long)k * 1024 + 2 * e);
+    if (!fwd && !y_in_ring(k))
+      for (int e = threadIdx.x; e < 16 * CB; e += nthr) {
+        const int rr = e / (CB / 2), cc = 2 * (e % (CB / 2));
+        cp_async16(ykb + (s & 1) * IR::RB + rr * IR::LDR + cc, ainv + (32LL * k + rr) * np + j0 + cc);
+      }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  issue(0);
+  for (int s = 0; s < total; ++s) {
+    const bool fwd = s < nfwd;
+    const int k = step_k(s), dm = step_dm(s, k);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    double p0 = 0.0, p1 = 0.0, r0 = 0.0, r1 = 0.0;
+    for (int d = 1; d <= dm; ++d) {
+      const double* tc = tiles + (d - 1) * INV_TILE;
+      const int bk = fwd ? k - d : k + d;   // the earlier result block
+      const double* yb = ring + (bk % RS) * IR::RB + q * IR::LDR + col0 + g;
+      if (fwd) {
+        const double* ta = tc + (row0 + g) * INV_LD + q;
+#pragma unroll
+        for (int m = 0; m < 32; m += 8) {
+          dmma(p0, p1, ta[m], yb[m * IR::LDR]);
+          dmma(r0, r1, ta[m + 4], yb[(m + 4) * IR::LDR]);
+        }
+      } else {
+        const double* ta = tc + q * INV_LD + row0 + g;   // A[row][m] = T[m][row]
+#pragma unroll
+        for (int m = 0; m < 32; m += 8) {
+          dmma(p0, p1, ta[m * INV_LD], yb[m * IR::LDR]);
+          dmma(r0, r1, ta[(m + 4) * INV_LD], yb[(m + 4) * IR::LDR]);
+        }
+      }
+    }
+    __syncthreads();   // the band tiles are read: the next step's loads may land
+    if (s + 1 < total) issue(s + 1);
+    const double* dg = diag + (s & 1) * INV_TILE;
+    double* out = ainv + (32LL * k + orow) * np + j0 + ocol;
+    double* rs = ring + (k % RS) * IR::RB + orow * IR::LDR + ocol;
+    if (fwd) {
+      const long long gr = 32LL * k + orow;
+      tmp[orow * IR::LDR + ocol] = (gr == j0 + ocol ? 1.0 : 0.0) - (p0 + r0);
+      tmp[orow * IR::LDR + ocol + 1] = (gr == j0 + ocol + 1 ? 1.0 : 0.0) - (p1 + r1);
+    } else {
+      const double* yk = y_in_ring(k) ? rs : ykb + (s & 1) * IR::RB + orow * IR::LDR + ocol;
+      const double sr = __ldg(sg + 32LL * k + orow);
+      tmp[orow * IR::LDR + ocol] = sr * yk[0] - (p0 + r0);
+      tmp[orow * IR::LDR + ocol + 1] = sr * yk[1] - (p1 + r1);
+    }
+    __syncthreads();
+    double y0 = 0.0, y1 = 0.0;
+    if (fwd) {
+#pragma unroll
+      for (int m = 0; m < 32; m += 4)
+        dmma(y0, y1, dg[(row0 + g) * INV_LD + m + q], tmp[(m + q) * IR::LDR + col0 + g]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < 32; m += 4)   // A = L_kk^-T
+        dmma(y0, y1, dg[(m + q) * INV_LD + row0 + g], tmp[(m + q) * IR::LDR + col0 + g]);
+    }
+    rs[0] = y0;
+    rs[1] = y1;
+    *reinterpret_cast<double2*>(out) = make_double2(y0, y1);
+    __syncthreads();
+  }
+}
+
 // a[i][j] = a[j][i] for i < j (copy the lower triangle onto the upper), 32 x 32 tiles via
 // shared memory; block (bi, bj) with bi <= bj writes tile (bi, bj)
 __global__ void k_sym_lower(double* __restrict__ a, long long np) {
@@ -944,6 +1067,18 @@ int lpb_band_inverse(double* ainv, const double* t, const double* linv, const do
   if (!lp_grid_ok(g) || !ainv || !t || !linv || !sgn) return LP_ERR_ARG;
   const LpBand bd = lp_band(g.NX(), g.NY(), g.NZ());
   const long long np = 32LL * bd.nt;
+  if (bd.D <= INV_RING_D) {
+    typedef InvRing<INV_RING_CB> IR;
+    const size_t smem = IR::smem(bd.D);
+    if (cudaFuncSetAttribute(k_band_inverse_ring<INV_RING_CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return LP_ERR_SIZE;
+    k_band_inverse_ring<INV_RING_CB>
+        <<<(unsigned)(np / INV_RING_CB), 32 * IR::NW, smem, LP_ST>>>(ainv, t, linv, sgn, bd);
+    k_sym_lower<<<dim3(bd.nt, bd.nt), 256, 0, LP_ST>>>(ainv, np);
+    LP_LAUNCH_CHECK();
+    return LP_OK;
+  }
   // as many (tile, block) pairs per chunk as fit in 227 KB next to the diagonal inverse and S
   int chunk = (int)((227 * 1024 / (INV_TILE * (long long)sizeof(double)) - 2) / 2);
   if (chunk > bd.D) chunk = bd.D;
