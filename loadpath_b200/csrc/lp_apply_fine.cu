@@ -278,27 +278,6 @@ __device__ __forceinline__ void store4(double* p, const double (&o)[4]) {
   *reinterpret_cast<double2*>(p + 2) = make_double2(o[2], o[3]);
 }
 
-// The work of a launch: units (tile, chunk), tile-major (tile = x tile + gx * y tile), block b
-// taking units [b U / B, (b + 1) U / B), so every block has the same number of chunks. A run of
-// consecutive chunks [cb, ce) of one tile is a segment; it loads one halo chunk below cb (its top
-// cell starts the z carry) and the chunk above ce - 1 (the upper plane of the last cell).
-struct FineSeg {
-  int tile, cb, ce;
-  int cstart, nload, nproc;   // loads from chunk cstart, nload of them; chunks processed
-};
-
-__device__ __forceinline__ FineSeg fine_seg(long long u, long long u1, int nchunks) {
-  FineSeg s;
-  s.tile = (int)(u / nchunks);
-  s.cb = (int)(u - (long long)s.tile * nchunks);
-  const long long left = u1 - u;
-  s.ce = left < (long long)(nchunks - s.cb) ? s.cb + (int)left : nchunks;
-  s.cstart = s.cb > 0 ? s.cb - 1 : 0;
-  s.nload = min(s.ce + 1, nchunks) - s.cstart;
-  s.nproc = s.ce - s.cstart;
-  return s;
-}
-
 // Persistent blocks, one barrier per chunk: each thread waits for its stages, forms its two pairs
 // of cells, publishes its y shares into the exchange buffer of the chunk's parity, and the block
 // meets once (which also settles a wait that gave up); the owners then add their -y neighbour's
@@ -365,11 +344,11 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
   // the producer (thread 0) walks the block's loads: its segment, the loads issued in it and in all
   int total = 0;
   long long pu = u0;
-  FineSeg ps = fine_seg(u0, u1, nchunks);
-  int pk = 0, issued = 0;
+  LpSeg ps = lp_seg(u0, u1, nchunks);
+  int pk = 0, issued = 0, pst = 0;   // (pst: the stage of the next load issued)
   if (tid == 0) {
     for (long long u = u0; u < u1;) {
-      const FineSeg q = fine_seg(u, u1, nchunks);
+      const LpSeg q = lp_seg(u, u1, nchunks);
       total += q.nload;
       u += q.ce - q.cb;
     }
@@ -380,10 +359,11 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
   auto issue_next = [&]() {
     if (pk == ps.nload) {
       pu += ps.ce - ps.cb;
-      ps = fine_seg(pu, u1, nchunks);
+      ps = lp_seg(pu, u1, nchunks);
       pk = 0;
     }
-    const int s = issued % NST;
+    const int s = pst;
+    pst = pst + 1 == NST ? 0 : pst + 1;
     const int x0 = (ps.tile % gx) * (TXC - 1), y0 = (ps.tile / gx) * (TYC - 1);
     lp_mbar_expect_tx(&sm.full[s], UBYTES + EBYTES);
     lp_tma_load_4d(sm.u[s].v, &maps.u, 4 * (x0 - 1), y0 - 1, ps.cstart + pk, 0, &sm.full[s]);
@@ -396,9 +376,17 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
   double pacc = 0.0;
   bool ok = true, failed = false;
   int n = 0;    // the block's load in hand (the chunk processed)
+  int sn = 0;   // its stage, n % NST, and the parity of its phase, (n / NST) & 1, kept as they advance
+  uint32_t pn = 0;
+  auto advance = [](int& s, uint32_t& p) {
+    if (++s == NST) {
+      s = 0;
+      p ^= 1u;
+    }
+  };
   int it = 0;   // chunks processed: the exchange buffer alternates with it
   for (long long u = u0; u < u1 && !failed;) {
-    const FineSeg sg = fine_seg(u, u1, nchunks);
+    const LpSeg sg = lp_seg(u, u1, nchunks);
     u += sg.ce - sg.cb;
     const int x0 = (sg.tile % gx) * (TXC - 1), y0 = (sg.tile / gx) * (TYC - 1);
     const int nx_ = x0 - 1 + i, ny_ = y0 - 1 + j;
@@ -411,19 +399,22 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
       for (int c = 0; c < 3; ++c) carry[q][c] = T(0);
     // modes of planes (0, 1) of the chunk in hand, formed by the iteration before
     P m01[4][3];
-    ok = ok && lp_mbar_wait(&sm.full[n % NST], (n / NST) & 1);
-    plane_modes<T>(sm, n % NST, i, j, 0, m01);
-    for (int k = 0; k < sg.nproc; ++k, ++n, ++it) {
+    ok = ok && lp_mbar_wait(&sm.full[sn], pn);
+    plane_modes<T>(sm, sn, i, j, 0, m01);
+    for (int k = 0; k < sg.nproc; ++k, ++n, ++it, advance(sn, pn)) {
       const int c = sg.cstart + k;
       const bool halo = c < sg.cb;
-      const int s = n % NST;
+      const int s = sn;
+      int s1 = sn;   // stage and phase of load n + 1
+      uint32_t p1 = pn;
+      advance(s1, p1);
       // the stages refilled here were last read before the previous chunk's barrier
       if (tid == 0)
         while (issued < n + NST && issued < total) issue_next();
       const uint32_t mb4 = (writer && !halo) ? __ldg(reinterpret_cast<const uint32_t*>(mask + obase + c * zcs)) : 0u;
-      ok = ok && lp_mbar_wait(&sm.full[s], (n / NST) & 1);
+      ok = ok && lp_mbar_wait(&sm.full[s], pn);
       const bool has_next = k + 1 < sg.nload;
-      if (has_next) ok = ok && lp_mbar_wait(&sm.full[(n + 1) % NST], ((n + 1) / NST) & 1);
+      if (has_next) ok = ok && lp_mbar_wait(&sm.full[s1], p1);
       // a wait that gave up leaves stale but in-bounds data; the barrier below then stops the block
       const T* ecol = &sm.e[s].v[(j * TXC + i) * 4];
       P m23[4][3];
@@ -452,7 +443,7 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
       }
       // the next chunk's planes (0, 1), kept for the next iteration
       if (has_next) {
-        plane_modes<T>(sm, (n + 1) % NST, i, j, 0, m01);
+        plane_modes<T>(sm, s1, i, j, 0, m01);
       } else {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -510,7 +501,10 @@ k_apply_fine(const __grid_constant__ FineMaps maps, T* __restrict__ out, const u
       }
     }
     // the segment's last load (the chunk above) was only read as the next chunk's planes
-    if (!failed && sg.nload > sg.nproc) ++n;
+    if (!failed && sg.nload > sg.nproc) {
+      ++n;
+      advance(sn, pn);
+    }
   }
   if (dotp) {
     __shared__ double sh[32];

@@ -141,6 +141,27 @@ static inline LpBand lp_band(int NX, int NY, int NZ) {
   return b;
 }
 
+// The work of a launch: units (tile, chunk), tile-major (tile = x tile + gx * y tile), block b
+// taking units [b U / B, (b + 1) U / B), so every block has the same number of chunks. A run of
+// consecutive chunks [cb, ce) of one tile is a segment; it loads one halo chunk below cb (its top
+// cell starts the z carry) and the chunk above ce - 1 (the upper plane of the last cell).
+struct LpSeg {
+  int tile, cb, ce;
+  int cstart, nload, nproc;   // loads from chunk cstart, nload of them; chunks processed
+};
+
+__device__ __forceinline__ LpSeg lp_seg(long long u, long long u1, int nchunks) {
+  LpSeg s;
+  s.tile = (int)(u / nchunks);
+  s.cb = (int)(u - (long long)s.tile * nchunks);
+  const long long left = u1 - u;
+  s.ce = left < (long long)(nchunks - s.cb) ? s.cb + (int)left : nchunks;
+  s.cstart = s.cb > 0 ? s.cb - 1 : 0;
+  s.nload = min(s.ce + 1, nchunks) - s.cstart;
+  s.nproc = s.ce - s.cstart;
+  return s;
+}
+
 #define LP_LAUNCH_CHECK()                                   \
   do {                                                      \
     cudaError_t _e = cudaGetLastError();                    \
