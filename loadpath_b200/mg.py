@@ -366,6 +366,14 @@ class GridElasticity:
         self._ev_pw_fork = torch.cuda.Event()
         self._ev_pw_join = torch.cuda.Event()
         self._part_pw = torch.zeros(lib().lpb_reduce_blocks() * 2, dtype=torch.float64, device=self.device)
+        # the fine two levels' power iterations: on the working stream, or (a planned rebuild) on a
+        # stream of their own as soon as level 1 is built, beside the coarser levels' Galerkin
+        # products; their own reduction scratch either way
+        self._pw01_stream = torch.cuda.Stream(device=self.device)
+        self._ev_pw01_fork = torch.cuda.Event()
+        self._ev_pw01_join = torch.cuda.Event()
+        self._part_pw01 = torch.zeros(lib().lpb_reduce_blocks() * 2, dtype=torch.float64, device=self.device)
+        self._pw01_early = False
         self._joined = True
 
     # --- layout conversion (loadpath/mg.py:495-511) -----------------------------------
@@ -447,6 +455,10 @@ class GridElasticity:
         dt = self.tdtype
         chk = self._chk
         part = self._part
+        # power iterations launched early by a build before this one are done before anything of
+        # this one is written
+        torch.cuda.current_stream().wait_event(self._ev_pw01_join)
+        self._pw01_early = False
         if plan is None:
             self._gen += 1       # captured graphs may hold launch parameters of the last structure
         l0 = DevLevel("scaled", g0, torch.float64)
@@ -519,6 +531,10 @@ class GridElasticity:
             counts.append(None if plan else int(chk[depth].item()))
             levels.append(coarse)
             fine = coarse
+            if plan is not None and depth == 1:
+                self.levels = levels
+                self._l0s = l0s
+                self._lmax_fine_early(plan["depth"] + 1)
         self.levels = levels
         self._l0s = l0s
         info = self._build_coarse(levels[-1])
@@ -775,24 +791,46 @@ class GridElasticity:
         L.lpb_cheb_coef(self._coef[16 * i:].data_ptr(), pw.data_ptr(), pw[16:].data_ptr(), its,
                         max(self.degree, 1), LMAX_SAFETY, st)
 
+    def _run_lmax(self, i, nl, part):
+        if self.use_graphs:
+            self._replay(self._graph(("lmax", i, nl), lambda: self._estimate_lmax(i, part=part)))
+        else:
+            self._estimate_lmax(i, part=part)
+
+    def _lmax_fine_early(self, nl):
+        """A planned rebuild (the level count known): levels 0 and 1's power iterations on their
+        own stream as soon as level 1 is built, beside the Galerkin products of the coarser levels
+        and the coarsest factorisation; _all_lmax joins them."""
+        for i in range(2):
+            self._op(i).coef = self._coef[16 * i:16 * (i + 1)]
+            self._lmax_vectors(i)
+        self._ev_pw01_fork.record()
+        with torch.cuda.stream(self._pw01_stream):
+            self._pw01_stream.wait_event(self._ev_pw01_fork)
+            for i in range(2):
+                self._run_lmax(i, nl, self._part_pw01)
+            self._ev_pw01_join.record()
+        self._pw01_early = True
+
     def _all_lmax(self, nl):
         """λmax of every level. The levels are independent: the fine two run on the working
-        stream, the coarse ones (chains of small kernels) on a stream of their own beside them;
-        with graphs on, each level's twelve iterations are one graph launch."""
+        stream (or already run on their own, _lmax_fine_early), the coarse ones (chains of small
+        kernels) on a stream of their own beside them; with graphs on, each level's twelve
+        iterations are one graph launch."""
         for i in range(nl):
             self._op(i).coef = self._coef[16 * i:16 * (i + 1)]
             self._lmax_vectors(i)
 
         def run(i, part):
-            if self.use_graphs:
-                self._replay(self._graph(("lmax", i, nl), lambda: self._estimate_lmax(i, part=part)))
-            else:
-                self._estimate_lmax(i, part=part)
+            self._run_lmax(i, nl, part)
 
         if nl > 2:
             self._ev_pw_fork.record()
-        for i in range(min(nl, 2)):
-            run(i, self._part)
+        if self._pw01_early:
+            torch.cuda.current_stream().wait_event(self._ev_pw01_join)
+        else:
+            for i in range(min(nl, 2)):
+                run(i, self._part_pw01)
         if nl > 2:
             with torch.cuda.stream(self._pw_stream):
                 self._pw_stream.wait_event(self._ev_pw_fork)
