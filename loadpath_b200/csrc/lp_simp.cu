@@ -18,37 +18,103 @@ namespace {
 //   mode 0: out = H v
 //   mode 1: out = H (v / hs_in)
 //   mode 2: out = (H v) / hs_out ; e_out = emin + out^p (1 - emin) if e_out != null
-__global__ void k_filter(double* __restrict__ out, const double* __restrict__ v, const int* __restrict__ toff,
-                         const double* __restrict__ tw, int ntaps, const double* __restrict__ hs_in,
-                         const double* __restrict__ hs_out, double* __restrict__ e_out, double penal, double emin,
-                         LpGrid g) {
+// A block takes a tile of 32 x 8 cell columns times one z chunk (4 cells): it stages the tile with
+// its halo of reach R (the largest |offset| of the taps, up to LP_FT_R) in shared memory, v / hs_in
+// formed once per staged cell and zeros outside the grid, and each thread sums the taps for the 4
+// cells of its column in the taps' order, so the sums are those of a gather cell by cell. The
+// staging reads whole rows of chunks (32-byte sectors, contiguous along x). Taps reaching further
+// than LP_FT_R are gathered from global memory instead, cell by cell.
+#define LP_FT_X 32
+#define LP_FT_Y 8
+#define LP_FT_R 2
+__global__ void __launch_bounds__(256) k_filter(double* __restrict__ out, const double* __restrict__ v,
+                                                const int* __restrict__ toff, const double* __restrict__ tw,
+                                                int ntaps, const double* __restrict__ hs_in,
+                                                const double* __restrict__ hs_out, double* __restrict__ e_out,
+                                                double penal, double emin, LpGrid g) {
   extern __shared__ unsigned char smem_raw[];
+  __shared__ double tile[(4 + 2 * LP_FT_R) * (LP_FT_Y + 2 * LP_FT_R) * (LP_FT_X + 2 * LP_FT_R)];
+  __shared__ int s_reach;
   int* so = reinterpret_cast<int*>(smem_raw);
   double* sw = reinterpret_cast<double*>(smem_raw + ((3 * ntaps * sizeof(int) + 15) & ~15));
+  if (threadIdx.x == 0) s_reach = 0;
+  __syncthreads();
+  int reach = 0;
   for (int i = threadIdx.x; i < ntaps; i += blockDim.x) {
-    so[3 * i] = toff[3 * i];
-    so[3 * i + 1] = toff[3 * i + 1];
-    so[3 * i + 2] = toff[3 * i + 2];
+    const int dx = toff[3 * i], dy = toff[3 * i + 1], dz = toff[3 * i + 2];
+    so[3 * i] = dx;
+    so[3 * i + 1] = dy;
+    so[3 * i + 2] = dz;
     sw[i] = tw[i];
+    reach = max(reach, max(abs(dx), max(abs(dy), abs(dz))));
+  }
+  if (reach) atomicMax(&s_reach, reach);
+  __syncthreads();
+  const int R = s_reach;
+  const int nbx = (g.nx + LP_FT_X - 1) / LP_FT_X, nby = (g.ny + LP_FT_Y - 1) / LP_FT_Y;
+  const int bx = (int)(blockIdx.x % nbx), rest = (int)(blockIdx.x / nbx);
+  const int by = rest % nby, cz = rest / nby;
+  const int x0 = bx * LP_FT_X, y0 = by * LP_FT_Y;
+  const int x = x0 + (int)(threadIdx.x & 31), y = y0 + (int)(threadIdx.x >> 5);
+  const bool own = x < g.nx && y < g.ny;
+  if (R > LP_FT_R) {
+    if (!own) return;
+    for (int zq = 0; zq < 4; ++zq) {
+      const int z = 4 * cz + zq;
+      if (z >= g.nz) break;
+      double acc = 0.0;
+      for (int i = 0; i < ntaps; ++i) {
+        const int xx = x + so[3 * i], yy = y + so[3 * i + 1], zz = z + so[3 * i + 2];
+        if (xx < 0 || yy < 0 || zz < 0 || xx >= g.nx || yy >= g.ny || zz >= g.nz) continue;
+        const long long c = g.cell(xx, yy, zz);
+        double vi = v[c];
+        if (hs_in) vi = vi / hs_in[c];
+        acc += sw[i] * vi;
+      }
+      const long long c = g.cell(x, y, z);
+      if (hs_out) acc = acc / hs_out[c];
+      out[c] = acc;
+      if (e_out) e_out[c] = emin + pow(acc, penal) * (1.0 - emin);
+    }
+    return;
+  }
+  const int XH = LP_FT_X + 2 * R, YH = LP_FT_Y + 2 * R, ZH = 4 + 2 * R, P = XH * YH;
+  const int CR = (R + 3) / 4;  // halo chunks on each side
+  const int rowlen = 4 * XH, nitems = (2 * CR + 1) * YH * rowlen;
+  for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
+    const int row = i / rowlen, j = i - row * rowlen;
+    const int cr = row / YH, yl = row - cr * YH;
+    const int xl = j >> 2, gz = 4 * (cz - CR + cr) + (j & 3);
+    const int zl = gz - (4 * cz - R);
+    if (zl < 0 || zl >= ZH) continue;
+    const int gx = x0 - R + xl, gy = y0 - R + yl;
+    double val = 0.0;
+    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) {
+      const long long c = g.cell(gx, gy, gz);
+      val = v[c];
+      if (hs_in) val = val / hs_in[c];
+    }
+    tile[(zl * YH + yl) * XH + xl] = val;
   }
   __syncthreads();
-  const long long total = g.cells_padded();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int x, y, z;
-    if (!g.cell_at(t, x, y, z)) continue;
-    double s = 0.0;
-    for (int i = 0; i < ntaps; ++i) {
-      int xx = x + so[3 * i], yy = y + so[3 * i + 1], zz = z + so[3 * i + 2];
-      if (xx < 0 || yy < 0 || zz < 0 || xx >= g.nx || yy >= g.ny || zz >= g.nz) continue;
-      long long c = g.cell(xx, yy, zz);
-      double vi = v[c];
-      if (hs_in) vi = vi / hs_in[c];
-      s += sw[i] * vi;
-    }
-    long long c = g.cell(x, y, z);
-    if (hs_out) s = s / hs_out[c];
-    out[c] = s;
-    if (e_out) e_out[c] = emin + pow(s, penal) * (1.0 - emin);
+  if (!own) return;
+  const int ctr = (R * YH + R + (int)(threadIdx.x >> 5)) * XH + R + (int)(threadIdx.x & 31);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = 0; i < ntaps; ++i) {
+    const int o = ctr + (so[3 * i + 2] * YH + so[3 * i + 1]) * XH + so[3 * i];
+    const double w = sw[i];
+#pragma unroll
+    for (int zq = 0; zq < 4; ++zq) acc[zq] += w * tile[o + zq * P];
+  }
+#pragma unroll
+  for (int zq = 0; zq < 4; ++zq) {
+    const int z = 4 * cz + zq;
+    if (z >= g.nz) break;
+    const long long c = g.cell(x, y, z);
+    double r = acc[zq];
+    if (hs_out) r = r / hs_out[c];
+    out[c] = r;
+    if (e_out) e_out[c] = emin + pow(r, penal) * (1.0 - emin);
   }
 }
 
@@ -166,11 +232,25 @@ __global__ void k_sensitivity(double* __restrict__ dc, const double* __restrict_
 // weighs a cell's share of the filtered volume. The step is formed as
 // (x sqrt(-dc / dv)) / sqrt(lambda_j): one square root per cell; only the volume comparisons use
 // it, the accepted step is recomputed with the reference's expression by k_oc_apply.
+//
+// The kernel is bound by latency and instruction issue, not by DRAM (32 bytes per cell): each
+// thread loads its next cell's four values before working on the current one, the clip is two
+// compare-and-selects (fmin / fmax on doubles take several instructions more; the selects give
+// the same values, a NaN step clipping to the upper bound as fmin does), and the 1 / sqrt(lambda_j)
+// are read from shared memory at each use (volatile loads, so that they take no registers: 114
+// registers, two blocks per SM). The padding of the cell z pitch lies in the z chunks from nz / 4
+// up, so comparisons of t with those chunks' starts stand for the division of LpGrid::cell_at.
+__device__ __forceinline__ double lds_volatile_f64(const double* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
+
 template <int NL>
-__global__ void __launch_bounds__(256) k_oc_volumes(const double* __restrict__ x, const double* __restrict__ dc,
-                                                    const double* __restrict__ dv, const double* __restrict__ gv,
-                                                    const double* __restrict__ lam, double move, LpGrid g,
-                                                    double* __restrict__ part) {
+__global__ void __launch_bounds__(256, 2) k_oc_volumes(const double* __restrict__ x, const double* __restrict__ dc,
+                                                       const double* __restrict__ dv, const double* __restrict__ gv,
+                                                       const double* __restrict__ lam, double move, LpGrid g,
+                                                       double* __restrict__ part) {
   __shared__ double s_isl[NL];
   __shared__ double sacc[NL][8];
   if (threadIdx.x < NL) s_isl[threadIdx.x] = 1.0 / sqrt(lam[threadIdx.x]);
@@ -179,15 +259,29 @@ __global__ void __launch_bounds__(256) k_oc_volumes(const double* __restrict__ x
 #pragma unroll
   for (int j = 0; j < NL; ++j) acc[j] = 0.0;
   const long long total = g.cells_padded();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-    int x_, y_, z;
-    if (!g.cell_at(t, x_, y_, z)) continue;
-    const long long c = t;
-    double xv = x[c], gw = gv[c];
-    double ts = xv * sqrt(-dc[c] / dv[c]);
-    double lo = fmax(0.0, xv - move), hi = fmin(1.0, xv + move);
+  // chunks below nz / 4 hold cells only; chunk nz / 4 holds nz % 4 cells at its start, the chunks
+  // above it padding only
+  const long long pad_from = (long long)(g.nz >> 2) * g.cell_zc_stride();
+  const long long pad_all = pad_from + g.cell_zc_stride();
+  const int zr = g.nz & 3;
+  const long long step = (long long)gridDim.x * blockDim.x;
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double nx_ = 0.0, ngw = 0.0, ndc = -1.0, ndv = 1.0;
+  if (t < total) { nx_ = x[t]; ngw = gv[t]; ndc = dc[t]; ndv = dv[t]; }
+  for (; t < total; t += step) {
+    const double xv = nx_, gw = ngw, dcv = ndc, dvv = ndv;
+    const long long tn = t + step;
+    if (tn < total) { nx_ = x[tn]; ngw = gv[tn]; ndc = dc[tn]; ndv = dv[tn]; }
+    if (t >= pad_from && (t >= pad_all || (int)(t & 3) >= zr)) continue;
+    const double ts = xv * sqrt(-dcv / dvv);
+    const double lo = fmax(0.0, xv - move), hi = fmin(1.0, xv + move);
 #pragma unroll
-    for (int j = 0; j < NL; ++j) acc[j] += fmax(lo, fmin(hi, ts * s_isl[j])) * gw;
+    for (int j = 0; j < NL; ++j) {
+      const double p = ts * lds_volatile_f64(&s_isl[j]);
+      double v = p < hi ? p : hi;
+      v = v > lo ? v : lo;
+      acc[j] += v * gw;
+    }
   }
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -453,8 +547,10 @@ int lpb_filter(double* out, const double* v, const int* toff, const double* tw, 
   if (!lp_grid_ok(g) || !out || !v || !toff || !tw || ntaps < 1 || ntaps > LP_MAX_TAPS) return LP_ERR_ARG;
   if (out == v) return LP_ERR_ARG;
   size_t smem = ((3 * ntaps * sizeof(int) + 15) & ~(size_t)15) + ntaps * sizeof(double);
-  long long total = g.cells_padded();
-  k_filter<<<lp_blocks(total, 256), 256, smem, LP_ST>>>(out, v, toff, tw, ntaps, hs_in, hs_out, e_out, penal, emin, g);
+  const long long tiles = (long long)((g.nx + LP_FT_X - 1) / LP_FT_X) * ((g.ny + LP_FT_Y - 1) / LP_FT_Y) *
+                          ((g.nz + 3) / 4);
+  if (tiles > 2147483647LL) return LP_ERR_ARG;
+  k_filter<<<(unsigned)tiles, 256, smem, LP_ST>>>(out, v, toff, tw, ntaps, hs_in, hs_out, e_out, penal, emin, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }
