@@ -126,6 +126,8 @@ int lpb_diag_explicit_f64(double* d, const double* k, int nx, int ny, int nz, in
 int lpb_masks(uint8_t* mask, double* dinv64, float* dinv32, const double* d, const uint8_t* held_bits, const float* kept, int nx, int ny, int nz, int pz, int cpz, double alive_thr, double live_thr, const double* thr_scale, void* stream);
 /* *out = max(a[0:n]); part: >= 1024 doubles of scratch (loadpath/mg.py:560) */
 int lpb_max_f64(const double* a, long long n, double* part, double* out, void* stream);
+/* max |a - b| over n doubles (the SIMP loop's design change, loadpath/simp.py:2379) */
+int lpb_max_abs_diff_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream);
 /* counts into a device float64 scalar (exact), part: >= 592 doubles of scratch. Cells with
  * modulus > 0 (loadpath/mg.py:559), active cells of a level-1 (weights) or explicit level
  * (loadpath/mg.py:593-599: _active_cells), and positions where two byte arrays differ (the
@@ -287,8 +289,9 @@ int lpb_project(double* xp, double* dxp, const double* xt, double beta, double e
 /* xn = clip(x sqrt(-dc / dv) / sqrt(lm), max(0, x - move), min(1, x + move)), held cells 1 / 0
  * (loadpath/simp.py:2314-2318, the optimality-criteria step at one volume multiplier) */
 int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* dv, double lm, double move, const uint8_t* flags, int nx, int ny, int nz, int pz, int cpz, void* stream);
-/* out = a * b (b NULL: a), 0 on held cells, then min(out, 0) when clip0: the products the filter
- * chain rule feeds to H^T (loadpath/simp.py:2001, :2077, :2191) */
+/* out = a * b (b NULL: a), 0 on held cells, then min(out, 0) (clip0 1) or max(out, 1e-12) (clip0 2):
+ * the products the filter chain rule feeds to H^T and its clips (loadpath/simp.py:2001, :2077, :2191,
+ * :2204) */
 int lpb_cell_product(double* out, const double* a, const double* b, const uint8_t* flags, int clip0, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
 /* ---- CUDA graphs of a stream's work (the solver records one CG iteration per solve) */

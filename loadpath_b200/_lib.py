@@ -25,7 +25,7 @@ _CTYPES = {
 }
 _STATUS = {-1: "bad arguments", -2: "kernel launch failed", -3: "size beyond the kernel's limit"}
 # kernels each entry point launches (1 when not listed; 0 for host-only entries)
-_KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_max_f64": 2, "lpb_dot_f64": 2,
+_KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_max_f64": 2, "lpb_max_abs_diff_f64": 2, "lpb_dot_f64": 2,
             "lpb_dot_f32": 2, "lpb_dot_f64_f32": 2, "lpb_cg_step": 2, "lpb_cg_step_r": 2, "lpb_apply_fine_dot_f64": 2, "lpb_oc_volumes": 2, "lpb_oc_apply": 2, "lpb_oc_apply_at": 2, "lpb_oc_walk_init": 2,
             "lpb_band_dims": 0, "lpb_band_inverse": 2, "lpb_band_solve_f32": 2, "lpb_band_solve_f64": 2,
             "lpb_count_positive_f64": 2, "lpb_count_active_weights_f32": 2, "lpb_count_active_weights_f64": 2,

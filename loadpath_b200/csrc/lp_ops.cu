@@ -240,6 +240,22 @@ __global__ void k_masks(uint8_t* __restrict__ mask, double* __restrict__ dinv64,
 
 // max of a float64 array (one block per slice; partials then a final pass on the host side
 // of the caller, which reads back one value per block)
+__global__ void k_max_abs_diff_partial(const double* __restrict__ a, const double* __restrict__ b, long long n,
+                                       double* __restrict__ part) {
+  __shared__ double sh[32];
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(a[i] - b[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+  }
+}
+
 __global__ void k_max_partial(const double* __restrict__ a, long long n, double* __restrict__ part) {
   __shared__ double sh[32];
   double m = -1e308;
@@ -452,6 +468,17 @@ int lpb_max_f64(const double* a, long long n, double* part, double* out, void* s
   int blocks = lp_blocks(n, 256);
   if (blocks > 1024) blocks = 1024;
   k_max_partial<<<blocks, 256, 0, (cudaStream_t)stream>>>(a, n, part);
+  k_max_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, blocks, out);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// max |a - b| over n doubles into *out (device; 0 for n = 0); part: scratch of at least 1024 doubles
+int lpb_max_abs_diff_f64(const double* a, const double* b, long long n, double* part, double* out, void* stream) {
+  if (!a || !b || !part || !out || n < 0) return LP_ERR_ARG;
+  int blocks = lp_blocks(n, 256);
+  if (blocks > 1024) blocks = 1024;
+  k_max_abs_diff_partial<<<blocks, 256, 0, (cudaStream_t)stream>>>(a, b, n, part);
   k_max_final<<<1, 1024, 0, (cudaStream_t)stream>>>(part, blocks, out);
   LP_LAUNCH_CHECK();
   return LP_OK;

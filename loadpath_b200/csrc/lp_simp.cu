@@ -498,7 +498,8 @@ __global__ void k_cell_product(double* __restrict__ out, const double* __restric
     if (!g.cell_at(t, x_, y_, z)) continue;
     double v = b ? a[t] * b[t] : a[t];
     if (flags && (flags[t] & 3)) v = 0.0;
-    if (clip0) v = fmin(v, 0.0);
+    if (clip0 == 1) v = fmin(v, 0.0);
+    else if (clip0 == 2) v = fmax(v, 1e-12);
     out[t] = v;
   }
 }
@@ -679,11 +680,11 @@ int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* 
   return LP_OK;
 }
 
-// out = a * b (b NULL: a), zero on flagged cells, then min(., 0) when clip0
+// out = a * b (b NULL: a), zero on flagged cells, then min(., 0) (clip0 1) or max(., 1e-12) (clip0 2)
 int lpb_cell_product(double* out, const double* a, const double* b, const uint8_t* flags, int clip0, LP_GRID_ARGS,
                      void* stream) {
   LpGrid g = LP_GRID;
-  if (!lp_grid_ok(g) || !out || !a) return LP_ERR_ARG;
+  if (!lp_grid_ok(g) || !out || !a || clip0 < 0 || clip0 > 2) return LP_ERR_ARG;
   k_cell_product<<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(out, a, b, flags, clip0, g);
   LP_LAUNCH_CHECK();
   return LP_OK;

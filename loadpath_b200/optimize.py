@@ -1,4 +1,13 @@
-"""SIMP with the MMA update and a penalty continuation, its sensitivities from the autograd path.
+"""The SIMP loops over the device pieces.
+
+`OptimizeLoop`: loadpath's own SIMP loop (loadpath/simp.py:1640-2455, `simp.optimize` /
+`_optimize_run`) for a plain compliance problem: blueprint and eroded projections of the filtered
+design, the SIMP law on the eroded one, MG-PCG solves, sensitivities carried back through the
+eroded projection and the filter, the volume's through the blueprint's, the measured step length,
+the optimality-criteria step whose volume multiplier is solved to rounding, beta continuation and
+the stopping rules. Described in its docstring.
+
+`MMALoop`: SIMP with the MMA update and a penalty continuation, its sensitivities from the autograd path.
 
 Each iteration: the penalty p_k = p0 + (p - p0) min(k, ramp) / ramp; compliance c(x) through
 `autograd.Compliance` (filter, SIMP law, MG-PCG) and its gradient from the backward (element
@@ -13,15 +22,60 @@ The design lives in grid order (nx, ny, nz) as a float64 CUDA tensor; every n-si
 """
 from __future__ import annotations
 
+import math
+import os
+from dataclasses import dataclass
+
 import numpy as np
 import torch
 
 from ._lib import lib
 from .autograd import Compliance, SimpProblem
-from .grid import stream_handle
+from .grid import ptr, stream_handle
+from .mg import BoxMesh, GridElasticity
 from .mma import MMA
+from .simp import DeviceFilter, LiveCells, ProjectedDesign, _cells_touching
 
-__all__ = ["MMALoop"]
+__all__ = ["MMALoop", "OptimizeLoop", "SimpOptions", "E_MIN", "PENALTY"]
+
+E_MIN = 1e-6          # void modulus of loadpath's SIMP loop (loadpath/simp.py:42)
+PENALTY = 3.0         # SIMP exponent (loadpath/simp.py:55)
+STEP_SHRINK = 0.5     # the measured step's limits per iteration (loadpath/simp.py:1239-1240)
+STEP_GROW = 1.2
+
+
+@dataclass
+class SimpOptions:
+    """The options of loadpath's SIMP loop that `OptimizeLoop` runs, with the reference's names,
+    meanings and defaults (loadpath/simp.py:899-1000). Options of terms this package does not run
+    (build direction, access, extrusion, pattern, mirror, heat, buckling and the rest) are not
+    listed; the delivered part's post-processing (opening, pruning) is not part of the loop."""
+    volume_fraction: float
+    filter_radius: float
+    max_iterations: int = 120
+    beta_max: float = 32.0
+    beta_every: int = 10
+    beta_schedule: tuple | None = None
+    move: float = 0.2
+    adaptive_move: bool = True
+    tol: float = 0.01
+    solve_rtol: float = 1e-4
+    adaptive_rtol: bool = False
+    stall_rtol: float = 2e-3
+    stall_window: int = 6
+    stiffness_bound: bool = False
+    eta: float = 0.5
+    erode: float = 0.15
+    beta_start: float = 1.0
+    pad_filter: bool | None = None
+    x0: np.ndarray | None = None
+
+
+def beta_hold(opts: SimpOptions, beta: float) -> int:
+    """Most iterations at projection sharpness beta (loadpath/simp.py:1436-1440)."""
+    s = opts.beta_schedule
+    k = int(round(math.log2(max(beta, 1.0))))
+    return s[k] if s is not None and k < len(s) else opts.beta_every
 
 
 class MMALoop:
@@ -89,3 +143,236 @@ class MMALoop:
     def xphys_host(self):
         """The last forward's filtered design (grid order)."""
         return self.problem.grid.cells_to_host(self.problem.xphys)
+
+
+class OptimizeLoop:
+    """loadpath's SIMP loop (loadpath/simp.py:1640-2455) on the device, for compliance under one or
+    more weighted load cases at a volume fraction, with passive solid / void cells.
+
+    Per iteration, as the reference's loop body: the blueprint xp = P(H x / hs, beta, eta) and the
+    eroded xe = P(H x / hs, beta, eta + erode) (`physical`, `eroded`, :1775-1814); moduli
+    E = E_MIN + xe^3 (1 - E_MIN); one MG-PCG solve per case, warm-started from the last one, on the
+    cells the reference's analysis solves (`_Analysis`, :114-330: when fewer than 80 % of the cells
+    are alive only the alive cells connected to a support, `LiveCells`); compliance sum_k w_k f_k.u_k;
+    dc = min(H^T(dc_xe P'(xt, eta + erode) / hs), 0) and dv = max(H^T(w P'(xt, eta) / hs), 1e-12)
+    (:1994-2204); the move limit measured from the slope of the Lagrangian along the last step
+    (:2229-2243) or the fixed schedule (move, then move / 2 past beta 4); the optimality-criteria
+    step with its volume multiplier bracketed in log space from the last one and found by
+    false position with the Illinois halving (`ProjectedDesign.oc_step`, :2249-2376); then beta
+    continuation and the stopping rules (:2418-2450). Every cell-sized pass runs on the device; the
+    host reads the loop's scalars, as the reference's loop does.
+
+    dims: cells (even); fixed_grid: bool (3, nx+1, ny+1, nz+1); loads: node-grid force arrays
+    (3, nx+1, ny+1, nz+1), one per case; preserve / void: bool cell grids or None; pitch: the cell
+    size (Ke and the filter scale with it as the reference's `_Analysis` and `density_filter` do);
+    dtype: the V-cycle's precision (the CG is float64)."""
+
+    def __init__(self, dims, fixed_grid, loads, nu, opts: SimpOptions, preserve=None, void=None,
+                 case_weights=None, pitch=1.0, element="im", dtype=np.float32, coarse_cells=2000,
+                 maxiter=2000, live_cells=True, device="cuda"):
+        dims = tuple(int(d) for d in dims)
+        if any(d % 2 for d in dims):
+            raise ValueError("the device SIMP loop takes even cell counts")
+        self.dims, self.opts, self.pitch = dims, opts, float(pitch)
+        self.mesh = BoxMesh(dims)
+        flat = np.asarray(fixed_grid, bool).reshape(3, -1)
+        fixed = np.empty(self.mesh.n_dof, bool)
+        for i in range(3):
+            fixed[i::3] = flat[i]
+        self.ge = GridElasticity(self.mesh, nu, fixed, rtol=opts.solve_rtol, maxiter=maxiter,
+                                 coarse_cells=coarse_cells, dtype=dtype, element=element, device=device)
+        g = self.ge.g0
+        self.grid = g
+        pad = True if opts.pad_filter is None else bool(opts.pad_filter)
+        self.filter = DeviceFilter(g, opts.filter_radius, self.pitch, pad=pad)
+        pres = np.zeros(dims, bool) if preserve is None else np.asarray(preserve, bool)
+        vd = np.zeros(dims, bool) if void is None else np.asarray(void, bool)
+        design = ~pres
+        if not design.any():
+            raise ValueError("nothing to optimize: every cell is preserved")
+        self.n_design = int(design.sum())
+        flags = (pres & ~vd).astype(np.uint8) | (vd.astype(np.uint8) << 1)
+        self.flags = g.set_cells(g.cell_field(torch.uint8), torch.from_numpy(flags))
+        self.w = g.cells_to_dev(design.astype(np.float64), torch.float64)
+        self.pd = ProjectedDesign(self.filter, w=self.w, flags=self.flags)
+        self.target = float(opts.volume_fraction) * float(design.sum())
+        x = np.full(dims, float(opts.volume_fraction))
+        if opts.x0 is not None:
+            x = np.clip(np.asarray(opts.x0, np.float64).reshape(dims), 0.0, 1.0)
+        x[pres] = 1.0
+        x[vd] = 0.0
+        self.x = g.cells_to_dev(x, torch.float64)
+        cases = list(loads) if isinstance(loads, (list, tuple)) else [loads]
+        self.fs = [g.nodes_to_dev(np.asarray(f, np.float64), torch.float64) for f in cases]
+        self.weights = [1.0] * len(cases) if case_weights is None else [float(c) for c in case_weights]
+        self.us = [None] * len(cases)
+        self.live = None
+        if live_cells:
+            held = np.asarray(fixed_grid, bool).reshape(g.node_shape).any(axis=0)
+            loaded = np.zeros(g.node_shape[1:], bool)
+            for f in cases:
+                loaded |= (np.asarray(f).reshape(g.node_shape) != 0).any(axis=0)
+            self.live = LiveCells(g, _cells_touching(held), _cells_touching(held | loaded) | pres)
+        cf = lambda: g.cell_field(torch.float64)   # noqa: E731
+        self.xp, self.dproj, self.xe, self.dproj_e, self.e, self.ce = cf(), cf(), cf(), cf(), cf(), cf()
+        self.dc_xe, self.dc, self.dv, self.dx, self.gp, self._tmp = cf(), cf(), cf(), cf(), cf(), cf()
+        self._part = torch.zeros(4096, dtype=torch.float64, device=g.device)
+        self._s = torch.zeros(8, dtype=torch.float64, device=g.device)
+        self.n = self.x.numel()
+        self.beta = float(opts.beta_start)
+        self.since_beta = 0
+        self.step_prev = None     # the last step's multiplier while dx / gp hold its step and gradient
+        self.move_k = float(opts.move)
+        self.lam_last = None
+        self.c0 = None
+        self.it = 0
+        self.history = []
+        self.converged = False
+        self.reduced = False
+        self.measured = bool(opts.adaptive_move)
+        self.scheduled = (self.measured and os.environ.get("LOADPATH_STOP", "hold") != "stall"
+                          and not opts.stiffness_bound)
+
+    # ---- device helpers ------------------------------------------------------------------------
+    def _dot(self, a, b):
+        lib().lpb_dot_f64(a.data_ptr(), b.data_ptr(), a.numel(), self._part.data_ptr(), self._s.data_ptr(),
+                          stream_handle())
+        return float(self._s[0].item())
+
+    def _axpby(self, out, a, x, b, y):
+        lib().lpb_axpby_f64(out.data_ptr(), float(a), x.data_ptr(), float(b), y.data_ptr(), out.numel(),
+                            stream_handle())
+        return out
+
+    def _solve(self, rtol):
+        """The cases' displacements on the moduli self.e (the reference's `_Analysis.solve`); returns
+        sum_k w_k f_k.u_k and leaves dc_xe = -sum_k w_k p xe^(p-1) (1 - E_MIN) ce_k / pitch."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        self.ge.rtol = rtol
+        self.reduced = False
+        if self.live is not None:
+            self.reduced = self.ge.set_moduli_live(self.e, self.live, self.xe, self.fs)
+        else:
+            self.ge.set_moduli_device(self.e)
+        try:
+            us = [self.ge.solve_device(f, u) for f, u in zip(self.fs, self.us)]
+        except RuntimeError:
+            if not self.reduced:
+                raise
+            # a reduced system the multigrid cannot hold: the full grid, void at E_MIN
+            # (loadpath/simp.py:815-822)
+            self.reduced = False
+            self.ge.set_moduli_device(self.e)
+            us = [self.ge.solve_device(f, None) for f in self.fs]
+        self.us = us
+        comp = 0.0
+        # K scales with the pitch (loadpath/simp.py:159): u, its energies and f.u by 1 / pitch
+        for k, (f, u, wk) in enumerate(zip(self.fs, us, self.weights)):
+            self.ge.strain_energy_device(u, out=self.ce)
+            L.lpb_sensitivity(self.dc_xe.data_ptr(), self.xe.data_ptr(), self.ce.data_ptr(), self.e.data_ptr(),
+                              PENALTY, E_MIN, wk / self.pitch, int(k > 0), self._part.data_ptr(), None, *g.args, st)
+            comp += wk * self._dot(f, u) / self.pitch
+        return comp
+
+    def step(self):
+        """One iteration; returns its record (the reference's keys)."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        o = self.opts
+        self.it += 1
+        beta = self.beta
+        eta, eta_e = o.eta, o.eta + o.erode
+        pd = self.pd
+        # blueprint (and its volume on the design cells) and eroded design, both from xt = H x / hs
+        vol_b = pd.physical(self.x, beta, eta, xp=self.xp, dxp=self.dproj)
+        L.lpb_project(self.xe.data_ptr(), self.dproj_e.data_ptr(), pd.xt.data_ptr(), beta, eta_e,
+                      self.flags.data_ptr(), None, None, None, *g.args, st)
+        L.lpb_simp_law(self.e.data_ptr(), self.xe.data_ptr(), PENALTY, E_MIN, *g.args, st)
+        rtol = o.solve_rtol * (10.0 if beta <= 2 else 3.0 if beta <= 8 else 1.0) if o.adaptive_rtol \
+            else o.solve_rtol
+        comp = self._solve(rtol)
+        if self.c0 is None:
+            self.c0 = comp
+        pd.chain(self.dc, self.dc_xe, self.dproj_e, clip=True)
+        pd.chain(self.dv, self.w, self.dproj)
+        L.lpb_cell_product(self.dv.data_ptr(), self.dv.data_ptr(), None, None, 2, *g.args, st)
+        sec = None
+        if self.measured:
+            if self.step_prev is not None:
+                a_s = self._dot(self.gp, self.dx)
+                b_s = self._dot(self._axpby(self._tmp, 1.0, self.dc, self.step_prev, self.dv), self.dx)
+                if a_s < 0:
+                    t_s = a_s / (a_s - b_s) if b_s > a_s else math.inf
+                    sec = t_s
+                    self.move_k = min(self.move_k * min(max(t_s, STEP_SHRINK), STEP_GROW), o.move)
+            move = self.move_k
+        else:
+            move = o.move if beta <= 4 else o.move / 2
+        pd.lam_last = self.lam_last
+        xn, lm, held = pd.oc_step(self.x, self.dc, self.dv, move, beta, eta, self.target)
+        self.lam_last = lm
+        L.lpb_max_abs_diff_f64(xn.data_ptr(), self.x.data_ptr(), self.n, self._part.data_ptr(),
+                               self._s[1:].data_ptr(), st)
+        change = float(self._s[1].item())
+        if self.measured:
+            self._axpby(self.dx, 1.0, xn, -1.0, self.x)
+            self._axpby(self.gp, 1.0, self.dc, lm, self.dv)
+            self.step_prev = lm
+        L.lpb_memcpy_async(self.x.data_ptr(), xn.data_ptr(), self.n * 8, st)
+        self.since_beta += 1
+        its = self.ge.last_iters
+        rec = {"iteration": self.it, "compliance": comp, "relative": comp / self.c0 if self.c0 else 1.0,
+               "volume": vol_b / self.n_design, "beta": beta, "change": change,
+               "cgIterations": max(its) if isinstance(its, (list, tuple)) else its,
+               "reduced": self.reduced, "volumeSolves": pd.n_eval}
+        if o.adaptive_move:
+            rec["move"] = move
+            if sec is not None:
+                rec["stepFit"] = float(min(sec, 99.0))
+        self.history.append(rec)
+        self._continue(change, move, comp, held)
+        return rec
+
+    def _continue(self, change, move, comp, held):
+        """beta continuation and the stopping rules (loadpath/simp.py:2418-2450)."""
+        o = self.opts
+        free_step = not self.measured or change < 0.999 * move
+        if self.beta < o.beta_max and ((change < o.tol * 2 and free_step)
+                                       or self.since_beta >= beta_hold(o, self.beta)):
+            self.beta = min(self.beta * 2, o.beta_max)
+            self.since_beta = 0
+            # twice as steep a projection: half as long a step
+            self.step_prev = None
+            self.move_k = self.move_k / 2
+        elif self.beta >= o.beta_max and self.it >= 3:
+            if change < o.tol and free_step:
+                self.converged = True
+                return
+            w = o.stall_window
+            if self.scheduled and held:
+                if self.since_beta >= beta_hold(o, self.beta):
+                    self.converged = True
+            elif self.since_beta >= w and len(self.history) > w:
+                old = self.history[-1 - w]["compliance"]
+                if abs(comp - old) <= o.stall_rtol * abs(old):
+                    self.converged = True
+
+    def run(self, on_iter=None):
+        """Iterate until a stopping rule holds or max_iterations; returns the history."""
+        while self.it < self.opts.max_iterations and not self.converged:
+            rec = self.step()
+            if on_iter is not None:
+                on_iter(rec)
+        return self.history
+
+    def xphys_host(self):
+        """The blueprint of the current design (grid order), as the loop delivers it before
+        post-processing (loadpath/simp.py:2454)."""
+        self.pd.physical(self.x, self.beta, self.opts.eta, xp=self._tmp)
+        return self.grid.cells_to_host(self._tmp)
+
+    def x_host(self):
+        return self.grid.cells_to_host(self.x)

@@ -910,6 +910,75 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
     return x, xphys, hist_c, hist_ch
 
 
+def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=None, pad=True, pitch=1.0,
+                  eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0):
+    """loadpath's own SIMP loop for one load case with its default options (loadpath/simp.py:
+    1640-2455): blueprint and eroded projections of xt = H x / hs (`physical`, `eroded`), the SIMP
+    law on the eroded design, the solve with the live-cell reduction (live_solve, the anchor cells
+    being those touching a support or the load and the pinned ones), dc = min(H (dc_xe P'_e / hs), 0),
+    dv = max(H (w P'_b / hs), 1e-12), the move limit measured from the Lagrangian's slope along
+    the last step (t = a / (a - b), the limit times t clipped to [0.5, 1.2], capped at move), the
+    step of oc_loadpath_step, and beta doubling after beta_every iterations or a free step of
+    change < 2 tol, halving the limit. Ke and the loads' work scale with the pitch. Returns the
+    per-iteration records (compliance, beta, change, move, volume, volumeSolves, xphys) and x."""
+    pres = np.zeros(dims, bool) if pres is None else np.asarray(pres, bool)
+    design = ~pres
+    w = design.astype(float)
+    taps = filter_taps(radius, pitch)
+    hs = np.full(dims, sum(t for _, t in taps)) if pad else filter_row_sums(dims, taps)
+    hap = lambda v: grid_filter(v, taps)   # noqa: E731
+    held = np.asarray(fixed_grid, bool).any(axis=0)
+    loaded = (np.asarray(f_grid) != 0).any(axis=0)
+    solve = live_solve(ke * pitch, fixed_grid, f_grid, cells_touching(held),
+                       cells_touching(held | loaded) | pres)
+    x = np.full(dims, volfrac)
+    x[pres] = 1.0
+    target = volfrac * float(w.sum())
+    beta, since_beta, move_k, lam_last, step_prev = 1.0, 0, move, None, None
+    recs = []
+    for _ in range(iters):
+        xt = hap(x) / hs
+        xp = project(xt, beta, eta)
+        xp[pres] = 1.0
+        xe = project(xt, beta, eta + erode)
+        xe[pres] = 1.0
+        e = emin + xe ** penal * (1 - emin)
+        u = solve(e, xe)
+        comp = float(np.sum(np.asarray(f_grid) * u))
+        g = gather_cells(u, dims).reshape(24, -1)
+        ce = np.einsum("in,in->n", g, (ke * pitch) @ g).reshape(dims)
+        dc_xe = -penal * xe ** (penal - 1) * (1 - emin) * ce
+        dpe = dproject(xt, beta, eta + erode)
+        dpe[pres] = 0.0
+        dpb = dproject(xt, beta, eta)
+        dpb[pres] = 0.0
+        dc = np.minimum(hap(dc_xe * dpe / hs), 0.0)
+        dv = np.maximum(hap(w * dpb / hs), 1e-12)
+        if step_prev is not None:
+            dxp, gp, lam_p = step_prev
+            a_s = float(np.sum(gp * dxp))
+            b_s = float(np.sum((dc + lam_p * dv) * dxp))
+            if a_s < 0:
+                t_s = a_s / (a_s - b_s) if b_s > a_s else np.inf
+                move_k = min(move_k * min(max(t_s, 0.5), 1.2), move)
+        mv = move_k
+        x_new, lm, n_eval, _ = oc_loadpath_step(x, dc, dv, mv, beta, eta, hap, hs, w, target, pres=pres,
+                                                lam_last=lam_last)
+        lam_last = lm
+        change = float(np.abs(x_new - x)[design].max())
+        step_prev = (x_new - x, dc + lm * dv, lm)
+        x = x_new
+        since_beta += 1
+        recs.append(dict(compliance=comp, beta=beta, change=change, move=mv, volume=float(xp[design].mean()),
+                         volumeSolves=n_eval, xphys=xp))
+        if beta < beta_max and ((change < 2 * tol and change < 0.999 * mv) or since_beta >= beta_every):
+            beta = min(2 * beta, beta_max)
+            since_beta = 0
+            step_prev = None
+            move_k = move_k / 2
+    return recs, x
+
+
 # --------------------------------------------------------------------------
 # MMA (loadpath/mma.py:31-214), restated from Svanberg's published method
 # --------------------------------------------------------------------------

@@ -4,7 +4,7 @@ Run in a container that has the loadpath source tree (read-only is fine):
 
     LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
 
-(names: element transfers femops filter mma hierarchies top3d config0 oc_step; default all but config0,
+(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize; default all but config0,
 which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
@@ -330,6 +330,57 @@ def make_oc_step():
     np.savez_compressed(os.path.join(HERE, "oc_step.npz"), **out)
 
 
+def make_optimize():
+    """loadpath's own SIMP loop as a whole (loadpath/simp.py:1640-2455, simp.optimize with its
+    default options: blueprint and eroded projections, the measured step length, beta
+    continuation, the volume multiplier solved to rounding) on two top3d cantilevers of its
+    benchmarks (domain_for: load and support cells pinned, padded filter), with the solves
+    tightened to rtol 1e-10 so that a solver of another kind can be compared iteration by
+    iteration. Stored per case: the domain on the node / cell grid (supports, load, pinned cells),
+    the options, and per iteration the record the loop reports and the blueprint density it
+    started from; and the last design."""
+    os.environ["LOADPATH_HEX8"] = "im"
+    import loadpath.simp as S
+    from loadpath.benchmarks.problems import cantilever_3d
+    from loadpath.benchmarks.run import NU, design_volfrac, domain_for
+
+    out = {}
+    for name, (dims, rmin, iters) in {"small": ((12, 4, 6), 1.5, 30), "medium": ((20, 6, 10), 2.0, 24)}.items():
+        p = cantilever_3d(*dims, 0.3, rmin)
+        dom, _ = domain_for(p)
+        mesh = dom.mesh
+        assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1 and dom.springs is None
+        opts = S.SimpOptions(volume_fraction=design_volfrac(p, dom), filter_radius=p.rmin, max_iterations=iters,
+                             solve_rtol=1e-10)
+        recs, xps = [], []
+        res = S.optimize(dom, NU, opts, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
+        nxyz = np.array(dims) + 1
+        fixed = np.zeros((3, *nxyz), bool)
+        f = np.zeros((3, *nxyz))
+        nijk = tuple(mesh.node_ijk.T)
+        for c in range(3):
+            fixed[c][nijk] = dom.fixed[c::3]
+            f[c][nijk] = dom.loads[0][c::3]
+        cells = tuple(mesh.elem_ijk.T)
+
+        def grid(v):
+            g = np.zeros(dims, np.asarray(v).dtype)
+            g[cells] = v
+            return g
+
+        keys = ("compliance", "relative", "volume", "beta", "change", "move", "volumeSolves", "solvedCells")
+        out.update({f"{name}_dims": np.array(dims), f"{name}_pitch": float(mesh.pitch), f"{name}_nu": float(NU),
+                    f"{name}_fixed": fixed, f"{name}_f": f, f"{name}_pres": grid(dom.preserve),
+                    f"{name}_volfrac": float(opts.volume_fraction), f"{name}_radius": float(opts.filter_radius),
+                    f"{name}_pad": bool(S._pad(opts)), f"{name}_emin": float(S.E_MIN),
+                    f"{name}_penal": float(S.PENALTY), f"{name}_iterations": len(recs),
+                    f"{name}_xphys": np.stack([grid(v) for v in xps]), f"{name}_x_last": grid(res.x)})
+        for k in keys:
+            out[f"{name}_{k}"] = np.array([float(r[k]) for r in recs])
+        out[f"{name}_stepFit"] = np.array([float(r.get("stepFit", np.nan)) for r in recs])
+    np.savez_compressed(os.path.join(HERE, "optimize.npz"), **out)
+
+
 def main(names=None):
     gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
             "mma": make_mma,
@@ -337,7 +388,8 @@ def main(names=None):
                                     make_hierarchy("odd_plain", (11, 5, 7), "plain", 2, 30, 0.0),
                                     make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
                                     make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
-            "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step}
+            "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step,
+            "optimize": make_optimize}
     for name in names or [k for k in gens if k != "config0"]:
         gens[name]()
 

@@ -169,3 +169,62 @@ def test_mgops_cells_fields():
                 assert flat[c.base[i] + c.off[3 * k + d]] == field[d, x + (k & 1), y + (k >> 1 & 1), z + (k >> 2 & 1)]
     assert c.ft(np.float32).shape == (24, c.n) and c.ft(np.float32) is c.ft("float32")
     assert c.base.dtype == c.off.dtype == c.cells.dtype == np.int64
+
+
+def _loop_state(**kw):
+    from loadpath_b200.optimize import OptimizeLoop, SimpOptions
+
+    lp = object.__new__(OptimizeLoop)
+    lp.opts = SimpOptions(volume_fraction=0.3, filter_radius=1.5, **kw.pop("opts", {}))
+    lp.measured, lp.scheduled = True, True
+    lp.beta, lp.since_beta, lp.step_prev, lp.move_k = 1.0, 0, 0.5, 0.2
+    lp.it, lp.history, lp.converged = 1, [], False
+    for key, v in kw.items():
+        setattr(lp, key, v)
+    return lp
+
+
+def test_optimize_loop_beta_continuation_and_stops():
+    """OptimizeLoop's continuation and stopping rules (loadpath/simp.py:2418-2450): beta doubles
+    after beta_every iterations or a free step under 2 tol, dropping the measured step and halving
+    the limit; at beta_max a free step under tol stops, the schedule stops a held volume after its
+    hold, and otherwise the compliance's stall over stall_window iterations stops."""
+    from loadpath_b200.optimize import beta_hold
+
+    assert beta_hold(_loop_state().opts, 1.0) == 10
+    sched = _loop_state(opts={"beta_schedule": (20, 15)}).opts
+    assert (beta_hold(sched, 1.0), beta_hold(sched, 2.0), beta_hold(sched, 4.0)) == (20, 15, 10)
+    # nine iterations at beta 1, a large change: no doubling
+    lp = _loop_state(since_beta=9)
+    lp._continue(change=0.1, move=0.2, comp=1.0, held=True)
+    assert lp.beta == 1.0 and lp.step_prev == 0.5
+    # the tenth: doubling
+    lp = _loop_state(since_beta=10)
+    lp._continue(change=0.1, move=0.2, comp=1.0, held=True)
+    assert (lp.beta, lp.since_beta, lp.step_prev, lp.move_k) == (2.0, 0, None, 0.1)
+    # a small change doubles early only as a free step (not held at the move limit)
+    lp = _loop_state(since_beta=3)
+    lp._continue(change=0.015, move=0.015, comp=1.0, held=True)
+    assert lp.beta == 1.0
+    lp._continue(change=0.015, move=0.2, comp=1.0, held=True)
+    assert lp.beta == 2.0
+    # at beta_max: a free step under tol stops
+    lp = _loop_state(beta=32.0, it=5, since_beta=2)
+    lp._continue(change=0.005, move=0.2, comp=1.0, held=True)
+    assert lp.converged
+    # scheduled with the volume held: stops after the hold, not before
+    lp = _loop_state(beta=32.0, it=5, since_beta=9)
+    lp._continue(change=0.05, move=0.2, comp=1.0, held=True)
+    assert not lp.converged
+    lp.since_beta = 10
+    lp._continue(change=0.05, move=0.2, comp=1.0, held=True)
+    assert lp.converged
+    # the volume off target (held False): the stall rule over stall_window = 6 compares with the
+    # compliance seven records back
+    hist = [{"compliance": c} for c in (10.0, 9.0, 8.5, 8.31, 8.305, 8.30, 8.30, 8.30)]
+    lp = _loop_state(beta=32.0, it=8, since_beta=6, history=hist)
+    lp._continue(change=0.05, move=0.2, comp=8.30, held=False)
+    assert not lp.converged           # against 9.0
+    hist += [{"compliance": 8.30}, {"compliance": 8.30}]
+    lp._continue(change=0.05, move=0.2, comp=8.30, held=False)
+    assert lp.converged               # against 8.31: within 2e-3

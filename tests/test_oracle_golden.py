@@ -257,3 +257,28 @@ def test_oracle_oc_loadpath_step_matches_reference_run():
         assert n_eval == int(g[f"n_eval{k}"])
         np.testing.assert_allclose(lm, float(g[f"lm{k}"]), rtol=1e-12)
         np.testing.assert_allclose(xn, grid(g[f"x_new{k}"]), rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("case", ["small", "medium"])
+def test_oracle_optimize_loop_matches_reference_run(case):
+    """The oracle's restatement of loadpath's SIMP loop (optimize_loop) against the reference's
+    own simp.optimize (tests/golden/optimize.npz): every iteration's projection sharpness, move
+    limit, multiplier trial count, compliance, change, volume and blueprint, and the last design.
+    The medium case's last iterations solve on the live cells only."""
+    g = _load("optimize.npz")
+    k = lambda s: g[f"{case}_{s}"]   # noqa: E731
+    dims = tuple(int(d) for d in k("dims"))
+    recs, x = R.optimize_loop(dims, R.hex8_ke(float(k("nu")), "im"), k("fixed"), k("f"), float(k("volfrac")),
+                              float(k("radius")), int(k("iterations")), pres=k("pres"), pad=bool(k("pad")),
+                              pitch=float(k("pitch")), emin=float(k("emin")), penal=float(k("penal")))
+    col = lambda key: np.array([r[key] for r in recs], float)   # noqa: E731
+    np.testing.assert_array_equal(col("beta"), k("beta"))
+    np.testing.assert_array_equal(col("volumeSolves"), k("volumeSolves"))
+    np.testing.assert_allclose(col("compliance"), k("compliance"), rtol=1e-10)
+    np.testing.assert_allclose(col("move"), k("move"), rtol=1e-12)
+    np.testing.assert_allclose(col("change"), k("change"), rtol=0, atol=1e-10)
+    np.testing.assert_allclose(col("volume"), k("volume"), rtol=1e-12)
+    np.testing.assert_allclose(np.stack([r["xphys"] for r in recs]), k("xphys"), rtol=0, atol=1e-9)
+    np.testing.assert_allclose(x, k("x_last"), rtol=0, atol=1e-9)
+    if case == "medium":
+        assert k("solvedCells")[-1] < np.prod(dims)
