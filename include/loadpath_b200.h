@@ -293,6 +293,9 @@ int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* 
  * the products the filter chain rule feeds to H^T and its clips (loadpath/simp.py:2001, :2077, :2191,
  * :2204) */
 int lpb_cell_product(double* out, const double* a, const double* b, const uint8_t* flags, int clip0, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* v = (v + v mirrored across the grid's mid-plane normal to axis) / 2 in place, axis 0 x, 1 y, 2 z
+ * (loadpath/simp.py:1476-1482 `_symmetrize`, every cell of the box having its mirror image) */
+int lpb_mirror_average(double* v, int axis, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
 /* ---- CUDA graphs of a stream's work (the solver records one CG iteration per solve) */
 int lpb_capture_begin(void* stream);

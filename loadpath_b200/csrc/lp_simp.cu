@@ -504,6 +504,28 @@ __global__ void k_cell_product(double* __restrict__ out, const double* __restric
   }
 }
 
+// v[c] = v[m(c)] = (v[c] + v[m(c)]) / 2 for every cell c and its mirror image m(c) across the
+// grid's mid-plane normal to axis (loadpath/simp.py:1476-1482 `_symmetrize` on a box whose every cell
+// has a mirror): one thread per pair, the cell below the mid-plane; the middle cell of an odd
+// extent is its own image and keeps its value.
+__global__ void k_mirror_average(double* __restrict__ v, int axis, LpGrid g) {
+  const long long total = g.cells_padded();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    if (!g.cell_at(t, x, y, z)) continue;
+    int mx = x, my = y, mz = z;
+    if (axis == 0) mx = g.nx - 1 - x;
+    else if (axis == 1) my = g.ny - 1 - y;
+    else mz = g.nz - 1 - z;
+    const long long m = g.cell(mx, my, mz);
+    if (m <= t) continue;
+    const double a = v[t], b = v[m];
+    const double h = 0.5 * (a + b);
+    v[t] = h;
+    v[m] = h;
+  }
+}
+
 // ce[e] = u_e^T ke v_e over a general mesh, u_e the 24 values at edof[e, :] (femops.element_energy,
 // loadpath/femops.py:236-242); v NULL: v = u. One thread per element, ke in shared memory; the
 // caller has checked every index against the vectors' length.
@@ -676,6 +698,15 @@ int lpb_oc_stepped(double* xn, const double* x, const double* dc, const double* 
   LpGrid g = LP_GRID;
   if (!lp_grid_ok(g) || !xn || !x || !dc || !dv || !(lm > 0.0)) return LP_ERR_ARG;
   k_oc_stepped<<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(xn, x, dc, dv, lm, move, flags, g);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// the mirror average across axis (0 x, 1 y, 2 z), in place
+int lpb_mirror_average(double* v, int axis, LP_GRID_ARGS, void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !v || axis < 0 || axis > 2) return LP_ERR_ARG;
+  k_mirror_average<<<lp_blocks(g.cells_padded(), 256), 256, 0, LP_ST>>>(v, axis, g);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -165,10 +165,12 @@ class OptimizeLoop:
     dims: cells (even); fixed_grid: bool (3, nx+1, ny+1, nz+1); loads: node-grid force arrays
     (3, nx+1, ny+1, nz+1), one per case; preserve / void: bool cell grids or None; pitch: the cell
     size (Ke and the filter scale with it as the reference's `_Analysis` and `density_filter` do);
+    mirror: the mirror planes of a symmetric problem ('x', 'y', 'z' in the domain's order), whose
+    sensitivities and trial designs are averaged across them (loadpath/simp.py:2222-2224, 2300);
     dtype: the V-cycle's precision (the CG is float64)."""
 
     def __init__(self, dims, fixed_grid, loads, nu, opts: SimpOptions, preserve=None, void=None,
-                 case_weights=None, pitch=1.0, element="im", dtype=np.float32, coarse_cells=2000,
+                 case_weights=None, pitch=1.0, mirror=(), element="im", dtype=np.float32, coarse_cells=2000,
                  maxiter=2000, live_cells=True, device="cuda"):
         dims = tuple(int(d) for d in dims)
         if any(d % 2 for d in dims):
@@ -194,7 +196,9 @@ class OptimizeLoop:
         flags = (pres & ~vd).astype(np.uint8) | (vd.astype(np.uint8) << 1)
         self.flags = g.set_cells(g.cell_field(torch.uint8), torch.from_numpy(flags))
         self.w = g.cells_to_dev(design.astype(np.float64), torch.float64)
-        self.pd = ProjectedDesign(self.filter, w=self.w, flags=self.flags)
+        axes = {"x": 0, "y": 1, "z": 2}
+        self.mirror = tuple(axes.get(a, a) for a in mirror)
+        self.pd = ProjectedDesign(self.filter, w=self.w, flags=self.flags, mirror=self.mirror)
         self.target = float(opts.volume_fraction) * float(design.sum())
         x = np.full(dims, float(opts.volume_fraction))
         if opts.x0 is not None:
@@ -299,6 +303,9 @@ class OptimizeLoop:
         pd.chain(self.dc, self.dc_xe, self.dproj_e, clip=True)
         pd.chain(self.dv, self.w, self.dproj)
         L.lpb_cell_product(self.dv.data_ptr(), self.dv.data_ptr(), None, None, 2, *g.args, st)
+        for ax in self.mirror:
+            L.lpb_mirror_average(self.dc.data_ptr(), ax, *g.args, st)
+            L.lpb_mirror_average(self.dv.data_ptr(), ax, *g.args, st)
         sec = None
         if self.measured:
             if self.step_prev is not None:

@@ -257,12 +257,16 @@ class ProjectedDesign:
 
     flt: the grid's DeviceFilter (H symmetric, as the reference's cone filter); w: volume weight per
     cell (float64 cell field; None: 1 on every cell); flags: uint8 cell field, bit 0 passive solid
-    (held at 1), bit 1 passive void (held at 0), or None. The reference's mirror symmetry, column
-    extrusion, printed-hook and blockage terms are not part of this step."""
+    (held at 1), bit 1 passive void (held at 0), or None; mirror: the axes (0 x, 1 y, 2 z, in the
+    reference's order) whose mirror symmetry each trial design is averaged onto (loadpath/simp.py:
+    2300-2301, `_symmetrize`; the pinned and void cells mirror-symmetric, as the reference's
+    domains build them). The reference's column extrusion, printed-hook and blockage terms are not
+    part of this step."""
 
-    def __init__(self, flt: DeviceFilter, w=None, flags=None):
+    def __init__(self, flt: DeviceFilter, w=None, flags=None, mirror=()):
         g = flt.grid
         self.flt, self.grid, self.flags = flt, g, flags
+        self.mirror = tuple(int(a) for a in mirror)
         self.w = w if w is not None else g.set_cells(g.cell_field(torch.float64), 1.0)
         self.xt = g.cell_field(torch.float64)
         self.xp = g.cell_field(torch.float64)
@@ -308,6 +312,8 @@ class ProjectedDesign:
             n_eval[0] += 1
             L.lpb_oc_stepped(self.xn.data_ptr(), x.data_ptr(), dc.data_ptr(), dv.data_ptr(), float(lm_), float(move),
                              ptr(self.flags), *g.args, st)
+            for ax in self.mirror:
+                L.lpb_mirror_average(self.xn.data_ptr(), ax, *g.args, st)
             return self.physical(self.xn, beta, eta) - target
 
         l1, l2 = 1e-12, 1e12

@@ -702,8 +702,16 @@ def dproject(xt, beta, eta):
 VOLUME_RTOL = 1e-13   # loadpath/simp.py:1234
 
 
+def mirror_average(v, mirror):
+    """loadpath/simp.py:1476-1482 `_symmetrize` on a box whose every cell has a mirror image: per
+    axis in order, v = (v + v mirrored across the mid-plane) / 2."""
+    for ax in mirror:
+        v = 0.5 * (v + np.flip(v, axis=ax))
+    return v
+
+
 def oc_loadpath_step(x, dc, dv, move, beta, eta, h_apply, hs, w, target, pres=None, void=None,
-                     lam_last=None):
+                     lam_last=None, mirror=()):
     """loadpath's optimality-criteria step (loadpath/simp.py:2249-2376, the volume-constrained
     path: no thermal swing constraint, mirror, extrusion or blockage term). The step
     x sqrt(-dc / dv / lm) clipped to [max(0, x - move), min(1, x + move)] (passive cells held),
@@ -730,6 +738,8 @@ def oc_loadpath_step(x, dc, dv, move, beta, eta, h_apply, hs, w, target, pres=No
             xn[pres] = 1.0
         if void is not None:
             xn[void] = 0.0
+        if mirror:
+            xn = mirror_average(xn, mirror)
         return xn, float(np.sum(physical(xn) * w)) - target
 
     l1, l2 = 1e-12, 1e12
@@ -911,7 +921,8 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
 
 
 def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=None, pad=True, pitch=1.0,
-                  eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0):
+                  eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0,
+                  mirror=()):
     """loadpath's own SIMP loop for one load case with its default options (loadpath/simp.py:
     1640-2455): blueprint and eroded projections of xt = H x / hs (`physical`, `eroded`), the SIMP
     law on the eroded design, the solve with the live-cell reduction (live_solve, the anchor cells
@@ -919,7 +930,8 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
     dv = max(H (w P'_b / hs), 1e-12), the move limit measured from the Lagrangian's slope along
     the last step (t = a / (a - b), the limit times t clipped to [0.5, 1.2], capped at move), the
     step of oc_loadpath_step, and beta doubling after beta_every iterations or a free step of
-    change < 2 tol, halving the limit. Ke and the loads' work scale with the pitch. Returns the
+    change < 2 tol, halving the limit; with mirror planes (axes) dc, dv and every trial design are
+    averaged across them (:2222-2224, :2300). Ke and the loads' work scale with the pitch. Returns the
     per-iteration records (compliance, beta, change, move, volume, volumeSolves, xphys) and x."""
     pres = np.zeros(dims, bool) if pres is None else np.asarray(pres, bool)
     design = ~pres
@@ -954,6 +966,8 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
         dpb[pres] = 0.0
         dc = np.minimum(hap(dc_xe * dpe / hs), 0.0)
         dv = np.maximum(hap(w * dpb / hs), 1e-12)
+        if mirror:
+            dc, dv = mirror_average(dc, mirror), mirror_average(dv, mirror)
         if step_prev is not None:
             dxp, gp, lam_p = step_prev
             a_s = float(np.sum(gp * dxp))
@@ -963,7 +977,7 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
                 move_k = min(move_k * min(max(t_s, 0.5), 1.2), move)
         mv = move_k
         x_new, lm, n_eval, _ = oc_loadpath_step(x, dc, dv, mv, beta, eta, hap, hs, w, target, pres=pres,
-                                                lam_last=lam_last)
+                                                lam_last=lam_last, mirror=mirror)
         lam_last = lm
         change = float(np.abs(x_new - x)[design].max())
         step_prev = (x_new - x, dc + lm * dv, lm)

@@ -333,23 +333,32 @@ def make_oc_step():
 def make_optimize():
     """loadpath's own SIMP loop as a whole (loadpath/simp.py:1640-2455, simp.optimize with its
     default options: blueprint and eroded projections, the measured step length, beta
-    continuation, the volume multiplier solved to rounding) on two top3d cantilevers of its
-    benchmarks (domain_for: load and support cells pinned, padded filter), with the solves
+    continuation, the volume multiplier solved to rounding) on two top3d cantilevers and a bridge
+    mirrored in x and y, of its benchmarks (domain_for: load and support cells pinned, padded
+    filter), with the solves
     tightened to rtol 1e-10 so that a solver of another kind can be compared iteration by
     iteration. Stored per case: the domain on the node / cell grid (supports, load, pinned cells),
     the options, and per iteration the record the loop reports and the blueprint density it
     started from; and the last design."""
     os.environ["LOADPATH_HEX8"] = "im"
     import loadpath.simp as S
-    from loadpath.benchmarks.problems import cantilever_3d
+    from loadpath.benchmarks.problems import bridge_3d, cantilever_3d
     from loadpath.benchmarks.run import NU, design_volfrac, domain_for
 
     out = {}
-    for name, (dims, rmin, iters) in {"small": ((12, 4, 6), 1.5, 30), "medium": ((20, 6, 10), 2.0, 24)}.items():
-        p = cantilever_3d(*dims, 0.3, rmin)
+    cases = {"small": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 30), "medium": (cantilever_3d, (20, 6, 10), 0.3, 2.0, 24),
+             "bridge": (bridge_3d, (16, 4, 6), 0.15, 1.5, 24)}
+    for name, (problem, dims, vf, rmin, iters) in cases.items():
+        p = problem(*dims, vf, rmin)
         dom, _ = domain_for(p)
         mesh = dom.mesh
         assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1 and dom.springs is None
+        axes = {"x": 0, "y": 1, "z": 2}
+        for ax, m in dom.mirror.items():
+            assert np.all(m >= 0)
+            mirrored = mesh.elem_ijk.copy()
+            mirrored[:, axes[ax]] = dims[axes[ax]] - 1 - mirrored[:, axes[ax]]
+            assert np.array_equal(mesh.elem_ijk[m], mirrored)
         opts = S.SimpOptions(volume_fraction=design_volfrac(p, dom), filter_radius=p.rmin, max_iterations=iters,
                              solve_rtol=1e-10)
         recs, xps = [], []
@@ -374,6 +383,7 @@ def make_optimize():
                     f"{name}_volfrac": float(opts.volume_fraction), f"{name}_radius": float(opts.filter_radius),
                     f"{name}_pad": bool(S._pad(opts)), f"{name}_emin": float(S.E_MIN),
                     f"{name}_penal": float(S.PENALTY), f"{name}_iterations": len(recs),
+                    f"{name}_mirror": np.array([axes[a] for a in dom.mirror], np.int64),
                     f"{name}_xphys": np.stack([grid(v) for v in xps]), f"{name}_x_last": grid(res.x)})
         for k in keys:
             out[f"{name}_{k}"] = np.array([float(r[k]) for r in recs])
