@@ -80,28 +80,35 @@ __global__ void __launch_bounds__(256) k_filter(double* __restrict__ out, const 
   }
   const int XH = LP_FT_X + 2 * R, YH = LP_FT_Y + 2 * R, ZH = 4 + 2 * R, P = XH * YH;
   const int CR = (R + 3) / 4;  // halo chunks on each side
-  const int rowlen = 4 * XH, nitems = (2 * CR + 1) * YH * rowlen;
-  for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
-    const int row = i / rowlen, j = i - row * rowlen;
+  // the taps' offsets in the staged tile, written over their first coordinate
+  for (int i = threadIdx.x; i < ntaps; i += blockDim.x) so[3 * i] += (so[3 * i + 2] * YH + so[3 * i + 1]) * XH;
+  // a warp stages a (chunk, y) row at a time: 4 XH doubles contiguous in memory, lanes along it
+  const int rowlen = 4 * XH, nrows = (2 * CR + 1) * YH;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5), nwarps = (int)(blockDim.x >> 5);
+  for (int row = warp; row < nrows; row += nwarps) {
     const int cr = row / YH, yl = row - cr * YH;
-    const int xl = j >> 2, gz = 4 * (cz - CR + cr) + (j & 3);
-    const int zl = gz - (4 * cz - R);
-    if (zl < 0 || zl >= ZH) continue;
-    const int gx = x0 - R + xl, gy = y0 - R + yl;
-    double val = 0.0;
-    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) {
-      const long long c = g.cell(gx, gy, gz);
-      val = v[c];
-      if (hs_in) val = val / hs_in[c];
+    const int gy = y0 - R + yl, zbase = 4 * (cz - CR + cr);
+    const bool yok = gy >= 0 && gy < g.ny;
+    for (int j = lane; j < rowlen; j += 32) {
+      const int xl = j >> 2, gz = zbase + (j & 3);
+      const int zl = gz - (4 * cz - R);
+      if (zl < 0 || zl >= ZH) continue;
+      const int gx = x0 - R + xl;
+      double val = 0.0;
+      if (yok && gx >= 0 && gx < g.nx && gz >= 0 && gz < g.nz) {
+        const long long c = g.cell(gx, gy, gz);
+        val = v[c];
+        if (hs_in) val = val / hs_in[c];
+      }
+      tile[(zl * YH + yl) * XH + xl] = val;
     }
-    tile[(zl * YH + yl) * XH + xl] = val;
   }
   __syncthreads();
   if (!own) return;
   const int ctr = (R * YH + R + (int)(threadIdx.x >> 5)) * XH + R + (int)(threadIdx.x & 31);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int i = 0; i < ntaps; ++i) {
-    const int o = ctr + (so[3 * i + 2] * YH + so[3 * i + 1]) * XH + so[3 * i];
+    const int o = ctr + so[3 * i];
     const double w = sw[i];
 #pragma unroll
     for (int zq = 0; zq < 4; ++zq) acc[zq] += w * tile[o + zq * P];
