@@ -347,6 +347,9 @@ int lpb_live_seed(uint8_t* state, const double* xp, const uint8_t* flags, double
 int lpb_live_flood(uint8_t* state, int* changed, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_live_moduli(double* e_out, const double* e, const uint8_t* state, int nx, int ny, int nz, int pz, int cpz, void* stream);
 int lpb_dead_loads(const double* f, const uint8_t* mask, double* part, double* count, int nx, int ny, int nz, int pz, int cpz, void* stream);
+/* *count = cells alive in a seeded state (nonzero) but not kept (2) in an earlier flooded state:
+ * zero lets the direct solver's reduced system be reused (loadpath/simp.py:288-297) */
+int lpb_live_outside(const uint8_t* state, const uint8_t* keep, double* part, double* count, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
 /* ---- MMA (loadpath/mma.py:31-214, MMA.update and MMA._subsolv): the n-sized work of one
  * update over n variables and m <= 8 constraints, float64, device arrays; P, Q, df are (m, n)

@@ -34,7 +34,7 @@ _KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_m
             "lpb_capture_end": 0, "lpb_graph_launch": 0, "lpb_graph_free": 0, "lpb_while_begin": 0, "lpb_tune_set": 0, "lpb_tune_get": 0,
             "lpb_while_end": 0,
             "lpb_mma_part_len": 0, "lpb_mma_prepare": 2, "lpb_mma_newton_a": 2, "lpb_mma_newton_b": 2,
-            "lpb_mma_trial": 2, "lpb_project": 2, "lpb_live_seed": 2,
+            "lpb_mma_trial": 2, "lpb_project": 2, "lpb_live_seed": 2, "lpb_live_outside": 2,
             "lpb_dead_loads": 2, "lpb_apply_rf_f32": 2, "lpb_apply_explicit_modal_f32": 2,
             "lpb_apply_explicit_modal_cheb_f32": 2, "lpb_modal_sym": 0, "lpb_hex8_ke": 0,
             "lpb_level1_products": 0, "lpb_uniform_numpy": 0, "lpb_layout_dims": 0, "lpb_layout_nodes_f64": 0,

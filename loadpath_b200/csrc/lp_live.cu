@@ -41,6 +41,18 @@ __global__ void k_live_seed(uint8_t* __restrict__ state, const double* __restric
   if (threadIdx.x == 0) part[blockIdx.x] = cnt;
 }
 
+// partial counts of the cells alive in state (seeded: nonzero) but not kept in keep (a flooded state: 2)
+__global__ void k_live_outside(const uint8_t* __restrict__ state, const uint8_t* __restrict__ keep, LpGrid g,
+                               double* __restrict__ part) {
+  __shared__ double sh[32];
+  const long long total = g.cells_padded();
+  double cnt = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x)
+    if (state[t] != 0 && keep[t] != 2) cnt += 1.0;
+  cnt = lp_block_sum(cnt, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = cnt;
+}
+
 __global__ void k_live_count_final(const double* __restrict__ part, int n, double* __restrict__ out) {
   __shared__ double sh[32];
   double s = 0.0;
@@ -144,6 +156,19 @@ int lpb_live_moduli(double* e_out, const double* e, const uint8_t* state, LP_GRI
   if (!lp_grid_ok(g) || !e_out || !e || !state) return LP_ERR_ARG;
   const long long n = g.cells_padded();
   k_live_moduli<<<lp_blocks(n, 256), 256, 0, LP_ST>>>(e_out, e, state, n);
+  LP_LAUNCH_CHECK();
+  return LP_OK;
+}
+
+// *count = cells alive in a seeded state but outside the kept cells of an earlier flooded state
+// (the reference's test for reusing a reduced system, loadpath/simp.py:295); padding cells are 0
+// in both
+int lpb_live_outside(const uint8_t* state, const uint8_t* keep, double* part, double* count, LP_GRID_ARGS,
+                     void* stream) {
+  LpGrid g = LP_GRID;
+  if (!lp_grid_ok(g) || !state || !keep || !part || !count) return LP_ERR_ARG;
+  k_live_outside<<<LP_LIVE_BLOCKS, 256, 0, LP_ST>>>(state, keep, g, part);
+  k_live_count_final<<<1, 1024, 0, LP_ST>>>(part, LP_LIVE_BLOCKS, count);
   LP_LAUNCH_CHECK();
   return LP_OK;
 }

@@ -1781,6 +1781,8 @@ class GridElasticity:
         er = self._tbuf("e_live", e_dev.shape, torch.float64)
         live.moduli(e_dev, er)
         self.set_moduli_device(er)
+        if getattr(live, "reused", False):
+            return True          # a cached reduced system: its loads were found held when it was built
         L = lib()
         st = stream_handle()
         g = self.g0
@@ -1789,8 +1791,12 @@ class GridElasticity:
             L.lpb_dead_loads(f.data_ptr(), self.levels[0].mask.data_ptr(), self._part.data_ptr(), cnt.data_ptr(),
                              *g.args, st)
             if float(cnt.item()) > 0:
+                if hasattr(live, "record"):
+                    live.record(False)
                 self.set_moduli_device(e_dev)
                 return False
+        if hasattr(live, "record"):
+            live.record(True)
         return True
 
     def check_device(self):

@@ -34,7 +34,7 @@ from .autograd import Compliance, SimpProblem
 from .grid import ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 from .mma import MMA
-from .simp import DeviceFilter, LiveCells, ProjectedDesign, _cells_touching
+from .simp import MG_MIN_CELLS, SUB_REUSE, DeviceFilter, LiveCells, ProjectedDesign, _cells_touching
 
 __all__ = ["MMALoop", "OptimizeLoop", "SimpOptions", "E_MIN", "PENALTY"]
 
@@ -153,7 +153,8 @@ class OptimizeLoop:
     eroded xe = P(H x / hs, beta, eta + erode) (`physical`, `eroded`, :1775-1814); moduli
     E = E_MIN + xe^3 (1 - E_MIN); one MG-PCG solve per case, warm-started from the last one, on the
     cells the reference's analysis solves (`_Analysis`, :114-330: when fewer than 80 % of the cells
-    are alive only the alive cells connected to a support, `LiveCells`); compliance sum_k w_k f_k.u_k;
+    are alive only the alive cells connected to a support, `LiveCells`, a reduced system reused
+    while the alive cells stay in it on grids the reference solves directly); compliance sum_k w_k f_k.u_k;
     dc = min(H^T(dc_xe P'(xt, eta + erode) / hs), 0) and dv = max(H^T(w P'(xt, eta) / hs), 1e-12)
     (:1994-2204); the move limit measured from the slope of the Lagrangian along the last step
     (:2229-2243) or the fixed schedule (move, then move / 2 past beta 4); the optimality-criteria
@@ -216,7 +217,9 @@ class OptimizeLoop:
             loaded = np.zeros(g.node_shape[1:], bool)
             for f in cases:
                 loaded |= (np.asarray(f).reshape(g.node_shape) != 0).any(axis=0)
-            self.live = LiveCells(g, _cells_touching(held), _cells_touching(held | loaded) | pres)
+            # the reference's analysis reuses a reduced system on grids it solves directly
+            reuse = SUB_REUSE if int(np.prod(dims)) < MG_MIN_CELLS else 0
+            self.live = LiveCells(g, _cells_touching(held), _cells_touching(held | loaded) | pres, reuse=reuse)
         cf = lambda: g.cell_field(torch.float64)   # noqa: E731
         self.xp, self.dproj, self.xe, self.dproj_e, self.e, self.ce = cf(), cf(), cf(), cf(), cf(), cf()
         self.dc_xe, self.dc, self.dv, self.dx, self.gp, self._tmp = cf(), cf(), cf(), cf(), cf(), cf()
@@ -266,8 +269,9 @@ class OptimizeLoop:
             if not self.reduced:
                 raise
             # a reduced system the multigrid cannot hold: the full grid, void at E_MIN
-            # (loadpath/simp.py:815-822)
+            # (loadpath/simp.py:815-822), and no reduced system kept for reuse
             self.reduced = False
+            self.live._cache = None
             self.ge.set_moduli_device(self.e)
             us = [self.ge.solve_device(f, None) for f in self.fs]
         self.us = us

@@ -179,6 +179,8 @@ REDUCE_BELOW = 0.8    # ...once fewer than this share of the cells are alive (lo
 MG_SLOW_ITERS = 60    # CG iterations past which the SIMP driver leaves the multigrid (loadpath/simp.py:85)
 OC_TOL = 1e-3         # top3d's bisection stops at (l2 - l1) / (l1 + l2) <= 1e-3 (loadpath/benchmarks/reference.py:100)
 MG_MAXITER = 2000     # the SIMP driver's CG cap for its multigrid (loadpath/simp.py:182)
+MG_MIN_CELLS = 100_000  # grids the SIMP driver solves by multigrid from; smaller ones directly (loadpath/simp.py:69)
+SUB_REUSE = 6         # solves the direct path keeps a reduced system for (loadpath/simp.py:288)
 
 
 def _cells_touching(node_flags):
@@ -201,10 +203,18 @@ class LiveCells:
     the others get modulus 0 on the fixed grid. The components are found by a flood fill from
     those support cells (lp_live.cu), the union the reference's labelling keeps.
 
-    support_touch, anchor: bool (nx, ny, nz) host arrays in grid order."""
+    support_touch, anchor: bool (nx, ny, nz) host arrays in grid order. reuse: 0 for the multigrid
+    path's rule above (the kept cells found again every solve); n > 0 for the direct path's
+    (loadpath/simp.py:288-315 `_subsystem`, grids under MG_MIN_CELLS cells): a reduced system is
+    kept for up to n further solves while every alive cell stays inside it, its cells keeping their
+    moduli (set_moduli_live records it once its loads are found held)."""
 
-    def __init__(self, grid: DevGrid, support_touch, anchor):
+    def __init__(self, grid: DevGrid, support_touch, anchor, reuse=0):
         self.grid = grid
+        self.reuse = int(reuse)
+        self._cache = None       # the reduced system's kept cells (a flooded state), or None
+        self._age = 0
+        self.reused = False      # the last keep() handed back the cached system
         st = np.asarray(support_touch, bool)
         an = np.asarray(anchor, bool)
         bits = torch.from_numpy((st.astype(np.uint8) | (an.astype(np.uint8) << 1)))
@@ -227,8 +237,16 @@ class LiveCells:
                         self._cnt.data_ptr(), *g.args, st)
         self.alive_share = float(self._cnt.item()) / self.n_cells
         self.passes = 0
+        self.reused = False
         if self.alive_share >= REDUCE_BELOW:
             return None
+        if self.reuse and self._cache is not None and self._age < self.reuse:
+            L.lpb_live_outside(self.state.data_ptr(), self._cache.data_ptr(), self._part.data_ptr(),
+                               self._cnt.data_ptr(), *g.args, st)
+            if float(self._cnt.item()) == 0.0:
+                self._age += 1
+                self.reused = True
+                return self._cache
         while self.passes < max_passes:
             L.lpb_memset_async(self._changed.data_ptr(), 0, 4, st)
             for _ in range(4):   # a few passes between reads of the flag
@@ -240,8 +258,20 @@ class LiveCells:
 
     def moduli(self, e, out):
         """out = e on the kept cells, 0 elsewhere (after keep())."""
-        lib().lpb_live_moduli(out.data_ptr(), e.data_ptr(), self.state.data_ptr(), *self.grid.args, stream_handle())
+        kept = self._cache if self.reused else self.state
+        lib().lpb_live_moduli(out.data_ptr(), e.data_ptr(), kept.data_ptr(), *self.grid.args, stream_handle())
         return out
+
+    def record(self, held):
+        """After a fresh reduction (not a reused one): keep it for reuse when its loads are held,
+        drop any cached one when they are not."""
+        if not self.reuse or self.reused:
+            return
+        if held:
+            self._cache = self.state.clone()
+            self._age = 0
+        else:
+            self._cache = None
 
 
 VOLUME_RTOL = 1e-13   # the volume multiplier's stopping tolerance (loadpath/simp.py:1234)

@@ -842,6 +842,51 @@ def live_solve(ke, fixed_grid, f_grid, support_touch, anchor):
     return solve
 
 
+class LiveSystem:
+    """The SIMP driver's solves with the live-cell reduction (loadpath/simp.py:114-330 `_Analysis`):
+    alive = xphys > ALIVE or an anchor cell; under REDUCE_BELOW alive, only the cells connected_keep
+    keeps carry their moduli (dofs without stiffness dropped, zero in u), unless a load is left
+    on such a dof. reuse = 0 is the multigrid path's rule (:795-826, the kept cells found every
+    solve); reuse = n the direct path's (:288-315 `_subsystem`): a reduced system is kept for up
+    to n further solves while every alive cell is inside it. resolve() solves another right-hand
+    side on the last solve's system (:828-876). Direct sparse solves (assembled_solve)."""
+
+    def __init__(self, ke, fixed_grid, support_touch, anchor, reuse=0):
+        self.ke, self.fixed = ke, np.asarray(fixed_grid, bool)
+        self.support_touch, self.anchor, self.reuse = support_touch, anchor, reuse
+        self.cache, self.age = None, 0
+        self.er, self.drop, self.cells = None, False, None
+
+    def _stiff_nodes(self, cells):
+        dims = cells.shape
+        stiff = np.zeros(tuple(d + 1 for d in dims), bool)
+        for (i, j, k) in OFFS:
+            stiff[i:i + dims[0], j:j + dims[1], k:k + dims[2]] |= cells
+        return stiff
+
+    def solve(self, e, xphys, f_grid):
+        f_grid = np.asarray(f_grid, float)
+        alive = (xphys > ALIVE) | self.anchor
+        self.er, self.drop, self.cells = e, False, e.size
+        if alive.mean() < REDUCE_BELOW and not np.any(f_grid[:, ~self._stiff_nodes(alive)]):
+            keep = None
+            if self.reuse and self.cache is not None and self.age < self.reuse and not np.any(alive & ~self.cache):
+                self.age += 1
+                keep = self.cache
+            else:
+                keep = connected_keep(alive, self.support_touch)
+                if np.any(f_grid[:, ~self._stiff_nodes(keep)]):
+                    self.cache, keep = None, None
+                elif self.reuse:
+                    self.cache, self.age = keep, 0
+            if keep is not None:
+                self.er, self.drop, self.cells = np.where(keep, e, 0.0), True, int(keep.sum())
+        return assembled_solve(self.ke, self.er, self.fixed, f_grid, drop_dead=self.drop)
+
+    def resolve(self, rhs):
+        return assembled_solve(self.ke, self.er, self.fixed, rhs, drop_dead=self.drop)
+
+
 # --------------------------------------------------------------------------
 # assembled direct solve for tiny grids (loadpath/benchmarks/evaluate.py:111-117)
 # --------------------------------------------------------------------------
@@ -922,11 +967,12 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
 
 def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=None, pad=True, pitch=1.0,
                   eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0,
-                  mirror=()):
+                  mirror=(), reuse=6):
     """loadpath's own SIMP loop for one load case with its default options (loadpath/simp.py:
     1640-2455): blueprint and eroded projections of xt = H x / hs (`physical`, `eroded`), the SIMP
-    law on the eroded design, the solve with the live-cell reduction (live_solve, the anchor cells
-    being those touching a support or the load and the pinned ones), dc = min(H (dc_xe P'_e / hs), 0),
+    law on the eroded design, the solve with the live-cell reduction (LiveSystem with the direct
+    path's reuse of a reduced system, the anchor cells being those touching a support or the load
+    and the pinned ones), dc = min(H (dc_xe P'_e / hs), 0),
     dv = max(H (w P'_b / hs), 1e-12), the move limit measured from the Lagrangian's slope along
     the last step (t = a / (a - b), the limit times t clipped to [0.5, 1.2], capped at move), the
     step of oc_loadpath_step, and beta doubling after beta_every iterations or a free step of
@@ -941,8 +987,9 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
     hap = lambda v: grid_filter(v, taps)   # noqa: E731
     held = np.asarray(fixed_grid, bool).any(axis=0)
     loaded = (np.asarray(f_grid) != 0).any(axis=0)
-    solve = live_solve(ke * pitch, fixed_grid, f_grid, cells_touching(held),
-                       cells_touching(held | loaded) | pres)
+    system = LiveSystem(ke * pitch, fixed_grid, cells_touching(held), cells_touching(held | loaded) | pres,
+                        reuse=reuse)
+    solve = lambda e, xp_: system.solve(e, xp_, f_grid)   # noqa: E731
     x = np.full(dims, volfrac)
     x[pres] = 1.0
     target = volfrac * float(w.sum())
@@ -993,6 +1040,175 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
     return recs, x
 
 
+VM = np.array([[1.0, -0.5, -0.5, 0, 0, 0], [-0.5, 1.0, -0.5, 0, 0, 0], [-0.5, -0.5, 1.0, 0, 0, 0],
+               [0, 0, 0, 3.0, 0, 0], [0, 0, 0, 0, 3.0, 0], [0, 0, 0, 0, 0, 3.0]])   # loadpath/constrained.py:107-114
+
+
+def hex8_b(xi, eta, zeta, nu, element="im"):
+    """Strain-displacement (6x24) of the unit cube at a natural point with the condensed
+    bubbles' strain (loadpath/fem.py:227-237)."""
+    c = elastic_c(nu)
+    g = 1.0 / np.sqrt(3.0)
+    kua = np.zeros((24, 9))
+    kaa = np.zeros((9, 9))
+    for a in (-g, g):
+        for b_ in (-g, g):
+            for cz in (-g, g):
+                b = b_matrix(a, b_, cz)
+                ba = b_bubble(a, b_, cz)
+                kua += b.T @ c @ ba * 0.125
+                kaa += ba.T @ c @ ba * 0.125
+    out = b_matrix(xi, eta, zeta)
+    if element == "im":
+        out = out + b_bubble(xi, eta, zeta) @ (-np.linalg.solve(kaa, kua.T))
+    return out
+
+
+def corner_stress_ops(nu, pitch=1.0, element="im"):
+    """The 8 (6x24) stress operators C B at the cube's corners, x outermost
+    (loadpath/constrained.py:443-446, STRESS_POINTS = "corners")."""
+    c = elastic_c(nu)
+    return [c @ hex8_b(a, b, cz, nu, element) / pitch for a in (-1.0, 1.0) for b in (-1.0, 1.0) for cz in (-1.0, 1.0)]
+
+
+def scatter_cells(fe, dims):
+    """Node field (3, nx+1, ny+1, nz+1) summing per-cell 24-vectors fe (24, nx, ny, nz) onto the
+    cells' corners (the transpose of gather_cells)."""
+    out = np.zeros((3,) + tuple(d + 1 for d in dims))
+    nx, ny, nz = dims
+    for k, (dx, dy, dz) in enumerate(OFFS):
+        out[:, dx:dx + nx, dy:dy + ny, dz:dz + nz] += fe[3 * k:3 * k + 3]
+    return out
+
+
+def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_limit, deflection_limit, modulus,
+                     pres=None, pad=True, pitch=1.0, mirror=(), eta=0.5, erode=0.15, move=0.2, tol=0.01,
+                     beta_max=32.0, beta_every=10, stall_window=6, emin=1e-6, penal=3.0, element="im", reuse=6):
+    """loadpath's minimum-mass loop under a stress and a deflection limit for one load case
+    (loadpath/constrained.py:295-854 with Limits(stress, deflection, modulus) and default options):
+    per iteration the blueprint and eroded designs, the solve on the live cells (LiveSystem, as
+    optimize_loop) and the adjoint solves on the same system, the deflection f.u / (sum_n |f_n| E) against its limit with gradient
+    -dE ce / (sum |f| E); the relaxed von Mises xe * vm(C B_k u_e) / limit at the 8 corners of every
+    cell that moved and touches no support or load, aggregated by a P-mean (P = 8) over the counted
+    corners with the adaptive normalisation kappa (Le et al.), its adjoint solve and gradient;
+    the volume objective 10 mean(xp) over the design cells; MMA (move 0.1, halved and its asymptotes
+    tightened while the worst constraint grows above 0.02, grown by 1.2 up to the cap inside);
+    beta doubling once feasible after beta_every iterations or a small change (or after 3
+    beta_every), the cap times 0.6; at beta_max the lightest feasible design is kept and the run
+    stops on a feasible small change or a stalled volume. Returns (records, x, converged)."""
+    pres = np.zeros(dims, bool) if pres is None else np.asarray(pres, bool)
+    design = ~pres
+    free = np.flatnonzero(design.reshape(-1))
+    taps = filter_taps(radius, pitch)
+    hs = np.full(dims, sum(t for _, t in taps)) if pad else filter_row_sums(dims, taps)
+    hap = lambda v: grid_filter(v, taps)   # noqa: E731
+    ke = hex8_ke(nu, element) * pitch
+    f_grid = np.asarray(f_grid, float)
+    held = np.asarray(fixed_grid, bool).any(axis=0)
+    loaded = (f_grid != 0).any(axis=0)
+    system = LiveSystem(ke, fixed_grid, cells_touching(held), cells_touching(held | loaded) | pres, reuse=reuse)
+    counted = ~cells_touching(held | loaded)
+    nc = max(int(counted.sum()), 1) * 8
+    load_size = float(np.linalg.norm(f_grid.reshape(3, -1), axis=0).sum())
+    cbs = corner_stress_ops(nu, pitch, element)
+    sym = (lambda v: mirror_average(v, mirror)) if mirror else (lambda v: v)   # noqa: E731
+    x = np.full(dims, vf0)
+    x[pres] = 1.0
+    mma = MMA(len(free), 2, 0.0, 1.0, move=min(move, 0.1))
+    move_cap = mma.move
+    worst_prev, kappa, beta, since_beta = np.inf, 1.0, 1.0, 0
+    best, trail, recs, converged = None, [], [], False
+    for it in range(1, iters + 1):
+        x_now = x
+        xt = hap(x) / hs
+        xp = project(xt, beta, eta)
+        xp[pres] = 1.0
+        xe = project(xt, beta, eta + erode)
+        xe[pres] = 1.0
+        dpb = dproject(xt, beta, eta)
+        dpb[pres] = 0.0
+        dpe = dproject(xt, beta, eta + erode)
+        dpe[pres] = 0.0
+        e = emin + xe ** penal * (1 - emin)
+        de = penal * xe ** (penal - 1) * (1 - emin)
+        u = system.solve(e, xe, f_grid)
+        to_x = lambda g: hap(g * dpe / hs)   # noqa: E731
+        ue = gather_cells(u, dims).reshape(24, -1)
+        ce = np.einsum("in,in->n", ue, ke @ ue).reshape(dims)
+        comp = float(np.sum(f_grid * u))
+        defl = comp / (load_size * modulus)
+        cons = [defl / deflection_limit - 1.0]
+        grads = [to_x(-de * ce / (load_size * modulus)) / deflection_limit]
+        moved = np.any(ue != 0, axis=0)
+        act = (moved & counted.reshape(-1))
+        xa = xe.reshape(-1)[act]
+        ua = ue[:, act]
+        parts = []
+        for cbk in cbs:
+            sig = cbk @ ua
+            sv = VM @ sig
+            vm = np.sqrt(np.maximum(np.einsum("in,in->n", sv, sig), 1e-30))
+            parts.append((cbk, sv, vm, xa * vm / stress_limit))
+        smax = max((float(p[3].max()) for p in parts if p[3].size), default=0.0)
+        sc = max(smax, 1e-30)
+        pm = sc * (sum(float(np.sum((p[3] / sc) ** 8)) for p in parts) / nc) ** (1.0 / 8)
+        kk = smax / max(pm, 1e-30)
+        kappa = 0.5 * (kappa + kk) if it > 1 else kk
+        g = kappa * pm
+        g_xe = np.zeros(ue.shape[1])
+        fe = np.zeros((24, ue.shape[1]))
+        for cbk, sv, vm, srel in parts:
+            dg_ds = kappa * (srel / max(pm, 1e-30)) ** 7 / nc
+            g_xe[act] += dg_ds * (vm / stress_limit)
+            fe[:, act] += (dg_ds * (xa / (vm * stress_limit)))[None, :] * (cbk.T @ sv)
+        rhs = scatter_cells(fe.reshape((24,) + dims), dims)
+        rhs[np.asarray(fixed_grid, bool)] = 0.0
+        lam = system.resolve(rhs)
+        le = gather_cells(lam, dims).reshape(24, -1)
+        g_xe[moved] -= de.reshape(-1)[moved] * np.einsum("in,in->n", le, ke @ ue)[moved]
+        cons.append(g - 1.0)
+        grads.append(to_x(g_xe.reshape(dims)))
+
+        f0 = 10.0 * float(xp[design].mean())
+        df0 = sym(hap(10.0 * design / design.sum() * dpb / hs))
+        grads = [sym(gr) for gr in grads]
+        worst = max(cons)
+        if worst > 0.02 and worst > worst_prev:
+            mma.move = max(0.02, 0.5 * mma.move)
+            mma.tighten(0.5)
+        elif worst <= 0.02:
+            mma.move = min(move_cap, 1.2 * mma.move)
+        worst_prev = worst
+        xf = mma.update(x.reshape(-1)[free], f0, df0.reshape(-1)[free], np.array(cons),
+                        np.array([gr.reshape(-1)[free] for gr in grads]))
+        xnew = x.copy().reshape(-1)
+        xnew[free] = xf
+        xnew = sym(xnew.reshape(dims))
+        change = float(np.abs(xnew - x)[design].max())
+        x = xnew
+        since_beta += 1
+        rec = dict(volume=float(xp[design].mean()), beta=beta, change=change, constraints=list(cons),
+                   deflection=defl, stress=smax * stress_limit, xphys=xp)
+        recs.append(rec)
+        feasible = max(cons) <= 0.02
+        if beta < beta_max and ((feasible and (since_beta >= beta_every or change < 2 * tol))
+                                or since_beta >= 3 * beta_every):
+            beta = min(beta * 2, beta_max)
+            since_beta = 0
+            move_cap = max(0.02, move_cap * 0.6)
+            mma.move = min(mma.move, move_cap)
+        elif beta >= beta_max:
+            if feasible and (best is None or rec["volume"] < best[1]["volume"]):
+                best = (x_now, rec)
+            trail.append(best[1]["volume"] if best is not None else np.inf)
+            if best is not None and ((feasible and change < tol) or (
+                    len(trail) > stall_window and trail[-1] > (1.0 - 5e-3) * trail[-1 - stall_window])):
+                converged = True
+                break
+    if best is not None:
+        x = best[0]
+    return recs, x, converged
+
 # --------------------------------------------------------------------------
 # MMA (loadpath/mma.py:31-214), restated from Svanberg's published method
 # --------------------------------------------------------------------------
@@ -1010,6 +1226,12 @@ class MMA:
         self.asyinit, self.asyincr, self.asydecr = asyinit, asyincr, asydecr
         self.xold1 = self.xold2 = self.low = self.upp = None
         self.iter = 0
+
+    def tighten(self, factor):
+        """Pull the asymptotes toward the last design by factor (loadpath/mma.py:49-55)."""
+        if self.xold1 is not None and self.low is not None:
+            self.low = self.xold1 - factor * (self.xold1 - self.low)
+            self.upp = self.xold1 + factor * (self.upp - self.xold1)
 
     def update(self, x, f0, df0, f, df):
         """One MMA step (loadpath/mma.py:57-112)."""

@@ -4,7 +4,7 @@ Run in a container that has the loadpath source tree (read-only is fine):
 
     LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
 
-(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize; default all but config0,
+(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize constrained; default all but config0,
 which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
@@ -391,6 +391,59 @@ def make_optimize():
     np.savez_compressed(os.path.join(HERE, "optimize.npz"), **out)
 
 
+def make_constrained():
+    """loadpath's minimum-mass loop under stress and deflection limits (loadpath/constrained.py:
+    295-854, optimize_constrained: relaxed von Mises at the cells' corners aggregated by a P-mean
+    with the adaptive normalisation, one adjoint solve per case, MMA on the free cells, its own
+    beta continuation) on the 12x4x6 top3d cantilever (domain_for), from a uniform 0.5, 40
+    iterations, solves at rtol 1e-10. Stored: the domain, the limits, and per iteration the
+    record (volume, beta, change, constraints, deflection and stress readings, solved cells) and
+    the blueprint; and the last design."""
+    os.environ["LOADPATH_HEX8"] = "im"
+    import loadpath.simp as S
+    from loadpath.benchmarks.problems import cantilever_3d
+    from loadpath.benchmarks.run import NU, domain_for
+    from loadpath.constrained import Limits, optimize_constrained
+
+    dims, iters = (12, 4, 6), 40
+    p = cantilever_3d(*dims, 0.3, 1.5)
+    dom, _ = domain_for(p)
+    mesh = dom.mesh
+    assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1
+    lim = Limits(12.0, 0.6, 1000.0)
+    opts = S.SimpOptions(volume_fraction=0.5, filter_radius=p.rmin, max_iterations=iters, solve_rtol=1e-10)
+    recs, xps = [], []
+    res = optimize_constrained(dom, NU, opts, lim, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
+    nxyz = np.array(dims) + 1
+    fixed = np.zeros((3, *nxyz), bool)
+    f = np.zeros((3, *nxyz))
+    nijk = tuple(mesh.node_ijk.T)
+    for c in range(3):
+        fixed[c][nijk] = dom.fixed[c::3]
+        f[c][nijk] = dom.loads[0][c::3]
+    cells = tuple(mesh.elem_ijk.T)
+
+    def grid(v):
+        g = np.zeros(dims, np.asarray(v).dtype)
+        g[cells] = v
+        return g
+
+    axes = {"x": 0, "y": 1, "z": 2}
+    name = dom.case_names[0]
+    out = dict(dims=np.array(dims), pitch=float(mesh.pitch), nu=float(NU), fixed=fixed, f=f, pres=grid(dom.preserve),
+               volfrac=float(opts.volume_fraction), radius=float(opts.filter_radius), pad=bool(S._pad(opts)),
+               mirror=np.array([axes[a] for a in dom.mirror], np.int64), stress_limit=lim.stress,
+               deflection_limit=lim.deflection, modulus=lim.modulus, iterations=len(recs),
+               converged=bool(res.converged), xphys=np.stack([grid(v) for v in xps]), x_last=grid(res.x),
+               constraints=np.array([r["constraints"] for r in recs]),
+               deflection=np.array([r[f"deflection.{name}"] for r in recs]),
+               stress=np.array([r[f"stress.{name}"] for r in recs]),
+               contact=grid((dom.support_nodes | dom.load_nodes)[mesh.enode].any(axis=1)))
+    for k in ("volume", "beta", "change", "solvedCells"):
+        out[k] = np.array([float(r[k]) for r in recs])
+    np.savez_compressed(os.path.join(HERE, "constrained.npz"), **out)
+
+
 def main(names=None):
     gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
             "mma": make_mma,
@@ -399,7 +452,7 @@ def main(names=None):
                                     make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
                                     make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
             "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step,
-            "optimize": make_optimize}
+            "optimize": make_optimize, "constrained": make_constrained}
     for name in names or [k for k in gens if k != "config0"]:
         gens[name]()
 
