@@ -1071,7 +1071,7 @@ def corner_stress_ops(nu, pitch=1.0, element="im"):
     return [c @ hex8_b(a, b, cz, nu, element) / pitch for a in (-1.0, 1.0) for b in (-1.0, 1.0) for cz in (-1.0, 1.0)]
 
 
-def scatter_cells(fe, dims):
+def scatter_cell_vectors(fe, dims):
     """Node field (3, nx+1, ny+1, nz+1) summing per-cell 24-vectors fe (24, nx, ny, nz) onto the
     cells' corners (the transpose of gather_cells)."""
     out = np.zeros((3,) + tuple(d + 1 for d in dims))
@@ -1161,7 +1161,7 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
             dg_ds = kappa * (srel / max(pm, 1e-30)) ** 7 / nc
             g_xe[act] += dg_ds * (vm / stress_limit)
             fe[:, act] += (dg_ds * (xa / (vm * stress_limit)))[None, :] * (cbk.T @ sv)
-        rhs = scatter_cells(fe.reshape((24,) + dims), dims)
+        rhs = scatter_cell_vectors(fe.reshape((24,) + dims), dims)
         rhs[np.asarray(fixed_grid, bool)] = 0.0
         lam = system.resolve(rhs)
         le = gather_cells(lam, dims).reshape(24, -1)
