@@ -297,6 +297,17 @@ int lpb_cell_product(double* out, const double* a, const double* b, const uint8_
  * (loadpath/simp.py:1476-1482 `_symmetrize`, every cell of the box having its mirror image) */
 int lpb_mirror_average(double* v, int axis, int nx, int ny, int nz, int pz, int cpz, void* stream);
 
+/* ---- the minimum-mass loop's cell stresses (loadpath/constrained.py:597-652, corner points):
+ * lpb_stress_pass over the cells that moved and are counted (counted: uint8 cell field, nonzero)
+ * forms the corner stresses C B_k u_e (cb: 8 x 6 x 24 float64 on the device, corners x
+ * outermost, already divided by the pitch), vm = sqrt(s . VM s) and r = xe vm / lim; mode 0:
+ * *out = max r; mode 1: *out = sum (r / sc)^8; mode 2: gxe = sum_k w_k vm_k / lim per cell and fe
+ * (cells_padded x 24) = sum_k w_k xe / (vm_k lim) B_k^T C VM s_k, w_k = kappa (r_k / pm)^7 / nc
+ * (0 on inactive cells). part: 1184 doubles. lpb_cell_vectors_to_nodes sums each node's share of
+ * the cells' 24-vectors into a node field (the adjoint right-hand side). */
+int lpb_stress_pass(int mode, const double* u, const double* xe, const uint8_t* counted, const double* cb, double lim, double sc, double pm, double kappa, double nc, double* part, double* out, double* gxe, double* fe, int nx, int ny, int nz, int pz, int cpz, void* stream);
+int lpb_cell_vectors_to_nodes(double* out, const double* fe, int nx, int ny, int nz, int pz, int cpz, void* stream);
+
 /* ---- CUDA graphs of a stream's work (the solver records one CG iteration per solve) */
 int lpb_capture_begin(void* stream);
 int lpb_capture_end(void* stream, void** exec);

@@ -43,7 +43,7 @@ _KERNELS = {"lpb_modal_ke": 0, "lpb_modal_g1": 0, "lpb_reduce_blocks": 0, "lpb_m
             # the handle's entries launch on its own stream; their kernels are not counted here
             "lpb_mg_create": 0, "lpb_mg_set_moduli": 0, "lpb_mg_solve": 0}
 # entries whose kernel count depends on their arguments
-_VARIABLE = {"lpb_sensitivity": lambda a: 1 + (a[9] is not None),
+_VARIABLE = {"lpb_sensitivity": lambda a: 1 + (a[9] is not None), "lpb_stress_pass": lambda a: 1 + (a[0] < 2),
              "lpb_band_solve_cols_f32": lambda a: a[3] + (a[3] + 7) // 8,
              "lpb_band_solve_cols_f64": lambda a: a[3] + (a[3] + 7) // 8}
 _COUNT = [0]

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-__all__ = ["CORNERS", "hex8_element", "hex8_ke", "elastic_c"]
+__all__ = ["CORNERS", "hex8_element", "hex8_ke", "elastic_c", "hex8_b", "corner_stress_ops"]
 
 CORNERS = np.array([[(k >> a) & 1 for a in range(3)] for k in range(8)])
 _ELEMENTS = ("im", "plain")
@@ -94,3 +94,30 @@ def hex8_ke(nu: float, element: str | None = None) -> np.ndarray:
             raise ValueError(element)
         _CACHE[key] = 0.5 * (k + k.T)
     return _CACHE[key].copy()
+
+
+def hex8_b(pt, nu: float, element: str | None = None) -> np.ndarray:
+    """Strain-displacement matrix (6x24) of the unit cube at the natural point pt: the trilinear
+    field plus, for the incompatible-mode element, the condensed bubbles' strain (zero at the
+    centre) (loadpath/fem.py:227-237). For side h, divide by h."""
+    element = element or hex8_element()
+    b = _strain_op(_corner_grads(pt))
+    if element == "plain":
+        return b
+    c = elastic_c(nu)
+    kua = np.zeros((24, 9))
+    kaa = np.zeros((9, 9))
+    for g in _gauss_points():
+        bg = _strain_op(_corner_grads(g))
+        ba = _strain_op(_bubble_grads(g))
+        kua += 0.125 * bg.T @ c @ ba
+        kaa += 0.125 * ba.T @ c @ ba
+    return b + _strain_op(_bubble_grads(pt)) @ (-np.linalg.solve(kaa, kua.T))
+
+
+def corner_stress_ops(nu: float, pitch: float = 1.0, element: str | None = None) -> np.ndarray:
+    """(8, 6, 24): the stress C B at the cube's eight corners per unit modulus, corners taken with
+    x outermost (loadpath/constrained.py:443-446, its STRESS_POINTS = "corners")."""
+    c = elastic_c(nu)
+    return np.array([c @ hex8_b((a, b, cz), nu, element) / pitch
+                     for a in (-1.0, 1.0) for b in (-1.0, 1.0) for cz in (-1.0, 1.0)])

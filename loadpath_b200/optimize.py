@@ -7,6 +7,9 @@ eroded projection and the filter, the volume's through the blueprint's, the meas
 the optimality-criteria step whose volume multiplier is solved to rounding, beta continuation and
 the stopping rules. Described in its docstring.
 
+`ConstrainedLoop`: loadpath's minimum-mass loop under stress and deflection limits
+(loadpath/constrained.py:295-854, `optimize_constrained`) over the same pieces, with MMA.
+
 `MMALoop`: SIMP with the MMA update and a penalty continuation, its sensitivities from the autograd path.
 
 Each iteration: the penalty p_k = p0 + (p - p0) min(k, ramp) / ramp; compliance c(x) through
@@ -31,12 +34,13 @@ import torch
 
 from ._lib import lib
 from .autograd import Compliance, SimpProblem
+from .fem import corner_stress_ops
 from .grid import ptr, stream_handle
 from .mg import BoxMesh, GridElasticity
 from .mma import MMA
 from .simp import MG_MIN_CELLS, SUB_REUSE, DeviceFilter, LiveCells, ProjectedDesign, _cells_touching
 
-__all__ = ["MMALoop", "OptimizeLoop", "SimpOptions", "E_MIN", "PENALTY"]
+__all__ = ["MMALoop", "OptimizeLoop", "ConstrainedLoop", "Limits", "SimpOptions", "E_MIN", "PENALTY"]
 
 E_MIN = 1e-6          # void modulus of loadpath's SIMP loop (loadpath/simp.py:42)
 PENALTY = 3.0         # SIMP exponent (loadpath/simp.py:55)
@@ -387,3 +391,236 @@ class OptimizeLoop:
 
     def x_host(self):
         return self.grid.cells_to_host(self.x)
+
+
+@dataclass
+class Limits:
+    """The limits of loadpath's minimum-mass loop (loadpath/constrained.py:117-144): the allowable
+    peak von Mises stress (MPa) and deflection at the loads (mm), either None, and the modulus
+    (MPa) that turns unit-modulus displacements into mm. The reference's buckling, layer-bond,
+    contact-band and averaging-radius options are not run here."""
+    stress: float | None
+    deflection: float | None
+    modulus: float
+
+
+STRESS_P = 8.0        # the P-mean's exponent (loadpath/constrained.py:46)
+STALL_GAIN = 5e-3     # the lightest feasible design's gain that ends the run (loadpath/constrained.py:66)
+
+
+class ConstrainedLoop:
+    """loadpath's minimum-mass loop under stress and deflection limits (loadpath/constrained.py:
+    295-854, `optimize_constrained` with Limits(stress, deflection, modulus) and default options)
+    on the device. Per iteration: the blueprint and eroded designs, the solves (as OptimizeLoop:
+    live cells, warm starts); per case with a deflection limit, the deflection f.u / (sum_n |f_n| E)
+    and its gradient -dE ce / (sum |f| E) through the eroded projection and the filter; per case,
+    with a stress limit, the relaxed von Mises ratio xe vm / limit at the 8 corners of every cell
+    that moved and touches no support or load (lpb_stress_pass), its P-mean (P = 8) scaled by
+    Le et al.'s adaptive normalisation, the adjoint solve on the same system (the right-hand side
+    gathered by lpb_cell_vectors_to_nodes) and its gradient; the objective 10 mean(xp) over the
+    design cells; one MMA step on the free cells (move 0.1 capped; halved with the asymptotes
+    tightened while the worst constraint grows above 0.02, grown by 1.2 up to the cap inside); the
+    loop's own beta continuation (once feasible, or after three holds; the cap times 0.6) and, at
+    beta_max, the lightest feasible design kept and the run stopped on a feasible small change or
+    a stalled volume. Constraints come in the reference's order: deflections, then stresses.
+
+    Arguments as OptimizeLoop's, with limits: Limits."""
+
+    def __init__(self, dims, fixed_grid, loads, nu, opts: SimpOptions, limits: Limits, preserve=None,
+                 pitch=1.0, mirror=(), element="im", dtype=np.float32, coarse_cells=2000, maxiter=2000,
+                 live_cells=True, device="cuda"):
+        if limits.stress is None and limits.deflection is None:
+            raise ValueError("optimize_constrained needs a stress or deflection limit")
+        base = OptimizeLoop(dims, fixed_grid, loads, nu, opts, preserve=preserve, pitch=pitch, mirror=mirror,
+                            element=element, dtype=dtype, coarse_cells=coarse_cells, maxiter=maxiter,
+                            live_cells=live_cells, device=device)
+        self.base, self.opts, self.limits = base, opts, limits
+        g = base.grid
+        self.grid, self.dims, self.pitch = g, base.dims, float(pitch)
+        cases = list(loads) if isinstance(loads, (list, tuple)) else [loads]
+        f = [np.asarray(c, np.float64).reshape(g.node_shape) for c in cases]
+        self.load_size = [float(np.linalg.norm(fk.reshape(3, -1), axis=0).sum()) for fk in f]
+        self.defl_cases = [c for c in range(len(f)) if limits.deflection is not None and self.load_size[c] > 0]
+        self.stress_cases = list(range(len(f))) if limits.stress is not None else []
+        self.m = len(self.defl_cases) + len(self.stress_cases)
+        # stress is not counted in the cells the loads and supports touch
+        held = np.asarray(fixed_grid, bool).reshape(g.node_shape).any(axis=0)
+        loaded = np.zeros(g.node_shape[1:], bool)
+        for fk in f:
+            loaded |= (fk != 0).any(axis=0)
+        counted = ~_cells_touching(held | loaded)
+        self.counted = g.set_cells(g.cell_field(torch.uint8), torch.from_numpy(counted.astype(np.uint8)))
+        self.nc = float(max(int(counted.sum()), 1) * 8)
+        # C B_k / pitch acts on the reference's displacement; the solver's is pitch times it
+        self.cb = torch.tensor(corner_stress_ops(nu, self.pitch, element) / self.pitch, dtype=torch.float64,
+                               device=g.device).reshape(-1).contiguous()
+        pres = np.zeros(self.dims, bool) if preserve is None else np.asarray(preserve, bool)
+        design = ~pres
+        self.n_design = int(design.sum())
+        # the design cells' positions in the padded cell layout, in grid (C) order as the reference's
+        # flatnonzero(design)
+        xs, ys, zs = np.nonzero(design)
+        pos = (((zs >> 2) * g.ny + ys) * g.nx + xs) * 4 + (zs & 3)
+        self.free = torch.from_numpy(pos.astype(np.int64)).to(g.device)
+        self.mma = MMA(self.free.numel(), self.m, 0.0, 1.0, min(opts.move, 0.1), device=device)
+        self.move_cap = self.mma.move
+        self.worst_prev = math.inf
+        self.kappa = [1.0] * len(f)
+        self.lams = [None] * len(f)
+        cf = lambda: g.cell_field(torch.float64)   # noqa: E731
+        self.gxe, self.df0 = cf(), cf()
+        self.grads = [cf() for _ in range(self.m)]
+        self.g0 = g.cells_to_dev(10.0 * design / design.sum(), torch.float64)
+        self.fe = torch.zeros(g.n_cell_field * 24, dtype=torch.float64, device=g.device)
+        self.rhs = g.node_field(torch.float64)
+        self._part = torch.zeros(4096, dtype=torch.float64, device=g.device)
+        self._s = torch.zeros(4, dtype=torch.float64, device=g.device)
+        self.beta = float(opts.beta_start)
+        self.since_beta = 0
+        self.it = 0
+        self.history = []
+        self.best = None
+        self.trail = []
+        self.converged = False
+
+    def _stress(self, c, u, pos):
+        """The stress constraint of case c (loadpath/constrained.py:597-652): its value g - 1 and its
+        gradient in grads[pos] (before the filter chain), the adjoint solved on the last system."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        b = self.base
+        lim = float(self.limits.stress)
+        args = (u.data_ptr(), b.xe.data_ptr(), self.counted.data_ptr(), self.cb.data_ptr(), lim)
+        L.lpb_stress_pass(0, *args, 0.0, 0.0, 0.0, self.nc, self._part.data_ptr(), self._s.data_ptr(), None, None,
+                          *g.args, st)
+        smax = float(self._s[0].item())
+        sc = max(smax, 1e-30)
+        L.lpb_stress_pass(1, *args, sc, 0.0, 0.0, self.nc, self._part.data_ptr(), self._s[1:].data_ptr(), None,
+                          None, *g.args, st)
+        pm = sc * (float(self._s[1].item()) / self.nc) ** (1.0 / STRESS_P)
+        k = smax / max(pm, 1e-30)
+        self.kappa[c] = 0.5 * (self.kappa[c] + k) if self.it > 1 else k
+        L.lpb_stress_pass(2, *args, sc, pm, self.kappa[c], self.nc, None, None, self.gxe.data_ptr(),
+                          self.fe.data_ptr(), *g.args, st)
+        L.lpb_cell_vectors_to_nodes(self.rhs.data_ptr(), self.fe.data_ptr(), *g.args, st)
+        lam = b.ge.solve_device(self.rhs, self.lams[c])
+        self.lams[c] = lam
+        # - dE lam_e . Ke u_e (loadpath/constrained.py:649-650): lam and u both the solver's
+        b.ge.strain_energy_device(u, lam, out=b.ce)
+        L.lpb_sensitivity(self.gxe.data_ptr(), b.xe.data_ptr(), b.ce.data_ptr(), b.e.data_ptr(), PENALTY, E_MIN, 1.0,
+                          1, self._part.data_ptr(), None, *g.args, st)
+        b.pd.chain(self.grads[pos], self.gxe, b.dproj_e)
+        return self.kappa[c] * pm - 1.0, smax * lim
+
+    def step(self):
+        """One iteration; returns its record (the reference's keys; the readings per case in
+        "deflection" and "stress" lists)."""
+        L = lib()
+        g = self.grid
+        st = stream_handle()
+        o, b, lim = self.opts, self.base, self.limits
+        self.it += 1
+        b.it = self.it
+        beta = self.beta
+        eta, eta_e = o.eta, o.eta + o.erode
+        x_now = b.x.clone()
+        vol_b = b.pd.physical(b.x, beta, eta, xp=b.xp, dxp=b.dproj)
+        L.lpb_project(b.xe.data_ptr(), b.dproj_e.data_ptr(), b.pd.xt.data_ptr(), beta, eta_e, b.flags.data_ptr(),
+                      None, None, None, *g.args, st)
+        L.lpb_simp_law(b.e.data_ptr(), b.xe.data_ptr(), PENALTY, E_MIN, *g.args, st)
+        b.ge.rtol = o.solve_rtol
+        b._solve(o.solve_rtol)   # the cases' displacements in b.us (its compliance sums are not used here)
+        cons, defl, stress = [], [], []
+        pos = 0
+        for c in self.defl_cases:
+            u, fk = b.us[c], b.fs[c]
+            d = b._dot(fk, u) / (self.load_size[c] * lim.modulus * self.pitch)
+            b.ge.strain_energy_device(u, out=b.ce)
+            L.lpb_sensitivity(self.gxe.data_ptr(), b.xe.data_ptr(), b.ce.data_ptr(), b.e.data_ptr(), PENALTY, E_MIN,
+                              1.0 / (self.load_size[c] * lim.modulus * self.pitch * lim.deflection), 0,
+                              self._part.data_ptr(), None, *g.args, st)
+            b.pd.chain(self.grads[pos], self.gxe, b.dproj_e)
+            cons.append(d / lim.deflection - 1.0)
+            defl.append(d)
+            pos += 1
+        for c in self.stress_cases:
+            v, smax = self._stress(c, b.us[c], pos)
+            cons.append(v)
+            stress.append(smax)
+            pos += 1
+        f0 = 10.0 * vol_b / self.n_design
+        b.pd.chain(self.df0, self.g0, b.dproj)
+        for ax in b.mirror:
+            L.lpb_mirror_average(self.df0.data_ptr(), ax, *g.args, st)
+            for gr in self.grads:
+                L.lpb_mirror_average(gr.data_ptr(), ax, *g.args, st)
+        worst = max(cons)
+        if worst > 0.02 and worst > self.worst_prev:
+            self.mma.move = max(0.02, 0.5 * self.mma.move)
+            self.mma.tighten(0.5)
+        elif worst <= 0.02:
+            self.mma.move = min(self.move_cap, 1.2 * self.mma.move)
+        self.worst_prev = worst
+        xf = b.x.reshape(-1)[self.free]
+        dfs = torch.stack([gr.reshape(-1)[self.free] for gr in self.grads])
+        xnew = self.mma.update(xf, f0, self.df0.reshape(-1)[self.free], np.array(cons), dfs)
+        b.xn = b.x.clone()
+        b.xn.reshape(-1)[self.free] = xnew
+        for ax in b.mirror:
+            L.lpb_mirror_average(b.xn.data_ptr(), ax, *g.args, st)
+        L.lpb_max_abs_diff_f64(b.xn.data_ptr(), b.x.data_ptr(), b.n, self._part.data_ptr(), self._s[2:].data_ptr(), st)
+        change = float(self._s[2].item())
+        b.x = b.xn
+        self.since_beta += 1
+        its = b.ge.last_iters
+        rec = {"iteration": self.it, "volume": vol_b / self.n_design, "beta": beta, "change": change,
+               "constraints": [float(v) for v in cons], "deflection": defl, "stress": stress,
+               "cgIterations": max(its) if isinstance(its, (list, tuple)) else its, "reduced": b.reduced}
+        self.history.append(rec)
+        self._continue(rec, x_now)
+        return rec
+
+    def _continue(self, rec, x_now):
+        """The loop's continuation, lightest-design record and stopping rules
+        (loadpath/constrained.py:789-829)."""
+        o = self.opts
+        feasible = max(rec["constraints"]) <= 0.02
+        change = rec["change"]
+        if self.beta < o.beta_max and ((feasible and (self.since_beta >= o.beta_every or change < 2 * o.tol))
+                                       or self.since_beta >= 3 * o.beta_every):
+            self.beta = min(self.beta * 2, o.beta_max)
+            self.since_beta = 0
+            self.move_cap = max(0.02, self.move_cap * 0.6)
+            self.mma.move = min(self.mma.move, self.move_cap)
+        elif self.beta >= o.beta_max:
+            if feasible and (self.best is None or rec["volume"] < self.best[1]["volume"]):
+                self.best = (x_now, rec)
+            self.trail.append(self.best[1]["volume"] if self.best is not None else math.inf)
+            w = o.stall_window
+            if self.best is not None and ((feasible and change < o.tol) or (
+                    len(self.trail) > w and self.trail[-1] > (1.0 - STALL_GAIN) * self.trail[-1 - w])):
+                self.converged = True
+
+    def run(self, on_iter=None):
+        """Iterate until a stopping rule holds or max_iterations; the design becomes the lightest
+        feasible one checked at beta_max when there is one (loadpath/constrained.py:831-839)."""
+        while self.it < self.opts.max_iterations and not self.converged:
+            rec = self.step()
+            if on_iter is not None:
+                on_iter(rec)
+        if self.best is not None:
+            self.base.x = self.best[0]
+        return self.history
+
+    @property
+    def x(self):
+        return self.base.x
+
+    def x_host(self):
+        return self.grid.cells_to_host(self.base.x)
+
+    @property
+    def xp(self):
+        """The blueprint the last iteration started from."""
+        return self.base.xp
