@@ -265,7 +265,8 @@ class GridElasticity:
 
     mesh: any object with elem_ijk (ne, 3), node_ijk (nn, 3) and pitch (a loadpath
     HexMesh or BoxMesh); nu: Poisson's ratio; fixed: bool per mesh dof. springs/lowrank are
-    not supported on this path (the benchmark problems have none)."""
+    not supported on this path (the benchmark problems have none). device: a CUDA device, or any
+    other name ("cpu", "auto", None) for the default CUDA device."""
 
     def __init__(self, mesh, nu, fixed, springs=None, rtol=1e-6, maxiter=500, coarse_cells=2000, degree=2,
                  dtype=np.float32, lu_max_dofs=60_000, device=None, lowrank=None, smoother="chebyshev",
@@ -286,7 +287,11 @@ class GridElasticity:
         self.lu_max_dofs = int(lu_max_dofs)
         self.smoother = smoother
         self.omega = float(omega)
-        self.device = torch.device(device if device not in (None, "b200", "auto") else "cuda")
+        # every solve of this package runs on a CUDA device: a caller's "cpu" (loadpath's build
+        # simulation asks for it, loadpath/buildsim.py:612) selects the default one as "auto" does
+        dev = torch.device(device) if isinstance(device, (str, torch.device)) and str(device).startswith("cuda") \
+            else torch.device("cuda")
+        self.device = dev
         cells = np.asarray(mesh.elem_ijk).max(axis=0) + 1
         cells = cells + cells % 2
         self.cells = tuple(int(c) for c in cells)

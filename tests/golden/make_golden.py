@@ -4,7 +4,7 @@ Run in a container that has the loadpath source tree (read-only is fine):
 
     LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
 
-(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize constrained; default all but config0,
+(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize constrained callers; default all but config0,
 which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
@@ -444,6 +444,55 @@ def make_constrained():
     np.savez_compressed(os.path.join(HERE, "constrained.npz"), **out)
 
 
+def make_callers():
+    """Two other users of GridElasticity, on a mesh that is not a full box (an L-shaped part:
+    a 12x6x8 box at pitch 0.5 without its upper +x quarter), held at its base:
+    - verification's re-solve on a delivered grid (loadpath/verify.py:1689-1704): one
+      set_moduli with per-cell moduli, two right-hand sides through solve_many;
+    - the build simulation's layer-by-layer solves (loadpath/buildsim.py:609-640): one solver,
+      set_moduli(e * active) as each layer of cells is added (the cells not yet built at modulus
+      0), one load per layer on the built nodes.
+    Solves at rtol 1e-10; the reference's own GridElasticity (device "cpu")."""
+    os.environ["LOADPATH_HEX8"] = "im"
+    from loadpath.fem import HexMesh
+    from loadpath.mg import GridElasticity
+
+    rng = np.random.default_rng(12)
+    full = np.ones((12, 6, 8), bool)
+    full[6:, :, 4:] = False
+    mesh = HexMesh(np.argwhere(full), 0.5, np.zeros(3))
+    fixed = np.zeros(mesh.n_dof, bool)
+    base = np.flatnonzero(mesh.node_ijk[:, 2] == 0)
+    for i in range(3):
+        fixed[3 * base + i] = True
+    e = 1700.0 * (0.5 + rng.random(mesh.n_elem))
+    top = mesh.node_ijk[:, 2] == mesh.node_ijk[:, 2].max()
+    f1 = np.zeros(mesh.n_dof)
+    f1[3 * np.flatnonzero(top) + 2] = -1.0
+    f2 = np.zeros(mesh.n_dof)
+    f2[3 * np.flatnonzero(mesh.node_ijk[:, 0] == mesh.node_ijk[:, 0].max()) + 1] = 0.5
+    ge = GridElasticity(mesh, 0.3, fixed, rtol=1e-10, maxiter=3000, device="cpu")
+    ge.set_moduli(e)
+    us = ge.solve_many([f1, f2])
+    out = dict(elem_ijk=mesh.elem_ijk, node_ijk=mesh.node_ijk, pitch=float(mesh.pitch), fixed=fixed, e=e, f1=f1,
+               f2=f2, verify_u1=us[0], verify_u2=us[1], verify_iters=np.array(ge.last_iters))
+    ge2 = GridElasticity(mesh, 0.3, fixed, rtol=1e-10, maxiter=3000, device="cpu")
+    layers = int(mesh.elem_ijk[:, 2].max()) + 1
+    for li in range(layers):
+        active = mesh.elem_ijk[:, 2] <= li
+        node_on = np.zeros(mesh.n_nodes, bool)
+        node_on[mesh.enode[active].ravel()] = True
+        f = np.where(np.repeat(node_on, 3), rng.standard_normal(mesh.n_dof), 0.0)
+        f[fixed] = 0.0
+        ge2.set_moduli(e * active)
+        du = ge2.solve_many([f])[0]
+        out[f"layer{li}_f"] = f
+        out[f"layer{li}_u"] = du
+        out[f"layer{li}_iters"] = np.array(ge2.last_iters)
+    out["layers"] = layers
+    np.savez_compressed(os.path.join(HERE, "callers.npz"), **out)
+
+
 def main(names=None):
     gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
             "mma": make_mma,
@@ -452,7 +501,7 @@ def main(names=None):
                                     make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
                                     make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
             "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step,
-            "optimize": make_optimize, "constrained": make_constrained}
+            "optimize": make_optimize, "constrained": make_constrained, "callers": make_callers}
     for name in names or [k for k in gens if k != "config0"]:
         gens[name]()
 
