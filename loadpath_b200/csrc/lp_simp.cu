@@ -305,13 +305,15 @@ __global__ void __launch_bounds__(256, 2) k_oc_volumes(const double* __restrict_
   }
 }
 
+// the nl volumes from the blocks' partial sums: one warp per multiplier, its lanes striding over
+// the blocks, then a shuffle tree (a fixed order, so the sums are the same every run)
 __global__ void k_oc_final(const double* __restrict__ part, int nblocks, int nl, double* __restrict__ out) {
-  __shared__ double sh[32];
-  for (int j = 0; j < nl; ++j) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int j = threadIdx.x >> 5; j < nl; j += nw) {
     double s = 0.0;
-    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) s += part[(long long)j * nblocks + i];
-    s = lp_block_sum(s, sh);
-    if (threadIdx.x == 0) out[j] = s;
+    for (int i = lane; i < nblocks; i += 32) s += part[(long long)j * nblocks + i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[j] = s;
   }
 }
 

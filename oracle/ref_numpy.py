@@ -1085,7 +1085,8 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
                      pres=None, pad=True, pitch=1.0, mirror=(), eta=0.5, erode=0.15, move=0.2, tol=0.01,
                      beta_max=32.0, beta_every=10, stall_window=6, emin=1e-6, penal=3.0, element="im", reuse=6):
     """loadpath's minimum-mass loop under a stress and a deflection limit for one load case
-    (loadpath/constrained.py:295-854 with Limits(stress, deflection, modulus) and default options):
+    (loadpath/constrained.py:295-854 with Limits(stress, deflection, modulus) and default options;
+    either limit may be None):
     per iteration the blueprint and eroded designs, the solve on the live cells (LiveSystem, as
     optimize_loop) and the adjoint solves on the same system, the deflection f.u / (sum_n |f_n| E) against its limit with gradient
     -dE ce / (sum |f| E); the relaxed von Mises xe * vm(C B_k u_e) / limit at the 8 corners of every
@@ -1114,7 +1115,8 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
     sym = (lambda v: mirror_average(v, mirror)) if mirror else (lambda v: v)   # noqa: E731
     x = np.full(dims, vf0)
     x[pres] = 1.0
-    mma = MMA(len(free), 2, 0.0, 1.0, move=min(move, 0.1))
+    mma = MMA(len(free), int(deflection_limit is not None) + int(stress_limit is not None), 0.0, 1.0,
+              move=min(move, 0.1))
     move_cap = mma.move
     worst_prev, kappa, beta, since_beta = np.inf, 1.0, 1.0, 0
     best, trail, recs, converged = None, [], [], False
@@ -1137,37 +1139,40 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
         ce = np.einsum("in,in->n", ue, ke @ ue).reshape(dims)
         comp = float(np.sum(f_grid * u))
         defl = comp / (load_size * modulus)
-        cons = [defl / deflection_limit - 1.0]
-        grads = [to_x(-de * ce / (load_size * modulus)) / deflection_limit]
-        moved = np.any(ue != 0, axis=0)
-        act = (moved & counted.reshape(-1))
-        xa = xe.reshape(-1)[act]
-        ua = ue[:, act]
-        parts = []
-        for cbk in cbs:
-            sig = cbk @ ua
-            sv = VM @ sig
-            vm = np.sqrt(np.maximum(np.einsum("in,in->n", sv, sig), 1e-30))
-            parts.append((cbk, sv, vm, xa * vm / stress_limit))
-        smax = max((float(p[3].max()) for p in parts if p[3].size), default=0.0)
-        sc = max(smax, 1e-30)
-        pm = sc * (sum(float(np.sum((p[3] / sc) ** 8)) for p in parts) / nc) ** (1.0 / 8)
-        kk = smax / max(pm, 1e-30)
-        kappa = 0.5 * (kappa + kk) if it > 1 else kk
-        g = kappa * pm
-        g_xe = np.zeros(ue.shape[1])
-        fe = np.zeros((24, ue.shape[1]))
-        for cbk, sv, vm, srel in parts:
-            dg_ds = kappa * (srel / max(pm, 1e-30)) ** 7 / nc
-            g_xe[act] += dg_ds * (vm / stress_limit)
-            fe[:, act] += (dg_ds * (xa / (vm * stress_limit)))[None, :] * (cbk.T @ sv)
-        rhs = scatter_cell_vectors(fe.reshape((24,) + dims), dims)
-        rhs[np.asarray(fixed_grid, bool)] = 0.0
-        lam = system.resolve(rhs)
-        le = gather_cells(lam, dims).reshape(24, -1)
-        g_xe[moved] -= de.reshape(-1)[moved] * np.einsum("in,in->n", le, ke @ ue)[moved]
-        cons.append(g - 1.0)
-        grads.append(to_x(g_xe.reshape(dims)))
+        cons, grads, smax = [], [], np.nan
+        if deflection_limit is not None:
+            cons.append(defl / deflection_limit - 1.0)
+            grads.append(to_x(-de * ce / (load_size * modulus)) / deflection_limit)
+        if stress_limit is not None:
+            moved = np.any(ue != 0, axis=0)
+            act = (moved & counted.reshape(-1))
+            xa = xe.reshape(-1)[act]
+            ua = ue[:, act]
+            parts = []
+            for cbk in cbs:
+                sig = cbk @ ua
+                sv = VM @ sig
+                vm = np.sqrt(np.maximum(np.einsum("in,in->n", sv, sig), 1e-30))
+                parts.append((cbk, sv, vm, xa * vm / stress_limit))
+            smax = max((float(p[3].max()) for p in parts if p[3].size), default=0.0)
+            sc = max(smax, 1e-30)
+            pm = sc * (sum(float(np.sum((p[3] / sc) ** 8)) for p in parts) / nc) ** (1.0 / 8)
+            kk = smax / max(pm, 1e-30)
+            kappa = 0.5 * (kappa + kk) if it > 1 else kk
+            g = kappa * pm
+            g_xe = np.zeros(ue.shape[1])
+            fe = np.zeros((24, ue.shape[1]))
+            for cbk, sv, vm, srel in parts:
+                dg_ds = kappa * (srel / max(pm, 1e-30)) ** 7 / nc
+                g_xe[act] += dg_ds * (vm / stress_limit)
+                fe[:, act] += (dg_ds * (xa / (vm * stress_limit)))[None, :] * (cbk.T @ sv)
+            rhs = scatter_cell_vectors(fe.reshape((24,) + dims), dims)
+            rhs[np.asarray(fixed_grid, bool)] = 0.0
+            lam = system.resolve(rhs)
+            le = gather_cells(lam, dims).reshape(24, -1)
+            g_xe[moved] -= de.reshape(-1)[moved] * np.einsum("in,in->n", le, ke @ ue)[moved]
+            cons.append(g - 1.0)
+            grads.append(to_x(g_xe.reshape(dims)))
 
         f0 = 10.0 * float(xp[design].mean())
         df0 = sym(hap(10.0 * design / design.sum() * dpb / hs))
@@ -1188,7 +1193,8 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
         x = xnew
         since_beta += 1
         rec = dict(volume=float(xp[design].mean()), beta=beta, change=change, constraints=list(cons),
-                   deflection=defl, stress=smax * stress_limit, xphys=xp)
+                   deflection=defl if deflection_limit is not None else np.nan,
+                   stress=smax * stress_limit if stress_limit is not None else np.nan, xphys=xp)
         recs.append(rec)
         feasible = max(cons) <= 0.02
         if beta < beta_max and ((feasible and (since_beta >= beta_every or change < 2 * tol))

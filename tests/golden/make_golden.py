@@ -395,8 +395,10 @@ def make_constrained():
     """loadpath's minimum-mass loop under stress and deflection limits (loadpath/constrained.py:
     295-854, optimize_constrained: relaxed von Mises at the cells' corners aggregated by a P-mean
     with the adaptive normalisation, one adjoint solve per case, MMA on the free cells, its own
-    beta continuation) on the 12x4x6 top3d cantilever (domain_for), from a uniform 0.5, 40
-    iterations, solves at rtol 1e-10. Stored: the domain, the limits, and per iteration the
+    beta continuation) on top3d cantilevers (domain_for), from a uniform 0.5, solves at rtol
+    1e-10: both limits on the 12x4x6 one for 40 iterations (constrained.npz), a deflection limit
+    alone and a stress limit alone on a 16x4x8 one for 30 (constrained_deflection.npz,
+    constrained_stress.npz). Stored: the domain, the limits, and per iteration the
     record (volume, beta, change, constraints, deflection and stress readings, solved cells) and
     the blueprint; and the last design."""
     os.environ["LOADPATH_HEX8"] = "im"
@@ -405,12 +407,17 @@ def make_constrained():
     from loadpath.benchmarks.run import NU, domain_for
     from loadpath.constrained import Limits, optimize_constrained
 
-    dims, iters = (12, 4, 6), 40
+    for tag, dims, iters, lim in (("", (12, 4, 6), 40, Limits(12.0, 0.6, 1000.0)),
+                                  ("_deflection", (16, 4, 8), 30, Limits(None, 0.5, 1000.0)),
+                                  ("_stress", (16, 4, 8), 30, Limits(9.0, None, 1000.0))):
+        _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim)
+
+
+def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim):
     p = cantilever_3d(*dims, 0.3, 1.5)
     dom, _ = domain_for(p)
     mesh = dom.mesh
     assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1
-    lim = Limits(12.0, 0.6, 1000.0)
     opts = S.SimpOptions(volume_fraction=0.5, filter_radius=p.rmin, max_iterations=iters, solve_rtol=1e-10)
     recs, xps = [], []
     res = optimize_constrained(dom, NU, opts, lim, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
@@ -432,16 +439,17 @@ def make_constrained():
     name = dom.case_names[0]
     out = dict(dims=np.array(dims), pitch=float(mesh.pitch), nu=float(NU), fixed=fixed, f=f, pres=grid(dom.preserve),
                volfrac=float(opts.volume_fraction), radius=float(opts.filter_radius), pad=bool(S._pad(opts)),
-               mirror=np.array([axes[a] for a in dom.mirror], np.int64), stress_limit=lim.stress,
-               deflection_limit=lim.deflection, modulus=lim.modulus, iterations=len(recs),
-               converged=bool(res.converged), xphys=np.stack([grid(v) for v in xps]), x_last=grid(res.x),
-               constraints=np.array([r["constraints"] for r in recs]),
-               deflection=np.array([r[f"deflection.{name}"] for r in recs]),
-               stress=np.array([r[f"stress.{name}"] for r in recs]),
+               mirror=np.array([axes[a] for a in dom.mirror], np.int64),
+               stress_limit=np.nan if lim.stress is None else lim.stress,
+               deflection_limit=np.nan if lim.deflection is None else lim.deflection, modulus=lim.modulus,
+               iterations=len(recs), converged=bool(res.converged), xphys=np.stack([grid(v) for v in xps]),
+               x_last=grid(res.x), constraints=np.array([r["constraints"] for r in recs]),
+               deflection=np.array([r.get(f"deflection.{name}", np.nan) for r in recs]),
+               stress=np.array([r.get(f"stress.{name}", np.nan) for r in recs]),
                contact=grid((dom.support_nodes | dom.load_nodes)[mesh.enode].any(axis=1)))
     for k in ("volume", "beta", "change", "solvedCells"):
         out[k] = np.array([float(r[k]) for r in recs])
-    np.savez_compressed(os.path.join(HERE, "constrained.npz"), **out)
+    np.savez_compressed(os.path.join(HERE, f"constrained{tag}.npz"), **out)
 
 
 def make_callers():

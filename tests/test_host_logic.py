@@ -228,3 +228,63 @@ def test_optimize_loop_beta_continuation_and_stops():
     hist += [{"compliance": 8.30}, {"compliance": 8.30}]
     lp._continue(change=0.05, move=0.2, comp=8.30, held=False)
     assert lp.converged               # against 8.31: within 2e-3
+
+
+def _constrained_state(**kw):
+    from types import SimpleNamespace
+
+    from loadpath_b200.optimize import ConstrainedLoop, SimpOptions
+
+    lp = object.__new__(ConstrainedLoop)
+    lp.opts = SimpOptions(volume_fraction=0.5, filter_radius=1.5, **kw.pop("opts", {}))
+    lp.mma = SimpleNamespace(move=0.1)
+    lp.move_cap = 0.1
+    lp.beta, lp.since_beta = 1.0, 0
+    lp.best, lp.trail, lp.converged = None, [], False
+    for key, v in kw.items():
+        setattr(lp, key, v)
+    return lp
+
+
+def test_constrained_loop_continuation_and_stops():
+    """ConstrainedLoop's rules (loadpath/constrained.py:789-829): beta doubles only once the design
+    is feasible (worst constraint <= 0.02) after beta_every iterations or a small change, or after
+    three holds whatever; each doubling shrinks the move cap by 0.6 (floor 0.02) and the move to it;
+    at beta_max the lightest feasible design is kept, and the run stops on a feasible change under
+    tol or when the kept volume gained under STALL_GAIN over stall_window iterations."""
+    rec = lambda v, c, ch: {"volume": v, "constraints": c, "change": ch}   # noqa: E731
+    # infeasible after the usual hold: no doubling
+    lp = _constrained_state(since_beta=10)
+    lp._continue(rec(0.4, [0.05, -0.1], 0.05), "x")
+    assert lp.beta == 1.0
+    # feasible after the hold: doubling, the cap 0.06
+    lp = _constrained_state(since_beta=10)
+    lp._continue(rec(0.4, [0.01, -0.1], 0.05), "x")
+    assert (lp.beta, lp.since_beta) == (2.0, 0) and abs(lp.move_cap - 0.06) < 1e-15 and lp.mma.move == lp.move_cap
+    # feasible with a small change before the hold: doubling
+    lp = _constrained_state(since_beta=2)
+    lp._continue(rec(0.4, [0.0], 0.015), "x")
+    assert lp.beta == 2.0
+    # three holds, infeasible: doubling all the same
+    lp = _constrained_state(since_beta=30)
+    lp._continue(rec(0.4, [0.3], 0.05), "x")
+    assert lp.beta == 2.0
+    # the cap's floor
+    lp = _constrained_state(since_beta=10, move_cap=0.03)
+    lp._continue(rec(0.4, [0.0], 0.05), "x")
+    assert lp.move_cap == 0.02
+    # at beta_max: the lightest feasible design is kept; an infeasible one is not
+    lp = _constrained_state(beta=32.0)
+    lp._continue(rec(0.40, [0.01], 0.05), "x1")
+    lp._continue(rec(0.38, [0.10], 0.05), "x2")
+    lp._continue(rec(0.39, [0.00], 0.05), "x3")
+    assert lp.best[0] == "x3" and lp.trail == [0.40, 0.40, 0.39] and not lp.converged
+    # a feasible small change stops
+    lp._continue(rec(0.389, [0.0], 0.005), "x4")
+    assert lp.converged and lp.best[0] == "x4"
+    # the stall over stall_window = 6 kept volumes
+    lp = _constrained_state(beta=32.0)
+    for k in range(7):
+        lp._continue(rec(0.40 - 1e-4 * k, [0.0], 0.05), f"x{k}")
+        assert not lp.converged or k == 6
+    assert lp.converged   # 0.3994 against 0.40 six records back: under STALL_GAIN

@@ -288,20 +288,23 @@ def test_oracle_optimize_loop_matches_reference_run(case):
         assert k("solvedCells")[-1] < np.prod(dims)
 
 
-def test_oracle_constrained_loop_matches_reference_run():
+@pytest.mark.parametrize("tag", ["", "_deflection", "_stress"])
+def test_oracle_constrained_loop_matches_reference_run(tag):
     """The oracle's restatement of loadpath's minimum-mass loop under stress and deflection limits
     (constrained_loop) against the reference's own optimize_constrained on the 12x4x6 cantilever
     (tests/golden/constrained.npz, 40 iterations, beta 1 to 8, the last ones on a reduced system
-    the direct path reuses): every iteration's constraints, readings, volume, change and
-    blueprint, and the last design; and the cells whose stress is not counted."""
-    g = _load("constrained.npz")
+    the direct path reuses; and a deflection limit or a stress limit alone on a 16x4x8 cantilever,
+    30 iterations): every iteration's constraints, readings, volume, change and blueprint, and the
+    last design; and the cells whose stress is not counted."""
+    g = _load(f"constrained{tag}.npz")
     dims = tuple(int(d) for d in g["dims"])
+    lim = lambda key: None if np.isnan(float(g[key])) else float(g[key])   # noqa: E731
     held = g["fixed"].any(axis=0)
     loaded = (g["f"] != 0).any(axis=0)
     np.testing.assert_array_equal(R.cells_touching(held | loaded), g["contact"])
     recs, x, conv = R.constrained_loop(dims, float(g["nu"]), g["fixed"], g["f"], float(g["volfrac"]),
-                                       float(g["radius"]), int(g["iterations"]), float(g["stress_limit"]),
-                                       float(g["deflection_limit"]), float(g["modulus"]), pres=g["pres"],
+                                       float(g["radius"]), int(g["iterations"]), lim("stress_limit"),
+                                       lim("deflection_limit"), float(g["modulus"]), pres=g["pres"],
                                        pad=bool(g["pad"]), pitch=float(g["pitch"]),
                                        mirror=tuple(int(a) for a in g["mirror"]))
     assert conv == bool(g["converged"]) and len(recs) == int(g["iterations"])
@@ -309,8 +312,9 @@ def test_oracle_constrained_loop_matches_reference_run():
     np.testing.assert_array_equal(col("beta"), g["beta"])
     np.testing.assert_allclose(np.array([r["constraints"] for r in recs]), g["constraints"], rtol=0, atol=1e-10)
     for key in ("deflection", "stress", "volume"):
-        np.testing.assert_allclose(col(key), g[key], rtol=1e-10)
+        np.testing.assert_allclose(col(key), g[key], rtol=1e-10, equal_nan=True)
     np.testing.assert_allclose(col("change"), g["change"], rtol=0, atol=1e-10)
     np.testing.assert_allclose(np.stack([r["xphys"] for r in recs]), g["xphys"], rtol=0, atol=1e-10)
     np.testing.assert_allclose(x, g["x_last"], rtol=0, atol=1e-10)
-    assert g["solvedCells"].min() < np.prod(dims)
+    if tag == "":
+        assert g["solvedCells"].min() < np.prod(dims)
