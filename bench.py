@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--evolve", action="store_true",
                    help="step the evolving SIMP loop (each step from the last step's design, warm-started "
                         "solves) instead of the fixed-work iteration from the seeded design")
-    p.add_argument("--micro", choices=["apply", "band", "cases", "full", "torchref"], default=None,
+    p.add_argument("--micro", choices=["apply", "band", "cases", "full", "torchref", "optimize"], default=None,
                    help="apply: only the K*u microbenchmarks (fine level in both precisions, then the "
                         "level-1 weights operator; applies on seeded N(0,1) vectors); band: only the "
                         "coarsest level's band assembly, factorisation and inverse; cases: the batched "
@@ -67,7 +67,9 @@ def parse():
                         "precision and on the plain FP64 GPU path, final compliance and design compared; torchref: "
                         "the reference's own torch-CUDA multigrid (loadpath.gpu.TorchMG under "
                         "mg.GridElasticity(device='cuda'), from the copy installed in baseline/_ref) on the bench's "
-                        "design: hierarchy build and one solve to rtol 1e-6, wall-clock, beside this package's")
+                        "design: hierarchy build and one solve to rtol 1e-6, wall-clock, beside this package's; "
+                        "optimize: loadpath's own SIMP loop (optimize.OptimizeLoop) and its stress-constrained "
+                        "loop (optimize.ConstrainedLoop) on the bench's cantilever, --iters iterations each")
     p.add_argument("--iters", type=int, default=100, help="SIMP iterations of --micro full")
     p.add_argument("--reps", type=int, default=100)
     p.add_argument("--eager", action="store_true",
@@ -817,6 +819,46 @@ def run_micro_full(args):
     return 0
 
 
+def run_micro_optimize(args):
+    """loadpath's own SIMP loop (default options: blueprint and eroded projections, live cells,
+    measured step, Illinois volume step, beta continuation) and its minimum-mass loop under a
+    stress and a deflection limit, on the bench's cantilever at the bench's size, mixed precision,
+    solves to rtol 1e-6; CUDA-event timed over --iters iterations after one untimed."""
+    import torch
+
+    from loadpath_b200.optimize import ConstrainedLoop, Limits, OptimizeLoop, SimpOptions
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dims = args.dims
+    fixed, f = cantilever(dims)
+    out = {}
+    opts = SimpOptions(volume_fraction=0.3, filter_radius=2.0, max_iterations=args.iters + 1, solve_rtol=RTOL)
+    copts = SimpOptions(volume_fraction=0.5, filter_radius=2.0, max_iterations=args.iters + 1, solve_rtol=RTOL)
+    for name, make in (("optimize", lambda: OptimizeLoop(dims, fixed, [f], 0.3, opts)),
+                       ("constrained", lambda: ConstrainedLoop(dims, fixed, [f], 0.3, copts,
+                                                               Limits(0.02, 0.5, 1000.0)))):
+        loop = make()
+        loop.step()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record()
+        for _ in range(args.iters):
+            loop.step()
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / args.iters
+        h = loop.history
+        out[name] = {"simp_iter_per_s": 1e3 / ms, "ms_per_iteration": ms,
+                     "cg_iterations": [r["cgIterations"] for r in h],
+                     "last": {k: v for k, v in h[-1].items() if k in ("compliance", "volume", "beta", "change",
+                                                                       "constraints", "volumeSolves", "move")}}
+        del loop
+        torch.cuda.empty_cache()
+    print(json.dumps({"micro": "loadpath SIMP loops", "dims": list(dims), "iterations": args.iters,
+                      "dtype": "f32+f64", "data": "synthetic (uniform start, cantilever)", **out}))
+    return 0
+
+
 def run_micro_torchref(args):
     """The reference's own GPU path on the bench's design: loadpath.mg.GridElasticity with
     device='cuda' (its hierarchy built on the host by numba, then loaded into torch tensors; the
@@ -965,6 +1007,8 @@ def main():
         return run_micro_full(args)
     if args.micro == "torchref":
         return run_micro_torchref(args)
+    if args.micro == "optimize":
+        return run_micro_optimize(args)
     if args.kernels:
         return run_kernels(args)
     if args.impl == "reference":
