@@ -193,6 +193,73 @@ def scatter_cells(f, out):
     return out
 
 
+def prolong_rows(fine_ijk, coarse_node_shape):
+    """Scalar trilinear prolongation rows (len(fine_ijk), coarse nodes) for the given fine nodes
+    (loadpath/mg.py:390-408): an odd index lies halfway between two coarse nodes (0.5 each), an
+    even one on its coarse node (1)."""
+    import scipy.sparse as sp
+
+    n = len(fine_ijk)
+    rows, cols, vals = [], [], []
+    for corner in range(8):
+        w = np.ones(n)
+        ci = np.empty((n, 3), np.int64)
+        for d in range(3):
+            i = fine_ijk[:, d]
+            odd = i % 2 == 1
+            hi = (corner >> d) & 1
+            ci[:, d] = i // 2 + (hi & odd)
+            w *= np.where(odd, 0.5, 1.0 if not hi else 0.0)
+        ok = w > 0
+        rows.append(np.nonzero(ok)[0])
+        cols.append(np.ravel_multi_index(tuple(ci[ok].T), coarse_node_shape))
+        vals.append(w[ok])
+    nc = int(np.prod(coarse_node_shape))
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, nc))
+
+
+def coarse_extra(fine, cdims, mask_fine):
+    """The fine level's extra operator S carried to the coarse level as P^T S P, P the trilinear
+    prolongation of the dofs S touches, each row times the fine mask at the first coarsening
+    (loadpath/mg.py:679-706). None without an extra operator."""
+    import scipy.sparse as sp
+
+    s = fine.extra
+    if s is None or s.nnz == 0:
+        return None
+    nshape_f = fine.node_shape[1:]
+    nshape_c = tuple(c + 1 for c in cdims)
+    nn_f, nn_c = int(np.prod(nshape_f)), int(np.prod(nshape_c))
+    s = s.tocsr()
+    mark = np.zeros(s.shape[0], bool)
+    mark[s.indices] = True
+    mark[np.diff(s.indptr) > 0] = True
+    dofs = np.flatnonzero(mark)
+    comp, node = np.divmod(dofs, nn_f)
+    ijk = np.stack(np.unravel_index(node, nshape_f), axis=1)
+    pr = prolong_rows(ijk, nshape_c).tocoo()
+    cols = comp[pr.row] * nn_c + pr.col
+    vals = pr.data
+    if mask_fine is not None:
+        vals = vals * np.asarray(mask_fine).reshape(-1)[dofs[pr.row]]
+    p = sp.csr_matrix((vals, (dofs[pr.row], cols)), shape=(s.shape[0], 3 * nn_c))
+    return (p.T @ s @ p).tocsr()
+
+
+def springs_to_grid(springs, node_ijk, node_shape):
+    """A sparse operator in mesh dof numbering (3 node + component) on the flat (3, nodes) grid
+    dofs (component nn + node) of a node grid of shape node_shape (loadpath/mg.py:475-513)."""
+    import scipy.sparse as sp
+
+    nn = int(np.prod(node_shape))
+    flat = np.ravel_multi_index(tuple(np.asarray(node_ijk).T), node_shape)
+    g = np.empty(3 * len(flat), np.int64)
+    for i in range(3):
+        g[i::3] = i * nn + flat
+    c = springs.tocoo()
+    return sp.csr_matrix((c.data, (g[c.row], g[c.col])), shape=(3 * nn, 3 * nn))
+
+
 class Level:
     """One grid level (loadpath/mg.py:174-199).
 
@@ -207,6 +274,7 @@ class Level:
         self.ke = self.e = self.mcat = self.w = None
         self.patch_ijk = self.patch_k = self.k = None
         self.mask = self.dinv = self.lmax = None
+        self.extra = None   # a sparse operator on the flat (3, nodes) dofs, added to K (springs)
 
     @property
     def node_shape(self):
@@ -246,6 +314,9 @@ class Level:
             idx = self.patch_index()
             fe = np.einsum("nij,nj->ni", self.patch_k.astype(u.dtype), u.reshape(-1)[idx])
             np.add.at(out.reshape(-1), idx.ravel(), fe.ravel())
+        if self.extra is not None:
+            # (loadpath/mg.py:278-296: the extra operator in float64, added in the level's dtype)
+            out += (self.extra @ u.reshape(-1).astype(np.float64)).astype(u.dtype).reshape(out.shape)
         return out
 
     def apply(self, u):
@@ -272,7 +343,10 @@ class Level:
         km = self.cell_matrices()
         dc = np.einsum("iixyz->ixyz", km)
         d = np.zeros(self.node_shape)
-        return scatter_cells(dc, d)
+        d = scatter_cells(dc, d)
+        if self.extra is not None:
+            d += self.extra.diagonal().reshape(d.shape)   # loadpath/mg.py:369-370
+        return d
 
     def active(self):
         """Cells with a nonzero matrix outside the patch (loadpath/mg.py:205-211)."""
@@ -295,7 +369,8 @@ class Hierarchy:
     even counts by the caller (loadpath/mg.py:438-442)."""
 
     def __init__(self, ke, cells, fixed_grid, rtol=1e-6, maxiter=500, coarse_cells=2000, degree=2,
-                 dtype=np.float32, lu_max_dofs=60_000):
+                 dtype=np.float32, lu_max_dofs=60_000, springs=None):
+        self.springs = None if springs is None else springs.tocsr()   # on the flat (3, nodes) dofs
         self.ke = np.asarray(ke, np.float64)
         self.cells = tuple(int(c) for c in cells)
         self.fixed_grid = np.asarray(fixed_grid, bool)
@@ -320,6 +395,7 @@ class Hierarchy:
         l0 = Level("scaled", self.cells, np.float64)
         l0.ke = self.ke
         l0.e = e_grid
+        l0.extra = self.springs
         d0 = l0.diagonal()
         alive = d0 > 1e-300
         l0.mask = (alive & ~self.fixed_grid).astype(np.float64)
@@ -331,6 +407,7 @@ class Hierarchy:
         s.e = e_grid.astype(dt)
         s.mask = l0.mask.astype(dt)
         s.dinv = l0.dinv.astype(dt)
+        s.extra = self.springs
         self.l0s = s
         fine = l0
         n_active = int((e_grid > 0).sum())
@@ -413,6 +490,7 @@ class Hierarchy:
             lv.w = w.astype(dt)
             lv.patch_ijk = pij
             lv.patch_k = pk.astype(dt)
+            lv.extra = coarse_extra(fine, cdims, fine.mask)
             return lv
         lv = Level("explicit", cdims, dt)
         k = np.zeros((24, 24) + cdims, dt)
@@ -429,6 +507,7 @@ class Hierarchy:
             t = np.einsum("ai,abn,bj->ijn", PK[ch], sub.reshape(24, 24, -1), PK[ch])
             k[:, :, :shp[0], :shp[1], :shp[2]] += t.reshape((24, 24) + shp).astype(dt)
         lv.k = k
+        lv.extra = coarse_extra(fine, cdims, None)
         return lv
 
     def build_coarse(self, lv):
@@ -464,6 +543,8 @@ class Hierarchy:
                 for comp in range(3):
                     dofs[3 * q + comp] = loc[comp * nn + node]
             kd[np.ix_(dofs, dofs)] += kall[:, :, i, j, l]
+        if lv.extra is not None:
+            kd += lv.extra[gdof][:, gdof].toarray()   # loadpath/mg.py:734-735
         m = lv.mask.reshape(-1)[gdof].astype(np.float64)
         kd = m[:, None] * kd * m[None, :] + np.diag(1.0 - m)
         kd = 0.5 * (kd + kd.T)

@@ -4,7 +4,8 @@ Run in a container that has the loadpath source tree (read-only is fine):
 
     LOADPATH_SRC=/path/to/loadpath python tests/golden/make_golden.py [name ...]
 
-(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize constrained callers; default all but config0,
+(names: element transfers femops filter mma hierarchies top3d config0 oc_step optimize constrained callers
+springs; default all but config0,
 which runs the reference's top3d port for 20 iterations at 60x20x10 and takes a few minutes).
 
 It imports loadpath's own modules (fem, mg, mgops, femops, simp, mma,
@@ -501,6 +502,54 @@ def make_callers():
     np.savez_compressed(os.path.join(HERE, "callers.npz"), **out)
 
 
+def make_springs():
+    """GridElasticity with a springs term (loadpath/mg.py:415-470, :274-296, :348-371, :679-706,
+    :734-735): the sparse operator added on the fine level, coarsened as P^T S P level by level
+    and added to the coarsest assembly. A 12x8x8 box at pitch 1 held by springs alone (diagonal
+    springs on every base node, as the build simulation's layer springs hold a part) plus a
+    spring coupling two top nodes (an off-diagonal term, as a cut cell's operator has); smoothed
+    seeded moduli, a top load; rtol 1e-10, coarse_cells 40 so that the hierarchy has three
+    levels. Stored: the mesh, the springs (mesh dof numbering, COO), the solve and its count,
+    and every level's lmax."""
+    os.environ["LOADPATH_HEX8"] = "im"
+    import scipy.sparse as sp
+    from loadpath.mg import GridElasticity
+
+    dims = (12, 8, 8)
+    mesh = _full_mesh(dims)
+    rng = np.random.default_rng(31)
+    x = _smoothed(np.exp(rng.uniform(np.log(1e-2), 0.0, dims)), 2.0).reshape(-1)
+    e = 1e-9 + x ** 3 * (1 - 1e-9)
+    base = np.flatnonzero(mesh.node_ijk[:, 2] == 0)
+    rows, cols, vals = [], [], []
+    for c in range(3):
+        rows += list(3 * base + c)
+        cols += list(3 * base + c)
+        vals += [0.05] * len(base)
+    top = np.flatnonzero(mesh.node_ijk[:, 2] == dims[2])
+    a, b = int(top[0]), int(top[-1])
+    for c in range(3):
+        for (i, j, v) in ((a, a, 0.2), (b, b, 0.2), (a, b, -0.2), (b, a, -0.2)):
+            rows.append(3 * i + c)
+            cols.append(3 * j + c)
+            vals.append(v)
+    s = sp.csr_matrix((vals, (rows, cols)), shape=(mesh.n_dof, mesh.n_dof))
+    fixed = np.zeros(mesh.n_dof, bool)
+    f = np.zeros(mesh.n_dof)
+    f[3 * top + 2] = -1.0 / len(top)
+    f[3 * top + 0] = 0.3 / len(top)
+    ge = GridElasticity(mesh, 0.3, fixed, springs=s, rtol=1e-10, maxiter=3000, coarse_cells=40, device="cpu")
+    ge.set_moduli(e)
+    u = ge.solve_many([f])[0]
+    coo = s.tocoo()
+    np.savez_compressed(os.path.join(HERE, "springs.npz"), dims=np.array(dims), e_mesh=e, f_mesh=f,
+                        fixed_mesh=fixed, s_row=coo.row, s_col=coo.col, s_val=coo.data, u_mesh=u,
+                        iters=np.array(ge.last_iters), nlevels=len(ge.levels),
+                        lmax=np.array([ge._op(i).lmax for i in range(len(ge.levels))]), strict=ge.strict,
+                        u_grid=ge.to_grid(u), f_grid=ge.to_grid(f), e_grid=ge.cell_grid(e))
+    print("springs: levels", len(ge.levels), "iters", ge.last_iters, "strict", ge.strict)
+
+
 def main(names=None):
     gens = {"element": make_element, "transfers": make_transfers, "femops": make_femops, "filter": make_filter,
             "mma": make_mma,
@@ -509,7 +558,8 @@ def main(names=None):
                                     make_hierarchy("deep_im", (16, 8, 8), "im", 3, 20, 0.0),
                                     make_hierarchy("rough_strict", (8, 4, 4), "im", 4, 20, 0.05, smooth=False)),
             "top3d": make_top3d, "config0": make_config0, "oc_step": make_oc_step,
-            "optimize": make_optimize, "constrained": make_constrained, "callers": make_callers}
+            "optimize": make_optimize, "constrained": make_constrained, "callers": make_callers,
+            "springs": make_springs}
     for name in names or [k for k in gens if k != "config0"]:
         gens[name]()
 

@@ -318,3 +318,30 @@ def test_oracle_constrained_loop_matches_reference_run(tag):
     np.testing.assert_allclose(x, g["x_last"], rtol=0, atol=1e-10)
     if tag == "":
         assert g["solvedCells"].min() < np.prod(dims)
+
+
+def test_oracle_springs_solve_matches_reference():
+    """The oracle's hierarchy with a springs term (the operator added on the fine level, carried
+    to every coarse level as P^T S P and into the coarsest assembly; loadpath/mg.py:274-296,
+    :348-371, :679-706, :734-735) against the reference's own GridElasticity with springs
+    (tests/golden/springs.npz): a box held by springs alone at its base plus one spring coupling
+    two top nodes. Every level's lmax, the solution and the CG count."""
+    import scipy.sparse as sp
+
+    g = _load("springs.npz")
+    dims = tuple(int(d) for d in g["dims"])
+    nshape = tuple(d + 1 for d in dims)
+    node_ijk = np.stack(np.meshgrid(*[np.arange(n) for n in nshape], indexing="ij"), -1).reshape(-1, 3)
+    ndof = 3 * len(node_ijk)
+    s = sp.csr_matrix((g["s_val"], (g["s_row"], g["s_col"])), shape=(ndof, ndof))
+    fixed = np.zeros((3,) + nshape, bool)
+    h = R.Hierarchy(R.hex8_ke(0.3, "im"), dims, fixed, rtol=1e-10, maxiter=3000, coarse_cells=40,
+                    springs=R.springs_to_grid(s, node_ijk, nshape))
+    h.set_moduli(g["e_grid"])
+    assert len(h.levels) == int(g["nlevels"]) and h.strict == bool(g["strict"])
+    np.testing.assert_allclose([h.op(i).lmax for i in range(len(h.levels))], g["lmax"], rtol=1e-4)
+    u = h.solve(g["f_grid"])
+    np.testing.assert_allclose(u, g["u_grid"], rtol=0, atol=1e-8 * np.abs(g["u_grid"]).max())
+    assert abs(h.last_iters - int(g["iters"])) <= 2, (h.last_iters, int(g["iters"]))
+    # springs on every level: a coarse operator without them is singular (nothing else holds the box)
+    assert all(h.op(i).extra is not None for i in range(len(h.levels)))
