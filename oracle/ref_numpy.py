@@ -1048,7 +1048,7 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
 
 def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=None, pad=True, pitch=1.0,
                   eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0,
-                  mirror=(), reuse=6):
+                  mirror=(), reuse=6, adaptive_move=True, stall_rtol=2e-3, stall_window=6):
     """loadpath's own SIMP loop for one load case with its default options (loadpath/simp.py:
     1640-2455): blueprint and eroded projections of xt = H x / hs (`physical`, `eroded`), the SIMP
     law on the eroded design, the solve with the live-cell reduction (LiveSystem with the direct
@@ -1057,8 +1057,9 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
     dv = max(H (w P'_b / hs), 1e-12), the move limit measured from the Lagrangian's slope along
     the last step (t = a / (a - b), the limit times t clipped to [0.5, 1.2], capped at move), the
     step of oc_loadpath_step, and beta doubling after beta_every iterations or a free step of
-    change < 2 tol, halving the limit; with mirror planes (axes) dc, dv and every trial design are
-    averaged across them (:2222-2224, :2300). Ke and the loads' work scale with the pitch. Returns the
+    change < 2 tol, halving the limit (with adaptive_move off, the fixed limits: move, move / 2 past
+    beta 4), and at beta_max the stopping rules; with mirror planes (axes) dc, dv and every trial
+    design are averaged across them (:2222-2224, :2300). Ke and the loads' work scale with the pitch. Returns the
     per-iteration records (compliance, beta, change, move, volume, volumeSolves, xphys) and x."""
     pres = np.zeros(dims, bool) if pres is None else np.asarray(pres, bool)
     design = ~pres
@@ -1096,28 +1097,44 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
         dv = np.maximum(hap(w * dpb / hs), 1e-12)
         if mirror:
             dc, dv = mirror_average(dc, mirror), mirror_average(dv, mirror)
-        if step_prev is not None:
-            dxp, gp, lam_p = step_prev
-            a_s = float(np.sum(gp * dxp))
-            b_s = float(np.sum((dc + lam_p * dv) * dxp))
-            if a_s < 0:
-                t_s = a_s / (a_s - b_s) if b_s > a_s else np.inf
-                move_k = min(move_k * min(max(t_s, 0.5), 1.2), move)
-        mv = move_k
-        x_new, lm, n_eval, _ = oc_loadpath_step(x, dc, dv, mv, beta, eta, hap, hs, w, target, pres=pres,
+        if adaptive_move:
+            if step_prev is not None:
+                dxp, gp, lam_p = step_prev
+                a_s = float(np.sum(gp * dxp))
+                b_s = float(np.sum((dc + lam_p * dv) * dxp))
+                if a_s < 0:
+                    t_s = a_s / (a_s - b_s) if b_s > a_s else np.inf
+                    move_k = min(move_k * min(max(t_s, 0.5), 1.2), move)
+            mv = move_k
+        else:
+            mv = move if beta <= 4 else move / 2
+        x_new, lm, n_eval, held = oc_loadpath_step(x, dc, dv, mv, beta, eta, hap, hs, w, target, pres=pres,
                                                 lam_last=lam_last, mirror=mirror)
         lam_last = lm
         change = float(np.abs(x_new - x)[design].max())
         step_prev = (x_new - x, dc + lm * dv, lm)
         x = x_new
         since_beta += 1
-        recs.append(dict(compliance=comp, beta=beta, change=change, move=mv, volume=float(xp[design].mean()),
-                         volumeSolves=n_eval, xphys=xp))
-        if beta < beta_max and ((change < 2 * tol and change < 0.999 * mv) or since_beta >= beta_every):
+        recs.append(dict(compliance=comp, beta=beta, change=change, move=mv if adaptive_move else np.nan,
+                         volume=float(xp[design].mean()), volumeSolves=n_eval, xphys=xp))
+        free_step = not adaptive_move or change < 0.999 * mv
+        if beta < beta_max and ((change < 2 * tol and free_step) or since_beta >= beta_every):
             beta = min(2 * beta, beta_max)
             since_beta = 0
             step_prev = None
             move_k = move_k / 2
+        elif beta >= beta_max and len(recs) >= 3:
+            # the stopping rules (loadpath/simp.py:2431-2450); the schedule's rule needs the
+            # measured step, the stall rule holds otherwise
+            if change < tol and free_step:
+                break
+            if adaptive_move and held:
+                if since_beta >= beta_every:
+                    break
+            elif since_beta >= stall_window and len(recs) > stall_window:
+                old = recs[-1 - stall_window]["compliance"]
+                if abs(comp - old) <= stall_rtol * abs(old):
+                    break
     return recs, x
 
 

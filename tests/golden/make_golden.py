@@ -335,7 +335,8 @@ def make_optimize():
     """loadpath's own SIMP loop as a whole (loadpath/simp.py:1640-2455, simp.optimize with its
     default options: blueprint and eroded projections, the measured step length, beta
     continuation, the volume multiplier solved to rounding) on two top3d cantilevers and a bridge
-    mirrored in x and y, of its benchmarks (domain_for: load and support cells pinned, padded
+    mirrored in x and y, and with the fixed move schedule (adaptive_move off, beta up to 8, run
+    to its stall rule) on the small cantilever, of its benchmarks (domain_for: load and support cells pinned, padded
     filter), with the solves
     tightened to rtol 1e-10 so that a solver of another kind can be compared iteration by
     iteration. Stored per case: the domain on the node / cell grid (supports, load, pinned cells),
@@ -347,9 +348,11 @@ def make_optimize():
     from loadpath.benchmarks.run import NU, design_volfrac, domain_for
 
     out = {}
-    cases = {"small": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 30), "medium": (cantilever_3d, (20, 6, 10), 0.3, 2.0, 24),
-             "bridge": (bridge_3d, (16, 4, 6), 0.15, 1.5, 24)}
-    for name, (problem, dims, vf, rmin, iters) in cases.items():
+    cases = {"small": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 30, {}),
+             "medium": (cantilever_3d, (20, 6, 10), 0.3, 2.0, 24, {}),
+             "bridge": (bridge_3d, (16, 4, 6), 0.15, 1.5, 24, {}),
+             "fixedmove": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 48, {"adaptive_move": False, "beta_max": 8.0})}
+    for name, (problem, dims, vf, rmin, iters, extra) in cases.items():
         p = problem(*dims, vf, rmin)
         dom, _ = domain_for(p)
         mesh = dom.mesh
@@ -361,7 +364,7 @@ def make_optimize():
             mirrored[:, axes[ax]] = dims[axes[ax]] - 1 - mirrored[:, axes[ax]]
             assert np.array_equal(mesh.elem_ijk[m], mirrored)
         opts = S.SimpOptions(volume_fraction=design_volfrac(p, dom), filter_radius=p.rmin, max_iterations=iters,
-                             solve_rtol=1e-10)
+                             solve_rtol=1e-10, **extra)
         recs, xps = [], []
         res = S.optimize(dom, NU, opts, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
         nxyz = np.array(dims) + 1
@@ -385,9 +388,11 @@ def make_optimize():
                     f"{name}_pad": bool(S._pad(opts)), f"{name}_emin": float(S.E_MIN),
                     f"{name}_penal": float(S.PENALTY), f"{name}_iterations": len(recs),
                     f"{name}_mirror": np.array([axes[a] for a in dom.mirror], np.int64),
+                    f"{name}_adaptive_move": bool(opts.adaptive_move), f"{name}_beta_max": float(opts.beta_max),
+                    f"{name}_converged": bool(res.converged),
                     f"{name}_xphys": np.stack([grid(v) for v in xps]), f"{name}_x_last": grid(res.x)})
         for k in keys:
-            out[f"{name}_{k}"] = np.array([float(r[k]) for r in recs])
+            out[f"{name}_{k}"] = np.array([float(r.get(k, np.nan)) for r in recs])
         out[f"{name}_stepFit"] = np.array([float(r.get("stepFit", np.nan)) for r in recs])
     np.savez_compressed(os.path.join(HERE, "optimize.npz"), **out)
 

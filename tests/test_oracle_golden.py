@@ -259,7 +259,7 @@ def test_oracle_oc_loadpath_step_matches_reference_run():
         np.testing.assert_allclose(xn, grid(g[f"x_new{k}"]), rtol=0, atol=1e-13)
 
 
-@pytest.mark.parametrize("case", ["small", "medium", "bridge"])
+@pytest.mark.parametrize("case", ["small", "medium", "bridge", "fixedmove"])
 def test_oracle_optimize_loop_matches_reference_run(case):
     """The oracle's restatement of loadpath's SIMP loop (optimize_loop) against the reference's
     own simp.optimize (tests/golden/optimize.npz): every iteration's projection sharpness, move
@@ -272,14 +272,16 @@ def test_oracle_optimize_loop_matches_reference_run(case):
     recs, x = R.optimize_loop(dims, R.hex8_ke(float(k("nu")), "im"), k("fixed"), k("f"), float(k("volfrac")),
                               float(k("radius")), int(k("iterations")), pres=k("pres"), pad=bool(k("pad")),
                               pitch=float(k("pitch")), emin=float(k("emin")), penal=float(k("penal")),
-                              mirror=tuple(int(a) for a in k("mirror")))
+                              mirror=tuple(int(a) for a in k("mirror")), adaptive_move=bool(k("adaptive_move")),
+                              beta_max=float(k("beta_max")))
     col = lambda key: np.array([r[key] for r in recs], float)   # noqa: E731
     np.testing.assert_array_equal(col("beta"), k("beta"))
     np.testing.assert_array_equal(col("volumeSolves"), k("volumeSolves"))
     # the bridge (volume fraction 0.01, held at its four bottom corners' edges) is badly conditioned:
     # two direct factorisations of it agree on the energy to a few parts in 10^9
     np.testing.assert_allclose(col("compliance"), k("compliance"), rtol=1e-10 if case != "bridge" else 2e-8)
-    np.testing.assert_allclose(col("move"), k("move"), rtol=1e-12)
+    np.testing.assert_allclose(col("move"), k("move"), rtol=1e-12, equal_nan=True)
+    assert len(recs) == int(k("iterations"))
     np.testing.assert_allclose(col("change"), k("change"), rtol=0, atol=1e-10 if case != "bridge" else 1e-9)
     np.testing.assert_allclose(col("volume"), k("volume"), rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(np.stack([r["xphys"] for r in recs]), k("xphys"), rtol=0, atol=1e-9)
