@@ -35,7 +35,7 @@ import torch
 from ._lib import lib
 from .autograd import Compliance, SimpProblem
 from .fem import corner_stress_ops
-from .grid import ptr, stream_handle
+from .grid import stream_handle
 from .mg import BoxMesh, GridElasticity
 from .mma import MMA
 from .simp import MG_MIN_CELLS, SUB_REUSE, DeviceFilter, LiveCells, ProjectedDesign, _cells_touching
