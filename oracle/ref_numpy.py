@@ -946,23 +946,28 @@ class LiveSystem:
         return stiff
 
     def solve(self, e, xphys, f_grid):
-        f_grid = np.asarray(f_grid, float)
+        """u for the load f_grid, or the list of u for a list of loads (the reduction decided on all
+        of them, as the reference's analysis decides it on every case)."""
+        many = isinstance(f_grid, (list, tuple))
+        fs = [np.asarray(f, float) for f in (f_grid if many else [f_grid])]
+        dead = lambda nodes: any(np.any(f[:, ~nodes]) for f in fs)   # noqa: E731
         alive = (xphys > ALIVE) | self.anchor
         self.er, self.drop, self.cells = e, False, e.size
-        if alive.mean() < REDUCE_BELOW and not np.any(f_grid[:, ~self._stiff_nodes(alive)]):
+        if alive.mean() < REDUCE_BELOW and not dead(self._stiff_nodes(alive)):
             keep = None
             if self.reuse and self.cache is not None and self.age < self.reuse and not np.any(alive & ~self.cache):
                 self.age += 1
                 keep = self.cache
             else:
                 keep = connected_keep(alive, self.support_touch)
-                if np.any(f_grid[:, ~self._stiff_nodes(keep)]):
+                if dead(self._stiff_nodes(keep)):
                     self.cache, keep = None, None
                 elif self.reuse:
                     self.cache, self.age = keep, 0
             if keep is not None:
                 self.er, self.drop, self.cells = np.where(keep, e, 0.0), True, int(keep.sum())
-        return assembled_solve(self.ke, self.er, self.fixed, f_grid, drop_dead=self.drop)
+        us = [assembled_solve(self.ke, self.er, self.fixed, f, drop_dead=self.drop) for f in fs]
+        return us if many else us[0]
 
     def resolve(self, rhs):
         return assembled_solve(self.ke, self.er, self.fixed, rhs, drop_dead=self.drop)
@@ -1048,7 +1053,7 @@ def top3d_loop(dims, volfrac, rmin, ke, fixed_grid, f_grid, iters, penal=3.0, em
 
 def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=None, pad=True, pitch=1.0,
                   eta=0.5, erode=0.15, move=0.2, tol=0.01, beta_max=32.0, beta_every=10, emin=1e-6, penal=3.0,
-                  mirror=(), reuse=6, adaptive_move=True, stall_rtol=2e-3, stall_window=6):
+                  mirror=(), reuse=6, adaptive_move=True, stall_rtol=2e-3, stall_window=6, weights=None):
     """loadpath's own SIMP loop for one load case with its default options (loadpath/simp.py:
     1640-2455): blueprint and eroded projections of xt = H x / hs (`physical`, `eroded`), the SIMP
     law on the eroded design, the solve with the live-cell reduction (LiveSystem with the direct
@@ -1067,11 +1072,14 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
     taps = filter_taps(radius, pitch)
     hs = np.full(dims, sum(t for _, t in taps)) if pad else filter_row_sums(dims, taps)
     hap = lambda v: grid_filter(v, taps)   # noqa: E731
+    fs = [np.asarray(f, float) for f in (f_grid if isinstance(f_grid, (list, tuple)) else [f_grid])]
+    weights = [1.0] * len(fs) if weights is None else [float(w_) for w_ in weights]
     held = np.asarray(fixed_grid, bool).any(axis=0)
-    loaded = (np.asarray(f_grid) != 0).any(axis=0)
+    loaded = np.zeros(held.shape, bool)
+    for f in fs:
+        loaded |= (f != 0).any(axis=0)
     system = LiveSystem(ke * pitch, fixed_grid, cells_touching(held), cells_touching(held | loaded) | pres,
                         reuse=reuse)
-    solve = lambda e, xp_: system.solve(e, xp_, f_grid)   # noqa: E731
     x = np.full(dims, volfrac)
     x[pres] = 1.0
     target = volfrac * float(w.sum())
@@ -1084,11 +1092,14 @@ def optimize_loop(dims, ke, fixed_grid, f_grid, volfrac, radius, iters, pres=Non
         xe = project(xt, beta, eta + erode)
         xe[pres] = 1.0
         e = emin + xe ** penal * (1 - emin)
-        u = solve(e, xe)
-        comp = float(np.sum(np.asarray(f_grid) * u))
-        g = gather_cells(u, dims).reshape(24, -1)
-        ce = np.einsum("in,in->n", g, (ke * pitch) @ g).reshape(dims)
-        dc_xe = -penal * xe ** (penal - 1) * (1 - emin) * ce
+        us = system.solve(e, xe, fs)
+        comp, dc_xe = 0.0, np.zeros(dims)
+        for f, u, wk in zip(fs, us, weights):
+            # per case: its weight times f.u, and its sensitivity (loadpath/simp.py:1901-1904)
+            g = gather_cells(u, dims).reshape(24, -1)
+            ce = np.einsum("in,in->n", g, (ke * pitch) @ g).reshape(dims)
+            comp += wk * float(np.sum(f * u))
+            dc_xe -= wk * penal * xe ** (penal - 1) * (1 - emin) * ce
         dpe = dproject(xt, beta, eta + erode)
         dpe[pres] = 0.0
         dpb = dproject(xt, beta, eta)

@@ -351,12 +351,23 @@ def make_optimize():
     cases = {"small": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 30, {}),
              "medium": (cantilever_3d, (20, 6, 10), 0.3, 2.0, 24, {}),
              "bridge": (bridge_3d, (16, 4, 6), 0.15, 1.5, 24, {}),
-             "fixedmove": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 48, {"adaptive_move": False, "beta_max": 8.0})}
+             "fixedmove": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 48, {"adaptive_move": False, "beta_max": 8.0}),
+             "twocase": (cantilever_3d, (12, 4, 6), 0.3, 1.5, 24, {})}
     for name, (problem, dims, vf, rmin, iters, extra) in cases.items():
         p = problem(*dims, vf, rmin)
         dom, _ = domain_for(p)
         mesh = dom.mesh
         assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1 and dom.springs is None
+        f_second = None
+        if name == "twocase":
+            # a second case on the same nodes, an axial pull, weighed at half the first
+            f_second = np.zeros_like(dom.loads[0])
+            on = np.flatnonzero(dom.loads[0].reshape(-1, 3).any(axis=1))
+            f_second[3 * on] = 0.8
+            dom.loads = [dom.loads[0], f_second]
+            dom.case_weights = [1.0, 0.5]
+            dom.spreads = [None, None]
+            dom.case_names = ["down", "pull"]
         axes = {"x": 0, "y": 1, "z": 2}
         for ax, m in dom.mirror.items():
             assert np.all(m >= 0)
@@ -371,9 +382,14 @@ def make_optimize():
         fixed = np.zeros((3, *nxyz), bool)
         f = np.zeros((3, *nxyz))
         nijk = tuple(mesh.node_ijk.T)
+        f2 = np.zeros((3, *nxyz))
         for c in range(3):
             fixed[c][nijk] = dom.fixed[c::3]
             f[c][nijk] = dom.loads[0][c::3]
+            if f_second is not None:
+                f2[c][nijk] = f_second[c::3]
+        if f_second is not None:
+            out[f"{name}_f2"] = f2
         cells = tuple(mesh.elem_ijk.T)
 
         def grid(v):
@@ -389,7 +405,7 @@ def make_optimize():
                     f"{name}_penal": float(S.PENALTY), f"{name}_iterations": len(recs),
                     f"{name}_mirror": np.array([axes[a] for a in dom.mirror], np.int64),
                     f"{name}_adaptive_move": bool(opts.adaptive_move), f"{name}_beta_max": float(opts.beta_max),
-                    f"{name}_converged": bool(res.converged),
+                    f"{name}_converged": bool(res.converged), f"{name}_weights": np.array(dom.case_weights, float),
                     f"{name}_xphys": np.stack([grid(v) for v in xps]), f"{name}_x_last": grid(res.x)})
         for k in keys:
             out[f"{name}_{k}"] = np.array([float(r.get(k, np.nan)) for r in recs])

@@ -259,7 +259,7 @@ def test_oracle_oc_loadpath_step_matches_reference_run():
         np.testing.assert_allclose(xn, grid(g[f"x_new{k}"]), rtol=0, atol=1e-13)
 
 
-@pytest.mark.parametrize("case", ["small", "medium", "bridge", "fixedmove"])
+@pytest.mark.parametrize("case", ["small", "medium", "bridge", "fixedmove", "twocase"])
 def test_oracle_optimize_loop_matches_reference_run(case):
     """The oracle's restatement of loadpath's SIMP loop (optimize_loop) against the reference's
     own simp.optimize (tests/golden/optimize.npz): every iteration's projection sharpness, move
@@ -269,11 +269,12 @@ def test_oracle_optimize_loop_matches_reference_run(case):
     g = _load("optimize.npz")
     k = lambda s: g[f"{case}_{s}"]   # noqa: E731
     dims = tuple(int(d) for d in k("dims"))
-    recs, x = R.optimize_loop(dims, R.hex8_ke(float(k("nu")), "im"), k("fixed"), k("f"), float(k("volfrac")),
+    loads = [k("f"), k("f2")] if f"{case}_f2" in g.files else k("f")
+    recs, x = R.optimize_loop(dims, R.hex8_ke(float(k("nu")), "im"), k("fixed"), loads, float(k("volfrac")),
                               float(k("radius")), int(k("iterations")), pres=k("pres"), pad=bool(k("pad")),
                               pitch=float(k("pitch")), emin=float(k("emin")), penal=float(k("penal")),
                               mirror=tuple(int(a) for a in k("mirror")), adaptive_move=bool(k("adaptive_move")),
-                              beta_max=float(k("beta_max")))
+                              beta_max=float(k("beta_max")), weights=k("weights"))
     col = lambda key: np.array([r[key] for r in recs], float)   # noqa: E731
     np.testing.assert_array_equal(col("beta"), k("beta"))
     np.testing.assert_array_equal(col("volumeSolves"), k("volumeSolves"))
