@@ -420,7 +420,8 @@ def make_constrained():
     beta continuation) on top3d cantilevers (domain_for), from a uniform 0.5, solves at rtol
     1e-10: both limits on the 12x4x6 one for 40 iterations (constrained.npz), a deflection limit
     alone and a stress limit alone on a 16x4x8 one for 30 (constrained_deflection.npz,
-    constrained_stress.npz). Stored: the domain, the limits, and per iteration the
+    constrained_stress.npz), and both limits with beta_max 4 run to the loop's own stop
+    (constrained_converge.npz: the lightest feasible design delivered). Stored: the domain, the limits, and per iteration the
     record (volume, beta, change, constraints, deflection and stress readings, solved cells) and
     the blueprint; and the last design."""
     os.environ["LOADPATH_HEX8"] = "im"
@@ -429,18 +430,20 @@ def make_constrained():
     from loadpath.benchmarks.run import NU, domain_for
     from loadpath.constrained import Limits, optimize_constrained
 
-    for tag, dims, iters, lim in (("", (12, 4, 6), 40, Limits(12.0, 0.6, 1000.0)),
-                                  ("_deflection", (16, 4, 8), 30, Limits(None, 0.5, 1000.0)),
-                                  ("_stress", (16, 4, 8), 30, Limits(9.0, None, 1000.0))):
-        _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim)
+    for tag, dims, iters, lim, extra in (("", (12, 4, 6), 40, Limits(12.0, 0.6, 1000.0), {}),
+                                         ("_deflection", (16, 4, 8), 30, Limits(None, 0.5, 1000.0), {}),
+                                         ("_stress", (16, 4, 8), 30, Limits(9.0, None, 1000.0), {}),
+                                         ("_converge", (12, 4, 6), 100, Limits(12.0, 0.6, 1000.0),
+                                          {"beta_max": 4.0})):
+        _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim, extra)
 
 
-def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim):
+def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim, extra):
     p = cantilever_3d(*dims, 0.3, 1.5)
     dom, _ = domain_for(p)
     mesh = dom.mesh
     assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1
-    opts = S.SimpOptions(volume_fraction=0.5, filter_radius=p.rmin, max_iterations=iters, solve_rtol=1e-10)
+    opts = S.SimpOptions(volume_fraction=0.5, filter_radius=p.rmin, max_iterations=iters, solve_rtol=1e-10, **extra)
     recs, xps = [], []
     res = optimize_constrained(dom, NU, opts, lim, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
     nxyz = np.array(dims) + 1
@@ -468,7 +471,9 @@ def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, ta
                x_last=grid(res.x), constraints=np.array([r["constraints"] for r in recs]),
                deflection=np.array([r.get(f"deflection.{name}", np.nan) for r in recs]),
                stress=np.array([r.get(f"stress.{name}", np.nan) for r in recs]),
-               contact=grid((dom.support_nodes | dom.load_nodes)[mesh.enode].any(axis=1)))
+               contact=grid((dom.support_nodes | dom.load_nodes)[mesh.enode].any(axis=1)),
+               beta_max=float(opts.beta_max), max_iterations=int(iters),
+               delivered_iteration=int(res.delivered["iteration"]) if res.delivered else -1)
     for k in ("volume", "beta", "change", "solvedCells"):
         out[k] = np.array([float(r[k]) for r in recs])
     np.savez_compressed(os.path.join(HERE, f"constrained{tag}.npz"), **out)

@@ -291,14 +291,15 @@ def test_oracle_optimize_loop_matches_reference_run(case):
         assert k("solvedCells")[-1] < np.prod(dims)
 
 
-@pytest.mark.parametrize("tag", ["", "_deflection", "_stress"])
+@pytest.mark.parametrize("tag", ["", "_deflection", "_stress", "_converge"])
 def test_oracle_constrained_loop_matches_reference_run(tag):
     """The oracle's restatement of loadpath's minimum-mass loop under stress and deflection limits
     (constrained_loop) against the reference's own optimize_constrained on the 12x4x6 cantilever
     (tests/golden/constrained.npz, 40 iterations, beta 1 to 8, the last ones on a reduced system
-    the direct path reuses; and a deflection limit or a stress limit alone on a 16x4x8 cantilever,
-    30 iterations): every iteration's constraints, readings, volume, change and blueprint, and the
-    last design; and the cells whose stress is not counted."""
+    the direct path reuses; a deflection limit or a stress limit alone on a 16x4x8 cantilever,
+    30 iterations; and both limits with beta_max 4, run to the loop's own stop): every iteration's
+    constraints, readings, volume, change and blueprint, and the delivered design (the last one,
+    or the lightest feasible one at beta_max); and the cells whose stress is not counted."""
     g = _load(f"constrained{tag}.npz")
     dims = tuple(int(d) for d in g["dims"])
     lim = lambda key: None if np.isnan(float(g[key])) else float(g[key])   # noqa: E731
@@ -306,10 +307,10 @@ def test_oracle_constrained_loop_matches_reference_run(tag):
     loaded = (g["f"] != 0).any(axis=0)
     np.testing.assert_array_equal(R.cells_touching(held | loaded), g["contact"])
     recs, x, conv = R.constrained_loop(dims, float(g["nu"]), g["fixed"], g["f"], float(g["volfrac"]),
-                                       float(g["radius"]), int(g["iterations"]), lim("stress_limit"),
+                                       float(g["radius"]), int(g["max_iterations"]), lim("stress_limit"),
                                        lim("deflection_limit"), float(g["modulus"]), pres=g["pres"],
                                        pad=bool(g["pad"]), pitch=float(g["pitch"]),
-                                       mirror=tuple(int(a) for a in g["mirror"]))
+                                       mirror=tuple(int(a) for a in g["mirror"]), beta_max=float(g["beta_max"]))
     assert conv == bool(g["converged"]) and len(recs) == int(g["iterations"])
     col = lambda key: np.array([r[key] for r in recs], float)   # noqa: E731
     np.testing.assert_array_equal(col("beta"), g["beta"])
