@@ -1195,7 +1195,8 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
                      beta_max=32.0, beta_every=10, stall_window=6, emin=1e-6, penal=3.0, element="im", reuse=6):
     """loadpath's minimum-mass loop under a stress and a deflection limit for one load case
     (loadpath/constrained.py:295-854 with Limits(stress, deflection, modulus) and default options;
-    either limit may be None):
+    either limit may be None; f_grid one load or a list of load cases, each with its own
+    deflection and stress constraint, deflections first):
     per iteration the blueprint and eroded designs, the solve on the live cells (LiveSystem, as
     optimize_loop) and the adjoint solves on the same system, the deflection f.u / (sum_n |f_n| E) against its limit with gradient
     -dE ce / (sum |f| E); the relaxed von Mises xe * vm(C B_k u_e) / limit at the 8 corners of every
@@ -1213,21 +1214,24 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
     hs = np.full(dims, sum(t for _, t in taps)) if pad else filter_row_sums(dims, taps)
     hap = lambda v: grid_filter(v, taps)   # noqa: E731
     ke = hex8_ke(nu, element) * pitch
-    f_grid = np.asarray(f_grid, float)
+    fs = [np.asarray(f, float) for f in (f_grid if isinstance(f_grid, (list, tuple)) else [f_grid])]
     held = np.asarray(fixed_grid, bool).any(axis=0)
-    loaded = (f_grid != 0).any(axis=0)
+    loaded = np.zeros(held.shape, bool)
+    for f in fs:
+        loaded |= (f != 0).any(axis=0)
     system = LiveSystem(ke, fixed_grid, cells_touching(held), cells_touching(held | loaded) | pres, reuse=reuse)
     counted = ~cells_touching(held | loaded)
     nc = max(int(counted.sum()), 1) * 8
-    load_size = float(np.linalg.norm(f_grid.reshape(3, -1), axis=0).sum())
+    load_size = [float(np.linalg.norm(f.reshape(3, -1), axis=0).sum()) for f in fs]
+    defl_cases = [c for c in range(len(fs)) if deflection_limit is not None and load_size[c] > 0]
+    stress_cases = list(range(len(fs))) if stress_limit is not None else []
     cbs = corner_stress_ops(nu, pitch, element)
     sym = (lambda v: mirror_average(v, mirror)) if mirror else (lambda v: v)   # noqa: E731
     x = np.full(dims, vf0)
     x[pres] = 1.0
-    mma = MMA(len(free), int(deflection_limit is not None) + int(stress_limit is not None), 0.0, 1.0,
-              move=min(move, 0.1))
+    mma = MMA(len(free), len(defl_cases) + len(stress_cases), 0.0, 1.0, move=min(move, 0.1))
     move_cap = mma.move
-    worst_prev, kappa, beta, since_beta = np.inf, 1.0, 1.0, 0
+    worst_prev, kappa, beta, since_beta = np.inf, [1.0] * len(fs), 1.0, 0
     best, trail, recs, converged = None, [], [], False
     for it in range(1, iters + 1):
         x_now = x
@@ -1242,17 +1246,18 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
         dpe[pres] = 0.0
         e = emin + xe ** penal * (1 - emin)
         de = penal * xe ** (penal - 1) * (1 - emin)
-        u = system.solve(e, xe, f_grid)
+        us = system.solve(e, xe, fs)
         to_x = lambda g: hap(g * dpe / hs)   # noqa: E731
-        ue = gather_cells(u, dims).reshape(24, -1)
-        ce = np.einsum("in,in->n", ue, ke @ ue).reshape(dims)
-        comp = float(np.sum(f_grid * u))
-        defl = comp / (load_size * modulus)
-        cons, grads, smax = [], [], np.nan
-        if deflection_limit is not None:
+        ues = [gather_cells(u, dims).reshape(24, -1) for u in us]
+        cons, grads, defls, stresses = [], [], [], []
+        for c in defl_cases:
+            ce = np.einsum("in,in->n", ues[c], ke @ ues[c]).reshape(dims)
+            defl = float(np.sum(fs[c] * us[c])) / (load_size[c] * modulus)
             cons.append(defl / deflection_limit - 1.0)
-            grads.append(to_x(-de * ce / (load_size * modulus)) / deflection_limit)
-        if stress_limit is not None:
+            grads.append(to_x(-de * ce / (load_size[c] * modulus)) / deflection_limit)
+            defls.append(defl)
+        for c in stress_cases:
+            ue = ues[c]
             moved = np.any(ue != 0, axis=0)
             act = (moved & counted.reshape(-1))
             xa = xe.reshape(-1)[act]
@@ -1267,12 +1272,12 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
             sc = max(smax, 1e-30)
             pm = sc * (sum(float(np.sum((p[3] / sc) ** 8)) for p in parts) / nc) ** (1.0 / 8)
             kk = smax / max(pm, 1e-30)
-            kappa = 0.5 * (kappa + kk) if it > 1 else kk
-            g = kappa * pm
+            kappa[c] = 0.5 * (kappa[c] + kk) if it > 1 else kk
+            g = kappa[c] * pm
             g_xe = np.zeros(ue.shape[1])
             fe = np.zeros((24, ue.shape[1]))
             for cbk, sv, vm, srel in parts:
-                dg_ds = kappa * (srel / max(pm, 1e-30)) ** 7 / nc
+                dg_ds = kappa[c] * (srel / max(pm, 1e-30)) ** 7 / nc
                 g_xe[act] += dg_ds * (vm / stress_limit)
                 fe[:, act] += (dg_ds * (xa / (vm * stress_limit)))[None, :] * (cbk.T @ sv)
             rhs = scatter_cell_vectors(fe.reshape((24,) + dims), dims)
@@ -1282,6 +1287,7 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
             g_xe[moved] -= de.reshape(-1)[moved] * np.einsum("in,in->n", le, ke @ ue)[moved]
             cons.append(g - 1.0)
             grads.append(to_x(g_xe.reshape(dims)))
+            stresses.append(smax * stress_limit)
 
         f0 = 10.0 * float(xp[design].mean())
         df0 = sym(hap(10.0 * design / design.sum() * dpb / hs))
@@ -1302,8 +1308,8 @@ def constrained_loop(dims, nu, fixed_grid, f_grid, vf0, radius, iters, stress_li
         x = xnew
         since_beta += 1
         rec = dict(volume=float(xp[design].mean()), beta=beta, change=change, constraints=list(cons),
-                   deflection=defl if deflection_limit is not None else np.nan,
-                   stress=smax * stress_limit if stress_limit is not None else np.nan, xphys=xp)
+                   deflection=defls[0] if defls else np.nan, stress=stresses[0] if stresses else np.nan,
+                   deflections=defls, stresses=stresses, xphys=xp)
         recs.append(rec)
         feasible = max(cons) <= 0.02
         if beta < beta_max and ((feasible and (since_beta >= beta_every or change < 2 * tol))

@@ -420,8 +420,10 @@ def make_constrained():
     beta continuation) on top3d cantilevers (domain_for), from a uniform 0.5, solves at rtol
     1e-10: both limits on the 12x4x6 one for 40 iterations (constrained.npz), a deflection limit
     alone and a stress limit alone on a 16x4x8 one for 30 (constrained_deflection.npz,
-    constrained_stress.npz), and both limits with beta_max 4 run to the loop's own stop
-    (constrained_converge.npz: the lightest feasible design delivered). Stored: the domain, the limits, and per iteration the
+    constrained_stress.npz), both limits with beta_max 4 run to the loop's own stop
+    (constrained_converge.npz: the lightest feasible design delivered), and both limits on two
+    load cases, the second an axial pull on the loaded nodes (constrained_twocase.npz: four
+    constraints). Stored: the domain, the limits, and per iteration the
     record (volume, beta, change, constraints, deflection and stress readings, solved cells) and
     the blueprint; and the last design."""
     os.environ["LOADPATH_HEX8"] = "im"
@@ -434,7 +436,8 @@ def make_constrained():
                                          ("_deflection", (16, 4, 8), 30, Limits(None, 0.5, 1000.0), {}),
                                          ("_stress", (16, 4, 8), 30, Limits(9.0, None, 1000.0), {}),
                                          ("_converge", (12, 4, 6), 100, Limits(12.0, 0.6, 1000.0),
-                                          {"beta_max": 4.0})):
+                                          {"beta_max": 4.0}),
+                                         ("_twocase", (12, 4, 6), 30, Limits(12.0, 0.6, 1000.0), {})):
         _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, tag, dims, iters, lim, extra)
 
 
@@ -443,6 +446,16 @@ def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, ta
     dom, _ = domain_for(p)
     mesh = dom.mesh
     assert mesh.n_elem == int(np.prod(dims)) and len(dom.loads) == 1
+    f_second = None
+    if tag == "_twocase":
+        # a second case on the same nodes, an axial pull (its own deflection and stress limits)
+        f_second = np.zeros_like(dom.loads[0])
+        on = np.flatnonzero(dom.loads[0].reshape(-1, 3).any(axis=1))
+        f_second[3 * on] = 0.8
+        dom.loads = [dom.loads[0], f_second]
+        dom.case_weights = [1.0, 0.5]
+        dom.spreads = [None, None]
+        dom.case_names = ["down", "pull"]
     opts = S.SimpOptions(volume_fraction=0.5, filter_radius=p.rmin, max_iterations=iters, solve_rtol=1e-10, **extra)
     recs, xps = [], []
     res = optimize_constrained(dom, NU, opts, lim, on_iter=lambda r, xp: (recs.append(r), xps.append(np.array(xp))))
@@ -474,6 +487,13 @@ def _constrained_case(S, cantilever_3d, NU, domain_for, optimize_constrained, ta
                contact=grid((dom.support_nodes | dom.load_nodes)[mesh.enode].any(axis=1)),
                beta_max=float(opts.beta_max), max_iterations=int(iters),
                delivered_iteration=int(res.delivered["iteration"]) if res.delivered else -1)
+    if f_second is not None:
+        f2 = np.zeros((3, *nxyz))
+        for c in range(3):
+            f2[c][nijk] = f_second[c::3]
+        out["f2"] = f2
+        out["deflection_cases"] = np.array([[r.get(f"deflection.{n}", np.nan) for n in dom.case_names] for r in recs])
+        out["stress_cases"] = np.array([[r.get(f"stress.{n}", np.nan) for n in dom.case_names] for r in recs])
     for k in ("volume", "beta", "change", "solvedCells"):
         out[k] = np.array([float(r[k]) for r in recs])
     np.savez_compressed(os.path.join(HERE, f"constrained{tag}.npz"), **out)

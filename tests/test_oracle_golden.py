@@ -291,13 +291,14 @@ def test_oracle_optimize_loop_matches_reference_run(case):
         assert k("solvedCells")[-1] < np.prod(dims)
 
 
-@pytest.mark.parametrize("tag", ["", "_deflection", "_stress", "_converge"])
+@pytest.mark.parametrize("tag", ["", "_deflection", "_stress", "_converge", "_twocase"])
 def test_oracle_constrained_loop_matches_reference_run(tag):
     """The oracle's restatement of loadpath's minimum-mass loop under stress and deflection limits
     (constrained_loop) against the reference's own optimize_constrained on the 12x4x6 cantilever
     (tests/golden/constrained.npz, 40 iterations, beta 1 to 8, the last ones on a reduced system
     the direct path reuses; a deflection limit or a stress limit alone on a 16x4x8 cantilever,
-    30 iterations; and both limits with beta_max 4, run to the loop's own stop): every iteration's
+    30 iterations; both limits with beta_max 4, run to the loop's own stop; and both limits on two
+    load cases, four constraints): every iteration's
     constraints, readings, volume, change and blueprint, and the delivered design (the last one,
     or the lightest feasible one at beta_max); and the cells whose stress is not counted."""
     g = _load(f"constrained{tag}.npz")
@@ -306,7 +307,8 @@ def test_oracle_constrained_loop_matches_reference_run(tag):
     held = g["fixed"].any(axis=0)
     loaded = (g["f"] != 0).any(axis=0)
     np.testing.assert_array_equal(R.cells_touching(held | loaded), g["contact"])
-    recs, x, conv = R.constrained_loop(dims, float(g["nu"]), g["fixed"], g["f"], float(g["volfrac"]),
+    loads = [g["f"], g["f2"]] if "f2" in g.files else g["f"]
+    recs, x, conv = R.constrained_loop(dims, float(g["nu"]), g["fixed"], loads, float(g["volfrac"]),
                                        float(g["radius"]), int(g["max_iterations"]), lim("stress_limit"),
                                        lim("deflection_limit"), float(g["modulus"]), pres=g["pres"],
                                        pad=bool(g["pad"]), pitch=float(g["pitch"]),
@@ -318,6 +320,9 @@ def test_oracle_constrained_loop_matches_reference_run(tag):
     for key in ("deflection", "stress", "volume"):
         np.testing.assert_allclose(col(key), g[key], rtol=1e-10, equal_nan=True)
     np.testing.assert_allclose(col("change"), g["change"], rtol=0, atol=1e-10)
+    if "f2" in g.files:
+        np.testing.assert_allclose([r["deflections"] for r in recs], g["deflection_cases"], rtol=1e-10)
+        np.testing.assert_allclose([r["stresses"] for r in recs], g["stress_cases"], rtol=1e-10)
     np.testing.assert_allclose(np.stack([r["xphys"] for r in recs]), g["xphys"], rtol=0, atol=1e-10)
     np.testing.assert_allclose(x, g["x_last"], rtol=0, atol=1e-10)
     if tag == "":
