@@ -188,8 +188,33 @@ class Clocks:
 
 
 # ---- CPU baseline: the oracle's C port of the reference's two-pass CPU operator ---------------
+def level1_apply(e, m, ke):
+    """The C port's level-1 (weights) operator of the reference's hierarchy for cell moduli e and
+    the fine mask m (x = 0 face held): the first Galerkin coarsening of the oracle (the children's
+    moduli as weights, the cells touching held nodes as explicit patch matrices), its mask from
+    its diagonal (loadpath/mg.py:601-677, :560-591), formed without the dense per-cell matrices."""
+    from oracle import cport
+    from oracle import ref_numpy as R
+
+    dims = e.shape
+    l0 = R.Level("scaled", dims, np.float64)
+    l0.ke, l0.e, l0.mask = ke, e, m
+    h = R.Hierarchy(ke, dims, m == 0, dtype=np.float32)
+    h.alive = np.ones(m.shape, bool)
+    l1 = h.coarsen(l0, first=True)
+    dm = np.einsum("kii->ki", np.asarray(l1.mcat, np.float64).reshape(8, 24, 24))
+    d = R.scatter_cells((dm.T @ l1.w.reshape(8, -1).astype(np.float64)).reshape((24,) + l1.dims),
+                        np.zeros(l1.node_shape))
+    if l1.patch_ijk is not None and len(l1.patch_ijk):
+        np.add.at(d.reshape(-1), l1.patch_index().ravel(),
+                  np.einsum("nii->ni", np.asarray(l1.patch_k, np.float64)).ravel())
+    l1.mask = (d > 1e-12 * d.max()).astype(np.float32)
+    return cport.WeightsApply(l1), l1.node_shape
+
+
 def cpu_apply_times(dims, reps64=3, reps32=3):
-    """Seconds per fine-level apply (float64, float32) of the C port on all host cores."""
+    """Seconds per fine-level apply (float64, float32) and per level-1 apply (float32) of the C
+    port on all host cores."""
     from oracle import cport
     from oracle import ref_numpy as R
 
@@ -210,6 +235,14 @@ def cpu_apply_times(dims, reps64=3, reps32=3):
         for _ in range(reps):
             op(uu, o)
         out[np.dtype(dt).name] = (time.perf_counter() - t0) / reps
+    op1, shape1 = level1_apply(e, m, ke)
+    u1 = rng.standard_normal(shape1).astype(np.float32)
+    o1 = np.empty_like(u1)
+    op1(u1, o1)
+    t0 = time.perf_counter()
+    for _ in range(reps32):
+        op1(u1, o1)
+    out["level1"] = (time.perf_counter() - t0) / reps32
     return out, cport.threads()
 
 
@@ -232,20 +265,22 @@ def fine_applies(cg_iters):
 
 def cpu_iteration_estimate(dims, n64, n32):
     t, cores = cpu_apply_times(dims)
-    sec = n64 * t["float64"] + n32 * t["float32"]
+    sec = n64 * t["float64"] + n32 * (t["float32"] + t["level1"])
     return {"value": 1.0 / sec, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
-            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) on {cores} threads, "
-                       f"3 applies per precision: {t['float64'] * 1e3:.1f} ms per float64 and "
-                       f"{t['float32'] * 1e3:.1f} ms per float32 fine-level apply at {dims[0]}x{dims[1]}x{dims[2]}, "
-                       f"scaled to the {n64} float64 + {n32} float32 fine applies one SIMP iteration makes; coarse "
-                       "levels, setup, filter and OC not counted (a lower bound on the CPU iteration time)")}
+            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) and of its level-1 "
+                       f"operator on {cores} threads, 3 applies each: {t['float64'] * 1e3:.1f} ms per float64 and "
+                       f"{t['float32'] * 1e3:.1f} ms per float32 fine-level apply, {t['level1'] * 1e3:.1f} ms per "
+                       f"level-1 apply at {dims[0]}x{dims[1]}x{dims[2]}, scaled to the {n64} float64 + {n32} float32 "
+                       f"fine and {n32} level-1 applies one SIMP iteration makes; deeper levels, transfers, setup, "
+                       "filter and OC not counted (a lower bound on the CPU iteration time)")}
 
 
 def run_reference(args):
-    """The reference arm: every fine-level apply one SIMP iteration of the workload makes
-    (its solve's float64 CG applies and float32 V-cycle and power-iteration applies), executed
-    by the oracle's C port of the reference's CPU operator on all host cores, per step. Coarse
-    levels, setup, filter and OC are not run (a lower bound on the reference's CPU time)."""
+    """The reference arm: every fine-level and level-1 apply one SIMP iteration of the workload
+    makes (its solve's float64 CG applies, float32 V-cycle and power-iteration applies on the fine
+    level and as many on level 1), executed by the oracle's C port of the reference's CPU
+    operators on all host cores, per step. Deeper levels, transfers, setup, filter and OC are not
+    run (a lower bound on the reference's CPU time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -266,12 +301,17 @@ def run_reference(args):
         op = cport.MaskedApply(ke, e, m, dt)
         uu = u.astype(dt)
         ops[dt] = (op, uu, np.empty_like(uu))
+    op1, shape1 = level1_apply(e, m, ke)
+    u1 = rng.standard_normal(shape1).astype(np.float32)
+    o1 = np.empty_like(u1)
 
     def step():
         for dt, n in ((np.float64, n64), (np.float32, n32)):
             op, uu, o = ops[dt]
             for _ in range(n):
                 op(uu, o)
+        for _ in range(n32):
+            op1(u1, o1)
 
     for _ in range(args.warmup):
         step()
@@ -282,11 +322,11 @@ def run_reference(args):
     v = 1.0 / sec
     cores = cport.threads()
     cb = {"value": v, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
-          "sample": (f"per step, the {n64} float64 + {n32} float32 fine-level applies one SIMP iteration of the "
-                     f"workload makes ({CG_REFERENCE_256} CG iterations, the reference's own count on this design), "
-                     f"executed by the C port of the reference's two-pass CPU operator (loadpath/mgops.py) on "
-                     f"{cores} threads at {nx}x{ny}x{nz}; coarse levels, setup, filter and OC not run (a lower "
-                     "bound on the CPU iteration time)")}
+          "sample": (f"per step, the {n64} float64 + {n32} float32 fine-level applies and {n32} level-1 applies "
+                     f"one SIMP iteration of the workload makes ({CG_REFERENCE_256} CG iterations, the reference's "
+                     f"own count on this design), executed by the C port of the reference's two-pass CPU operators "
+                     f"(loadpath/mgops.py, loadpath/mg.py) on {cores} threads at {nx}x{ny}x{nz}; deeper levels, "
+                     "transfers, setup, filter and OC not run (a lower bound on the CPU iteration time)")}
     line = {"metric": METRIC, "value": v, "unit": "SIMP iter/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",

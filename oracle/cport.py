@@ -19,6 +19,10 @@ def lib():
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [ctypes.c_void_p]
         _LIB.lpo_threads.restype = ctypes.c_int
+        fn = _LIB.lpo_apply_weights_f32
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2 + [ctypes.c_longlong,
+                                                                                           ctypes.c_void_p]
     return _LIB
 
 
@@ -45,4 +49,30 @@ class MaskedApply:
         nx, ny, nz = self.dims
         self.fn(out.ctypes.data, u.ctypes.data, self.e.ctypes.data, self.m.ctypes.data, self.ke.ctypes.data,
                 nx, ny, nz, self.ft.ctypes.data)
+        return out
+
+
+class WeightsApply:
+    """The level-1 ("weights") operator out = m K1 (m u) + (1 - m) u of the reference's hierarchy
+    in float32 (loadpath/mg.py:213-230, :251-276, :317-346), from an oracle Level of kind
+    "weights" (its w, mcat, patch cells and mask)."""
+
+    def __init__(self, level):
+        assert level.kind == "weights"
+        self.dims = tuple(level.dims)
+        self.w = np.ascontiguousarray(level.w.reshape(8, -1), np.float32)
+        self.mcat = np.ascontiguousarray(np.asarray(level.mcat, np.float64).reshape(8, 24, 24))
+        self.m = np.ascontiguousarray(level.mask, np.float32)
+        has_patch = level.patch_ijk is not None and len(level.patch_ijk)
+        self.pidx = np.ascontiguousarray(level.patch_index() if has_patch else np.zeros((0, 24)), np.int64)
+        self.pk = np.ascontiguousarray(level.patch_k if has_patch else np.zeros((0, 24, 24)), np.float32)
+        self.ft = np.empty((24, int(np.prod(self.dims))), np.float32)
+
+    def __call__(self, u, out=None):
+        u = np.ascontiguousarray(u, np.float32)
+        out = np.empty_like(u) if out is None else out
+        nx, ny, nz = self.dims
+        lib().lpo_apply_weights_f32(out.ctypes.data, u.ctypes.data, self.w.ctypes.data, self.mcat.ctypes.data,
+                                    self.m.ctypes.data, nx, ny, nz, self.pidx.ctypes.data, self.pk.ctypes.data,
+                                    len(self.pidx), self.ft.ctypes.data)
         return out

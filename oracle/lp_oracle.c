@@ -91,3 +91,83 @@ int lpo_threads(void) {
 #endif
   return n;
 }
+
+/* lpo_apply_weights_f32: the level-1 ("weights") operator of the reference's hierarchy,
+ * out = m * K1 (m * u) + (1 - m) * u on the coarse node grid, K1 = sum over cells of
+ * sum_k w[k, c] M_k (M_k = P_k^T ke P_k, the eight children's Galerkin matrices) plus the patch
+ * cells' explicit matrices (loadpath/mg.py:213-230, :251-276, :317-346; loadpath/mgops.py:247-261):
+ * a product pass over blocks of cells (the masked corner values gathered once, the eight
+ * children's products weighted and summed), the node pass, the patch cells' products added
+ * node by node (serially, in the patch list's order), then the mask finish.
+ * w: (8, cells) in C order over (x, y, z); mcat64: (8, 24, 24); pidx: (np, 24) flat
+ * (component nn + node) dof indices of the patch cells; pk: (np, 24, 24). */
+int lpo_apply_weights_f32(float* out, const float* u, const float* w, const double* mcat64, const float* m,
+                          int nx, int ny, int nz, const long long* pidx, const float* pk, long long np,
+                          float* ft) {
+  const long long NX = nx + 1, NY = ny + 1, NZ = nz + 1;
+  const long long nn = NX * NY * NZ, ncell = (long long)nx * ny * nz;
+  float mk[8 * 576];
+  for (int i = 0; i < 8 * 576; ++i) mk[i] = (float)mcat64[i];
+  long long off[24];
+  for (int k = 0; k < 8; ++k)
+    for (int d = 0; d < 3; ++d) off[3 * k + d] = d * nn + (k & 1) * NY * NZ + ((k >> 1) & 1) * NZ + ((k >> 2) & 1);
+  const long long nblk = (ncell + BLOCK - 1) / BLOCK;
+#pragma omp parallel for schedule(static)
+  for (long long b = 0; b < nblk; ++b) {
+    float ubt[24][BLOCK], g[BLOCK];
+    long long c0 = b * BLOCK;
+    int cnt = (int)((ncell - c0) < BLOCK ? (ncell - c0) : BLOCK);
+    long long base[BLOCK];
+    for (int c = 0; c < cnt; ++c) {
+      long long cell = c0 + c;
+      long long z = cell % nz, y = (cell / nz) % ny, x = cell / ((long long)nz * ny);
+      base[c] = (x * NY + y) * NZ + z;
+    }
+    for (int i = 0; i < 24; ++i)
+      for (int c = 0; c < cnt; ++c) {
+        long long k = base[c] + off[i];
+        ubt[i][c] = u[k] * m[k];
+      }
+    for (int i = 0; i < 24; ++i) {
+      float* fr = ft + (long long)i * ncell + c0;
+      for (int c = 0; c < cnt; ++c) fr[c] = 0.0f;
+      for (int k = 0; k < 8; ++k) {
+        const float* wk = w + (long long)k * ncell + c0;
+        for (int c = 0; c < cnt; ++c) g[c] = 0.0f;
+        for (int j = 0; j < 24; ++j) {
+          float kij = mk[(k * 24 + i) * 24 + j];
+          for (int c = 0; c < cnt; ++c) g[c] += kij * ubt[j][c];
+        }
+        for (int c = 0; c < cnt; ++c) fr[c] += g[c] * wk[c];
+      }
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (long long xy = 0; xy < NX * NY; ++xy) {
+    long long x = xy / NY, y = xy % NY;
+    for (long long z = 0; z < NZ; ++z) {
+      float a[3] = {0, 0, 0};
+      for (int k = 0; k < 8; ++k) {
+        long long cx = x - (k & 1), cy = y - ((k >> 1) & 1), cz = z - ((k >> 2) & 1);
+        if (cx < 0 || cy < 0 || cz < 0 || cx >= nx || cy >= ny || cz >= nz) continue;
+        long long r = (cx * ny + cy) * nz + cz;
+        for (int d = 0; d < 3; ++d) a[d] += ft[(long long)(3 * k + d) * ncell + r];
+      }
+      long long n = (x * NY + y) * NZ + z;
+      for (int d = 0; d < 3; ++d) out[d * nn + n] = a[d];
+    }
+  }
+  for (long long p = 0; p < np; ++p) {
+    const long long* id = pidx + p * 24;
+    float ue[24];
+    for (int j = 0; j < 24; ++j) ue[j] = u[id[j]] * m[id[j]];
+    for (int i = 0; i < 24; ++i) {
+      float s = 0.0f;
+      for (int j = 0; j < 24; ++j) s += pk[(p * 24 + i) * 24 + j] * ue[j];
+      out[id[i]] += s;
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < 3 * nn; ++i) out[i] = out[i] * m[i] + (1.0f - m[i]) * u[i];
+  return 0;
+}

@@ -193,6 +193,20 @@ def test_c_port_apply_matches_golden(name):
     np.testing.assert_allclose(op32(g["L0_u"]), want, rtol=2e-5, atol=2e-5 * np.abs(want).max())
 
 
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_c_port_weights_apply_matches_golden(name):
+    """The oracle's C port of the reference's level-1 (weights) operator, patch cells included
+    (the reference arm's level-1 applies), gives the reference's level-1 operator in float32."""
+    from oracle import cport
+
+    g, h = _hierarchy(name)
+    if len(h.levels) < 2 or h.levels[1].kind != "weights":
+        pytest.skip("no weights level in this hierarchy")
+    op = cport.WeightsApply(h.levels[1])
+    want = g["L1_apply"]
+    np.testing.assert_allclose(op(g["L1_u"]), want, rtol=2e-5, atol=2e-5 * np.abs(want).max())
+
+
 def test_projection_matches_reference():
     g = _load("filter.npz")
     for beta in (1.0, 8.0):
