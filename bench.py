@@ -209,7 +209,23 @@ def level1_apply(e, m, ke):
         np.add.at(d.reshape(-1), l1.patch_index().ravel(),
                   np.einsum("nii->ni", np.asarray(l1.patch_k, np.float64)).ravel())
     l1.mask = (d > 1e-12 * d.max()).astype(np.float32)
-    return cport.WeightsApply(l1), l1.node_shape
+    return cport.WeightsApply(l1), l1.node_shape, l1.mask
+
+
+def transfer_step(m, cm, rng):
+    """One V-cycle's transfers between the fine level and level 1 in the C port: the restriction
+    of the residual and the prolongation of the correction, on seeded fields."""
+    from oracle import cport
+
+    m32 = np.ascontiguousarray(m, np.float32)
+    b, ax, x = (rng.standard_normal(m.shape).astype(np.float32) for _ in range(3))
+    xc = rng.standard_normal(cm.shape).astype(np.float32)
+    rc = np.empty(cm.shape, np.float32)
+
+    def run():
+        cport.coarse_residual(b, ax, m32, cm, rc)
+        cport.add_correction(xc, cm, m32, x)
+    return run
 
 
 def cpu_apply_times(dims, reps64=3, reps32=3):
@@ -235,7 +251,7 @@ def cpu_apply_times(dims, reps64=3, reps32=3):
         for _ in range(reps):
             op(uu, o)
         out[np.dtype(dt).name] = (time.perf_counter() - t0) / reps
-    op1, shape1 = level1_apply(e, m, ke)
+    op1, shape1, cm = level1_apply(e, m, ke)
     u1 = rng.standard_normal(shape1).astype(np.float32)
     o1 = np.empty_like(u1)
     op1(u1, o1)
@@ -243,6 +259,12 @@ def cpu_apply_times(dims, reps64=3, reps32=3):
     for _ in range(reps32):
         op1(u1, o1)
     out["level1"] = (time.perf_counter() - t0) / reps32
+    tr = transfer_step(m, cm, rng)
+    tr()
+    t0 = time.perf_counter()
+    for _ in range(reps32):
+        tr()
+    out["transfers"] = (time.perf_counter() - t0) / reps32
     return out, cport.threads()
 
 
@@ -265,22 +287,25 @@ def fine_applies(cg_iters):
 
 def cpu_iteration_estimate(dims, n64, n32):
     t, cores = cpu_apply_times(dims)
-    sec = n64 * t["float64"] + n32 * (t["float32"] + t["level1"])
+    nv = (n32 - 12) // 4   # V-cycles (four float32 fine applies each besides the 12 power iterations)
+    sec = n64 * t["float64"] + n32 * (t["float32"] + t["level1"]) + nv * t["transfers"]
     return {"value": 1.0 / sec, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
-            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py) and of its level-1 "
-                       f"operator on {cores} threads, 3 applies each: {t['float64'] * 1e3:.1f} ms per float64 and "
-                       f"{t['float32'] * 1e3:.1f} ms per float32 fine-level apply, {t['level1'] * 1e3:.1f} ms per "
-                       f"level-1 apply at {dims[0]}x{dims[1]}x{dims[2]}, scaled to the {n64} float64 + {n32} float32 "
-                       f"fine and {n32} level-1 applies one SIMP iteration makes; deeper levels, transfers, setup, "
-                       "filter and OC not counted (a lower bound on the CPU iteration time)")}
+            "sample": (f"C port of the reference's two-pass CPU operator (loadpath/mgops.py), of its level-1 "
+                       f"operator and of its fine-level transfers on {cores} threads, 3 runs each: "
+                       f"{t['float64'] * 1e3:.1f} ms per float64 and {t['float32'] * 1e3:.1f} ms per float32 "
+                       f"fine-level apply, {t['level1'] * 1e3:.1f} ms per level-1 apply, "
+                       f"{t['transfers'] * 1e3:.1f} ms per V-cycle's transfers at {dims[0]}x{dims[1]}x{dims[2]}, "
+                       f"scaled to the {n64} float64 + {n32} float32 fine and {n32} level-1 applies and {nv} V-cycles "
+                       "one SIMP iteration makes; deeper levels, vector passes, setup, filter and OC not counted "
+                       "(a lower bound on the CPU iteration time)")}
 
 
 def run_reference(args):
     """The reference arm: every fine-level and level-1 apply one SIMP iteration of the workload
     makes (its solve's float64 CG applies, float32 V-cycle and power-iteration applies on the fine
-    level and as many on level 1), executed by the oracle's C port of the reference's CPU
-    operators on all host cores, per step. Deeper levels, transfers, setup, filter and OC are not
-    run (a lower bound on the reference's CPU time)."""
+    level and as many on level 1) and its V-cycles' fine-level transfers, executed by the oracle's
+    C port of the reference's CPU operators on all host cores, per step. Deeper levels, vector
+    passes, setup, filter and OC are not run (a lower bound on the reference's CPU time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -301,9 +326,11 @@ def run_reference(args):
         op = cport.MaskedApply(ke, e, m, dt)
         uu = u.astype(dt)
         ops[dt] = (op, uu, np.empty_like(uu))
-    op1, shape1 = level1_apply(e, m, ke)
+    op1, shape1, cm = level1_apply(e, m, ke)
     u1 = rng.standard_normal(shape1).astype(np.float32)
     o1 = np.empty_like(u1)
+    tr = transfer_step(m, cm, rng)
+    nv = (n32 - 12) // 4
 
     def step():
         for dt, n in ((np.float64, n64), (np.float32, n32)):
@@ -312,6 +339,8 @@ def run_reference(args):
                 op(uu, o)
         for _ in range(n32):
             op1(u1, o1)
+        for _ in range(nv):
+            tr()
 
     for _ in range(args.warmup):
         step()
@@ -322,11 +351,12 @@ def run_reference(args):
     v = 1.0 / sec
     cores = cport.threads()
     cb = {"value": v, "unit": "SIMP iter/s", "cores": cores, "kind": "port",
-          "sample": (f"per step, the {n64} float64 + {n32} float32 fine-level applies and {n32} level-1 applies "
-                     f"one SIMP iteration of the workload makes ({CG_REFERENCE_256} CG iterations, the reference's "
-                     f"own count on this design), executed by the C port of the reference's two-pass CPU operators "
-                     f"(loadpath/mgops.py, loadpath/mg.py) on {cores} threads at {nx}x{ny}x{nz}; deeper levels, "
-                     "transfers, setup, filter and OC not run (a lower bound on the CPU iteration time)")}
+          "sample": (f"per step, the {n64} float64 + {n32} float32 fine-level applies, {n32} level-1 applies and "
+                     f"the fine-level transfers of {nv} V-cycles one SIMP iteration of the workload makes "
+                     f"({CG_REFERENCE_256} CG iterations, the reference's own count on this design), executed by the "
+                     f"C port of the reference's CPU operators and transfers (loadpath/mgops.py, loadpath/mg.py) on "
+                     f"{cores} threads at {nx}x{ny}x{nz}; deeper levels, vector passes, setup, filter and OC not run "
+                     "(a lower bound on the CPU iteration time)")}
     line = {"metric": METRIC, "value": v, "unit": "SIMP iter/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",

@@ -19,6 +19,10 @@ def lib():
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [ctypes.c_void_p]
         _LIB.lpo_threads.restype = ctypes.c_int
+        for name in ("lpo_coarse_residual_f32", "lpo_add_correction_f32"):
+            f_ = getattr(_LIB, name)
+            f_.restype = ctypes.c_int
+            f_.argtypes = [ctypes.c_void_p] * (5 if name == "lpo_coarse_residual_f32" else 4) + [ctypes.c_int] * 6
         fn = _LIB.lpo_apply_weights_f32
         fn.restype = ctypes.c_int
         fn.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2 + [ctypes.c_longlong,
@@ -76,3 +80,21 @@ class WeightsApply:
                                     self.m.ctypes.data, nx, ny, nz, self.pidx.ctypes.data, self.pk.ctypes.data,
                                     len(self.pidx), self.ft.ctypes.data)
         return out
+
+
+def coarse_residual(b, ax, m, cm, out=None):
+    """rc = cm * R((b - ax) * m) in float32 (the C port of loadpath/mgops.py:753-763)."""
+    b, ax, m, cm = (np.ascontiguousarray(a, np.float32) for a in (b, ax, m, cm))
+    out = np.empty(cm.shape, np.float32) if out is None else out
+    lib().lpo_coarse_residual_f32(out.ctypes.data, b.ctypes.data, ax.ctypes.data, m.ctypes.data, cm.ctypes.data,
+                                  *b.shape[1:], *cm.shape[1:])
+    return out
+
+
+def add_correction(xc, cm, m, x):
+    """x += m * P(cm * xc) in float32, in place (the C port of loadpath/mgops.py:766-773)."""
+    xc, cm, m = (np.ascontiguousarray(a, np.float32) for a in (xc, cm, m))
+    assert x.dtype == np.float32 and x.flags.c_contiguous
+    lib().lpo_add_correction_f32(x.ctypes.data, xc.ctypes.data, cm.ctypes.data, m.ctypes.data, *x.shape[1:],
+                                 *cm.shape[1:])
+    return x

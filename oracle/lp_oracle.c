@@ -171,3 +171,65 @@ int lpo_apply_weights_f32(float* out, const float* u, const float* w, const doub
   for (long long i = 0; i < 3 * nn; ++i) out[i] = out[i] * m[i] + (1.0f - m[i]) * u[i];
   return 0;
 }
+
+/* lpo_coarse_residual_f32 / lpo_add_correction_f32: the V-cycle's transfers between a level and
+ * the next coarser one in float32 (loadpath/mgops.py:666-711, :753-773). The coarse residual
+ * rc = cm * R((b - ax) * m), R the transpose of trilinear prolongation over the fine nodes (a
+ * coarse node sums the fine nodes within one step of its fine twin, weights 1, 1/2, 1/4, 1/8 by
+ * the number of odd offsets; fine nodes past the fine grid count zero); the correction
+ * x += m * P(cm * xc), a fine node taking its one to eight coarse neighbours' values at those
+ * weights. Fields (3, n0, n1, n2) in C order; fine (3, F0, F1, F2), coarse (3, C0, C1, C2). */
+int lpo_coarse_residual_f32(float* rc, const float* b, const float* ax, const float* m, const float* cm,
+                            int F0, int F1, int F2, int C0, int C1, int C2) {
+  const long long nf = (long long)F0 * F1 * F2, nc = (long long)C0 * C1 * C2;
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < 3 * nc; ++t) {
+    const long long d = t / nc, r = t % nc;
+    const long long I = r / ((long long)C1 * C2), J = (r / C2) % C1, K = r % C2;
+    float s = 0.0f;
+    for (int di = -1; di <= 1; ++di) {
+      const long long i = 2 * I + di;
+      if (i < 0 || i >= F0) continue;
+      for (int dj = -1; dj <= 1; ++dj) {
+        const long long j = 2 * J + dj;
+        if (j < 0 || j >= F1) continue;
+        for (int dk = -1; dk <= 1; ++dk) {
+          const long long k = 2 * K + dk;
+          if (k < 0 || k >= F2) continue;
+          const float w = (di ? 0.5f : 1.0f) * (dj ? 0.5f : 1.0f) * (dk ? 0.5f : 1.0f);
+          const long long f = d * nf + (i * F1 + j) * F2 + k;
+          s += w * ((b[f] - ax[f]) * m[f]);
+        }
+      }
+    }
+    rc[t] = s * cm[t];
+  }
+  return 0;
+}
+
+int lpo_add_correction_f32(float* x, const float* xc, const float* cm, const float* m, int F0, int F1, int F2,
+                           int C0, int C1, int C2) {
+  const long long nf = (long long)F0 * F1 * F2, nc = (long long)C0 * C1 * C2;
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < 3 * nf; ++t) {
+    const long long d = t / nf, r = t % nf;
+    const long long i = r / ((long long)F1 * F2), j = (r / F2) % F1, k = r % F2;
+    const long long i0 = i / 2, j0 = j / 2, k0 = k / 2;
+    const int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
+    const float wi = (i & 1) ? 0.5f : 1.0f, wj = (j & 1) ? 0.5f : 1.0f, wk = (k & 1) ? 0.5f : 1.0f;
+    float s = 0.0f;
+    for (int a = 0; a < ni; ++a) {
+      if (i0 + a >= C0) continue;
+      for (int bb = 0; bb < nj; ++bb) {
+        if (j0 + bb >= C1) continue;
+        for (int c = 0; c < nk; ++c) {
+          if (k0 + c >= C2) continue;
+          const long long q = d * nc + ((i0 + a) * C1 + (j0 + bb)) * C2 + (k0 + c);
+          s += wi * wj * wk * (xc[q] * cm[q]);
+        }
+      }
+    }
+    x[t] += s * m[t];
+  }
+  return 0;
+}

@@ -207,6 +207,23 @@ def test_c_port_weights_apply_matches_golden(name):
     np.testing.assert_allclose(op(g["L1_u"]), want, rtol=2e-5, atol=2e-5 * np.abs(want).max())
 
 
+@pytest.mark.parametrize("name", sorted(COARSE_CELLS))
+def test_c_port_transfers_match_golden(name):
+    """The oracle's C port of the reference's V-cycle transfers (the reference arm's restriction
+    of the residual and prolongation of the correction) against the reference's float32 outputs."""
+    from oracle import cport
+
+    g, h = _hierarchy(name)
+    if "t_b" not in g:
+        pytest.skip("a single-level hierarchy")
+    lv, nxt = h.op(0), h.op(1)
+    rc = cport.coarse_residual(g["t_b"], g["t_ax"], lv.mask, nxt.mask)
+    np.testing.assert_allclose(rc, g["t_coarse_residual"], rtol=1e-6, atol=1e-6)
+    x = np.ascontiguousarray(g["t_x"], np.float32).copy()
+    cport.add_correction(g["t_xc"], nxt.mask, lv.mask, x)
+    np.testing.assert_allclose(x, g["t_add_correction"], rtol=1e-6, atol=1e-6)
+
+
 def test_projection_matches_reference():
     g = _load("filter.npz")
     for beta in (1.0, 8.0):
